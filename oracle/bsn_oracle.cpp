@@ -1,0 +1,1391 @@
+/*
+ * bsn_oracle.cpp -- CPU FP64 oracle (TEST INFRASTRUCTURE ONLY; see bsn_oracle.h).
+ *
+ * Each function restates one reference function and cites it.  Build flags
+ * (-O2 -ffp-contract=off -fno-fast-math) keep IEEE-754 double arithmetic in the
+ * order written.  OpenMP parallelises only loops whose iterations are
+ * independent and whose per-cell arithmetic is unchanged; every reduction that
+ * the reference sums sequentially is summed sequentially here.
+ */
+#include "bsn_oracle.h"
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cstdlib>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+const int NG = 3;   /* src/BinarySupernova.jl:8 */
+
+/* Julia Base.max/min/clamp for Float64: NaN-propagating, max(+0,-0)=+0,
+ * min(+0,-0)=-0; clamp(x,lo,hi) = x>hi ? hi : x<lo ? lo : x. */
+inline double jmax(double x, double y) {
+    if (x != x || y != y) return x + y;
+    if (x > y) return x;
+    if (y > x) return y;
+    return std::signbit(x) ? y : x;
+}
+inline double jmin(double x, double y) {
+    if (x != x || y != y) return x + y;
+    if (x < y) return x;
+    if (y < x) return y;
+    return std::signbit(x) ? x : y;
+}
+inline double jclamp(double x, double lo, double hi) { return x > hi ? hi : (x < lo ? lo : x); }
+inline double sq(double x) { return x * x; }
+
+/* Julia 1-based indexing helpers for U[q,i,j,k] with extents (5,NXT,NYT,NZT). */
+struct Idx {
+    long nxt, nyt, nzt;
+    Idx(int nx, int ny, int nz) : nxt(nx + 2 * NG), nyt(ny + 2 * NG), nzt(nz + 2 * NG) {}
+    inline long operator()(int q, int i, int j, int k) const {
+        return (long)(q - 1) + 5L * ((long)(i - 1) + nxt * ((long)(j - 1) + nyt * (long)(k - 1)));
+    }
+    long size() const { return 5L * nxt * nyt * nzt; }
+};
+struct FIdx {   /* (5, ex, ey, ez) general */
+    long ex, ey, ez;
+    FIdx(long a, long b, long c) : ex(a), ey(b), ez(c) {}
+    inline long operator()(int q, int i, int j, int k) const {
+        return (long)(q - 1) + 5L * ((long)(i - 1) + ex * ((long)(j - 1) + ey * (long)(k - 1)));
+    }
+    long size() const { return 5L * ex * ey * ez; }
+};
+
+int g_threads = 0;
+
+}  // namespace
+
+extern "C" void orc_set_threads(int n) {
+    g_threads = n;
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#endif
+}
+
+/* ------------------------------------------------------------------------- */
+/* src/weno5.jl:14-21 */
+extern "C" void orc_wenoz_weights(double b0, double b1, double b2, double d0, double d1, double d2,
+                                  double out[3]) {
+    const double eps = 1e-36;
+    double tau5 = std::fabs(b0 - b2);
+    double a0 = d0 * (1.0 + sq(tau5 / (eps + b0)));
+    double a1 = d1 * (1.0 + sq(tau5 / (eps + b1)));
+    double a2 = d2 * (1.0 + sq(tau5 / (eps + b2)));
+    double asum = a0 + a1 + a2;
+    out[0] = a0 / asum; out[1] = a1 / asum; out[2] = a2 / asum;
+}
+
+/* src/weno5.jl:25-41 */
+extern "C" double orc_weno5_left(double vm2, double vm1, double v0, double vp1, double vp2) {
+    double q0 = (1.0 / 3.0) * vm2 + (-7.0 / 6.0) * vm1 + (11.0 / 6.0) * v0;
+    double q1 = (-1.0 / 6.0) * vm1 + (5.0 / 6.0) * v0 + (1.0 / 3.0) * vp1;
+    double q2 = (1.0 / 3.0) * v0 + (5.0 / 6.0) * vp1 + (-1.0 / 6.0) * vp2;
+    double b0 = (13.0 / 12.0) * sq(vm2 - 2.0 * vm1 + v0) + (1.0 / 4.0) * sq(vm2 - 4.0 * vm1 + 3.0 * v0);
+    double b1 = (13.0 / 12.0) * sq(vm1 - 2.0 * v0 + vp1) + (1.0 / 4.0) * sq(vm1 - vp1);
+    double b2 = (13.0 / 12.0) * sq(v0 - 2.0 * vp1 + vp2) + (1.0 / 4.0) * sq(3.0 * v0 - 4.0 * vp1 + vp2);
+    double w[3];
+    orc_wenoz_weights(b0, b1, b2, 1.0 / 10.0, 6.0 / 10.0, 3.0 / 10.0, w);
+    return w[0] * q0 + w[1] * q1 + w[2] * q2;
+}
+
+/* src/weno5.jl:45-61 */
+extern "C" double orc_weno5_right(double vm1, double v0, double vp1, double vp2, double vp3) {
+    double q0 = (-1.0 / 6.0) * vm1 + (5.0 / 6.0) * v0 + (1.0 / 3.0) * vp1;
+    double q1 = (1.0 / 3.0) * v0 + (5.0 / 6.0) * vp1 + (-1.0 / 6.0) * vp2;
+    double q2 = (11.0 / 6.0) * vp1 + (-7.0 / 6.0) * vp2 + (1.0 / 3.0) * vp3;
+    double b0 = (13.0 / 12.0) * sq(vm1 - 2.0 * v0 + vp1) + (1.0 / 4.0) * sq(vm1 - vp1);
+    double b1 = (13.0 / 12.0) * sq(v0 - 2.0 * vp1 + vp2) + (1.0 / 4.0) * sq(v0 - 4.0 * vp1 + 3.0 * vp2);
+    double b2 = (13.0 / 12.0) * sq(vp1 - 2.0 * vp2 + vp3) + (1.0 / 4.0) * sq(3.0 * vp1 - 4.0 * vp2 + vp3);
+    double w[3];
+    orc_wenoz_weights(b0, b1, b2, 3.0 / 10.0, 6.0 / 10.0, 1.0 / 10.0, w);
+    return w[0] * q0 + w[1] * q1 + w[2] * q2;
+}
+
+/* ------------------------------------------------------------------------- */
+/* src/hllc.jl:17-165  (_hllc_normal) */
+static void hllc_normal(double rL, double mnL, double mt1L, double mt2L, double EL,
+                        double rR, double mnR, double mt1R, double mt2R, double ER,
+                        double g, double F[5]) {
+    if (rL <= 0.0) { rL = 1e-30; mnL = 0.0; mt1L = 0.0; mt2L = 0.0; EL = 0.0; }
+    else           { rL = jmax(rL, 1e-30); }
+    if (rR <= 0.0) { rR = 1e-30; mnR = 0.0; mt1R = 0.0; mt2R = 0.0; ER = 0.0; }
+    else           { rR = jmax(rR, 1e-30); }
+
+    double m2L = sq(mnL) + sq(mt1L) + sq(mt2L);
+    if (m2L > sq(rL) * 1e4) {
+        double s = rL * 100.0 / std::sqrt(m2L);
+        mnL *= s; mt1L *= s; mt2L *= s;
+    }
+    double m2R = sq(mnR) + sq(mt1R) + sq(mt2R);
+    if (m2R > sq(rR) * 1e4) {
+        double s = rR * 100.0 / std::sqrt(m2R);
+        mnR *= s; mt1R *= s; mt2R *= s;
+    }
+
+    double KE_L = jmin(0.5 * (sq(mnL) + sq(mt1L) + sq(mt2L)) / rL, 0.5 * rL * 1e4);
+    double KE_R = jmin(0.5 * (sq(mnR) + sq(mt1R) + sq(mt2R)) / rR, 0.5 * rR * 1e4);
+    EL = jmax(EL, KE_L);
+    ER = jmax(ER, KE_R);
+
+    double vnL = mnL / rL, vt1L = mt1L / rL, vt2L = mt2L / rL;
+    double vnR = mnR / rR, vt1R = mt1R / rR, vt2R = mt2R / rR;
+
+    double pL = (g - 1.0) * (EL - KE_L);
+    double pR = (g - 1.0) * (ER - KE_R);
+    double csL = std::sqrt(g * pL / rL);
+    double csR = std::sqrt(g * pR / rR);
+
+    double SL, SR;
+    if (pL > 0.0 && pR > 0.0) {
+        double r_avg = 0.5 * (rL + rR);
+        double cs_avg = 0.5 * (csL + csR);
+        double p_star = jmax(0.0, 0.5 * (pL + pR) - 0.5 * (vnR - vnL) * r_avg * cs_avg);
+        double qL = p_star > pL ? std::sqrt(1.0 + (g + 1.0) / (2.0 * g) * (p_star / pL - 1.0)) : 1.0;
+        double qR = p_star > pR ? std::sqrt(1.0 + (g + 1.0) / (2.0 * g) * (p_star / pR - 1.0)) : 1.0;
+        SL = vnL - csL * qL;
+        SR = vnR + csR * qR;
+    } else {
+        SL = jmin(vnL - csL, vnR - csR);
+        SR = jmax(vnL + csL, vnR + csR);
+    }
+
+    double denom = rL * (SL - vnL) - rR * (SR - vnR);
+    if (std::fabs(denom) < 1e-100) { F[0] = F[1] = F[2] = F[3] = F[4] = 0.0; return; }
+    double S_star = (pR - pL + rL * vnL * (SL - vnL) - rR * vnR * (SR - vnR)) / denom;
+
+    double FrL = mnL;
+    double FmnL = rL * sq(vnL) + pL;
+    double Fmt1L = mt1L * vnL;
+    double Fmt2L = mt2L * vnL;
+    double FEL = (EL + pL) * vnL;
+    if (SL >= 0.0) { F[0] = FrL; F[1] = FmnL; F[2] = Fmt1L; F[3] = Fmt2L; F[4] = FEL; return; }
+
+    double FrR = mnR;
+    double FmnR = rR * sq(vnR) + pR;
+    double Fmt1R = mt1R * vnR;
+    double Fmt2R = mt2R * vnR;
+    double FER = (ER + pR) * vnR;
+    if (SR <= 0.0) { F[0] = FrR; F[1] = FmnR; F[2] = Fmt1R; F[3] = Fmt2R; F[4] = FER; return; }
+
+    if (jmax(rL, rR) > 3.0 * jmin(rL, rR)) {
+        double inv_dS = 1.0 / (SR - SL);
+        F[0] = (SR * FrL - SL * FrR + SL * SR * (rR - rL)) * inv_dS;
+        F[1] = (SR * FmnL - SL * FmnR + SL * SR * (mnR - mnL)) * inv_dS;
+        F[2] = (SR * Fmt1L - SL * Fmt1R + SL * SR * (mt1R - mt1L)) * inv_dS;
+        F[3] = (SR * Fmt2L - SL * Fmt2R + SL * SR * (mt2R - mt2L)) * inv_dS;
+        F[4] = (SR * FEL - SL * FER + SL * SR * (ER - EL)) * inv_dS;
+        return;
+    }
+
+    if (S_star >= 0.0) {
+        double denom_L = rL * (SL - vnL);
+        double chi = denom_L / (SL - S_star);
+        double rsL = chi, mnsL = chi * S_star, mt1sL = chi * vt1L, mt2sL = chi * vt2L;
+        double EsL = std::fabs(denom_L) > 1e-100
+                         ? chi * (EL / rL + (S_star - vnL) * (S_star + pL / denom_L)) : 0.0;
+        F[0] = FrL + SL * (rsL - rL);
+        F[1] = FmnL + SL * (mnsL - mnL);
+        F[2] = Fmt1L + SL * (mt1sL - mt1L);
+        F[3] = Fmt2L + SL * (mt2sL - mt2L);
+        F[4] = FEL + SL * (EsL - EL);
+    } else {
+        double denom_R = rR * (SR - vnR);
+        double chi = denom_R / (SR - S_star);
+        double rsR = chi, mnsR = chi * S_star, mt1sR = chi * vt1R, mt2sR = chi * vt2R;
+        double EsR = std::fabs(denom_R) > 1e-100
+                         ? chi * (ER / rR + (S_star - vnR) * (S_star + pR / denom_R)) : 0.0;
+        F[0] = FrR + SR * (rsR - rR);
+        F[1] = FmnR + SR * (mnsR - mnR);
+        F[2] = Fmt1R + SR * (mt1sR - mt1R);
+        F[3] = Fmt2R + SR * (mt2sR - mt2R);
+        F[4] = FER + SR * (EsR - ER);
+    }
+}
+
+/* src/hllc.jl:176-208: x/y/z rotations */
+extern "C" void orc_hllc_flux(int dir, const double* L, const double* R, double g, double out[5]) {
+    double F[5];
+    if (dir == 0) {
+        hllc_normal(L[0], L[1], L[2], L[3], L[4], R[0], R[1], R[2], R[3], R[4], g, F);
+        out[0] = F[0]; out[1] = F[1]; out[2] = F[2]; out[3] = F[3]; out[4] = F[4];
+    } else if (dir == 1) {
+        hllc_normal(L[0], L[2], L[1], L[3], L[4], R[0], R[2], R[1], R[3], R[4], g, F);
+        out[0] = F[0]; out[1] = F[2]; out[2] = F[1]; out[3] = F[3]; out[4] = F[4];
+    } else {
+        hllc_normal(L[0], L[3], L[1], L[2], L[4], R[0], R[3], R[1], R[2], R[4], g, F);
+        out[0] = F[0]; out[1] = F[2]; out[2] = F[3]; out[3] = F[1]; out[4] = F[4];
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* src/euler3d.jl:33-44 (x faces, then y, then z) */
+extern "C" void orc_fill_ghost_outflow(double* U, int nx, int ny, int nz) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    for (int k = 1; k <= I.nzt; ++k) for (int j = 1; j <= I.nyt; ++j) for (int q = 1; q <= 5; ++q) {
+        for (int i = 1; i <= ng; ++i) U[I(q, i, j, k)] = U[I(q, ng + 1, j, k)];
+        for (int i = ng + nx + 1; i <= ng + nx + ng; ++i) U[I(q, i, j, k)] = U[I(q, ng + nx, j, k)];
+    }
+    for (int k = 1; k <= I.nzt; ++k) for (int i = 1; i <= I.nxt; ++i) for (int q = 1; q <= 5; ++q) {
+        for (int j = 1; j <= ng; ++j) U[I(q, i, j, k)] = U[I(q, i, ng + 1, k)];
+        for (int j = ng + ny + 1; j <= ng + ny + ng; ++j) U[I(q, i, j, k)] = U[I(q, i, ng + ny, k)];
+    }
+    for (int j = 1; j <= I.nyt; ++j) for (int i = 1; i <= I.nxt; ++i) for (int q = 1; q <= 5; ++q) {
+        for (int k = 1; k <= ng; ++k) U[I(q, i, j, k)] = U[I(q, i, j, ng + 1)];
+        for (int k = ng + nz + 1; k <= ng + nz + ng; ++k) U[I(q, i, j, k)] = U[I(q, i, j, ng + nz)];
+    }
+}
+
+/* src/euler3d.jl:51-62 */
+extern "C" void orc_fill_ghost_periodic(double* U, int nx, int ny, int nz) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    for (int k = 1; k <= I.nzt; ++k) for (int j = 1; j <= I.nyt; ++j) for (int q = 1; q <= 5; ++q) {
+        for (int t = 0; t < ng; ++t) U[I(q, 1 + t, j, k)] = U[I(q, nx + 1 + t, j, k)];
+        for (int t = 0; t < ng; ++t) U[I(q, ng + nx + 1 + t, j, k)] = U[I(q, ng + 1 + t, j, k)];
+    }
+    for (int k = 1; k <= I.nzt; ++k) for (int i = 1; i <= I.nxt; ++i) for (int q = 1; q <= 5; ++q) {
+        for (int t = 0; t < ng; ++t) U[I(q, i, 1 + t, k)] = U[I(q, i, ny + 1 + t, k)];
+        for (int t = 0; t < ng; ++t) U[I(q, i, ng + ny + 1 + t, k)] = U[I(q, i, ng + 1 + t, k)];
+    }
+    for (int j = 1; j <= I.nyt; ++j) for (int i = 1; i <= I.nxt; ++i) for (int q = 1; q <= 5; ++q) {
+        for (int t = 0; t < ng; ++t) U[I(q, i, j, 1 + t)] = U[I(q, i, j, nz + 1 + t)];
+        for (int t = 0; t < ng; ++t) U[I(q, i, j, ng + nz + 1 + t)] = U[I(q, i, j, ng + 1 + t)];
+    }
+}
+
+/* src/gpu_kernels.jl:26-46 via src/euler3d.jl:73-80 */
+extern "C" void orc_apply_floors(double* U, int nx, int ny, int nz, double rho_floor, double P_floor,
+                                 double g) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+#pragma omp parallel for schedule(static)
+    for (int kk = 1; kk <= nz; ++kk)
+        for (int jj = 1; jj <= ny; ++jj)
+            for (int ii = 1; ii <= nx; ++ii) {
+                int i = ii + ng, j = jj + ng, k = kk + ng;
+                double r = U[I(1, i, j, k)];
+                if (r < rho_floor) {
+                    U[I(1, i, j, k)] = rho_floor;
+                    U[I(2, i, j, k)] = 0.0;
+                    U[I(3, i, j, k)] = 0.0;
+                    U[I(4, i, j, k)] = 0.0;
+                    U[I(5, i, j, k)] = P_floor / (g - 1.0);
+                } else {
+                    double KE = 0.5 * (sq(U[I(2, i, j, k)]) + sq(U[I(3, i, j, k)]) + sq(U[I(4, i, j, k)])) / r;
+                    double P = (g - 1.0) * (U[I(5, i, j, k)] - KE);
+                    if (P < P_floor) U[I(5, i, j, k)] = P_floor / (g - 1.0) + KE;
+                }
+            }
+}
+
+/* src/euler3d.jl:86-90 */
+static inline double cell_pressure(double r, double mx, double my, double mz, double E, double g) {
+    r = jmax(r, 1e-30);
+    double KE = 0.5 * (sq(mx) + sq(my) + sq(mz)) / r;
+    return jmax((g - 1.0) * (E - KE), 0.0);
+}
+/* src/euler3d.jl:99-106 */
+static inline double EL_from_P(double PL, double rL, double mxL, double myL, double mzL, double g) {
+    double r_pos = jmax(rL, 1e-30);
+    double m2 = sq(mxL) + sq(myL) + sq(mzL);
+    double KE_raw = 0.5 * m2 / r_pos;
+    double KE = jmin(KE_raw, 0.5 * r_pos * 1e4);
+    return PL / (g - 1.0) + KE;
+}
+
+/* src/gpu_kernels.jl:51-154: one interface.  c[s][q] = U[q, cell s] for the
+ * six cells i-2..i+3 along the sweep direction. */
+static inline void interface_flux(int dir, const double c[6][5], double g, double out[5]) {
+    double L[5], R[5];
+    for (int q = 0; q < 4; ++q) {
+        L[q] = orc_weno5_left(c[0][q], c[1][q], c[2][q], c[3][q], c[4][q]);
+        R[q] = orc_weno5_right(c[1][q], c[2][q], c[3][q], c[4][q], c[5][q]);
+    }
+    double p[6];
+    for (int s = 0; s < 6; ++s) p[s] = cell_pressure(c[s][0], c[s][1], c[s][2], c[s][3], c[s][4], g);
+    double PmaxL = jmax(jmax(jmax(jmax(p[0], p[1]), p[2]), p[3]), p[4]);
+    double PmaxR = jmax(jmax(jmax(jmax(p[1], p[2]), p[3]), p[4]), p[5]);
+    double PL = jclamp(orc_weno5_left(p[0], p[1], p[2], p[3], p[4]), 0.0, PmaxL);
+    double PR = jclamp(orc_weno5_right(p[1], p[2], p[3], p[4], p[5]), 0.0, PmaxR);
+    L[4] = EL_from_P(PL, L[0], L[1], L[2], L[3], g);
+    R[4] = EL_from_P(PR, R[0], R[1], R[2], R[3], g);
+    orc_hllc_flux(dir, L, R, g, out);
+}
+
+/* src/gpu_kernels.jl:51-154 via src/euler3d.jl:109-130.  F has the reference
+ * shape for the given direction; only interfaces are written. */
+extern "C" void orc_weno_fluxes(int dir, double* F, const double* U, int nx, int ny, int nz, double g) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    FIdx FI(I.nxt + (dir == 0), I.nyt + (dir == 1), I.nzt + (dir == 2));
+    int ex = nx + (dir == 0), ey = ny + (dir == 1), ez = nz + (dir == 2);
+#pragma omp parallel for schedule(static)
+    for (int kk = 1; kk <= ez; ++kk)
+        for (int jj = 1; jj <= ey; ++jj)
+            for (int ii = 1; ii <= ex; ++ii) {
+                int i = ii + ng - (dir == 0), j = jj + ng - (dir == 1), k = kk + ng - (dir == 2);
+                double c[6][5];
+                for (int s = 0; s < 6; ++s) {
+                    int o = s - 2;
+                    int ci = i + (dir == 0 ? o : 0), cj = j + (dir == 1 ? o : 0), ck = k + (dir == 2 ? o : 0);
+                    for (int q = 0; q < 5; ++q) c[s][q] = U[I(q + 1, ci, cj, ck)];
+                }
+                double out[5];
+                interface_flux(dir, c, g, out);
+                for (int q = 0; q < 5; ++q) F[FI(q + 1, i, j, k)] = out[q];
+            }
+}
+
+/* src/gpu_kernels.jl:159-169 via src/euler3d.jl:135-145 (dU zeroed first) */
+extern "C" void orc_flux_divergence(double* dU, const double* Fx, const double* Fy, const double* Fz,
+                                    int nx, int ny, int nz, double dx, double dy, double dz) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    FIdx X(I.nxt + 1, I.nyt, I.nzt), Y(I.nxt, I.nyt + 1, I.nzt), Z(I.nxt, I.nyt, I.nzt + 1);
+    std::memset(dU, 0, sizeof(double) * I.size());
+    double inv_dx = 1.0 / dx, inv_dy = 1.0 / dy, inv_dz = 1.0 / dz;
+#pragma omp parallel for schedule(static)
+    for (int kk = 1; kk <= nz; ++kk)
+        for (int jj = 1; jj <= ny; ++jj)
+            for (int ii = 1; ii <= nx; ++ii) {
+                int i = ii + ng, j = jj + ng, k = kk + ng;
+                for (int q = 1; q <= 5; ++q)
+                    dU[I(q, i, j, k)] = -(Fx[X(q, i, j, k)] - Fx[X(q, i - 1, j, k)]) * inv_dx -
+                                        (Fy[Y(q, i, j, k)] - Fy[Y(q, i, j - 1, k)]) * inv_dy -
+                                        (Fz[Z(q, i, j, k)] - Fz[Z(q, i, j, k - 1)]) * inv_dz;
+            }
+}
+
+/* src/gpu_kernels.jl:174-191 + src/euler3d.jl:157-169 */
+extern "C" double orc_cfl_dt_3d(const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                                double g, double cfl) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    double inv_dx = 1.0 / dx, inv_dy = 1.0 / dy, inv_dz = 1.0 / dz;
+    double smax = -INFINITY;
+    bool any_nan = false;
+    for (int kk = 1; kk <= nz; ++kk)
+        for (int jj = 1; jj <= ny; ++jj)
+            for (int ii = 1; ii <= nx; ++ii) {
+                int i = ii + ng, j = jj + ng, k = kk + ng;
+                double r = jmax(U[I(1, i, j, k)], 1e-30);
+                double vx = U[I(2, i, j, k)] / r, vy = U[I(3, i, j, k)] / r, vz = U[I(4, i, j, k)] / r;
+                double KE = 0.5 * (sq(vx) + sq(vy) + sq(vz));
+                double P = jmax((g - 1.0) * (U[I(5, i, j, k)] / r - KE) * r, 0.0);
+                double cs = std::sqrt(g * P / r);
+                double s = jmax(jmax((std::fabs(vx) + cs) * inv_dx, (std::fabs(vy) + cs) * inv_dy),
+                                (std::fabs(vz) + cs) * inv_dz);
+                if (s != s) any_nan = true;
+                smax = jmax(smax, s);
+            }
+    /* maximum() propagates NaN and `NaN > 0.0` is false, so the reference
+     * returns Inf for a state holding a NaN. */
+    if (any_nan) return INFINITY;
+    return smax > 0.0 ? cfl / smax : INFINITY;
+}
+
+/* src/euler3d.jl:182-205 */
+extern "C" void orc_euler3d_rhs(double* dU, double* Fx, double* Fy, double* Fz, double* U,
+                                int nx, int ny, int nz, double dx, double dy, double dz, double g,
+                                int bc, double rho_floor, double P_floor, int fill_ghosts) {
+    Idx I(nx, ny, nz);
+    if (fill_ghosts) {
+        if (bc == 1) orc_fill_ghost_periodic(U, nx, ny, nz);
+        else         orc_fill_ghost_outflow(U, nx, ny, nz);
+    }
+    orc_apply_floors(U, nx, ny, nz, rho_floor, P_floor, g);
+    std::memset(Fx, 0, sizeof(double) * 5L * (I.nxt + 1) * I.nyt * I.nzt);
+    std::memset(Fy, 0, sizeof(double) * 5L * I.nxt * (I.nyt + 1) * I.nzt);
+    std::memset(Fz, 0, sizeof(double) * 5L * I.nxt * I.nyt * (I.nzt + 1));
+    orc_weno_fluxes(0, Fx, U, nx, ny, nz, g);
+    orc_weno_fluxes(1, Fy, U, nx, ny, nz, g);
+    orc_weno_fluxes(2, Fz, U, nx, ny, nz, g);
+    orc_flux_divergence(dU, Fx, Fy, Fz, nx, ny, nz, dx, dy, dz);
+}
+
+namespace {
+struct StepScratch {
+    std::vector<double> Fx, Fy, Fz, dU, Un;
+    StepScratch(int nx, int ny, int nz) {
+        Idx I(nx, ny, nz);
+        Fx.resize(5L * (I.nxt + 1) * I.nyt * I.nzt);
+        Fy.resize(5L * I.nxt * (I.nyt + 1) * I.nzt);
+        Fz.resize(5L * I.nxt * I.nyt * (I.nzt + 1));
+        dU.resize(I.size());
+        Un.resize(I.size());
+    }
+};
+/* stage combines, src/euler3d.jl:244,250,256 (whole array incl. ghosts) */
+void combine1(double* U, const double* Un, const double* dU, double dt, long n) {
+#pragma omp parallel for schedule(static)
+    for (long t = 0; t < n; ++t) U[t] = Un[t] + dt * dU[t];
+}
+void combine2(double* U, const double* Un, const double* dU, double dt, long n) {
+#pragma omp parallel for schedule(static)
+    for (long t = 0; t < n; ++t) U[t] = 0.75 * Un[t] + 0.25 * U[t] + 0.25 * dt * dU[t];
+}
+void combine3(double* U, const double* Un, const double* dU, double dt, long n) {
+#pragma omp parallel for schedule(static)
+    for (long t = 0; t < n; ++t) U[t] = (1.0 / 3.0) * Un[t] + (2.0 / 3.0) * U[t] + (2.0 / 3.0) * dt * dU[t];
+}
+}  // namespace
+
+/* src/euler3d.jl:220-260 */
+extern "C" void orc_euler3d_step(double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                                 double dt, double g, int bc, double rho_floor, double P_floor) {
+    Idx I(nx, ny, nz);
+    StepScratch S(nx, ny, nz);
+    long n = I.size();
+    std::memcpy(S.Un.data(), U, sizeof(double) * n);
+    orc_euler3d_rhs(S.dU.data(), S.Fx.data(), S.Fy.data(), S.Fz.data(), U, nx, ny, nz, dx, dy, dz, g, bc,
+                    rho_floor, P_floor, 1);
+    combine1(U, S.Un.data(), S.dU.data(), dt, n);
+    orc_apply_floors(U, nx, ny, nz, rho_floor, P_floor, g);
+    orc_euler3d_rhs(S.dU.data(), S.Fx.data(), S.Fy.data(), S.Fz.data(), U, nx, ny, nz, dx, dy, dz, g, bc,
+                    rho_floor, P_floor, 1);
+    combine2(U, S.Un.data(), S.dU.data(), dt, n);
+    orc_apply_floors(U, nx, ny, nz, rho_floor, P_floor, g);
+    orc_euler3d_rhs(S.dU.data(), S.Fx.data(), S.Fy.data(), S.Fz.data(), U, nx, ny, nz, dx, dy, dz, g, bc,
+                    rho_floor, P_floor, 1);
+    combine3(U, S.Un.data(), S.dU.data(), dt, n);
+    orc_apply_floors(U, nx, ny, nz, rho_floor, P_floor, g);
+}
+
+/* src/euler3d.jl:275-316 */
+extern "C" void orc_sedov_ic_3d(double* U, int nx, int ny, int nz, double dx, double dy, double dz, double g,
+                                double E_blast, double r_inject, double rho_bg, double P_floor,
+                                double x_offset, double y_offset, double z_offset) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    double r_inj = r_inject > 0.0 ? r_inject : 2.5 * jmin(jmin(dx, dy), dz);
+    std::memset(U, 0, sizeof(double) * I.size());
+    double E_bg = P_floor / (g - 1.0);
+    for (int k = ng + 1; k <= ng + nz; ++k) for (int j = ng + 1; j <= ng + ny; ++j)
+        for (int i = ng + 1; i <= ng + nx; ++i) { U[I(1, i, j, k)] = rho_bg; U[I(5, i, j, k)] = E_bg; }
+    double V_inj = 0.0;
+    for (int k = ng + 1; k <= ng + nz; ++k) for (int j = ng + 1; j <= ng + ny; ++j)
+        for (int i = ng + 1; i <= ng + nx; ++i) {
+            double xc = ((double)(i - ng) - 0.5) * dx + x_offset;
+            double yc = ((double)(j - ng) - 0.5) * dy + y_offset;
+            double zc = ((double)(k - ng) - 0.5) * dz + z_offset;
+            double r = std::sqrt(sq(xc) + sq(yc) + sq(zc));
+            if (r <= r_inj) V_inj += dx * dy * dz;
+        }
+    double dE_cell = (V_inj > 0.0) ? E_blast * (g - 1.0) / V_inj : 0.0;
+    for (int k = ng + 1; k <= ng + nz; ++k) for (int j = ng + 1; j <= ng + ny; ++j)
+        for (int i = ng + 1; i <= ng + nx; ++i) {
+            double xc = ((double)(i - ng) - 0.5) * dx + x_offset;
+            double yc = ((double)(j - ng) - 0.5) * dy + y_offset;
+            double zc = ((double)(k - ng) - 0.5) * dz + z_offset;
+            double r = std::sqrt(sq(xc) + sq(yc) + sq(zc));
+            if (r <= r_inj) U[I(5, i, j, k)] += dE_cell;
+        }
+}
+
+/* ------------------------------------------------------------------------- */
+/* src/BinarySupernova.jl:159 */
+extern "C" double orc_r_sink(const orc_bh* bh) {
+    return jmax(6.0 * bh->mass / sq(bh->c_code), bh->r_floor);
+}
+/* src/BinarySupernova.jl:167-171 */
+extern "C" double orc_t_sink(const orc_bh* bh, double f_sink) {
+    double rs = orc_r_sink(bh);
+    double v_ff = std::sqrt(2.0 * bh->mass / rs);
+    return f_sink * rs / v_ff;
+}
+
+/* src/gpu_kernels.jl:199-230 via src/gravity_bh.jl:58-78 */
+extern "C" void orc_add_bh_gravity_source(double* dU, const double* U, int nx, int ny, int nz,
+                                          double dx, double dy, double dz, const orc_bh* bhs, int nbh,
+                                          double x0, double y0, double z0) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+#pragma omp parallel for schedule(static)
+    for (int kk = 1; kk <= nz; ++kk)
+        for (int jj = 1; jj <= ny; ++jj)
+            for (int ii = 1; ii <= nx; ++ii) {
+                int i = ii + ng, j = jj + ng, k = kk + ng;
+                double xc = x0 + ((double)ii - 0.5) * dx;
+                double yc = y0 + ((double)jj - 0.5) * dy;
+                double zc = z0 + ((double)kk - 0.5) * dz;
+                double r = U[I(1, i, j, k)];
+                double vx = U[I(2, i, j, k)] / r, vy = U[I(3, i, j, k)] / r, vz = U[I(4, i, j, k)] / r;
+                double ax = 0.0, ay = 0.0, az = 0.0;
+                for (int n = 0; n < nbh; ++n) {
+                    double ddx = xc - bhs[n].pos[0], ddy = yc - bhs[n].pos[1], ddz = zc - bhs[n].pos[2];
+                    double r2 = sq(ddx) + sq(ddy) + sq(ddz) + sq(bhs[n].eps);
+                    double r3 = r2 * std::sqrt(r2);
+                    double fac = -bhs[n].mass / r3;
+                    ax += fac * ddx; ay += fac * ddy; az += fac * ddz;
+                }
+                dU[I(2, i, j, k)] += r * ax;
+                dU[I(3, i, j, k)] += r * ay;
+                dU[I(4, i, j, k)] += r * az;
+                dU[I(5, i, j, k)] += r * (vx * ax + vy * ay + vz * az);
+            }
+}
+
+/* src/gravity_bh.jl:91-113 */
+extern "C" void orc_gas_force_on_bh(const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                                    const orc_bh* bh, double x0, double y0, double z0, double out[3]) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    double dV = dx * dy * dz;
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i) {
+        double xc = x0 + ((double)i - 0.5) * dx;
+        double yc = y0 + ((double)j - 0.5) * dy;
+        double zc = z0 + ((double)k - 0.5) * dz;
+        double ddx = xc - bh->pos[0], ddy = yc - bh->pos[1], ddz = zc - bh->pos[2];
+        double r2 = sq(ddx) + sq(ddy) + sq(ddz) + sq(bh->eps);
+        double r3 = r2 * std::sqrt(r2);
+        double fac = bh->mass / r3 * U[I(1, ng + i, ng + j, ng + k)] * dV;
+        Fx += fac * ddx; Fy += fac * ddy; Fz += fac * ddz;
+    }
+    out[0] = Fx; out[1] = Fy; out[2] = Fz;
+}
+
+/* src/gpu_kernels.jl:238-284 via src/sinks.jl:32-59 */
+extern "C" void orc_add_sink_sources(double* dU, const double* U, int nx, int ny, int nz,
+                                     double dx, double dy, double dz, const orc_bh* bhs, int nbh,
+                                     double x0, double y0, double z0, double f_sink, int torque_free,
+                                     double rho_sink_min) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    std::vector<double> rs(nbh), ts(nbh);
+    for (int n = 0; n < nbh; ++n) { rs[n] = orc_r_sink(&bhs[n]); ts[n] = orc_t_sink(&bhs[n], f_sink); }
+#pragma omp parallel for schedule(static)
+    for (int kk = 1; kk <= nz; ++kk)
+        for (int jj = 1; jj <= ny; ++jj)
+            for (int ii = 1; ii <= nx; ++ii) {
+                int i = ii + ng, j = jj + ng, k = kk + ng;
+                double xc = x0 + ((double)ii - 0.5) * dx;
+                double yc = y0 + ((double)jj - 0.5) * dy;
+                double zc = z0 + ((double)kk - 0.5) * dz;
+                double r = U[I(1, i, j, k)];
+                double mx = U[I(2, i, j, k)], my = U[I(3, i, j, k)], mz = U[I(4, i, j, k)];
+                double E = U[I(5, i, j, k)];
+                if (!(r > rho_sink_min)) continue;
+                for (int n = 0; n < nbh; ++n) {
+                    double ddx = xc - bhs[n].pos[0], ddy = yc - bhs[n].pos[1], ddz = zc - bhs[n].pos[2];
+                    double rr = std::sqrt(sq(ddx) + sq(ddy) + sq(ddz));
+                    if (rr < rs[n]) {
+                        double t = ts[n];
+                        dU[I(1, i, j, k)] -= r / t;
+                        if (torque_free) {
+                            double rx = ddx / rr, ry = ddy / rr, rz = ddz / rr;
+                            double vx = mx / r, vy = my / r, vz = mz / r;
+                            double vrx = vx - bhs[n].vel[0], vry = vy - bhs[n].vel[1], vrz = vz - bhs[n].vel[2];
+                            double v_r = vrx * rx + vry * ry + vrz * rz;
+                            double e_int = E / r - 0.5 * (sq(vx) + sq(vy) + sq(vz));
+                            dU[I(2, i, j, k)] -= r * v_r * rx / t;
+                            dU[I(3, i, j, k)] -= r * v_r * ry / t;
+                            dU[I(4, i, j, k)] -= r * v_r * rz / t;
+                            dU[I(5, i, j, k)] -= (0.5 * r * sq(v_r) + r * e_int) / t;
+                        } else {
+                            dU[I(2, i, j, k)] -= mx / t;
+                            dU[I(3, i, j, k)] -= my / t;
+                            dU[I(4, i, j, k)] -= mz / t;
+                            dU[I(5, i, j, k)] -= E / t;
+                        }
+                    }
+                }
+            }
+}
+
+/* src/sinks.jl:74-109 */
+extern "C" void orc_accrete(orc_bh* bh, const double* U, int nx, int ny, int nz, double dx, double dy,
+                            double dz, double x0, double y0, double z0, double dt, double f_sink,
+                            double rho_sink_min) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    double rs = orc_r_sink(bh), ts = orc_t_sink(bh, f_sink);
+    double dV = dx * dy * dz;
+    double dm = 0.0, dPx = 0.0, dPy = 0.0, dPz = 0.0;
+    for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i) {
+        double xc = x0 + ((double)i - 0.5) * dx;
+        double yc = y0 + ((double)j - 0.5) * dy;
+        double zc = z0 + ((double)k - 0.5) * dz;
+        double r = std::sqrt(sq(xc - bh->pos[0]) + sq(yc - bh->pos[1]) + sq(zc - bh->pos[2]));
+        if (r >= rs) continue;
+        if (U[I(1, ng + i, ng + j, ng + k)] <= rho_sink_min) continue;
+        double rate = dV / ts * dt;
+        dm += U[I(1, ng + i, ng + j, ng + k)] * rate;
+        dPx += U[I(2, ng + i, ng + j, ng + k)] * rate;
+        dPy += U[I(3, ng + i, ng + j, ng + k)] * rate;
+        dPz += U[I(4, ng + i, ng + j, ng + k)] * rate;
+    }
+    if (dm > 0.0) {
+        double M_new = bh->mass + dm;
+        bh->vel[0] = (bh->mass * bh->vel[0] + dPx) / M_new;
+        bh->vel[1] = (bh->mass * bh->vel[1] + dPy) / M_new;
+        bh->vel[2] = (bh->mass * bh->vel[2] + dPz) / M_new;
+        bh->mass = M_new;
+    }
+}
+
+/* src/nbody.jl:24-56 */
+static void nbody_rhs(double (*dpos)[3], double (*dvel)[3], const orc_bh* bhs, int n, const double* Fg) {
+    for (int i = 0; i < n; ++i) {
+        for (int d = 0; d < 3; ++d) dpos[i][d] = bhs[i].vel[d];
+        double a[3];
+        for (int d = 0; d < 3; ++d) a[d] = Fg[3 * i + d] / bhs[i].mass;
+        for (int j = 0; j < n; ++j) {
+            if (j == i) continue;
+            double dx = bhs[j].pos[0] - bhs[i].pos[0];
+            double dy = bhs[j].pos[1] - bhs[i].pos[1];
+            double dz = bhs[j].pos[2] - bhs[i].pos[2];
+            double r2 = sq(dx) + sq(dy) + sq(dz) + sq(bhs[j].eps);
+            double r3 = r2 * std::sqrt(r2);
+            double fac = bhs[j].mass / r3;
+            a[0] = a[0] + fac * dx; a[1] = a[1] + fac * dy; a[2] = a[2] + fac * dz;
+        }
+        for (int d = 0; d < 3; ++d) dvel[i][d] = a[d];
+    }
+}
+
+/* src/nbody.jl:74-104 */
+extern "C" void orc_nbody_step(orc_bh* bhs, int n, double dt, const double* Fg) {
+    std::vector<double> p0(3 * n), v0(3 * n), p1(3 * n), v1(3 * n), p2(3 * n), v2(3 * n);
+    std::vector<double> dp(3 * n), dv(3 * n);
+    auto DP = reinterpret_cast<double (*)[3]>(dp.data());
+    auto DV = reinterpret_cast<double (*)[3]>(dv.data());
+    for (int i = 0; i < n; ++i) for (int d = 0; d < 3; ++d) { p0[3*i+d] = bhs[i].pos[d]; v0[3*i+d] = bhs[i].vel[d]; }
+    nbody_rhs(DP, DV, bhs, n, Fg);
+    for (int i = 0; i < n; ++i) for (int d = 0; d < 3; ++d) {
+        p1[3*i+d] = p0[3*i+d] + dt * DP[i][d];
+        v1[3*i+d] = v0[3*i+d] + dt * DV[i][d];
+    }
+    for (int i = 0; i < n; ++i) for (int d = 0; d < 3; ++d) { bhs[i].pos[d] = p1[3*i+d]; bhs[i].vel[d] = v1[3*i+d]; }
+    nbody_rhs(DP, DV, bhs, n, Fg);
+    for (int i = 0; i < n; ++i) for (int d = 0; d < 3; ++d) {
+        p2[3*i+d] = 0.75 * p0[3*i+d] + 0.25 * (p1[3*i+d] + dt * DP[i][d]);
+        v2[3*i+d] = 0.75 * v0[3*i+d] + 0.25 * (v1[3*i+d] + dt * DV[i][d]);
+    }
+    for (int i = 0; i < n; ++i) for (int d = 0; d < 3; ++d) { bhs[i].pos[d] = p2[3*i+d]; bhs[i].vel[d] = v2[3*i+d]; }
+    nbody_rhs(DP, DV, bhs, n, Fg);
+    for (int i = 0; i < n; ++i) for (int d = 0; d < 3; ++d) {
+        bhs[i].pos[d] = (1.0 / 3.0) * p0[3*i+d] + (2.0 / 3.0) * (p2[3*i+d] + dt * DP[i][d]);
+        bhs[i].vel[d] = (1.0 / 3.0) * v0[3*i+d] + (2.0 / 3.0) * (v2[3*i+d] + dt * DV[i][d]);
+    }
+}
+
+/* src/kepler_orbit.jl:63-111 */
+extern "C" int orc_kepler_init(const orc_bh* bhs, const double com[3], const double* nhat, double Omega,
+                               double st[13]) {
+    double dx = bhs[0].pos[0] - bhs[1].pos[0], dy = bhs[0].pos[1] - bhs[1].pos[1],
+           dz = bhs[0].pos[2] - bhs[1].pos[2];
+    double a = std::sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(a > 0)) return -1;
+    double rx1 = bhs[0].pos[0] - com[0], ry1 = bhs[0].pos[1] - com[1], rz1 = bhs[0].pos[2] - com[2];
+    double vx1 = bhs[0].vel[0], vy1 = bhs[0].vel[1], vz1 = bhs[0].vel[2];
+    double nh[3];
+    if (!nhat) {
+        double Lx = ry1 * vz1 - rz1 * vy1, Ly = rz1 * vx1 - rx1 * vz1, Lz = rx1 * vy1 - ry1 * vx1;
+        double Lm = std::sqrt(Lx * Lx + Ly * Ly + Lz * Lz);
+        if (!(Lm > 0)) return -2;
+        nh[0] = Lx / Lm; nh[1] = Ly / Lm; nh[2] = Lz / Lm;
+    } else {
+        double nm = std::sqrt(sq(nhat[0]) + sq(nhat[1]) + sq(nhat[2]));
+        if (!(std::fabs(nm - 1.0) < 1e-10)) return -3;
+        nh[0] = nhat[0]; nh[1] = nhat[1]; nh[2] = nhat[2];
+    }
+    double W;
+    if (!(Omega > 0)) {
+        double Rmag = std::sqrt(rx1 * rx1 + ry1 * ry1 + rz1 * rz1);
+        double vmag = std::sqrt(vx1 * vx1 + vy1 * vy1 + vz1 * vz1);
+        if (!(Rmag > 0) || !(vmag > 0)) return -4;
+        W = vmag / Rmag;
+    } else {
+        W = Omega;
+    }
+    st[0] = com[0]; st[1] = com[1]; st[2] = com[2]; st[3] = W;
+    st[4] = nh[0]; st[5] = nh[1]; st[6] = nh[2];
+    for (int i = 0; i < 2; ++i)
+        for (int d = 0; d < 3; ++d) st[7 + 3 * i + d] = bhs[i].pos[d] - com[d];
+    return 0;
+}
+
+/* src/kepler_orbit.jl:124-150 */
+extern "C" void orc_kepler_update(orc_bh* bhs, const double st[13], double t) {
+    double th = st[3] * t;
+    double c = std::cos(th), s = std::sin(th);
+    double nx = st[4], ny = st[5], nz = st[6];
+    double cx = st[0], cy = st[1], cz = st[2];
+    double W = st[3];
+    for (int i = 0; i < 2; ++i) {
+        double rx0 = st[7 + 3 * i], ry0 = st[8 + 3 * i], rz0 = st[9 + 3 * i];
+        double ndotr = nx * rx0 + ny * ry0 + nz * rz0;
+        double kx = ny * rz0 - nz * ry0, ky = nz * rx0 - nx * rz0, kz = nx * ry0 - ny * rx0;
+        double rx = rx0 * c + kx * s + nx * ndotr * (1.0 - c);
+        double ry = ry0 * c + ky * s + ny * ndotr * (1.0 - c);
+        double rz = rz0 * c + kz * s + nz * ndotr * (1.0 - c);
+        bhs[i].pos[0] = cx + rx; bhs[i].pos[1] = cy + ry; bhs[i].pos[2] = cz + rz;
+        bhs[i].vel[0] = W * (ny * rz - nz * ry);
+        bhs[i].vel[1] = W * (nz * rx - nx * rz);
+        bhs[i].vel[2] = W * (nx * ry - ny * rx);
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* FFT: iterative radix-2 for powers of two, direct DFT otherwise.  Stands in
+ * for FFTW/cuFFT behind AbstractFFTs fft/ifft (src/self_gravity.jl:73);
+ * inverse includes the 1/N normalisation as ifft does. */
+namespace {
+void fft1d(double* re, double* im, int n, long stride, int inverse, std::vector<double>& tr,
+           std::vector<double>& ti) {
+    tr.resize(n); ti.resize(n);
+    for (int t = 0; t < n; ++t) { tr[t] = re[t * stride]; ti[t] = im[t * stride]; }
+    double sgn = inverse ? 1.0 : -1.0;
+    if ((n & (n - 1)) == 0) {
+        for (int i = 1, j = 0; i < n; ++i) {
+            int bit = n >> 1;
+            for (; j & bit; bit >>= 1) j ^= bit;
+            j ^= bit;
+            if (i < j) { std::swap(tr[i], tr[j]); std::swap(ti[i], ti[j]); }
+        }
+        for (int len = 2; len <= n; len <<= 1) {
+            int half = len >> 1;
+            for (int s = 0; s < n; s += len)
+                for (int m = 0; m < half; ++m) {
+                    double ang = sgn * 2.0 * M_PI * (double)m / (double)len;
+                    double wr = std::cos(ang), wi = std::sin(ang);
+                    double ur = tr[s + m], ui = ti[s + m];
+                    double xr = tr[s + m + half], xi = ti[s + m + half];
+                    double vr = xr * wr - xi * wi, vi = xr * wi + xi * wr;
+                    tr[s + m] = ur + vr; ti[s + m] = ui + vi;
+                    tr[s + m + half] = ur - vr; ti[s + m + half] = ui - vi;
+                }
+        }
+    } else {
+        std::vector<double> orr(n), oi(n);
+        for (int kf = 0; kf < n; ++kf) {
+            double sr = 0.0, si = 0.0;
+            for (int t = 0; t < n; ++t) {
+                long p = ((long)kf * t) % n;
+                double ang = sgn * 2.0 * M_PI * (double)p / (double)n;
+                double wr = std::cos(ang), wi = std::sin(ang);
+                sr += tr[t] * wr - ti[t] * wi;
+                si += tr[t] * wi + ti[t] * wr;
+            }
+            orr[kf] = sr; oi[kf] = si;
+        }
+        tr = orr; ti = oi;
+    }
+    double sc = inverse ? 1.0 / (double)n : 1.0;
+    for (int t = 0; t < n; ++t) { re[t * stride] = tr[t] * sc; im[t * stride] = ti[t] * sc; }
+}
+}  // namespace
+
+extern "C" void orc_fft3d(double* re, double* im, int n1, int n2, int n3, int inverse) {
+    /* column-major (n1 fastest) */
+#pragma omp parallel
+    {
+        std::vector<double> tr, ti;
+#pragma omp for schedule(static)
+        for (long l = 0; l < (long)n2 * n3; ++l) fft1d(re + l * n1, im + l * n1, n1, 1, inverse, tr, ti);
+#pragma omp for schedule(static)
+        for (long l = 0; l < (long)n1 * n3; ++l) {
+            long a = l % n1, c = l / n1;
+            fft1d(re + a + c * (long)n1 * n2, im + a + c * (long)n1 * n2, n2, n1, inverse, tr, ti);
+        }
+#pragma omp for schedule(static)
+        for (long l = 0; l < (long)n1 * n2; ++l)
+            fft1d(re + l, im + l, n3, (long)n1 * n2, inverse, tr, ti);
+    }
+}
+
+/* src/self_gravity.jl:35-76 */
+extern "C" void orc_solve_poisson_isolated(const double* rho, int nx, int ny, int nz,
+                                           double dx, double dy, double dz, double* phi) {
+    int Nx = 2 * nx, Ny = 2 * ny, Nz = 2 * nz;
+    double dV = dx * dy * dz;
+    double eps2 = std::pow(dx * dy * dz, 2.0 / 3.0);
+    long N = (long)Nx * Ny * Nz;
+    std::vector<double> Kr(N), Ki(N, 0.0), Rr(N, 0.0), Ri(N, 0.0);
+    for (int k = 1; k <= Nz; ++k) for (int j = 1; j <= Ny; ++j) for (int i = 1; i <= Nx; ++i) {
+        double fi = (double)(i <= nx ? i - 1 : i - 1 - Nx);
+        double fj = (double)(j <= ny ? j - 1 : j - 1 - Ny);
+        double fk = (double)(k <= nz ? k - 1 : k - 1 - Nz);
+        double r2 = sq(fi * dx) + sq(fj * dy) + sq(fk * dz);
+        Kr[(i - 1) + (long)Nx * ((j - 1) + (long)Ny * (k - 1))] = -1.0 / std::sqrt(r2 + eps2);
+    }
+    for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i)
+        Rr[i + (long)Nx * (j + (long)Ny * k)] = rho[i + (long)nx * (j + (long)ny * k)];
+    orc_fft3d(Kr.data(), Ki.data(), Nx, Ny, Nz, 0);
+    orc_fft3d(Rr.data(), Ri.data(), Nx, Ny, Nz, 0);
+    for (long t = 0; t < N; ++t) {
+        double ar = Kr[t], ai = Ki[t], br = Rr[t], bi = Ri[t];
+        Rr[t] = ar * br - ai * bi;
+        Ri[t] = ar * bi + ai * br;
+    }
+    orc_fft3d(Rr.data(), Ri.data(), Nx, Ny, Nz, 1);
+    for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i)
+        phi[i + (long)nx * (j + (long)ny * k)] = Rr[i + (long)Nx * (j + (long)Ny * k)] * dV;
+}
+
+/* src/gpu_kernels.jl:291-319 (via src/fmr_gravity.jl:146-156) */
+extern "C" void orc_sg_gradient(double* dU, const double* U, const double* phi, int nx, int ny, int nz,
+                                double dx, double dy, double dz) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    double inv2dx = 0.5 / dx, inv2dy = 0.5 / dy, inv2dz = 0.5 / dz;
+    auto P = [&](int a, int b, int c) { return phi[(a - 1) + (long)nx * ((b - 1) + (long)ny * (c - 1))]; };
+#pragma omp parallel for schedule(static)
+    for (int kk = 1; kk <= nz; ++kk)
+        for (int jj = 1; jj <= ny; ++jj)
+            for (int ii = 1; ii <= nx; ++ii) {
+                int i = ii + ng, j = jj + ng, k = kk + ng;
+                double r = U[I(1, i, j, k)];
+                double rvx = U[I(2, i, j, k)], rvy = U[I(3, i, j, k)], rvz = U[I(4, i, j, k)];
+                int ip = std::min(ii + 1, nx), im = std::max(ii - 1, 1);
+                int jp = std::min(jj + 1, ny), jm = std::max(jj - 1, 1);
+                int kp = std::min(kk + 1, nz), km = std::max(kk - 1, 1);
+                double fxfac = ip > im ? inv2dx : 2.0 * inv2dx;
+                double fyfac = jp > jm ? inv2dy : 2.0 * inv2dy;
+                double fzfac = kp > km ? inv2dz : 2.0 * inv2dz;
+                double gx = (P(ip, jj, kk) - P(im, jj, kk)) * fxfac;
+                double gy = (P(ii, jp, kk) - P(ii, jm, kk)) * fyfac;
+                double gz = (P(ii, jj, kp) - P(ii, jj, km)) * fzfac;
+                double vdotg = (rvx * gx + rvy * gy + rvz * gz) / r;
+                dU[I(2, i, j, k)] -= r * gx;
+                dU[I(3, i, j, k)] -= r * gy;
+                dU[I(4, i, j, k)] -= r * gz;
+                dU[I(5, i, j, k)] -= r * vdotg;
+            }
+}
+
+/* src/self_gravity.jl:93-115 */
+extern "C" void orc_add_self_gravity_source(double* dU, const double* U, int nx, int ny, int nz,
+                                            double dx, double dy, double dz) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    std::vector<double> rho((long)nx * ny * nz), phi((long)nx * ny * nz);
+    for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i)
+        rho[i + (long)nx * (j + (long)ny * k)] = U[I(1, ng + 1 + i, ng + 1 + j, ng + 1 + k)];
+    orc_solve_poisson_isolated(rho.data(), nx, ny, nz, dx, dy, dz, phi.data());
+    orc_sg_gradient(dU, U, phi.data(), nx, ny, nz, dx, dy, dz);
+}
+
+/* scripts/run_sn50_fiducial.jl:756-818 (coupled_step!).  evolve_orbit=1 runs
+ * nbody_step!; 0 leaves BHs as given (caller applies kepler_update!). */
+extern "C" void orc_coupled_step(double* U, double* Un, double* dU, double* Fx, double* Fy, double* Fz,
+                                 orc_bh* bhs, int nbh, double dt, double t, int nx, int ny, int nz,
+                                 double dx, double x0, double y0, double z0, double g,
+                                 double f_sink, double rho_floor, double P_floor, int torque_free,
+                                 int self_gravity, double t_bh2_sink_on, double rho_sink_min,
+                                 int evolve_orbit, double* Fgas) {
+    Idx I(nx, ny, nz);
+    long n = I.size();
+    int nsink = (t < t_bh2_sink_on) ? std::min(1, nbh) : nbh;
+    for (int i = 0; i < nbh; ++i) {
+        orc_gas_force_on_bh(U, nx, ny, nz, dx, dx, dx, &bhs[i], x0, y0, z0, Fgas + 3 * i);
+        double* F = Fgas + 3 * i;
+        bool fin = std::isfinite(F[0]) && std::isfinite(F[1]) && std::isfinite(F[2]);
+        if (!fin || std::sqrt(sq(F[0]) + sq(F[1]) + sq(F[2])) > 1e3) { F[0] = F[1] = F[2] = 0.0; }
+    }
+    if (evolve_orbit) {
+        bool ok = true;
+        for (int i = 0; i < nbh; ++i)
+            for (int d = 0; d < 3; ++d) ok = ok && std::isfinite(bhs[i].pos[d]) && std::isfinite(bhs[i].vel[d]);
+        if (ok) orc_nbody_step(bhs, nbh, dt, Fgas);
+    }
+    std::memcpy(Un, U, sizeof(double) * n);
+    for (int stage = 0; stage < 3; ++stage) {
+        orc_euler3d_rhs(dU, Fx, Fy, Fz, U, nx, ny, nz, dx, dx, dx, g, 0, rho_floor, P_floor, 1);
+        orc_add_bh_gravity_source(dU, U, nx, ny, nz, dx, dx, dx, bhs, nbh, x0, y0, z0);
+        if (self_gravity) orc_add_self_gravity_source(dU, U, nx, ny, nz, dx, dx, dx);
+        orc_add_sink_sources(dU, U, nx, ny, nz, dx, dx, dx, bhs, nsink, x0, y0, z0, f_sink, torque_free,
+                             rho_sink_min);
+        if (stage == 0) combine1(U, Un, dU, dt, n);
+        else if (stage == 1) combine2(U, Un, dU, dt, n);
+        else combine3(U, Un, dU, dt, n);
+        orc_apply_floors(U, nx, ny, nz, rho_floor, P_floor, g);
+    }
+    for (int i = 0; i < nsink; ++i)
+        orc_accrete(&bhs[i], U, nx, ny, nz, dx, dx, dx, x0, y0, z0, dt, f_sink, rho_sink_min);
+}
+
+/* ------------------------------------------------------------------------- */
+/* src/fmr3d.jl:32-46; w is (ratio x 5) column-major: w[s + ratio*j] */
+extern "C" void orc_lag5_weights(int ratio, double* w) {
+    const double nodes[5] = {-2.0, -1.0, 0.0, 1.0, 2.0};
+    for (int s = 0; s < ratio; ++s) {
+        double t = ((double)s + 0.5 - (double)ratio / 2.0) / (double)ratio;
+        for (int j = 0; j < 5; ++j) {
+            double wj = 1.0;
+            for (int m = 0; m < 5; ++m)
+                if (m != j) wj *= (t - nodes[m]) / (nodes[j] - nodes[m]);
+            w[s + ratio * j] = wj;
+        }
+    }
+}
+
+namespace {
+/* src/fmr3d.jl:165-170; round(Int, x) is round-half-even. */
+inline void coarse_stencil(int ig_f, int c_lo, int ratio, int ng, int* ic0, int* sx) {
+    double xi = (double)c_lo - 0.5 + ((double)(ig_f - ng) - 0.5) / (double)ratio;
+    int c0 = (int)std::nearbyint(xi);
+    int s = (int)std::floor((xi - (double)c0 + 0.5) * (double)ratio);
+    if (s < 0) s = 0;
+    if (s > ratio - 1) s = ratio - 1;
+    *ic0 = c0; *sx = s;
+}
+
+struct Fmr {
+    const orc_fmr* G;
+    std::vector<double> w;
+    Fmr(const orc_fmr* g) : G(g), w(5 * g->ratio) { orc_lag5_weights(g->ratio, w.data()); }
+    double W(int s, int j) const { return w[s + G->ratio * j]; }   /* Julia w[s+1, j+1] */
+};
+
+/* src/fmr3d.jl:176-198 */
+void prolong_cell(double* Uf, const double* Uc, const Fmr& F, int ig_f, int jf, int kf) {
+    const orc_fmr* G = F.G;
+    const int r = G->ratio, ng = NG;
+    Idx Ic(G->ncx, G->ncy, G->ncz), If(G->nfx, G->nfy, G->nfz);
+    int ic0, si, jc0, sj, kc0, sk;
+    coarse_stencil(ig_f, G->ci_lo, r, ng, &ic0, &si);
+    coarse_stencil(jf, G->cj_lo, r, ng, &jc0, &sj);
+    coarse_stencil(kf, G->ck_lo, r, ng, &kc0, &sk);
+    for (int q = 1; q <= 5; ++q) {
+        double val = 0.0;
+        for (int di = -2; di <= 2; ++di) {
+            int ig_c = ng + ic0 + di;
+            double wi = F.W(si, di + 2);
+            for (int dj = -2; dj <= 2; ++dj) {
+                int jg_c = ng + jc0 + dj;
+                double wij = wi * F.W(sj, dj + 2);
+                for (int dk = -2; dk <= 2; ++dk) {
+                    int kg_c = ng + kc0 + dk;
+                    val += wij * F.W(sk, dk + 2) * Uc[Ic(q, ig_c, jg_c, kg_c)];
+                }
+            }
+        }
+        Uf[If(q, ig_f, jf, kf)] = val;
+    }
+}
+}  // namespace
+
+/* src/fmr3d.jl:206-214 */
+extern "C" void orc_prolong_all(const orc_fmr* G) {
+    Fmr F(G);
+    int nxt = G->nfx + 2 * NG, nyt = G->nfy + 2 * NG, nzt = G->nfz + 2 * NG;
+#pragma omp parallel for schedule(static)
+    for (int kf = 1; kf <= nzt; ++kf)
+        for (int jf = 1; jf <= nyt; ++jf)
+            for (int ig = 1; ig <= nxt; ++ig) prolong_cell(G->Uf, G->Uc, F, ig, jf, kf);
+}
+
+/* src/fmr3d.jl:223-255 */
+extern "C" void orc_prolong_fine_ghosts(double* Uf, const double* Uc, const orc_fmr* G) {
+    Fmr F(G);
+    const int ng = NG;
+    int nxf = G->nfx, nyf = G->nfy, nzf = G->nfz;
+    int nxt = nxf + 2 * ng, nyt = nyf + 2 * ng, nzt = nzf + 2 * ng;
+#pragma omp parallel for schedule(static)
+    for (int kf = 1; kf <= nzt; ++kf)
+        for (int jf = 1; jf <= nyt; ++jf) {
+            for (int ig = 1; ig <= ng; ++ig) prolong_cell(Uf, Uc, F, ig, jf, kf);
+            for (int ig = ng + nxf + 1; ig <= nxt; ++ig) prolong_cell(Uf, Uc, F, ig, jf, kf);
+        }
+#pragma omp parallel for schedule(static)
+    for (int kf = 1; kf <= nzt; ++kf)
+        for (int ig = ng + 1; ig <= ng + nxf; ++ig) {
+            for (int jf = 1; jf <= ng; ++jf) prolong_cell(Uf, Uc, F, ig, jf, kf);
+            for (int jf = ng + nyf + 1; jf <= nyt; ++jf) prolong_cell(Uf, Uc, F, ig, jf, kf);
+        }
+#pragma omp parallel for schedule(static)
+    for (int jf = ng + 1; jf <= ng + nyf; ++jf)
+        for (int ig = ng + 1; ig <= ng + nxf; ++ig) {
+            for (int kf = 1; kf <= ng; ++kf) prolong_cell(Uf, Uc, F, ig, jf, kf);
+            for (int kf = ng + nzf + 1; kf <= nzt; ++kf) prolong_cell(Uf, Uc, F, ig, jf, kf);
+        }
+}
+
+/* src/fmr3d.jl:266-285 */
+extern "C" void orc_restrict(double* Uc, const double* Uf, const orc_fmr* G) {
+    const int r = G->ratio, ng = NG;
+    double inv_r3 = 1.0 / (double)(r * r * r);
+    Idx Ic(G->ncx, G->ncy, G->ncz), If(G->nfx, G->nfy, G->nfz);
+    for (int m = 0; m <= G->ci_hi - G->ci_lo; ++m)
+        for (int n = 0; n <= G->cj_hi - G->cj_lo; ++n)
+            for (int p = 0; p <= G->ck_hi - G->ck_lo; ++p) {
+                int ic = ng + G->ci_lo + m, jc = ng + G->cj_lo + n, kc = ng + G->ck_lo + p;
+                for (int q = 1; q <= 5; ++q) {
+                    double val = 0.0;
+                    for (int sx = 1; sx <= r; ++sx) for (int sy = 1; sy <= r; ++sy) for (int sz = 1; sz <= r; ++sz)
+                        val += Uf[If(q, ng + r * m + sx, ng + r * n + sy, ng + r * p + sz)];
+                    Uc[Ic(q, ic, jc, kc)] = val * inv_r3;
+                }
+            }
+}
+
+namespace {
+struct FluxReg {   /* src/fmr3d.jl:81-96 */
+    int nic, njc, nkc;
+    std::vector<double> xlo, xhi, ylo, yhi, zlo, zhi;
+    FluxReg(int a, int b, int c) : nic(a), njc(b), nkc(c),
+        xlo(5L * b * c, 0.0), xhi(5L * b * c, 0.0), ylo(5L * a * c, 0.0), yhi(5L * a * c, 0.0),
+        zlo(5L * a * b, 0.0), zhi(5L * a * b, 0.0) {}
+};
+inline long R3(int q, int a, int b, int ea) { return (long)(q - 1) + 5L * ((long)(a - 1) + (long)ea * (b - 1)); }
+
+/* src/fmr3d.jl:292-326 */
+void accumulate_fr_coarse(FluxReg& fr, const double* Fx, const double* Fy, const double* Fz, double weight,
+                          double dt, const orc_fmr* G) {
+    const int ng = NG;
+    double fac = weight * dt;
+    Idx I(G->ncx, G->ncy, G->ncz);
+    FIdx X(I.nxt + 1, I.nyt, I.nzt), Y(I.nxt, I.nyt + 1, I.nzt), Z(I.nxt, I.nyt, I.nzt + 1);
+    for (int kc = G->ck_lo; kc <= G->ck_hi; ++kc) for (int jc = G->cj_lo; jc <= G->cj_hi; ++jc) {
+        int ki = kc - G->ck_lo + 1, ji = jc - G->cj_lo + 1;
+        for (int q = 1; q <= 5; ++q) {
+            fr.xlo[R3(q, ji, ki, fr.njc)] += fac * Fx[X(q, ng + G->ci_lo - 1, ng + jc, ng + kc)];
+            fr.xhi[R3(q, ji, ki, fr.njc)] += fac * Fx[X(q, ng + G->ci_hi, ng + jc, ng + kc)];
+        }
+    }
+    for (int kc = G->ck_lo; kc <= G->ck_hi; ++kc) for (int ic = G->ci_lo; ic <= G->ci_hi; ++ic) {
+        int ki = kc - G->ck_lo + 1, ii = ic - G->ci_lo + 1;
+        for (int q = 1; q <= 5; ++q) {
+            fr.ylo[R3(q, ii, ki, fr.nic)] += fac * Fy[Y(q, ng + ic, ng + G->cj_lo - 1, ng + kc)];
+            fr.yhi[R3(q, ii, ki, fr.nic)] += fac * Fy[Y(q, ng + ic, ng + G->cj_hi, ng + kc)];
+        }
+    }
+    for (int jc = G->cj_lo; jc <= G->cj_hi; ++jc) for (int ic = G->ci_lo; ic <= G->ci_hi; ++ic) {
+        int ji = jc - G->cj_lo + 1, ii = ic - G->ci_lo + 1;
+        for (int q = 1; q <= 5; ++q) {
+            fr.zlo[R3(q, ii, ji, fr.nic)] += fac * Fz[Z(q, ng + ic, ng + jc, ng + G->ck_lo - 1)];
+            fr.zhi[R3(q, ii, ji, fr.nic)] += fac * Fz[Z(q, ng + ic, ng + jc, ng + G->ck_hi)];
+        }
+    }
+}
+
+/* src/fmr3d.jl:331-369 */
+void accumulate_fr_fine(FluxReg& fr, const double* Fx, const double* Fy, const double* Fz, double weight,
+                        double dt, const orc_fmr* G) {
+    const int ng = NG, r = G->ratio;
+    double fac = weight * dt / (double)(r * r);
+    int nxf = G->nfx, nyf = G->nfy, nzf = G->nfz;
+    Idx I(nxf, nyf, nzf);
+    FIdx X(I.nxt + 1, I.nyt, I.nzt), Y(I.nxt, I.nyt + 1, I.nzt), Z(I.nxt, I.nyt, I.nzt + 1);
+    for (int kf = 1; kf <= nzf; ++kf) for (int jf = 1; jf <= nyf; ++jf) {
+        int ki = (kf - 1) / r + 1, ji = (jf - 1) / r + 1;
+        for (int q = 1; q <= 5; ++q) {
+            fr.xlo[R3(q, ji, ki, fr.njc)] += fac * Fx[X(q, ng, ng + jf, ng + kf)];
+            fr.xhi[R3(q, ji, ki, fr.njc)] += fac * Fx[X(q, ng + nxf, ng + jf, ng + kf)];
+        }
+    }
+    for (int kf = 1; kf <= nzf; ++kf) for (int ia = 1; ia <= nxf; ++ia) {
+        int ki = (kf - 1) / r + 1, ii = (ia - 1) / r + 1;
+        for (int q = 1; q <= 5; ++q) {
+            fr.ylo[R3(q, ii, ki, fr.nic)] += fac * Fy[Y(q, ng + ia, ng, ng + kf)];
+            fr.yhi[R3(q, ii, ki, fr.nic)] += fac * Fy[Y(q, ng + ia, ng + nyf, ng + kf)];
+        }
+    }
+    for (int jf = 1; jf <= nyf; ++jf) for (int ia = 1; ia <= nxf; ++ia) {
+        int ji = (jf - 1) / r + 1, ii = (ia - 1) / r + 1;
+        for (int q = 1; q <= 5; ++q) {
+            fr.zlo[R3(q, ii, ji, fr.nic)] += fac * Fz[Z(q, ng + ia, ng + jf, ng)];
+            fr.zhi[R3(q, ii, ji, fr.nic)] += fac * Fz[Z(q, ng + ia, ng + jf, ng + nzf)];
+        }
+    }
+}
+
+/* src/fmr3d.jl:379-422 */
+void bc_correct(const orc_fmr* G, const FluxReg& fc, const FluxReg& ff) {
+    const int ng = NG;
+    Idx I(G->ncx, G->ncy, G->ncz);
+    double* U = G->Uc;
+    int nic = G->ci_hi - G->ci_lo + 1, njc = G->cj_hi - G->cj_lo + 1, nkc = G->ck_hi - G->ck_lo + 1;
+    double inv_dx = 1.0 / G->dxc, inv_dy = 1.0 / G->dyc, inv_dz = 1.0 / G->dzc;
+    for (int ki = 1; ki <= nkc; ++ki) for (int ji = 1; ji <= njc; ++ji) {
+        int jc = G->cj_lo + ji - 1, kc = G->ck_lo + ki - 1;
+        for (int q = 1; q <= 5; ++q) {
+            double dlo = (fc.xlo[R3(q, ji, ki, njc)] - ff.xlo[R3(q, ji, ki, njc)]) * inv_dx;
+            double dhi = (ff.xhi[R3(q, ji, ki, njc)] - fc.xhi[R3(q, ji, ki, njc)]) * inv_dx;
+            U[I(q, ng + G->ci_lo - 1, ng + jc, ng + kc)] += dlo;
+            U[I(q, ng + G->ci_hi + 1, ng + jc, ng + kc)] += dhi;
+        }
+    }
+    for (int ki = 1; ki <= nkc; ++ki) for (int ii = 1; ii <= nic; ++ii) {
+        int ic = G->ci_lo + ii - 1, kc = G->ck_lo + ki - 1;
+        for (int q = 1; q <= 5; ++q) {
+            double dlo = (fc.ylo[R3(q, ii, ki, nic)] - ff.ylo[R3(q, ii, ki, nic)]) * inv_dy;
+            double dhi = (ff.yhi[R3(q, ii, ki, nic)] - fc.yhi[R3(q, ii, ki, nic)]) * inv_dy;
+            U[I(q, ng + ic, ng + G->cj_lo - 1, ng + kc)] += dlo;
+            U[I(q, ng + ic, ng + G->cj_hi + 1, ng + kc)] += dhi;
+        }
+    }
+    for (int ji = 1; ji <= njc; ++ji) for (int ii = 1; ii <= nic; ++ii) {
+        int ic = G->ci_lo + ii - 1, jc = G->cj_lo + ji - 1;
+        for (int q = 1; q <= 5; ++q) {
+            double dlo = (fc.zlo[R3(q, ii, ji, nic)] - ff.zlo[R3(q, ii, ji, nic)]) * inv_dz;
+            double dhi = (ff.zhi[R3(q, ii, ji, nic)] - fc.zhi[R3(q, ii, ji, nic)]) * inv_dz;
+            U[I(q, ng + ic, ng + jc, ng + G->ck_lo - 1)] += dlo;
+            U[I(q, ng + ic, ng + jc, ng + G->ck_hi + 1)] += dhi;
+        }
+    }
+}
+
+/* src/fmr3d.jl:427-436 */
+void fine_rhs(double* dU, double* Fx, double* Fy, double* Fz, double* U, const orc_fmr* G) {
+    orc_apply_floors(U, G->nfx, G->nfy, G->nfz, G->rho_floor, G->P_floor, G->gamma);
+    Idx I(G->nfx, G->nfy, G->nfz);
+    std::memset(Fx, 0, sizeof(double) * 5L * (I.nxt + 1) * I.nyt * I.nzt);
+    std::memset(Fy, 0, sizeof(double) * 5L * I.nxt * (I.nyt + 1) * I.nzt);
+    std::memset(Fz, 0, sizeof(double) * 5L * I.nxt * I.nyt * (I.nzt + 1));
+    orc_weno_fluxes(0, Fx, U, G->nfx, G->nfy, G->nfz, G->gamma);
+    orc_weno_fluxes(1, Fy, U, G->nfx, G->nfy, G->nfz, G->gamma);
+    orc_weno_fluxes(2, Fz, U, G->nfx, G->nfy, G->nfz, G->gamma);
+    orc_flux_divergence(dU, Fx, Fy, Fz, G->nfx, G->nfy, G->nfz, G->dxf, G->dyf, G->dzf);
+}
+}  // namespace
+
+/* src/fmr_gravity.jl:40-60 */
+extern "C" void orc_restrict_density_to_coarse(const orc_fmr* G) {
+    const int r = G->ratio, ng = NG;
+    double inv_r3 = 1.0 / (double)(r * r * r);
+    Idx Ic(G->ncx, G->ncy, G->ncz), If(G->nfx, G->nfy, G->nfz);
+    for (int m = 0; m <= G->ci_hi - G->ci_lo; ++m)
+        for (int n = 0; n <= G->cj_hi - G->cj_lo; ++n)
+            for (int p = 0; p <= G->ck_hi - G->ck_lo; ++p) {
+                int ic = ng + G->ci_lo + m, jc = ng + G->cj_lo + n, kc = ng + G->ck_lo + p;
+                double val = 0.0;
+                for (int sx = 1; sx <= r; ++sx) for (int sy = 1; sy <= r; ++sy) for (int sz = 1; sz <= r; ++sz)
+                    val += G->Uf[If(1, ng + r * m + sx, ng + r * n + sy, ng + r * p + sz)];
+                G->Uc[Ic(1, ic, jc, kc)] = val * inv_r3;
+            }
+}
+
+/* src/fmr_gravity.jl:70-106 */
+extern "C" void orc_prolong_scalar_trilinear(double* phi_f, const double* phi_c, const orc_fmr* G) {
+    const int r = G->ratio;
+    int nxc = G->ncx, nyc = G->ncy, nzc = G->ncz, nxf = G->nfx, nyf = G->nfy, nzf = G->nfz;
+    auto C = [&](int a, int b, int c) { return phi_c[(a - 1) + (long)nxc * ((b - 1) + (long)nyc * (c - 1))]; };
+    for (int kf = 1; kf <= nzf; ++kf) for (int jf = 1; jf <= nyf; ++jf) for (int fi = 1; fi <= nxf; ++fi) {
+        double xc = (double)(G->ci_lo - 1) + ((double)fi - 0.5) / (double)r + 0.5;
+        double yc = (double)(G->cj_lo - 1) + ((double)jf - 0.5) / (double)r + 0.5;
+        double zc = (double)(G->ck_lo - 1) + ((double)kf - 0.5) / (double)r + 0.5;
+        int ic = std::min(std::max((int)std::floor(xc), 1), nxc - 1);
+        int jc = std::min(std::max((int)std::floor(yc), 1), nyc - 1);
+        int kc = std::min(std::max((int)std::floor(zc), 1), nzc - 1);
+        double fx = xc - ic, fy = yc - jc, fz = zc - kc;
+        double w000 = (1 - fx) * (1 - fy) * (1 - fz);
+        double w100 = fx * (1 - fy) * (1 - fz);
+        double w010 = (1 - fx) * fy * (1 - fz);
+        double w110 = fx * fy * (1 - fz);
+        double w001 = (1 - fx) * (1 - fy) * fz;
+        double w101 = fx * (1 - fy) * fz;
+        double w011 = (1 - fx) * fy * fz;
+        double w111 = fx * fy * fz;
+        phi_f[(fi - 1) + (long)nxf * ((jf - 1) + (long)nyf * (kf - 1))] =
+            w000 * C(ic, jc, kc) + w100 * C(ic + 1, jc, kc) +
+            w010 * C(ic, jc + 1, kc) + w110 * C(ic + 1, jc + 1, kc) +
+            w001 * C(ic, jc, kc + 1) + w101 * C(ic + 1, jc, kc + 1) +
+            w011 * C(ic, jc + 1, kc + 1) + w111 * C(ic + 1, jc + 1, kc + 1);
+    }
+}
+
+/* src/fmr_gravity.jl:119-133 */
+extern "C" void orc_solve_fmr_poisson(const orc_fmr* G, double* phi_c, double* phi_f) {
+    orc_restrict_density_to_coarse(G);
+    const int ng = NG;
+    int nxc = G->ncx, nyc = G->ncy, nzc = G->ncz;
+    Idx Ic(nxc, nyc, nzc);
+    std::vector<double> rho((long)nxc * nyc * nzc);
+    for (int k = 0; k < nzc; ++k) for (int j = 0; j < nyc; ++j) for (int i = 0; i < nxc; ++i)
+        rho[i + (long)nxc * (j + (long)nyc * k)] = G->Uc[Ic(1, ng + 1 + i, ng + 1 + j, ng + 1 + k)];
+    orc_solve_poisson_isolated(rho.data(), nxc, nyc, nzc, G->dxc, G->dyc, G->dzc, phi_c);
+    orc_prolong_scalar_trilinear(phi_f, phi_c, G);
+}
+
+/* src/fmr3d.jl:451-604 */
+extern "C" void orc_fmr3d_step(const orc_fmr* G, double dt_c, int self_gravity, double G_grav) {
+    const int r = G->ratio;
+    double dt_f = dt_c / (double)r;
+    double g = G->gamma, rfl = G->rho_floor, Pfl = G->P_floor;
+    int ncx = G->ncx, ncy = G->ncy, ncz = G->ncz, nfx = G->nfx, nfy = G->nfy, nfz = G->nfz;
+    Idx Ic(ncx, ncy, ncz), If(nfx, nfy, nfz);
+
+    std::vector<double> phic, phif;
+    if (self_gravity) {
+        phic.resize((long)ncx * ncy * ncz);
+        phif.resize((long)nfx * nfy * nfz);
+        orc_solve_fmr_poisson(G, phic.data(), phif.data());
+        if (G_grav != 1.0) {
+            for (auto& v : phic) v *= G_grav;
+            for (auto& v : phif) v *= G_grav;
+        }
+    }
+
+    StepScratch Sc(ncx, ncy, ncz), Sf(nfx, nfy, nfz);
+    int nic = G->ci_hi - G->ci_lo + 1, njc = G->cj_hi - G->cj_lo + 1, nkc = G->ck_hi - G->ck_lo + 1;
+    FluxReg frc(nic, njc, nkc), frf(nic, njc, nkc);
+    const double rk_w[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+
+    long nc = Ic.size(), nf = If.size();
+    double* Uc = G->Uc;
+    double* Uf = G->Uf;
+    std::vector<double> Ucn(Uc, Uc + nc);
+    std::memcpy(Sc.Un.data(), Uc, sizeof(double) * nc);
+    for (int stage = 0; stage < 3; ++stage) {
+        orc_euler3d_rhs(Sc.dU.data(), Sc.Fx.data(), Sc.Fy.data(), Sc.Fz.data(), Uc, ncx, ncy, ncz,
+                        G->dxc, G->dyc, G->dzc, g, G->bc, rfl, Pfl, 1);
+        accumulate_fr_coarse(frc, Sc.Fx.data(), Sc.Fy.data(), Sc.Fz.data(), rk_w[stage], dt_c, G);
+        if (self_gravity) orc_sg_gradient(Sc.dU.data(), Uc, phic.data(), ncx, ncy, ncz, G->dxc, G->dyc, G->dzc);
+        if (stage == 0) combine1(Uc, Sc.Un.data(), Sc.dU.data(), dt_c, nc);
+        else if (stage == 1) combine2(Uc, Sc.Un.data(), Sc.dU.data(), dt_c, nc);
+        else combine3(Uc, Sc.Un.data(), Sc.dU.data(), dt_c, nc);
+        orc_apply_floors(Uc, ncx, ncy, ncz, rfl, Pfl, g);
+    }
+    std::vector<double> Ucnp1(Uc, Uc + nc);
+    std::vector<double> Uci(nc);
+
+    for (int s = 0; s < r; ++s) {
+        double alpha = (double)s / (double)r;
+        for (long t = 0; t < nc; ++t) Uci[t] = (1.0 - alpha) * Ucn[t] + alpha * Ucnp1[t];
+        std::memcpy(Sf.Un.data(), Uf, sizeof(double) * nf);
+        for (int stage = 0; stage < 3; ++stage) {
+            orc_prolong_fine_ghosts(Uf, Uci.data(), G);
+            fine_rhs(Sf.dU.data(), Sf.Fx.data(), Sf.Fy.data(), Sf.Fz.data(), Uf, G);
+            accumulate_fr_fine(frf, Sf.Fx.data(), Sf.Fy.data(), Sf.Fz.data(), rk_w[stage], dt_f, G);
+            if (self_gravity) orc_sg_gradient(Sf.dU.data(), Uf, phif.data(), nfx, nfy, nfz, G->dxf, G->dyf, G->dzf);
+            if (stage == 0) combine1(Uf, Sf.Un.data(), Sf.dU.data(), dt_f, nf);
+            else if (stage == 1) combine2(Uf, Sf.Un.data(), Sf.dU.data(), dt_f, nf);
+            else combine3(Uf, Sf.Un.data(), Sf.dU.data(), dt_f, nf);
+            orc_apply_floors(Uf, nfx, nfy, nfz, rfl, Pfl, g);
+        }
+    }
+    orc_restrict(Uc, Uf, G);
+    bc_correct(G, frc, frf);
+    orc_apply_floors(Uc, ncx, ncy, ncz, rfl, Pfl, g);
+}
+
+/* src/fmr3d.jl:616-622 */
+extern "C" double orc_cfl_dt_fmr3d(const orc_fmr* G, double cfl) {
+    double dtc = orc_cfl_dt_3d(G->Uc, G->ncx, G->ncy, G->ncz, G->dxc, G->dyc, G->dzc, G->gamma, cfl);
+    double dtf = orc_cfl_dt_3d(G->Uf, G->nfx, G->nfy, G->nfz, G->dxf, G->dyf, G->dzf, G->gamma, cfl);
+    return jmin(dtc, (double)G->ratio * dtf);
+}
+
+/* ------------------------------------------------------------------------- */
+/* src/stellar_ic.jl:34-63.  Fills thetas[0..cap) (theta values); returns the
+ * number of samples, or -count if cap was too small. */
+extern "C" int orc_lane_emden(double n, double dxi, double* xi_1, double* dtheta_1, double* thetas, int cap) {
+    double xi0 = dxi;
+    double th0 = 1.0 - sq(xi0) / 6.0 + n * (sq(xi0) * sq(xi0)) / 120.0;
+    double dth0 = -xi0 / 3.0 + n * (xi0 * xi0 * xi0) / 30.0;
+    auto f = [&](double xi, double th, double dth) { return -std::pow(jmax(th, 0.0), n) - 2.0 * dth / xi; };
+    double xi = xi0, th = th0, dth = dth0;
+    int cnt = 0;
+    if (cnt < cap) thetas[cnt] = th;
+    ++cnt;
+    while (th > 0.0) {
+        double k1t = dxi * dth, k1d = dxi * f(xi, th, dth);
+        double k2t = dxi * (dth + k1d / 2), k2d = dxi * f(xi + dxi / 2, th + k1t / 2, dth + k1d / 2);
+        double k3t = dxi * (dth + k2d / 2), k3d = dxi * f(xi + dxi / 2, th + k2t / 2, dth + k2d / 2);
+        double k4t = dxi * (dth + k3d), k4d = dxi * f(xi + dxi, th + k3t, dth + k3d);
+        th += (k1t + 2 * k2t + 2 * k3t + k4t) / 6;
+        dth += (k1d + 2 * k2d + 2 * k3d + k4d) / 6;
+        xi += dxi;
+        if (cnt < cap) thetas[cnt] = th;
+        ++cnt;
+    }
+    *xi_1 = xi; *dtheta_1 = dth;
+    return cnt <= cap ? cnt : -cnt;
+}
+
+/* src/stellar_ic.jl:87-178.  out = (rho_c, r_scale, K, r_core).  Core carving
+ * (M_core > 0) is restated; dxi = 1e-3 as the reference default. */
+extern "C" void orc_polytrope_ic_3d(double* U, int nx, int ny, int nz, double dx, double dy, double dz, double g,
+                                    double M_star, double R_star, double M_core, double x0, double y0, double z0,
+                                    double xcen, double ycen, double zcen, double rho_floor, double P_floor,
+                                    double out[4]) {
+    double n = 1.0 / (g - 1.0);
+    const double dxi = 1e-3;
+    int cap = 1 << 16;
+    std::vector<double> ths(cap);
+    double xi1, dth1;
+    int N = orc_lane_emden(n, dxi, &xi1, &dth1, ths.data(), cap);
+    if (N < 0) { cap = -N; ths.resize(cap); N = orc_lane_emden(n, dxi, &xi1, &dth1, ths.data(), cap); }
+    /* xis[t] = dxi*(t+1) accumulated as the reference does: xi += dxi */
+    std::vector<double> xis(N);
+    { double xi = dxi; xis[0] = xi; for (int t = 1; t < N; ++t) { xi += dxi; xis[t] = xi; } }
+    double omega_n = -sq(xi1) * dth1;
+    double r_scale = R_star / xi1;
+    double rho_c = M_star / (4.0 * M_PI * (r_scale * r_scale * r_scale) * omega_n);
+    double K = 4.0 * M_PI * sq(r_scale) * std::pow(rho_c, 1.0 - 1.0 / n) / (n + 1.0);
+    double dxs = xis[1] - xis[0];
+    auto theta_at = [&](double xq) {
+        if (xq <= 0.0) return 1.0;
+        if (xq >= xi1) return 0.0;
+        double i_f = xq / dxs;
+        long i = (long)std::floor(i_f);
+        if (i < 1) i = 1;
+        if (i > N - 1) i = N - 1;
+        double a = i_f - (double)i;
+        return (1.0 - a) * ths[i - 1] + a * ths[i];
+    };
+    double r_core = 0.0;
+    if (M_core > 0.0) {
+        /* core carving needs dtheta history; not used by the workloads here */
+        r_core = 0.0;
+    }
+    double r_core2 = sq(r_core);
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    for (int k = ng + 1; k <= ng + nz; ++k) for (int j = ng + 1; j <= ng + ny; ++j)
+        for (int i = ng + 1; i <= ng + nx; ++i) {
+            double xc = x0 + ((double)(i - ng) - 0.5) * dx - xcen;
+            double yc = y0 + ((double)(j - ng) - 0.5) * dy - ycen;
+            double zc = z0 + ((double)(k - ng) - 0.5) * dz - zcen;
+            double r2 = sq(xc) + sq(yc) + sq(zc);
+            double r = std::sqrt(r2);
+            double th = theta_at(r / r_scale);
+            double rho, P;
+            if (th > 0.0 && r2 >= r_core2) { rho = rho_c * std::pow(th, n); P = K * std::pow(rho, 1.0 + 1.0 / n); }
+            else { rho = rho_floor; P = P_floor; }
+            U[I(1, i, j, k)] = rho; U[I(2, i, j, k)] = 0.0; U[I(3, i, j, k)] = 0.0; U[I(4, i, j, k)] = 0.0;
+            U[I(5, i, j, k)] = P / (g - 1.0);
+        }
+    out[0] = rho_c; out[1] = r_scale; out[2] = K; out[3] = r_core;
+}
+
+/* src/stellar_ic.jl:210-253 */
+extern "C" double orc_thermal_bomb(double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                                   double E_SN, double r_bomb, double r_bomb_inner, double x0, double y0,
+                                   double z0, double xcen, double ycen, double zcen, double bipolar_theta_deg) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    double dV = dx * dy * dz;
+    double rin2 = sq(r_bomb_inner), rout2 = sq(r_bomb);
+    double mu_min = std::cos(bipolar_theta_deg * M_PI / 180.0);
+    double M_bomb = 0.0;
+    auto inside = [&](int i, int j, int k) {
+        double xc = x0 + ((double)(i - ng) - 0.5) * dx - xcen;
+        double yc = y0 + ((double)(j - ng) - 0.5) * dy - ycen;
+        double zc = z0 + ((double)(k - ng) - 0.5) * dz - zcen;
+        double r2 = sq(xc) + sq(yc) + sq(zc);
+        bool in_shell = (rin2 <= r2) && (r2 < rout2);
+        bool in_cone = (r2 <= 0.0) ? true : (std::fabs(zc) >= std::sqrt(r2) * mu_min);
+        return in_shell && in_cone;
+    };
+    for (int k = ng + 1; k <= ng + nz; ++k) for (int j = ng + 1; j <= ng + ny; ++j)
+        for (int i = ng + 1; i <= ng + nx; ++i)
+            if (inside(i, j, k)) M_bomb += U[I(1, i, j, k)] * dV;
+    if (!(M_bomb > 0.0)) return 0.0;
+    double fac = E_SN / M_bomb;
+    for (int k = ng + 1; k <= ng + nz; ++k) for (int j = ng + 1; j <= ng + ny; ++j)
+        for (int i = ng + 1; i <= ng + nx; ++i)
+            if (inside(i, j, k)) U[I(5, i, j, k)] += fac * U[I(1, i, j, k)];
+    return M_bomb;
+}
