@@ -1,0 +1,293 @@
+"""Benchmark: cell-updates/s per SSP-RK3 step on the 3D Sedov blast.
+
+Workload (default): Sedov 256^3 on [-1,1]^3, gamma=5/3, ambient rho=1,
+p=1e-5, E=1 deposited in r < 3.5 dx (the reference's sedov_ic_3d!), outflow,
+floors rho 1e-6 / P 1e-6.  A step is one CFL dt reduction plus one full RK3
+step, the loop the reference drivers run (cfl_dt_3d + euler3d_step!).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bsn|reference]
+                  [--n 256] [--path f64]
+
+`value` is device-resident throughput over K steps (state in HBM).  `e2e`
+runs the same step through the public host-buffer path: the state is copied
+host->device from pinned memory, stepped, and copied back every step.  With
+N>1 (torchrun) every rank runs an independent replica ("replicas only": the
+reference path is single-device) and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "binary-supernova_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+NG = 3
+GAMMA = 5.0 / 3.0
+CFL = 0.4
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def sedov_host(n):
+    """Sedov initial state (src/euler3d.jl:275-316) on the host, F-ordered."""
+    import oracle
+    L = 1.0
+    dx = 2 * L / n
+    U = oracle.state(n, n, n)
+    oracle.sedov_ic_3d(U, dx, dx, dx, GAMMA, E_blast=1.0, r_inject=3.5 * dx, rho_bg=1.0, P_floor=1e-5,
+                       x_offset=-L, y_offset=-L, z_offset=-L)
+    return U, dx
+
+
+def cpu_reference_rate(n, threads, nz_sample, steps):
+    """Oracle (CPU restatement of the reference path) on a z-slab sample of
+    the Sedov n^3 workload: cell-updates/s with `threads` OpenMP threads."""
+    import numpy as np
+    import oracle
+    oracle.build()
+    oracle.set_threads(threads)
+    U, dx = sedov_host(n)
+    k0 = NG + n // 2 - nz_sample // 2
+    S = np.asfortranarray(U[:, :, :, k0 - NG:k0 + nz_sample + NG])
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = oracle.cfl_dt_3d(S, dx, dx, dx, GAMMA, CFL)
+        oracle.euler3d_step(S, dx, dx, dx, dt, GAMMA, rho_floor=1e-6, P_floor=1e-6)
+    el = time.perf_counter() - t0
+    return n * n * nz_sample * steps / el, el
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    nz = max(4, min(args.n, int(os.environ.get("BSN_REF_SLAB", "16"))))
+    for _ in range(args.warmup):
+        cpu_reference_rate(args.n, threads, nz, 1)
+    rate, el = cpu_reference_rate(args.n, threads, nz, args.steps)
+    line = {
+        "impl": "reference", "metric": "cell-updates/s per RK3 step (Sedov 3D, FP64)", "value": rate,
+        "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (Sedov initial condition)",
+        "config": {"workload": f"sedov{args.n}^3", "path": "reference CPU restatement (oracle), FP64",
+                   "sample": f"{args.n}x{args.n}x{nz} z-slab through the blast centre per step"},
+        "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} RK3 steps of a {args.n}x{args.n}x{nz} slab of Sedov {args.n}^3"},
+        "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_bsn(args, rank, world):
+    import ctypes as C
+    import numpy as np
+    import torch
+    import bsn
+    from bsn._lib import load
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    n = args.n
+    U0, dx = sedov_host(n)
+    ncell = n ** 3
+    kw = dict(rho_floor=1e-6, P_floor=1e-6)
+    Ud = torch.from_numpy(U0).cuda()
+    ctx = bsn.context()
+    L = load()
+
+    def step(U):
+        dt = bsn.cfl_dt_3d(U, n, n, n, dx, dx, dx, GAMMA, CFL)
+        bsn.euler3d_step(U, n, n, n, dx, dx, dx, dt, GAMMA, **kw)
+
+    for _ in range(args.warmup):
+        step(Ud)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = bsn.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            step(Ud)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = bsn.launch_count() - launches0
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * ncell * args.steps / (ms / 1e3)
+
+    # roofline: average stage-kernel launch time from events around each launch
+    L.bsn_ctx_set_profiling(ctx, 1)
+    for _ in range(3):
+        step(Ud)
+    tot, cnt = C.c_double(), C.c_longlong()
+    L.bsn_ctx_kernel_stats(ctx, b"stage_kernel", C.byref(tot), C.byref(cnt))
+    L.bsn_ctx_set_profiling(ctx, 0)
+    t_stage = tot.value / max(cnt.value, 1) / 1e3
+    # algorithmic state traffic: 40 words/cell per RK3 step over 3 stage launches
+    alg_bytes = 40 * 8 * ncell / 3.0
+    hbm, hbm_kind = peaks()
+    achieved = alg_bytes / t_stage / 1e9
+
+    # e2e through the host-buffer path (pinned host state, H2D + step + D2H)
+    Uh = torch.from_numpy(U0.copy(order="F")).pin_memory()
+    Ue = torch.empty_like(Ud)
+    nbytes = Uh.numel() * 8
+    for _ in range(2):
+        Ue.copy_(Uh, non_blocking=True); step(Ue); Uh.copy_(Ue, non_blocking=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    k_e2e = max(2, min(args.steps, 10))
+    e0.record()
+    for _ in range(k_e2e):
+        Ue.copy_(Uh, non_blocking=True)
+        step(Ue)
+        Uh.copy_(Ue, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = world * ncell * k_e2e / (ms_e2e / 1e3)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        nz = 16
+        rate, el = cpu_reference_rate(n, threads, nz, 2)
+        cpu = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+               "sample": f"2 RK3 steps (oracle, FP64) of a {n}x{n}x{nz} z-slab of Sedov {n}^3, {el:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s per RK3 step (Sedov 3D, FP64 WENO5-Z+HLLC+SSP-RK3)",
+            "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (Sedov initial condition, sedov_ic_3d!)",
+            "config": {"workload": f"sedov{n}^3", "grid": [n, n, n], "path": args.path,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": f"state {Ud.numel() * 8 / 1e6:.0f} MB per array > 126 MB L2 (no flush needed)"},
+            "roofline": {"bound": "hbm", "kernel": "stage_kernel", "achieved": achieved, "peak": hbm,
+                         "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": t_stage * 1e3,
+                         "note": "FP64 stencil kernel is FP64-pipe bound; HBM fraction of algorithmic bytes"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes, "steps": k_e2e},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="bsn", choices=["bsn", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--path", default="f64", choices=["f64"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_bsn(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

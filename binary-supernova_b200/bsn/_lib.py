@@ -1,0 +1,112 @@
+"""ctypes binding of libbsn.so (the C ABI declared in include/bsn.h).
+
+The library is built in-tree (binary-supernova_b200/build_lib.py) and loaded
+from this package directory.  There is no fallback: if the shared library is
+missing or a CUDA device is absent, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbsn.so")
+
+BSN_OK, BSN_ERR_ARG, BSN_ERR_CUDA, BSN_ERR_TIMEOUT, BSN_ERR_NONFINITE, BSN_ERR_UNSUPPORTED, BSN_ERR_NOMEM = range(7)
+_ERRNAMES = {1: "BSN_ERR_ARG", 2: "BSN_ERR_CUDA", 3: "BSN_ERR_TIMEOUT", 4: "BSN_ERR_NONFINITE",
+             5: "BSN_ERR_UNSUPPORTED", 6: "BSN_ERR_NOMEM"}
+
+
+class BSNError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class bsn_bh(C.Structure):
+    """Mirror of the reference's mutable BlackHole (src/BinarySupernova.jl:130-137)."""
+    _fields_ = [("pos", C.c_double * 3), ("vel", C.c_double * 3), ("mass", C.c_double),
+                ("eps", C.c_double), ("c_code", C.c_double), ("r_floor", C.c_double)]
+
+    def __repr__(self):
+        return (f"BlackHole(pos={list(self.pos)}, vel={list(self.vel)}, mass={self.mass}, eps={self.eps}, "
+                f"c_code={self.c_code}, r_floor={self.r_floor})")
+
+
+class bsn_fmr2(C.Structure):
+    _fields_ = [("Uc", C.c_void_p), ("ncx", C.c_int), ("ncy", C.c_int), ("ncz", C.c_int),
+                ("dxc", C.c_double), ("dyc", C.c_double), ("dzc", C.c_double),
+                ("Uf", C.c_void_p), ("nfx", C.c_int), ("nfy", C.c_int), ("nfz", C.c_int),
+                ("dxf", C.c_double), ("dyf", C.c_double), ("dzf", C.c_double),
+                ("ratio", C.c_int),
+                ("ci_lo", C.c_int), ("ci_hi", C.c_int), ("cj_lo", C.c_int), ("cj_hi", C.c_int),
+                ("ck_lo", C.c_int), ("ck_hi", C.c_int),
+                ("gamma", C.c_double), ("bc", C.c_int), ("rho_floor", C.c_double), ("P_floor", C.c_double)]
+
+
+_V, _I, _D, _P, _LL = C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_longlong
+_dp = C.POINTER(C.c_double)
+_BH = C.POINTER(bsn_bh)
+_FMR = C.POINTER(bsn_fmr2)
+
+# name -> (restype, argtypes); mirrors include/bsn.h
+SIGNATURES = {
+    "bsn_ctx_create": (_I, [C.POINTER(C.c_void_p), _I, _V]),
+    "bsn_ctx_destroy": (_I, [_V]),
+    "bsn_ctx_set_stream": (_I, [_V, _V]),
+    "bsn_ctx_synchronize": (_I, [_V]),
+    "bsn_last_error": (C.c_char_p, [_V]),
+    "bsn_version": (C.c_char_p, []),
+    "bsn_ctx_launch_count": (_LL, [_V]),
+    "bsn_ctx_set_profiling": (_I, [_V, _I]),
+    "bsn_ctx_kernel_stats": (_I, [_V, C.c_char_p, _dp, C.POINTER(C.c_longlong)]),
+    "bsn_fill_ghost_3d_f64": (_I, [_V, _P, _I, _I, _I, _I]),
+    "bsn_apply_floors_3d_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D]),
+    "bsn_euler3d_rhs_f64": (_I, [_V, _P, _P, _P, _P, _P, _I, _I, _I, _D, _D, _D, _D, _I, _D, _D, _I]),
+    "bsn_euler3d_step_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _I, _D, _D]),
+    "bsn_cfl_dt_3d_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _dp]),
+    "bsn_add_bh_gravity_source_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D, _BH, _I, _D, _D, _D]),
+    "bsn_gas_force_on_bh_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _BH, _D, _D, _D, _dp]),
+    "bsn_add_sink_sources_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D, _BH, _I, _D, _D, _D, _D, _I, _D]),
+    "bsn_accrete_f64": (_I, [_V, _BH, _P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _D, _D, _D]),
+    "bsn_nbody_step": (_I, [_BH, _I, _D, _dp]),
+    "bsn_kepler_init": (_I, [_BH, _dp, _dp, _D, _dp]),
+    "bsn_kepler_update": (_I, [_BH, _dp, _D]),
+    "bsn_solve_poisson_isolated_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _P]),
+    "bsn_sg_gradient_f64": (_I, [_V, _P, _P, _P, _I, _I, _I, _D, _D, _D]),
+    "bsn_add_self_gravity_source_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D]),
+    "bsn_coupled_step_f64": (_I, [_V, _P, _BH, _I, _D, _D, _I, _I, _I, _D, _D, _D, _D, _D, _D, _D, _D,
+                                  _I, _I, _D, _D, _I, _dp]),
+    "bsn_fmr_prolong_all_f64": (_I, [_V, _FMR]),
+    "bsn_fmr_prolong_fine_ghosts_f64": (_I, [_V, _P, _P, _FMR]),
+    "bsn_fmr_restrict_f64": (_I, [_V, _P, _P, _FMR]),
+    "bsn_fmr3d_step_f64": (_I, [_V, _FMR, _D, _I, _D]),
+    "bsn_cfl_dt_fmr3d_f64": (_I, [_V, _FMR, _D, _dp]),
+    "bsn_restrict_density_to_coarse_f64": (_I, [_V, _FMR]),
+    "bsn_solve_fmr_poisson_f64": (_I, [_V, _FMR, _P, _P]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load():
+    """Load libbsn.so and declare every exported entry point."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"libbsn.so not found at {LIB_PATH}: build it with "
+                                   "`python binary-supernova_b200/build_lib.py` (no CPU fallback exists)")
+            L = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+            _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return sorted(SIGNATURES)

@@ -1,0 +1,336 @@
+"""Reference-named entry points over libbsn (FP64 parity path).
+
+Array conventions (the reference's Julia layout, column-major):
+  * state U: torch.float64 CUDA tensor of shape (5, nx+6, ny+6, nz+6) with
+    strides (1, 5, 5*(nx+6), 5*(nx+6)*(ny+6)) -- `state()` makes one, and
+    `torch.from_numpy(fortran_array).cuda()` keeps these strides.
+  * flux arrays: shapes (5,NXT+1,NYT,NZT), (5,NXT,NYT+1,NZT), (5,NXT,NYT,NZT+1).
+  * potentials/densities on the active grid: shape (nx, ny, nz), strides
+    (1, nx, nx*ny).
+Errors raise BSNError (the reference throws on bad input).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from ._lib import BSNError, bsn_bh, bsn_fmr2, load
+
+NG = 3
+BC = {"outflow": 0, "periodic": 1}
+
+__all__ = [
+    "NG", "BSNError", "BlackHole", "state", "flux_arrays", "active_grid", "context", "launch_count",
+    "fill_ghost_3d_outflow", "fill_ghost_3d_periodic", "apply_floors_3d", "euler3d_rhs", "euler3d_step",
+    "cfl_dt_3d", "add_bh_gravity_source", "gas_force_on_bh", "add_sink_sources", "accrete", "r_sink", "t_sink",
+    "nbody_step", "KeplerOrbit", "kepler_update", "solve_poisson_isolated", "add_self_gravity_source",
+    "apply_sg_force_level", "coupled_step", "FMRGrid3D", "fmr3d_step", "cfl_dt_fmr3d", "solve_fmr_poisson",
+    "restrict_density_to_coarse",
+]
+
+# ---------------------------------------------------------------------------
+# context / stream plumbing
+
+_ctx = {}
+
+
+def context(device: int | None = None) -> C.c_void_p:
+    """The library context of a CUDA device (created once per device)."""
+    if not torch.cuda.is_available():
+        raise RuntimeError("bsn needs a CUDA device (sm_100a); no CPU fallback exists")
+    dev = torch.cuda.current_device() if device is None else int(device)
+    if dev not in _ctx:
+        L = load()
+        h = C.c_void_p()
+        rc = L.bsn_ctx_create(C.byref(h), dev, None)
+        if rc != 0:
+            raise BSNError(rc, f"bsn_ctx_create(device={dev}) failed")
+        _ctx[dev] = h
+    h = _ctx[dev]
+    load().bsn_ctx_set_stream(h, C.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    return h
+
+
+def launch_count(device: int | None = None) -> int:
+    """Kernels this process's context has launched on `device`."""
+    return int(load().bsn_ctx_launch_count(context(device)))
+
+
+def _call(name: str, *args):
+    L = load()
+    rc = getattr(L, name)(*args)
+    if rc != 0:
+        msg = L.bsn_last_error(args[0]).decode() if args and isinstance(args[0], C.c_void_p) else name
+        raise BSNError(rc, msg)
+
+
+def _ptr(t) -> C.c_void_p | None:
+    if t is None:
+        return None
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64):
+        raise TypeError("expected a CUDA float64 tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _check_state(U: torch.Tensor, nx: int, ny: int, nz: int, name="U"):
+    want = (5, nx + 2 * NG, ny + 2 * NG, nz + 2 * NG)
+    if tuple(U.shape) != want:
+        raise ValueError(f"{name} has shape {tuple(U.shape)}, expected {want}")
+    X, Y = nx + 2 * NG, ny + 2 * NG
+    if U.stride() != (1, 5, 5 * X, 5 * X * Y):
+        raise ValueError(f"{name} must use the reference column-major layout (strides {U.stride()})")
+
+
+def _check_grid(a: torch.Tensor, nx: int, ny: int, nz: int, name: str):
+    if tuple(a.shape) != (nx, ny, nz) or a.stride() != (1, nx, nx * ny):
+        raise ValueError(f"{name} must be a column-major (nx,ny,nz) array")
+
+
+def state(nx: int, ny: int, nz: int, device="cuda", dtype=torch.float64) -> torch.Tensor:
+    """Zeroed state array U[q,i,j,k] of the reference (5, nx+6, ny+6, nz+6)."""
+    X, Y, Z = nx + 2 * NG, ny + 2 * NG, nz + 2 * NG
+    return torch.zeros((Z, Y, X, 5), device=device, dtype=dtype).permute(3, 2, 1, 0)
+
+
+def flux_arrays(nx: int, ny: int, nz: int, device="cuda"):
+    X, Y, Z = nx + 2 * NG, ny + 2 * NG, nz + 2 * NG
+    mk = lambda a, b, c: torch.zeros((c, b, a, 5), device=device, dtype=torch.float64).permute(3, 2, 1, 0)
+    return mk(X + 1, Y, Z), mk(X, Y + 1, Z), mk(X, Y, Z + 1)
+
+
+def active_grid(nx: int, ny: int, nz: int, device="cuda") -> torch.Tensor:
+    return torch.zeros((nz, ny, nx), device=device, dtype=torch.float64).permute(2, 1, 0)
+
+
+# ---------------------------------------------------------------------------
+# black holes (src/BinarySupernova.jl:130-171)
+
+def BlackHole(pos, vel, mass, eps, c_code, r_floor) -> bsn_bh:
+    return bsn_bh((C.c_double * 3)(*pos), (C.c_double * 3)(*vel), float(mass), float(eps), float(c_code),
+                  float(r_floor))
+
+
+def _bh_array(bhs: Sequence[bsn_bh]):
+    arr = (bsn_bh * max(1, len(bhs)))()
+    for i, b in enumerate(bhs):
+        arr[i] = b
+    return arr
+
+
+def _bh_writeback(bhs, arr):
+    for i, b in enumerate(bhs):
+        C.memmove(C.addressof(b), C.addressof(arr[i]), C.sizeof(bsn_bh))
+
+
+def r_sink(bh: bsn_bh) -> float:
+    """src/BinarySupernova.jl:159"""
+    v = 6.0 * bh.mass / bh.c_code ** 2
+    return v if v > bh.r_floor else bh.r_floor
+
+
+def t_sink(bh: bsn_bh, f_sink: float = 1.0) -> float:
+    """src/BinarySupernova.jl:167-171"""
+    rs = r_sink(bh)
+    return f_sink * rs / math.sqrt(2.0 * bh.mass / rs)
+
+
+# ---------------------------------------------------------------------------
+# src/euler3d.jl
+
+def fill_ghost_3d_outflow(U, nx, ny, nz):
+    _check_state(U, nx, ny, nz)
+    _call("bsn_fill_ghost_3d_f64", context(), _ptr(U), nx, ny, nz, 0)
+
+
+def fill_ghost_3d_periodic(U, nx, ny, nz):
+    _check_state(U, nx, ny, nz)
+    _call("bsn_fill_ghost_3d_f64", context(), _ptr(U), nx, ny, nz, 1)
+
+
+def apply_floors_3d(U, nx, ny, nz, rho_floor, P_floor, gamma):
+    _check_state(U, nx, ny, nz)
+    _call("bsn_apply_floors_3d_f64", context(), _ptr(U), nx, ny, nz, float(rho_floor), float(P_floor), float(gamma))
+
+
+def euler3d_rhs(dU, Fx, Fy, Fz, U, nx, ny, nz, dx, dy, dz, gamma, *, bc="outflow", rho_floor=0.0, P_floor=0.0,
+                fill_ghosts=True):
+    _check_state(U, nx, ny, nz)
+    _check_state(dU, nx, ny, nz, "dU")
+    _call("bsn_euler3d_rhs_f64", context(), _ptr(dU), _ptr(Fx), _ptr(Fy), _ptr(Fz), _ptr(U), nx, ny, nz,
+          float(dx), float(dy), float(dz), float(gamma), BC[bc], float(rho_floor), float(P_floor), int(fill_ghosts))
+
+
+def euler3d_step(U, nx, ny, nz, dx, dy, dz, dt, gamma, *, bc="outflow", rho_floor=0.0, P_floor=0.0):
+    _check_state(U, nx, ny, nz)
+    _call("bsn_euler3d_step_f64", context(), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz), float(dt),
+          float(gamma), BC[bc], float(rho_floor), float(P_floor))
+
+
+def cfl_dt_3d(U, nx, ny, nz, dx, dy, dz, gamma, cfl) -> float:
+    _check_state(U, nx, ny, nz)
+    out = C.c_double()
+    _call("bsn_cfl_dt_3d_f64", context(), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz), float(gamma),
+          float(cfl), C.byref(out))
+    return out.value
+
+
+# ---------------------------------------------------------------------------
+# src/gravity_bh.jl, src/sinks.jl, src/nbody.jl, src/kepler_orbit.jl
+
+def add_bh_gravity_source(dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0):
+    arr = _bh_array(bhs)
+    _call("bsn_add_bh_gravity_source_f64", context(), _ptr(dU), _ptr(U), nx, ny, nz, float(dx), float(dy),
+          float(dz), arr, len(bhs), float(x0), float(y0), float(z0))
+
+
+def gas_force_on_bh(U, nx, ny, nz, dx, dy, dz, bh, x0, y0, z0) -> np.ndarray:
+    out = (C.c_double * 3)()
+    _call("bsn_gas_force_on_bh_f64", context(), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz),
+          C.byref(bh), float(x0), float(y0), float(z0), out)
+    return np.array(out[:])
+
+
+def add_sink_sources(dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0, *, f_sink=1.0, torque_free=True,
+                     rho_sink_min=0.0):
+    arr = _bh_array(bhs)
+    _call("bsn_add_sink_sources_f64", context(), _ptr(dU), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz),
+          arr, len(bhs), float(x0), float(y0), float(z0), float(f_sink), int(bool(torque_free)),
+          float(rho_sink_min))
+
+
+def accrete(bh, U, nx, ny, nz, dx, dy, dz, x0, y0, z0, dt, *, f_sink=1.0, rho_sink_min=0.0):
+    _call("bsn_accrete_f64", context(), C.byref(bh), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz),
+          float(x0), float(y0), float(z0), float(dt), float(f_sink), float(rho_sink_min))
+
+
+def nbody_step(bhs, dt, F_gas):
+    arr = _bh_array(bhs)
+    F = np.ascontiguousarray(np.asarray(F_gas, dtype=np.float64).reshape(-1))
+    rc = load().bsn_nbody_step(arr, len(bhs), float(dt), F.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise BSNError(rc, "nbody_step")
+    _bh_writeback(bhs, arr)
+
+
+class KeplerOrbit:
+    """src/kepler_orbit.jl:36-111 (state kept as the 13 doubles of the C ABI)."""
+
+    def __init__(self, bhs, com=(0.0, 0.0, 0.0), nhat=None, Omega=None):
+        self._st = (C.c_double * 13)()
+        c = (C.c_double * 3)(*com)
+        nh = None if nhat is None else (C.c_double * 3)(*nhat)
+        rc = load().bsn_kepler_init(_bh_array(bhs), c, nh, -1.0 if Omega is None else float(Omega), self._st)
+        if rc != 0:
+            raise BSNError(rc, "KeplerOrbit: degenerate two-BH state")
+
+    @property
+    def Omega(self):
+        return self._st[3]
+
+    @property
+    def com(self):
+        return tuple(self._st[0:3])
+
+    @property
+    def nhat(self):
+        return tuple(self._st[4:7])
+
+
+def kepler_update(bhs, orbit: KeplerOrbit, t):
+    arr = _bh_array(bhs)
+    load().bsn_kepler_update(arr, orbit._st, float(t))
+    _bh_writeback(bhs, arr)
+
+
+# ---------------------------------------------------------------------------
+# src/self_gravity.jl, src/fmr_gravity.jl
+
+def solve_poisson_isolated(rho, nx, ny, nz, dx, dy, dz) -> torch.Tensor:
+    _check_grid(rho, nx, ny, nz, "rho")
+    phi = active_grid(nx, ny, nz, device=rho.device)
+    _call("bsn_solve_poisson_isolated_f64", context(), _ptr(rho), nx, ny, nz, float(dx), float(dy), float(dz),
+          _ptr(phi))
+    return phi
+
+
+def apply_sg_force_level(dU, U, phi, nx, ny, nz, dx, dy, dz):
+    """_apply_sg_force_level! (src/fmr_gravity.jl:146-156)."""
+    _check_grid(phi, nx, ny, nz, "phi")
+    _call("bsn_sg_gradient_f64", context(), _ptr(dU), _ptr(U), _ptr(phi), nx, ny, nz, float(dx), float(dy),
+          float(dz))
+
+
+def add_self_gravity_source(dU, U, nx, ny, nz, dx, dy, dz):
+    _call("bsn_add_self_gravity_source_f64", context(), _ptr(dU), _ptr(U), nx, ny, nz, float(dx), float(dy),
+          float(dz))
+
+
+# ---------------------------------------------------------------------------
+# scripts/run_sn50_fiducial.jl:756-818
+
+def coupled_step(U, bhs, dt, t, nx, ny, nz, dx, x0, y0, z0, gamma, f_sink, rho_floor, P_floor, torque_free,
+                 self_gravity, t_bh2_sink_on, rho_sink_min, evolve_orbit=True):
+    """One production step; returns F_gas (nbh x 3).  `bhs` is updated in place."""
+    arr = _bh_array(bhs)
+    Fg = (C.c_double * (3 * max(1, len(bhs))))()
+    _call("bsn_coupled_step_f64", context(), _ptr(U), arr, len(bhs), float(dt), float(t), nx, ny, nz, float(dx),
+          float(x0), float(y0), float(z0), float(gamma), float(f_sink), float(rho_floor), float(P_floor),
+          int(bool(torque_free)), int(bool(self_gravity)), float(t_bh2_sink_on), float(rho_sink_min),
+          int(bool(evolve_orbit)), Fg)
+    _bh_writeback(bhs, arr)
+    return np.array(Fg[: 3 * len(bhs)]).reshape(len(bhs), 3)
+
+
+# ---------------------------------------------------------------------------
+# src/fmr3d.jl
+
+class FMRGrid3D:
+    """Two-level FMR grid over device level arrays (src/fmr3d.jl:109-151)."""
+
+    def __init__(self, Uc, ncx, ncy, ncz, dxc, ci_lo, ci_hi, cj_lo, cj_hi, ck_lo, ck_hi, ratio, gamma, *,
+                 bc="outflow", rho_floor=0.0, P_floor=0.0, dyc=None, dzc=None, init=True):
+        _check_state(Uc, ncx, ncy, ncz, "Uc")
+        dyc = dxc if dyc is None else dyc
+        dzc = dxc if dzc is None else dzc
+        nfx, nfy, nfz = (ci_hi - ci_lo + 1) * ratio, (cj_hi - cj_lo + 1) * ratio, (ck_hi - ck_lo + 1) * ratio
+        self.Uc = Uc
+        self.Uf = state(nfx, nfy, nfz, device=Uc.device)
+        self.coarse_dims = (ncx, ncy, ncz)
+        self.fine_dims = (nfx, nfy, nfz)
+        self.s = bsn_fmr2(Uc.data_ptr(), ncx, ncy, ncz, dxc, dyc, dzc, self.Uf.data_ptr(), nfx, nfy, nfz,
+                          dxc / ratio, dyc / ratio, dzc / ratio, ratio, ci_lo, ci_hi, cj_lo, cj_hi, ck_lo, ck_hi,
+                          float(gamma), BC[bc], float(rho_floor), float(P_floor))
+        if init:
+            _call("bsn_fmr_prolong_all_f64", context(), C.byref(self.s))
+
+    def prolong_fine_ghosts(self, Uc_src=None):
+        src = self.Uc if Uc_src is None else Uc_src
+        _call("bsn_fmr_prolong_fine_ghosts_f64", context(), _ptr(self.Uf), _ptr(src), C.byref(self.s))
+
+    def restrict(self):
+        _call("bsn_fmr_restrict_f64", context(), _ptr(self.Uc), _ptr(self.Uf), C.byref(self.s))
+
+
+def fmr3d_step(G: FMRGrid3D, dt_c, *, self_gravity=False, G_grav=1.0):
+    _call("bsn_fmr3d_step_f64", context(), C.byref(G.s), float(dt_c), int(bool(self_gravity)), float(G_grav))
+
+
+def cfl_dt_fmr3d(G: FMRGrid3D, cfl) -> float:
+    out = C.c_double()
+    _call("bsn_cfl_dt_fmr3d_f64", context(), C.byref(G.s), float(cfl), C.byref(out))
+    return out.value
+
+
+def restrict_density_to_coarse(G: FMRGrid3D):
+    _call("bsn_restrict_density_to_coarse_f64", context(), C.byref(G.s))
+
+
+def solve_fmr_poisson(G: FMRGrid3D):
+    phic = active_grid(*G.coarse_dims, device=G.Uc.device)
+    phif = active_grid(*G.fine_dims, device=G.Uc.device)
+    _call("bsn_solve_fmr_poisson_f64", context(), C.byref(G.s), _ptr(phic), _ptr(phif))
+    return phic, phif

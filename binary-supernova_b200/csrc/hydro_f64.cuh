@@ -1,0 +1,39 @@
+// hydro_f64.cuh -- internal interface of the FP64 uniform-grid path, shared by
+// the coupled step, self-gravity and FMR drivers.
+#pragma once
+
+#include <cmath>
+#include <cstring>
+#include <algorithm>
+
+#include "stage_f64.cuh"
+
+namespace bsn {
+
+bsn_status check_dims(bsn_ctx* ctx, int nx, int ny, int nz);
+bsn_status f64_fill_ghosts(bsn_ctx* ctx, double* U, int nx, int ny, int nz, int bc);
+bsn_status f64_floors(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double rho_floor, double P_floor, double gamma);
+bsn_status f64_ghost_combine(bsn_ctx* ctx, double* U, const double* S, const double* Gh, int nx, int ny, int nz,
+                             int bc, double dt);
+void stage_args_init(f64::StageArgs& A, int nx, int ny, int nz, double dx, double dy, double dz, double gamma, int bc,
+                     double rho_floor, double P_floor);
+void set_stage(f64::StageArgs& A, int stage, double dt);
+bsn_status f64_launch_stage(bsn_ctx* ctx, const f64::StageArgs& A);
+bsn_status f64_rk3(bsn_ctx* ctx, f64::StageArgs base, double* U, double dt, const double* phi_per_stage[3],
+                   unsigned long long* cfl_max, unsigned int* cfl_nan);
+bsn_status f64_cfl_dt(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                      double gamma, double cfl, double* dt_out);
+bsn_status cfl_from_device(bsn_ctx* ctx, const unsigned long long* red, double cfl, double* dt_out);
+
+// r_sink / t_sink of src/BinarySupernova.jl:159-171 (host FP64).
+inline double bh_r_sink(const bsn_bh& b) {
+    double v = 6.0 * b.mass / (b.c_code * b.c_code);
+    return jmax(v, b.r_floor);
+}
+inline double bh_t_sink(const bsn_bh& b, double f_sink) {
+    double rs = bh_r_sink(b);
+    double v_ff = std::sqrt(2.0 * b.mass / rs);
+    return f_sink * rs / v_ff;
+}
+
+}  // namespace bsn

@@ -1,0 +1,19 @@
+// poisson.cuh -- isolated-boundary FFT Poisson solver interface (internal).
+#pragma once
+
+#include "hydro_f64.cuh"
+
+namespace bsn {
+
+void fft_state_free(bsn_ctx* ctx);
+// Phi = solve_poisson_isolated(rho) for rho on the active grid (nx,ny,nz).
+bsn_status poisson_solve(bsn_ctx* ctx, const double* rho, int nx, int ny, int nz, double dx, double dy, double dz,
+                         double* phi);
+// Same, with rho taken from the state U (density floored at rho_floor when
+// rho_floor >= 0, as euler3d_rhs! floors before add_self_gravity_source!).
+bsn_status poisson_from_state(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                              double rho_floor, double* phi);
+// RK3 step whose every stage solves Poisson on its floored input density.
+bsn_status f64_rk3_selfgrav(bsn_ctx* ctx, f64::StageArgs base, double* U, double dt);
+
+}  // namespace bsn

@@ -1,0 +1,184 @@
+/*
+ * bsn.h -- C ABI of libbsn, the B200 (sm_100a) finite-volume library for
+ * Binary-Supernova's hot path.
+ *
+ * Every entry point replaces one function of the reference Julia package
+ * (macfadyen/Binary-Supernova); the citation beside each declaration names
+ * the function it stands in for (file:line in the reference).  Arguments keep
+ * the reference's meaning and order; Julia keyword arguments become trailing
+ * positional arguments.
+ *
+ * Memory and layout
+ *   - Pointers named U, dU, Fx, Fy, Fz, rho, phi are DEVICE pointers owned by
+ *     the caller (e.g. `pointer(::CuArray)` from Julia, `tensor.data_ptr()`
+ *     from torch).  The library never frees caller memory.
+ *   - State arrays use the reference layout U[q,i,j,k] (Julia column-major,
+ *     5 conserved variables fastest, NG = 3 ghost cells per side):
+ *         U[q + 5*(i + NXT*(j + NYT*k))],  NXT = nx+6, NYT = ny+6, NZT = nz+6,
+ *     q = 0..4 = (rho, rho vx, rho vy, rho vz, E), i,j,k 0-based ghosted.
+ *     Flux arrays: Fx (5, NXT+1, NYT, NZT), Fy (5, NXT, NYT+1, NZT),
+ *     Fz (5, NXT, NYT, NZT+1).  Potentials and densities without ghosts:
+ *     phi[i + nx*(j + ny*k)].
+ *   - bsn_bh arrays are HOST memory (the reference passes BH data by value).
+ *
+ * Execution
+ *   - Work is ordered on the context's stream.  Functions that return host
+ *     values (dt, forces, accretion) synchronise that stream.
+ *   - One context per host thread; contexts share nothing.
+ *
+ * Errors: every call returns bsn_status; bsn_last_error(ctx) gives a message.
+ */
+#ifndef BSN_H
+#define BSN_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int bsn_status;
+enum {
+    BSN_OK = 0,
+    BSN_ERR_ARG = 1,        /* invalid argument (sizes, null pointers, ranges) */
+    BSN_ERR_CUDA = 2,       /* a CUDA runtime/driver call failed */
+    BSN_ERR_TIMEOUT = 3,    /* a bounded device-side wait expired */
+    BSN_ERR_NONFINITE = 4,  /* a NaN/Inf was detected where the reference would throw */
+    BSN_ERR_UNSUPPORTED = 5,/* size/feature outside what this build supports */
+    BSN_ERR_NOMEM = 6       /* workspace allocation failed */
+};
+
+enum { BSN_BC_OUTFLOW = 0, BSN_BC_PERIODIC = 1 };
+
+typedef struct bsn_ctx bsn_ctx;
+
+/* Mirrors the reference's mutable BlackHole (src/BinarySupernova.jl:130-137).
+ * r_sink/t_sink are derived exactly as src/BinarySupernova.jl:159-171. */
+typedef struct {
+    double pos[3];
+    double vel[3];
+    double mass;
+    double eps;
+    double c_code;
+    double r_floor;
+} bsn_bh;
+
+/* Two-level FMR grid (src/fmr3d.jl:109-122, FMRGrid3D).  Uc/Uf are device
+ * arrays in the state layout; index bounds are the reference's 1-based coarse
+ * active-cell indices of the fine patch. */
+typedef struct {
+    double* Uc; int ncx, ncy, ncz; double dxc, dyc, dzc;
+    double* Uf; int nfx, nfy, nfz; double dxf, dyf, dzf;
+    int ratio;
+    int ci_lo, ci_hi, cj_lo, cj_hi, ck_lo, ck_hi;
+    double gamma;
+    int bc;
+    double rho_floor, P_floor;
+} bsn_fmr2;
+
+/* ---- context (replaces KA.get_backend(U) dispatch, src/gpu_kernels.jl:1-21) */
+bsn_status  bsn_ctx_create(bsn_ctx** out, int device, void* cuda_stream);
+bsn_status  bsn_ctx_destroy(bsn_ctx* ctx);
+bsn_status  bsn_ctx_set_stream(bsn_ctx* ctx, void* cuda_stream);
+bsn_status  bsn_ctx_synchronize(bsn_ctx* ctx);
+const char* bsn_last_error(const bsn_ctx* ctx);
+const char* bsn_version(void);
+/* Kernels launched by this context since creation (device launches only). */
+long long   bsn_ctx_launch_count(const bsn_ctx* ctx);
+/* Per-kernel CUDA-event timing on the context stream.  The reference has no
+ * tracing beyond wall-clock progress logs (scripts/run_sn50_fiducial.jl:890-893);
+ * these two calls are the library's own instrumentation.  Enabling or
+ * disabling clears the records; stats sum every recorded launch of `name`. */
+bsn_status  bsn_ctx_set_profiling(bsn_ctx* ctx, int on);
+bsn_status  bsn_ctx_kernel_stats(bsn_ctx* ctx, const char* name, double* total_ms, long long* count);
+
+/* ---- src/euler3d.jl ------------------------------------------------------ */
+/* fill_ghost_3d_outflow! / fill_ghost_3d_periodic! (src/euler3d.jl:33-62) */
+bsn_status bsn_fill_ghost_3d_f64(bsn_ctx* ctx, double* U, int nx, int ny, int nz, int bc);
+/* apply_floors_3d! (src/euler3d.jl:73-80; kernel src/gpu_kernels.jl:26-46) */
+bsn_status bsn_apply_floors_3d_f64(bsn_ctx* ctx, double* U, int nx, int ny, int nz,
+                                   double rho_floor, double P_floor, double gamma);
+/* euler3d_rhs! (src/euler3d.jl:182-205).  Mutates U (ghost fill when
+ * fill_ghosts != 0, floors on active cells), fills Fx/Fy/Fz (zero off the
+ * interfaces) and dU (zero ghosts).  Fx, Fy, Fz may be NULL to skip them. */
+bsn_status bsn_euler3d_rhs_f64(bsn_ctx* ctx, double* dU, double* Fx, double* Fy, double* Fz,
+                               double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                               double gamma, int bc, double rho_floor, double P_floor,
+                               int fill_ghosts);
+/* euler3d_step! (src/euler3d.jl:220-260): one SSP-RK3 step in place. */
+bsn_status bsn_euler3d_step_f64(bsn_ctx* ctx, double* U, int nx, int ny, int nz,
+                                double dx, double dy, double dz, double dt, double gamma,
+                                int bc, double rho_floor, double P_floor);
+/* cfl_dt_3d (src/euler3d.jl:157-169; kernel src/gpu_kernels.jl:174-191). */
+bsn_status bsn_cfl_dt_3d_f64(bsn_ctx* ctx, const double* U, int nx, int ny, int nz,
+                             double dx, double dy, double dz, double gamma, double cfl,
+                             double* dt_out);
+
+/* ---- src/gravity_bh.jl, src/sinks.jl ------------------------------------ */
+/* add_bh_gravity_source! (src/gravity_bh.jl:58-78; src/gpu_kernels.jl:199-230) */
+bsn_status bsn_add_bh_gravity_source_f64(bsn_ctx* ctx, double* dU, const double* U,
+                                         int nx, int ny, int nz, double dx, double dy, double dz,
+                                         const bsn_bh* bhs, int nbh, double x0, double y0, double z0);
+/* gas_force_on_bh (src/gravity_bh.jl:91-113) -> out[3] (host). */
+bsn_status bsn_gas_force_on_bh_f64(bsn_ctx* ctx, const double* U, int nx, int ny, int nz,
+                                   double dx, double dy, double dz, const bsn_bh* bh,
+                                   double x0, double y0, double z0, double out[3]);
+/* add_sink_sources! (src/sinks.jl:32-59; src/gpu_kernels.jl:238-284) */
+bsn_status bsn_add_sink_sources_f64(bsn_ctx* ctx, double* dU, const double* U,
+                                    int nx, int ny, int nz, double dx, double dy, double dz,
+                                    const bsn_bh* bhs, int nbh, double x0, double y0, double z0,
+                                    double f_sink, int torque_free, double rho_sink_min);
+/* accrete! (src/sinks.jl:74-109): mutates *bh (host). */
+bsn_status bsn_accrete_f64(bsn_ctx* ctx, bsn_bh* bh, const double* U, int nx, int ny, int nz,
+                           double dx, double dy, double dz, double x0, double y0, double z0,
+                           double dt, double f_sink, double rho_sink_min);
+/* nbody_step! (src/nbody.jl:74-104), host FP64.  F_gas is nbh*3 host doubles. */
+bsn_status bsn_nbody_step(bsn_bh* bhs, int nbh, double dt, const double* F_gas);
+/* KeplerOrbit(bhs; com, nhat, Omega) (src/kepler_orbit.jl:63-111), host FP64.
+ * nhat may be NULL (inferred), Omega <= 0 means inferred.  state[13] out. */
+bsn_status bsn_kepler_init(const bsn_bh* bhs, const double com[3], const double* nhat,
+                           double Omega, double state[13]);
+/* kepler_update! (src/kepler_orbit.jl:124-150), host FP64. */
+bsn_status bsn_kepler_update(bsn_bh* bhs, const double state[13], double t);
+
+/* ---- src/self_gravity.jl, src/fmr_gravity.jl ---------------------------- */
+/* solve_poisson_isolated (src/self_gravity.jl:35-76): rho, phi device (nx,ny,nz). */
+bsn_status bsn_solve_poisson_isolated_f64(bsn_ctx* ctx, const double* rho, int nx, int ny, int nz,
+                                          double dx, double dy, double dz, double* phi);
+/* _apply_sg_force_level! (src/fmr_gravity.jl:146-156; src/gpu_kernels.jl:291-319) */
+bsn_status bsn_sg_gradient_f64(bsn_ctx* ctx, double* dU, const double* U, const double* phi,
+                               int nx, int ny, int nz, double dx, double dy, double dz);
+/* add_self_gravity_source! (src/self_gravity.jl:93-115) */
+bsn_status bsn_add_self_gravity_source_f64(bsn_ctx* ctx, double* dU, const double* U,
+                                           int nx, int ny, int nz, double dx, double dy, double dz);
+
+/* ---- driver stage order: coupled_step! (scripts/run_sn50_fiducial.jl:756-818)
+ * BH forces, optional nbody_step! (evolve_orbit), three fused RK3 stages with
+ * BH gravity, optional self-gravity and sinks, then accrete!.  bhs is host
+ * memory and is updated; Fgas_out (host, nbh*3, may be NULL) receives F_gas. */
+bsn_status bsn_coupled_step_f64(bsn_ctx* ctx, double* U, bsn_bh* bhs, int nbh, double dt, double t,
+                                int nx, int ny, int nz, double dx, double x0, double y0, double z0,
+                                double gamma, double f_sink, double rho_floor, double P_floor,
+                                int torque_free, int self_gravity, double t_bh2_sink_on,
+                                double rho_sink_min, int evolve_orbit, double* Fgas_out);
+
+/* ---- src/fmr3d.jl ----------------------------------------------------------- */
+/* FMRGrid3D constructor's _prolong_all! (src/fmr3d.jl:131-151, 206-214) */
+bsn_status bsn_fmr_prolong_all_f64(bsn_ctx* ctx, const bsn_fmr2* G);
+/* _prolong_fine_ghosts! (src/fmr3d.jl:223-255) from coarse array Uc_src */
+bsn_status bsn_fmr_prolong_fine_ghosts_f64(bsn_ctx* ctx, double* Uf, const double* Uc_src,
+                                           const bsn_fmr2* G);
+/* _restrict! (src/fmr3d.jl:266-285) */
+bsn_status bsn_fmr_restrict_f64(bsn_ctx* ctx, double* Uc, const double* Uf, const bsn_fmr2* G);
+/* fmr3d_step! (src/fmr3d.jl:451-604) */
+bsn_status bsn_fmr3d_step_f64(bsn_ctx* ctx, const bsn_fmr2* G, double dt_c, int self_gravity,
+                              double G_grav);
+/* cfl_dt_fmr3d (src/fmr3d.jl:616-622) */
+bsn_status bsn_cfl_dt_fmr3d_f64(bsn_ctx* ctx, const bsn_fmr2* G, double cfl, double* dt_out);
+/* restrict_density_to_coarse! (src/fmr_gravity.jl:40-60) */
+bsn_status bsn_restrict_density_to_coarse_f64(bsn_ctx* ctx, const bsn_fmr2* G);
+/* solve_fmr_poisson (src/fmr_gravity.jl:119-133): phi_c (ncx,ncy,ncz), phi_f (nfx,nfy,nfz) device */
+bsn_status bsn_solve_fmr_poisson_f64(bsn_ctx* ctx, const bsn_fmr2* G, double* phi_c, double* phi_f);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BSN_H */
