@@ -66,6 +66,7 @@ SIGNATURES = {
     "bsn_euler3d_rhs_f64": (_I, [_V, _P, _P, _P, _P, _P, _I, _I, _I, _D, _D, _D, _D, _I, _D, _D, _I]),
     "bsn_euler3d_step_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _I, _D, _D]),
     "bsn_cfl_dt_3d_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _dp]),
+    "bsn_cfl_dt_3d_f64_noalloc": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _dp]),
     "bsn_add_bh_gravity_source_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D, _BH, _I, _D, _D, _D]),
     "bsn_gas_force_on_bh_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _BH, _D, _D, _D, _dp]),
     "bsn_add_sink_sources_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D, _BH, _I, _D, _D, _D, _D, _I, _D]),

@@ -22,7 +22,7 @@ OUT = os.path.join(HERE, "bsn", "libbsn.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 BASE = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
-FP64_PARITY = {"hydro_f64.cu", "sources_f64.cu", "fmr_f64.cu", "poisson.cu", "context.cu"}
+FP64_PARITY = {"hydro_f64.cu", "sources_f64.cu", "fmr_f64.cu", "poisson.cu", "context.cu", "cfl_noalloc.cu"}
 
 
 def sources():

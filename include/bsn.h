@@ -111,6 +111,18 @@ bsn_status bsn_euler3d_step_f64(bsn_ctx* ctx, double* U, int nx, int ny, int nz,
 bsn_status bsn_cfl_dt_3d_f64(bsn_ctx* ctx, const double* U, int nx, int ny, int nz,
                              double dx, double dy, double dz, double gamma, double cfl,
                              double* dt_out);
+/* No counterpart in the reference: the same dt as bsn_cfl_dt_3d_f64, for
+ * callers that must not allocate GPU memory (a host runtime that owns a fixed
+ * device-memory pool, or a job that sizes all its memory at start-up).  Its
+ * scratch is a file-scope static device array of 512 KiB held on every GPU
+ * that loads the library until exit; grids above 512^3 = 134,217,728 active
+ * cells are rejected with BSN_ERR_UNSUPPORTED.  The first call on a device
+ * looks up the array's address with that device current; this first call
+ * should come before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race.  The success path allocates nothing. */
+bsn_status bsn_cfl_dt_3d_f64_noalloc(bsn_ctx* ctx, const double* U, int nx, int ny, int nz,
+                                     double dx, double dy, double dz, double gamma, double cfl,
+                                     double* dt_out);
 
 /* ---- src/gravity_bh.jl, src/sinks.jl ------------------------------------ */
 /* add_bh_gravity_source! (src/gravity_bh.jl:58-78; src/gpu_kernels.jl:199-230) */
