@@ -1,15 +1,477 @@
-// fmr_f64.cu -- two-level FMR on the device (src/fmr3d.jl, src/fmr_gravity.jl).
+// fmr_f64.cu -- two-level fixed mesh refinement on the device (FP64 parity
+// path): src/fmr3d.jl (prolongation, restriction, flux registers,
+// Berger-Colella correction, fmr3d_step!, cfl_dt_fmr3d) and
+// src/fmr_gravity.jl (composite-density Poisson, trilinear potential).
+//
+// The reference runs all of this as host loops over host arrays.  Here:
+//   * fine ghost cells are prolonged once per fine subcycle into a ghost
+//     buffer read by all three stage kernels of that subcycle; the reference
+//     refills them before every stage from the same interpolated coarse state,
+//     so the values are identical;
+//   * the coarse flux registers are accumulated by the fused stage kernel at
+//     the coarse-fine faces it computes anyway (no flux arrays in HBM);
+//   * the fine stage kernels write their boundary faces to a small buffer that
+//     one kernel folds into the fine registers in the reference's loop order,
+//     so the register sums are bit-identical.
 #include "poisson.cuh"
 
+namespace bsn {
+namespace fmr {
+
+constexpr int MAXR = 8;
+
+struct Geo {
+    int ncx, ncy, ncz, nfx, nfy, nfz, r;
+    int lo[3], hi[3];        // 1-based coarse active index range of the patch
+    double w[MAXR * 5];      // Lagrange-5 weights, w[s + r*j] (src/fmr3d.jl:32-46)
+};
+
+// src/fmr3d.jl:165-170 for a 0-based ghosted fine index g (Julia ig_f = g+1).
+__device__ __forceinline__ void coarse_stencil(int g, int c_lo, int r, int& ic0, int& s) {
+    double xi = (double)c_lo - 0.5 + ((double)(g + 1 - BSN_NG) - 0.5) / (double)r;
+    double c0 = rint(xi);   // round-half-even, as round(Int, x)
+    int ss = (int)floor((xi - c0 + 0.5) * (double)r);
+    s = ss < 0 ? 0 : (ss > r - 1 ? r - 1 : ss);
+    ic0 = (int)c0;
+}
+
+// Prolong one fine cell (0-based ghosted fine i,j,k) from the coarse source
+// (1-alpha) Ucn + alpha Ucnp1 (src/fmr3d.jl:176-198, 547-551); Ucnp1 may be
+// null (alpha unused).  Writes 5 values at dst.
+__device__ __forceinline__ void prolong_cell(const Geo& G, const double* Ucn, const double* Ucnp1, double alpha,
+                                             int i, int j, int k, double* dst) {
+    int ic0, si, jc0, sj, kc0, sk;
+    coarse_stencil(i, G.lo[0], G.r, ic0, si);
+    coarse_stencil(j, G.lo[1], G.r, jc0, sj);
+    coarse_stencil(k, G.lo[2], G.r, kc0, sk);
+    Geom C(G.ncx, G.ncy, G.ncz);
+    double val[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const double om = 1.0 - alpha;
+    for (int di = -2; di <= 2; ++di) {
+        int ic = BSN_NG + ic0 + di - 1;     // 0-based ghosted coarse
+        double wi = G.w[si + G.r * (di + 2)];
+        for (int dj = -2; dj <= 2; ++dj) {
+            int jc = BSN_NG + jc0 + dj - 1;
+            double wij = wi * G.w[sj + G.r * (dj + 2)];
+            for (int dk = -2; dk <= 2; ++dk) {
+                int kc = BSN_NG + kc0 + dk - 1;
+                double wijk = wij * G.w[sk + G.r * (dk + 2)];
+                long long o = C.at(ic, jc, kc);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    double u = Ucnp1 ? om * Ucn[o + q] + alpha * Ucnp1[o + q] : Ucn[o + q];
+                    val[q] += wijk * u;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) dst[q] = val[q];
+}
+
+// every fine cell (active and ghost): _prolong_all! (src/fmr3d.jl:206-214)
+__global__ void prolong_all_kernel(Geo G, const double* Uc, double* Uf) {
+    Geom F(G.nfx, G.nfy, G.nfz);
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= F.ncell()) return;
+    int X = G.nfx + 2 * BSN_NG, Y = G.nfy + 2 * BSN_NG;
+    int i = (int)(t % X); long long r = t / X; int j = (int)(r % Y); int k = (int)(r / Y);
+    prolong_cell(G, Uc, nullptr, 0.0, i, j, k, Uf + F.at(i, j, k));
+}
+
+// ghost cells only (src/fmr3d.jl:223-255), slab enumeration as the ghost fill
+__global__ void prolong_ghosts_kernel(Geo G, const double* Ucn, const double* Ucnp1, double alpha, double* dst) {
+    int nx = G.nfx, ny = G.nfy, nz = G.nfz;
+    long long X = nx + 2 * BSN_NG, Y = ny + 2 * BSN_NG;
+    long long nzg = 2LL * BSN_NG * X * Y, nyg = 2LL * BSN_NG * X * nz, nxg = 2LL * BSN_NG * ny * nz;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nzg + nyg + nxg) return;
+    int i, j, k;
+    if (t < nzg) {
+        i = (int)(t % X); long long r = t / X; j = (int)(r % Y); int s = (int)(r / Y);
+        k = s < BSN_NG ? s : nz + s;
+    } else if ((t -= nzg) < nyg) {
+        i = (int)(t % X); long long r = t / X; int s = (int)(r % (2 * BSN_NG)); k = (int)(r / (2 * BSN_NG)) + BSN_NG;
+        j = s < BSN_NG ? s : ny + s;
+    } else {
+        t -= nyg;
+        int s = (int)(t % (2 * BSN_NG)); long long r = t / (2 * BSN_NG);
+        j = (int)(r % ny) + BSN_NG; k = (int)(r / ny) + BSN_NG;
+        i = s < BSN_NG ? s : nx + s;
+    }
+    Geom F(nx, ny, nz);
+    prolong_cell(G, Ucn, Ucnp1, alpha, i, j, k, dst + F.at(i, j, k));
+}
+
+// _restrict! (src/fmr3d.jl:266-285); qmax = 5, or 1 for
+// restrict_density_to_coarse! (src/fmr_gravity.jl:40-60)
+__global__ void restrict_kernel(Geo G, double* Uc, const double* Uf, int qmax) {
+    int nic = G.hi[0] - G.lo[0] + 1, njc = G.hi[1] - G.lo[1] + 1, nkc = G.hi[2] - G.lo[2] + 1;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nic * njc * nkc) return;
+    int m = (int)(t % nic); long long rr = t / nic; int n = (int)(rr % njc); int p = (int)(rr / njc);
+    Geom C(G.ncx, G.ncy, G.ncz), F(G.nfx, G.nfy, G.nfz);
+    const int r = G.r;
+    const double inv_r3 = 1.0 / (double)(r * r * r);
+    long long oc = C.at(BSN_NG + G.lo[0] + m - 1, BSN_NG + G.lo[1] + n - 1, BSN_NG + G.lo[2] + p - 1);
+    for (int q = 0; q < qmax; ++q) {
+        double val = 0.0;
+        for (int sx = 1; sx <= r; ++sx)
+            for (int sy = 1; sy <= r; ++sy)
+                for (int sz = 1; sz <= r; ++sz)
+                    val += Uf[F.at(BSN_NG + r * m + sx - 1, BSN_NG + r * n + sy - 1, BSN_NG + r * p + sz - 1) + q];
+        Uc[oc + q] = val * inv_r3;
+    }
+}
+
+// Fine register accumulation (src/fmr3d.jl:331-369): one thread per coarse
+// register element adds its r^2 fine faces in the reference's loop order.
+// bnd[2D+side] holds fine faces (5, n1, n2) over the fine active transverse.
+struct Regs {
+    double* r[6];           // xlo, xhi, ylo, yhi, zlo, zhi: (5, t1, t2) coarse
+    const double* bnd[6];
+};
+__global__ void fine_reg_kernel(Geo G, Regs R, double fac) {
+    int nic = G.hi[0] - G.lo[0] + 1, njc = G.hi[1] - G.lo[1] + 1, nkc = G.hi[2] - G.lo[2] + 1;
+    long long nx_ = 5LL * njc * nkc, ny_ = 5LL * nic * nkc, nz_ = 5LL * nic * njc;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int D;
+    if (t < 2 * nx_) D = 0;
+    else if ((t -= 2 * nx_) < 2 * ny_) D = 1;
+    else if ((t -= 2 * ny_) < 2 * nz_) D = 2;
+    else return;
+    long long per = D == 0 ? nx_ : (D == 1 ? ny_ : nz_);
+    int side = (int)(t / per);
+    long long e = t % per;
+    int q = (int)(e % 5);
+    long long c = e / 5;
+    int n1 = D == 0 ? njc : nic;
+    int a = (int)(c % n1), b = (int)(c / n1);         // coarse transverse (0-based)
+    int f1 = D == 0 ? G.nfy : G.nfx;                   // fine transverse extent of the first axis
+    const double* src = R.bnd[2 * D + side];
+    double* dst = R.r[2 * D + side];
+    const int r = G.r;
+    double acc = dst[e];
+    // loops: x faces `for kf, jf`; y faces `for kf, ia`; z faces `for jf, ia`
+    for (int ob = b * r; ob < b * r + r; ++ob)
+        for (int oa = a * r; oa < a * r + r; ++oa)
+            acc += fac * src[5LL * (oa + (long long)f1 * ob) + q];
+    dst[e] = acc;
+}
+
+// Berger-Colella correction (src/fmr3d.jl:379-422).  The x-, y- and z-face
+// corrected coarse cells are disjoint, so every element is independent.
+__global__ void bc_correct_kernel(Geo G, Regs Rc, Regs Rf, double* Uc, double idx, double idy, double idz) {
+    int nic = G.hi[0] - G.lo[0] + 1, njc = G.hi[1] - G.lo[1] + 1, nkc = G.hi[2] - G.lo[2] + 1;
+    long long nx_ = 5LL * njc * nkc, ny_ = 5LL * nic * nkc, nz_ = 5LL * nic * njc;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int D;
+    if (t < nx_) D = 0;
+    else if ((t -= nx_) < ny_) D = 1;
+    else if ((t -= ny_) < nz_) D = 2;
+    else return;
+    int q = (int)(t % 5);
+    long long c = t / 5;
+    int n1 = D == 0 ? njc : nic;
+    int a = (int)(c % n1), b = (int)(c / n1);
+    double inv = D == 0 ? idx : (D == 1 ? idy : idz);
+    double dlo = (Rc.r[2 * D][t] - Rf.r[2 * D][t]) * inv;
+    double dhi = (Rf.r[2 * D + 1][t] - Rc.r[2 * D + 1][t]) * inv;
+    Geom C(G.ncx, G.ncy, G.ncz);
+    // 0-based ghosted coarse coordinates of the two corrected cells
+    int p[3], s[3];
+    int ax1 = D == 0 ? 1 : 0, ax2 = D == 2 ? 1 : 2;
+    p[ax1] = s[ax1] = BSN_NG + G.lo[ax1] + a - 1;
+    p[ax2] = s[ax2] = BSN_NG + G.lo[ax2] + b - 1;
+    p[D] = BSN_NG + G.lo[D] - 2;   // ci_lo - 1 (1-based) -> 0-based ghosted
+    s[D] = BSN_NG + G.hi[D];       // ci_hi + 1 (1-based) -> 0-based ghosted
+    Uc[C.at(p[0], p[1], p[2]) + q] += dlo;
+    Uc[C.at(s[0], s[1], s[2]) + q] += dhi;
+}
+
+// _prolong_scalar_trilinear! (src/fmr_gravity.jl:70-106)
+__global__ void trilinear_kernel(Geo G, const double* pc, double* pf) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long n = (long long)G.nfx * G.nfy * G.nfz;
+    if (t >= n) return;
+    int fi = (int)(t % G.nfx) + 1; long long rr = t / G.nfx; int jf = (int)(rr % G.nfy) + 1; int kf = (int)(rr / G.nfy) + 1;
+    const int r = G.r;
+    double xc = (double)(G.lo[0] - 1) + ((double)fi - 0.5) / (double)r + 0.5;
+    double yc = (double)(G.lo[1] - 1) + ((double)jf - 0.5) / (double)r + 0.5;
+    double zc = (double)(G.lo[2] - 1) + ((double)kf - 0.5) / (double)r + 0.5;
+    int ic = min(max((int)floor(xc), 1), G.ncx - 1);
+    int jc = min(max((int)floor(yc), 1), G.ncy - 1);
+    int kc = min(max((int)floor(zc), 1), G.ncz - 1);
+    double fx = xc - ic, fy = yc - jc, fz = zc - kc;
+    auto P = [&](int a, int b, int c) { return pc[(a - 1) + (long long)G.ncx * ((b - 1) + (long long)G.ncy * (c - 1))]; };
+    double w000 = (1 - fx) * (1 - fy) * (1 - fz), w100 = fx * (1 - fy) * (1 - fz);
+    double w010 = (1 - fx) * fy * (1 - fz), w110 = fx * fy * (1 - fz);
+    double w001 = (1 - fx) * (1 - fy) * fz, w101 = fx * (1 - fy) * fz;
+    double w011 = (1 - fx) * fy * fz, w111 = fx * fy * fz;
+    pf[t] = w000 * P(ic, jc, kc) + w100 * P(ic + 1, jc, kc) + w010 * P(ic, jc + 1, kc) + w110 * P(ic + 1, jc + 1, kc) +
+            w001 * P(ic, jc, kc + 1) + w101 * P(ic + 1, jc, kc + 1) + w011 * P(ic, jc + 1, kc + 1) +
+            w111 * P(ic + 1, jc + 1, kc + 1);
+}
+
+__global__ void scale_kernel(double* a, long long n, double s) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) a[t] *= s;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+bsn_status make_geo(bsn_ctx* ctx, const bsn_fmr2* g, Geo& G) {
+    if (!g || !g->Uc || !g->Uf) return set_err(ctx, BSN_ERR_ARG, "FMR grid or level array is null");
+    if (g->ratio < 1 || g->ratio > MAXR) return set_err(ctx, BSN_ERR_UNSUPPORTED, "ratio %d outside 1..%d", g->ratio, MAXR);
+    memset(&G, 0, sizeof(G));
+    G.ncx = g->ncx; G.ncy = g->ncy; G.ncz = g->ncz; G.nfx = g->nfx; G.nfy = g->nfy; G.nfz = g->nfz; G.r = g->ratio;
+    G.lo[0] = g->ci_lo; G.lo[1] = g->cj_lo; G.lo[2] = g->ck_lo;
+    G.hi[0] = g->ci_hi; G.hi[1] = g->cj_hi; G.hi[2] = g->ck_hi;
+    int nc[3] = {g->ncx, g->ncy, g->ncz}, nf[3] = {g->nfx, g->nfy, g->nfz};
+    for (int d = 0; d < 3; ++d) {
+        if (G.lo[d] < 1 || G.hi[d] > nc[d] || G.hi[d] < G.lo[d])
+            return set_err(ctx, BSN_ERR_ARG, "patch range [%d,%d] outside coarse axis %d of %d cells", G.lo[d], G.hi[d],
+                           d, nc[d]);
+        if (nf[d] != (G.hi[d] - G.lo[d] + 1) * G.r)
+            return set_err(ctx, BSN_ERR_ARG, "fine extent %d != (hi-lo+1)*ratio on axis %d", nf[d], d);
+        // every Lagrange stencil of a fine cell (ghosts included) must stay
+        // inside the coarse ghosted array (the reference reads it unchecked)
+        for (int g2 : {0, nf[d] + 2 * BSN_NG - 1}) {
+            double xi = (double)G.lo[d] - 0.5 + ((double)(g2 + 1 - BSN_NG) - 0.5) / (double)G.r;
+            int c0 = (int)std::nearbyint(xi);
+            int lo = BSN_NG + c0 - 2 - 1, hi = BSN_NG + c0 + 2 - 1;
+            if (lo < 0 || hi > nc[d] + 2 * BSN_NG - 1)
+                return set_err(ctx, BSN_ERR_ARG, "prolongation stencil leaves the coarse array on axis %d "
+                               "(patch too close to the boundary)", d);
+        }
+    }
+    // _lag5_weights (src/fmr3d.jl:32-46)
+    const double nodes[5] = {-2.0, -1.0, 0.0, 1.0, 2.0};
+    for (int s = 0; s < G.r; ++s) {
+        double t = ((double)s + 0.5 - (double)G.r / 2.0) / (double)G.r;
+        for (int j = 0; j < 5; ++j) {
+            double wj = 1.0;
+            for (int m = 0; m < 5; ++m)
+                if (m != j) wj *= (t - nodes[m]) / (nodes[j] - nodes[m]);
+            G.w[s + G.r * j] = wj;
+        }
+    }
+    return BSN_OK;
+}
+
+long long ghost_count(int nx, int ny, int nz) {
+    long long X = nx + 2 * BSN_NG, Y = ny + 2 * BSN_NG;
+    return 2LL * BSN_NG * (X * Y + X * nz + (long long)ny * nz);
+}
+
+bsn_status prolong_ghosts(bsn_ctx* ctx, const Geo& G, const double* Ucn, const double* Ucnp1, double alpha,
+                          double* dst) {
+    long long n = ghost_count(G.nfx, G.nfy, G.nfz);
+    prof_begin(ctx);
+    prolong_ghosts_kernel<<<grid1d(n, 128), 128, 0, ctx->stream>>>(G, Ucn, Ucnp1, alpha, dst);
+    return launch_check(ctx, "prolong_ghosts_kernel");
+}
+
+bsn_status restrict_(bsn_ctx* ctx, const Geo& G, double* Uc, const double* Uf, int qmax) {
+    long long n = (long long)(G.hi[0] - G.lo[0] + 1) * (G.hi[1] - G.lo[1] + 1) * (G.hi[2] - G.lo[2] + 1);
+    prof_begin(ctx);
+    restrict_kernel<<<grid1d(n, 128), 128, 0, ctx->stream>>>(G, Uc, Uf, qmax);
+    return launch_check(ctx, "restrict_kernel");
+}
+
+bsn_status fmr_poisson(bsn_ctx* ctx, const bsn_fmr2* g, const Geo& G, double* phic, double* phif) {
+    BSN_TRY(restrict_(ctx, G, g->Uc, g->Uf, 1));
+    BSN_TRY(poisson_from_state(ctx, g->Uc, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, -1.0, phic));
+    long long n = (long long)g->nfx * g->nfy * g->nfz;
+    prof_begin(ctx);
+    trilinear_kernel<<<grid1d(n, 256), 256, 0, ctx->stream>>>(G, phic, phif);
+    return launch_check(ctx, "trilinear_kernel");
+}
+
+struct RegSet {
+    Regs c, f;
+    double* base;
+    size_t bytes;
+};
+
+bsn_status make_regs(bsn_ctx* ctx, const Geo& G, RegSet& R) {
+    long long nic = G.hi[0] - G.lo[0] + 1, njc = G.hi[1] - G.lo[1] + 1, nkc = G.hi[2] - G.lo[2] + 1;
+    long long e[3] = {5 * njc * nkc, 5 * nic * nkc, 5 * nic * njc};
+    long long per = 2 * (e[0] + e[1] + e[2]);
+    bsn_status st;
+    double* b = (double*)slot(ctx, SLOT_FMR_REG, sizeof(double) * 2 * per, &st); BSN_TRY(st);
+    R.base = b;
+    R.bytes = sizeof(double) * 2 * per;
+    double* p = b;
+    for (int D = 0; D < 3; ++D) for (int s = 0; s < 2; ++s) { R.c.r[2 * D + s] = p; p += e[D]; }
+    for (int D = 0; D < 3; ++D) for (int s = 0; s < 2; ++s) { R.f.r[2 * D + s] = p; p += e[D]; }
+    // fine boundary-face capture: (5, n1f, n2f) per face
+    long long ef[3] = {5LL * G.nfy * G.nfz, 5LL * G.nfx * G.nfz, 5LL * G.nfx * G.nfy};
+    double* bf = (double*)slot(ctx, SLOT_FMR_BF, sizeof(double) * 2 * (ef[0] + ef[1] + ef[2]), &st); BSN_TRY(st);
+    for (int D = 0; D < 3; ++D) for (int s = 0; s < 2; ++s) { R.f.bnd[2 * D + s] = bf; bf += ef[D]; }
+    for (int i = 0; i < 6; ++i) R.c.bnd[i] = nullptr;
+    BSN_CUDA(ctx, cudaMemsetAsync(b, 0, R.bytes, ctx->stream));
+    return BSN_OK;
+}
+
+// src/fmr3d.jl:451-604
+bsn_status fmr3d_step(bsn_ctx* ctx, const bsn_fmr2* g, double dt_c, int self_gravity, double G_grav) {
+    Geo G;
+    BSN_TRY(make_geo(ctx, g, G));
+    const int r = g->ratio;
+    const double dt_f = dt_c / (double)r;
+    Geom C(g->ncx, g->ncy, g->ncz), F(g->nfx, g->nfy, g->nfz);
+    bsn_status st;
+    double *phic = nullptr, *phif = nullptr;
+    if (self_gravity) {
+        phic = (double*)slot(ctx, SLOT_PHI, sizeof(double) * (size_t)g->ncx * g->ncy * g->ncz, &st); BSN_TRY(st);
+        phif = (double*)slot(ctx, SLOT_PHI2, sizeof(double) * (size_t)g->nfx * g->nfy * g->nfz, &st); BSN_TRY(st);
+        BSN_TRY(fmr_poisson(ctx, g, G, phic, phif));
+        if (G_grav != 1.0) {
+            long long nc = (long long)g->ncx * g->ncy * g->ncz, nf = (long long)g->nfx * g->nfy * g->nfz;
+            scale_kernel<<<grid1d(nc, 256), 256, 0, ctx->stream>>>(phic, nc, G_grav);
+            BSN_TRY(launch_check(ctx, "scale_kernel"));
+            scale_kernel<<<grid1d(nf, 256), 256, 0, ctx->stream>>>(phif, nf, G_grav);
+            BSN_TRY(launch_check(ctx, "scale_kernel"));
+        }
+    }
+    double* Ucn = (double*)slot(ctx, SLOT_FMR_UCN, sizeof(double) * C.nelem(), &st); BSN_TRY(st);
+    BSN_CUDA(ctx, cudaMemcpyAsync(Ucn, g->Uc, sizeof(double) * C.nelem(), cudaMemcpyDeviceToDevice, ctx->stream));
+    RegSet R;
+    BSN_TRY(make_regs(ctx, G, R));
+    const double rk_w[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+
+    // ---- coarse SSP-RK3 with coarse-fine flux registers
+    double* Ac = (double*)slot(ctx, SLOT_A, sizeof(double) * C.nelem(), &st); BSN_TRY(st);
+    double* Bc = (double*)slot(ctx, SLOT_B, sizeof(double) * C.nelem(), &st); BSN_TRY(st);
+    {
+        f64::StageArgs base;
+        stage_args_init(base, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, g->gamma, g->bc, g->rho_floor,
+                        g->P_floor);
+        base.use_reg = 1;
+        for (int i = 0; i < 6; ++i) base.reg.reg[i] = R.c.r[i];
+        for (int d = 0; d < 3; ++d) {
+            base.reg.lo[d] = G.lo[d] - 1;
+            base.reg.hi[d] = G.hi[d];
+            base.reg.t0[d] = G.lo[d] - 1;
+            base.reg.t1[d] = G.hi[d] - 1;
+        }
+        if (self_gravity) { base.use_sg = 1; base.phi = phic; }
+        double* in[3] = {g->Uc, Ac, Bc};
+        double* out[3] = {Ac, Bc, g->Uc};
+        for (int s = 0; s < 3; ++s) {
+            f64::StageArgs a = base;
+            a.Uin = in[s]; a.Un = g->Uc; a.Uout = out[s];
+            set_stage(a, s + 1, dt_c);
+            a.reg.fac = rk_w[s] * dt_c;
+            BSN_TRY(f64_launch_stage(ctx, a));
+        }
+        BSN_TRY(f64_ghost_combine(ctx, g->Uc, Bc, nullptr, g->ncx, g->ncy, g->ncz, g->bc, dt_c));
+    }
+
+    // ---- fine subcycles: ghosts from (1-a) U_c^n + a U_c^{n+1}
+    double* Gh = (double*)slot(ctx, SLOT_FMR_GH, sizeof(double) * F.nelem(), &st); BSN_TRY(st);
+    double* Af = (double*)slot(ctx, SLOT_FMR_FA, sizeof(double) * F.nelem(), &st); BSN_TRY(st);
+    double* Bf = (double*)slot(ctx, SLOT_FMR_FB, sizeof(double) * F.nelem(), &st); BSN_TRY(st);
+    f64::StageArgs fb;
+    stage_args_init(fb, g->nfx, g->nfy, g->nfz, g->dxf, g->dyf, g->dzf, g->gamma, g->bc, g->rho_floor, g->P_floor);
+    fb.Gh = Gh;
+    fb.use_bnd = 1;
+    for (int i = 0; i < 6; ++i) fb.bnd.f[i] = const_cast<double*>(R.f.bnd[i]);
+    if (self_gravity) { fb.use_sg = 1; fb.phi = phif; }
+    long long nic = G.hi[0] - G.lo[0] + 1, njc = G.hi[1] - G.lo[1] + 1, nkc = G.hi[2] - G.lo[2] + 1;
+    long long nreg = 2 * 5 * (njc * nkc + nic * nkc + nic * njc);
+    for (int s_sub = 0; s_sub < r; ++s_sub) {
+        double alpha = (double)s_sub / (double)r;
+        BSN_TRY(prolong_ghosts(ctx, G, Ucn, g->Uc, alpha, Gh));
+        double* in[3] = {g->Uf, Af, Bf};
+        double* out[3] = {Af, Bf, g->Uf};
+        for (int s = 0; s < 3; ++s) {
+            f64::StageArgs a = fb;
+            a.Uin = in[s]; a.Un = g->Uf; a.Uout = out[s];
+            set_stage(a, s + 1, dt_f);
+            BSN_TRY(f64_launch_stage(ctx, a));
+            double fac = rk_w[s] * dt_f / (double)(r * r);
+            prof_begin(ctx);
+            fine_reg_kernel<<<grid1d(nreg, 128), 128, 0, ctx->stream>>>(G, R.f, fac);
+            BSN_TRY(launch_check(ctx, "fine_reg_kernel"));
+        }
+        BSN_TRY(f64_ghost_combine(ctx, g->Uf, nullptr, Gh, g->nfx, g->nfy, g->nfz, g->bc, dt_f));
+    }
+
+    // ---- restrict, Berger-Colella correction, coarse floors
+    BSN_TRY(restrict_(ctx, G, g->Uc, g->Uf, 5));
+    long long ncorr = 5 * (njc * nkc + nic * nkc + nic * njc);
+    prof_begin(ctx);
+    bc_correct_kernel<<<grid1d(ncorr, 128), 128, 0, ctx->stream>>>(G, R.c, R.f, g->Uc, 1.0 / g->dxc, 1.0 / g->dyc,
+                                                                    1.0 / g->dzc);
+    BSN_TRY(launch_check(ctx, "bc_correct_kernel"));
+    return f64_floors(ctx, g->Uc, g->ncx, g->ncy, g->ncz, g->rho_floor, g->P_floor, g->gamma);
+}
+
+}  // namespace fmr
+}  // namespace bsn
+
 using namespace bsn;
+using namespace bsn::fmr;
 
-#define BSN_FMR_TODO(name) \
-    extern "C" bsn_status name { return set_err(ctx, BSN_ERR_UNSUPPORTED, #name " not built yet"); }
+extern "C" bsn_status bsn_fmr_prolong_all_f64(bsn_ctx* ctx, const bsn_fmr2* g) {
+    if (!ctx) return BSN_ERR_ARG;
+    Geo G;
+    BSN_TRY(make_geo(ctx, g, G));
+    Geom F(g->nfx, g->nfy, g->nfz);
+    prof_begin(ctx);
+    prolong_all_kernel<<<grid1d(F.ncell(), 128), 128, 0, ctx->stream>>>(G, g->Uc, g->Uf);
+    return launch_check(ctx, "prolong_all_kernel");
+}
 
-BSN_FMR_TODO(bsn_fmr_prolong_all_f64(bsn_ctx* ctx, const bsn_fmr2*))
-BSN_FMR_TODO(bsn_fmr_prolong_fine_ghosts_f64(bsn_ctx* ctx, double*, const double*, const bsn_fmr2*))
-BSN_FMR_TODO(bsn_fmr_restrict_f64(bsn_ctx* ctx, double*, const double*, const bsn_fmr2*))
-BSN_FMR_TODO(bsn_fmr3d_step_f64(bsn_ctx* ctx, const bsn_fmr2*, double, int, double))
-BSN_FMR_TODO(bsn_cfl_dt_fmr3d_f64(bsn_ctx* ctx, const bsn_fmr2*, double, double*))
-BSN_FMR_TODO(bsn_restrict_density_to_coarse_f64(bsn_ctx* ctx, const bsn_fmr2*))
-BSN_FMR_TODO(bsn_solve_fmr_poisson_f64(bsn_ctx* ctx, const bsn_fmr2*, double*, double*))
+extern "C" bsn_status bsn_fmr_prolong_fine_ghosts_f64(bsn_ctx* ctx, double* Uf, const double* Uc_src,
+                                                      const bsn_fmr2* g) {
+    if (!ctx) return BSN_ERR_ARG;
+    if (!Uf || !Uc_src) return set_err(ctx, BSN_ERR_ARG, "null array");
+    Geo G;
+    BSN_TRY(make_geo(ctx, g, G));
+    return prolong_ghosts(ctx, G, Uc_src, nullptr, 0.0, Uf);
+}
+
+extern "C" bsn_status bsn_fmr_restrict_f64(bsn_ctx* ctx, double* Uc, const double* Uf, const bsn_fmr2* g) {
+    if (!ctx) return BSN_ERR_ARG;
+    if (!Uc || !Uf) return set_err(ctx, BSN_ERR_ARG, "null array");
+    Geo G;
+    BSN_TRY(make_geo(ctx, g, G));
+    return restrict_(ctx, G, Uc, Uf, 5);
+}
+
+extern "C" bsn_status bsn_fmr3d_step_f64(bsn_ctx* ctx, const bsn_fmr2* g, double dt_c, int self_gravity,
+                                         double G_grav) {
+    if (!ctx) return BSN_ERR_ARG;
+    return fmr3d_step(ctx, g, dt_c, self_gravity, G_grav);
+}
+
+extern "C" bsn_status bsn_cfl_dt_fmr3d_f64(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, double* dt_out) {
+    if (!ctx) return BSN_ERR_ARG;
+    if (!dt_out) return set_err(ctx, BSN_ERR_ARG, "dt_out is null");
+    Geo G;
+    BSN_TRY(make_geo(ctx, g, G));
+    double dtc, dtf;
+    BSN_TRY(f64_cfl_dt(ctx, g->Uc, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, g->gamma, cfl, &dtc));
+    BSN_TRY(f64_cfl_dt(ctx, g->Uf, g->nfx, g->nfy, g->nfz, g->dxf, g->dyf, g->dzf, g->gamma, cfl, &dtf));
+    *dt_out = jmin(dtc, (double)g->ratio * dtf);
+    return BSN_OK;
+}
+
+extern "C" bsn_status bsn_restrict_density_to_coarse_f64(bsn_ctx* ctx, const bsn_fmr2* g) {
+    if (!ctx) return BSN_ERR_ARG;
+    Geo G;
+    BSN_TRY(make_geo(ctx, g, G));
+    return restrict_(ctx, G, g->Uc, g->Uf, 1);
+}
+
+extern "C" bsn_status bsn_solve_fmr_poisson_f64(bsn_ctx* ctx, const bsn_fmr2* g, double* phi_c, double* phi_f) {
+    if (!ctx) return BSN_ERR_ARG;
+    if (!phi_c || !phi_f) return set_err(ctx, BSN_ERR_ARG, "null potential array");
+    Geo G;
+    BSN_TRY(make_geo(ctx, g, G));
+    return fmr_poisson(ctx, g, G, phi_c, phi_f);
+}

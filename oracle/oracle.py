@@ -100,7 +100,7 @@ def _declare(L):
         "orc_solve_fmr_poisson": (V, [C.POINTER(OrcFMR), P, P]),
         "orc_lane_emden": (i, [d, d, P, P, P, i]),
         "orc_polytrope_ic_3d": (V, [P, i, i, i, d, d, d, d, d, d, d, d, d, d, d, d, d, d, d, P]),
-        "orc_thermal_bomb": (d, [P, i, i, i, d, d, d, d, d, d, d, d, d, d, d, d]),
+        "orc_thermal_bomb": (d, [P, i, i, i] + [d] * 13),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
