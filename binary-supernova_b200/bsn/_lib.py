@@ -67,6 +67,12 @@ SIGNATURES = {
     "bsn_euler3d_step_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _I, _D, _D]),
     "bsn_cfl_dt_3d_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _dp]),
     "bsn_cfl_dt_3d_f64_noalloc": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _dp]),
+    "bsn_euler3d_step_f32": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _I, _D, _D]),
+    "bsn_run_steps": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _I, _D, _D, _I, _I, _D, _dp,
+                           C.POINTER(C.c_int)]),
+    "bsn_tile_variant_count": (_I, [_I]),
+    "bsn_ctx_set_tile": (_I, [_V, _I, _I]),
+    "bsn_ctx_get_tile": (_I, [_V, _I, _I, _I, _I, C.POINTER(C.c_int)]),
     "bsn_add_bh_gravity_source_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D, _BH, _I, _D, _D, _D]),
     "bsn_gas_force_on_bh_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _BH, _D, _D, _D, _dp]),
     "bsn_add_sink_sources_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D, _BH, _I, _D, _D, _D, _D, _I, _D]),

@@ -334,3 +334,58 @@ def solve_fmr_poisson(G: FMRGrid3D):
     phif = active_grid(*G.fine_dims, device=G.Uc.device)
     _call("bsn_solve_fmr_poisson_f64", context(), C.byref(G.s), _ptr(phic), _ptr(phif))
     return phic, phif
+
+
+# ---------------------------------------------------------------------------
+# fast path, device time loop, tile autotuner (no single reference counterpart:
+# the reference driver loop test/test_sedov.jl:45-52 run on the device)
+
+PREC = {"f64": 0, "f32": 1}
+
+
+def euler3d_step_f32(U, nx, ny, nz, dx, dy, dz, dt, gamma, *, bc="outflow", rho_floor=0.0, P_floor=0.0):
+    """euler3d_step! with FP32 stencils/fluxes; FP64 state and RK3 accumulation."""
+    _check_state(U, nx, ny, nz)
+    _call("bsn_euler3d_step_f32", context(), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz), float(dt),
+          float(gamma), BC[bc], float(rho_floor), float(P_floor))
+
+
+def run_steps(U, nx, ny, nz, dx, dy, dz, gamma, cfl, *, n_steps, t=0.0, t_end=0.0, bc="outflow", rho_floor=0.0,
+              P_floor=0.0, precision="f64"):
+    """Up to n_steps CFL-limited RK3 steps on the device; returns (t, steps)."""
+    _check_state(U, nx, ny, nz)
+    tt = C.c_double(float(t))
+    nd = C.c_int(0)
+    _call("bsn_run_steps", context(), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz), float(gamma), float(cfl),
+          BC[bc], float(rho_floor), float(P_floor), PREC[precision], int(n_steps), float(t_end), C.byref(tt),
+          C.byref(nd))
+    return tt.value, nd.value
+
+
+def tile_variants(precision="f64") -> int:
+    return int(load().bsn_tile_variant_count(PREC[precision]))
+
+
+def set_tile(precision="f64", variant=-1):
+    _call("bsn_ctx_set_tile", context(), PREC[precision], int(variant))
+
+
+def get_tile(nx, ny, nz, precision="f64"):
+    out = (C.c_int * 4)()
+    _call("bsn_ctx_get_tile", context(), PREC[precision], nx, ny, nz, out)
+    return tuple(out)
+
+
+def kernel_time(name: str):
+    """(total ms, launches) of kernel `name` since profiling was enabled."""
+    tot, cnt = C.c_double(), C.c_longlong()
+    _call("bsn_ctx_kernel_stats", context(), name.encode(), C.byref(tot), C.byref(cnt))
+    return tot.value, cnt.value
+
+
+def set_profiling(on: bool):
+    _call("bsn_ctx_set_profiling", context(), int(bool(on)))
+
+
+__all__ += ["euler3d_step_f32", "run_steps", "tile_variants", "set_tile", "get_tile", "kernel_time",
+            "set_profiling", "PREC"]

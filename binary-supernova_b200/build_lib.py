@@ -22,7 +22,11 @@ OUT = os.path.join(HERE, "bsn", "libbsn.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 BASE = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
-FP64_PARITY = {"hydro_f64.cu", "sources_f64.cu", "fmr_f64.cu", "poisson.cu", "context.cu", "cfl_noalloc.cu"}
+FP64_PARITY = {"hydro_f64.cu", "sources_f64.cu", "fmr_f64.cu", "poisson.cu", "context.cu", "cfl_noalloc.cu",
+               "run_steps.cu", "autotune.cu"}
+# the FP32 fast path: contraction on, approximate division and square root
+FAST = {"stage_fast.cu"}
+FAST_FLAGS = ["--ftz=true", "--prec-div=false", "--prec-sqrt=false", "--fmad=true"]
 
 
 def sources():
@@ -43,6 +47,8 @@ def _compile(src: str, force: bool, verbose: bool):
     flags = list(BASE)
     if src in FP64_PARITY:
         flags += ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]
+    elif src in FAST:
+        flags += FAST_FLAGS
     cmd = [NVCC] + ARCH + flags + ["-c", srcp, "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

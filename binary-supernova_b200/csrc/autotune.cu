@@ -1,0 +1,115 @@
+// autotune.cu -- picks the tile shape of the fused stage kernel per grid.
+//
+// On the first stage of a new (precision, nx, ny, nz) the autotuner launches
+// every tile variant on stage-1 work (reading the caller's state, writing a
+// scratch array), times two launches of each with CUDA events after one
+// warm-up, and keeps the fastest for the life of the context.  FP64 variants
+// give bit-identical results, so the choice never changes a result.
+#include "hydro_f64.cuh"
+#include "stage_launch.cuh"
+
+namespace bsn {
+
+static int variant_count(int prec) { return prec == PREC_F64 ? f64_variant_count() : f32_variant_count(); }
+static bsn_status launch_variant(bsn_ctx* ctx, int prec, int idx, const f64::StageArgs& A) {
+    return prec == PREC_F64 ? f64_launch_variant(ctx, idx, A) : f32_launch_variant(ctx, idx, A);
+}
+
+bsn_status stage_autotune(bsn_ctx* ctx, int prec, const f64::StageArgs& probe, double* scratch) {
+    auto key = std::make_tuple(prec, probe.nx, probe.ny, probe.nz);
+    if (ctx->tile_choice.count(key)) return BSN_OK;
+    int nv = variant_count(prec);
+    if (ctx->forced_tile[prec] >= 0 || nv == 1) {
+        ctx->tile_choice[key] = ctx->forced_tile[prec] >= 0 ? ctx->forced_tile[prec] : 0;
+        return BSN_OK;
+    }
+    f64::StageArgs a = probe;
+    a.Un = probe.Uin;
+    a.Uout = scratch;
+    a.mode = 0;
+    a.stage = 1;
+    a.dt = 0.0;
+    a.cfl_max = nullptr;
+    a.cfl_nan = nullptr;
+    a.use_reg = 0;
+    a.use_bnd = 0;
+    a.F[0] = a.F[1] = a.F[2] = nullptr;
+    a.dt_dev = nullptr;
+    a.done_dev = nullptr;
+    cudaEvent_t e0, e1;
+    BSN_CUDA(ctx, cudaEventCreate(&e0));
+    BSN_CUDA(ctx, cudaEventCreate(&e1));
+    int best = 0;
+    float best_ms = 1e30f;
+    bool prof = ctx->profiling;
+    ctx->profiling = false;
+    bsn_status st = BSN_OK;
+    for (int v = 0; v < nv && st == BSN_OK; ++v) {
+        st = launch_variant(ctx, prec, v, a);   // warm-up (sets smem attributes)
+        if (st != BSN_OK) break;
+        float ms = 1e30f;
+        for (int r = 0; r < 2 && st == BSN_OK; ++r) {
+            cudaEventRecord(e0, ctx->stream);
+            st = launch_variant(ctx, prec, v, a);
+            cudaEventRecord(e1, ctx->stream);
+            cudaEventSynchronize(e1);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            ms = t < ms ? t : ms;
+        }
+        if (ms < best_ms) { best_ms = ms; best = v; }
+    }
+    ctx->profiling = prof;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    BSN_TRY(st);
+    ctx->tile_choice[key] = best;
+    return BSN_OK;
+}
+
+bsn_status stage_launch(bsn_ctx* ctx, int prec, const f64::StageArgs& A) {
+    auto key = std::make_tuple(prec, A.nx, A.ny, A.nz);
+    auto it = ctx->tile_choice.find(key);
+    if (it == ctx->tile_choice.end()) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(ctx->stream, &cs);
+        if (ctx->forced_tile[prec] >= 0 || cs != cudaStreamCaptureStatusNone) {
+            int v = ctx->forced_tile[prec] >= 0 ? ctx->forced_tile[prec] : 0;
+            return launch_variant(ctx, prec, v, A);
+        }
+        Geom G(A.nx, A.ny, A.nz);
+        bsn_status st;
+        double* scratch = (double*)slot(ctx, SLOT_UN, sizeof(double) * (size_t)G.nelem(), &st);
+        BSN_TRY(st);
+        BSN_TRY(stage_autotune(ctx, prec, A, scratch));
+        it = ctx->tile_choice.find(key);
+    }
+    return launch_variant(ctx, prec, it->second, A);
+}
+
+}  // namespace bsn
+
+using namespace bsn;
+
+extern "C" bsn_status bsn_ctx_set_tile(bsn_ctx* ctx, int precision, int variant) {
+    if (!ctx) return BSN_ERR_ARG;
+    if (precision != PREC_F64 && precision != PREC_F32) return set_err(ctx, BSN_ERR_ARG, "bad precision %d", precision);
+    if (variant >= variant_count(precision)) return set_err(ctx, BSN_ERR_ARG, "no tile variant %d", variant);
+    ctx->forced_tile[precision] = variant < 0 ? -1 : variant;
+    for (auto it = ctx->tile_choice.begin(); it != ctx->tile_choice.end();)
+        it = std::get<0>(it->first) == precision ? ctx->tile_choice.erase(it) : std::next(it);
+    return BSN_OK;
+}
+
+extern "C" bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int ny, int nz, int out[4]) {
+    if (!ctx || !out) return BSN_ERR_ARG;
+    auto it = ctx->tile_choice.find(std::make_tuple(precision, nx, ny, nz));
+    if (it == ctx->tile_choice.end()) return set_err(ctx, BSN_ERR_ARG, "no tile chosen yet for this grid");
+    TileVariant v = precision == PREC_F64 ? f64_variant(it->second) : f32_variant(it->second);
+    out[0] = v.tx; out[1] = v.ty; out[2] = v.tz; out[3] = v.nt;
+    return BSN_OK;
+}
+
+extern "C" int bsn_tile_variant_count(int precision) {
+    return precision == PREC_F64 ? f64_variant_count() : (precision == PREC_F32 ? f32_variant_count() : 0);
+}

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -29,6 +31,11 @@ struct bsn_ctx {
     cudaEvent_t pending_start = nullptr;
     struct Rec { std::string name; cudaEvent_t a, b; };
     std::vector<Rec> recs;
+    // stage-kernel tile choice per (precision, nx, ny, nz): autotuned or forced
+    std::map<std::tuple<int, int, int, int>, int> tile_choice;
+    int forced_tile[2] = {-1, -1};
+    // graph-captured device time loop (run_steps.cu)
+    void* run_state = nullptr;
 };
 
 namespace bsn {
@@ -36,7 +43,7 @@ namespace bsn {
 enum Slot {
     SLOT_A = 0, SLOT_B, SLOT_UN, SLOT_RED, SLOT_FFT0, SLOT_FFT1, SLOT_PHI, SLOT_RHO,
     SLOT_FMR_UCN, SLOT_FMR_UCNP1, SLOT_FMR_GH, SLOT_FMR_FA, SLOT_FMR_FB, SLOT_FMR_REG,
-    SLOT_FMR_BF, SLOT_PHI2, SLOT_COUNT
+    SLOT_FMR_BF, SLOT_PHI2, SLOT_RUN, SLOT_COUNT
 };
 
 bsn_status set_err(bsn_ctx* ctx, bsn_status code, const char* fmt, ...);

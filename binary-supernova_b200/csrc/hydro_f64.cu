@@ -1,8 +1,9 @@
 // hydro_f64.cu -- FP64 (parity) uniform-grid path: ghost fill, floors, the
 // fused RK3 stage, euler3d_rhs!, euler3d_step!, cfl_dt_3d.
 // Compiled with -fmad=false: bit-identical to the reference's CPU arithmetic.
-#define BSN_DEFINE_STAGE_KERNEL 1
 #include "hydro_f64.cuh"
+#include "stage_launch.cuh"
+#include "stage_tile.cuh"
 
 namespace bsn {
 namespace f64 {
@@ -58,7 +59,9 @@ __global__ void ghost_fill_kernel(double* U, int nx, int ny, int nz, int bc) {
 // U_g = ((1/3) U_g + (2/3) S_g) + ((2/3) dt) * 0.  S is the stage-2 state
 // seen through the boundary map (Gh == null) or an explicit ghost buffer.
 __global__ void ghost_combine_kernel(double* U, const double* S, const double* Gh, int nx, int ny, int nz,
-                                     int bc, double cz) {
+                                     int bc, double cz, const double* dt_dev, const int* done_dev) {
+    if (done_dev && *done_dev) return;
+    if (dt_dev) cz = ((2.0 / 3.0) * *dt_dev) * 0.0;
     GhostEnum E(nx, ny, nz);
     Geom G(nx, ny, nz);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -147,11 +150,12 @@ bsn_status f64_floors(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double rh
 }
 
 bsn_status f64_ghost_combine(bsn_ctx* ctx, double* U, const double* S, const double* Gh, int nx, int ny, int nz,
-                             int bc, double dt) {
+                             int bc, double dt, const double* dt_dev, const int* done_dev) {
     GhostEnum E(nx, ny, nz);
     double cz = ((2.0 / 3.0) * dt) * 0.0;
     prof_begin(ctx);
-    ghost_combine_kernel<<<grid1d(E.total(), 256), 256, 0, ctx->stream>>>(U, S, Gh, nx, ny, nz, bc, cz);
+    ghost_combine_kernel<<<grid1d(E.total(), 256), 256, 0, ctx->stream>>>(U, S, Gh, nx, ny, nz, bc, cz, dt_dev,
+                                                                          done_dev);
     return launch_check(ctx, "ghost_combine_kernel");
 }
 
@@ -166,19 +170,43 @@ void stage_args_init(StageArgs& A, int nx, int ny, int nz, double dx, double dy,
     A.inv2dx = 0.5 / dx; A.inv2dy = 0.5 / dy; A.inv2dz = 0.5 / dz;
 }
 
-bsn_status f64_launch_stage(bsn_ctx* ctx, const StageArgs& A) {
+// FP64 tile variants of the fused stage kernel (bitwise identical results:
+// every interface and every cell is computed by the same arithmetic whatever
+// the tiling).  MINB keeps two 256-thread CTAs (or the equivalent) per SM.
+namespace {
+const TileVariant kF64Variants[] = {{8, 8, 8, 256}, {8, 8, 4, 128}, {16, 8, 4, 256}, {16, 8, 8, 512}};
+
+template <int TX, int TY, int TZ, int NT, int MINB>
+bsn_status launch_f64(bsn_ctx* ctx, const StageArgs& A) {
+    auto fn = tile::stage_kernel<tile::F64Physics, TX, TY, TZ, NT, MINB>;
+    constexpr int smem = tile::smem_bytes<tile::F64Physics, TX, TY, TZ>();
     static bool attr_done[64] = {false};
     int dev = ctx->device & 63;
     if (!attr_done[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return cuda_check(ctx, e, "cudaFuncSetAttribute(stage_kernel)");
         attr_done[dev] = true;
     }
     dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + TZ - 1) / TZ);
     prof_begin(ctx);
-    stage_kernel<<<grid, NT, SMEM_BYTES, ctx->stream>>>(A);
+    fn<<<grid, NT, smem, ctx->stream>>>(A);
     return launch_check(ctx, "stage_kernel");
 }
+}  // namespace
+
+int f64_variant_count() { return (int)(sizeof(kF64Variants) / sizeof(kF64Variants[0])); }
+TileVariant f64_variant(int idx) { return kF64Variants[idx]; }
+bsn_status f64_launch_variant(bsn_ctx* ctx, int idx, const StageArgs& A) {
+    switch (idx) {
+        case 0: return launch_f64<8, 8, 8, 256, 2>(ctx, A);
+        case 1: return launch_f64<8, 8, 4, 128, 4>(ctx, A);
+        case 2: return launch_f64<16, 8, 4, 256, 2>(ctx, A);
+        case 3: return launch_f64<16, 8, 8, 512, 1>(ctx, A);
+        default: return set_err(ctx, BSN_ERR_ARG, "no FP64 tile variant %d", idx);
+    }
+}
+
+bsn_status f64_launch_stage(bsn_ctx* ctx, const StageArgs& A) { return stage_launch(ctx, PREC_F64, A); }
 
 void set_stage(StageArgs& A, int stage, double dt) {
     A.stage = stage;
@@ -206,7 +234,7 @@ bsn_status f64_rk3(bsn_ctx* ctx, StageArgs base, double* U, double dt, const dou
         a.cfl_nan = cfl_nan;
         BSN_TRY(f64_launch_stage(ctx, a));
     }
-    return f64_ghost_combine(ctx, U, B, nullptr, base.nx, base.ny, base.nz, base.bc, dt);
+    return f64_ghost_combine(ctx, U, B, nullptr, base.nx, base.ny, base.nz, base.bc, dt, nullptr, nullptr);
 }
 
 bsn_status f64_cfl_dt(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
@@ -221,6 +249,16 @@ bsn_status f64_cfl_dt(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, dou
                                                 red, (unsigned int*)(red + 1));
     BSN_TRY(launch_check(ctx, "cfl_kernel"));
     return cfl_from_device(ctx, red, cfl, dt_out);
+}
+
+bsn_status f64_cfl_fold(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                        double gamma, unsigned long long* smax, unsigned int* nanflag) {
+    long long n = (long long)nx * ny * nz;
+    int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 8);
+    prof_begin(ctx);
+    cfl_kernel<<<blocks, 256, 0, ctx->stream>>>(U, nx, ny, nz, gamma, gamma - 1.0, 1.0 / dx, 1.0 / dy, 1.0 / dz, smax,
+                                                nanflag);
+    return launch_check(ctx, "cfl_kernel");
 }
 
 bsn_status cfl_from_device(bsn_ctx* ctx, const unsigned long long* red, double cfl, double* dt_out) {

@@ -14,7 +14,7 @@ bsn_status check_dims(bsn_ctx* ctx, int nx, int ny, int nz);
 bsn_status f64_fill_ghosts(bsn_ctx* ctx, double* U, int nx, int ny, int nz, int bc);
 bsn_status f64_floors(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double rho_floor, double P_floor, double gamma);
 bsn_status f64_ghost_combine(bsn_ctx* ctx, double* U, const double* S, const double* Gh, int nx, int ny, int nz,
-                             int bc, double dt);
+                             int bc, double dt, const double* dt_dev = nullptr, const int* done_dev = nullptr);
 void stage_args_init(f64::StageArgs& A, int nx, int ny, int nz, double dx, double dy, double dz, double gamma, int bc,
                      double rho_floor, double P_floor);
 void set_stage(f64::StageArgs& A, int stage, double dt);
@@ -23,6 +23,8 @@ bsn_status f64_rk3(bsn_ctx* ctx, f64::StageArgs base, double* U, double dt, cons
                    unsigned long long* cfl_max, unsigned int* cfl_nan);
 bsn_status f64_cfl_dt(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
                       double gamma, double cfl, double* dt_out);
+bsn_status f64_cfl_fold(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                        double gamma, unsigned long long* smax, unsigned int* nanflag);
 bsn_status cfl_from_device(bsn_ctx* ctx, const unsigned long long* red, double cfl, double* dt_out);
 
 // r_sink / t_sink of src/BinarySupernova.jl:159-171 (host FP64).

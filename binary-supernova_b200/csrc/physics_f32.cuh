@@ -1,0 +1,176 @@
+// physics_f32.cuh -- FP32 stencil physics of the fast path.
+//
+// Same method as the reference (WENO5-Z of rho, m, P with the P clamp, face
+// energy from P, HLLC with its guards), evaluated in FP32 with contraction to
+// FMA and approximate reciprocals/square roots (the translation unit is built
+// with --ftz=true --prec-div=false --prec-sqrt=false).  FP32-specific guards:
+//   * WENO-Z: tau/(eps+beta) is clamped to 1e18 before squaring, so the
+//     weights cannot overflow to Inf/Inf when beta ~ 0 and tau != 0 (with the
+//     reference's eps = 1e-36 the unclamped square overflows FP32);
+//   * the 1e-100 guards of HLLC become 1e-36 (1e-100 is zero in FP32).
+// Results differ from the FP64 path by rounding; their effect on the solution
+// is reported as L1 errors against the FP64 oracle.
+#pragma once
+
+#include "bsn_internal.cuh"
+
+namespace bsn {
+namespace f32 {
+
+__device__ __forceinline__ float wz(float b0, float b1, float b2, float d0, float d1, float d2, float q0, float q1,
+                                    float q2) {
+    const float eps = 1e-36f, cap = 1e18f;
+    float tau = fabsf(b0 - b2);
+    float t0 = fminf(tau / (eps + b0), cap);
+    float t1 = fminf(tau / (eps + b1), cap);
+    float t2 = fminf(tau / (eps + b2), cap);
+    float a0 = d0 * fmaf(t0, t0, 1.0f);
+    float a1 = d1 * fmaf(t1, t1, 1.0f);
+    float a2 = d2 * fmaf(t2, t2, 1.0f);
+    float num = fmaf(a0, q0, fmaf(a1, q1, a2 * q2));
+    return num / (a0 + a1 + a2);
+}
+
+// Left/right WENO5-Z at the interface between c2 and c3 (src/weno5.jl:25-61).
+__device__ __forceinline__ void weno5_lr(float c0, float c1, float c2, float c3, float c4, float c5, float& L,
+                                         float& R) {
+    const float t13 = 1.0f / 3.0f, m76 = -7.0f / 6.0f, e116 = 11.0f / 6.0f, m16 = -1.0f / 6.0f, f56 = 5.0f / 6.0f;
+    const float k1312 = 13.0f / 12.0f;
+    float qA = t13 * c0 + m76 * c1 + e116 * c2;
+    float qB = m16 * c1 + f56 * c2 + t13 * c3;
+    float qC = t13 * c2 + f56 * c3 + m16 * c4;
+    float qD = e116 * c3 + m76 * c4 + t13 * c5;
+    float s0 = c0 - 2.0f * c1 + c2, s1 = c1 - 2.0f * c2 + c3, s2 = c2 - 2.0f * c3 + c4, s3 = c3 - 2.0f * c4 + c5;
+    float a = c0 - 4.0f * c1 + 3.0f * c2;
+    float b = c1 - c3;
+    float c = 3.0f * c2 - 4.0f * c3 + c4;
+    float d = c2 - 4.0f * c3 + 3.0f * c4;
+    float e = 3.0f * c3 - 4.0f * c4 + c5;
+    float bA = fmaf(k1312 * s0, s0, 0.25f * a * a);
+    float bB = fmaf(k1312 * s1, s1, 0.25f * b * b);
+    float x2 = k1312 * s2 * s2;
+    float bC = fmaf(0.25f * c, c, x2);
+    float bD = fmaf(0.25f * d, d, x2);
+    float bE = fmaf(k1312 * s3, s3, 0.25f * e * e);
+    L = wz(bA, bB, bC, 0.1f, 0.6f, 0.3f, qA, qB, qC);
+    R = wz(bB, bD, bE, 0.3f, 0.6f, 0.1f, qB, qC, qD);
+}
+
+__device__ __forceinline__ float cell_pressure(float r, float mx, float my, float mz, float E, float gm1) {
+    r = fmaxf(r, 1e-30f);
+    float KE = 0.5f * (mx * mx + my * my + mz * mz) / r;
+    return fmaxf(gm1 * (E - KE), 0.0f);
+}
+
+__device__ __forceinline__ float EL_from_P(float PL, float rL, float mx, float my, float mz, float inv_gm1) {
+    float rp = fmaxf(rL, 1e-30f);
+    float KE = fminf(0.5f * (mx * mx + my * my + mz * mz) / rp, 0.5f * rp * 1e4f);
+    return fmaf(PL, inv_gm1, KE);
+}
+
+// HLLC (src/hllc.jl:17-165) in the rotated (normal, t1, t2) ordering.
+__device__ __forceinline__ void hllc_normal(float rL, float mnL, float mt1L, float mt2L, float EL, float rR, float mnR,
+                                            float mt1R, float mt2R, float ER, float g, float gm1, float gg,
+                                            float F[5]) {
+    if (rL <= 0.0f) { rL = 1e-30f; mnL = 0.0f; mt1L = 0.0f; mt2L = 0.0f; EL = 0.0f; }
+    if (rR <= 0.0f) { rR = 1e-30f; mnR = 0.0f; mt1R = 0.0f; mt2R = 0.0f; ER = 0.0f; }
+    rL = fmaxf(rL, 1e-30f);
+    rR = fmaxf(rR, 1e-30f);
+    float m2L = mnL * mnL + mt1L * mt1L + mt2L * mt2L;
+    if (m2L > rL * rL * 1e4f) {
+        float s = rL * 100.0f * rsqrtf(m2L);
+        mnL *= s; mt1L *= s; mt2L *= s;
+        m2L = mnL * mnL + mt1L * mt1L + mt2L * mt2L;
+    }
+    float m2R = mnR * mnR + mt1R * mt1R + mt2R * mt2R;
+    if (m2R > rR * rR * 1e4f) {
+        float s = rR * 100.0f * rsqrtf(m2R);
+        mnR *= s; mt1R *= s; mt2R *= s;
+        m2R = mnR * mnR + mt1R * mt1R + mt2R * mt2R;
+    }
+    float iL = 1.0f / rL, iR = 1.0f / rR;
+    float KE_L = fminf(0.5f * m2L * iL, 0.5f * rL * 1e4f);
+    float KE_R = fminf(0.5f * m2R * iR, 0.5f * rR * 1e4f);
+    EL = fmaxf(EL, KE_L);
+    ER = fmaxf(ER, KE_R);
+    float vnL = mnL * iL, vt1L = mt1L * iL, vt2L = mt2L * iL;
+    float vnR = mnR * iR, vt1R = mt1R * iR, vt2R = mt2R * iR;
+    float pL = gm1 * (EL - KE_L), pR = gm1 * (ER - KE_R);
+    float csL = sqrtf(g * pL * iL), csR = sqrtf(g * pR * iR);
+    float SL, SR;
+    if (pL > 0.0f && pR > 0.0f) {
+        float r_avg = 0.5f * (rL + rR), cs_avg = 0.5f * (csL + csR);
+        float p_star = fmaxf(0.0f, 0.5f * (pL + pR) - 0.5f * (vnR - vnL) * r_avg * cs_avg);
+        float qL = p_star > pL ? sqrtf(fmaf(gg, p_star / pL - 1.0f, 1.0f)) : 1.0f;
+        float qR = p_star > pR ? sqrtf(fmaf(gg, p_star / pR - 1.0f, 1.0f)) : 1.0f;
+        SL = vnL - csL * qL;
+        SR = vnR + csR * qR;
+    } else {
+        SL = fminf(vnL - csL, vnR - csR);
+        SR = fmaxf(vnL + csL, vnR + csR);
+    }
+    float dL = rL * (SL - vnL), dR = rR * (SR - vnR);
+    float denom = dL - dR;
+    if (fabsf(denom) < 1e-36f) { F[0] = F[1] = F[2] = F[3] = F[4] = 0.0f; return; }
+    float S_star = (pR - pL + mnL * (SL - vnL) - mnR * (SR - vnR)) / denom;
+    float FrL = mnL, FmnL = fmaf(mnL, vnL, pL), Fmt1L = mt1L * vnL, Fmt2L = mt2L * vnL, FEL = (EL + pL) * vnL;
+    if (SL >= 0.0f) { F[0] = FrL; F[1] = FmnL; F[2] = Fmt1L; F[3] = Fmt2L; F[4] = FEL; return; }
+    float FrR = mnR, FmnR = fmaf(mnR, vnR, pR), Fmt1R = mt1R * vnR, Fmt2R = mt2R * vnR, FER = (ER + pR) * vnR;
+    if (SR <= 0.0f) { F[0] = FrR; F[1] = FmnR; F[2] = Fmt1R; F[3] = Fmt2R; F[4] = FER; return; }
+    if (fmaxf(rL, rR) > 3.0f * fminf(rL, rR)) {
+        float inv = 1.0f / (SR - SL), SLSR = SL * SR;
+        F[0] = (SR * FrL - SL * FrR + SLSR * (rR - rL)) * inv;
+        F[1] = (SR * FmnL - SL * FmnR + SLSR * (mnR - mnL)) * inv;
+        F[2] = (SR * Fmt1L - SL * Fmt1R + SLSR * (mt1R - mt1L)) * inv;
+        F[3] = (SR * Fmt2L - SL * Fmt2R + SLSR * (mt2R - mt2L)) * inv;
+        F[4] = (SR * FEL - SL * FER + SLSR * (ER - EL)) * inv;
+        return;
+    }
+    if (S_star >= 0.0f) {
+        float chi = dL / (SL - S_star);
+        float EsL = fabsf(dL) > 1e-36f ? chi * (EL * iL + (S_star - vnL) * (S_star + pL / dL)) : 0.0f;
+        F[0] = FrL + SL * (chi - rL);
+        F[1] = FmnL + SL * (chi * S_star - mnL);
+        F[2] = Fmt1L + SL * (chi * vt1L - mt1L);
+        F[3] = Fmt2L + SL * (chi * vt2L - mt2L);
+        F[4] = FEL + SL * (EsL - EL);
+    } else {
+        float chi = dR / (SR - S_star);
+        float EsR = fabsf(dR) > 1e-36f ? chi * (ER * iR + (S_star - vnR) * (S_star + pR / dR)) : 0.0f;
+        F[0] = FrR + SR * (chi - rR);
+        F[1] = FmnR + SR * (chi * S_star - mnR);
+        F[2] = Fmt1R + SR * (chi * vt1R - mt1R);
+        F[3] = Fmt2R + SR * (chi * vt2R - mt2R);
+        F[4] = FER + SR * (EsR - ER);
+    }
+}
+
+template <int D>
+__device__ __forceinline__ void interface_flux(const float (&c)[6][6], float g, float gm1, float inv_gm1, float gg,
+                                               float F[5]) {
+    float L[5], R[5];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) weno5_lr(c[0][q], c[1][q], c[2][q], c[3][q], c[4][q], c[5][q], L[q], R[q]);
+    float PL, PR;
+    weno5_lr(c[0][5], c[1][5], c[2][5], c[3][5], c[4][5], c[5][5], PL, PR);
+    float PmaxL = fmaxf(fmaxf(fmaxf(fmaxf(c[0][5], c[1][5]), c[2][5]), c[3][5]), c[4][5]);
+    float PmaxR = fmaxf(fmaxf(fmaxf(fmaxf(c[1][5], c[2][5]), c[3][5]), c[4][5]), c[5][5]);
+    PL = fminf(fmaxf(PL, 0.0f), PmaxL);
+    PR = fminf(fmaxf(PR, 0.0f), PmaxR);
+    float EL = EL_from_P(PL, L[0], L[1], L[2], L[3], inv_gm1);
+    float ER = EL_from_P(PR, R[0], R[1], R[2], R[3], inv_gm1);
+    float Fr[5];
+    if (D == 0) {
+        hllc_normal(L[0], L[1], L[2], L[3], EL, R[0], R[1], R[2], R[3], ER, g, gm1, gg, Fr);
+        F[0] = Fr[0]; F[1] = Fr[1]; F[2] = Fr[2]; F[3] = Fr[3]; F[4] = Fr[4];
+    } else if (D == 1) {
+        hllc_normal(L[0], L[2], L[1], L[3], EL, R[0], R[2], R[1], R[3], ER, g, gm1, gg, Fr);
+        F[0] = Fr[0]; F[1] = Fr[2]; F[2] = Fr[1]; F[3] = Fr[3]; F[4] = Fr[4];
+    } else {
+        hllc_normal(L[0], L[3], L[1], L[2], EL, R[0], R[3], R[1], R[2], ER, g, gm1, gg, Fr);
+        F[0] = Fr[0]; F[1] = Fr[2]; F[2] = Fr[3]; F[3] = Fr[1]; F[4] = Fr[4];
+    }
+}
+
+}  // namespace f32
+}  // namespace bsn

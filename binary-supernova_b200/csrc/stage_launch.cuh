@@ -1,0 +1,30 @@
+// stage_launch.cuh -- tile variants of the fused stage kernel, the autotuner
+// that picks one per grid, and the launch dispatch (autotune.cu).
+#pragma once
+
+#include "stage_f64.cuh"
+
+namespace bsn {
+
+enum Precision { PREC_F64 = 0, PREC_F32 = 1 };
+
+struct TileVariant {
+    int tx, ty, tz, nt;
+};
+
+// per-precision variant tables (hydro_f64.cu: FP64, stage_fast.cu: FP32)
+int f64_variant_count();
+TileVariant f64_variant(int idx);
+bsn_status f64_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A);
+int f32_variant_count();
+TileVariant f32_variant(int idx);
+bsn_status f32_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A);
+
+// Launch one stage with the tile chosen for (precision, nx, ny, nz); the
+// first call for a grid runs the autotuner unless a tile was forced.
+bsn_status stage_launch(bsn_ctx* ctx, int precision, const f64::StageArgs& A);
+// Autotune explicitly (must not run during stream capture): times every
+// variant on stage-1 work writing to `scratch` and records the fastest.
+bsn_status stage_autotune(bsn_ctx* ctx, int precision, const f64::StageArgs& probe, double* scratch);
+
+}  // namespace bsn

@@ -1,0 +1,329 @@
+// stage_tile.cuh -- the fused RK3-stage kernel as a template over the stencil
+// physics (FP64 parity or FP32 fast) and the tile shape (chosen by the
+// autotuner).  Included only by the translation units that instantiate it:
+// hydro_f64.cu (FP64 physics, built with -fmad=false) and stage_fast.cu (FP32
+// physics, built with FMA contraction and approximate division/sqrt).
+//
+// A CTA owns a TX x TY x TZ block of active cells.  For each sweep direction
+// it stages the block plus a 3-cell halo along that direction in shared memory
+// (SoA; floors applied in FP64 to active cells, ghost cells taken raw through
+// the boundary map or from a ghost buffer, the cell pressure computed once per
+// staged cell), computes every interface of the block once, and accumulates
+// the flux divergence of its cells in FP64 registers.  The epilogue adds the
+// source terms in the driver's order (BH gravity, self-gravity, sinks), the
+// SSP-RK3 combine and the floors in FP64, stores the stage result and folds
+// the next CFL speed into a device-wide max.
+#pragma once
+
+#include "stage_f64.cuh"
+
+namespace bsn {
+namespace tile {
+
+template <int TX, int TY, int TZ>
+struct Shape {
+    static constexpr int T[3] = {TX, TY, TZ};
+    static constexpr int NCELL = TX * TY * TZ;
+    static constexpr int EX0 = (TX + 6) * TY * TZ, EX1 = TX * (TY + 6) * TZ, EX2 = TX * TY * (TZ + 6);
+    static constexpr int NEXT = EX0 > EX1 ? (EX0 > EX2 ? EX0 : EX2) : (EX1 > EX2 ? EX1 : EX2);
+    static constexpr int FC0 = (TX + 1) * TY * TZ, FC1 = TX * (TY + 1) * TZ, FC2 = TX * TY * (TZ + 1);
+    static constexpr int NFACE = FC0 > FC1 ? (FC0 > FC2 ? FC0 : FC2) : (FC1 > FC2 ? FC1 : FC2);
+};
+
+// Physics policies --------------------------------------------------------
+struct F64Physics {
+    using real = double;
+    static constexpr bool kCenterFromSmem = true;   // smem holds the floored FP64 state
+    struct Consts { double g, gm1; };
+    __device__ static Consts consts(const f64::StageArgs& A) { return {A.g, A.gm1}; }
+    __device__ static double pressure(const double v[5], const Consts& k) {
+        return f64::cell_pressure(v[0], v[1], v[2], v[3], v[4], k.gm1);
+    }
+    template <int D>
+    __device__ static void flux(const double (&c)[6][6], const Consts& k, double F[5]) {
+        f64::interface_flux<D>(c, k.g, k.gm1, F);
+    }
+};
+
+// F32Physics (the fast path's policy) lives in stage_fast.cu.
+
+__device__ __forceinline__ void load_cell(const f64::StageArgs& A, const Geom& G, int d, int a, int b, int c,
+                                          double v[5], bool& active) {
+    int n[3] = {G.nx, G.ny, G.nz};
+    int p[3] = {a, b, c};
+#pragma unroll
+    for (int t = 0; t < 3; ++t)
+        if (t != d) p[t] = p[t] < n[t] ? p[t] : n[t] - 1;   // partial tile: clamp (value unused)
+    int pd = p[d];
+    active = (pd >= 0 && pd < n[d]);
+    const double* src = A.Uin;
+    if (!active) {
+        if (A.Gh) {
+            pd = pd < -BSN_NG ? -BSN_NG : (pd > n[d] + BSN_NG - 1 ? n[d] + BSN_NG - 1 : pd);
+            p[d] = pd;
+            src = A.Gh;
+        } else {
+            p[d] = bc_map(pd, n[d], A.bc);
+        }
+    }
+    long long off = G.act(p[0], p[1], p[2]);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) v[q] = src[off + q];
+}
+
+template <class P, int TX, int TY, int TZ, int NT, int D>
+__device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::Consts& k, int a0, int b0, int c0,
+                      typename P::real* sC, typename P::real* sF, double (&acc)[Shape<TX, TY, TZ>::NCELL / NT][5]) {
+    using S = Shape<TX, TY, TZ>;
+    using real = typename P::real;
+    constexpr int CPT = S::NCELL / NT;
+    constexpr int LX = TX + (D == 0 ? 6 : 0), LY = TY + (D == 1 ? 6 : 0), LZ = TZ + (D == 2 ? 6 : 0);
+    constexpr int FX = TX + (D == 0), FY = TY + (D == 1), FZ = TZ + (D == 2);
+    constexpr int NE = LX * LY * LZ, NF = FX * FY * FZ;
+    constexpr int TD = D == 0 ? TX : (D == 1 ? TY : TZ);
+    const int tid = threadIdx.x;
+    const int n[3] = {G.nx, G.ny, G.nz};
+    const int o[3] = {a0, b0, c0};
+
+    __syncthreads();
+    for (int e = tid; e < NE; e += NT) {
+        int ex = e % LX, r = e / LX, ey = r % LY, ez = r / LY;
+        int a = a0 + ex - (D == 0 ? 3 : 0);
+        int b = b0 + ey - (D == 1 ? 3 : 0);
+        int c = c0 + ez - (D == 2 ? 3 : 0);
+        double v[5];
+        bool act;
+        load_cell(A, G, D, a, b, c, v, act);
+        if (act) f64::apply_floor(v[0], v[1], v[2], v[3], v[4], A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+        real w[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) { w[q] = (real)v[q]; sC[q * S::NEXT + e] = w[q]; }
+        sC[5 * S::NEXT + e] = P::pressure(w, k);
+    }
+    __syncthreads();
+
+    constexpr int SD = (D == 0) ? 1 : (D == 1 ? LX : LX * LY);
+    for (int f = tid; f < NF; f += NT) {
+        int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
+        int fpos[3] = {fx, fy, fz};
+        bool valid = true;
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            int gpos = o[t] + fpos[t];
+            valid = valid && (t == D ? gpos <= n[t] : gpos < n[t]);
+        }
+        if (!valid) continue;
+        int base = fx + LX * (fy + LY * fz);
+        real c[6][6];
+#pragma unroll
+        for (int s = 0; s < 6; ++s)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) c[s][q] = sC[q * S::NEXT + base + s * SD];
+        real F[5];
+        P::template flux<D>(c, k, F);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) sF[q * S::NFACE + f] = F[q];
+
+        int gd = o[D] + fpos[D];
+        bool owner = (fpos[D] < TD) || (gd == n[D]);
+        if (!owner) continue;
+        int ga = o[0] + fx, gb = o[1] + fy, gc = o[2] + fz;
+        if (A.F[D]) {
+            long long ex_ = (G.nx + 2 * BSN_NG) + (D == 0), ey_ = (G.ny + 2 * BSN_NG) + (D == 1);
+            long long ii = ga + BSN_NG - (D == 0), jj = gb + BSN_NG - (D == 1), kk = gc + BSN_NG - (D == 2);
+            long long off = 5LL * (ii + ex_ * (jj + ey_ * kk));
+#pragma unroll
+            for (int q = 0; q < 5; ++q) A.F[D][off + q] = (double)F[q];
+        }
+        if (A.use_reg) {
+            const f64::RegFaces& R = A.reg;
+            int ta = (D == 0) ? gb : ga, tb = (D == 2) ? gb : gc;
+            int ax1 = (D == 0) ? 1 : 0, ax2 = (D == 2) ? 1 : 2;
+            if (ta >= R.t0[ax1] && ta <= R.t1[ax1] && tb >= R.t0[ax2] && tb <= R.t1[ax2]) {
+                int n1 = R.t1[ax1] - R.t0[ax1] + 1;
+                long long roff = 5LL * ((ta - R.t0[ax1]) + (long long)n1 * (tb - R.t0[ax2]));
+                double* dst = nullptr;
+                if (gd == R.lo[D]) dst = R.reg[2 * D];
+                else if (gd == R.hi[D]) dst = R.reg[2 * D + 1];
+                if (dst) {
+                    double fac = A.dt_dev ? A.reg.wt * *A.dt_dev : R.fac;
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) dst[roff + q] += fac * (double)F[q];
+                }
+            }
+        }
+        if (A.use_bnd && (gd == 0 || gd == n[D])) {
+            int ta = (D == 0) ? gb : ga, tb = (D == 2) ? gb : gc;
+            int n1 = (D == 0) ? G.ny : G.nx;
+            long long roff = 5LL * (ta + (long long)n1 * tb);
+            double* dst = A.bnd.f[2 * D + (gd == 0 ? 0 : 1)];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) dst[roff + q] = (double)F[q];
+        }
+    }
+    __syncthreads();
+
+    const double inv = (D == 0) ? A.idx : (D == 1 ? A.idy : A.idz);
+    constexpr int FS = (D == 0) ? 1 : (D == 1 ? FX : FX * FY);
+#pragma unroll
+    for (int m = 0; m < CPT; ++m) {
+        int cell = tid + m * NT;
+        int i = cell % TX, j = (cell / TX) % TY, kk = cell / (TX * TY);
+        int fl = i + FX * (j + FY * kk);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            double dF = (double)sF[q * S::NFACE + fl + FS] - (double)sF[q * S::NFACE + fl];
+            if (D == 0) acc[m][q] = -dF * inv;
+            else acc[m][q] = acc[m][q] - dF * inv;
+        }
+    }
+}
+
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(f64::StageArgs A) {
+    using S = Shape<TX, TY, TZ>;
+    using real = typename P::real;
+    static_assert(S::NCELL % NT == 0, "cells must divide evenly among threads");
+    constexpr int CPT = S::NCELL / NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    real* sC = reinterpret_cast<real*>(smem_raw);
+    real* sF = sC + 6 * S::NEXT;
+    __shared__ double red[NT / 32];
+    __shared__ unsigned int nanflag;
+
+    if (A.done_dev && *A.done_dev) return;   // device time loop already reached t_end
+    Geom G(A.nx, A.ny, A.nz);
+    const int a0 = blockIdx.x * TX, b0 = blockIdx.y * TY, c0 = blockIdx.z * TZ;
+    const int tid = threadIdx.x;
+    if (tid == 0) nanflag = 0;
+    const typename P::Consts k = P::consts(A);
+
+    double acc[CPT][5];
+    sweep<P, TX, TY, TZ, NT, 0>(A, G, k, a0, b0, c0, sC, sF, acc);
+    sweep<P, TX, TY, TZ, NT, 1>(A, G, k, a0, b0, c0, sC, sF, acc);
+    sweep<P, TX, TY, TZ, NT, 2>(A, G, k, a0, b0, c0, sC, sF, acc);
+
+    const double dt = A.dt_dev ? *A.dt_dev : A.dt;
+    const double cdt = A.stage == 2 ? 0.25 * dt : (A.stage == 3 ? (2.0 / 3.0) * dt : dt);
+    double smax = 0.0;
+#pragma unroll
+    for (int m = 0; m < CPT; ++m) {
+        int cell = tid + m * NT;
+        int i = cell % TX, j = (cell / TX) % TY, kk = cell / (TX * TY);
+        int a = a0 + i, b = b0 + j, c = c0 + kk;
+        if (a >= A.nx || b >= A.ny || c >= A.nz) continue;
+        long long off = G.act(a, b, c);
+        double u0, u1, u2, u3, u4;
+        if (P::kCenterFromSmem) {
+            int e = i + TX * (j + TY * (kk + 3));   // z-extended block of the last sweep
+            u0 = (double)sC[0 * S::NEXT + e]; u1 = (double)sC[1 * S::NEXT + e]; u2 = (double)sC[2 * S::NEXT + e];
+            u3 = (double)sC[3 * S::NEXT + e]; u4 = (double)sC[4 * S::NEXT + e];
+        } else {
+            u0 = A.Uin[off]; u1 = A.Uin[off + 1]; u2 = A.Uin[off + 2]; u3 = A.Uin[off + 3]; u4 = A.Uin[off + 4];
+            f64::apply_floor(u0, u1, u2, u3, u4, A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+        }
+        double* d = acc[m];
+        double xc = A.x0 + ((double)(a + 1) - 0.5) * A.dx;
+        double yc = A.y0 + ((double)(b + 1) - 0.5) * A.dy;
+        double zc = A.z0 + ((double)(c + 1) - 0.5) * A.dz;
+        if (A.use_bh) {   // src/gpu_kernels.jl:199-230
+            double vx = u1 / u0, vy = u2 / u0, vz = u3 / u0;
+            double ax = 0.0, ay = 0.0, az = 0.0;
+            for (int nb = 0; nb < A.bh.n; ++nb) {
+                double ddx = xc - A.bh.px[nb], ddy = yc - A.bh.py[nb], ddz = zc - A.bh.pz[nb];
+                double r2 = sq(ddx) + sq(ddy) + sq(ddz) + sq(A.bh.eps[nb]);
+                double r3 = r2 * sqrt(r2);
+                double fac = -A.bh.mass[nb] / r3;
+                ax += fac * ddx; ay += fac * ddy; az += fac * ddz;
+            }
+            d[1] += u0 * ax; d[2] += u0 * ay; d[3] += u0 * az;
+            d[4] += u0 * (vx * ax + vy * ay + vz * az);
+        }
+        if (A.use_sg) {   // src/gpu_kernels.jl:291-319
+            int nx = A.nx, ny = A.ny, nz = A.nz;
+            int ip = min(a + 1, nx - 1), im = max(a - 1, 0);
+            int jp = min(b + 1, ny - 1), jm = max(b - 1, 0);
+            int kp = min(c + 1, nz - 1), km = max(c - 1, 0);
+            double fx = ip > im ? A.inv2dx : 2.0 * A.inv2dx;
+            double fy = jp > jm ? A.inv2dy : 2.0 * A.inv2dy;
+            double fz = kp > km ? A.inv2dz : 2.0 * A.inv2dz;
+            const double* Pp = A.phi;
+            long long sy = nx, sz = (long long)nx * ny;
+            double gx = (Pp[ip + sy * b + sz * c] - Pp[im + sy * b + sz * c]) * fx;
+            double gy = (Pp[a + sy * jp + sz * c] - Pp[a + sy * jm + sz * c]) * fy;
+            double gz = (Pp[a + sy * b + sz * kp] - Pp[a + sy * b + sz * km]) * fz;
+            double vdotg = (u1 * gx + u2 * gy + u3 * gz) / u0;
+            d[1] -= u0 * gx; d[2] -= u0 * gy; d[3] -= u0 * gz; d[4] -= u0 * vdotg;
+        }
+        if (A.use_sink && u0 > A.sk.rho_min) {   // src/gpu_kernels.jl:238-284
+            for (int nb = 0; nb < A.sk.n; ++nb) {
+                double ddx = xc - A.sk.px[nb], ddy = yc - A.sk.py[nb], ddz = zc - A.sk.pz[nb];
+                double rr = sqrt(sq(ddx) + sq(ddy) + sq(ddz));
+                if (rr < A.sk.rs[nb]) {
+                    double ts = A.sk.ts[nb];
+                    d[0] -= u0 / ts;
+                    if (A.sk.torque_free) {
+                        double rx = ddx / rr, ry = ddy / rr, rz = ddz / rr;
+                        double vx = u1 / u0, vy = u2 / u0, vz = u3 / u0;
+                        double vrx = vx - A.sk.vx[nb], vry = vy - A.sk.vy[nb], vrz = vz - A.sk.vz[nb];
+                        double v_r = vrx * rx + vry * ry + vrz * rz;
+                        double e_int = u4 / u0 - 0.5 * (sq(vx) + sq(vy) + sq(vz));
+                        d[1] -= u0 * v_r * rx / ts;
+                        d[2] -= u0 * v_r * ry / ts;
+                        d[3] -= u0 * v_r * rz / ts;
+                        d[4] -= (0.5 * u0 * sq(v_r) + u0 * e_int) / ts;
+                    } else {
+                        d[1] -= u1 / ts; d[2] -= u2 / ts; d[3] -= u3 / ts; d[4] -= u4 / ts;
+                    }
+                }
+            }
+        }
+        if (A.mode == 1) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) A.dU[off + q] = d[q];
+            A.Uin[off + 0] = u0; A.Uin[off + 1] = u1; A.Uin[off + 2] = u2; A.Uin[off + 3] = u3; A.Uin[off + 4] = u4;
+            continue;
+        }
+        double un[5], w[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) un[q] = A.Un[off + q];
+        const double uu[5] = {u0, u1, u2, u3, u4};
+        if (A.stage == 1) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) w[q] = un[q] + dt * d[q];
+        } else if (A.stage == 2) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) w[q] = 0.75 * un[q] + 0.25 * uu[q] + cdt * d[q];
+        } else {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) w[q] = (1.0 / 3.0) * un[q] + (2.0 / 3.0) * uu[q] + cdt * d[q];
+        }
+        f64::apply_floor(w[0], w[1], w[2], w[3], w[4], A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) A.Uout[off + q] = w[q];
+        if (A.cfl_max) {
+            double s = f64::cfl_speed(w[0], w[1], w[2], w[3], w[4], A.g, A.gm1, A.idx, A.idy, A.idz);
+            if (s != s) nanflag = 1;
+            else smax = fmax(smax, s);
+        }
+    }
+    if (A.cfl_max) {
+        for (int o = 16; o > 0; o >>= 1) smax = fmax(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+        if ((tid & 31) == 0) red[tid >> 5] = smax;
+        __syncthreads();
+        if (tid == 0) {
+            double m = 0.0;
+            for (int w = 0; w < NT / 32; ++w) m = fmax(m, red[w]);
+            atomicMax(A.cfl_max, (unsigned long long)__double_as_longlong(m));
+            if (nanflag) atomicOr(A.cfl_nan, 1u);
+        }
+    }
+}
+
+template <class P, int TX, int TY, int TZ>
+constexpr int smem_bytes() {
+    return (6 * Shape<TX, TY, TZ>::NEXT + 5 * Shape<TX, TY, TZ>::NFACE) * (int)sizeof(typename P::real) + 16;
+}
+
+}  // namespace tile
+}  // namespace bsn

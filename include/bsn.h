@@ -124,6 +124,33 @@ bsn_status bsn_cfl_dt_3d_f64_noalloc(bsn_ctx* ctx, const double* U, int nx, int 
                                      double dx, double dy, double dz, double gamma, double cfl,
                                      double* dt_out);
 
+/* ---- fast path and device time loop (no single counterpart in the reference:
+ * they run the reference's driver loop, test/test_sedov.jl:45-52 /
+ * scripts/run_production.jl:132-135, `dt = cfl_dt_3d; dt = min(dt, t_end-t);
+ * euler3d_step!; t += dt`) ---------------------------------------------- */
+enum { BSN_PREC_F64 = 0,   /* stencils in FP64, bit-identical to the reference */
+       BSN_PREC_F32 = 1 }; /* stencils, fluxes and pressures in FP32; state, floors,
+                              divergence, sources and RK3 accumulation in FP64 */
+/* euler3d_step! with FP32 stencils (BSN_PREC_F32); same arguments. */
+bsn_status bsn_euler3d_step_f32(bsn_ctx* ctx, double* U, int nx, int ny, int nz,
+                                double dx, double dy, double dz, double dt, double gamma,
+                                int bc, double rho_floor, double P_floor);
+/* Up to n_steps CFL-limited SSP-RK3 steps with dt, t and the CFL maximum kept
+ * on the device (one CUDA graph per step).  t_end > 0 stops at t_end exactly
+ * as the reference loop; t_end <= 0 runs n_steps.  *t_inout: start time in,
+ * final time out; *steps_done (may be NULL): steps taken. */
+bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double dx, double dy,
+                         double dz, double gamma, double cfl, int bc, double rho_floor,
+                         double P_floor, int precision, int n_steps, double t_end,
+                         double* t_inout, int* steps_done);
+/* Tile shape of the fused stage kernel: the library's autotuner times every
+ * variant on the first stage of each grid and keeps the fastest.
+ * bsn_ctx_set_tile forces variant `variant` (-1: autotune again);
+ * bsn_ctx_get_tile reports the choice for a grid as {tx, ty, tz, threads}. */
+int        bsn_tile_variant_count(int precision);
+bsn_status bsn_ctx_set_tile(bsn_ctx* ctx, int precision, int variant);
+bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int ny, int nz, int out[4]);
+
 /* ---- src/gravity_bh.jl, src/sinks.jl ------------------------------------ */
 /* add_bh_gravity_source! (src/gravity_bh.jl:58-78; src/gpu_kernels.jl:199-230) */
 bsn_status bsn_add_bh_gravity_source_f64(bsn_ctx* ctx, double* dU, const double* U,

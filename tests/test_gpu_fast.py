@@ -1,0 +1,127 @@
+"""GPU tests of the tile autotuner, the graph-captured device time loop and
+the FP32-stencil fast path.
+
+* Every FP64 tile variant gives bit-identical results (the tiling changes
+  only which CTA computes an interface, never the arithmetic).
+* bsn_run_steps (dt, t and the CFL maximum on the device, one CUDA graph per
+  step) reproduces the reference driver loop `dt = cfl_dt_3d; dt = min(dt,
+  t_end - t); euler3d_step!; t += dt` bit for bit, including the step count.
+* The FP32 path (FP32 stencils, FP64 state) stays within a stated L1 distance
+  of the FP64 oracle: L1(rho) and L1(E) relative below 1e-5 on Sedov 32^3 to
+  t = 0.1 and on one random-state step.
+"""
+import numpy as np
+import pytest
+
+from gpu_util import NG, assert_bitwise, dev, host, random_state
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def bsn():
+    import bsn as b
+    return b
+
+
+def _sedov(orc, n=32, L=1.0, g=5 / 3):
+    dx = 2 * L / n
+    U = orc.state(n, n, n)
+    orc.sedov_ic_3d(U, dx, dx, dx, g, E_blast=1.0, r_inject=3.5 * dx, rho_bg=1.0, P_floor=1e-5,
+                    x_offset=-L, y_offset=-L, z_offset=-L)
+    return U, dx
+
+
+def test_every_fp64_tile_variant_is_bitwise(orc, bsn):
+    n = (37, 21, 19)
+    U = random_state(*n, seed=41, vacuum=True)
+    ref = U.copy(order="F")
+    orc.euler3d_step(ref, 0.1, 0.07, 0.13, 2e-3, 1.4, rho_floor=1e-6, P_floor=1e-4)
+    try:
+        for v in range(bsn.tile_variants("f64")):
+            bsn.set_tile("f64", v)
+            Ud = dev(U)
+            bsn.euler3d_step(Ud, *n, 0.1, 0.07, 0.13, 2e-3, 1.4, rho_floor=1e-6, P_floor=1e-4)
+            assert_bitwise(host(Ud), ref, f"tile variant {v}")
+    finally:
+        bsn.set_tile("f64", -1)
+
+
+def test_autotuner_picks_a_variant(bsn):
+    U = bsn.state(40, 40, 40)
+    U[0] = 1.0
+    U[4] = 2.5
+    bsn.euler3d_step(U, 40, 40, 40, 0.1, 0.1, 0.1, 1e-3, 1.4)
+    tx, ty, tz, nt = bsn.get_tile(40, 40, 40, "f64")
+    assert tx * ty * tz % nt == 0 and nt in (128, 256, 512)
+
+
+@pytest.mark.parametrize("bc", ["outflow", "periodic"])
+def test_run_steps_f64_matches_reference_loop(orc, bsn, bc):
+    U, dx = _sedov(orc)
+    Ud = dev(U)
+    g, tend = 5 / 3, 0.02
+    t, steps = 0.0, 0
+    while t < tend:
+        dt = min(orc.cfl_dt_3d(U, dx, dx, dx, g, 0.4), tend - t)
+        orc.euler3d_step(U, dx, dx, dx, dt, g, bc=bc, rho_floor=1e-6, P_floor=1e-6)
+        t += dt
+        steps += 1
+    # more graph launches than needed: the loop must stop at t_end by itself
+    tg, ng = bsn.run_steps(Ud, 32, 32, 32, dx, dx, dx, g, 0.4, n_steps=steps + 5, t=0.0, t_end=tend, bc=bc,
+                           rho_floor=1e-6, P_floor=1e-6, precision="f64")
+    assert ng == steps and tg == t
+    assert_bitwise(host(Ud), U, "run_steps end state")
+
+
+def test_run_steps_fixed_count_and_resume(orc, bsn):
+    U, dx = _sedov(orc, n=24)
+    Ud = dev(U)
+    g = 5 / 3
+    t = 0.0
+    for _ in range(4):
+        dt = orc.cfl_dt_3d(U, dx, dx, dx, g, 0.4)
+        orc.euler3d_step(U, dx, dx, dx, dt, g, rho_floor=1e-6, P_floor=1e-6)
+        t += dt
+    t1, n1 = bsn.run_steps(Ud, 24, 24, 24, dx, dx, dx, g, 0.4, n_steps=2, rho_floor=1e-6, P_floor=1e-6)
+    t2, n2 = bsn.run_steps(Ud, 24, 24, 24, dx, dx, dx, g, 0.4, n_steps=2, t=t1, rho_floor=1e-6, P_floor=1e-6)
+    assert (n1, n2) == (2, 2) and t2 == t
+    assert_bitwise(host(Ud), U, "resumed run")
+
+
+def _l1_rel(a, b):
+    return np.abs(a - b).sum() / np.abs(b).sum()
+
+
+def test_fp32_step_close_to_fp64(orc, bsn):
+    n = (24, 20, 16)
+    U = random_state(*n, seed=42)
+    ref = U.copy(order="F")
+    orc.euler3d_step(ref, 0.1, 0.1, 0.1, 1e-3, 1.4, rho_floor=1e-6, P_floor=1e-4)
+    Ud = dev(U)
+    bsn.euler3d_step_f32(Ud, *n, 0.1, 0.1, 0.1, 1e-3, 1.4, rho_floor=1e-6, P_floor=1e-4)
+    G = host(Ud)
+    a = (slice(NG, -NG),) * 3
+    assert _l1_rel(G[(0,) + a], ref[(0,) + a]) < 1e-5
+    assert _l1_rel(G[(4,) + a], ref[(4,) + a]) < 1e-5
+
+
+def test_fp32_sedov_run_l1_vs_fp64(orc, bsn):
+    U, dx = _sedov(orc)
+    Ud = dev(U)
+    g, tend = 5 / 3, 0.1
+    t = 0.0
+    while t < tend:
+        dt = min(orc.cfl_dt_3d(U, dx, dx, dx, g, 0.4), tend - t)
+        orc.euler3d_step(U, dx, dx, dx, dt, g, rho_floor=1e-6, P_floor=1e-6)
+        t += dt
+    tg, ng = bsn.run_steps(Ud, 32, 32, 32, dx, dx, dx, g, 0.4, n_steps=10000, t_end=tend, rho_floor=1e-6,
+                           P_floor=1e-6, precision="f32")
+    assert abs(tg - tend) < 1e-12
+    G = host(Ud)
+    a = (slice(NG, -NG),) * 3
+    e_rho = _l1_rel(G[(0,) + a], U[(0,) + a])
+    e_E = _l1_rel(G[(4,) + a], U[(4,) + a])
+    print(f"FP32 vs FP64 Sedov 32^3 t=0.1: L1 rho {e_rho:.3e}, L1 E {e_E:.3e}, steps {ng}")
+    assert e_rho < 1e-5 and e_E < 1e-5
