@@ -6,7 +6,7 @@ floors rho 1e-6 / P 1e-6.  A step is one CFL dt reduction plus one full RK3
 step, the loop the reference drivers run (cfl_dt_3d + euler3d_step!).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bsn|reference]
-                  [--n 256] [--path f64]
+                  [--n 256] [--path f32|f64] [--tile V] [--no-cpu]
 
 `value` is device-resident throughput over K steps (state in HBM).  `e2e`
 runs the same step through the public host-buffer path: the state is copied
@@ -148,11 +148,9 @@ def run_reference(args, rank, world):
 
 
 def run_bsn(args, rank, world):
-    import ctypes as C
     import numpy as np
     import torch
     import bsn
-    from bsn._lib import load
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -164,71 +162,87 @@ def run_bsn(args, rank, world):
     ncell = n ** 3
     kw = dict(rho_floor=1e-6, P_floor=1e-6)
     Ud = torch.from_numpy(U0).cuda()
-    ctx = bsn.context()
-    L = load()
 
-    def step(U):
-        dt = bsn.cfl_dt_3d(U, n, n, n, dx, dx, dx, GAMMA, CFL)
-        bsn.euler3d_step(U, n, n, n, dx, dx, dx, dt, GAMMA, **kw)
+    def steps(U, k, prec, t=0.0):
+        return bsn.run_steps(U, n, n, n, dx, dx, dx, GAMMA, CFL, n_steps=k, t=t, precision=prec, **kw)
 
-    for _ in range(args.warmup):
-        step(Ud)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = bsn.launch_count()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    def timed(prec, k):
+        """K device-resident RK3 steps (dt on the device, one graph per step)."""
+        U = torch.from_numpy(U0).cuda()
+        t, _ = steps(U, args.warmup, prec)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = bsn.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(args.steps):
-            step(Ud)
+        steps(U, k, prec, t)
         e1.record()
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    launches = bsn.launch_count() - launches0
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
-    value = world * ncell * args.steps / (ms / 1e3)
+        ms = e0.elapsed_time(e1)
+        if dist:
+            tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        return ms, bsn.launch_count() - l0
 
-    # roofline: average stage-kernel launch time from events around each launch
-    L.bsn_ctx_set_profiling(ctx, 1)
+    prec = args.path
+    other = "f64" if prec == "f32" else "f32"
+    if args.tile >= 0:
+        for p_ in ("f32", "f64"):
+            bsn.set_tile(p_, min(args.tile, bsn.tile_variants(p_) - 1))
+    with ClockSampler(local) as clk:
+        ms, launches = timed(prec, args.steps)
+    ms_other, _ = timed(other, args.steps)
+    value = world * ncell * args.steps / (ms / 1e3)
+    value_other = world * ncell * args.steps / (ms_other / 1e3)
+
+    # roofline of the dominant kernel: stage-kernel launches timed with CUDA
+    # events around each launch (per-step entry point, same kernels)
+    kname = "stage_kernel_f32" if prec == "f32" else "stage_kernel"
+    step_fn = bsn.euler3d_step_f32 if prec == "f32" else bsn.euler3d_step
+    Up = torch.from_numpy(U0).cuda()
+    dt0 = bsn.cfl_dt_3d(Up, n, n, n, dx, dx, dx, GAMMA, CFL)
+    step_fn(Up, n, n, n, dx, dx, dx, dt0, GAMMA, **kw)
+    bsn.set_profiling(True)
     for _ in range(3):
-        step(Ud)
-    tot, cnt = C.c_double(), C.c_longlong()
-    L.bsn_ctx_kernel_stats(ctx, b"stage_kernel", C.byref(tot), C.byref(cnt))
-    L.bsn_ctx_set_profiling(ctx, 0)
-    t_stage = tot.value / max(cnt.value, 1) / 1e3
-    # algorithmic state traffic: 40 words/cell per RK3 step over 3 stage launches
-    alg_bytes = 40 * 8 * ncell / 3.0
+        step_fn(Up, n, n, n, dx, dx, dx, dt0, GAMMA, **kw)
+    tot, cnt = bsn.kernel_time(kname)
+    bsn.set_profiling(False)
+    t_stage = tot / max(cnt, 1) / 1e3
+    alg_bytes = 40 * 8 * ncell / 3.0     # 40 FP64 state words per cell per RK3 step, 3 stage launches
     hbm, hbm_kind = peaks()
     achieved = alg_bytes / t_stage / 1e9
+    tile = bsn.get_tile(n, n, n, prec)
+    del Up
 
-    # e2e through the host-buffer path (pinned host state, H2D + step + D2H)
+    # e2e: host-buffer path -- pinned host state -> device, one CFL-limited
+    # RK3 step through the public entry point, device -> host, every step
     Uh = torch.from_numpy(U0.copy(order="F")).pin_memory()
     Ue = torch.empty_like(Ud)
     nbytes = Uh.numel() * 8
     for _ in range(2):
-        Ue.copy_(Uh, non_blocking=True); step(Ue); Uh.copy_(Ue, non_blocking=True)
+        Ue.copy_(Uh, non_blocking=True)
+        steps(Ue, 1, prec)
+        Uh.copy_(Ue, non_blocking=True)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     k_e2e = max(2, min(args.steps, 10))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(k_e2e):
         Ue.copy_(Uh, non_blocking=True)
-        step(Ue)
+        steps(Ue, 1, prec)
         Uh.copy_(Ue, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
     if dist:
-        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+        tt = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_e2e = float(tt.item())
     e2e = world * ncell * k_e2e / (ms_e2e / 1e3)
 
     cpu = None
@@ -239,18 +253,24 @@ def run_bsn(args, rank, world):
         cpu = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
                "sample": f"2 RK3 steps (oracle, FP64) of a {n}x{n}x{nz} z-slab of Sedov {n}^3, {el:.1f} s"}
     if rank == 0:
+        desc = {"f32": "FP32 stencils/fluxes, FP64 state and RK3 accumulation",
+                "f64": "FP64, bit-identical to the reference CPU path"}
         line = {
-            "metric": "cell-updates/s per RK3 step (Sedov 3D, FP64 WENO5-Z+HLLC+SSP-RK3)",
+            "metric": "cell-updates/s per RK3 step (Sedov 3D, WENO5-Z+HLLC+SSP-RK3)",
             "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (Sedov initial condition, sedov_ic_3d!)",
-            "config": {"workload": f"sedov{n}^3", "grid": [n, n, n], "path": args.path,
+            "dtype": "f32" if prec == "f32" else "f64", "data": "synthetic (Sedov initial condition, sedov_ic_3d!)",
+            "config": {"workload": f"sedov{n}^3", "grid": [n, n, n], "path": desc[prec],
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "tile": list(tile), "time_loop": "device-resident dt, one CUDA graph per step",
                        "l2": f"state {Ud.numel() * 8 / 1e6:.0f} MB per array > 126 MB L2 (no flush needed)"},
-            "roofline": {"bound": "hbm", "kernel": "stage_kernel", "achieved": achieved, "peak": hbm,
-                         "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+            "compare": {f"{other}_value": value_other, f"{other}_ms_per_step": ms_other / args.steps,
+                        f"speedup_vs_{other}": value / value_other},
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_kind": hbm_kind,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": t_stage * 1e3,
-                         "note": "FP64 stencil kernel is FP64-pipe bound; HBM fraction of algorithmic bytes"},
+                         "note": "the fused stencil kernel is FP-pipe bound (FP32/FP64), not HBM bound; "
+                                 "HBM fraction of the algorithmic 40 words/cell-step"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "steps": k_e2e},
@@ -267,8 +287,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="bsn", choices=["bsn", "reference"])
     ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--path", default="f64", choices=["f64"])
+    ap.add_argument("--path", default="f32", choices=["f32", "f64"],
+                    help="stencil precision of the timed path (the other is reported beside it)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--tile", type=int, default=-1,
+                    help="force this stage-kernel tile variant for both precisions (default: autotune)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
