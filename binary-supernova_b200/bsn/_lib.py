@@ -70,6 +70,14 @@ SIGNATURES = {
     "bsn_euler3d_step_f32": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _I, _D, _D]),
     "bsn_run_steps": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _I, _D, _D, _I, _I, _D, _dp,
                            C.POINTER(C.c_int)]),
+    "bsn_euler3d_step_learned": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _I, _D, _D]),
+    "bsn_learned_param_count": (_I, []),
+    "bsn_learned_collect": (_I, [_V, _P, _I, _I, _I, _I, _D, _I, C.c_ulonglong, _P, _P, _LL,
+                                 C.POINTER(C.c_longlong)]),
+    "bsn_learned_grad": (_I, [_V, _P, _LL, _P, _P, _dp]),
+    "bsn_learned_train": (_I, [_V, _P, _LL, _P, _I, _I, C.c_float, C.c_ulonglong, _dp]),
+    "bsn_learned_set_params": (_I, [_V, _P, _P]),
+    "bsn_learned_eval": (_I, [_V, _P, _LL, _P, _P, _I]),
     "bsn_tile_variant_count": (_I, [_I]),
     "bsn_ctx_set_tile": (_I, [_V, _I, _I]),
     "bsn_ctx_get_tile": (_I, [_V, _I, _I, _I, _I, C.POINTER(C.c_int)]),

@@ -340,13 +340,20 @@ def solve_fmr_poisson(G: FMRGrid3D):
 # fast path, device time loop, tile autotuner (no single reference counterpart:
 # the reference driver loop test/test_sedov.jl:45-52 run on the device)
 
-PREC = {"f64": 0, "f32": 1}
+PREC = {"f64": 0, "f32": 1, "learned": 2}
 
 
 def euler3d_step_f32(U, nx, ny, nz, dx, dy, dz, dt, gamma, *, bc="outflow", rho_floor=0.0, P_floor=0.0):
     """euler3d_step! with FP32 stencils/fluxes; FP64 state and RK3 accumulation."""
     _check_state(U, nx, ny, nz)
     _call("bsn_euler3d_step_f32", context(), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz), float(dt),
+          float(gamma), BC[bc], float(rho_floor), float(P_floor))
+
+
+def euler3d_step_learned(U, nx, ny, nz, dx, dy, dz, dt, gamma, *, bc="outflow", rho_floor=0.0, P_floor=0.0):
+    """euler3d_step! with the learned WENO weights on smooth stencils (FP32 stencils, FP64 state)."""
+    _check_state(U, nx, ny, nz)
+    _call("bsn_euler3d_step_learned", context(), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz), float(dt),
           float(gamma), BC[bc], float(rho_floor), float(P_floor))
 
 
@@ -387,5 +394,5 @@ def set_profiling(on: bool):
     _call("bsn_ctx_set_profiling", context(), int(bool(on)))
 
 
-__all__ += ["euler3d_step_f32", "run_steps", "tile_variants", "set_tile", "get_tile", "kernel_time",
+__all__ += ["euler3d_step_f32", "euler3d_step_learned", "run_steps", "tile_variants", "set_tile", "get_tile", "kernel_time",
             "set_profiling", "PREC"]

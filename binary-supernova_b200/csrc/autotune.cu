@@ -10,10 +10,18 @@
 
 namespace bsn {
 
-static int variant_count(int prec) { return prec == PREC_F64 ? f64_variant_count() : f32_variant_count(); }
-static bsn_status launch_variant(bsn_ctx* ctx, int prec, int idx, const f64::StageArgs& A) {
-    return prec == PREC_F64 ? f64_launch_variant(ctx, idx, A) : f32_launch_variant(ctx, idx, A);
+static int variant_count(int prec) {
+    return prec == PREC_F64 ? f64_variant_count() : (prec == PREC_F32 ? f32_variant_count() : learned_variant_count());
 }
+static TileVariant variant(int prec, int idx) {
+    return prec == PREC_F64 ? f64_variant(idx) : (prec == PREC_F32 ? f32_variant(idx) : learned_variant(idx));
+}
+static bsn_status launch_variant(bsn_ctx* ctx, int prec, int idx, const f64::StageArgs& A) {
+    if (prec == PREC_F64) return f64_launch_variant(ctx, idx, A);
+    if (prec == PREC_F32) return f32_launch_variant(ctx, idx, A);
+    return learned_launch_variant(ctx, idx, A);
+}
+static bool prec_ok(int p) { return p == PREC_F64 || p == PREC_F32 || p == PREC_LEARNED; }
 
 bsn_status stage_autotune(bsn_ctx* ctx, int prec, const f64::StageArgs& probe, double* scratch) {
     auto key = std::make_tuple(prec, probe.nx, probe.ny, probe.nz);
@@ -93,7 +101,7 @@ using namespace bsn;
 
 extern "C" bsn_status bsn_ctx_set_tile(bsn_ctx* ctx, int precision, int variant) {
     if (!ctx) return BSN_ERR_ARG;
-    if (precision != PREC_F64 && precision != PREC_F32) return set_err(ctx, BSN_ERR_ARG, "bad precision %d", precision);
+    if (!prec_ok(precision)) return set_err(ctx, BSN_ERR_ARG, "bad precision %d", precision);
     if (variant >= variant_count(precision)) return set_err(ctx, BSN_ERR_ARG, "no tile variant %d", variant);
     ctx->forced_tile[precision] = variant < 0 ? -1 : variant;
     for (auto it = ctx->tile_choice.begin(); it != ctx->tile_choice.end();)
@@ -105,11 +113,12 @@ extern "C" bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int 
     if (!ctx || !out) return BSN_ERR_ARG;
     auto it = ctx->tile_choice.find(std::make_tuple(precision, nx, ny, nz));
     if (it == ctx->tile_choice.end()) return set_err(ctx, BSN_ERR_ARG, "no tile chosen yet for this grid");
-    TileVariant v = precision == PREC_F64 ? f64_variant(it->second) : f32_variant(it->second);
+    if (!prec_ok(precision)) return set_err(ctx, BSN_ERR_ARG, "bad precision %d", precision);
+    TileVariant v = variant(precision, it->second);
     out[0] = v.tx; out[1] = v.ty; out[2] = v.tz; out[3] = v.nt;
     return BSN_OK;
 }
 
 extern "C" int bsn_tile_variant_count(int precision) {
-    return precision == PREC_F64 ? f64_variant_count() : (precision == PREC_F32 ? f32_variant_count() : 0);
+    return prec_ok(precision) ? variant_count(precision) : 0;
 }

@@ -33,7 +33,8 @@ struct bsn_ctx {
     std::vector<Rec> recs;
     // stage-kernel tile choice per (precision, nx, ny, nz): autotuned or forced
     std::map<std::tuple<int, int, int, int>, int> tile_choice;
-    int forced_tile[2] = {-1, -1};
+    int forced_tile[3] = {-1, -1, -1};
+    void* learned_state = nullptr;   // learned.cu: packed network parameters
     // graph-captured device time loop (run_steps.cu)
     void* run_state = nullptr;
 };

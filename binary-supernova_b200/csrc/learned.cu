@@ -1,0 +1,668 @@
+// learned.cu -- the learned WENO-weight network: sample collection from the
+// method's own runs, hand-written training kernels (forward, backward, Adam),
+// BF16 tensor-core inference (mma.sync m16n8k16, FP32 accumulation) used by
+// the learned stencil kernel, and a standalone evaluator for tests.
+//
+// Tensor-core choice: the network is tiny (K = 16/32, N = 32/8) and its output
+// is consumed immediately by the same thread's reconstruction.  Warp-level
+// mma.sync keeps the fragments in registers, and the accumulator fragment of
+// one layer is the A fragment of the next without any data movement; tcgen05
+// would need the activations in shared memory and the accumulators in TMEM,
+// i.e. a shared-memory/TMEM round trip per layer per 128-row tile inside the
+// stencil kernel.  Built with the fast-path flags (FMA, approximate div/sqrt).
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <vector>
+
+#include "hydro_f64.cuh"
+#include "learned.cuh"
+#include "physics_f32.cuh"
+#include "stage_launch.cuh"
+#include "stage_tile.cuh"
+
+namespace bsn {
+namespace learned {
+
+// ---------------------------------------------------------------------------
+// reference WENO-Z weights in FP64 (src/weno5.jl:14-61) of one side
+__device__ inline void wenoz_weights64(const double v[5], int side, double w[3]) {
+    const double k = 13.0 / 12.0, q = 1.0 / 4.0;
+    double b0, b1, b2, d0, d1, d2;
+    if (side == 0) {
+        b0 = k * sq(v[0] - 2.0 * v[1] + v[2]) + q * sq(v[0] - 4.0 * v[1] + 3.0 * v[2]);
+        b1 = k * sq(v[1] - 2.0 * v[2] + v[3]) + q * sq(v[1] - v[3]);
+        b2 = k * sq(v[2] - 2.0 * v[3] + v[4]) + q * sq(3.0 * v[2] - 4.0 * v[3] + v[4]);
+        d0 = 1.0 / 10.0; d1 = 6.0 / 10.0; d2 = 3.0 / 10.0;
+    } else {
+        b0 = k * sq(v[0] - 2.0 * v[1] + v[2]) + q * sq(v[0] - v[2]);
+        b1 = k * sq(v[1] - 2.0 * v[2] + v[3]) + q * sq(v[1] - 4.0 * v[2] + 3.0 * v[3]);
+        b2 = k * sq(v[2] - 2.0 * v[3] + v[4]) + q * sq(3.0 * v[2] - 4.0 * v[3] + v[4]);
+        d0 = 3.0 / 10.0; d1 = 6.0 / 10.0; d2 = 1.0 / 10.0;
+    }
+    const double eps = 1e-36;
+    double tau = fabs(b0 - b2);
+    double a0 = d0 * (1.0 + sq(tau / (eps + b0)));
+    double a1 = d1 * (1.0 + sq(tau / (eps + b1)));
+    double a2 = d2 * (1.0 + sq(tau / (eps + b2)));
+    double s = a0 + a1 + a2;
+    w[0] = a0 / s; w[1] = a1 / s; w[2] = a2 / s;
+}
+
+__device__ __forceinline__ uint32_t mix32(uint64_t x) {
+    x ^= x >> 33; x *= 0xff51afd7ed558ccdull; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ull; x ^= x >> 33;
+    return (uint32_t)x;
+}
+
+// One thread per (interface, field): left and right stencils of the six
+// cells around the interface, WENO-Z weights in FP64, normalised inputs;
+// smooth stencils with a spread above rounding level are kept with
+// probability 1/stride.
+__global__ void collect_kernel(const double* U, int nx, int ny, int nz, int bc, double gm1, int stride,
+                               unsigned long long seed, float* outL, float* outR, unsigned long long* count,
+                               long long cap) {
+    Geom G(nx, ny, nz);
+    long long nfx = (long long)(nx + 1) * ny * nz, nfy = (long long)nx * (ny + 1) * nz,
+              nfz = (long long)nx * ny * (nz + 1);
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long tot = 5 * (nfx + nfy + nfz);
+    if (t >= tot) return;
+    int fld = (int)(t % 5);
+    long long f = t / 5;
+    int d;
+    if (f < nfx) d = 0;
+    else if ((f -= nfx) < nfy) d = 1;
+    else { f -= nfy; d = 2; }
+    int ex = nx + (d == 0), ey = ny + (d == 1);
+    int a = (int)(f % ex), b = (int)((f / ex) % ey), c = (int)(f / ((long long)ex * ey));
+    // face between cells (p-1) and p along d, p = a/b/c: cells p-3 .. p+2
+    double v[6];
+    for (int s = 0; s < 6; ++s) {
+        int o = s - 3;
+        int p[3] = {a, b, c};
+        p[d] += o;
+        int n[3] = {nx, ny, nz};
+        for (int ax = 0; ax < 3; ++ax) p[ax] = bc_map(p[ax], n[ax], bc);
+        long long off = G.act(p[0], p[1], p[2]);
+        if (fld < 4) v[s] = U[off + fld];
+        else v[s] = f64::cell_pressure(U[off], U[off + 1], U[off + 2], U[off + 3], U[off + 4], gm1);
+    }
+    for (int side = 0; side < 2; ++side) {
+        if (mix32(seed ^ (uint64_t)(2 * t + side)) % (uint32_t)stride != 0) continue;
+        double s5[5];
+        for (int i = 0; i < 5; ++i) s5[i] = v[i + side];
+        double u[5];
+        if (!normalise<double>(s5, side, u)) continue;
+        // Stencils whose spread is at the rounding level of their values (or
+        // so small that WENO-Z's 1e-36 epsilon sets the weights) reconstruct
+        // to within that spread with any weights and their normalised shape
+        // is noise: no information.  Constant stencils are among them.
+        double cen = side == 0 ? s5[2] : s5[1], spread = 0.0;
+        for (int i = 0; i < 5; ++i) spread = fmax(spread, fabs(s5[i] - cen));
+        if (!(spread > 1e-15 && spread > 1e-12 * fabs(cen))) continue;
+        double w[3];
+        wenoz_weights64(s5, side, w);
+        unsigned long long idx = atomicAdd(&count[side], 1ull);
+        if ((long long)idx >= cap) continue;
+        float* o = (side == 0 ? outL : outR) + (long long)idx * SAMPLE;
+        for (int i = 0; i < 5; ++i) o[i] = (float)u[i];
+        for (int i = 0; i < 3; ++i) o[5 + i] = (float)w[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// training: one block of TB samples computes per-sample activations and
+// deltas into shared memory, then the block's weight gradients as dot
+// products over its samples, accumulated into `grad` with atomics.
+constexpr int TB = 128;
+
+__device__ __forceinline__ long long pick(unsigned long long seed, long long step, long long i, long long n,
+                                          int random) {
+    if (!random) return i;
+    return (long long)((((uint64_t)mix32(seed ^ ((uint64_t)step << 32) ^ (uint64_t)i) << 32) |
+                        (uint64_t)mix32(seed * 31ull + (uint64_t)i * 977ull + (uint64_t)step)) %
+                       (uint64_t)n);
+}
+
+__global__ void __launch_bounds__(TB) train_grad_kernel(const float* samples, long long n, const float* P,
+                                                        float* grad, double* loss, unsigned long long seed,
+                                                        long long step, long long first, int random) {
+    extern __shared__ float sm[];
+    float* sP = sm;                          // NPARAM
+    float* sU = sP + NPARAM;                 // NIN*TB
+    float* sH1 = sU + NIN * TB;              // NH*TB
+    float* sH2 = sH1 + NH * TB;              // NH*TB
+    float* sDZ = sH2 + NH * TB;              // NOUT*TB
+    float* sD2 = sDZ + NOUT * TB;            // NH*TB
+    float* sD1 = sD2 + NH * TB;              // NH*TB
+    __shared__ double sloss[TB / 32];
+    const int t = threadIdx.x;
+    for (int i = t; i < NPARAM; i += TB) sP[i] = P[i];
+    __syncthreads();
+    long long gi = first + (long long)blockIdx.x * TB + t;
+    bool live = random ? true : gi < n;
+    float u[NIN], tg[NOUT];
+    if (live) {
+        long long s = pick(seed, step, gi, n, random);
+        const float* x = samples + s * SAMPLE;
+        for (int i = 0; i < NIN; ++i) u[i] = x[i];
+        for (int i = 0; i < NOUT; ++i) tg[i] = x[NIN + i];
+    } else {
+        for (int i = 0; i < NIN; ++i) u[i] = 0.f;
+        for (int i = 0; i < NOUT; ++i) tg[i] = 0.f;
+    }
+    for (int i = 0; i < NIN; ++i) sU[i * TB + t] = live ? u[i] : 0.f;
+    const float* W1 = sP + OFF_W1; const float* b1 = sP + OFF_B1;
+    const float* W2 = sP + OFF_W2; const float* b2 = sP + OFF_B2;
+    const float* W3 = sP + OFF_W3; const float* b3 = sP + OFF_B3;
+    for (int j = 0; j < NH; ++j) {
+        float z = b1[j];
+        for (int i = 0; i < NIN; ++i) z = fmaf(W1[j * NIN + i], u[i], z);
+        sH1[j * TB + t] = fmaxf(z, 0.f);
+    }
+    for (int j = 0; j < NH; ++j) {
+        float z = b2[j];
+        for (int i = 0; i < NH; ++i) z = fmaf(W2[j * NH + i], sH1[i * TB + t], z);
+        sH2[j * TB + t] = fmaxf(z, 0.f);
+    }
+    float zo[NOUT], om[NOUT];
+    float zmax = -1e30f;
+    for (int k = 0; k < NOUT; ++k) {
+        float z = b3[k];
+        for (int i = 0; i < NH; ++i) z = fmaf(W3[k * NH + i], sH2[i * TB + t], z);
+        zo[k] = z;
+        zmax = fmaxf(zmax, z);
+    }
+    float es = 0.f;
+    for (int k = 0; k < NOUT; ++k) { om[k] = expf(zo[k] - zmax); es += om[k]; }
+    float lsum = 0.f, g[NOUT], gdot = 0.f;
+    for (int k = 0; k < NOUT; ++k) {
+        om[k] /= es;
+        float e = om[k] - tg[k];
+        lsum += e * e;
+        g[k] = 2.f * e;
+        gdot += om[k] * g[k];
+    }
+    for (int k = 0; k < NOUT; ++k) sDZ[k * TB + t] = live ? om[k] * (g[k] - gdot) : 0.f;
+    for (int i = 0; i < NH; ++i) {
+        float s = 0.f;
+        for (int k = 0; k < NOUT; ++k) s = fmaf(W3[k * NH + i], sDZ[k * TB + t], s);
+        sD2[i * TB + t] = sH2[i * TB + t] > 0.f ? s : 0.f;
+    }
+    for (int j = 0; j < NH; ++j) {
+        float s = 0.f;
+        for (int i = 0; i < NH; ++i) s = fmaf(W2[i * NH + j], sD2[i * TB + t], s);
+        sD1[j * TB + t] = sH1[j * TB + t] > 0.f ? s : 0.f;
+    }
+    // block loss
+    double lv = live ? (double)lsum : 0.0;
+    for (int o = 16; o > 0; o >>= 1) lv += __shfl_xor_sync(0xffffffffu, lv, o);
+    if ((t & 31) == 0) sloss[t >> 5] = lv;
+    __syncthreads();
+    if (t == 0) {
+        double s = 0.0;
+        for (int w = 0; w < TB / 32; ++w) s += sloss[w];
+        atomicAdd(loss, s);
+    }
+    // weight gradients: dot products over the block's samples
+    for (int e = t; e < NPARAM; e += TB) {
+        const float *x, *y;
+        if (e < OFF_B1) { int j = e / NIN, i = e % NIN; x = sD1 + j * TB; y = sU + i * TB; }
+        else if (e < OFF_W2) { x = sD1 + (e - OFF_B1) * TB; y = nullptr; }
+        else if (e < OFF_B2) { int r = e - OFF_W2, j = r / NH, i = r % NH; x = sD2 + j * TB; y = sH1 + i * TB; }
+        else if (e < OFF_W3) { x = sD2 + (e - OFF_B2) * TB; y = nullptr; }
+        else if (e < OFF_B3) { int r = e - OFF_W3, k = r / NH, i = r % NH; x = sDZ + k * TB; y = sH2 + i * TB; }
+        else { x = sDZ + (e - OFF_B3) * TB; y = nullptr; }
+        float s = 0.f;
+        if (y) for (int b = 0; b < TB; ++b) s = fmaf(x[b], y[b], s);
+        else for (int b = 0; b < TB; ++b) s += x[b];
+        atomicAdd(&grad[e], s);
+    }
+}
+
+__global__ void adam_kernel(float* P, float* grad, float* m, float* v, float scale, float lr, float b1, float b2,
+                            float eps, float bc1, float bc2) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= NPARAM) return;
+    float g = grad[i] * scale;
+    m[i] = b1 * m[i] + (1.f - b1) * g;
+    v[i] = b2 * v[i] + (1.f - b2) * g * g;
+    float mh = m[i] / bc1, vh = v[i] / bc2;
+    P[i] -= lr * mh / (sqrtf(vh) + eps);
+    grad[i] = 0.f;
+}
+
+// ---------------------------------------------------------------------------
+// BF16 tensor-core inference.  Packed parameters (per side): W1b[32][16],
+// W2b[32][32], W3b[8][32] as BF16 (row = output unit, zero padded), then
+// b1[32], b2[32], b3[8] as FP32.
+constexpr int PK_W1 = 0, PK_W2 = PK_W1 + 32 * 16 * 2, PK_W3 = PK_W2 + 32 * 32 * 2, PK_B1 = PK_W3 + 8 * 32 * 2,
+              PK_B2 = PK_B1 + 32 * 4, PK_B3 = PK_B2 + 32 * 4, PK_BYTES = PK_B3 + 8 * 4;   // bytes per side
+
+__global__ void pack_kernel(const float* P, unsigned char* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    __nv_bfloat16* W1 = (__nv_bfloat16*)(out + PK_W1);
+    __nv_bfloat16* W2 = (__nv_bfloat16*)(out + PK_W2);
+    __nv_bfloat16* W3 = (__nv_bfloat16*)(out + PK_W3);
+    float* B1 = (float*)(out + PK_B1);
+    float* B2 = (float*)(out + PK_B2);
+    float* B3 = (float*)(out + PK_B3);
+    if (i < 32 * 16) { int n = i / 16, k = i % 16; W1[i] = __float2bfloat16(k < NIN ? P[OFF_W1 + n * NIN + k] : 0.f); }
+    if (i < 32 * 32) W2[i] = __float2bfloat16(P[OFF_W2 + i]);
+    if (i < 8 * 32) { int n = i / 32, k = i % 32; W3[i] = __float2bfloat16(n < NOUT ? P[OFF_W3 + n * NH + k] : 0.f); }
+    if (i < 32) { B1[i] = P[OFF_B1 + i]; B2[i] = P[OFF_B2 + i]; }
+    if (i < 8) B3[i] = i < NOUT ? P[OFF_B3 + i] : 0.f;
+}
+
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+
+__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Warp-collective MLP over `ntiles` tiles of 16 rows.  rows: BF16 inputs,
+// 16 per row (5 used), 32 B per row.  Logits of row r are written to
+// out[4*r .. 4*r+2] (may alias rows of tiles already consumed).
+__device__ void mlp_tiles(const unsigned char* pk, const uint32_t* rows, float* out, int ntiles) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
+    const uint32_t* W1 = (const uint32_t*)(pk + PK_W1);   // row n: 8 words
+    const uint32_t* W2 = (const uint32_t*)(pk + PK_W2);   // row n: 16 words
+    const uint32_t* W3 = (const uint32_t*)(pk + PK_W3);   // row n: 16 words
+    const float* B1 = (const float*)(pk + PK_B1);
+    const float* B2 = (const float*)(pk + PK_B2);
+    const float* B3 = (const float*)(pk + PK_B3);
+    for (int tile = 0; tile < ntiles; ++tile) {
+        int r0 = tile * 16 + g, r1 = r0 + 8;
+        uint32_t a[4] = {rows[r0 * 8 + tg], rows[r1 * 8 + tg], rows[r0 * 8 + 4 + tg], rows[r1 * 8 + 4 + tg]};
+        __syncwarp();
+        // layer 1: 16 -> 32
+        float h[4][4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float c0 = B1[8 * j + 2 * tg], c1 = B1[8 * j + 2 * tg + 1];
+            h[j][0] = c0; h[j][1] = c1; h[j][2] = c0; h[j][3] = c1;
+            mma16816(h[j], a, W1[(8 * j + g) * 8 + tg], W1[(8 * j + g) * 8 + 4 + tg]);
+        }
+        uint32_t a2[2][4];
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {
+            a2[kk][0] = pack2(fmaxf(h[2 * kk][0], 0.f), fmaxf(h[2 * kk][1], 0.f));
+            a2[kk][1] = pack2(fmaxf(h[2 * kk][2], 0.f), fmaxf(h[2 * kk][3], 0.f));
+            a2[kk][2] = pack2(fmaxf(h[2 * kk + 1][0], 0.f), fmaxf(h[2 * kk + 1][1], 0.f));
+            a2[kk][3] = pack2(fmaxf(h[2 * kk + 1][2], 0.f), fmaxf(h[2 * kk + 1][3], 0.f));
+        }
+        // layer 2: 32 -> 32
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float c0 = B2[8 * j + 2 * tg], c1 = B2[8 * j + 2 * tg + 1];
+            h[j][0] = c0; h[j][1] = c1; h[j][2] = c0; h[j][3] = c1;
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk)
+                mma16816(h[j], a2[kk], W2[(8 * j + g) * 16 + 8 * kk + tg], W2[(8 * j + g) * 16 + 8 * kk + 4 + tg]);
+        }
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {
+            a2[kk][0] = pack2(fmaxf(h[2 * kk][0], 0.f), fmaxf(h[2 * kk][1], 0.f));
+            a2[kk][1] = pack2(fmaxf(h[2 * kk][2], 0.f), fmaxf(h[2 * kk][3], 0.f));
+            a2[kk][2] = pack2(fmaxf(h[2 * kk + 1][0], 0.f), fmaxf(h[2 * kk + 1][1], 0.f));
+            a2[kk][3] = pack2(fmaxf(h[2 * kk + 1][2], 0.f), fmaxf(h[2 * kk + 1][3], 0.f));
+        }
+        // layer 3: 32 -> 8 (3 used)
+        float o[4] = {B3[2 * tg], B3[2 * tg + 1], B3[2 * tg], B3[2 * tg + 1]};
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) mma16816(o, a2[kk], W3[g * 16 + 8 * kk + tg], W3[g * 16 + 8 * kk + 4 + tg]);
+        __syncwarp();
+        if (tg == 0) {
+            out[4 * r0 + 0] = o[0]; out[4 * r0 + 1] = o[1];
+            out[4 * r1 + 0] = o[2]; out[4 * r1 + 1] = o[3];
+        } else if (tg == 1) {
+            out[4 * r0 + 2] = o[0];
+            out[4 * r1 + 2] = o[2];
+        }
+        __syncwarp();
+    }
+}
+
+__device__ __forceinline__ void softmax3(const float* z, float w[3]) {
+    float m = fmaxf(fmaxf(z[0], z[1]), z[2]);
+    float e0 = __expf(z[0] - m), e1 = __expf(z[1] - m), e2 = __expf(z[2] - m);
+    float inv = 1.0f / (e0 + e1 + e2);
+    w[0] = e0 * inv; w[1] = e1 * inv; w[2] = e2 * inv;
+}
+
+// FP32 CUDA-core forward (the training kernels' arithmetic), for checking.
+__device__ void mlp_fp32(const float* P, const float u[5], float w[3]) {
+    float h1[NH], h2[NH], z[NOUT];
+    for (int j = 0; j < NH; ++j) {
+        float s = P[OFF_B1 + j];
+        for (int i = 0; i < NIN; ++i) s = fmaf(P[OFF_W1 + j * NIN + i], u[i], s);
+        h1[j] = fmaxf(s, 0.f);
+    }
+    for (int j = 0; j < NH; ++j) {
+        float s = P[OFF_B2 + j];
+        for (int i = 0; i < NH; ++i) s = fmaf(P[OFF_W2 + j * NH + i], h1[i], s);
+        h2[j] = fmaxf(s, 0.f);
+    }
+    for (int k = 0; k < NOUT; ++k) {
+        float s = P[OFF_B3 + k];
+        for (int i = 0; i < NH; ++i) s = fmaf(P[OFF_W3 + k * NH + i], h2[i], s);
+        z[k] = s;
+    }
+    softmax3(z, w);
+}
+
+// Standalone evaluation of n normalised stencils: tc = 0 FP32 CUDA cores,
+// tc = 1 the BF16 tensor-core path of the stencil kernel.
+__global__ void eval_kernel(const float* u, long long n, const float* P, const unsigned char* pk, float* w, int tc) {
+    __shared__ __align__(16) uint32_t rows[4][32 * 8];     // 32 rows per warp
+    __shared__ __align__(16) unsigned char spk[PK_BYTES];
+    __shared__ float logits[4][32 * 4];
+    for (int i = threadIdx.x; i < PK_BYTES; i += blockDim.x) spk[i] = pk[i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    float x[5] = {0, 0, 0, 0, 0};
+    if (i < n) for (int k = 0; k < 5; ++k) x[k] = u[i * 5 + k];
+    if (!tc) {
+        if (i < n) { float o[3]; mlp_fp32(P, x, o); for (int k = 0; k < 3; ++k) w[i * 3 + k] = o[k]; }
+        return;
+    }
+    uint32_t* R = rows[warp];
+    R[lane * 8 + 0] = pack2(x[0], x[1]);
+    R[lane * 8 + 1] = pack2(x[2], x[3]);
+    R[lane * 8 + 2] = pack2(x[4], 0.f);
+    for (int k = 3; k < 8; ++k) R[lane * 8 + k] = 0u;
+    __syncwarp();
+    mlp_tiles(spk, R, logits[warp], 2);
+    if (i < n) { float o[3]; softmax3(&logits[warp][4 * lane], o); for (int k = 0; k < 3; ++k) w[i * 3 + k] = o[k]; }
+}
+
+struct State {
+    unsigned char* packed = nullptr;   // 2 sides * PK_BYTES, device
+    bool ready = false;
+};
+
+}  // namespace learned
+
+// ---------------------------------------------------------------------------
+// the learned stencil policy: FP32 stencil physics whose WENO weights come
+// from the network (BF16 tensor cores) where the stencil is smooth.
+namespace tile {
+
+struct F32Learned {
+    using real = float;
+    static constexpr bool kCenterFromSmem = false;
+    static constexpr bool kWarpFaces = true;
+    // packed parameters of both sides + per-warp row buffers (160 rows x 32 B)
+    static constexpr int kExtraSmem(int nt) { return 2 * learned::PK_BYTES + (nt / 32) * 160 * 32; }
+    struct Consts { float g, gm1, inv_gm1, gg; };
+    __device__ static Consts consts(const f64::StageArgs& A) {
+        float g = (float)A.g;
+        return {g, (float)A.gm1, 1.0f / (float)A.gm1, (g + 1.0f) / (2.0f * g)};
+    }
+    __device__ static float pressure(const float v[5], const Consts& k) {
+        return f32::cell_pressure(v[0], v[1], v[2], v[3], v[4], k.gm1);
+    }
+    __device__ static void prologue(unsigned char* psm, const f64::StageArgs& A, int nt) {
+        const unsigned char* src = (const unsigned char*)A.mlp;
+        for (int i = threadIdx.x; i < 2 * learned::PK_BYTES; i += nt) psm[i] = src[i];
+    }
+    // WENO weights of one reconstruction in FP32 (plain WENO5-Z)
+    __device__ static void wenoz_w(const float s[5], int side, float w[3]) {
+        const float k = 13.0f / 12.0f;
+        float b0, b1, b2, d0, d1, d2;
+        if (side == 0) {
+            float x = s[0] - 2.f * s[1] + s[2], y = s[0] - 4.f * s[1] + 3.f * s[2];
+            b0 = fmaf(k * x, x, 0.25f * y * y);
+            x = s[1] - 2.f * s[2] + s[3]; y = s[1] - s[3];
+            b1 = fmaf(k * x, x, 0.25f * y * y);
+            x = s[2] - 2.f * s[3] + s[4]; y = 3.f * s[2] - 4.f * s[3] + s[4];
+            b2 = fmaf(k * x, x, 0.25f * y * y);
+            d0 = 0.1f; d1 = 0.6f; d2 = 0.3f;
+        } else {
+            float x = s[0] - 2.f * s[1] + s[2], y = s[0] - s[2];
+            b0 = fmaf(k * x, x, 0.25f * y * y);
+            x = s[1] - 2.f * s[2] + s[3]; y = s[1] - 4.f * s[2] + 3.f * s[3];
+            b1 = fmaf(k * x, x, 0.25f * y * y);
+            x = s[2] - 2.f * s[3] + s[4]; y = 3.f * s[2] - 4.f * s[3] + s[4];
+            b2 = fmaf(k * x, x, 0.25f * y * y);
+            d0 = 0.3f; d1 = 0.6f; d2 = 0.1f;
+        }
+        const float eps = 1e-36f, cap = 1e18f;
+        float tau = fabsf(b0 - b2);
+        float t0 = fminf(tau / (eps + b0), cap), t1 = fminf(tau / (eps + b1), cap), t2 = fminf(tau / (eps + b2), cap);
+        float a0 = d0 * fmaf(t0, t0, 1.f), a1 = d1 * fmaf(t1, t1, 1.f), a2 = d2 * fmaf(t2, t2, 1.f);
+        float inv = 1.0f / (a0 + a1 + a2);
+        w[0] = a0 * inv; w[1] = a1 * inv; w[2] = a2 * inv;
+    }
+    // One interface per lane; every lane of the warp calls this (valid or not)
+    template <int D>
+    __device__ static void warp_flux(const float (&c)[6][6], bool valid, const Consts& k, float F[5],
+                                     unsigned char* psm, int warp) {
+        const int lane = threadIdx.x & 31;
+        uint32_t* R = (uint32_t*)(psm + 2 * learned::PK_BYTES + warp * 160 * 32);
+        float* logit = (float*)R;
+        float L[5], Rv[5];
+        const float t13 = 1.0f / 3.0f, m76 = -7.0f / 6.0f, e116 = 11.0f / 6.0f, m16 = -1.0f / 6.0f,
+                    f56 = 5.0f / 6.0f;
+        bool use[2][5];
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                float s[5], u[5];
+#pragma unroll
+                for (int i = 0; i < 5; ++i) s[i] = valid ? c[i + side][q] : 0.f;
+                use[side][q] = learned::normalise<float>(s, side, u);
+                int r = lane * 5 + q;
+                R[r * 8 + 0] = learned::pack2(u[0], u[1]);
+                R[r * 8 + 1] = learned::pack2(u[2], u[3]);
+                R[r * 8 + 2] = learned::pack2(u[4], 0.f);
+                R[r * 8 + 3] = 0u; R[r * 8 + 4] = 0u; R[r * 8 + 5] = 0u; R[r * 8 + 6] = 0u; R[r * 8 + 7] = 0u;
+            }
+            __syncwarp();
+            learned::mlp_tiles(psm + side * learned::PK_BYTES, R, logit, 10);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                float s[5];
+#pragma unroll
+                for (int i = 0; i < 5; ++i) s[i] = c[i + side][q];
+                float w[3];
+                if (use[side][q]) learned::softmax3(&logit[4 * (lane * 5 + q)], w);
+                else wenoz_w(s, side, w);
+                float qa, qb, qc;
+                if (side == 0) {
+                    qa = t13 * s[0] + m76 * s[1] + e116 * s[2];
+                    qb = m16 * s[1] + f56 * s[2] + t13 * s[3];
+                    qc = t13 * s[2] + f56 * s[3] + m16 * s[4];
+                } else {
+                    qa = m16 * s[0] + f56 * s[1] + t13 * s[2];
+                    qb = t13 * s[1] + f56 * s[2] + m16 * s[3];
+                    qc = e116 * s[2] + m76 * s[3] + t13 * s[4];
+                }
+                float v = fmaf(w[0], qa, fmaf(w[1], qb, w[2] * qc));
+                if (side == 0) L[q] = v; else Rv[q] = v;
+            }
+            __syncwarp();
+        }
+        float PmaxL = fmaxf(fmaxf(fmaxf(fmaxf(c[0][5], c[1][5]), c[2][5]), c[3][5]), c[4][5]);
+        float PmaxR = fmaxf(fmaxf(fmaxf(fmaxf(c[1][5], c[2][5]), c[3][5]), c[4][5]), c[5][5]);
+        float PL = fminf(fmaxf(L[4], 0.0f), PmaxL);
+        float PR = fminf(fmaxf(Rv[4], 0.0f), PmaxR);
+        float EL = f32::EL_from_P(PL, L[0], L[1], L[2], L[3], k.inv_gm1);
+        float ER = f32::EL_from_P(PR, Rv[0], Rv[1], Rv[2], Rv[3], k.inv_gm1);
+        float Fr[5];
+        if (D == 0) {
+            f32::hllc_normal(L[0], L[1], L[2], L[3], EL, Rv[0], Rv[1], Rv[2], Rv[3], ER, k.g, k.gm1, k.gg, Fr);
+            F[0] = Fr[0]; F[1] = Fr[1]; F[2] = Fr[2]; F[3] = Fr[3]; F[4] = Fr[4];
+        } else if (D == 1) {
+            f32::hllc_normal(L[0], L[2], L[1], L[3], EL, Rv[0], Rv[2], Rv[1], Rv[3], ER, k.g, k.gm1, k.gg, Fr);
+            F[0] = Fr[0]; F[1] = Fr[2]; F[2] = Fr[1]; F[3] = Fr[3]; F[4] = Fr[4];
+        } else {
+            f32::hllc_normal(L[0], L[3], L[1], L[2], EL, Rv[0], Rv[3], Rv[1], Rv[2], ER, k.g, k.gm1, k.gg, Fr);
+            F[0] = Fr[0]; F[1] = Fr[2]; F[2] = Fr[3]; F[3] = Fr[1]; F[4] = Fr[4];
+        }
+    }
+    template <int D>
+    __device__ static void flux(const float (&)[6][6], const Consts&, float F[5]) {
+        F[0] = F[1] = F[2] = F[3] = F[4] = 0.f;   // unused: kWarpFaces
+    }
+};
+
+}  // namespace tile
+
+namespace {
+const TileVariant kLearnedVariants[] = {{8, 8, 8, 256}, {16, 8, 4, 256}};
+
+template <int TX, int TY, int TZ, int NT, int MINB>
+bsn_status launch_learned(bsn_ctx* ctx, const f64::StageArgs& A) {
+    auto fn = tile::stage_kernel<tile::F32Learned, TX, TY, TZ, NT, MINB>;
+    constexpr int smem = tile::smem_bytes<tile::F32Learned, TX, TY, TZ>() + tile::F32Learned::kExtraSmem(NT) + 16;
+    static bool attr_done[64] = {false};
+    int dev = ctx->device & 63;
+    if (!attr_done[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaFuncSetAttribute(stage_kernel_learned)");
+        attr_done[dev] = true;
+    }
+    dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + TZ - 1) / TZ);
+    prof_begin(ctx);
+    fn<<<grid, NT, smem, ctx->stream>>>(A);
+    return launch_check(ctx, "stage_kernel_learned");
+}
+}  // namespace
+
+int learned_variant_count() { return (int)(sizeof(kLearnedVariants) / sizeof(kLearnedVariants[0])); }
+TileVariant learned_variant(int idx) { return kLearnedVariants[idx]; }
+bsn_status learned_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A0) {
+    learned::State* S = (learned::State*)ctx->learned_state;
+    if (!S || !S->ready) return set_err(ctx, BSN_ERR_ARG, "no learned WENO weights set (bsn_learned_set_params)");
+    f64::StageArgs A = A0;
+    A.mlp = S->packed;
+    switch (idx) {
+        case 0: return launch_learned<8, 8, 8, 256, 2>(ctx, A);
+        case 1: return launch_learned<16, 8, 4, 256, 2>(ctx, A);
+        default: return set_err(ctx, BSN_ERR_ARG, "no learned tile variant %d", idx);
+    }
+}
+
+void learned_state_free(bsn_ctx* ctx) {
+    if (!ctx->learned_state) return;
+    learned::State* S = (learned::State*)ctx->learned_state;
+    if (S->packed) cudaFree(S->packed);
+    delete S;
+    ctx->learned_state = nullptr;
+}
+
+}  // namespace bsn
+
+using namespace bsn;
+using namespace bsn::learned;
+
+extern "C" int bsn_learned_param_count(void) { return NPARAM; }
+
+extern "C" bsn_status bsn_learned_collect(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, int bc, double gamma,
+                                          int stride, unsigned long long seed, float* out_left, float* out_right,
+                                          long long cap, long long counts[2]) {
+    BSN_TRY(check_dims(ctx, nx, ny, nz));
+    if (!U || !out_left || !out_right || !counts || stride < 1 || cap < 0)
+        return set_err(ctx, BSN_ERR_ARG, "bad arguments to bsn_learned_collect");
+    bsn_status st;
+    unsigned long long* cnt = (unsigned long long*)slot(ctx, SLOT_RED, 64, &st); BSN_TRY(st);
+    // resume counting from the caller's counts (appending to the buffers)
+    unsigned long long h0[2] = {(unsigned long long)counts[0], (unsigned long long)counts[1]};
+    BSN_CUDA(ctx, cudaMemcpyAsync(cnt, h0, 16, cudaMemcpyHostToDevice, ctx->stream));
+    long long tot = 5LL * ((long long)(nx + 1) * ny * nz + (long long)nx * (ny + 1) * nz + (long long)nx * ny * (nz + 1));
+    collect_kernel<<<grid1d(tot, 256), 256, 0, ctx->stream>>>(U, nx, ny, nz, bc, gamma - 1.0, stride, seed, out_left,
+                                                              out_right, cnt, cap);
+    BSN_TRY(launch_check(ctx, "collect_kernel"));
+    unsigned long long h[2];
+    BSN_CUDA(ctx, cudaMemcpyAsync(h, cnt, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    counts[0] = (long long)std::min<unsigned long long>(h[0], (unsigned long long)cap);
+    counts[1] = (long long)std::min<unsigned long long>(h[1], (unsigned long long)cap);
+    return BSN_OK;
+}
+
+static size_t train_smem() { return sizeof(float) * (NPARAM + (NIN + 4 * NH + NOUT) * TB); }
+
+extern "C" bsn_status bsn_learned_grad(bsn_ctx* ctx, const float* samples, long long n, const float* params,
+                                       float* grad, double* loss) {
+    if (!ctx || !samples || !params || !grad || !loss || n < 1) return BSN_ERR_ARG;
+    bsn_status st;
+    double* dl = (double*)slot(ctx, SLOT_RED, 64, &st); BSN_TRY(st);
+    BSN_CUDA(ctx, cudaMemsetAsync(dl, 0, 8, ctx->stream));
+    BSN_CUDA(ctx, cudaMemsetAsync(grad, 0, sizeof(float) * NPARAM, ctx->stream));
+    BSN_CUDA(ctx, cudaFuncSetAttribute(train_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem()));
+    train_grad_kernel<<<grid1d(n, TB), TB, train_smem(), ctx->stream>>>(samples, n, params, grad, dl, 0ull, 0, 0, 0);
+    BSN_TRY(launch_check(ctx, "train_grad_kernel"));
+    BSN_CUDA(ctx, cudaMemcpyAsync(loss, dl, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return BSN_OK;
+}
+
+// Adam on mini-batches drawn uniformly (with replacement) from the samples,
+// learning rate decayed from lr to 0 along a cosine over the steps.
+extern "C" bsn_status bsn_learned_train(bsn_ctx* ctx, const float* samples, long long n, float* params, int steps,
+                                        int batch, float lr, unsigned long long seed, double* last_loss) {
+    if (!ctx || !samples || !params || n < 1 || steps < 0 || batch < TB || batch % TB)
+        return set_err(ctx, BSN_ERR_ARG, "bad arguments to bsn_learned_train (batch must be a multiple of %d)", TB);
+    bsn_status st;
+    float* buf = (float*)slot(ctx, SLOT_UN, sizeof(float) * 3 * NPARAM + 64, &st); BSN_TRY(st);
+    float *grad = buf, *m = buf + NPARAM, *v = buf + 2 * NPARAM;
+    double* dl = (double*)slot(ctx, SLOT_RED, 64, &st); BSN_TRY(st);
+    BSN_CUDA(ctx, cudaMemsetAsync(buf, 0, sizeof(float) * 3 * NPARAM, ctx->stream));
+    BSN_CUDA(ctx, cudaFuncSetAttribute(train_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem()));
+    const float b1 = 0.9f, b2 = 0.999f;
+    double bc1 = 1.0, bc2 = 1.0;
+    for (int s = 0; s < steps; ++s) {
+        bool last = s == steps - 1;
+        if (last) BSN_CUDA(ctx, cudaMemsetAsync(dl, 0, 8, ctx->stream));
+        train_grad_kernel<<<batch / TB, TB, train_smem(), ctx->stream>>>(samples, n, params, grad, dl, seed, s, 0, 1);
+        BSN_TRY(launch_check(ctx, "train_grad_kernel"));
+        bc1 *= b1; bc2 *= b2;
+        float lr_s = (float)(0.5 * lr * (1.0 + std::cos(3.14159265358979323846 * (double)s / (double)steps)));
+        adam_kernel<<<(NPARAM + 255) / 256, 256, 0, ctx->stream>>>(params, grad, m, v, 1.0f / (float)batch, lr_s, b1,
+                                                                    b2, 1e-8f, (float)(1.0 - bc1), (float)(1.0 - bc2));
+        BSN_TRY(launch_check(ctx, "adam_kernel"));
+    }
+    if (last_loss) {
+        double h = 0.0;
+        BSN_CUDA(ctx, cudaMemcpyAsync(&h, dl, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        *last_loss = steps > 0 ? h / (double)batch : 0.0;
+    }
+    return BSN_OK;
+}
+
+// params_left/right: device FP32 parameters; packed to BF16 for the tensor cores
+extern "C" bsn_status bsn_learned_set_params(bsn_ctx* ctx, const float* params_left, const float* params_right) {
+    if (!ctx || !params_left || !params_right) return BSN_ERR_ARG;
+    if (!ctx->learned_state) ctx->learned_state = new learned::State();
+    learned::State* S = (learned::State*)ctx->learned_state;
+    if (!S->packed) BSN_CUDA(ctx, cudaMalloc(&S->packed, 2 * PK_BYTES));
+    pack_kernel<<<4, 256, 0, ctx->stream>>>(params_left, S->packed);
+    BSN_TRY(launch_check(ctx, "pack_kernel"));
+    pack_kernel<<<4, 256, 0, ctx->stream>>>(params_right, S->packed + PK_BYTES);
+    BSN_TRY(launch_check(ctx, "pack_kernel"));
+    S->ready = true;
+    return BSN_OK;
+}
+
+extern "C" bsn_status bsn_learned_eval(bsn_ctx* ctx, const float* u, long long n, const float* params, float* w,
+                                       int tensor_cores) {
+    if (!ctx || !u || !params || !w || n < 0) return BSN_ERR_ARG;
+    bsn_status st;
+    unsigned char* pk = (unsigned char*)slot(ctx, SLOT_PHI2, PK_BYTES, &st); BSN_TRY(st);
+    pack_kernel<<<4, 256, 0, ctx->stream>>>(params, pk);
+    BSN_TRY(launch_check(ctx, "pack_kernel"));
+    eval_kernel<<<grid1d(n, 128), 128, 0, ctx->stream>>>(u, n, params, pk, w, tensor_cores);
+    return launch_check(ctx, "eval_kernel");
+}

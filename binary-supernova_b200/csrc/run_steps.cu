@@ -114,7 +114,8 @@ static bsn_status check_step_args(bsn_ctx* ctx, double* U, int nx, int ny, int n
     if (bc != BSN_BC_OUTFLOW && bc != BSN_BC_PERIODIC) return set_err(ctx, BSN_ERR_ARG, "bad bc %d", bc);
     if (bc == BSN_BC_PERIODIC && (nx < BSN_NG || ny < BSN_NG || nz < BSN_NG))
         return set_err(ctx, BSN_ERR_ARG, "periodic boundaries need n >= 3 per axis");
-    if (prec != PREC_F64 && prec != PREC_F32) return set_err(ctx, BSN_ERR_ARG, "bad precision %d", prec);
+    if (prec != PREC_F64 && prec != PREC_F32 && prec != PREC_LEARNED)
+        return set_err(ctx, BSN_ERR_ARG, "bad precision %d", prec);
     return BSN_OK;
 }
 
@@ -125,6 +126,15 @@ extern "C" bsn_status bsn_euler3d_step_f32(bsn_ctx* ctx, double* U, int nx, int 
     f64::StageArgs A;
     stage_args_init(A, nx, ny, nz, dx, dy, dz, gamma, bc, rho_floor, P_floor);
     return rk3_prec(ctx, A, U, dt, PREC_F32);
+}
+
+extern "C" bsn_status bsn_euler3d_step_learned(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double dx,
+                                               double dy, double dz, double dt, double gamma, int bc,
+                                               double rho_floor, double P_floor) {
+    BSN_TRY(check_step_args(ctx, U, nx, ny, nz, bc, PREC_LEARNED));
+    f64::StageArgs A;
+    stage_args_init(A, nx, ny, nz, dx, dy, dz, gamma, bc, rho_floor, P_floor);
+    return rk3_prec(ctx, A, U, dt, PREC_LEARNED);
 }
 
 extern "C" bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double dx, double dy, double dz,

@@ -61,6 +61,7 @@ struct StageArgs {
     unsigned int* cfl_nan;
     const double* dt_dev;    // non-null: dt read on the device (graph-captured time loop)
     const int* done_dev;     // non-null and *done_dev != 0: the device time loop has finished
+    const void* mlp;         // learned stencil path: packed network parameters
 };
 
 

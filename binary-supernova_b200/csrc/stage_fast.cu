@@ -12,6 +12,9 @@ namespace tile {
 struct F32Physics {
     using real = float;
     static constexpr bool kCenterFromSmem = false;  // smem holds FP32 copies: reload FP64 state
+    static constexpr bool kWarpFaces = false;
+    static constexpr int kExtraSmem(int) { return 0; }
+    __device__ static void prologue(unsigned char*, const f64::StageArgs&, int) {}
     struct Consts { float g, gm1, inv_gm1, gg; };
     __device__ static Consts consts(const f64::StageArgs& A) {
         float g = (float)A.g;

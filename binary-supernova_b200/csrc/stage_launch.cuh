@@ -6,7 +6,7 @@
 
 namespace bsn {
 
-enum Precision { PREC_F64 = 0, PREC_F32 = 1 };
+enum Precision { PREC_F64 = 0, PREC_F32 = 1, PREC_LEARNED = 2 };
 
 struct TileVariant {
     int tx, ty, tz, nt;
@@ -19,6 +19,9 @@ bsn_status f64_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A);
 int f32_variant_count();
 TileVariant f32_variant(int idx);
 bsn_status f32_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A);
+int learned_variant_count();
+TileVariant learned_variant(int idx);
+bsn_status learned_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A);
 
 // Launch one stage with the tile chosen for (precision, nx, ny, nz); the
 // first call for a grid runs the autotuner unless a tile was forced.

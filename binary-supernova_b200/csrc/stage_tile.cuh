@@ -34,6 +34,9 @@ struct Shape {
 struct F64Physics {
     using real = double;
     static constexpr bool kCenterFromSmem = true;   // smem holds the floored FP64 state
+    static constexpr bool kWarpFaces = false;       // faces computed thread by thread
+    static constexpr int kExtraSmem(int) { return 0; }
+    __device__ static void prologue(unsigned char*, const f64::StageArgs&, int) {}
     struct Consts { double g, gm1; };
     __device__ static Consts consts(const f64::StageArgs& A) { return {A.g, A.gm1}; }
     __device__ static double pressure(const double v[5], const Consts& k) {
@@ -73,7 +76,8 @@ __device__ __forceinline__ void load_cell(const f64::StageArgs& A, const Geom& G
 
 template <class P, int TX, int TY, int TZ, int NT, int D>
 __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::Consts& k, int a0, int b0, int c0,
-                      typename P::real* sC, typename P::real* sF, double (&acc)[Shape<TX, TY, TZ>::NCELL / NT][5]) {
+                      typename P::real* sC, typename P::real* sF, unsigned char* psm,
+                      double (&acc)[Shape<TX, TY, TZ>::NCELL / NT][5]) {
     using S = Shape<TX, TY, TZ>;
     using real = typename P::real;
     constexpr int CPT = S::NCELL / NT;
@@ -103,30 +107,15 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
     __syncthreads();
 
     constexpr int SD = (D == 0) ? 1 : (D == 1 ? LX : LX * LY);
-    for (int f = tid; f < NF; f += NT) {
-        int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
-        int fpos[3] = {fx, fy, fz};
-        bool valid = true;
-#pragma unroll
-        for (int t = 0; t < 3; ++t) {
-            int gpos = o[t] + fpos[t];
-            valid = valid && (t == D ? gpos <= n[t] : gpos < n[t]);
-        }
-        if (!valid) continue;
-        int base = fx + LX * (fy + LY * fz);
-        real c[6][6];
-#pragma unroll
-        for (int s = 0; s < 6; ++s)
-#pragma unroll
-            for (int q = 0; q < 6; ++q) c[s][q] = sC[q * S::NEXT + base + s * SD];
-        real F[5];
-        P::template flux<D>(c, k, F);
+    // one face: write it to smem and, if this tile owns it, to the optional
+    // flux arrays, coarse flux registers and fine boundary-face buffers
+    auto emit = [&](int f, int fx, int fy, int fz, const real (&F)[5]) {
 #pragma unroll
         for (int q = 0; q < 5; ++q) sF[q * S::NFACE + f] = F[q];
-
+        int fpos[3] = {fx, fy, fz};
         int gd = o[D] + fpos[D];
         bool owner = (fpos[D] < TD) || (gd == n[D]);
-        if (!owner) continue;
+        if (!owner) return;
         int ga = o[0] + fx, gb = o[1] + fy, gc = o[2] + fz;
         if (A.F[D]) {
             long long ex_ = (G.nx + 2 * BSN_NG) + (D == 0), ey_ = (G.ny + 2 * BSN_NG) + (D == 1);
@@ -159,6 +148,49 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
             double* dst = A.bnd.f[2 * D + (gd == 0 ? 0 : 1)];
 #pragma unroll
             for (int q = 0; q < 5; ++q) dst[roff + q] = (double)F[q];
+        }
+    };
+    auto face_valid = [&](int fx, int fy, int fz) {
+        int fpos[3] = {fx, fy, fz};
+        bool valid = true;
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            int gpos = o[t] + fpos[t];
+            valid = valid && (t == D ? gpos <= n[t] : gpos < n[t]);
+        }
+        return valid;
+    };
+    if constexpr (P::kWarpFaces) {
+        // warp-collective faces (tensor-core work inside the flux): every lane
+        // of a warp takes part in every iteration, valid face or not
+        const int warp = tid >> 5, lane = tid & 31;
+        for (int fb = warp * 32; fb < NF; fb += NT) {
+            int f = fb + lane;
+            int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
+            bool valid = f < NF && face_valid(fx, fy, fz);
+            real c[6][6];
+            int base = valid ? fx + LX * (fy + LY * fz) : 0;
+#pragma unroll
+            for (int s = 0; s < 6; ++s)
+#pragma unroll
+                for (int q = 0; q < 6; ++q) c[s][q] = valid ? sC[q * S::NEXT + base + s * SD] : (real)0;
+            real F[5];
+            P::template warp_flux<D>(c, valid, k, F, psm, warp);
+            if (valid) emit(f, fx, fy, fz, F);
+        }
+    } else {
+        for (int f = tid; f < NF; f += NT) {
+            int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
+            if (!face_valid(fx, fy, fz)) continue;
+            int base = fx + LX * (fy + LY * fz);
+            real c[6][6];
+#pragma unroll
+            for (int s = 0; s < 6; ++s)
+#pragma unroll
+                for (int q = 0; q < 6; ++q) c[s][q] = sC[q * S::NEXT + base + s * SD];
+            real F[5];
+            P::template flux<D>(c, k, F);
+            emit(f, fx, fy, fz, F);
         }
     }
     __syncthreads();
@@ -198,10 +230,12 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(f64::StageArgs A) {
     if (tid == 0) nanflag = 0;
     const typename P::Consts k = P::consts(A);
 
+    unsigned char* psm = smem_raw + ((sizeof(real) * (6 * S::NEXT + 5 * S::NFACE) + 15) / 16) * 16;
+    P::prologue(psm, A, NT);   // visible to all threads after the first sweep's barrier
     double acc[CPT][5];
-    sweep<P, TX, TY, TZ, NT, 0>(A, G, k, a0, b0, c0, sC, sF, acc);
-    sweep<P, TX, TY, TZ, NT, 1>(A, G, k, a0, b0, c0, sC, sF, acc);
-    sweep<P, TX, TY, TZ, NT, 2>(A, G, k, a0, b0, c0, sC, sF, acc);
+    sweep<P, TX, TY, TZ, NT, 0>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
+    sweep<P, TX, TY, TZ, NT, 1>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
+    sweep<P, TX, TY, TZ, NT, 2>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
 
     const double dt = A.dt_dev ? *A.dt_dev : A.dt;
     const double cdt = A.stage == 2 ? 0.25 * dt : (A.stage == 3 ? (2.0 / 3.0) * dt : dt);

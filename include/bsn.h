@@ -128,13 +128,20 @@ bsn_status bsn_cfl_dt_3d_f64_noalloc(bsn_ctx* ctx, const double* U, int nx, int 
  * they run the reference's driver loop, test/test_sedov.jl:45-52 /
  * scripts/run_production.jl:132-135, `dt = cfl_dt_3d; dt = min(dt, t_end-t);
  * euler3d_step!; t += dt`) ---------------------------------------------- */
-enum { BSN_PREC_F64 = 0,   /* stencils in FP64, bit-identical to the reference */
-       BSN_PREC_F32 = 1 }; /* stencils, fluxes and pressures in FP32; state, floors,
-                              divergence, sources and RK3 accumulation in FP64 */
+enum { BSN_PREC_F64 = 0,     /* stencils in FP64, bit-identical to the reference */
+       BSN_PREC_F32 = 1,     /* stencils, fluxes and pressures in FP32; state, floors,
+                                divergence, sources and RK3 accumulation in FP64 */
+       BSN_PREC_LEARNED = 2  /* as BSN_PREC_F32, with the WENO-Z weights of smooth
+                                stencils from the learned network (see below) */ };
 /* euler3d_step! with FP32 stencils (BSN_PREC_F32); same arguments. */
 bsn_status bsn_euler3d_step_f32(bsn_ctx* ctx, double* U, int nx, int ny, int nz,
                                 double dx, double dy, double dz, double dt, double gamma,
                                 int bc, double rho_floor, double P_floor);
+/* euler3d_step! with the learned WENO weights (BSN_PREC_LEARNED); needs
+ * bsn_learned_set_params first. */
+bsn_status bsn_euler3d_step_learned(bsn_ctx* ctx, double* U, int nx, int ny, int nz,
+                                    double dx, double dy, double dz, double dt, double gamma,
+                                    int bc, double rho_floor, double P_floor);
 /* Up to n_steps CFL-limited SSP-RK3 steps with dt, t and the CFL maximum kept
  * on the device (one CUDA graph per step).  t_end > 0 stops at t_end exactly
  * as the reference loop; t_end <= 0 runs n_steps.  *t_inout: start time in,
@@ -150,6 +157,42 @@ bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double
 int        bsn_tile_variant_count(int precision);
 bsn_status bsn_ctx_set_tile(bsn_ctx* ctx, int precision, int variant);
 bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int ny, int nz, int out[4]);
+
+/* ---- learned WENO weights (no counterpart in the reference; plain WENO5-Z of
+ * src/weno5.jl:14-61 is its judge).  Two networks, for the left- and the
+ * right-biased reconstruction, each 5 -> 32 -> 32 -> 3 (ReLU, softmax), map
+ * a normalised 5-point stencil u_i = (v_i - v_c)/max|v_j - v_c| to the three
+ * weights.  A reconstruction uses the network only where the smoothness
+ * indicators of u say the stencil is smooth (tau5 <= 4 (min beta + 1e-3));
+ * elsewhere plain WENO5-Z.  Parameters: FP32, bsn_learned_param_count()
+ * floats per network, layout W1[32][5] b1[32] W2[32][32] b2[32] W3[3][32] b3[3].
+ * All arrays below are device memory. */
+int        bsn_learned_param_count(void);
+/* Training samples from a state: for every interface and field (rho, m, P),
+ * the normalised left/right stencils and their FP64 WENO-Z weights, smooth
+ * stencils only, and only those whose spread max|v_i - v_c| exceeds both
+ * 1e-15 and 1e-12 |v_c| (below that any weights reconstruct to rounding
+ * level), each kept with probability 1/stride.  Samples are 8 floats
+ * (u[5], omega[3]) appended at counts[side] (in: current, out: new) up to cap. */
+bsn_status bsn_learned_collect(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, int bc,
+                               double gamma, int stride, unsigned long long seed,
+                               float* out_left, float* out_right, long long cap, long long counts[2]);
+/* Mean-squared-error gradient of one network over all n samples (sum over
+ * samples; *loss = summed squared error), by the training kernels. */
+bsn_status bsn_learned_grad(bsn_ctx* ctx, const float* samples, long long n, const float* params,
+                            float* grad, double* loss);
+/* Adam on mini-batches of `batch` samples (multiple of 128) drawn uniformly
+ * with replacement, learning rate decayed from lr to 0 on a cosine; params
+ * updated in place; *last_loss = mean squared error of the last batch. */
+bsn_status bsn_learned_train(bsn_ctx* ctx, const float* samples, long long n, float* params, int steps,
+                             int batch, float lr, unsigned long long seed, double* last_loss);
+/* Install trained parameters for BSN_PREC_LEARNED (packed to BF16 for the
+ * tensor cores; FP32 biases). */
+bsn_status bsn_learned_set_params(bsn_ctx* ctx, const float* params_left, const float* params_right);
+/* Weights of n normalised stencils u[n][5] -> w[n][3]: tensor_cores = 0 runs
+ * the FP32 training arithmetic, 1 the BF16 mma path of the stencil kernel. */
+bsn_status bsn_learned_eval(bsn_ctx* ctx, const float* u, long long n, const float* params, float* w,
+                            int tensor_cores);
 
 /* ---- src/gravity_bh.jl, src/sinks.jl ------------------------------------ */
 /* add_bh_gravity_source! (src/gravity_bh.jl:58-78; src/gpu_kernels.jl:199-230) */
