@@ -6,7 +6,8 @@ floors rho 1e-6 / P 1e-6.  A step is one CFL dt reduction plus one full RK3
 step, the loop the reference drivers run (cfl_dt_3d + euler3d_step!).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bsn|reference]
-                  [--n 256] [--path f32|f64] [--tile V] [--no-cpu]
+                  [--n 256] [--path learned|f32|f64] [--tile V] [--no-cpu]
+                  [--no-accuracy]
 
 `value` is device-resident throughput over K steps (state in HBM).  `e2e`
 runs the same step through the public host-buffer path: the state is copied
@@ -33,6 +34,16 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 NG = 3
 GAMMA = 5.0 / 3.0
 CFL = 0.4
+T_MID = 0.025     # start of the timed steps (Sedov run to t = 0.05)
+T_END = 0.05
+
+
+_T0 = time.time()
+
+
+def log(msg):
+    """Progress on stderr (the JSON line is the only stdout output)."""
+    print(f"[bench {time.time() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
 def peaks():
@@ -57,7 +68,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -96,33 +107,45 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def sedov_host(n):
-    """Sedov initial state (src/euler3d.jl:275-316) on the host, F-ordered."""
-    import oracle
+def sedov_host(n, cpu_leg=False):
+    """Sedov initial state (src/euler3d.jl:275-316) on the host, F-ordered:
+    from the package's IC generator, or, for the CPU reference leg (which
+    must not touch the package), from the oracle's (bit-identical)."""
+    import numpy as np
     L = 1.0
     dx = 2 * L / n
-    U = oracle.state(n, n, n)
-    oracle.sedov_ic_3d(U, dx, dx, dx, GAMMA, E_blast=1.0, r_inject=3.5 * dx, rho_bg=1.0, P_floor=1e-5,
-                       x_offset=-L, y_offset=-L, z_offset=-L)
+    kw = dict(E_blast=1.0, r_inject=3.5 * dx, rho_bg=1.0, P_floor=1e-5, x_offset=-L, y_offset=-L, z_offset=-L)
+    if cpu_leg:
+        import oracle
+        U = oracle.state(n, n, n)
+        oracle.sedov_ic_3d(U, dx, dx, dx, GAMMA, **kw)
+        return U, dx
+    from bsn import ics
+    U = np.zeros((5, n + 2 * NG, n + 2 * NG, n + 2 * NG), dtype=np.float64, order="F")
+    ics.sedov_ic_3d(U, n, n, n, dx, dx, dx, GAMMA, **kw)
     return U, dx
 
 
-def cpu_reference_rate(n, threads, nz_sample, steps):
+def cpu_reference_rate(n, threads, nz_sample, steps, min_seconds=0.0, max_steps=64):
     """Oracle (CPU restatement of the reference path) on a z-slab sample of
-    the Sedov n^3 workload: cell-updates/s with `threads` OpenMP threads."""
+    the Sedov n^3 workload: cell-updates/s with `threads` OpenMP threads,
+    over `steps` RK3 steps, continued until `min_seconds` have elapsed (at
+    most `max_steps`).  Returns (rate, seconds, steps)."""
     import numpy as np
     import oracle
     oracle.build()
     oracle.set_threads(threads)
-    U, dx = sedov_host(n)
+    U, dx = sedov_host(n, cpu_leg=True)
     k0 = NG + n // 2 - nz_sample // 2
     S = np.asfortranarray(U[:, :, :, k0 - NG:k0 + nz_sample + NG])
     t0 = time.perf_counter()
-    for _ in range(steps):
+    k = 0
+    while k < steps or (time.perf_counter() - t0 < min_seconds and k < max_steps):
         dt = oracle.cfl_dt_3d(S, dx, dx, dx, GAMMA, CFL)
         oracle.euler3d_step(S, dx, dx, dx, dt, GAMMA, rho_floor=1e-6, P_floor=1e-6)
+        k += 1
     el = time.perf_counter() - t0
-    return n * n * nz_sample * steps / el, el
+    return n * n * nz_sample * k / el, el, k
 
 
 def run_reference(args, rank, world):
@@ -132,7 +155,7 @@ def run_reference(args, rank, world):
     nz = max(4, min(args.n, int(os.environ.get("BSN_REF_SLAB", "16"))))
     for _ in range(args.warmup):
         cpu_reference_rate(args.n, threads, nz, 1)
-    rate, el = cpu_reference_rate(args.n, threads, nz, args.steps)
+    rate, el, _ = cpu_reference_rate(args.n, threads, nz, args.steps)
     line = {
         "impl": "reference", "metric": "cell-updates/s per RK3 step (Sedov 3D, FP64)", "value": rate,
         "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -147,6 +170,49 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def accuracy(bsn, torch, U0, n, dx, kw, t_end=T_END):
+    """Sedov n^3 from the initial state to t_end on each path (device-resident
+    CFL loop): L1 density / energy differences against the FP64 path and L1
+    density error against the Sedov-Taylor similarity solution for the
+    deposited energy (sedov_ic_3d! deposits E_blast (gamma-1))."""
+    import numpy as np
+    from bsn.analytic import sedov_taylor
+    a = (slice(NG, NG + n),) * 3
+    E_bg = 1e-5 / (GAMMA - 1)
+    E_dep = float((U0[(4,) + a] - E_bg).sum() * dx ** 3)
+    xc = (np.arange(1, n + 1) - 0.5) * dx - 1.0
+    r = np.sqrt(xc[:, None, None] ** 2 + xc[None, :, None] ** 2 + xc[None, None, :] ** 2)
+    rho_ex = sedov_taylor(r, t_end, E=E_dep, rho0=1.0, gamma=GAMMA)[0]
+    out = {"t_end": t_end, "E_deposited": E_dep}
+    fields = {}
+    for p_ in ("f64", "f32", "learned"):
+        U = torch.from_numpy(U0).cuda()
+        bsn.run_steps(U, n, n, n, dx, dx, dx, GAMMA, CFL, n_steps=1, precision=p_, **kw)   # autotune, graph
+        U = torch.from_numpy(U0).cuda()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        t, k = bsn.run_steps(U, n, n, n, dx, dx, dx, GAMMA, CFL, n_steps=1_000_000, t_end=t_end, precision=p_,
+                             **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"{p_}_run_cell_updates_per_s"] = n ** 3 * k / (e0.elapsed_time(e1) / 1e3)
+        log(f"accuracy run {p_}: {k} steps to t={t:.4g} in {e0.elapsed_time(e1) / 1e3:.1f} s")
+        h = U.cpu().numpy()
+        fields[p_] = (h[(0,) + a].copy(), h[(4,) + a].copy())
+        out[f"{p_}_steps"] = k
+        del U, h
+    r64, e64 = fields["f64"]
+    for p_, (rh, en) in fields.items():
+        out[f"l1_rho_vs_exact_{p_}"] = float(np.abs(rh - rho_ex).sum() / rho_ex.sum())
+        if p_ != "f64":
+            out[f"l1_rho_vs_f64_{p_}"] = float(np.abs(rh - r64).sum() / np.abs(r64).sum())
+            out[f"l1_E_vs_f64_{p_}"] = float(np.abs(en - e64).sum() / np.abs(e64).sum())
+    for p_ in ("f32", "learned"):
+        out[f"exact_error_ratio_{p_}_over_f64"] = out[f"l1_rho_vs_exact_{p_}"] / out["l1_rho_vs_exact_f64"]
+    return out
+
+
 def run_bsn(args, rank, world):
     import numpy as np
     import torch
@@ -159,17 +225,26 @@ def run_bsn(args, rank, world):
         import torch.distributed as dist
     n = args.n
     U0, dx = sedov_host(n)
+    log(f"Sedov {n}^3 initial state built")
     ncell = n ** 3
     kw = dict(rho_floor=1e-6, P_floor=1e-6)
-    Ud = torch.from_numpy(U0).cuda()
 
-    def steps(U, k, prec, t=0.0):
-        return bsn.run_steps(U, n, n, n, dx, dx, dx, GAMMA, CFL, n_steps=k, t=t, precision=prec, **kw)
+    def steps(U, k, prec, t=0.0, t_end=0.0):
+        return bsn.run_steps(U, n, n, n, dx, dx, dx, GAMMA, CFL, n_steps=k, t=t, t_end=t_end, precision=prec,
+                             **kw)
+
+    # the timed steps start from the blast half-way to t = 0.05 (FP64 run),
+    # so every path sees the mix of quiescent, smooth and shocked stencils of
+    # the run rather than the nearly empty initial grid
+    Ud = torch.from_numpy(U0).cuda()
+    t_mid, k_mid = steps(Ud, 1_000_000, "f64", 0.0, T_MID)
+    log(f"FP64 run to t={t_mid:.4g}: {k_mid} steps")
+    U_mid = Ud.cpu().numpy()
 
     def timed(prec, k):
         """K device-resident RK3 steps (dt on the device, one graph per step)."""
-        U = torch.from_numpy(U0).cuda()
-        t, _ = steps(U, args.warmup, prec)
+        U = Ud.clone()
+        t, _ = steps(U, args.warmup, prec, t_mid)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
@@ -188,21 +263,27 @@ def run_bsn(args, rank, world):
         return ms, bsn.launch_count() - l0
 
     prec = args.path
-    other = "f64" if prec == "f32" else "f32"
+    others = [p_ for p_ in ("learned", "f32", "f64") if p_ != prec]
+    if "learned" in (prec,) + tuple(others):
+        from bsn import learned as LW
+        LW.install(*LW.load_params())
     if args.tile >= 0:
-        for p_ in ("f32", "f64"):
+        for p_ in ("f32", "f64", "learned"):
             bsn.set_tile(p_, min(args.tile, bsn.tile_variants(p_) - 1))
     with ClockSampler(local) as clk:
         ms, launches = timed(prec, args.steps)
-    ms_other, _ = timed(other, args.steps)
+    log(f"{prec}: {ms / args.steps:.3f} ms/step")
+    ms_other = {}
+    for p_ in others:
+        ms_other[p_] = timed(p_, args.steps)[0]
+        log(f"{p_}: {ms_other[p_] / args.steps:.3f} ms/step")
     value = world * ncell * args.steps / (ms / 1e3)
-    value_other = world * ncell * args.steps / (ms_other / 1e3)
 
     # roofline of the dominant kernel: stage-kernel launches timed with CUDA
     # events around each launch (per-step entry point, same kernels)
-    kname = "stage_kernel_f32" if prec == "f32" else "stage_kernel"
-    step_fn = bsn.euler3d_step_f32 if prec == "f32" else bsn.euler3d_step
-    Up = torch.from_numpy(U0).cuda()
+    kname = {"f32": "stage_kernel_f32", "f64": "stage_kernel", "learned": "stage_kernel_learned"}[prec]
+    step_fn = {"f32": bsn.euler3d_step_f32, "f64": bsn.euler3d_step, "learned": bsn.euler3d_step_learned}[prec]
+    Up = Ud.clone()
     dt0 = bsn.cfl_dt_3d(Up, n, n, n, dx, dx, dx, GAMMA, CFL)
     step_fn(Up, n, n, n, dx, dx, dx, dt0, GAMMA, **kw)
     bsn.set_profiling(True)
@@ -217,14 +298,17 @@ def run_bsn(args, rank, world):
     tile = bsn.get_tile(n, n, n, prec)
     del Up
 
+    log(f"roofline: {kname} {t_stage * 1e3:.3f} ms per launch")
+    acc = accuracy(bsn, torch, U0, n, dx, kw) if not args.no_accuracy else None
+
     # e2e: host-buffer path -- pinned host state -> device, one CFL-limited
     # RK3 step through the public entry point, device -> host, every step
-    Uh = torch.from_numpy(U0.copy(order="F")).pin_memory()
+    Uh = torch.from_numpy(U_mid.copy(order="F")).pin_memory()
     Ue = torch.empty_like(Ud)
     nbytes = Uh.numel() * 8
     for _ in range(2):
         Ue.copy_(Uh, non_blocking=True)
-        steps(Ue, 1, prec)
+        steps(Ue, 1, prec, t_mid)
         Uh.copy_(Ue, non_blocking=True)
     torch.cuda.synchronize()
     if dist:
@@ -234,7 +318,7 @@ def run_bsn(args, rank, world):
     e0.record()
     for _ in range(k_e2e):
         Ue.copy_(Uh, non_blocking=True)
-        steps(Ue, 1, prec)
+        steps(Ue, 1, prec, t_mid)
         Uh.copy_(Ue, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
@@ -248,24 +332,33 @@ def run_bsn(args, rank, world):
     cpu = None
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        nz = 16
-        rate, el = cpu_reference_rate(n, threads, nz, 2)
+        nz = min(n, 32)
+        rate, el, k = cpu_reference_rate(n, threads, nz, 1, min_seconds=12.0)
         cpu = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-               "sample": f"2 RK3 steps (oracle, FP64) of a {n}x{n}x{nz} z-slab of Sedov {n}^3, {el:.1f} s"}
+               "sample": f"{k} RK3 steps (oracle, FP64) of a {n}x{n}x{nz} z-slab of Sedov {n}^3, {el:.1f} s"}
     if rank == 0:
         desc = {"f32": "FP32 stencils/fluxes, FP64 state and RK3 accumulation",
-                "f64": "FP64, bit-identical to the reference CPU path"}
+                "f64": "FP64, bit-identical to the reference CPU path",
+                "learned": "FP32 stencils/fluxes with learned WENO weights (BF16 tensor-core MLP, WENO5-Z "
+                           "fallback at flagged stencils), FP64 state and RK3 accumulation"}
+        compare = {}
+        for p_, m_ in ms_other.items():
+            v_ = world * ncell * args.steps / (m_ / 1e3)
+            compare[f"{p_}_value"] = v_
+            compare[f"{p_}_ms_per_step"] = m_ / args.steps
+            compare[f"speedup_vs_{p_}"] = value / v_
         line = {
             "metric": "cell-updates/s per RK3 step (Sedov 3D, WENO5-Z+HLLC+SSP-RK3)",
             "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if prec == "f32" else "f64", "data": "synthetic (Sedov initial condition, sedov_ic_3d!)",
+            "dtype": "f64" if prec == "f64" else ("f32+bf16" if prec == "learned" else "f32"), "data": "synthetic (Sedov initial condition, sedov_ic_3d!)",
             "config": {"workload": f"sedov{n}^3", "grid": [n, n, n], "path": desc[prec],
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "tile": list(tile), "time_loop": "device-resident dt, one CUDA graph per step",
+                       "timed_from": f"Sedov state at t={T_MID} (FP64 run from the initial condition)",
                        "l2": f"state {Ud.numel() * 8 / 1e6:.0f} MB per array > 126 MB L2 (no flush needed)"},
-            "compare": {f"{other}_value": value_other, f"{other}_ms_per_step": ms_other / args.steps,
-                        f"speedup_vs_{other}": value / value_other},
+            "compare": compare,
+            "accuracy": acc,
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_kind": hbm_kind,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": t_stage * 1e3,
@@ -287,8 +380,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="bsn", choices=["bsn", "reference"])
     ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--path", default="f32", choices=["f32", "f64"],
-                    help="stencil precision of the timed path (the other is reported beside it)")
+    ap.add_argument("--path", default="learned", choices=["learned", "f32", "f64"],
+                    help="stencil path of the headline (the others are timed beside it)")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the Sedov-to-t=0.05 accuracy runs of the three paths")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--tile", type=int, default=-1,
                     help="force this stage-kernel tile variant for both precisions (default: autotune)")

@@ -378,7 +378,7 @@ def set_tile(precision="f64", variant=-1):
 
 
 def get_tile(nx, ny, nz, precision="f64"):
-    out = (C.c_int * 4)()
+    out = (C.c_int * 5)()
     _call("bsn_ctx_get_tile", context(), PREC[precision], nx, ny, nz, out)
     return tuple(out)
 

@@ -50,11 +50,15 @@ class SampleBuffers:
               C.c_ulonglong(seed), _fptr(self.L), _fptr(self.R), C.c_longlong(self.cap), self.counts)
         return tuple(self.counts)
 
+    @property
+    def stored(self):
+        return min(self.counts[0], self.cap), min(self.counts[1], self.cap)
+
     def left(self):
-        return self.L[: self.counts[0]]
+        return self.L[: self.stored[0]]
 
     def right(self):
-        return self.R[: self.counts[1]]
+        return self.R[: self.stored[1]]
 
 
 IDEAL = {0: (0.1, 0.6, 0.3), 1: (0.3, 0.6, 0.1)}   # linear weights of src/weno5.jl:37,57

@@ -109,13 +109,13 @@ extern "C" bsn_status bsn_ctx_set_tile(bsn_ctx* ctx, int precision, int variant)
     return BSN_OK;
 }
 
-extern "C" bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int ny, int nz, int out[4]) {
+extern "C" bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int ny, int nz, int out[5]) {
     if (!ctx || !out) return BSN_ERR_ARG;
     auto it = ctx->tile_choice.find(std::make_tuple(precision, nx, ny, nz));
     if (it == ctx->tile_choice.end()) return set_err(ctx, BSN_ERR_ARG, "no tile chosen yet for this grid");
     if (!prec_ok(precision)) return set_err(ctx, BSN_ERR_ARG, "bad precision %d", precision);
     TileVariant v = variant(precision, it->second);
-    out[0] = v.tx; out[1] = v.ty; out[2] = v.tz; out[3] = v.nt;
+    out[0] = v.tx; out[1] = v.ty; out[2] = v.tz; out[3] = v.nt; out[4] = v.minb;
     return BSN_OK;
 }
 

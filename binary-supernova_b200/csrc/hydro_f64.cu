@@ -174,7 +174,7 @@ void stage_args_init(StageArgs& A, int nx, int ny, int nz, double dx, double dy,
 // every interface and every cell is computed by the same arithmetic whatever
 // the tiling).  MINB keeps two 256-thread CTAs (or the equivalent) per SM.
 namespace {
-const TileVariant kF64Variants[] = {{8, 8, 8, 256}, {8, 8, 4, 128}, {16, 8, 4, 256}, {16, 8, 8, 512}};
+const TileVariant kF64Variants[] = {{8, 8, 8, 256, 2}, {8, 8, 4, 128, 4}, {16, 8, 4, 256, 2}, {16, 8, 8, 512, 1}};
 
 template <int TX, int TY, int TZ, int NT, int MINB>
 bsn_status launch_f64(bsn_ctx* ctx, const StageArgs& A) {

@@ -99,7 +99,7 @@ __global__ void collect_kernel(const double* U, int nx, int ny, int nz, int bc, 
         // is noise: no information.  Constant stencils are among them.
         double cen = side == 0 ? s5[2] : s5[1], spread = 0.0;
         for (int i = 0; i < 5; ++i) spread = fmax(spread, fabs(s5[i] - cen));
-        if (!(spread > 1e-15 && spread > 1e-12 * fabs(cen))) continue;
+        if (!(spread > (double)SPREAD_ABS && spread > SPREAD_REL_F64 * fabs(cen))) continue;
         double w[3];
         wenoz_weights64(s5, side, w);
         unsigned long long idx = atomicAdd(&count[side], 1ull);
@@ -267,9 +267,18 @@ __device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+__device__ __forceinline__ void mma1688(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(b0));
+}
+
 // Warp-collective MLP over `ntiles` tiles of 16 rows.  rows: BF16 inputs,
-// 16 per row (5 used), 32 B per row.  Logits of row r are written to
-// out[4*r .. 4*r+2] (may alias rows of tiles already consumed).
+// 8 per row (5 used, the rest zero), 16 B per row; the first layer is one
+// k = 8 MMA per 8 outputs.  Logits of row r are written to out[4*r .. 4*r+2];
+// out may alias rows (a tile's rows are in registers before its logits are
+// stored, and tile t's logits land below tile t+1's rows).
 __device__ void mlp_tiles(const unsigned char* pk, const uint32_t* rows, float* out, int ntiles) {
     const int lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
     const uint32_t* W1 = (const uint32_t*)(pk + PK_W1);   // row n: 8 words
@@ -280,15 +289,15 @@ __device__ void mlp_tiles(const unsigned char* pk, const uint32_t* rows, float* 
     const float* B3 = (const float*)(pk + PK_B3);
     for (int tile = 0; tile < ntiles; ++tile) {
         int r0 = tile * 16 + g, r1 = r0 + 8;
-        uint32_t a[4] = {rows[r0 * 8 + tg], rows[r1 * 8 + tg], rows[r0 * 8 + 4 + tg], rows[r1 * 8 + 4 + tg]};
+        const uint32_t a0 = rows[r0 * 4 + tg], a1 = rows[r1 * 4 + tg];
         __syncwarp();
-        // layer 1: 16 -> 32
+        // layer 1: 8 (5 used) -> 32
         float h[4][4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             float c0 = B1[8 * j + 2 * tg], c1 = B1[8 * j + 2 * tg + 1];
             h[j][0] = c0; h[j][1] = c1; h[j][2] = c0; h[j][3] = c1;
-            mma16816(h[j], a, W1[(8 * j + g) * 8 + tg], W1[(8 * j + g) * 8 + 4 + tg]);
+            mma1688(h[j], a0, a1, W1[(8 * j + g) * 8 + tg]);
         }
         uint32_t a2[2][4];
 #pragma unroll
@@ -361,7 +370,7 @@ __device__ void mlp_fp32(const float* P, const float u[5], float w[3]) {
 // Standalone evaluation of n normalised stencils: tc = 0 FP32 CUDA cores,
 // tc = 1 the BF16 tensor-core path of the stencil kernel.
 __global__ void eval_kernel(const float* u, long long n, const float* P, const unsigned char* pk, float* w, int tc) {
-    __shared__ __align__(16) uint32_t rows[4][32 * 8];     // 32 rows per warp
+    __shared__ __align__(16) uint32_t rows[4][32 * 4];     // 32 rows per warp
     __shared__ __align__(16) unsigned char spk[PK_BYTES];
     __shared__ float logits[4][32 * 4];
     for (int i = threadIdx.x; i < PK_BYTES; i += blockDim.x) spk[i] = pk[i];
@@ -375,10 +384,10 @@ __global__ void eval_kernel(const float* u, long long n, const float* P, const u
         return;
     }
     uint32_t* R = rows[warp];
-    R[lane * 8 + 0] = pack2(x[0], x[1]);
-    R[lane * 8 + 1] = pack2(x[2], x[3]);
-    R[lane * 8 + 2] = pack2(x[4], 0.f);
-    for (int k = 3; k < 8; ++k) R[lane * 8 + k] = 0u;
+    R[lane * 4 + 0] = pack2(x[0], x[1]);
+    R[lane * 4 + 1] = pack2(x[2], x[3]);
+    R[lane * 4 + 2] = pack2(x[4], 0.f);
+    R[lane * 4 + 3] = 0u;
     __syncwarp();
     mlp_tiles(spk, R, logits[warp], 2);
     if (i < n) { float o[3]; softmax3(&logits[warp][4 * lane], o); for (int k = 0; k < 3; ++k) w[i * 3 + k] = o[k]; }
@@ -400,8 +409,8 @@ struct F32Learned {
     using real = float;
     static constexpr bool kCenterFromSmem = false;
     static constexpr bool kWarpFaces = true;
-    // packed parameters of both sides + per-warp row buffers (160 rows x 32 B)
-    static constexpr int kExtraSmem(int nt) { return 2 * learned::PK_BYTES + (nt / 32) * 160 * 32; }
+    // packed parameters of both sides + per-warp row buffers (160 rows x 16 B)
+    static constexpr int kExtraSmem(int nt) { return 2 * learned::PK_BYTES + (nt / 32) * 160 * 16; }
     struct Consts { float g, gm1, inv_gm1, gg; };
     __device__ static Consts consts(const f64::StageArgs& A) {
         float g = (float)A.g;
@@ -414,84 +423,11 @@ struct F32Learned {
         const unsigned char* src = (const unsigned char*)A.mlp;
         for (int i = threadIdx.x; i < 2 * learned::PK_BYTES; i += nt) psm[i] = src[i];
     }
-    // WENO weights of one reconstruction in FP32 (plain WENO5-Z)
-    __device__ static void wenoz_w(const float s[5], int side, float w[3]) {
-        const float k = 13.0f / 12.0f;
-        float b0, b1, b2, d0, d1, d2;
-        if (side == 0) {
-            float x = s[0] - 2.f * s[1] + s[2], y = s[0] - 4.f * s[1] + 3.f * s[2];
-            b0 = fmaf(k * x, x, 0.25f * y * y);
-            x = s[1] - 2.f * s[2] + s[3]; y = s[1] - s[3];
-            b1 = fmaf(k * x, x, 0.25f * y * y);
-            x = s[2] - 2.f * s[3] + s[4]; y = 3.f * s[2] - 4.f * s[3] + s[4];
-            b2 = fmaf(k * x, x, 0.25f * y * y);
-            d0 = 0.1f; d1 = 0.6f; d2 = 0.3f;
-        } else {
-            float x = s[0] - 2.f * s[1] + s[2], y = s[0] - s[2];
-            b0 = fmaf(k * x, x, 0.25f * y * y);
-            x = s[1] - 2.f * s[2] + s[3]; y = s[1] - 4.f * s[2] + 3.f * s[3];
-            b1 = fmaf(k * x, x, 0.25f * y * y);
-            x = s[2] - 2.f * s[3] + s[4]; y = 3.f * s[2] - 4.f * s[3] + s[4];
-            b2 = fmaf(k * x, x, 0.25f * y * y);
-            d0 = 0.3f; d1 = 0.6f; d2 = 0.1f;
-        }
-        const float eps = 1e-36f, cap = 1e18f;
-        float tau = fabsf(b0 - b2);
-        float t0 = fminf(tau / (eps + b0), cap), t1 = fminf(tau / (eps + b1), cap), t2 = fminf(tau / (eps + b2), cap);
-        float a0 = d0 * fmaf(t0, t0, 1.f), a1 = d1 * fmaf(t1, t1, 1.f), a2 = d2 * fmaf(t2, t2, 1.f);
-        float inv = 1.0f / (a0 + a1 + a2);
-        w[0] = a0 * inv; w[1] = a1 * inv; w[2] = a2 * inv;
-    }
-    // One interface per lane; every lane of the warp calls this (valid or not)
+    // P clamp, face energy and HLLC of one interface from its reconstructed
+    // (rho, m, P) on both sides (same arithmetic as the FP32 path)
     template <int D>
-    __device__ static void warp_flux(const float (&c)[6][6], bool valid, const Consts& k, float F[5],
-                                     unsigned char* psm, int warp) {
-        const int lane = threadIdx.x & 31;
-        uint32_t* R = (uint32_t*)(psm + 2 * learned::PK_BYTES + warp * 160 * 32);
-        float* logit = (float*)R;
-        float L[5], Rv[5];
-        const float t13 = 1.0f / 3.0f, m76 = -7.0f / 6.0f, e116 = 11.0f / 6.0f, m16 = -1.0f / 6.0f,
-                    f56 = 5.0f / 6.0f;
-        bool use[2][5];
-#pragma unroll
-        for (int side = 0; side < 2; ++side) {
-#pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                float s[5], u[5];
-#pragma unroll
-                for (int i = 0; i < 5; ++i) s[i] = valid ? c[i + side][q] : 0.f;
-                use[side][q] = learned::normalise<float>(s, side, u);
-                int r = lane * 5 + q;
-                R[r * 8 + 0] = learned::pack2(u[0], u[1]);
-                R[r * 8 + 1] = learned::pack2(u[2], u[3]);
-                R[r * 8 + 2] = learned::pack2(u[4], 0.f);
-                R[r * 8 + 3] = 0u; R[r * 8 + 4] = 0u; R[r * 8 + 5] = 0u; R[r * 8 + 6] = 0u; R[r * 8 + 7] = 0u;
-            }
-            __syncwarp();
-            learned::mlp_tiles(psm + side * learned::PK_BYTES, R, logit, 10);
-#pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                float s[5];
-#pragma unroll
-                for (int i = 0; i < 5; ++i) s[i] = c[i + side][q];
-                float w[3];
-                if (use[side][q]) learned::softmax3(&logit[4 * (lane * 5 + q)], w);
-                else wenoz_w(s, side, w);
-                float qa, qb, qc;
-                if (side == 0) {
-                    qa = t13 * s[0] + m76 * s[1] + e116 * s[2];
-                    qb = m16 * s[1] + f56 * s[2] + t13 * s[3];
-                    qc = t13 * s[2] + f56 * s[3] + m16 * s[4];
-                } else {
-                    qa = m16 * s[0] + f56 * s[1] + t13 * s[2];
-                    qb = t13 * s[1] + f56 * s[2] + m16 * s[3];
-                    qc = e116 * s[2] + m76 * s[3] + t13 * s[4];
-                }
-                float v = fmaf(w[0], qa, fmaf(w[1], qb, w[2] * qc));
-                if (side == 0) L[q] = v; else Rv[q] = v;
-            }
-            __syncwarp();
-        }
+    __device__ static void finish(const float (&c)[6][6], const Consts& k, const float (&L)[5], const float (&Rv)[5],
+                                  float F[5]) {
         float PmaxL = fmaxf(fmaxf(fmaxf(fmaxf(c[0][5], c[1][5]), c[2][5]), c[3][5]), c[4][5]);
         float PmaxR = fmaxf(fmaxf(fmaxf(fmaxf(c[1][5], c[2][5]), c[3][5]), c[4][5]), c[5][5]);
         float PL = fminf(fmaxf(L[4], 0.0f), PmaxL);
@@ -510,6 +446,134 @@ struct F32Learned {
             F[0] = Fr[0]; F[1] = Fr[2]; F[2] = Fr[3]; F[3] = Fr[1]; F[4] = Fr[4];
         }
     }
+
+    // One interface per lane; every lane of the warp calls this (valid or not).
+    // c[cell][col]: cols 0-3 rho, m_x, m_y, m_z, col 4 E, col 5 P; the
+    // reconstructed fields are rho, m and P (cols 0-3 and 5), as the
+    // reference's (src/gpu_kernels.jl:61-80).
+    //
+    // Every reconstruction first takes the FP32 WENO5-Z value (the fallback),
+    // sharing candidates and smoothness indicators between the left and right
+    // stencils exactly as the FP32 path does.  The network replaces it where
+    // the stencil is smooth and not constant: the test tau <= THETA (min beta
+    // + BETA_EPS) on the normalised stencil u = (v - v_c)/s is evaluated on
+    // the raw indicators (beta scales with s^2), so only network rows pay
+    // for the normalisation; the spread s must also exceed SPREAD_ABS and
+    // SPREAD_REL_F32 |v_c|.  Network rows are compacted over the warp
+    // (prefix sum of the lanes' counts), one side at a time, so the tensor
+    // cores run ceil(rows / 16) tiles and none when the warp's stencils are
+    // all quiescent or shocked.
+    template <int D>
+    __device__ static void warp_flux(const float (&c)[6][6], bool valid, const Consts& k, float F[5],
+                                     unsigned char* psm, int warp) {
+        const int lane = threadIdx.x & 31;
+        uint32_t* R = (uint32_t*)(psm + 2 * learned::PK_BYTES + warp * 160 * 16);
+        float* logit = (float*)R;
+        const float t13 = 1.0f / 3.0f, m76 = -7.0f / 6.0f, e116 = 11.0f / 6.0f, m16 = -1.0f / 6.0f,
+                    f56 = 5.0f / 6.0f, k1312 = 13.0f / 12.0f;
+        float L[5], Rv[5];
+        unsigned need[2] = {0u, 0u};
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const int col = q < 4 ? q : 5;
+            float c0 = c[0][col], c1 = c[1][col], c2 = c[2][col], c3 = c[3][col], c4 = c[4][col], c5 = c[5][col];
+            if (!valid) c0 = c1 = c2 = c3 = c4 = c5 = 0.f;
+            float qA = t13 * c0 + m76 * c1 + e116 * c2;
+            float qB = m16 * c1 + f56 * c2 + t13 * c3;
+            float qC = t13 * c2 + f56 * c3 + m16 * c4;
+            float qD = e116 * c3 + m76 * c4 + t13 * c5;
+            float s0 = c0 - 2.0f * c1 + c2, s1 = c1 - 2.0f * c2 + c3, s2 = c2 - 2.0f * c3 + c4,
+                  s3 = c3 - 2.0f * c4 + c5;
+            float a = c0 - 4.0f * c1 + 3.0f * c2, b = c1 - c3, cc = 3.0f * c2 - 4.0f * c3 + c4,
+                  d = c2 - 4.0f * c3 + 3.0f * c4, e = 3.0f * c3 - 4.0f * c4 + c5;
+            float bA = fmaf(k1312 * s0, s0, 0.25f * a * a);
+            float bB = fmaf(k1312 * s1, s1, 0.25f * b * b);
+            float x2 = k1312 * s2 * s2;
+            float bC = fmaf(0.25f * cc, cc, x2);
+            float bD = fmaf(0.25f * d, d, x2);
+            float bE = fmaf(k1312 * s3, s3, 0.25f * e * e);
+            L[q] = f32::wz(bA, bB, bC, 0.1f, 0.6f, 0.3f, qA, qB, qC);
+            Rv[q] = f32::wz(bB, bD, bE, 0.3f, 0.6f, 0.1f, qB, qC, qD);
+            // spreads about the common centre c2: left stencil c0..c4, right c1..c5
+            float m14 = fmaxf(fmaxf(fabsf(c1 - c2), fabsf(c3 - c2)), fabsf(c4 - c2));
+            float sL = fmaxf(m14, fabsf(c0 - c2)), sR = fmaxf(m14, fabsf(c5 - c2));
+            bool smL = fabsf(bA - bC) <= learned::THETA * (fminf(fminf(bA, bB), bC) + learned::BETA_EPS * sL * sL);
+            bool smR = fabsf(bB - bE) <= learned::THETA * (fminf(fminf(bB, bD), bE) + learned::BETA_EPS * sR * sR);
+            // spreads at FP32 rounding level of the centre value (or below
+            // WENO-Z's epsilon scale) carry no shape: WENO-Z stays.  This
+            // also keeps the network off the 1e-30-level precursor noise that
+            // upwind stencils leave ahead of a shock.
+            const float smin = fmaxf(learned::SPREAD_ABS, learned::SPREAD_REL_F32 * fabsf(c2));
+            need[0] |= (unsigned)(smL && sL > smin) << q;
+            need[1] |= (unsigned)(smR && sR > smin) << q;
+        }
+        // both sides' row counts in one prefix sum (8 bits each: at most 160 rows a side)
+        const int packed = __popc(need[0]) | (__popc(need[1]) << 8);
+        if (!__any_sync(0xffffffffu, packed != 0)) return finish<D>(c, k, L, Rv, F);   // warp-uniform
+        int incl = packed;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int tot = __shfl_sync(0xffffffffu, incl, 31), excl = incl - packed;
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const int total = (tot >> (8 * side)) & 255;
+            if (total == 0) continue;   // warp-uniform
+            const int base = (excl >> (8 * side)) & 255;
+            int r = base;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                if (!((need[side] >> q) & 1u)) continue;
+                const int col = q < 4 ? q : 5;
+                const float vc = c[2][col];
+                float u[5], sp = 0.f;
+#pragma unroll
+                for (int i = 0; i < 5; ++i) {
+                    u[i] = c[i + side][col] - vc;
+                    sp = fmaxf(sp, fabsf(u[i]));
+                }
+                const float inv = 1.0f / sp;
+                *reinterpret_cast<uint4*>(R + r * 4) =
+                    make_uint4(learned::pack2(u[0] * inv, u[1] * inv), learned::pack2(u[2] * inv, u[3] * inv),
+                               learned::pack2(u[4] * inv, 0.f), 0u);
+                ++r;
+            }
+            const int ntiles = (total + 15) >> 4;
+            for (int rr = total + lane; rr < ntiles * 16; rr += 32)
+                *reinterpret_cast<uint4*>(R + rr * 4) = make_uint4(0u, 0u, 0u, 0u);
+            __syncwarp();
+            learned::mlp_tiles(psm + side * learned::PK_BYTES, R, logit, ntiles);
+            r = base;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                if (!((need[side] >> q) & 1u)) continue;
+                const int col = q < 4 ? q : 5;
+                float w[3];
+                const float4 z = *reinterpret_cast<const float4*>(logit + 4 * r);
+                const float zz[3] = {z.x, z.y, z.z};
+                learned::softmax3(zz, w);
+                ++r;
+                const float v0 = c[side][col], v1 = c[side + 1][col], v2 = c[side + 2][col], v3 = c[side + 3][col],
+                            v4 = c[side + 4][col];
+                float qa, qb, qc;
+                if (side == 0) {
+                    qa = t13 * v0 + m76 * v1 + e116 * v2;
+                    qb = m16 * v1 + f56 * v2 + t13 * v3;
+                    qc = t13 * v2 + f56 * v3 + m16 * v4;
+                    L[q] = fmaf(w[0], qa, fmaf(w[1], qb, w[2] * qc));
+                } else {
+                    qa = m16 * v0 + f56 * v1 + t13 * v2;
+                    qb = t13 * v1 + f56 * v2 + m16 * v3;
+                    qc = e116 * v2 + m76 * v3 + t13 * v4;
+                    Rv[q] = fmaf(w[0], qa, fmaf(w[1], qb, w[2] * qc));
+                }
+            }
+            __syncwarp();
+        }
+        finish<D>(c, k, L, Rv, F);
+    }
     template <int D>
     __device__ static void flux(const float (&)[6][6], const Consts&, float F[5]) {
         F[0] = F[1] = F[2] = F[3] = F[4] = 0.f;   // unused: kWarpFaces
@@ -519,7 +583,7 @@ struct F32Learned {
 }  // namespace tile
 
 namespace {
-const TileVariant kLearnedVariants[] = {{8, 8, 8, 256}, {16, 8, 4, 256}};
+const TileVariant kLearnedVariants[] = {{8, 8, 8, 256, 2}, {16, 8, 4, 256, 2}, {8, 8, 8, 256, 3}, {8, 8, 4, 128, 6}};
 
 template <int TX, int TY, int TZ, int NT, int MINB>
 bsn_status launch_learned(bsn_ctx* ctx, const f64::StageArgs& A) {
@@ -549,6 +613,8 @@ bsn_status learned_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A
     switch (idx) {
         case 0: return launch_learned<8, 8, 8, 256, 2>(ctx, A);
         case 1: return launch_learned<16, 8, 4, 256, 2>(ctx, A);
+        case 2: return launch_learned<8, 8, 8, 256, 3>(ctx, A);    // register-capped for 3 CTAs per SM
+        case 3: return launch_learned<8, 8, 4, 128, 6>(ctx, A);
         default: return set_err(ctx, BSN_ERR_ARG, "no learned tile variant %d", idx);
     }
 }
@@ -586,8 +652,8 @@ extern "C" bsn_status bsn_learned_collect(bsn_ctx* ctx, const double* U, int nx,
     unsigned long long h[2];
     BSN_CUDA(ctx, cudaMemcpyAsync(h, cnt, 16, cudaMemcpyDeviceToHost, ctx->stream));
     BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    counts[0] = (long long)std::min<unsigned long long>(h[0], (unsigned long long)cap);
-    counts[1] = (long long)std::min<unsigned long long>(h[1], (unsigned long long)cap);
+    counts[0] = (long long)h[0];   // offered; the buffers hold the first min(count, cap)
+    counts[1] = (long long)h[1];
     return BSN_OK;
 }
 

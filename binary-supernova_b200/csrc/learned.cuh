@@ -11,8 +11,9 @@
 //
 // Fallback: a reconstruction uses the network only where the WENO-Z
 // smoothness indicators of the normalised stencil say the data is smooth,
-//     tau5 <= THETA * (min_k beta_k + BETA_EPS);
-// elsewhere (discontinuities, strong extrema) it uses plain WENO5-Z.
+//     tau5 <= THETA * (min_k beta_k + BETA_EPS),
+// and the stencil's spread is above rounding level (SPREAD_*); elsewhere
+// (discontinuities, strong extrema, quiescent gas) it uses plain WENO5-Z.
 #pragma once
 
 #include <cstdint>
@@ -25,6 +26,13 @@ constexpr int NIN = 5, NH = 32, NOUT = 3;
 constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + NH * NIN, OFF_W2 = OFF_B1 + NH, OFF_B2 = OFF_W2 + NH * NH,
               OFF_W3 = OFF_B2 + NH, OFF_B3 = OFF_W3 + NOUT * NH, NPARAM = OFF_B3 + NOUT;
 constexpr float THETA = 4.0f, BETA_EPS = 1e-3f;
+// Minimum stencil spread max|v_i - v_c| for the network: below it the
+// weights cannot change the reconstruction beyond rounding.  Training
+// samples (FP64) need spread > SPREAD_ABS and > SPREAD_REL_F64 |v_c|; the
+// FP32 stencil kernel uses SPREAD_REL_F32 (FP32 rounding level).
+constexpr float SPREAD_ABS = 1e-15f;
+constexpr double SPREAD_REL_F64 = 1e-12;
+constexpr float SPREAD_REL_F32 = 1e-6f;
 constexpr int SAMPLE = 8;   // floats per training sample: u[5], target omega[3]
 
 // Normalised stencil and the fallback flag.  side 0: left-biased stencil

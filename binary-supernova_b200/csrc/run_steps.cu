@@ -38,6 +38,9 @@ __global__ void dt_kernel(Dev* r, double cfl, double t_end) {
         if (!(r->t < t_end)) { r->done = 1; return; }
         dt = jmin(dt, t_end - r->t);
     }
+    // an infinite signal speed (overflowed state) gives dt = 0: time cannot
+    // advance, stop and report instead of stepping in place
+    if (!(dt > 0.0)) { r->done = 2; return; }
     r->dt = dt;
     r->smax = 0ull;
     r->nanflag = 0u;
@@ -60,6 +63,7 @@ struct State {
     double *A = nullptr, *B = nullptr;
     Dev* r = nullptr;
     cudaStream_t cap = nullptr;   // private stream used only to capture (the caller's may be the legacy stream)
+    cudaEvent_t flag_ev[2] = {nullptr, nullptr};   // done-flag readbacks of the replay chunks
 };
 
 State* state(bsn_ctx* ctx) {
@@ -81,6 +85,8 @@ void run_state_free(bsn_ctx* ctx) {
     run::State* S = (run::State*)ctx->run_state;
     run::release(S);
     if (S->cap) cudaStreamDestroy(S->cap);
+    for (cudaEvent_t e : S->flag_ev)
+        if (e) cudaEventDestroy(e);
     delete S;
     ctx->run_state = nullptr;
 }
@@ -215,16 +221,44 @@ extern "C" bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int
         S->cfl = cfl; S->bc = bc; S->rho_floor = rho_floor; S->P_floor = P_floor; S->prec = precision;
         S->t_end = t_end; S->variant = variant; S->A = A; S->B = B; S->r = r;
     }
-    for (int i = 0; i < n_steps; ++i) {
-        BSN_CUDA(ctx, cudaGraphLaunch(S->exec, ctx->stream));
-        ctx->launches += S->kernels;
+    double* h = (double*)pinned(ctx, 128, &st); BSN_TRY(st);
+    if (t_end > 0.0) {
+        // Replays after t_end are no-ops, so launch in chunks and stop once
+        // the device says done: each chunk's done flag is read back behind
+        // it, and the host waits for the previous chunk's flag only after
+        // queueing the next chunk, keeping the GPU fed.
+        const int CHUNK = 16;
+        volatile int* hflag = (volatile int*)(h + 8);
+        for (int b = 0; b < 2; ++b)
+            if (!S->flag_ev[b]) BSN_CUDA(ctx, cudaEventCreateWithFlags(&S->flag_ev[b], cudaEventDisableTiming));
+        int launched = 0;
+        for (int chunk = 0; launched < n_steps; ++chunk) {
+            int c = std::min(CHUNK, n_steps - launched);
+            for (int i = 0; i < c; ++i) {
+                BSN_CUDA(ctx, cudaGraphLaunch(S->exec, ctx->stream));
+                ctx->launches += S->kernels;
+            }
+            launched += c;
+            BSN_CUDA(ctx, cudaMemcpyAsync((void*)(hflag + (chunk & 1)), &r->done, sizeof(int), cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+            BSN_CUDA(ctx, cudaEventRecord(S->flag_ev[chunk & 1], ctx->stream));
+            if (chunk > 0) {
+                BSN_CUDA(ctx, cudaEventSynchronize(S->flag_ev[(chunk - 1) & 1]));
+                if (hflag[(chunk - 1) & 1]) break;
+            }
+        }
+    } else {
+        for (int i = 0; i < n_steps; ++i) {
+            BSN_CUDA(ctx, cudaGraphLaunch(S->exec, ctx->stream));
+            ctx->launches += S->kernels;
+        }
     }
-    double* h = (double*)pinned(ctx, 64, &st); BSN_TRY(st);
     BSN_CUDA(ctx, cudaMemcpyAsync(h, r, sizeof(Dev), cudaMemcpyDeviceToHost, ctx->stream));
     BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     Dev d;
     memcpy(&d, h, sizeof(Dev));
     *t_inout = d.t;
     if (steps_done) *steps_done = d.steps;
+    if (d.done == 2) return set_err(ctx, BSN_ERR_NONFINITE, "time step collapsed to 0 at t = %.17g (infinite signal speed)", d.t);
     return BSN_OK;
 }

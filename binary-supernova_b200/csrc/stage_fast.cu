@@ -32,7 +32,8 @@ struct F32Physics {
 }  // namespace tile
 
 namespace {
-const TileVariant kF32Variants[] = {{8, 8, 8, 256}, {16, 8, 4, 256}, {8, 8, 4, 128}, {16, 8, 8, 256}, {16, 16, 4, 256}};
+const TileVariant kF32Variants[] = {{8, 8, 8, 256, 3}, {16, 8, 4, 256, 3}, {8, 8, 4, 128, 6}, {16, 8, 8, 256, 2},
+                                     {16, 16, 4, 256, 2}};
 
 template <int TX, int TY, int TZ, int NT, int MINB>
 bsn_status launch_f32(bsn_ctx* ctx, const f64::StageArgs& A) {

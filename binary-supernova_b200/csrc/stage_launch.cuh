@@ -9,7 +9,7 @@ namespace bsn {
 enum Precision { PREC_F64 = 0, PREC_F32 = 1, PREC_LEARNED = 2 };
 
 struct TileVariant {
-    int tx, ty, tz, nt;
+    int tx, ty, tz, nt, minb;   // block tile, threads per CTA, min CTAs per SM (register cap)
 };
 
 // per-precision variant tables (hydro_f64.cu: FP64, stage_fast.cu: FP32)

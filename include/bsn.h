@@ -145,7 +145,8 @@ bsn_status bsn_euler3d_step_learned(bsn_ctx* ctx, double* U, int nx, int ny, int
 /* Up to n_steps CFL-limited SSP-RK3 steps with dt, t and the CFL maximum kept
  * on the device (one CUDA graph per step).  t_end > 0 stops at t_end exactly
  * as the reference loop; t_end <= 0 runs n_steps.  *t_inout: start time in,
- * final time out; *steps_done (may be NULL): steps taken. */
+ * final time out; *steps_done (may be NULL): steps taken.  A dt of 0 (an
+ * infinite signal speed) stops the loop with BSN_ERR_NONFINITE. */
 bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double dx, double dy,
                          double dz, double gamma, double cfl, int bc, double rho_floor,
                          double P_floor, int precision, int n_steps, double t_end,
@@ -153,18 +154,20 @@ bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double
 /* Tile shape of the fused stage kernel: the library's autotuner times every
  * variant on the first stage of each grid and keeps the fastest.
  * bsn_ctx_set_tile forces variant `variant` (-1: autotune again);
- * bsn_ctx_get_tile reports the choice for a grid as {tx, ty, tz, threads}. */
+ * bsn_ctx_get_tile reports the choice for a grid as {tx, ty, tz, threads,
+ * minimum CTAs per SM the kernel's registers are capped for}. */
 int        bsn_tile_variant_count(int precision);
 bsn_status bsn_ctx_set_tile(bsn_ctx* ctx, int precision, int variant);
-bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int ny, int nz, int out[4]);
+bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int ny, int nz, int out[5]);
 
 /* ---- learned WENO weights (no counterpart in the reference; plain WENO5-Z of
  * src/weno5.jl:14-61 is its judge).  Two networks, for the left- and the
  * right-biased reconstruction, each 5 -> 32 -> 32 -> 3 (ReLU, softmax), map
  * a normalised 5-point stencil u_i = (v_i - v_c)/max|v_j - v_c| to the three
  * weights.  A reconstruction uses the network only where the smoothness
- * indicators of u say the stencil is smooth (tau5 <= 4 (min beta + 1e-3));
- * elsewhere plain WENO5-Z.  Parameters: FP32, bsn_learned_param_count()
+ * indicators of u say the stencil is smooth (tau5 <= 4 (min beta + 1e-3)) and
+ * its spread max|v_j - v_c| exceeds 1e-15 and 1e-6 |v_c| (FP32 rounding
+ * level); elsewhere plain WENO5-Z.  Parameters: FP32, bsn_learned_param_count()
  * floats per network, layout W1[32][5] b1[32] W2[32][32] b2[32] W3[3][32] b3[3].
  * All arrays below are device memory. */
 int        bsn_learned_param_count(void);
@@ -173,7 +176,8 @@ int        bsn_learned_param_count(void);
  * stencils only, and only those whose spread max|v_i - v_c| exceeds both
  * 1e-15 and 1e-12 |v_c| (below that any weights reconstruct to rounding
  * level), each kept with probability 1/stride.  Samples are 8 floats
- * (u[5], omega[3]) appended at counts[side] (in: current, out: new) up to cap. */
+ * (u[5], omega[3]) appended at index counts[side]; counts (in: current, out:
+ * new) count every kept stencil, the buffers hold the first min(count, cap). */
 bsn_status bsn_learned_collect(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, int bc,
                                double gamma, int stride, unsigned long long seed,
                                float* out_left, float* out_right, long long cap, long long counts[2]);

@@ -53,7 +53,7 @@ def test_autotuner_picks_a_variant(bsn):
     U[0] = 1.0
     U[4] = 2.5
     bsn.euler3d_step(U, 40, 40, 40, 0.1, 0.1, 0.1, 1e-3, 1.4)
-    tx, ty, tz, nt = bsn.get_tile(40, 40, 40, "f64")
+    tx, ty, tz, nt, minb = bsn.get_tile(40, 40, 40, "f64")
     assert tx * ty * tz % nt == 0 and nt in (128, 256, 512)
 
 

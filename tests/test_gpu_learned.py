@@ -80,7 +80,7 @@ def trained(orc, bsn, L):
     for k in range(3):
         bsn.run_steps(Usd, *dims, dx, dy, dz, 1.4, 0.4, n_steps=10)
         buf.collect(Usd, *dims, 1.4, stride=1, seed=10 + k)
-    nl, nr = buf.counts
+    nl, nr = buf.stored
     assert nl > 100_000 and nr > 100_000
     out = []
     for side, S in ((0, buf.left()), (1, buf.right())):
