@@ -293,6 +293,10 @@ def run_bsn(args, rank, world):
     bsn.set_profiling(False)
     t_stage = tot / max(cnt, 1) / 1e3
     alg_bytes = 40 * 8 * ncell / 3.0     # 40 FP64 state words per cell per RK3 step, 3 stage launches
+    # DRAM bytes of one stage-1 launch from an ncu capture at 128^3 (t = 0.025), scaled by the
+    # cell count (profiles/stage_kernel_*_sedov128_ncu.md); None where no capture exists
+    traffic_128 = {"learned": 144.1e6, "f32": 135.0e6}.get(prec)
+    traffic = traffic_128 * ncell / 128 ** 3 if traffic_128 else None
     hbm, hbm_kind = peaks()
     achieved = alg_bytes / t_stage / 1e9
     tile = bsn.get_tile(n, n, n, prec)
@@ -360,7 +364,8 @@ def run_bsn(args, rank, world):
             "compare": compare,
             "accuracy": acc,
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_kind": hbm_kind,
-                         "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "traffic_note": "DRAM read+write of one stage-1 launch, ncu at 128^3 scaled by cells",
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": t_stage * 1e3,
                          "note": "the fused stencil kernel is FP-pipe bound (FP32/FP64), not HBM bound; "
                                  "HBM fraction of the algorithmic 40 words/cell-step"},
