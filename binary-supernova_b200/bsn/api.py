@@ -325,6 +325,17 @@ def cfl_dt_fmr3d(G: FMRGrid3D, cfl) -> float:
     return out.value
 
 
+def fmr3d_run_steps(G: FMRGrid3D, cfl, *, n_steps, t=0.0, t_end=0.0, precision="f64", self_gravity=False,
+                    G_grav=1.0):
+    """Up to n_steps CFL-limited fmr3d_step!s on the device (one CUDA graph
+    per step, coarse step and first fine subcycle batched); returns (t, steps)."""
+    tt = C.c_double(float(t))
+    nd = C.c_int(0)
+    _call("bsn_fmr3d_run_steps", context(), C.byref(G.s), float(cfl), PREC[precision], int(bool(self_gravity)),
+          float(G_grav), int(n_steps), float(t_end), C.byref(tt), C.byref(nd))
+    return tt.value, nd.value
+
+
 def restrict_density_to_coarse(G: FMRGrid3D):
     _call("bsn_restrict_density_to_coarse_f64", context(), C.byref(G.s))
 
@@ -394,5 +405,5 @@ def set_profiling(on: bool):
     _call("bsn_ctx_set_profiling", context(), int(bool(on)))
 
 
-__all__ += ["euler3d_step_f32", "euler3d_step_learned", "run_steps", "tile_variants", "set_tile", "get_tile", "kernel_time",
+__all__ += ["euler3d_step_f32", "euler3d_step_learned", "run_steps", "fmr3d_run_steps", "tile_variants", "set_tile", "get_tile", "kernel_time",
             "set_profiling", "PREC"]

@@ -21,6 +21,11 @@ static bsn_status launch_variant(bsn_ctx* ctx, int prec, int idx, const f64::Sta
     if (prec == PREC_F32) return f32_launch_variant(ctx, idx, A);
     return learned_launch_variant(ctx, idx, A);
 }
+static bsn_status launch_batch_variant(bsn_ctx* ctx, int prec, int idx, const f64::StageBatch& B) {
+    if (prec == PREC_F64) return f64_launch_batch_variant(ctx, idx, B);
+    if (prec == PREC_F32) return f32_launch_batch_variant(ctx, idx, B);
+    return learned_launch_batch_variant(ctx, idx, B);
+}
 static bool prec_ok(int p) { return p == PREC_F64 || p == PREC_F32 || p == PREC_LEARNED; }
 
 bsn_status stage_autotune(bsn_ctx* ctx, int prec, const f64::StageArgs& probe, double* scratch) {
@@ -93,6 +98,34 @@ bsn_status stage_launch(bsn_ctx* ctx, int prec, const f64::StageArgs& A) {
         it = ctx->tile_choice.find(key);
     }
     return launch_variant(ctx, prec, it->second, A);
+}
+
+// The variant of a batch is the one chosen for its last level's grid (for
+// two-level FMR the fine level, the larger share of the work per step).
+static bsn_status choose(bsn_ctx* ctx, int prec, const f64::StageArgs& A, int& v) {
+    auto key = std::make_tuple(prec, A.nx, A.ny, A.nz);
+    auto it = ctx->tile_choice.find(key);
+    if (it != ctx->tile_choice.end()) { v = it->second; return BSN_OK; }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(ctx->stream, &cs);
+    if (ctx->forced_tile[prec] >= 0 || cs != cudaStreamCaptureStatusNone) {
+        v = ctx->forced_tile[prec] >= 0 ? ctx->forced_tile[prec] : 0;
+        return BSN_OK;
+    }
+    Geom G(A.nx, A.ny, A.nz);
+    bsn_status st;
+    double* scratch = (double*)slot(ctx, SLOT_UN, sizeof(double) * (size_t)G.nelem(), &st);
+    BSN_TRY(st);
+    BSN_TRY(stage_autotune(ctx, prec, A, scratch));
+    v = ctx->tile_choice[key];
+    return BSN_OK;
+}
+
+bsn_status stage_launch_batch(bsn_ctx* ctx, int prec, const f64::StageBatch& B) {
+    if (B.nlev < 1 || B.nlev > f64::MAXLEV) return set_err(ctx, BSN_ERR_ARG, "batch of %d levels", B.nlev);
+    int v = 0;
+    BSN_TRY(choose(ctx, prec, B.lv[B.nlev - 1], v));
+    return launch_batch_variant(ctx, prec, v, B);
 }
 
 }  // namespace bsn

@@ -96,6 +96,7 @@ void* pinned(bsn_ctx* ctx, size_t bytes, bsn_status* st) {
 void fft_state_free(bsn_ctx* ctx);   // poisson.cu
 void run_state_free(bsn_ctx* ctx);   // run_steps.cu
 void learned_state_free(bsn_ctx* ctx);   // learned.cu
+void fmr_run_state_free(bsn_ctx* ctx);   // fmr_f64.cu
 
 }  // namespace bsn
 
@@ -130,6 +131,7 @@ extern "C" bsn_status bsn_ctx_destroy(bsn_ctx* ctx) {
     fft_state_free(ctx);
     run_state_free(ctx);
     learned_state_free(ctx);
+    fmr_run_state_free(ctx);
     for (auto& r : ctx->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     delete ctx;
     return BSN_OK;

@@ -14,6 +14,7 @@
 //     one kernel folds into the fine registers in the reference's loop order,
 //     so the register sums are bit-identical.
 #include "poisson.cuh"
+#include "stage_launch.cuh"
 
 namespace bsn {
 namespace fmr {
@@ -80,7 +81,9 @@ __global__ void prolong_all_kernel(Geo G, const double* Uc, double* Uf) {
 }
 
 // ghost cells only (src/fmr3d.jl:223-255), slab enumeration as the ghost fill
-__global__ void prolong_ghosts_kernel(Geo G, const double* Ucn, const double* Ucnp1, double alpha, double* dst) {
+__global__ void prolong_ghosts_kernel(Geo G, const double* Ucn, const double* Ucnp1, double alpha, double* dst,
+                                      const int* done) {
+    if (done && *done) return;
     int nx = G.nfx, ny = G.nfy, nz = G.nfz;
     long long X = nx + 2 * BSN_NG, Y = ny + 2 * BSN_NG;
     long long nzg = 2LL * BSN_NG * X * Y, nyg = 2LL * BSN_NG * X * nz, nxg = 2LL * BSN_NG * ny * nz;
@@ -105,7 +108,8 @@ __global__ void prolong_ghosts_kernel(Geo G, const double* Ucn, const double* Uc
 
 // _restrict! (src/fmr3d.jl:266-285); qmax = 5, or 1 for
 // restrict_density_to_coarse! (src/fmr_gravity.jl:40-60)
-__global__ void restrict_kernel(Geo G, double* Uc, const double* Uf, int qmax) {
+__global__ void restrict_kernel(Geo G, double* Uc, const double* Uf, int qmax, const int* done) {
+    if (done && *done) return;
     int nic = G.hi[0] - G.lo[0] + 1, njc = G.hi[1] - G.lo[1] + 1, nkc = G.hi[2] - G.lo[2] + 1;
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)nic * njc * nkc) return;
@@ -131,7 +135,11 @@ struct Regs {
     double* r[6];           // xlo, xhi, ylo, yhi, zlo, zhi: (5, t1, t2) coarse
     const double* bnd[6];
 };
-__global__ void fine_reg_kernel(Geo G, Regs R, double fac) {
+// fac = weight * dt_f / r^2; with dtf_dev, (wt * *dtf_dev) / rr on the device.
+__global__ void fine_reg_kernel(Geo G, Regs R, double fac, const double* dtf_dev, double wt, double rr,
+                                const int* done) {
+    if (done && *done) return;
+    if (dtf_dev) fac = wt * *dtf_dev / rr;
     int nic = G.hi[0] - G.lo[0] + 1, njc = G.hi[1] - G.lo[1] + 1, nkc = G.hi[2] - G.lo[2] + 1;
     long long nx_ = 5LL * njc * nkc, ny_ = 5LL * nic * nkc, nz_ = 5LL * nic * njc;
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -161,7 +169,9 @@ __global__ void fine_reg_kernel(Geo G, Regs R, double fac) {
 
 // Berger-Colella correction (src/fmr3d.jl:379-422).  The x-, y- and z-face
 // corrected coarse cells are disjoint, so every element is independent.
-__global__ void bc_correct_kernel(Geo G, Regs Rc, Regs Rf, double* Uc, double idx, double idy, double idz) {
+__global__ void bc_correct_kernel(Geo G, Regs Rc, Regs Rf, double* Uc, double idx, double idy, double idz,
+                                  const int* done) {
+    if (done && *done) return;
     int nic = G.hi[0] - G.lo[0] + 1, njc = G.hi[1] - G.lo[1] + 1, nkc = G.hi[2] - G.lo[2] + 1;
     long long nx_ = 5LL * njc * nkc, ny_ = 5LL * nic * nkc, nz_ = 5LL * nic * njc;
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -266,17 +276,17 @@ long long ghost_count(int nx, int ny, int nz) {
 }
 
 bsn_status prolong_ghosts(bsn_ctx* ctx, const Geo& G, const double* Ucn, const double* Ucnp1, double alpha,
-                          double* dst) {
+                          double* dst, const int* done = nullptr) {
     long long n = ghost_count(G.nfx, G.nfy, G.nfz);
     prof_begin(ctx);
-    prolong_ghosts_kernel<<<grid1d(n, 128), 128, 0, ctx->stream>>>(G, Ucn, Ucnp1, alpha, dst);
+    prolong_ghosts_kernel<<<grid1d(n, 128), 128, 0, ctx->stream>>>(G, Ucn, Ucnp1, alpha, dst, done);
     return launch_check(ctx, "prolong_ghosts_kernel");
 }
 
-bsn_status restrict_(bsn_ctx* ctx, const Geo& G, double* Uc, const double* Uf, int qmax) {
+bsn_status restrict_(bsn_ctx* ctx, const Geo& G, double* Uc, const double* Uf, int qmax, const int* done = nullptr) {
     long long n = (long long)(G.hi[0] - G.lo[0] + 1) * (G.hi[1] - G.lo[1] + 1) * (G.hi[2] - G.lo[2] + 1);
     prof_begin(ctx);
-    restrict_kernel<<<grid1d(n, 128), 128, 0, ctx->stream>>>(G, Uc, Uf, qmax);
+    restrict_kernel<<<grid1d(n, 128), 128, 0, ctx->stream>>>(G, Uc, Uf, qmax, done);
     return launch_check(ctx, "restrict_kernel");
 }
 
@@ -394,7 +404,7 @@ bsn_status fmr3d_step(bsn_ctx* ctx, const bsn_fmr2* g, double dt_c, int self_gra
             BSN_TRY(f64_launch_stage(ctx, a));
             double fac = rk_w[s] * dt_f / (double)(r * r);
             prof_begin(ctx);
-            fine_reg_kernel<<<grid1d(nreg, 128), 128, 0, ctx->stream>>>(G, R.f, fac);
+            fine_reg_kernel<<<grid1d(nreg, 128), 128, 0, ctx->stream>>>(G, R.f, fac, nullptr, 0.0, 0.0, nullptr);
             BSN_TRY(launch_check(ctx, "fine_reg_kernel"));
         }
         BSN_TRY(f64_ghost_combine(ctx, g->Uf, nullptr, Gh, g->nfx, g->nfy, g->nfz, g->bc, dt_f));
@@ -405,11 +415,298 @@ bsn_status fmr3d_step(bsn_ctx* ctx, const bsn_fmr2* g, double dt_c, int self_gra
     long long ncorr = 5 * (njc * nkc + nic * nkc + nic * njc);
     prof_begin(ctx);
     bc_correct_kernel<<<grid1d(ncorr, 128), 128, 0, ctx->stream>>>(G, R.c, R.f, g->Uc, 1.0 / g->dxc, 1.0 / g->dyc,
-                                                                    1.0 / g->dzc);
+                                                                    1.0 / g->dzc, nullptr);
     BSN_TRY(launch_check(ctx, "bc_correct_kernel"));
     return f64_floors(ctx, g->Uc, g->ncx, g->ncy, g->ncz, g->rho_floor, g->P_floor, g->gamma);
 }
 
+
+// ---------------------------------------------------------------------------
+// Device-resident FMR time loop: the reference driver loop
+//     dt = cfl_dt_fmr3d(G, cfl); dt = min(dt, t_end - t); fmr3d_step!(G, dt); t += dt
+// (src/fmr3d.jl:451-622) with dt, t and both CFL maxima on the device and one
+// CUDA graph per step.  The coarse RK3 step and the first fine subcycle do
+// not depend on each other (subcycle 0 takes its ghosts from U_c^n), so each
+// of their three RK3 stages is one persistent launch over the blocks of both
+// levels (stage_kernel_batch); later subcycles need U_c^{n+1} and follow.
+
+struct RunDev {
+    double dt, dtf, t;
+    unsigned long long smc, smf;   // CFL maxima (double bits) of the coarse and fine level
+    unsigned int nanc, nanf;
+    int done, steps;
+};
+
+__global__ void run_init_kernel(RunDev* r, double t) {
+    r->dt = 0.0; r->dtf = 0.0; r->t = t; r->smc = 0ull; r->smf = 0ull; r->nanc = 0u; r->nanf = 0u;
+    r->done = 0; r->steps = 0;
+}
+
+// cfl_dt_fmr3d (src/fmr3d.jl:616-622): min(dt_c, ratio * dt_f), each
+// cfl / max speed (Inf for a NaN or zero maximum), then the t_end clamp.
+__global__ void run_dt_kernel(RunDev* r, double cfl, int ratio, double t_end) {
+    if (r->done) return;
+    double smc = __longlong_as_double((long long)r->smc), smf = __longlong_as_double((long long)r->smf);
+    double dtc = r->nanc ? INFINITY : (smc > 0.0 ? cfl / smc : INFINITY);
+    double dtf = r->nanf ? INFINITY : (smf > 0.0 ? cfl / smf : INFINITY);
+    double dt = jmin(dtc, (double)ratio * dtf);
+    r->smc = 0ull; r->smf = 0ull; r->nanc = 0u; r->nanf = 0u;
+    if (t_end > 0.0) {
+        if (!(r->t < t_end)) { r->done = 1; return; }
+        dt = jmin(dt, t_end - r->t);
+    }
+    if (!(dt > 0.0)) { r->done = 2; return; }
+    r->dt = dt;
+    r->dtf = dt / (double)ratio;
+}
+
+__global__ void run_advance_kernel(RunDev* r) {
+    if (r->done) return;
+    r->t += r->dt;
+    r->steps += 1;
+}
+
+__global__ void copy_kernel(double* dst, const double* src, long long n, const int* done) {
+    if (*done) return;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        dst[t] = src[t];
+}
+
+__global__ void zero_kernel(double* a, long long n, const int* done) {
+    if (*done) return;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        a[t] = 0.0;
+}
+
+struct RunState {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;
+    // key of the captured graph
+    bsn_fmr2 g;
+    int prec = -1, sg = 0, vc = -1, vf = -1;
+    double G_grav = 0, cfl = 0, t_end = 0;
+    const void* ptrs[12] = {};
+    cudaStream_t cap = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+};
+
+static bsn_status grid_blocks(long long n, int& blocks) {
+    blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 8);
+    return BSN_OK;
+}
+
+bsn_status fmr3d_run(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int prec, int self_gravity, double G_grav,
+                     int n_steps, double t_end, double* t_inout, int* steps_done) {
+    Geo G;
+    BSN_TRY(make_geo(ctx, g, G));
+    if (prec != PREC_F64 && prec != PREC_F32 && prec != PREC_LEARNED)
+        return set_err(ctx, BSN_ERR_ARG, "bad precision %d", prec);
+    if (n_steps < 0 || !t_inout) return set_err(ctx, BSN_ERR_ARG, "bad n_steps or null t_inout");
+    const int r = g->ratio;
+    Geom C(g->ncx, g->ncy, g->ncz), F(g->nfx, g->nfy, g->nfz);
+    bsn_status st;
+    double* Ucn = (double*)slot(ctx, SLOT_FMR_UCN, sizeof(double) * C.nelem(), &st); BSN_TRY(st);
+    double* Ac = (double*)slot(ctx, SLOT_A, sizeof(double) * C.nelem(), &st); BSN_TRY(st);
+    double* Bc = (double*)slot(ctx, SLOT_B, sizeof(double) * C.nelem(), &st); BSN_TRY(st);
+    double* Gh = (double*)slot(ctx, SLOT_FMR_GH, sizeof(double) * F.nelem(), &st); BSN_TRY(st);
+    double* Af = (double*)slot(ctx, SLOT_FMR_FA, sizeof(double) * F.nelem(), &st); BSN_TRY(st);
+    double* Bf = (double*)slot(ctx, SLOT_FMR_FB, sizeof(double) * F.nelem(), &st); BSN_TRY(st);
+    RunDev* rd = (RunDev*)slot(ctx, SLOT_FMR_RUN, sizeof(RunDev), &st); BSN_TRY(st);
+    RegSet R;
+    BSN_TRY(make_regs(ctx, G, R));
+    double *phic = nullptr, *phif = nullptr;
+    if (self_gravity) {
+        phic = (double*)slot(ctx, SLOT_PHI, sizeof(double) * (size_t)g->ncx * g->ncy * g->ncz, &st); BSN_TRY(st);
+        phif = (double*)slot(ctx, SLOT_PHI2, sizeof(double) * (size_t)g->nfx * g->nfy * g->nfz, &st); BSN_TRY(st);
+        // FFT workspace and Green's function outside the capture
+        BSN_TRY(poisson_prepare(ctx, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc));
+    }
+
+    // level arguments (as fmr3d_step), dt and done on the device
+    const double rk_w[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+    f64::StageArgs cb, fb;
+    stage_args_init(cb, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, g->gamma, g->bc, g->rho_floor, g->P_floor);
+    cb.use_reg = 1;
+    for (int i = 0; i < 6; ++i) cb.reg.reg[i] = R.c.r[i];
+    for (int d = 0; d < 3; ++d) {
+        cb.reg.lo[d] = G.lo[d] - 1;
+        cb.reg.hi[d] = G.hi[d];
+        cb.reg.t0[d] = G.lo[d] - 1;
+        cb.reg.t1[d] = G.hi[d] - 1;
+    }
+    if (self_gravity) { cb.use_sg = 1; cb.phi = phic; }
+    cb.dt_dev = &rd->dt;
+    cb.done_dev = &rd->done;
+    stage_args_init(fb, g->nfx, g->nfy, g->nfz, g->dxf, g->dyf, g->dzf, g->gamma, g->bc, g->rho_floor, g->P_floor);
+    fb.Gh = Gh;
+    fb.use_bnd = 1;
+    for (int i = 0; i < 6; ++i) fb.bnd.f[i] = const_cast<double*>(R.f.bnd[i]);
+    if (self_gravity) { fb.use_sg = 1; fb.phi = phif; }
+    fb.dt_dev = &rd->dtf;
+    fb.done_dev = &rd->done;
+
+    // tile choices before any capture (the autotuner launches and times)
+    {
+        double* scratch = (double*)slot(ctx, SLOT_UN, sizeof(double) * std::max(C.nelem(), F.nelem()), &st);
+        BSN_TRY(st);
+        f64::StageArgs pc = cb, pf = fb;
+        pc.Uin = g->Uc; pc.dt_dev = nullptr; pc.done_dev = nullptr; pc.use_reg = 0;
+        pf.Uin = g->Uf; pf.dt_dev = nullptr; pf.done_dev = nullptr; pf.use_bnd = 0; pf.Gh = nullptr;
+        BSN_TRY(stage_autotune(ctx, prec, pc, scratch));
+        BSN_TRY(stage_autotune(ctx, prec, pf, scratch));
+    }
+    const int vc = ctx->tile_choice[std::make_tuple(prec, g->ncx, g->ncy, g->ncz)];
+    const int vf = ctx->tile_choice[std::make_tuple(prec, g->nfx, g->nfy, g->nfz)];
+
+    run_init_kernel<<<1, 1, 0, ctx->stream>>>(rd, *t_inout);
+    BSN_TRY(launch_check(ctx, "fmr_run_init_kernel"));
+
+    if (!ctx->fmr_run_state) ctx->fmr_run_state = new RunState();
+    RunState* S = (RunState*)ctx->fmr_run_state;
+    const void* ptrs[12] = {Ucn, Ac, Bc, Gh, Af, Bf, rd, R.base, R.f.bnd[0], phic, phif, nullptr};
+    bool same = S->exec && memcmp(&S->g, g, sizeof(bsn_fmr2)) == 0 && S->prec == prec && S->sg == self_gravity &&
+                S->G_grav == G_grav && S->cfl == cfl && S->t_end == t_end && S->vc == vc && S->vf == vf &&
+                memcmp(S->ptrs, ptrs, sizeof(ptrs)) == 0;
+    if (!same) {
+        S->release();
+        if (!S->cap) BSN_CUDA(ctx, cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
+        bool prof = ctx->profiling;
+        ctx->profiling = false;
+        long long l0 = ctx->launches;
+        cudaStream_t user = ctx->stream;
+        ctx->stream = S->cap;
+        cudaError_t be = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (be != cudaSuccess) { ctx->stream = user; ctx->profiling = prof; return cuda_check(ctx, be, "cudaStreamBeginCapture"); }
+        const int* done = &rd->done;
+        auto body = [&]() -> bsn_status {
+            BSN_TRY(f64_cfl_fold(ctx, g->Uc, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, g->gamma, &rd->smc,
+                                 &rd->nanc));
+            BSN_TRY(f64_cfl_fold(ctx, g->Uf, g->nfx, g->nfy, g->nfz, g->dxf, g->dyf, g->dzf, g->gamma, &rd->smf,
+                                 &rd->nanf));
+            run_dt_kernel<<<1, 1, 0, ctx->stream>>>(rd, cfl, r, t_end);
+            BSN_TRY(launch_check(ctx, "fmr_run_dt_kernel"));
+            if (self_gravity) {
+                BSN_TRY(fmr_poisson(ctx, g, G, phic, phif));
+                if (G_grav != 1.0) {
+                    long long nc = (long long)g->ncx * g->ncy * g->ncz, nf = (long long)g->nfx * g->nfy * g->nfz;
+                    scale_kernel<<<grid1d(nc, 256), 256, 0, ctx->stream>>>(phic, nc, G_grav);
+                    BSN_TRY(launch_check(ctx, "scale_kernel"));
+                    scale_kernel<<<grid1d(nf, 256), 256, 0, ctx->stream>>>(phif, nf, G_grav);
+                    BSN_TRY(launch_check(ctx, "scale_kernel"));
+                }
+            }
+            int blocks;
+            grid_blocks(C.nelem(), blocks);
+            copy_kernel<<<blocks, 256, 0, ctx->stream>>>(Ucn, g->Uc, C.nelem(), done);
+            BSN_TRY(launch_check(ctx, "fmr_copy_kernel"));
+            long long nregw = (long long)(R.bytes / sizeof(double));
+            grid_blocks(nregw, blocks);
+            zero_kernel<<<blocks, 256, 0, ctx->stream>>>(R.base, nregw, done);
+            BSN_TRY(launch_check(ctx, "fmr_zero_kernel"));
+            long long nic = G.hi[0] - G.lo[0] + 1, njc = G.hi[1] - G.lo[1] + 1, nkc = G.hi[2] - G.lo[2] + 1;
+            long long nreg = 2 * 5 * (njc * nkc + nic * nkc + nic * njc);
+            const double rr = (double)(r * r);
+            // coarse step + fine subcycle 0 (ghosts from U_c^n), one launch per stage
+            BSN_TRY(prolong_ghosts(ctx, G, Ucn, nullptr, 0.0, Gh, done));
+            {
+                double* inc[3] = {g->Uc, Ac, Bc};
+                double* outc[3] = {Ac, Bc, g->Uc};
+                double* inf[3] = {g->Uf, Af, Bf};
+                double* outf[3] = {Af, Bf, g->Uf};
+                for (int s = 0; s < 3; ++s) {
+                    f64::StageBatch B;
+                    B.nlev = 2;
+                    B.lv[0] = cb;
+                    B.lv[0].Uin = inc[s]; B.lv[0].Un = g->Uc; B.lv[0].Uout = outc[s];
+                    set_stage(B.lv[0], s + 1, 0.0);
+                    B.lv[0].reg.wt = rk_w[s];
+                    B.lv[1] = fb;
+                    B.lv[1].Uin = inf[s]; B.lv[1].Un = g->Uf; B.lv[1].Uout = outf[s];
+                    set_stage(B.lv[1], s + 1, 0.0);
+                    BSN_TRY(stage_launch_batch(ctx, prec, B));
+                    fine_reg_kernel<<<grid1d(nreg, 128), 128, 0, ctx->stream>>>(G, R.f, 0.0, &rd->dtf, rk_w[s], rr,
+                                                                                 done);
+                    BSN_TRY(launch_check(ctx, "fine_reg_kernel"));
+                }
+            }
+            BSN_TRY(f64_ghost_combine(ctx, g->Uc, Bc, nullptr, g->ncx, g->ncy, g->ncz, g->bc, 0.0, &rd->dt, done));
+            BSN_TRY(f64_ghost_combine(ctx, g->Uf, nullptr, Gh, g->nfx, g->nfy, g->nfz, g->bc, 0.0, &rd->dtf, done));
+            // remaining fine subcycles: ghosts from (1-a) U_c^n + a U_c^{n+1}
+            for (int s_sub = 1; s_sub < r; ++s_sub) {
+                double alpha = (double)s_sub / (double)r;
+                BSN_TRY(prolong_ghosts(ctx, G, Ucn, g->Uc, alpha, Gh, done));
+                double* in[3] = {g->Uf, Af, Bf};
+                double* out[3] = {Af, Bf, g->Uf};
+                for (int s = 0; s < 3; ++s) {
+                    f64::StageArgs a = fb;
+                    a.Uin = in[s]; a.Un = g->Uf; a.Uout = out[s];
+                    set_stage(a, s + 1, 0.0);
+                    BSN_TRY(stage_launch(ctx, prec, a));
+                    fine_reg_kernel<<<grid1d(nreg, 128), 128, 0, ctx->stream>>>(G, R.f, 0.0, &rd->dtf, rk_w[s], rr,
+                                                                                 done);
+                    BSN_TRY(launch_check(ctx, "fine_reg_kernel"));
+                }
+                BSN_TRY(f64_ghost_combine(ctx, g->Uf, nullptr, Gh, g->nfx, g->nfy, g->nfz, g->bc, 0.0, &rd->dtf, done));
+            }
+            // restrict, Berger-Colella correction, coarse floors, advance t
+            BSN_TRY(restrict_(ctx, G, g->Uc, g->Uf, 5, done));
+            long long ncorr = 5 * (njc * nkc + nic * nkc + nic * njc);
+            bc_correct_kernel<<<grid1d(ncorr, 128), 128, 0, ctx->stream>>>(G, R.c, R.f, g->Uc, 1.0 / g->dxc,
+                                                                            1.0 / g->dyc, 1.0 / g->dzc, done);
+            BSN_TRY(launch_check(ctx, "bc_correct_kernel"));
+            BSN_TRY(f64_floors(ctx, g->Uc, g->ncx, g->ncy, g->ncz, g->rho_floor, g->P_floor, g->gamma, done));
+            run_advance_kernel<<<1, 1, 0, ctx->stream>>>(rd);
+            return launch_check(ctx, "fmr_run_advance_kernel");
+        };
+        bsn_status cst = body();
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        ctx->stream = user;
+        ctx->profiling = prof;
+        S->kernels = (int)(ctx->launches - l0);
+        ctx->launches = l0;
+        if (cst != BSN_OK) { if (graph) cudaGraphDestroy(graph); return cst; }
+        BSN_CUDA(ctx, e);
+        S->graph = graph;
+        BSN_CUDA(ctx, cudaGraphInstantiate(&S->exec, graph, 0));
+        S->g = *g; S->prec = prec; S->sg = self_gravity; S->G_grav = G_grav; S->cfl = cfl; S->t_end = t_end;
+        S->vc = vc; S->vf = vf;
+        memcpy(S->ptrs, ptrs, sizeof(ptrs));
+    }
+    double* h = (double*)pinned(ctx, 128, &st); BSN_TRY(st);
+    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps, t_end > 0.0, &rd->done, S->ev, (volatile int*)(h + 8)));
+    BSN_CUDA(ctx, cudaMemcpyAsync(h, rd, sizeof(RunDev), cudaMemcpyDeviceToHost, ctx->stream));
+    BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    RunDev d;
+    memcpy(&d, h, sizeof(RunDev));
+    *t_inout = d.t;
+    if (steps_done) *steps_done = d.steps;
+    if (d.done == 2)
+        return set_err(ctx, BSN_ERR_NONFINITE, "time step collapsed to 0 at t = %.17g (infinite signal speed)", d.t);
+    return BSN_OK;
+}
+
+}  // namespace fmr
+
+void fmr_run_state_free(bsn_ctx* ctx) {
+    if (!ctx->fmr_run_state) return;
+    fmr::RunState* S = (fmr::RunState*)ctx->fmr_run_state;
+    S->release();
+    if (S->cap) cudaStreamDestroy(S->cap);
+    for (cudaEvent_t e : S->ev)
+        if (e) cudaEventDestroy(e);
+    delete S;
+    ctx->fmr_run_state = nullptr;
+}
+
+namespace fmr {
 }  // namespace fmr
 }  // namespace bsn
 
@@ -474,4 +771,11 @@ extern "C" bsn_status bsn_solve_fmr_poisson_f64(bsn_ctx* ctx, const bsn_fmr2* g,
     Geo G;
     BSN_TRY(make_geo(ctx, g, G));
     return fmr_poisson(ctx, g, G, phi_c, phi_f);
+}
+
+extern "C" bsn_status bsn_fmr3d_run_steps(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int precision,
+                                          int self_gravity, double G_grav, int n_steps, double t_end,
+                                          double* t_inout, int* steps_done) {
+    if (!ctx) return BSN_ERR_ARG;
+    return fmr3d_run(ctx, g, cfl, precision, self_gravity, G_grav, n_steps, t_end, t_inout, steps_done);
 }

@@ -81,7 +81,8 @@ __global__ void ghost_combine_kernel(double* U, const double* S, const double* G
 }
 
 __global__ void floors_kernel(double* U, int nx, int ny, int nz, double rho_floor, double P_floor, double Pfl_gm1,
-                              double gm1) {
+                              double gm1, const int* done) {
+    if (done && *done) return;
     Geom G(nx, ny, nz);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long n = (long long)nx * ny * nz;
@@ -142,10 +143,12 @@ bsn_status f64_fill_ghosts(bsn_ctx* ctx, double* U, int nx, int ny, int nz, int 
     return launch_check(ctx, "ghost_fill_kernel");
 }
 
-bsn_status f64_floors(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double rho_floor, double P_floor, double gamma) {
+bsn_status f64_floors(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double rho_floor, double P_floor, double gamma,
+                      const int* done_dev) {
     double gm1 = gamma - 1.0;
+    prof_begin(ctx);
     floors_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(U, nx, ny, nz, rho_floor, P_floor,
-                                                                                   P_floor / gm1, gm1);
+                                                                                   P_floor / gm1, gm1, done_dev);
     return launch_check(ctx, "floors_kernel");
 }
 
@@ -202,6 +205,17 @@ bsn_status f64_launch_variant(bsn_ctx* ctx, int idx, const StageArgs& A) {
         case 1: return launch_f64<8, 8, 4, 128, 4>(ctx, A);
         case 2: return launch_f64<16, 8, 4, 256, 2>(ctx, A);
         case 3: return launch_f64<16, 8, 8, 512, 1>(ctx, A);
+        default: return set_err(ctx, BSN_ERR_ARG, "no FP64 tile variant %d", idx);
+    }
+}
+
+bsn_status f64_launch_batch_variant(bsn_ctx* ctx, int idx, const StageBatch& B) {
+    using P = tile::F64Physics;
+    switch (idx) {
+        case 0: return tile::launch_batch<P, 8, 8, 8, 256, 2>(ctx, B, tile::smem_bytes<P, 8, 8, 8>(), "stage_kernel_batch");
+        case 1: return tile::launch_batch<P, 8, 8, 4, 128, 4>(ctx, B, tile::smem_bytes<P, 8, 8, 4>(), "stage_kernel_batch");
+        case 2: return tile::launch_batch<P, 16, 8, 4, 256, 2>(ctx, B, tile::smem_bytes<P, 16, 8, 4>(), "stage_kernel_batch");
+        case 3: return tile::launch_batch<P, 16, 8, 8, 512, 1>(ctx, B, tile::smem_bytes<P, 16, 8, 8>(), "stage_kernel_batch");
         default: return set_err(ctx, BSN_ERR_ARG, "no FP64 tile variant %d", idx);
     }
 }

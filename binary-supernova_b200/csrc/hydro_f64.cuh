@@ -12,7 +12,8 @@ namespace bsn {
 
 bsn_status check_dims(bsn_ctx* ctx, int nx, int ny, int nz);
 bsn_status f64_fill_ghosts(bsn_ctx* ctx, double* U, int nx, int ny, int nz, int bc);
-bsn_status f64_floors(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double rho_floor, double P_floor, double gamma);
+bsn_status f64_floors(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double rho_floor, double P_floor, double gamma,
+                      const int* done_dev = nullptr);
 bsn_status f64_ghost_combine(bsn_ctx* ctx, double* U, const double* S, const double* Gh, int nx, int ny, int nz,
                              int bc, double dt, const double* dt_dev = nullptr, const int* done_dev = nullptr);
 void stage_args_init(f64::StageArgs& A, int nx, int ny, int nz, double dx, double dy, double dz, double gamma, int bc,
@@ -26,6 +27,13 @@ bsn_status f64_cfl_dt(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, dou
 bsn_status f64_cfl_fold(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
                         double gamma, unsigned long long* smax, unsigned int* nanflag);
 bsn_status cfl_from_device(bsn_ctx* ctx, const unsigned long long* red, double cfl, double* dt_out);
+// Replay a one-step graph up to n_steps times on ctx->stream.  With
+// until_done, replays go in chunks and stop once the device flag *done_dev
+// is set (each chunk's flag is read back behind it; the host waits for the
+// previous chunk's flag only after queueing the next).  ev: two events,
+// hflag: two pinned ints.
+bsn_status graph_replay(bsn_ctx* ctx, cudaGraphExec_t exec, int kernels, int n_steps, bool until_done,
+                        const int* done_dev, cudaEvent_t ev[2], volatile int* hflag);
 
 // r_sink / t_sink of src/BinarySupernova.jl:159-171 (host FP64).
 inline double bh_r_sink(const bsn_bh& b) {

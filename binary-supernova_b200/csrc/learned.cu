@@ -619,6 +619,23 @@ bsn_status learned_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A
     }
 }
 
+bsn_status learned_launch_batch_variant(bsn_ctx* ctx, int idx, const f64::StageBatch& B0) {
+    learned::State* S = (learned::State*)ctx->learned_state;
+    if (!S || !S->ready) return set_err(ctx, BSN_ERR_ARG, "no learned WENO weights set (bsn_learned_set_params)");
+    f64::StageBatch B = B0;
+    for (int l = 0; l < B.nlev; ++l) B.lv[l].mlp = S->packed;
+    using P = tile::F32Learned;
+    const char* nm = "stage_kernel_batch_learned";
+    auto sm = [](int base, int nt) { return base + P::kExtraSmem(nt) + 16; };
+    switch (idx) {
+        case 0: return tile::launch_batch<P, 8, 8, 8, 256, 2>(ctx, B, sm(tile::smem_bytes<P, 8, 8, 8>(), 256), nm);
+        case 1: return tile::launch_batch<P, 16, 8, 4, 256, 2>(ctx, B, sm(tile::smem_bytes<P, 16, 8, 4>(), 256), nm);
+        case 2: return tile::launch_batch<P, 8, 8, 8, 256, 3>(ctx, B, sm(tile::smem_bytes<P, 8, 8, 8>(), 256), nm);
+        case 3: return tile::launch_batch<P, 8, 8, 4, 128, 6>(ctx, B, sm(tile::smem_bytes<P, 8, 8, 4>(), 128), nm);
+        default: return set_err(ctx, BSN_ERR_ARG, "no learned tile variant %d", idx);
+    }
+}
+
 void learned_state_free(bsn_ctx* ctx) {
     if (!ctx->learned_state) return;
     learned::State* S = (learned::State*)ctx->learned_state;

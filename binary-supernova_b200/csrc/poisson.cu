@@ -468,6 +468,23 @@ void fft_state_free(bsn_ctx* ctx) {
     ctx->fft_state = nullptr;
 }
 
+bsn_status poisson_prepare(bsn_ctx* ctx, int nx, int ny, int nz, double dx, double dy, double dz) {
+    if (!fft::pow2(nx) || !fft::pow2(ny) || !fft::pow2(nz) || nx < 2 || ny < 2 || nz < 2)
+        return set_err(ctx, BSN_ERR_UNSUPPORTED, "FFT Poisson solve needs power-of-two sizes >= 2 (got %d,%d,%d)",
+                       nx, ny, nz);
+    BSN_TRY(fft::set_smem(ctx));
+    const double* K;
+    BSN_TRY(fft::khat(ctx, nx, ny, nz, dx, dy, dz, &K));
+    const double2* t;
+    BSN_TRY(fft::twiddles(ctx, 2 * nx, &t));
+    BSN_TRY(fft::twiddles(ctx, 2 * ny, &t));
+    BSN_TRY(fft::twiddles(ctx, 2 * nz, &t));
+    bsn_status st;
+    slot(ctx, SLOT_FFT0, sizeof(double2) * (size_t)(nx + 1) * ny * nz, &st); BSN_TRY(st);
+    slot(ctx, SLOT_FFT1, sizeof(double2) * (size_t)(nx + 1) * (2 * ny) * nz, &st); BSN_TRY(st);
+    return BSN_OK;
+}
+
 bsn_status poisson_solve(bsn_ctx* ctx, const double* rho, int nx, int ny, int nz, double dx, double dy, double dz,
                          double* phi) {
     if (!rho || !phi) return set_err(ctx, BSN_ERR_ARG, "rho and phi must be non-null");

@@ -6,6 +6,10 @@
 namespace bsn {
 
 void fft_state_free(bsn_ctx* ctx);
+// Allocate and build everything a solve on this grid needs (FFT workspace,
+// twiddles, the Green's-function transform) without touching any state, so
+// that the solve itself can be captured in a CUDA graph.
+bsn_status poisson_prepare(bsn_ctx* ctx, int nx, int ny, int nz, double dx, double dy, double dz);
 // Phi = solve_poisson_isolated(rho) for rho on the active grid (nx,ny,nz).
 bsn_status poisson_solve(bsn_ctx* ctx, const double* rho, int nx, int ny, int nz, double dx, double dy, double dz,
                          double* phi);

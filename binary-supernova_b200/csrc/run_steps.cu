@@ -109,6 +109,37 @@ bsn_status rk3_prec(bsn_ctx* ctx, f64::StageArgs base, double* U, double dt, int
     return f64_ghost_combine(ctx, U, B, nullptr, base.nx, base.ny, base.nz, base.bc, dt);
 }
 
+bsn_status graph_replay(bsn_ctx* ctx, cudaGraphExec_t exec, int kernels, int n_steps, bool until_done,
+                        const int* done_dev, cudaEvent_t ev[2], volatile int* hflag) {
+    if (!until_done) {
+        for (int i = 0; i < n_steps; ++i) {
+            BSN_CUDA(ctx, cudaGraphLaunch(exec, ctx->stream));
+            ctx->launches += kernels;
+        }
+        return BSN_OK;
+    }
+    const int CHUNK = 16;
+    for (int b = 0; b < 2; ++b)
+        if (!ev[b]) BSN_CUDA(ctx, cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming));
+    int launched = 0;
+    for (int chunk = 0; launched < n_steps; ++chunk) {
+        int c = std::min(CHUNK, n_steps - launched);
+        for (int i = 0; i < c; ++i) {
+            BSN_CUDA(ctx, cudaGraphLaunch(exec, ctx->stream));
+            ctx->launches += kernels;
+        }
+        launched += c;
+        BSN_CUDA(ctx, cudaMemcpyAsync((void*)(hflag + (chunk & 1)), done_dev, sizeof(int), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+        BSN_CUDA(ctx, cudaEventRecord(ev[chunk & 1], ctx->stream));
+        if (chunk > 0) {
+            BSN_CUDA(ctx, cudaEventSynchronize(ev[(chunk - 1) & 1]));
+            if (hflag[(chunk - 1) & 1]) break;
+        }
+    }
+    return BSN_OK;
+}
+
 }  // namespace bsn
 
 using namespace bsn;
@@ -222,37 +253,8 @@ extern "C" bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int
         S->t_end = t_end; S->variant = variant; S->A = A; S->B = B; S->r = r;
     }
     double* h = (double*)pinned(ctx, 128, &st); BSN_TRY(st);
-    if (t_end > 0.0) {
-        // Replays after t_end are no-ops, so launch in chunks and stop once
-        // the device says done: each chunk's done flag is read back behind
-        // it, and the host waits for the previous chunk's flag only after
-        // queueing the next chunk, keeping the GPU fed.
-        const int CHUNK = 16;
-        volatile int* hflag = (volatile int*)(h + 8);
-        for (int b = 0; b < 2; ++b)
-            if (!S->flag_ev[b]) BSN_CUDA(ctx, cudaEventCreateWithFlags(&S->flag_ev[b], cudaEventDisableTiming));
-        int launched = 0;
-        for (int chunk = 0; launched < n_steps; ++chunk) {
-            int c = std::min(CHUNK, n_steps - launched);
-            for (int i = 0; i < c; ++i) {
-                BSN_CUDA(ctx, cudaGraphLaunch(S->exec, ctx->stream));
-                ctx->launches += S->kernels;
-            }
-            launched += c;
-            BSN_CUDA(ctx, cudaMemcpyAsync((void*)(hflag + (chunk & 1)), &r->done, sizeof(int), cudaMemcpyDeviceToHost,
-                                          ctx->stream));
-            BSN_CUDA(ctx, cudaEventRecord(S->flag_ev[chunk & 1], ctx->stream));
-            if (chunk > 0) {
-                BSN_CUDA(ctx, cudaEventSynchronize(S->flag_ev[(chunk - 1) & 1]));
-                if (hflag[(chunk - 1) & 1]) break;
-            }
-        }
-    } else {
-        for (int i = 0; i < n_steps; ++i) {
-            BSN_CUDA(ctx, cudaGraphLaunch(S->exec, ctx->stream));
-            ctx->launches += S->kernels;
-        }
-    }
+    // replays after t_end are no-ops: with t_end, stop once the device says done
+    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps, t_end > 0.0, &r->done, S->flag_ev, (volatile int*)(h + 8)));
     BSN_CUDA(ctx, cudaMemcpyAsync(h, r, sizeof(Dev), cudaMemcpyDeviceToHost, ctx->stream));
     BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     Dev d;

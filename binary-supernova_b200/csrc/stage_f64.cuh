@@ -64,6 +64,17 @@ struct StageArgs {
     const void* mlp;         // learned stencil path: packed network parameters
 };
 
+// Several grids (mesh levels, patches of any size) updated by one launch:
+// level l's blocks are entries [start[l], start[l+1]) of one block list,
+// gx/gy its blocks along x and y (filled by the launcher from the tile).
+constexpr int MAXLEV = 2;
+struct StageBatch {
+    StageArgs lv[MAXLEV];
+    int nlev;
+    int gx[MAXLEV], gy[MAXLEV];
+    int start[MAXLEV + 1];
+};
+
 
 
 }  // namespace f64

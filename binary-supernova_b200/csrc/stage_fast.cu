@@ -66,4 +66,17 @@ bsn_status f32_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A) {
     }
 }
 
+bsn_status f32_launch_batch_variant(bsn_ctx* ctx, int idx, const f64::StageBatch& B) {
+    using P = tile::F32Physics;
+    const char* nm = "stage_kernel_batch_f32";
+    switch (idx) {
+        case 0: return tile::launch_batch<P, 8, 8, 8, 256, 3>(ctx, B, tile::smem_bytes<P, 8, 8, 8>(), nm);
+        case 1: return tile::launch_batch<P, 16, 8, 4, 256, 3>(ctx, B, tile::smem_bytes<P, 16, 8, 4>(), nm);
+        case 2: return tile::launch_batch<P, 8, 8, 4, 128, 6>(ctx, B, tile::smem_bytes<P, 8, 8, 4>(), nm);
+        case 3: return tile::launch_batch<P, 16, 8, 8, 256, 2>(ctx, B, tile::smem_bytes<P, 16, 8, 8>(), nm);
+        case 4: return tile::launch_batch<P, 16, 16, 4, 256, 2>(ctx, B, tile::smem_bytes<P, 16, 16, 4>(), nm);
+        default: return set_err(ctx, BSN_ERR_ARG, "no FP32 tile variant %d", idx);
+    }
+}
+
 }  // namespace bsn

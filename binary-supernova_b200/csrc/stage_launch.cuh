@@ -22,10 +22,17 @@ bsn_status f32_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A);
 int learned_variant_count();
 TileVariant learned_variant(int idx);
 bsn_status learned_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A);
+// batched (several grids in one persistent launch) counterparts
+bsn_status f64_launch_batch_variant(bsn_ctx* ctx, int idx, const f64::StageBatch& B);
+bsn_status f32_launch_batch_variant(bsn_ctx* ctx, int idx, const f64::StageBatch& B);
+bsn_status learned_launch_batch_variant(bsn_ctx* ctx, int idx, const f64::StageBatch& B);
 
 // Launch one stage with the tile chosen for (precision, nx, ny, nz); the
 // first call for a grid runs the autotuner unless a tile was forced.
 bsn_status stage_launch(bsn_ctx* ctx, int precision, const f64::StageArgs& A);
+// One stage on all levels of B in one launch, with the tile variant chosen
+// for the last level's grid (autotuned on first use unless forced).
+bsn_status stage_launch_batch(bsn_ctx* ctx, int precision, const f64::StageBatch& B);
 // Autotune explicitly (must not run during stream capture): times every
 // variant on stage-1 work writing to `scratch` and records the fastest.
 bsn_status stage_autotune(bsn_ctx* ctx, int precision, const f64::StageArgs& probe, double* scratch);

@@ -211,27 +211,33 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
     }
 }
 
-template <class P, int TX, int TY, int TZ, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) stage_kernel(f64::StageArgs A) {
+// Policy-specific shared memory (learned parameters, row buffers) after the
+// staged cells and faces.
+template <class P, int TX, int TY, int TZ>
+__device__ __forceinline__ unsigned char* policy_smem(unsigned char* smem_raw) {
+    using S = Shape<TX, TY, TZ>;
+    return smem_raw + ((sizeof(typename P::real) * (6 * S::NEXT + 5 * S::NFACE) + 15) / 16) * 16;
+}
+
+// One RK3 stage (or euler3d_rhs!) of the TX x TY x TZ block at active
+// origin (a0, b0, c0): three sweeps, sources, combine, floors, CFL fold.
+// Starts with a barrier (the first sweep's), so a CTA may call it for one
+// block after another.
+template <class P, int TX, int TY, int TZ, int NT>
+__device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int b0, int c0,
+                                            unsigned char* smem_raw, double* red, unsigned int& nanflag) {
     using S = Shape<TX, TY, TZ>;
     using real = typename P::real;
     static_assert(S::NCELL % NT == 0, "cells must divide evenly among threads");
     constexpr int CPT = S::NCELL / NT;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     real* sC = reinterpret_cast<real*>(smem_raw);
     real* sF = sC + 6 * S::NEXT;
-    __shared__ double red[NT / 32];
-    __shared__ unsigned int nanflag;
 
-    if (A.done_dev && *A.done_dev) return;   // device time loop already reached t_end
     Geom G(A.nx, A.ny, A.nz);
-    const int a0 = blockIdx.x * TX, b0 = blockIdx.y * TY, c0 = blockIdx.z * TZ;
     const int tid = threadIdx.x;
     if (tid == 0) nanflag = 0;
     const typename P::Consts k = P::consts(A);
-
-    unsigned char* psm = smem_raw + ((sizeof(real) * (6 * S::NEXT + 5 * S::NFACE) + 15) / 16) * 16;
-    P::prologue(psm, A, NT);   // visible to all threads after the first sweep's barrier
+    unsigned char* psm = policy_smem<P, TX, TY, TZ>(smem_raw);
     double acc[CPT][5];
     sweep<P, TX, TY, TZ, NT, 0>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
     sweep<P, TX, TY, TZ, NT, 1>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
@@ -354,9 +360,78 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(f64::StageArgs A) {
     }
 }
 
+// One launch per stage on one grid: CTA (x, y, z) owns block (x, y, z).
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(f64::StageArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[NT / 32];
+    __shared__ unsigned int nanflag;
+    if (A.done_dev && *A.done_dev) return;   // device time loop already reached t_end
+    P::prologue(policy_smem<P, TX, TY, TZ>(smem_raw), A, NT);   // visible after the first barrier
+    stage_block<P, TX, TY, TZ, NT>(A, blockIdx.x * TX, blockIdx.y * TY, blockIdx.z * TZ, smem_raw, red, nanflag);
+}
+
+// Several grids (mesh levels or patches of any size) in one launch: their
+// blocks form one list, level l owning entries [start[l], start[l+1]); a
+// persistent grid of CTAs walks the list.  Each level keeps its own
+// arguments (states, dt, flux registers, boundary capture), so every block
+// computes exactly what its level's own launch would.
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel_batch(const __grid_constant__ f64::StageBatch B) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[NT / 32];
+    __shared__ unsigned int nanflag;
+    if (B.lv[0].done_dev && *B.lv[0].done_dev) return;
+    P::prologue(policy_smem<P, TX, TY, TZ>(smem_raw), B.lv[0], NT);
+    const int total = B.start[B.nlev];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        int l = 0;
+        while (l + 1 < B.nlev && t >= B.start[l + 1]) ++l;
+        const f64::StageArgs& A = B.lv[l];
+        const int r = t - B.start[l], gx = B.gx[l], gy = B.gy[l];
+        stage_block<P, TX, TY, TZ, NT>(A, (r % gx) * TX, ((r / gx) % gy) * TY, (r / (gx * gy)) * TZ, smem_raw, red,
+                                       nanflag);
+    }
+}
+
 template <class P, int TX, int TY, int TZ>
 constexpr int smem_bytes() {
     return (6 * Shape<TX, TY, TZ>::NEXT + 5 * Shape<TX, TY, TZ>::NFACE) * (int)sizeof(typename P::real) + 16;
+}
+
+// Host: launch stage_kernel_batch for the levels in B with a persistent grid
+// (at most as many CTAs as fit on the device at once).
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+bsn_status launch_batch(bsn_ctx* ctx, f64::StageBatch B, int smem, const char* name) {
+    auto fn = stage_kernel_batch<P, TX, TY, TZ, NT, MINB>;
+    static int occ[64] = {0}, sms[64] = {0};
+    const int dev = ctx->device & 63;
+    if (!occ[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaFuncSetAttribute(stage_kernel_batch)");
+        int o = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, NT, smem);
+        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, ctx->device);
+        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaDeviceGetAttribute");
+        occ[dev] = o < 1 ? 1 : o;
+    }
+    if (B.nlev < 1 || B.nlev > f64::MAXLEV) return set_err(ctx, BSN_ERR_ARG, "batch of %d levels", B.nlev);
+    long long total = 0;
+    for (int l = 0; l < B.nlev; ++l) {
+        const f64::StageArgs& A = B.lv[l];
+        long long gx = (A.nx + TX - 1) / TX, gy = (A.ny + TY - 1) / TY, gz = (A.nz + TZ - 1) / TZ;
+        B.gx[l] = (int)gx;
+        B.gy[l] = (int)gy;
+        B.start[l] = (int)total;
+        total += gx * gy * gz;
+    }
+    if (total > 0x7fffffffLL) return set_err(ctx, BSN_ERR_UNSUPPORTED, "too many blocks in one batch");
+    B.start[B.nlev] = (int)total;
+    long long grid = std::min<long long>(total, (long long)occ[dev] * sms[dev]);
+    prof_begin(ctx);
+    fn<<<(unsigned)grid, NT, smem, ctx->stream>>>(B);
+    return launch_check(ctx, name);
 }
 
 }  // namespace tile

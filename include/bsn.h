@@ -263,6 +263,20 @@ bsn_status bsn_cfl_dt_fmr3d_f64(bsn_ctx* ctx, const bsn_fmr2* G, double cfl, dou
 bsn_status bsn_restrict_density_to_coarse_f64(bsn_ctx* ctx, const bsn_fmr2* G);
 /* solve_fmr_poisson (src/fmr_gravity.jl:119-133): phi_c (ncx,ncy,ncz), phi_f (nfx,nfy,nfz) device */
 bsn_status bsn_solve_fmr_poisson_f64(bsn_ctx* ctx, const bsn_fmr2* G, double* phi_c, double* phi_f);
+/* The FMR driver loop `dt = cfl_dt_fmr3d(G, cfl); dt = min(dt, t_end - t);
+ * fmr3d_step!(G, dt; self_gravity, G_grav); t += dt` (src/fmr3d.jl:451-622)
+ * run on the device: up to n_steps steps, t_end > 0 stops at t_end exactly
+ * (t_end <= 0 runs n_steps); dt, t and the CFL maxima stay on the device and
+ * each step is one CUDA graph.  The coarse RK3 step and the first fine
+ * subcycle are updated together, one persistent launch over the blocks of
+ * both levels per RK3 stage; the remaining subcycles follow.  precision:
+ * BSN_PREC_F64 (stencils as fmr3d_step), BSN_PREC_F32 or BSN_PREC_LEARNED.
+ * The first subcycle takes its ghosts from U_c^n itself where the reference
+ * interpolates 1*U_c^n + 0*U_c^{n+1}: results are equal except for the sign
+ * of a zero and a non-finite U_c^{n+1}.  *t_inout: start time in, final time
+ * out; *steps_done (may be NULL): steps taken. */
+bsn_status bsn_fmr3d_run_steps(bsn_ctx* ctx, const bsn_fmr2* G, double cfl, int precision, int self_gravity,
+                               double G_grav, int n_steps, double t_end, double* t_inout, int* steps_done);
 
 #ifdef __cplusplus
 }
