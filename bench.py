@@ -7,7 +7,7 @@ step, the loop the reference drivers run (cfl_dt_3d + euler3d_step!).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bsn|reference]
                   [--n 256] [--path learned|f32|f64] [--tile V] [--no-cpu]
-                  [--no-accuracy]
+                  [--no-accuracy] [--no-fmr]
 
 `value` is device-resident throughput over K steps (state in HBM).  `e2e`
 runs the same step through the public host-buffer path: the state is copied
@@ -213,6 +213,63 @@ def accuracy(bsn, torch, U0, n, dx, kw, t_end=T_END):
     return out
 
 
+def fmr_polytrope(bsn, torch, steps, warmup, log):
+    """Two-level FMR self-gravitating n=1 polytrope (M=1, R=0.5, G=1) in a
+    rho=1e-8 atmosphere: 128^3 base on [-2,2]^3, 128^3 fine on [-1,1]^3
+    (ratio 2), isolated FFT Poisson every step.  Times `steps` steps of the
+    device loop (one graph per step, coarse step + first subcycle batched)
+    for FP32 and FP64 stencils, and the FP64 host-driven loop (cfl_dt_fmr3d +
+    fmr3d_step per step, one launch per level and stage) beside them.
+    cell-updates/s counts the fine level once per subcycle."""
+    from bsn import ics
+    nc, ratio, gam = 128, 2, 2.0
+    dxc = 4.0 / nc
+    lo, hi = 33, 96          # coarse cells covering [-1, 1]
+    kw = dict(rho_floor=1e-8, P_floor=1e-10)
+    U0 = bsn.state(nc, nc, nc)
+    ics.polytrope_ic_3d(U0, nc, nc, nc, dxc, dxc, dxc, gam, M_star=1.0, R_star=0.5, x0=-2.0, y0=-2.0, z0=-2.0,
+                        **kw)
+    bsn.fill_ghost_3d_outflow(U0, nc, nc, nc)
+    nf = (hi - lo + 1) * ratio
+    units = nc ** 3 + ratio * nf ** 3
+
+    def grid():
+        return bsn.FMRGrid3D(U0.clone(), nc, nc, nc, dxc, lo, hi, lo, hi, lo, hi, ratio, gam, **kw)
+
+    out = {"workload": "polytrope FMR 128^3 + 128^3 (ratio 2), self-gravity", "steps": steps,
+           "unit": "cell-updates/s", "units_per_step": units}
+    for prec in ("f32", "f64"):
+        G = grid()
+        t, _ = bsn.fmr3d_run_steps(G, 0.4, n_steps=warmup, precision=prec, self_gravity=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        bsn.fmr3d_run_steps(G, 0.4, n_steps=steps, t=t, precision=prec, self_gravity=True)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[f"{prec}_batched_ms_per_step"] = ms
+        out[f"{prec}_batched_value"] = units / (ms / 1e3)
+        log(f"FMR polytrope {prec} batched: {ms:.3f} ms/step")
+        del G
+    G = grid()
+    for _ in range(warmup):
+        bsn.fmr3d_step(G, bsn.cfl_dt_fmr3d(G, 0.4), self_gravity=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        bsn.fmr3d_step(G, bsn.cfl_dt_fmr3d(G, 0.4), self_gravity=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    out["f64_host_loop_ms_per_step"] = ms
+    out["f64_host_loop_value"] = units / (ms / 1e3)
+    out["speedup_f32_batched_vs_f64_host_loop"] = out["f64_host_loop_ms_per_step"] / out["f32_batched_ms_per_step"]
+    log(f"FMR polytrope f64 host loop: {ms:.3f} ms/step")
+    return out
+
+
 def run_bsn(args, rank, world):
     import numpy as np
     import torch
@@ -304,6 +361,7 @@ def run_bsn(args, rank, world):
 
     log(f"roofline: {kname} {t_stage * 1e3:.3f} ms per launch")
     acc = accuracy(bsn, torch, U0, n, dx, kw) if not args.no_accuracy else None
+    fmr = fmr_polytrope(bsn, torch, max(5, min(args.steps, 20)), args.warmup, log) if not args.no_fmr else None
 
     # e2e: host-buffer path -- pinned host state -> device, one CFL-limited
     # RK3 step through the public entry point, device -> host, every step
@@ -363,6 +421,7 @@ def run_bsn(args, rank, world):
                        "l2": f"state {Ud.numel() * 8 / 1e6:.0f} MB per array > 126 MB L2 (no flush needed)"},
             "compare": compare,
             "accuracy": acc,
+            "fmr": fmr,
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_kind": hbm_kind,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "traffic_note": "DRAM read+write of one stage-1 launch, ncu at 128^3 scaled by cells",
@@ -390,6 +449,7 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the Sedov-to-t=0.05 accuracy runs of the three paths")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-fmr", action="store_true", help="skip the two-level FMR polytrope timing")
     ap.add_argument("--tile", type=int, default=-1,
                     help="force this stage-kernel tile variant for both precisions (default: autotune)")
     args = ap.parse_args()

@@ -435,11 +435,13 @@ struct RunDev {
     unsigned long long smc, smf;   // CFL maxima (double bits) of the coarse and fine level
     unsigned int nanc, nanf;
     int done, steps;
+    unsigned int queue[4];         // block queues of the batched stage launches (zeroed every step)
 };
 
 __global__ void run_init_kernel(RunDev* r, double t) {
     r->dt = 0.0; r->dtf = 0.0; r->t = t; r->smc = 0ull; r->smf = 0ull; r->nanc = 0u; r->nanf = 0u;
     r->done = 0; r->steps = 0;
+    for (int i = 0; i < 4; ++i) r->queue[i] = 0u;
 }
 
 // cfl_dt_fmr3d (src/fmr3d.jl:616-622): min(dt_c, ratio * dt_f), each
@@ -451,6 +453,7 @@ __global__ void run_dt_kernel(RunDev* r, double cfl, int ratio, double t_end) {
     double dtf = r->nanf ? INFINITY : (smf > 0.0 ? cfl / smf : INFINITY);
     double dt = jmin(dtc, (double)ratio * dtf);
     r->smc = 0ull; r->smf = 0ull; r->nanc = 0u; r->nanf = 0u;
+    for (int i = 0; i < 4; ++i) r->queue[i] = 0u;
     if (t_end > 0.0) {
         if (!(r->t < t_end)) { r->done = 1; return; }
         dt = jmin(dt, t_end - r->t);
@@ -623,6 +626,7 @@ bsn_status fmr3d_run(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int prec, int 
                 for (int s = 0; s < 3; ++s) {
                     f64::StageBatch B;
                     B.nlev = 2;
+                    B.queue = &rd->queue[s];
                     B.lv[0] = cb;
                     B.lv[0].Uin = inc[s]; B.lv[0].Un = g->Uc; B.lv[0].Uout = outc[s];
                     set_stage(B.lv[0], s + 1, 0.0);

@@ -67,9 +67,12 @@ struct StageArgs {
 // Several grids (mesh levels, patches of any size) updated by one launch:
 // level l's blocks are entries [start[l], start[l+1]) of one block list,
 // gx/gy its blocks along x and y (filled by the launcher from the tile).
+// queue: a zeroed counter the CTAs draw blocks from (dynamic schedule);
+// null: CTA b takes blocks b, b + gridDim, ...
 constexpr int MAXLEV = 2;
 struct StageBatch {
     StageArgs lv[MAXLEV];
+    unsigned int* queue;
     int nlev;
     int gx[MAXLEV], gy[MAXLEV];
     int start[MAXLEV + 1];

@@ -373,7 +373,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(f64::StageArgs A) {
 
 // Several grids (mesh levels or patches of any size) in one launch: their
 // blocks form one list, level l owning entries [start[l], start[l+1]); a
-// persistent grid of CTAs walks the list.  Each level keeps its own
+// persistent grid of CTAs (as many as fit at once) walks the list, drawing
+// blocks from an atomic queue when one is given.  Each level keeps its own
 // arguments (states, dt, flux registers, boundary capture), so every block
 // computes exactly what its level's own launch would.
 template <class P, int TX, int TY, int TZ, int NT, int MINB>
@@ -384,7 +385,14 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_batch(const __grid_cons
     if (B.lv[0].done_dev && *B.lv[0].done_dev) return;
     P::prologue(policy_smem<P, TX, TY, TZ>(smem_raw), B.lv[0], NT);
     const int total = B.start[B.nlev];
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    __shared__ int next;
+    for (int t = blockIdx.x;; t += gridDim.x) {
+        if (B.queue) {   // draw the next block; read by all before any thread draws again
+            if (threadIdx.x == 0) next = (int)atomicAdd(B.queue, 1u);
+            __syncthreads();
+            t = next;
+        }
+        if (t >= total) break;
         int l = 0;
         while (l + 1 < B.nlev && t >= B.start[l + 1]) ++l;
         const f64::StageArgs& A = B.lv[l];
