@@ -249,11 +249,12 @@ def kepler_update(bhs, orbit: KeplerOrbit, t):
 # ---------------------------------------------------------------------------
 # src/self_gravity.jl, src/fmr_gravity.jl
 
-def solve_poisson_isolated(rho, nx, ny, nz, dx, dy, dz) -> torch.Tensor:
+def solve_poisson_isolated(rho, nx, ny, nz, dx, dy, dz, *, precision="f64") -> torch.Tensor:
+    """precision "f64" (the reference's arithmetic) or "f32" (FP32 transforms)."""
     _check_grid(rho, nx, ny, nz, "rho")
     phi = active_grid(nx, ny, nz, device=rho.device)
-    _call("bsn_solve_poisson_isolated_f64", context(), _ptr(rho), nx, ny, nz, float(dx), float(dy), float(dz),
-          _ptr(phi))
+    name = {"f64": "bsn_solve_poisson_isolated_f64", "f32": "bsn_solve_poisson_isolated_f32"}[precision]
+    _call(name, context(), _ptr(rho), nx, ny, nz, float(dx), float(dy), float(dz), _ptr(phi))
     return phi
 
 

@@ -25,7 +25,7 @@ BASE = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE,
 FP64_PARITY = {"hydro_f64.cu", "sources_f64.cu", "fmr_f64.cu", "poisson.cu", "context.cu", "cfl_noalloc.cu",
                "run_steps.cu", "autotune.cu"}
 # the FP32 fast path: contraction on, approximate division and square root
-FAST = {"stage_fast.cu", "learned.cu"}
+FAST = {"stage_fast.cu", "learned.cu", "poisson_f32.cu"}
 FAST_FLAGS = ["--ftz=true", "--prec-div=false", "--prec-sqrt=false", "--fmad=true"]
 
 

@@ -26,6 +26,7 @@ struct bsn_ctx {
     void* pinned = nullptr;          // small pinned host buffer for scalar results
     size_t pinned_bytes = 0;
     void* fft_state = nullptr;       // poisson.cu plan/twiddle cache
+    void* fft32_state = nullptr;     // poisson_f32.cu FP32 twiddles and Khat
     // per-kernel CUDA-event timing (bsn_ctx_set_profiling)
     bool profiling = false;
     cudaEvent_t pending_start = nullptr;

@@ -94,6 +94,7 @@ void* pinned(bsn_ctx* ctx, size_t bytes, bsn_status* st) {
 }
 
 void fft_state_free(bsn_ctx* ctx);   // poisson.cu
+void fft32_state_free(bsn_ctx* ctx);   // poisson_f32.cu
 void run_state_free(bsn_ctx* ctx);   // run_steps.cu
 void learned_state_free(bsn_ctx* ctx);   // learned.cu
 void fmr_run_state_free(bsn_ctx* ctx);   // fmr_f64.cu
@@ -129,6 +130,7 @@ extern "C" bsn_status bsn_ctx_destroy(bsn_ctx* ctx) {
         if (p) cudaFree(p);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     fft_state_free(ctx);
+    fft32_state_free(ctx);
     run_state_free(ctx);
     learned_state_free(ctx);
     fmr_run_state_free(ctx);

@@ -290,9 +290,11 @@ bsn_status restrict_(bsn_ctx* ctx, const Geo& G, double* Uc, const double* Uf, i
     return launch_check(ctx, "restrict_kernel");
 }
 
-bsn_status fmr_poisson(bsn_ctx* ctx, const bsn_fmr2* g, const Geo& G, double* phic, double* phif) {
+// solve_fmr_poisson (src/fmr_gravity.jl:119-133); fp32: FP32 transforms
+bsn_status fmr_poisson(bsn_ctx* ctx, const bsn_fmr2* g, const Geo& G, double* phic, double* phif, bool fp32 = false) {
     BSN_TRY(restrict_(ctx, G, g->Uc, g->Uf, 1));
-    BSN_TRY(poisson_from_state(ctx, g->Uc, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, -1.0, phic));
+    if (fp32) BSN_TRY(poisson_from_state_f32(ctx, g->Uc, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, -1.0, phic));
+    else BSN_TRY(poisson_from_state(ctx, g->Uc, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, -1.0, phic));
     long long n = (long long)g->nfx * g->nfy * g->nfz;
     prof_begin(ctx);
     trilinear_kernel<<<grid1d(n, 256), 256, 0, ctx->stream>>>(G, phic, phif);
@@ -529,7 +531,8 @@ bsn_status fmr3d_run(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int prec, int 
         phic = (double*)slot(ctx, SLOT_PHI, sizeof(double) * (size_t)g->ncx * g->ncy * g->ncz, &st); BSN_TRY(st);
         phif = (double*)slot(ctx, SLOT_PHI2, sizeof(double) * (size_t)g->nfx * g->nfy * g->nfz, &st); BSN_TRY(st);
         // FFT workspace and Green's function outside the capture
-        BSN_TRY(poisson_prepare(ctx, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc));
+        if (prec == PREC_F64) BSN_TRY(poisson_prepare(ctx, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc));
+        else BSN_TRY(poisson_prepare_f32(ctx, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc));
     }
 
     // level arguments (as fmr3d_step), dt and done on the device
@@ -596,7 +599,7 @@ bsn_status fmr3d_run(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int prec, int 
             run_dt_kernel<<<1, 1, 0, ctx->stream>>>(rd, cfl, r, t_end);
             BSN_TRY(launch_check(ctx, "fmr_run_dt_kernel"));
             if (self_gravity) {
-                BSN_TRY(fmr_poisson(ctx, g, G, phic, phif));
+                BSN_TRY(fmr_poisson(ctx, g, G, phic, phif, prec != PREC_F64));
                 if (G_grav != 1.0) {
                     long long nc = (long long)g->ncx * g->ncy * g->ncz, nf = (long long)g->nfx * g->nfy * g->nfz;
                     scale_kernel<<<grid1d(nc, 256), 256, 0, ctx->stream>>>(phic, nc, G_grav);

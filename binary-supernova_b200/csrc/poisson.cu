@@ -23,6 +23,7 @@
 #include <cmath>
 #include <map>
 
+#include "fft_lines.cuh"
 #include "poisson.cuh"
 
 namespace bsn {
@@ -42,213 +43,6 @@ struct State {
     int knx = 0, kny = 0, knz = 0;
     double kdx = 0, kdy = 0, kdz = 0;
 };
-
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
-__device__ __forceinline__ int bitrev(int v, int logn) { return (int)(__brev((unsigned)v) >> (32 - logn)); }
-
-// In-place radix-2 FFT of `lines` lines of length N (log2 = logn) stored at
-// s[l*N + t].  DIT expects bit-reversed input and yields natural order; DIF
-// takes natural input and yields bit-reversed order.  sign < 0: forward.
-__device__ void fft_dit(double2* s, const double2* tw, int lines, int logn, bool inverse) {
-    const int N = 1 << logn, H = N >> 1;
-    for (int half = 1, lh = 0; half < N; half <<= 1, ++lh) {
-        __syncthreads();
-        for (int b = threadIdx.x; b < lines * H; b += blockDim.x) {
-            int l = b >> (logn - 1), j = b & (H - 1);
-            int grp = j >> lh, pos = j & (half - 1);
-            int i0 = l * N + (grp << (lh + 1)) + pos, i1 = i0 + half;
-            double2 w = tw[pos << (logn - 1 - lh)];
-            if (inverse) w.y = -w.y;
-            double2 a = s[i0], c = cmul(w, s[i1]);
-            s[i0] = make_double2(a.x + c.x, a.y + c.y);
-            s[i1] = make_double2(a.x - c.x, a.y - c.y);
-        }
-    }
-    __syncthreads();
-}
-
-__device__ void fft_dif(double2* s, const double2* tw, int lines, int logn, bool inverse) {
-    const int N = 1 << logn, H = N >> 1;
-    for (int half = H, lh = logn - 1; half >= 1; half >>= 1, --lh) {
-        __syncthreads();
-        for (int b = threadIdx.x; b < lines * H; b += blockDim.x) {
-            int l = b >> (logn - 1), j = b & (H - 1);
-            int grp = j >> lh, pos = j & (half - 1);
-            int i0 = l * N + (grp << (lh + 1)) + pos, i1 = i0 + half;
-            double2 w = tw[pos << (logn - 1 - lh)];
-            if (inverse) w.y = -w.y;
-            double2 a = s[i0], c = s[i1];
-            s[i0] = make_double2(a.x + c.x, a.y + c.y);
-            s[i1] = cmul(w, make_double2(a.x - c.x, a.y - c.y));
-        }
-    }
-    __syncthreads();
-}
-
-__device__ void load_twiddles(double2* stw, const double2* tw, int logn) {
-    for (int t = threadIdx.x; t < (1 << (logn - 1)); t += blockDim.x) stw[t] = tw[t];
-}
-
-// Density source: rho array (nx,ny,nz) or the state U (q = 0), optionally
-// floored as euler3d_rhs! floors before the source is added.
-struct RhoSrc {
-    const double* rho;
-    const double* U;
-    int nx, ny, nz;
-    double rho_floor;   // < 0: no floor
-    __device__ double at(int x, int y, int z) const {
-        double r;
-        if (rho) r = rho[x + (long long)nx * (y + (long long)ny * z)];
-        else {
-            long long X = nx + 2 * BSN_NG, Y = ny + 2 * BSN_NG;
-            r = U[5LL * ((x + BSN_NG) + X * ((y + BSN_NG) + Y * (long long)(z + BSN_NG)))];
-        }
-        if (rho_floor >= 0.0 && r < rho_floor) r = rho_floor;
-        return r;
-    }
-};
-
-// Pass 1: x-forward over the ny*nz rows holding density (rows are lines).
-// W1[kx + (nx+1)*(y + ny*z)], kx <= nx.
-__global__ void fwd_x_kernel(RhoSrc src, double2* W1, const double2* tw, int logn, int lines) {
-    extern __shared__ double2 sm[];
-    const int N = 1 << logn, nx = src.nx;
-    double2* stw = sm;
-    double2* s = sm + (N >> 1);
-    load_twiddles(stw, tw, logn);
-    long long nrows = (long long)src.ny * src.nz;
-    long long row0 = (long long)blockIdx.x * lines;
-    for (int t = threadIdx.x; t < lines * N; t += blockDim.x) s[t] = make_double2(0.0, 0.0);
-    __syncthreads();
-    for (int t = threadIdx.x; t < lines * nx; t += blockDim.x) {
-        int l = t / nx, x = t - l * nx;
-        long long row = row0 + l;
-        if (row >= nrows) continue;
-        int y = (int)(row % src.ny), z = (int)(row / src.ny);
-        s[l * N + bitrev(x, logn)] = make_double2(src.at(x, y, z), 0.0);
-    }
-    fft_dit(s, stw, lines, logn, false);
-    for (int t = threadIdx.x; t < lines * (nx + 1); t += blockDim.x) {
-        int l = t / (nx + 1), kx = t - l * (nx + 1);
-        long long row = row0 + l;
-        if (row >= nrows) continue;
-        W1[kx + (long long)(nx + 1) * row] = s[l * N + kx];
-    }
-}
-
-// Generic strided-line pass over a complex array: lines run along an axis of
-// stride `estride`; a CTA takes `lines` neighbouring lines (stride 1, the kx
-// axis, length nkx) at a fixed outer index.  Input samples t < n_in are read
-// (the rest are zero); outputs t < n_out are written.
-struct AxisIO {
-    const double2* in;
-    double2* out;
-    int nkx;              // extent of the contiguous (line-batch) axis
-    long long nouter;     // number of outer positions
-    long long in_estride, out_estride;   // element stride along the line
-    long long in_ostride, out_ostride;   // stride of the outer index
-    int n_in, n_out;
-};
-
-__global__ void axis_kernel(AxisIO io, const double2* tw, int logn, int lines, int inverse) {
-    extern __shared__ double2 sm[];
-    const int N = 1 << logn;
-    double2* stw = sm;
-    double2* s = sm + (N >> 1);
-    load_twiddles(stw, tw, logn);
-    int nbx = (io.nkx + lines - 1) / lines;
-    long long outer = blockIdx.x / nbx;
-    int kx0 = (int)(blockIdx.x % nbx) * lines;
-    for (int t = threadIdx.x; t < lines * N; t += blockDim.x) s[t] = make_double2(0.0, 0.0);
-    __syncthreads();
-    for (int t = threadIdx.x; t < lines * io.n_in; t += blockDim.x) {
-        int l = t % lines, e = t / lines;
-        int kx = kx0 + l;
-        if (kx >= io.nkx) continue;
-        s[l * N + bitrev(e, logn)] = io.in[kx + outer * io.in_ostride + e * io.in_estride];
-    }
-    fft_dit(s, stw, lines, logn, inverse != 0);
-    for (int t = threadIdx.x; t < lines * io.n_out; t += blockDim.x) {
-        int l = t % lines, e = t / lines;
-        int kx = kx0 + l;
-        if (kx >= io.nkx) continue;
-        io.out[kx + outer * io.out_ostride + e * io.out_estride] = s[l * N + e];
-    }
-}
-
-// z forward (DIF) * Khat (bit-reversed order) * z inverse (DIT), in place in
-// W2[kx + (nx+1)*(ky + N2*z)], z < nz in and out.
-__global__ void z_conv_kernel(double2* W2, const double* khat, int nx, int N2, int ny, int nz, int logn, int lines,
-                              const double2* tw) {
-    extern __shared__ double2 sm[];
-    const int N = 1 << logn;
-    double2* stw = sm;
-    double2* s = sm + (N >> 1);
-    load_twiddles(stw, tw, logn);
-    int nkx = nx + 1;
-    int nbx = (nkx + lines - 1) / lines;
-    int ky = blockIdx.x / nbx;
-    int kx0 = (blockIdx.x % nbx) * lines;
-    long long plane = (long long)nkx * N2;
-    for (int t = threadIdx.x; t < lines * N; t += blockDim.x) s[t] = make_double2(0.0, 0.0);
-    __syncthreads();
-    for (int t = threadIdx.x; t < lines * nz; t += blockDim.x) {
-        int l = t % lines, z = t / lines;
-        int kx = kx0 + l;
-        if (kx >= nkx) continue;
-        s[l * N + z] = W2[kx + (long long)nkx * ky + plane * z];
-    }
-    fft_dif(s, stw, lines, logn, false);
-    int kyf = ky <= ny ? ky : N2 - ky;
-    for (int t = threadIdx.x; t < lines * N; t += blockDim.x) {
-        int l = t / N, p = t - l * N;
-        int kx = kx0 + l;
-        if (kx >= nkx) continue;
-        int kz = bitrev(p, logn);
-        int kzf = kz <= nz ? kz : N - kz;
-        double k = khat[kx + (long long)nkx * (kyf + (long long)(ny + 1) * kzf)];
-        s[t] = make_double2(s[t].x * k, s[t].y * k);
-    }
-    fft_dit(s, stw, lines, logn, true);
-    for (int t = threadIdx.x; t < lines * nz; t += blockDim.x) {
-        int l = t % lines, z = t / lines;
-        int kx = kx0 + l;
-        if (kx >= nkx) continue;
-        W2[kx + (long long)nkx * ky + plane * z] = s[l * N + z];
-    }
-}
-
-// x inverse of the Hermitian rows W1[kx <= nx] -> real Phi[x < nx].
-__global__ void inv_x_kernel(const double2* W1, double* phi, int nx, int ny, int nz, int logn, int lines,
-                             const double2* tw) {
-    extern __shared__ double2 sm[];
-    const int N = 1 << logn;
-    double2* stw = sm;
-    double2* s = sm + (N >> 1);
-    load_twiddles(stw, tw, logn);
-    long long nrows = (long long)ny * nz;
-    long long row0 = (long long)blockIdx.x * lines;
-    for (int t = threadIdx.x; t < lines * N; t += blockDim.x) {
-        int l = t / N, k = t - l * N;
-        long long row = row0 + l;
-        double2 v = make_double2(0.0, 0.0);
-        if (row < nrows) {
-            if (k <= nx) v = W1[k + (long long)(nx + 1) * row];
-            else { double2 c = W1[(N - k) + (long long)(nx + 1) * row]; v = make_double2(c.x, -c.y); }
-        }
-        s[l * N + bitrev(k, logn)] = v;
-    }
-    fft_dit(s, stw, lines, logn, true);
-    for (int t = threadIdx.x; t < lines * nx; t += blockDim.x) {
-        int l = t / nx, x = t - l * nx;
-        long long row = row0 + l;
-        if (row >= nrows) continue;
-        phi[x + (long long)nx * row] = s[l * N + x].x;
-    }
-}
 
 // ---- Khat: three passes over K restricted to the non-negative octant ------
 // pass a: lines along x for (my <= ny, mz <= nz), K generated on the fly
@@ -350,8 +144,7 @@ bsn_status set_smem(bsn_ctx* ctx) {
     int dev = ctx->device & 63;
     if (done[dev]) return BSN_OK;
     int bytes = (int)(sizeof(double2) * (SMEM_COMPLEX + 2048));
-    const void* ks[] = {(const void*)fwd_x_kernel, (const void*)axis_kernel, (const void*)z_conv_kernel,
-                        (const void*)inv_x_kernel, (const void*)khat_x_kernel, (const void*)khat_even_kernel};
+    const void* ks[] = {(const void*)khat_x_kernel, (const void*)khat_even_kernel};
     for (const void* k : ks)
         BSN_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     done[dev] = true;
@@ -433,28 +226,7 @@ bsn_status solve(bsn_ctx* ctx, RhoSrc src, double dx, double dy, double dz, doub
     bsn_status st;
     double2* W1 = (double2*)slot(ctx, SLOT_FFT0, sizeof(double2) * w1, &st); BSN_TRY(st);
     double2* W2 = (double2*)slot(ctx, SLOT_FFT1, sizeof(double2) * w2, &st); BSN_TRY(st);
-    int l1 = lines_for(N1), l2 = lines_for(N2), l3 = lines_for(N3);
-    long long rows = (long long)ny * nz;
-    prof_begin(ctx);
-    fwd_x_kernel<<<grid1d(rows, l1), NT, smem_for(N1, l1), ctx->stream>>>(src, W1, t1, ilog2(N1), l1);
-    BSN_TRY(launch_check(ctx, "fwd_x_kernel"));
-    int nbx2 = (nx + 1 + l2 - 1) / l2;
-    AxisIO y1{W1, W2, nx + 1, nz, nx + 1, nx + 1, (long long)(nx + 1) * ny, (long long)(nx + 1) * N2, ny, N2};
-    prof_begin(ctx);
-    axis_kernel<<<(unsigned)(nbx2 * nz), NT, smem_for(N2, l2), ctx->stream>>>(y1, t2, ilog2(N2), l2, 0);
-    BSN_TRY(launch_check(ctx, "fft_y_kernel"));
-    int nbx3 = (nx + 1 + l3 - 1) / l3;
-    prof_begin(ctx);
-    z_conv_kernel<<<(unsigned)(nbx3 * N2), NT, smem_for(N3, l3), ctx->stream>>>(W2, K, nx, N2, ny, nz, ilog2(N3), l3,
-                                                                                 t3);
-    BSN_TRY(launch_check(ctx, "z_conv_kernel"));
-    AxisIO y2{W2, W1, nx + 1, nz, nx + 1, nx + 1, (long long)(nx + 1) * N2, (long long)(nx + 1) * ny, N2, ny};
-    prof_begin(ctx);
-    axis_kernel<<<(unsigned)(nbx2 * nz), NT, smem_for(N2, l2), ctx->stream>>>(y2, t2, ilog2(N2), l2, 1);
-    BSN_TRY(launch_check(ctx, "fft_y_kernel"));
-    prof_begin(ctx);
-    inv_x_kernel<<<grid1d(rows, l1), NT, smem_for(N1, l1), ctx->stream>>>(W1, phi, nx, ny, nz, ilog2(N1), l1, t1);
-    return launch_check(ctx, "inv_x_kernel");
+    return solve_lines<double2>(ctx, src, K, t1, t2, t3, W1, W2, phi, SMEM_COMPLEX, NT);
 }
 
 }  // namespace fft
@@ -466,6 +238,11 @@ void fft_state_free(bsn_ctx* ctx) {
     if (S->khat) cudaFree(S->khat);
     delete S;
     ctx->fft_state = nullptr;
+}
+
+bsn_status poisson_khat64(bsn_ctx* ctx, int nx, int ny, int nz, double dx, double dy, double dz, const double** K) {
+    BSN_TRY(fft::set_smem(ctx));
+    return fft::khat(ctx, nx, ny, nz, dx, dy, dz, K);
 }
 
 bsn_status poisson_prepare(bsn_ctx* ctx, int nx, int ny, int nz, double dx, double dy, double dz) {

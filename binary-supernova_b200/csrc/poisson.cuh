@@ -10,6 +10,15 @@ void fft_state_free(bsn_ctx* ctx);
 // twiddles, the Green's-function transform) without touching any state, so
 // that the solve itself can be captured in a CUDA graph.
 bsn_status poisson_prepare(bsn_ctx* ctx, int nx, int ny, int nz, double dx, double dy, double dz);
+// The cached FP64 Green's-function transform Khat of the grid (built on first use).
+bsn_status poisson_khat64(bsn_ctx* ctx, int nx, int ny, int nz, double dx, double dy, double dz, const double** K);
+// FP32-transform counterparts (poisson_f32.cu): FP64 density in, FP64 potential out.
+void fft32_state_free(bsn_ctx* ctx);
+bsn_status poisson_prepare_f32(bsn_ctx* ctx, int nx, int ny, int nz, double dx, double dy, double dz);
+bsn_status poisson_solve_f32(bsn_ctx* ctx, const double* rho, int nx, int ny, int nz, double dx, double dy, double dz,
+                             double* phi);
+bsn_status poisson_from_state_f32(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx, double dy,
+                                  double dz, double rho_floor, double* phi);
 // Phi = solve_poisson_isolated(rho) for rho on the active grid (nx,ny,nz).
 bsn_status poisson_solve(bsn_ctx* ctx, const double* rho, int nx, int ny, int nz, double dx, double dy, double dz,
                          double* phi);

@@ -229,6 +229,10 @@ bsn_status bsn_kepler_update(bsn_bh* bhs, const double state[13], double t);
 /* solve_poisson_isolated (src/self_gravity.jl:35-76): rho, phi device (nx,ny,nz). */
 bsn_status bsn_solve_poisson_isolated_f64(bsn_ctx* ctx, const double* rho, int nx, int ny, int nz,
                                           double dx, double dy, double dz, double* phi);
+/* The same solve with FP32 transforms (the precision form of the FFTs): FP64
+ * rho in and phi out, FP32 spectra and Green's function. */
+bsn_status bsn_solve_poisson_isolated_f32(bsn_ctx* ctx, const double* rho, int nx, int ny, int nz,
+                                          double dx, double dy, double dz, double* phi);
 /* _apply_sg_force_level! (src/fmr_gravity.jl:146-156; src/gpu_kernels.jl:291-319) */
 bsn_status bsn_sg_gradient_f64(bsn_ctx* ctx, double* dU, const double* U, const double* phi,
                                int nx, int ny, int nz, double dx, double dy, double dz);

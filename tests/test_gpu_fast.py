@@ -125,3 +125,18 @@ def test_fp32_sedov_run_l1_vs_fp64(orc, bsn):
     e_E = _l1_rel(G[(4,) + a], U[(4,) + a])
     print(f"FP32 vs FP64 Sedov 32^3 t=0.1: L1 rho {e_rho:.3e}, L1 E {e_E:.3e}, steps {ng}")
     assert e_rho < 1e-5 and e_E < 1e-5
+
+
+@pytest.mark.parametrize("dims", [(32, 32, 32), (64, 32, 16)])
+def test_poisson_fp32_transforms_close_to_fp64(bsn, dims):
+    """The FP32-transform solve (precision form of the FFTs) against the FP64
+    solve (itself checked against the oracle to 1e-12): max |dPhi| within
+    1e-5 of max |Phi| on a random positive density."""
+    nx, ny, nz = dims
+    rng = np.random.default_rng(41)
+    rho = torch.from_numpy(np.asfortranarray(rng.uniform(0.1, 2.0, (nx, ny, nz)))).cuda()
+    h = 1.0 / nx
+    p64 = bsn.solve_poisson_isolated(rho, nx, ny, nz, h, h, h)
+    p32 = bsn.solve_poisson_isolated(rho, nx, ny, nz, h, h, h, precision="f32")
+    err = (p32 - p64).abs().max().item() / p64.abs().max().item()
+    assert 0 < err < 1e-5, err

@@ -92,3 +92,15 @@ def test_fmr_run_steps_reduced_precision_close_to_fp64(orc, bsn, prec):
         a = (0,) + (slice(NG, -NG),) * 3
         assert np.isfinite(A).all()
         assert np.abs(A[a] - B[a]).sum() / np.abs(B[a]).sum() < tol
+
+
+def test_fmr_run_steps_selfgravity_fp32_transforms(orc, bsn):
+    """FP32 stencils and FP32 FFTs with self-gravity stay close to the FP64 loop."""
+    _, G64 = _smooth_sg_grid(orc, bsn)
+    _, G32 = _smooth_sg_grid(orc, bsn)
+    t64, _ = bsn.fmr3d_run_steps(G64, 0.4, n_steps=3, self_gravity=True)
+    t32, _ = bsn.fmr3d_run_steps(G32, 0.4, n_steps=3, self_gravity=True, precision="f32")
+    assert abs(t32 - t64) <= 1e-6 * t64
+    a = (0,) + (slice(NG, -NG),) * 3
+    for A, B in ((host(G32.Uc), host(G64.Uc)), (host(G32.Uf), host(G64.Uf))):
+        assert np.abs(A[a] - B[a]).sum() / np.abs(B[a]).sum() < 1e-5
