@@ -13,6 +13,8 @@ struct F32Physics {
     using real = float;
     static constexpr bool kCenterFromSmem = false;  // smem holds FP32 copies: reload FP64 state
     static constexpr bool kWarpFaces = false;
+    static constexpr bool kQuiescentSkip = false;
+    __device__ static bool same(float, float) { return true; }
     static constexpr int kExtraSmem(int) { return 0; }
     __device__ static void prologue(unsigned char*, const f64::StageArgs&, int) {}
     struct Consts { float g, gm1, inv_gm1, gg; };

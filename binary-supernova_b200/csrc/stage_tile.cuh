@@ -35,6 +35,8 @@ struct F64Physics {
     using real = double;
     static constexpr bool kCenterFromSmem = true;   // smem holds the floored FP64 state
     static constexpr bool kWarpFaces = false;       // faces computed thread by thread
+    static constexpr bool kQuiescentSkip = false;
+    __device__ static bool same(double, double) { return true; }
     static constexpr int kExtraSmem(int) { return 0; }
     __device__ static void prologue(unsigned char*, const f64::StageArgs&, int) {}
     struct Consts { double g, gm1; };
@@ -104,7 +106,24 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
         for (int q = 0; q < 5; ++q) { w[q] = (real)v[q]; sC[q * S::NEXT + e] = w[q]; }
         sC[5 * S::NEXT + e] = P::pressure(w, k);
     }
-    __syncthreads();
+    // policies with per-stencil work that only non-uniform data can need
+    // (the learned weights' fallback test) learn here whether every staged
+    // value of the sweep equals the first one within the policy's margin
+    bool quiet = false;
+    if constexpr (P::kQuiescentSkip) {
+        __syncthreads();
+        bool varied = false;
+        for (int e = tid; e < NE; e += NT) {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                if (q == 4) continue;   // E is not reconstructed
+                varied |= !P::same(sC[q * S::NEXT + e], sC[q * S::NEXT]);
+            }
+        }
+        quiet = !__syncthreads_or(varied);
+    } else {
+        __syncthreads();
+    }
 
     constexpr int SD = (D == 0) ? 1 : (D == 1 ? LX : LX * LY);
     // one face: write it to smem and, if this tile owns it, to the optional
@@ -175,7 +194,7 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
 #pragma unroll
                 for (int q = 0; q < 6; ++q) c[s][q] = valid ? sC[q * S::NEXT + base + s * SD] : (real)0;
             real F[5];
-            P::template warp_flux<D>(c, valid, k, F, psm, warp);
+            P::template warp_flux<D>(c, valid, k, F, psm, warp, quiet);
             if (valid) emit(f, fx, fy, fz, F);
         }
     } else {
