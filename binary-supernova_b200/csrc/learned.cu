@@ -584,8 +584,9 @@ struct F32Learned {
         finish<D>(c, k, L, Rv, F);
     }
     template <int D>
-    __device__ static void flux(const float (&)[6][6], const Consts&, float F[5]) {
-        F[0] = F[1] = F[2] = F[3] = F[4] = 0.f;   // unused: kWarpFaces
+    // uniform sweeps (kQuiescentSkip): no network row can occur, plain FP32 WENO5-Z + HLLC
+    __device__ static void flux(const float (&c)[6][6], const Consts& k, float F[5]) {
+        f32::interface_flux<D>(c, k.g, k.gm1, k.inv_gm1, k.gg, F);
     }
 };
 

@@ -179,25 +179,8 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
         }
         return valid;
     };
-    if constexpr (P::kWarpFaces) {
-        // warp-collective faces (tensor-core work inside the flux): every lane
-        // of a warp takes part in every iteration, valid face or not
-        const int warp = tid >> 5, lane = tid & 31;
-        for (int fb = warp * 32; fb < NF; fb += NT) {
-            int f = fb + lane;
-            int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
-            bool valid = f < NF && face_valid(fx, fy, fz);
-            real c[6][6];
-            int base = valid ? fx + LX * (fy + LY * fz) : 0;
-#pragma unroll
-            for (int s = 0; s < 6; ++s)
-#pragma unroll
-                for (int q = 0; q < 6; ++q) c[s][q] = valid ? sC[q * S::NEXT + base + s * SD] : (real)0;
-            real F[5];
-            P::template warp_flux<D>(c, valid, k, F, psm, warp, quiet);
-            if (valid) emit(f, fx, fy, fz, F);
-        }
-    } else {
+    // thread-per-face loop (the plain stencil physics)
+    auto plain_faces = [&]() {
         for (int f = tid; f < NF; f += NT) {
             int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
             if (!face_valid(fx, fy, fz)) continue;
@@ -211,6 +194,31 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
             P::template flux<D>(c, k, F);
             emit(f, fx, fy, fz, F);
         }
+    };
+    if constexpr (P::kWarpFaces) {
+        if (P::kQuiescentSkip && quiet) {
+            plain_faces();   // uniform sweep: no per-stencil work can apply, the policy's plain flux
+        } else {
+            // warp-collective faces (tensor-core work inside the flux): every
+            // lane of a warp takes part in every iteration, valid face or not
+            const int warp = tid >> 5, lane = tid & 31;
+            for (int fb = warp * 32; fb < NF; fb += NT) {
+                int f = fb + lane;
+                int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
+                bool valid = f < NF && face_valid(fx, fy, fz);
+                real c[6][6];
+                int base = valid ? fx + LX * (fy + LY * fz) : 0;
+#pragma unroll
+                for (int s = 0; s < 6; ++s)
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) c[s][q] = valid ? sC[q * S::NEXT + base + s * SD] : (real)0;
+                real F[5];
+                P::template warp_flux<D>(c, valid, k, F, psm, warp, quiet);
+                if (valid) emit(f, fx, fy, fz, F);
+            }
+        }
+    } else {
+        plain_faces();
     }
     __syncthreads();
 
