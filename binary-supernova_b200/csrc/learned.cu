@@ -409,6 +409,7 @@ struct F32Learned {
     using real = float;
     static constexpr bool kCenterFromSmem = false;
     static constexpr bool kWarpFaces = true;
+    static constexpr bool kCross = false;   // per-sweep staging: the row buffers need the shared memory
     // A sweep whose staged values all lie within a quarter of the network's
     // spread thresholds of the first one cannot hold a network row (every
     // stencil spread is at most twice that): its faces skip the fallback test.

@@ -11,6 +11,7 @@ namespace bsn {
 namespace tile {
 struct F32Physics {
     using real = float;
+    static constexpr bool kCross = true;
     static constexpr bool kCenterFromSmem = false;  // smem holds FP32 copies: reload FP64 state
     static constexpr bool kWarpFaces = false;
     static constexpr bool kQuiescentSkip = false;

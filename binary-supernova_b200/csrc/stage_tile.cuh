@@ -28,11 +28,17 @@ struct Shape {
     static constexpr int NEXT = EX0 > EX1 ? (EX0 > EX2 ? EX0 : EX2) : (EX1 > EX2 ? EX1 : EX2);
     static constexpr int FC0 = (TX + 1) * TY * TZ, FC1 = TX * (TY + 1) * TZ, FC2 = TX * TY * (TZ + 1);
     static constexpr int NFACE = FC0 > FC1 ? (FC0 > FC2 ? FC0 : FC2) : (FC1 > FC2 ? FC1 : FC2);
+    // "cross" staging (all three sweeps from one staged region): the block,
+    // then the 3-cell halos below/above it along x, y and z
+    static constexpr int HX = 3 * TY * TZ, HY = 3 * TX * TZ, HZ = 3 * TX * TY;
+    static constexpr int OXL = NCELL, OXH = OXL + HX, OYL = OXH + HX, OYH = OYL + HY, OZL = OYH + HY, OZH = OZL + HZ;
+    static constexpr int NCROSS = OZH + HZ;
 };
 
 // Physics policies --------------------------------------------------------
 struct F64Physics {
     using real = double;
+    static constexpr bool kCross = true;             // stage the block and all halos once
     static constexpr bool kCenterFromSmem = true;   // smem holds the floored FP64 state
     static constexpr bool kWarpFaces = false;       // faces computed thread by thread
     static constexpr bool kQuiescentSkip = false;
@@ -76,10 +82,42 @@ __device__ __forceinline__ void load_cell(const f64::StageArgs& A, const Geom& G
     for (int q = 0; q < 5; ++q) v[q] = src[off + q];
 }
 
+// Staged values of the cross region (P::kCross) at entry e, from active
+// coordinates (a, b, c) and the axis the cell may leave the grid along.
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ void cross_cell(int e, int a0, int b0, int c0, const Geom& G, int& a, int& b, int& c,
+                                           int& d) {
+    using S = Shape<TX, TY, TZ>;
+    if (e < S::OXL) {
+        int i = e % TX, r = e / TX, j = r % TY, kk = r / TY;
+        a = a0 + i; b = b0 + j; c = c0 + kk;
+        d = a >= G.nx ? 0 : (b >= G.ny ? 1 : 2);   // partial block: the axis it leaves (used only along it)
+    } else if (e < S::OYL) {
+        int r = e - S::OXL;
+        const bool hi = r >= S::HX;
+        if (hi) r -= S::HX;
+        int h = r % 3, rr = r / 3, j = rr % TY, kk = rr / TY;
+        a = hi ? a0 + TX + h : a0 - 3 + h; b = b0 + j; c = c0 + kk; d = 0;
+    } else if (e < S::OZL) {
+        int r = e - S::OYL;
+        const bool hi = r >= S::HY;
+        if (hi) r -= S::HY;
+        int i = r % TX, rr = r / TX, h = rr % 3, kk = rr / 3;
+        a = a0 + i; b = hi ? b0 + TY + h : b0 - 3 + h; c = c0 + kk; d = 1;
+    } else {
+        int r = e - S::OZL;
+        const bool hi = r >= S::HZ;
+        if (hi) r -= S::HZ;
+        int i = r % TX, rr = r / TX, j = rr % TY, h = rr / TY;
+        a = a0 + i; b = b0 + j; c = hi ? c0 + TZ + h : c0 - 3 + h; d = 2;
+    }
+}
+
 template <class P, int TX, int TY, int TZ, int NT, int D>
 __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::Consts& k, int a0, int b0, int c0,
                       typename P::real* sC, typename P::real* sF, unsigned char* psm,
                       double (&acc)[Shape<TX, TY, TZ>::NCELL / NT][5]) {
+    constexpr bool CROSS = P::kCross;
     using S = Shape<TX, TY, TZ>;
     using real = typename P::real;
     constexpr int CPT = S::NCELL / NT;
@@ -91,41 +129,60 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
     const int n[3] = {G.nx, G.ny, G.nz};
     const int o[3] = {a0, b0, c0};
 
-    __syncthreads();
-    for (int e = tid; e < NE; e += NT) {
-        int ex = e % LX, r = e / LX, ey = r % LY, ez = r / LY;
-        int a = a0 + ex - (D == 0 ? 3 : 0);
-        int b = b0 + ey - (D == 1 ? 3 : 0);
-        int c = c0 + ez - (D == 2 ? 3 : 0);
-        double v[5];
-        bool act;
-        load_cell(A, G, D, a, b, c, v, act);
-        if (act) f64::apply_floor(v[0], v[1], v[2], v[3], v[4], A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
-        real w[5];
-#pragma unroll
-        for (int q = 0; q < 5; ++q) { w[q] = (real)v[q]; sC[q * S::NEXT + e] = w[q]; }
-        sC[5 * S::NEXT + e] = P::pressure(w, k);
-    }
-    // policies with per-stencil work that only non-uniform data can need
-    // (the learned weights' fallback test) learn here whether every staged
-    // value of the sweep equals the first one within the policy's margin
     bool quiet = false;
-    if constexpr (P::kQuiescentSkip) {
-        __syncthreads();
-        bool varied = false;
-        for (int e = tid; e < NE; e += NT) {
-#pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                if (q == 4) continue;   // E is not reconstructed
-                varied |= !P::same(sC[q * S::NEXT + e], sC[q * S::NEXT]);
-            }
-        }
-        quiet = !__syncthreads_or(varied);
+    if constexpr (CROSS) {
+        __syncthreads();   // staged once by stage_block; sF free after the previous sweep's divergence
     } else {
         __syncthreads();
+        for (int e = tid; e < NE; e += NT) {
+            int ex = e % LX, r = e / LX, ey = r % LY, ez = r / LY;
+            int a = a0 + ex - (D == 0 ? 3 : 0);
+            int b = b0 + ey - (D == 1 ? 3 : 0);
+            int c = c0 + ez - (D == 2 ? 3 : 0);
+            double v[5];
+            bool act;
+            load_cell(A, G, D, a, b, c, v, act);
+            if (act) f64::apply_floor(v[0], v[1], v[2], v[3], v[4], A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+            real w[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) { w[q] = (real)v[q]; sC[q * S::NEXT + e] = w[q]; }
+            sC[5 * S::NEXT + e] = P::pressure(w, k);
+        }
+        // policies with per-stencil work that only non-uniform data can need
+        // (the learned weights' fallback test) learn here whether every staged
+        // value of the sweep equals the first one within the policy's margin
+        if constexpr (P::kQuiescentSkip) {
+            __syncthreads();
+            bool varied = false;
+            for (int e = tid; e < NE; e += NT) {
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    if (q == 4) continue;   // E is not reconstructed
+                    varied |= !P::same(sC[q * S::NEXT + e], sC[q * S::NEXT]);
+                }
+            }
+            quiet = !__syncthreads_or(varied);
+        } else {
+            __syncthreads();
+        }
     }
-
     constexpr int SD = (D == 0) ? 1 : (D == 1 ? LX : LX * LY);
+    constexpr int FSTR = CROSS ? S::NCROSS : S::NEXT;   // field stride of the staged values
+    // staged index of stencil cell s (0..5, cells fd-3 .. fd+2 along D) of face (fx, fy, fz)
+    auto sidx = [&](int fx, int fy, int fz, int s) -> int {
+        if constexpr (!CROSS) {
+            return fx + LX * (fy + LY * fz) + s * SD;
+        } else {
+            const int fd = D == 0 ? fx : (D == 1 ? fy : fz);
+            const int p = fd - 3 + s;
+            int cb, cs, lo, hs;
+            if (D == 0) { cb = TX * (fy + TY * fz); cs = 1; lo = S::OXL + 3 * (fy + TY * fz); hs = 1; }
+            else if (D == 1) { cb = fx + TX * TY * fz; cs = TX; lo = S::OYL + fx + 3 * TX * fz; hs = TX; }
+            else { cb = fx + TX * fy; cs = TX * TY; lo = S::OZL + fx + TX * fy; hs = TX * TY; }
+            constexpr int H = D == 0 ? S::HX : (D == 1 ? S::HY : S::HZ);
+            return p < 0 ? lo + (p + 3) * hs : (p < TD ? cb + p * cs : lo + H + (p - TD) * hs);
+        }
+    };
     // one face: write it to smem and, if this tile owns it, to the optional
     // flux arrays, coarse flux registers and fine boundary-face buffers
     auto emit = [&](int f, int fx, int fy, int fz, const real (&F)[5]) {
@@ -184,12 +241,13 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
         for (int f = tid; f < NF; f += NT) {
             int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
             if (!face_valid(fx, fy, fz)) continue;
-            int base = fx + LX * (fy + LY * fz);
             real c[6][6];
 #pragma unroll
-            for (int s = 0; s < 6; ++s)
+            for (int s = 0; s < 6; ++s) {
+                const int e = sidx(fx, fy, fz, s);
 #pragma unroll
-                for (int q = 0; q < 6; ++q) c[s][q] = sC[q * S::NEXT + base + s * SD];
+                for (int q = 0; q < 6; ++q) c[s][q] = sC[q * FSTR + e];
+            }
             real F[5];
             P::template flux<D>(c, k, F);
             emit(f, fx, fy, fz, F);
@@ -207,11 +265,12 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
                 int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
                 bool valid = f < NF && face_valid(fx, fy, fz);
                 real c[6][6];
-                int base = valid ? fx + LX * (fy + LY * fz) : 0;
 #pragma unroll
-                for (int s = 0; s < 6; ++s)
+                for (int s = 0; s < 6; ++s) {
+                    const int e = valid ? sidx(fx, fy, fz, s) : 0;
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) c[s][q] = valid ? sC[q * S::NEXT + base + s * SD] : (real)0;
+                    for (int q = 0; q < 6; ++q) c[s][q] = valid ? sC[q * FSTR + e] : (real)0;
+                }
                 real F[5];
                 P::template warp_flux<D>(c, valid, k, F, psm, warp, quiet);
                 if (valid) emit(f, fx, fy, fz, F);
@@ -243,7 +302,8 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
 template <class P, int TX, int TY, int TZ>
 __device__ __forceinline__ unsigned char* policy_smem(unsigned char* smem_raw) {
     using S = Shape<TX, TY, TZ>;
-    return smem_raw + ((sizeof(typename P::real) * (6 * S::NEXT + 5 * S::NFACE) + 15) / 16) * 16;
+    constexpr int NST = P::kCross ? S::NCROSS : S::NEXT;
+    return smem_raw + ((sizeof(typename P::real) * (6 * NST + 5 * S::NFACE) + 15) / 16) * 16;
 }
 
 // One RK3 stage (or euler3d_rhs!) of the TX x TY x TZ block at active
@@ -258,7 +318,7 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
     static_assert(S::NCELL % NT == 0, "cells must divide evenly among threads");
     constexpr int CPT = S::NCELL / NT;
     real* sC = reinterpret_cast<real*>(smem_raw);
-    real* sF = sC + 6 * S::NEXT;
+    real* sF = sC + 6 * (P::kCross ? S::NCROSS : S::NEXT);
 
     Geom G(A.nx, A.ny, A.nz);
     const int tid = threadIdx.x;
@@ -266,6 +326,23 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
     const typename P::Consts k = P::consts(A);
     unsigned char* psm = policy_smem<P, TX, TY, TZ>(smem_raw);
     double acc[CPT][5];
+    if constexpr (P::kCross) {
+        // the block and the halos of all three sweeps, staged once (floors in
+        // FP64 on active cells, ghosts raw, pressure once per cell)
+        __syncthreads();   // the previous block of a persistent CTA is done with smem
+        for (int e = tid; e < S::NCROSS; e += NT) {
+            int a, b, c, d;
+            cross_cell<TX, TY, TZ>(e, a0, b0, c0, G, a, b, c, d);
+            double v[5];
+            bool act;
+            load_cell(A, G, d, a, b, c, v, act);
+            if (act) f64::apply_floor(v[0], v[1], v[2], v[3], v[4], A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+            real w[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) { w[q] = (real)v[q]; sC[q * S::NCROSS + e] = w[q]; }
+            sC[5 * S::NCROSS + e] = P::pressure(w, k);
+        }
+    }
     sweep<P, TX, TY, TZ, NT, 0>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
     sweep<P, TX, TY, TZ, NT, 1>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
     sweep<P, TX, TY, TZ, NT, 2>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
@@ -282,9 +359,11 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
         long long off = G.act(a, b, c);
         double u0, u1, u2, u3, u4;
         if (P::kCenterFromSmem) {
-            int e = i + TX * (j + TY * (kk + 3));   // z-extended block of the last sweep
-            u0 = (double)sC[0 * S::NEXT + e]; u1 = (double)sC[1 * S::NEXT + e]; u2 = (double)sC[2 * S::NEXT + e];
-            u3 = (double)sC[3 * S::NEXT + e]; u4 = (double)sC[4 * S::NEXT + e];
+            // the block's cells: the cross region's first part, or the z-extended block of the last sweep
+            constexpr int FS = P::kCross ? S::NCROSS : S::NEXT;
+            int e = P::kCross ? i + TX * (j + TY * kk) : i + TX * (j + TY * (kk + 3));
+            u0 = (double)sC[0 * FS + e]; u1 = (double)sC[1 * FS + e]; u2 = (double)sC[2 * FS + e];
+            u3 = (double)sC[3 * FS + e]; u4 = (double)sC[4 * FS + e];
         } else {
             u0 = A.Uin[off]; u1 = A.Uin[off + 1]; u2 = A.Uin[off + 2]; u3 = A.Uin[off + 3]; u4 = A.Uin[off + 4];
             f64::apply_floor(u0, u1, u2, u3, u4, A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
@@ -431,7 +510,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_batch(const __grid_cons
 
 template <class P, int TX, int TY, int TZ>
 constexpr int smem_bytes() {
-    return (6 * Shape<TX, TY, TZ>::NEXT + 5 * Shape<TX, TY, TZ>::NFACE) * (int)sizeof(typename P::real) + 16;
+    using S = Shape<TX, TY, TZ>;
+    return (6 * (P::kCross ? S::NCROSS : S::NEXT) + 5 * S::NFACE) * (int)sizeof(typename P::real) + 16;
 }
 
 // Host: launch stage_kernel_batch for the levels in B with a persistent grid
