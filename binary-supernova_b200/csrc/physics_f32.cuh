@@ -17,18 +17,25 @@
 namespace bsn {
 namespace f32 {
 
+// Fast division (reciprocal approximation times the numerator).  Used where
+// the denominator lies in [1e-36, 2^126): the WENO-Z denominators eps + beta
+// and weight sums, densities floored at 1e-30, pressures, HLLC wave-speed
+// differences; a denominator above 2^126 would need state values beyond
+// 1e18, far outside what the path represents.
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+
 __device__ __forceinline__ float wz(float b0, float b1, float b2, float d0, float d1, float d2, float q0, float q1,
                                     float q2) {
     const float eps = 1e-36f, cap = 1e18f;
     float tau = fabsf(b0 - b2);
-    float t0 = fminf(tau / (eps + b0), cap);
-    float t1 = fminf(tau / (eps + b1), cap);
-    float t2 = fminf(tau / (eps + b2), cap);
+    float t0 = fminf(fdiv(tau, eps + b0), cap);
+    float t1 = fminf(fdiv(tau, eps + b1), cap);
+    float t2 = fminf(fdiv(tau, eps + b2), cap);
     float a0 = d0 * fmaf(t0, t0, 1.0f);
     float a1 = d1 * fmaf(t1, t1, 1.0f);
     float a2 = d2 * fmaf(t2, t2, 1.0f);
     float num = fmaf(a0, q0, fmaf(a1, q1, a2 * q2));
-    return num / (a0 + a1 + a2);
+    return fdiv(num, a0 + a1 + a2);
 }
 
 // Left/right WENO5-Z at the interface between c2 and c3 (src/weno5.jl:25-61).
@@ -58,13 +65,13 @@ __device__ __forceinline__ void weno5_lr(float c0, float c1, float c2, float c3,
 
 __device__ __forceinline__ float cell_pressure(float r, float mx, float my, float mz, float E, float gm1) {
     r = fmaxf(r, 1e-30f);
-    float KE = 0.5f * (mx * mx + my * my + mz * mz) / r;
+    float KE = fdiv(0.5f * (mx * mx + my * my + mz * mz), r);
     return fmaxf(gm1 * (E - KE), 0.0f);
 }
 
 __device__ __forceinline__ float EL_from_P(float PL, float rL, float mx, float my, float mz, float inv_gm1) {
     float rp = fmaxf(rL, 1e-30f);
-    float KE = fminf(0.5f * (mx * mx + my * my + mz * mz) / rp, 0.5f * rp * 1e4f);
+    float KE = fminf(fdiv(0.5f * (mx * mx + my * my + mz * mz), rp), 0.5f * rp * 1e4f);
     return fmaf(PL, inv_gm1, KE);
 }
 
@@ -88,7 +95,7 @@ __device__ __forceinline__ void hllc_normal(float rL, float mnL, float mt1L, flo
         mnR *= s; mt1R *= s; mt2R *= s;
         m2R = mnR * mnR + mt1R * mt1R + mt2R * mt2R;
     }
-    float iL = 1.0f / rL, iR = 1.0f / rR;
+    float iL = fdiv(1.0f, rL), iR = fdiv(1.0f, rR);
     float KE_L = fminf(0.5f * m2L * iL, 0.5f * rL * 1e4f);
     float KE_R = fminf(0.5f * m2R * iR, 0.5f * rR * 1e4f);
     EL = fmaxf(EL, KE_L);
@@ -101,8 +108,8 @@ __device__ __forceinline__ void hllc_normal(float rL, float mnL, float mt1L, flo
     if (pL > 0.0f && pR > 0.0f) {
         float r_avg = 0.5f * (rL + rR), cs_avg = 0.5f * (csL + csR);
         float p_star = fmaxf(0.0f, 0.5f * (pL + pR) - 0.5f * (vnR - vnL) * r_avg * cs_avg);
-        float qL = p_star > pL ? sqrtf(fmaf(gg, p_star / pL - 1.0f, 1.0f)) : 1.0f;
-        float qR = p_star > pR ? sqrtf(fmaf(gg, p_star / pR - 1.0f, 1.0f)) : 1.0f;
+        float qL = p_star > pL ? sqrtf(fmaf(gg, fdiv(p_star, pL) - 1.0f, 1.0f)) : 1.0f;
+        float qR = p_star > pR ? sqrtf(fmaf(gg, fdiv(p_star, pR) - 1.0f, 1.0f)) : 1.0f;
         SL = vnL - csL * qL;
         SR = vnR + csR * qR;
     } else {
@@ -112,13 +119,13 @@ __device__ __forceinline__ void hllc_normal(float rL, float mnL, float mt1L, flo
     float dL = rL * (SL - vnL), dR = rR * (SR - vnR);
     float denom = dL - dR;
     if (fabsf(denom) < 1e-36f) { F[0] = F[1] = F[2] = F[3] = F[4] = 0.0f; return; }
-    float S_star = (pR - pL + mnL * (SL - vnL) - mnR * (SR - vnR)) / denom;
+    float S_star = fdiv(pR - pL + mnL * (SL - vnL) - mnR * (SR - vnR), denom);
     float FrL = mnL, FmnL = fmaf(mnL, vnL, pL), Fmt1L = mt1L * vnL, Fmt2L = mt2L * vnL, FEL = (EL + pL) * vnL;
     if (SL >= 0.0f) { F[0] = FrL; F[1] = FmnL; F[2] = Fmt1L; F[3] = Fmt2L; F[4] = FEL; return; }
     float FrR = mnR, FmnR = fmaf(mnR, vnR, pR), Fmt1R = mt1R * vnR, Fmt2R = mt2R * vnR, FER = (ER + pR) * vnR;
     if (SR <= 0.0f) { F[0] = FrR; F[1] = FmnR; F[2] = Fmt1R; F[3] = Fmt2R; F[4] = FER; return; }
     if (fmaxf(rL, rR) > 3.0f * fminf(rL, rR)) {
-        float inv = 1.0f / (SR - SL), SLSR = SL * SR;
+        float inv = fdiv(1.0f, SR - SL), SLSR = SL * SR;
         F[0] = (SR * FrL - SL * FrR + SLSR * (rR - rL)) * inv;
         F[1] = (SR * FmnL - SL * FmnR + SLSR * (mnR - mnL)) * inv;
         F[2] = (SR * Fmt1L - SL * Fmt1R + SLSR * (mt1R - mt1L)) * inv;
@@ -127,16 +134,16 @@ __device__ __forceinline__ void hllc_normal(float rL, float mnL, float mt1L, flo
         return;
     }
     if (S_star >= 0.0f) {
-        float chi = dL / (SL - S_star);
-        float EsL = fabsf(dL) > 1e-36f ? chi * (EL * iL + (S_star - vnL) * (S_star + pL / dL)) : 0.0f;
+        float chi = fdiv(dL, SL - S_star);
+        float EsL = fabsf(dL) > 1e-36f ? chi * (EL * iL + (S_star - vnL) * (S_star + fdiv(pL, dL))) : 0.0f;
         F[0] = FrL + SL * (chi - rL);
         F[1] = FmnL + SL * (chi * S_star - mnL);
         F[2] = Fmt1L + SL * (chi * vt1L - mt1L);
         F[3] = Fmt2L + SL * (chi * vt2L - mt2L);
         F[4] = FEL + SL * (EsL - EL);
     } else {
-        float chi = dR / (SR - S_star);
-        float EsR = fabsf(dR) > 1e-36f ? chi * (ER * iR + (S_star - vnR) * (S_star + pR / dR)) : 0.0f;
+        float chi = fdiv(dR, SR - S_star);
+        float EsR = fabsf(dR) > 1e-36f ? chi * (ER * iR + (S_star - vnR) * (S_star + fdiv(pR, dR))) : 0.0f;
         F[0] = FrR + SR * (chi - rR);
         F[1] = FmnR + SR * (chi * S_star - mnR);
         F[2] = Fmt1R + SR * (chi * vt1R - mt1R);
