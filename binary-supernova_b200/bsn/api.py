@@ -286,6 +286,23 @@ def coupled_step(U, bhs, dt, t, nx, ny, nz, dx, x0, y0, z0, gamma, f_sink, rho_f
     return np.array(Fg[: 3 * len(bhs)]).reshape(len(bhs), 3)
 
 
+def coupled_run_steps(U, bhs, nx, ny, nz, dx, x0, y0, z0, gamma, cfl, *, n_steps, t=0.0, t_end=0.0, dt_max=0.0,
+                      f_sink=1.0, rho_floor=0.0, P_floor=0.0, torque_free=True, self_gravity=False,
+                      t_bh2_sink_on=0.0, rho_sink_min=0.0, evolve_orbit=True, precision="f64"):
+    """The coupled_step! driver loop on the device (one CUDA graph per step);
+    returns (t, steps) and updates `bhs` in place."""
+    _check_state(U, nx, ny, nz)
+    arr = _bh_array(bhs)
+    tt = C.c_double(float(t))
+    nd = C.c_int(0)
+    _call("bsn_coupled_run_steps", context(), _ptr(U), arr, len(bhs), nx, ny, nz, float(dx), float(x0), float(y0),
+          float(z0), float(gamma), float(cfl), float(dt_max), float(f_sink), float(rho_floor), float(P_floor),
+          int(bool(torque_free)), int(bool(self_gravity)), float(t_bh2_sink_on), float(rho_sink_min),
+          int(bool(evolve_orbit)), PREC[precision], int(n_steps), float(t_end), C.byref(tt), C.byref(nd))
+    _bh_writeback(bhs, arr)
+    return tt.value, nd.value
+
+
 # ---------------------------------------------------------------------------
 # src/fmr3d.jl
 
@@ -406,5 +423,5 @@ def set_profiling(on: bool):
     _call("bsn_ctx_set_profiling", context(), int(bool(on)))
 
 
-__all__ += ["euler3d_step_f32", "euler3d_step_learned", "run_steps", "fmr3d_run_steps", "tile_variants", "set_tile", "get_tile", "kernel_time",
+__all__ += ["euler3d_step_f32", "euler3d_step_learned", "run_steps", "fmr3d_run_steps", "coupled_run_steps", "tile_variants", "set_tile", "get_tile", "kernel_time",
             "set_profiling", "PREC"]

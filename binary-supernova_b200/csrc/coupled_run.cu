@@ -1,0 +1,439 @@
+// coupled_run.cu -- the production driver loop on the device: dt = CFL (capped
+// by dt_max, clamped to t_end), then coupled_step! (scripts/run_sn50_fiducial.jl
+// :756-818) -- gas force on every BH, the BH orbit (nbody_step!, FP64), the
+// SSP-RK3 stages with BH gravity, self-gravity and sinks in the driver's order,
+// accrete! on every active sink -- with the BHs, t and dt kept in device
+// memory and each step one CUDA graph.  Built with -fmad=false: the FP64
+// orbit, accretion and source arithmetic are the same operations in the same
+// order as the host versions (src/nbody.jl:24-104, src/sinks.jl:74-109).
+#include <cmath>
+#include <cstring>
+
+#include "hydro_f64.cuh"
+#include "poisson.cuh"
+#include "stage_launch.cuh"
+
+namespace bsn {
+namespace crun {
+
+using f64::MAXBH;
+
+struct Dev {
+    double dt, t;
+    unsigned long long smax;
+    unsigned int nanflag;
+    int done, steps;
+    int nbh, pad;
+    bsn_bh bh[MAXBH];
+    double Fg[3 * MAXBH];
+    f64::BHSrc bsrc;
+    f64::SinkSrc ssrc;
+};
+
+__global__ void init_kernel(Dev* r, double t, const bsn_bh* bhs, int nbh) {
+    r->dt = 0.0; r->t = t; r->smax = 0ull; r->nanflag = 0u; r->done = 0; r->steps = 0; r->nbh = nbh;
+    for (int i = 0; i < nbh; ++i) r->bh[i] = bhs[i];
+    for (int i = 0; i < 3 * MAXBH; ++i) r->Fg[i] = 0.0;
+}
+
+// dt = cfl / max speed (Inf for NaN or zero), capped by dt_max > 0, clamped to t_end > 0.
+__global__ void dt_kernel(Dev* r, double cfl, double t_end, double dt_max) {
+    if (r->done) return;
+    double smax = __longlong_as_double((long long)r->smax);
+    double dt = r->nanflag ? INFINITY : (smax > 0.0 ? cfl / smax : INFINITY);
+    if (dt_max > 0.0) dt = jmin(dt, dt_max);
+    if (t_end > 0.0) {
+        if (!(r->t < t_end)) { r->done = 1; return; }
+        dt = jmin(dt, t_end - r->t);
+    }
+    if (!(dt > 0.0)) { r->done = 2; return; }
+    r->dt = dt;
+    r->smax = 0ull;
+    r->nanflag = 0u;
+}
+
+__global__ void advance_kernel(Dev* r) {
+    if (r->done) return;
+    r->t += r->dt;
+    r->steps += 1;
+}
+
+// gas_force_on_bh partial sums for BH i (compensated, as f64::gas_force_kernel)
+struct DD { double hi, lo; };
+__device__ __forceinline__ void dd_add(DD& s, double x) {
+    double t = s.hi + x;
+    double bp = t - s.hi;
+    double e = (s.hi - (t - bp)) + (x - bp);
+    s.hi = t;
+    s.lo += e;
+}
+__device__ __forceinline__ DD dd_merge(DD a, DD b) {
+    DD s = a;
+    dd_add(s, b.hi);
+    s.lo += b.lo;
+    return s;
+}
+
+__global__ void gas_force_kernel(const double* U, int nx, int ny, int nz, double dx, double dy, double dz, double x0,
+                                 double y0, double z0, const Dev* r, int i, double* part) {
+    if (r->done) return;
+    const bsn_bh bh = r->bh[i];
+    Geom G(nx, ny, nz);
+    double dV = dx * dy * dz;
+    DD s[3] = {{0, 0}, {0, 0}, {0, 0}};
+    long long n = (long long)nx * ny * nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int a = (int)(t % nx); long long rr = t / nx; int b = (int)(rr % ny); int c = (int)(rr / ny);
+        double xc, yc, zc;
+        f64::cell_xyz(a, b, c, x0, y0, z0, dx, dy, dz, xc, yc, zc);
+        double ddx = xc - bh.pos[0], ddy = yc - bh.pos[1], ddz = zc - bh.pos[2];
+        double r2 = sq(ddx) + sq(ddy) + sq(ddz) + sq(bh.eps);
+        double r3 = r2 * sqrt(r2);
+        double fac = bh.mass / r3 * U[G.act(a, b, c)] * dV;
+        dd_add(s[0], fac * ddx);
+        dd_add(s[1], fac * ddy);
+        dd_add(s[2], fac * ddz);
+    }
+    __shared__ DD red[3][32];
+    for (int d = 0; d < 3; ++d) {
+        for (int o = 16; o > 0; o >>= 1) {
+            DD other = {__shfl_xor_sync(0xffffffffu, s[d].hi, o), __shfl_xor_sync(0xffffffffu, s[d].lo, o)};
+            s[d] = dd_merge(s[d], other);
+        }
+        if ((threadIdx.x & 31) == 0) red[d][threadIdx.x >> 5] = s[d];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int d = 0; d < 3; ++d) {
+            DD acc = red[d][0];
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) acc = dd_merge(acc, red[d][w]);
+            part[6 * blockIdx.x + 2 * d] = acc.hi;
+            part[6 * blockIdx.x + 2 * d + 1] = acc.lo;
+        }
+    }
+}
+
+// total of BH i's partials, zeroed when non-finite or above 1e3 in norm (the
+// driver's guard, scripts/run_sn50_fiducial.jl:765-769)
+__global__ void gas_force_finish(const double* part, int nblocks, Dev* r, int i) {
+    if (r->done || threadIdx.x != 0 || blockIdx.x != 0) return;
+    double F[3];
+    for (int d = 0; d < 3; ++d) {
+        DD acc = {0.0, 0.0};
+        for (int b = 0; b < nblocks; ++b) acc = dd_merge(acc, DD{part[6 * b + 2 * d], part[6 * b + 2 * d + 1]});
+        F[d] = acc.hi + acc.lo;
+    }
+    bool fin = isfinite(F[0]) && isfinite(F[1]) && isfinite(F[2]);
+    if (!fin || sqrt(F[0] * F[0] + F[1] * F[1] + F[2] * F[2]) > 1e3) F[0] = F[1] = F[2] = 0.0;
+    for (int d = 0; d < 3; ++d) r->Fg[3 * i + d] = F[d];
+}
+
+// nbody_step! (src/nbody.jl:24-104): SSP-RK3 of the BHs with frozen gas force
+__device__ void nbody_rhs(double (*dp)[3], double (*dv)[3], const bsn_bh* b, int n, const double* Fg) {
+    for (int i = 0; i < n; ++i) {
+        for (int d = 0; d < 3; ++d) dp[i][d] = b[i].vel[d];
+        double a[3] = {Fg[3 * i] / b[i].mass, Fg[3 * i + 1] / b[i].mass, Fg[3 * i + 2] / b[i].mass};
+        for (int j = 0; j < n; ++j) {
+            if (j == i) continue;
+            double x = b[j].pos[0] - b[i].pos[0], y = b[j].pos[1] - b[i].pos[1], z = b[j].pos[2] - b[i].pos[2];
+            double r2 = x * x + y * y + z * z + b[j].eps * b[j].eps;
+            double r3 = r2 * sqrt(r2);
+            double fac = b[j].mass / r3;
+            a[0] = a[0] + fac * x; a[1] = a[1] + fac * y; a[2] = a[2] + fac * z;
+        }
+        for (int d = 0; d < 3; ++d) dv[i][d] = a[d];
+    }
+}
+
+__global__ void nbody_kernel(Dev* r) {
+    if (r->done || threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int n = r->nbh;
+    bsn_bh* b = r->bh;
+    bool ok = n > 0;
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) ok = ok && isfinite(b[i].pos[d]) && isfinite(b[i].vel[d]);
+    if (!ok) return;
+    const double dt = r->dt;
+    double p0[MAXBH][3], v0[MAXBH][3], p1[MAXBH][3], v1[MAXBH][3], p2[MAXBH][3], v2[MAXBH][3], DP[MAXBH][3],
+        DV[MAXBH][3];
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) { p0[i][d] = b[i].pos[d]; v0[i][d] = b[i].vel[d]; }
+    nbody_rhs(DP, DV, b, n, r->Fg);   // stage 1
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            p1[i][d] = p0[i][d] + dt * DP[i][d];
+            v1[i][d] = v0[i][d] + dt * DV[i][d];
+            b[i].pos[d] = p1[i][d]; b[i].vel[d] = v1[i][d];
+        }
+    nbody_rhs(DP, DV, b, n, r->Fg);   // stage 2
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            p2[i][d] = 0.75 * p0[i][d] + 0.25 * (p1[i][d] + dt * DP[i][d]);
+            v2[i][d] = 0.75 * v0[i][d] + 0.25 * (v1[i][d] + dt * DV[i][d]);
+        }
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) { b[i].pos[d] = p2[i][d]; b[i].vel[d] = v2[i][d]; }
+    nbody_rhs(DP, DV, b, n, r->Fg);   // stage 3
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            b[i].pos[d] = (1.0 / 3.0) * p0[i][d] + (2.0 / 3.0) * (p2[i][d] + dt * DP[i][d]);
+            b[i].vel[d] = (1.0 / 3.0) * v0[i][d] + (2.0 / 3.0) * (v2[i][d] + dt * DV[i][d]);
+        }
+}
+
+// r_sink, t_sink (src/BinarySupernova.jl:159-171)
+__device__ __forceinline__ double r_sink(const bsn_bh& b) { return jmax(6.0 * b.mass / (b.c_code * b.c_code), b.r_floor); }
+__device__ __forceinline__ double t_sink(const bsn_bh& b, double f_sink) {
+    double rs = r_sink(b);
+    double v_ff = sqrt(2.0 * b.mass / rs);
+    return f_sink * rs / v_ff;
+}
+
+// the stage sources of the step from the (updated) BHs: gravity of all,
+// sinks of the first BH before t_bh2_sink_on and of all after
+__global__ void fill_kernel(Dev* r, double f_sink, int torque_free, double rho_min, double t_bh2_sink_on) {
+    if (r->done || threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int n = r->nbh;
+    const int ns = (r->t < t_bh2_sink_on) ? (n < 1 ? n : 1) : n;
+    f64::BHSrc& B = r->bsrc;
+    f64::SinkSrc& S = r->ssrc;
+    B.n = n;
+    S.n = ns; S.torque_free = torque_free ? 1 : 0; S.rho_min = rho_min;
+    for (int i = 0; i < MAXBH; ++i) {
+        const bool on = i < n;
+        B.px[i] = on ? r->bh[i].pos[0] : 0.0; B.py[i] = on ? r->bh[i].pos[1] : 0.0; B.pz[i] = on ? r->bh[i].pos[2] : 0.0;
+        B.mass[i] = on ? r->bh[i].mass : 0.0; B.eps[i] = on ? r->bh[i].eps : 0.0;
+        const bool sk = i < ns;
+        S.px[i] = sk ? r->bh[i].pos[0] : 0.0; S.py[i] = sk ? r->bh[i].pos[1] : 0.0; S.pz[i] = sk ? r->bh[i].pos[2] : 0.0;
+        S.vx[i] = sk ? r->bh[i].vel[0] : 0.0; S.vy[i] = sk ? r->bh[i].vel[1] : 0.0; S.vz[i] = sk ? r->bh[i].vel[2] : 0.0;
+        S.rs[i] = sk ? r_sink(r->bh[i]) : 0.0; S.ts[i] = sk ? t_sink(r->bh[i], f_sink) : 0.0;
+    }
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// accrete! (src/sinks.jl:74-109) for sink i from the end-of-step state, summed
+// in the reference's (k, j, i) order over the sphere's index box, one thread
+__global__ void accrete_kernel(const double* U, int nx, int ny, int nz, double dx, double dy, double dz, double x0,
+                               double y0, double z0, Dev* r, int i, double f_sink, double rho_min) {
+    if (r->done || threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (i >= r->ssrc.n) return;
+    bsn_bh& bh = r->bh[i];
+    const double rs = r_sink(bh), ts = t_sink(bh, f_sink);
+    const double dV = dx * dy * dz;
+    const double rate = dV / ts * r->dt;
+    int ilo = clampi((int)floor((bh.pos[0] - rs - x0) / dx) - 2, 0, nx - 1);
+    int ihi = clampi((int)ceil((bh.pos[0] + rs - x0) / dx) + 2, 0, nx - 1);
+    int jlo = clampi((int)floor((bh.pos[1] - rs - y0) / dy) - 2, 0, ny - 1);
+    int jhi = clampi((int)ceil((bh.pos[1] + rs - y0) / dy) + 2, 0, ny - 1);
+    int klo = clampi((int)floor((bh.pos[2] - rs - z0) / dz) - 2, 0, nz - 1);
+    int khi = clampi((int)ceil((bh.pos[2] + rs - z0) / dz) + 2, 0, nz - 1);
+    if (!isfinite(rs) || !isfinite(bh.pos[0]) || !isfinite(bh.pos[1]) || !isfinite(bh.pos[2])) {
+        ilo = 0; ihi = nx - 1; jlo = 0; jhi = ny - 1; klo = 0; khi = nz - 1;
+    }
+    Geom G(nx, ny, nz);
+    double dm = 0.0, dPx = 0.0, dPy = 0.0, dPz = 0.0;
+    for (int c = klo; c <= khi; ++c)
+        for (int b = jlo; b <= jhi; ++b)
+            for (int a = ilo; a <= ihi; ++a) {
+                double xc, yc, zc;
+                f64::cell_xyz(a, b, c, x0, y0, z0, dx, dy, dz, xc, yc, zc);
+                double rr = sqrt(sq(xc - bh.pos[0]) + sq(yc - bh.pos[1]) + sq(zc - bh.pos[2]));
+                if (rr >= rs) continue;
+                long long o = G.act(a, b, c);
+                if (U[o] <= rho_min) continue;
+                dm += U[o] * rate;
+                dPx += U[o + 1] * rate;
+                dPy += U[o + 2] * rate;
+                dPz += U[o + 3] * rate;
+            }
+    if (dm > 0.0) {
+        double M_new = bh.mass + dm;
+        bh.vel[0] = (bh.mass * bh.vel[0] + dPx) / M_new;
+        bh.vel[1] = (bh.mass * bh.vel[1] + dPy) / M_new;
+        bh.vel[2] = (bh.mass * bh.vel[2] + dPz) / M_new;
+        bh.mass = M_new;
+    }
+}
+
+struct State {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;
+    // key of the captured graph
+    double* U = nullptr;
+    int nx = 0, ny = 0, nz = 0, nbh = -1, prec = -1, variant = -1, sg = 0, torque_free = 0, evolve = 0;
+    double dx = 0, x0 = 0, y0 = 0, z0 = 0, gamma = 0, cfl = 0, dt_max = 0, f_sink = 0, rho_floor = 0, P_floor = 0,
+           t_on = 0, rho_min = 0, t_end = 0;
+    const void* ptrs[5] = {};
+    cudaStream_t cap = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+};
+
+}  // namespace crun
+
+void coupled_run_state_free(bsn_ctx* ctx) {
+    if (!ctx->coupled_run_state) return;
+    crun::State* S = (crun::State*)ctx->coupled_run_state;
+    S->release();
+    if (S->cap) cudaStreamDestroy(S->cap);
+    for (cudaEvent_t e : S->ev)
+        if (e) cudaEventDestroy(e);
+    delete S;
+    ctx->coupled_run_state = nullptr;
+}
+
+}  // namespace bsn
+
+using namespace bsn;
+using namespace bsn::crun;
+
+extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs, int nbh, int nx, int ny, int nz,
+                                            double dx, double x0, double y0, double z0, double gamma, double cfl,
+                                            double dt_max, double f_sink, double rho_floor, double P_floor,
+                                            int torque_free, int self_gravity, double t_bh2_sink_on,
+                                            double rho_sink_min, int evolve_orbit, int precision, int n_steps,
+                                            double t_end, double* t_inout, int* steps_done) {
+    if (!ctx) return BSN_ERR_ARG;
+    BSN_TRY(check_dims(ctx, nx, ny, nz));
+    if (!U || !t_inout || (nbh > 0 && !bhs)) return set_err(ctx, BSN_ERR_ARG, "null argument");
+    if (nbh < 0 || nbh > MAXBH) return set_err(ctx, BSN_ERR_UNSUPPORTED, "at most %d black holes", MAXBH);
+    if (n_steps < 0) return set_err(ctx, BSN_ERR_ARG, "n_steps < 0");
+    if (precision != PREC_F64 && precision != PREC_F32 && precision != PREC_LEARNED)
+        return set_err(ctx, BSN_ERR_ARG, "bad precision %d", precision);
+    Geom G(nx, ny, nz);
+    size_t bytes = sizeof(double) * (size_t)G.nelem();
+    bsn_status st;
+    double* A = (double*)slot(ctx, SLOT_A, bytes, &st); BSN_TRY(st);
+    double* B = (double*)slot(ctx, SLOT_B, bytes, &st); BSN_TRY(st);
+    Dev* r = (Dev*)slot(ctx, SLOT_CRUN, sizeof(Dev), &st); BSN_TRY(st);
+    const int blocks = 148 * 4;
+    double* part = (double*)slot(ctx, SLOT_CRED, sizeof(double) * 6 * blocks, &st); BSN_TRY(st);
+    double* phi = nullptr;
+    if (self_gravity) {
+        phi = (double*)slot(ctx, SLOT_PHI, sizeof(double) * (size_t)nx * ny * nz, &st); BSN_TRY(st);
+        if (precision == PREC_F64) BSN_TRY(poisson_prepare(ctx, nx, ny, nz, dx, dx, dx));
+        else BSN_TRY(poisson_prepare_f32(ctx, nx, ny, nz, dx, dx, dx));
+    }
+
+    f64::StageArgs base;
+    stage_args_init(base, nx, ny, nz, dx, dx, dx, gamma, BSN_BC_OUTFLOW, rho_floor, P_floor);
+    base.x0 = x0; base.y0 = y0; base.z0 = z0;
+    base.Uin = U; base.Un = U;
+    {
+        double* scratch = (double*)slot(ctx, SLOT_UN, bytes, &st); BSN_TRY(st);
+        BSN_TRY(stage_autotune(ctx, precision, base, scratch));
+    }
+    const int variant = ctx->tile_choice[std::make_tuple(precision, nx, ny, nz)];
+
+    // BHs to the device (through the context's pinned buffer, sized once for the
+    // whole call: BH staging now, the step counters and flags later), initial CFL fold
+    double* h = (double*)pinned(ctx, sizeof(Dev) + 128, &st); BSN_TRY(st);
+    bsn_bh* hb = (bsn_bh*)h;
+    for (int i = 0; i < nbh; ++i) hb[i] = bhs[i];
+    bsn_bh* db = (bsn_bh*)part;   // staging for the initial BHs (overwritten by the step's reductions)
+    BSN_CUDA(ctx, cudaMemcpyAsync(db, hb, sizeof(bsn_bh) * (nbh > 0 ? nbh : 1), cudaMemcpyHostToDevice, ctx->stream));
+    init_kernel<<<1, 1, 0, ctx->stream>>>(r, *t_inout, db, nbh);
+    BSN_TRY(launch_check(ctx, "coupled_init_kernel"));
+    BSN_TRY(f64_cfl_fold(ctx, U, nx, ny, nz, dx, dx, dx, gamma, &r->smax, &r->nanflag));
+
+    if (!ctx->coupled_run_state) ctx->coupled_run_state = new State();
+    State* S = (State*)ctx->coupled_run_state;
+    const void* ptrs[5] = {A, B, r, part, phi};
+    bool same = S->exec && S->U == U && S->nx == nx && S->ny == ny && S->nz == nz && S->nbh == nbh &&
+                S->prec == precision && S->variant == variant && S->sg == self_gravity &&
+                S->torque_free == torque_free && S->evolve == evolve_orbit && S->dx == dx && S->x0 == x0 &&
+                S->y0 == y0 && S->z0 == z0 && S->gamma == gamma && S->cfl == cfl && S->dt_max == dt_max &&
+                S->f_sink == f_sink && S->rho_floor == rho_floor && S->P_floor == P_floor &&
+                S->t_on == t_bh2_sink_on && S->rho_min == rho_sink_min && S->t_end == t_end &&
+                memcmp(S->ptrs, ptrs, sizeof(ptrs)) == 0;
+    if (!same) {
+        S->release();
+        if (!S->cap) BSN_CUDA(ctx, cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
+        bool prof = ctx->profiling;
+        ctx->profiling = false;
+        long long l0 = ctx->launches;
+        cudaStream_t user = ctx->stream;
+        ctx->stream = S->cap;
+        cudaError_t be = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (be != cudaSuccess) { ctx->stream = user; ctx->profiling = prof; return cuda_check(ctx, be, "cudaStreamBeginCapture"); }
+        auto body = [&]() -> bsn_status {
+            dt_kernel<<<1, 1, 0, ctx->stream>>>(r, cfl, t_end, dt_max);
+            BSN_TRY(launch_check(ctx, "coupled_dt_kernel"));
+            // gas force on every BH from the start-of-step state, then the orbit
+            for (int i = 0; i < nbh; ++i) {
+                gas_force_kernel<<<blocks, 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dx, dx, x0, y0, z0, r, i, part);
+                BSN_TRY(launch_check(ctx, "coupled_gas_force_kernel"));
+                gas_force_finish<<<1, 32, 0, ctx->stream>>>(part, blocks, r, i);
+                BSN_TRY(launch_check(ctx, "coupled_gas_force_finish"));
+            }
+            if (evolve_orbit && nbh > 0) {
+                nbody_kernel<<<1, 32, 0, ctx->stream>>>(r);
+                BSN_TRY(launch_check(ctx, "coupled_nbody_kernel"));
+            }
+            fill_kernel<<<1, 32, 0, ctx->stream>>>(r, f_sink, torque_free, rho_sink_min, t_bh2_sink_on);
+            BSN_TRY(launch_check(ctx, "coupled_fill_kernel"));
+            // SSP-RK3 with the sources in the driver's order (stage epilogue)
+            double* in[3] = {U, A, B};
+            double* out[3] = {A, B, U};
+            for (int s = 0; s < 3; ++s) {
+                f64::StageArgs a = base;
+                a.Uin = in[s]; a.Un = U; a.Uout = out[s]; a.mode = 0;
+                set_stage(a, s + 1, 0.0);
+                a.dt_dev = &r->dt;
+                a.done_dev = &r->done;
+                if (nbh > 0) { a.use_bh = 1; a.bh_dev = &r->bsrc; a.use_sink = 1; a.sk_dev = &r->ssrc; }
+                if (self_gravity) {
+                    if (precision == PREC_F64) BSN_TRY(poisson_from_state(ctx, in[s], nx, ny, nz, dx, dx, dx, rho_floor, phi));
+                    else BSN_TRY(poisson_from_state_f32(ctx, in[s], nx, ny, nz, dx, dx, dx, rho_floor, phi));
+                    a.phi = phi; a.use_sg = 1;
+                }
+                if (s == 2) { a.cfl_max = &r->smax; a.cfl_nan = &r->nanflag; }
+                BSN_TRY(stage_launch(ctx, precision, a));
+            }
+            BSN_TRY(f64_ghost_combine(ctx, U, B, nullptr, nx, ny, nz, BSN_BC_OUTFLOW, 0.0, &r->dt, &r->done));
+            for (int i = 0; i < nbh; ++i) {
+                accrete_kernel<<<1, 32, 0, ctx->stream>>>(U, nx, ny, nz, dx, dx, dx, x0, y0, z0, r, i, f_sink,
+                                                          rho_sink_min);
+                BSN_TRY(launch_check(ctx, "coupled_accrete_kernel"));
+            }
+            advance_kernel<<<1, 1, 0, ctx->stream>>>(r);
+            return launch_check(ctx, "coupled_advance_kernel");
+        };
+        bsn_status cst = body();
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        ctx->stream = user;
+        ctx->profiling = prof;
+        S->kernels = (int)(ctx->launches - l0);
+        ctx->launches = l0;
+        if (cst != BSN_OK) { if (graph) cudaGraphDestroy(graph); return cst; }
+        BSN_CUDA(ctx, e);
+        S->graph = graph;
+        BSN_CUDA(ctx, cudaGraphInstantiate(&S->exec, graph, 0));
+        S->U = U; S->nx = nx; S->ny = ny; S->nz = nz; S->nbh = nbh; S->prec = precision; S->variant = variant;
+        S->sg = self_gravity; S->torque_free = torque_free; S->evolve = evolve_orbit; S->dx = dx; S->x0 = x0;
+        S->y0 = y0; S->z0 = z0; S->gamma = gamma; S->cfl = cfl; S->dt_max = dt_max; S->f_sink = f_sink;
+        S->rho_floor = rho_floor; S->P_floor = P_floor; S->t_on = t_bh2_sink_on; S->rho_min = rho_sink_min;
+        S->t_end = t_end;
+        memcpy(S->ptrs, ptrs, sizeof(ptrs));
+    }
+    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps, t_end > 0.0, &r->done, S->ev,
+                         (volatile int*)((char*)h + sizeof(Dev))));
+    BSN_CUDA(ctx, cudaMemcpyAsync(h, r, sizeof(Dev), cudaMemcpyDeviceToHost, ctx->stream));
+    BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    Dev d;
+    memcpy(&d, h, sizeof(Dev));
+    *t_inout = d.t;
+    if (steps_done) *steps_done = d.steps;
+    for (int i = 0; i < nbh; ++i) bhs[i] = d.bh[i];
+    if (d.done == 2)
+        return set_err(ctx, BSN_ERR_NONFINITE, "time step collapsed to 0 at t = %.17g (infinite signal speed)", d.t);
+    return BSN_OK;
+}

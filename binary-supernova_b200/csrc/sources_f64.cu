@@ -9,12 +9,6 @@
 namespace bsn {
 namespace f64 {
 
-__device__ __forceinline__ void cell_xyz(int a, int b, int c, double x0, double y0, double z0, double dx, double dy,
-                                         double dz, double& xc, double& yc, double& zc) {
-    xc = x0 + ((double)(a + 1) - 0.5) * dx;
-    yc = y0 + ((double)(b + 1) - 0.5) * dy;
-    zc = z0 + ((double)(c + 1) - 0.5) * dz;
-}
 
 // add_bh_gravity_source! (src/gpu_kernels.jl:199-230)
 __global__ void bh_gravity_kernel(double* dU, const double* U, int nx, int ny, int nz, double dx, double dy,

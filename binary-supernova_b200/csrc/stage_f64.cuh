@@ -62,7 +62,18 @@ struct StageArgs {
     const double* dt_dev;    // non-null: dt read on the device (graph-captured time loop)
     const int* done_dev;     // non-null and *done_dev != 0: the device time loop has finished
     const void* mlp;         // learned stencil path: packed network parameters
+    const BHSrc* bh_dev;     // non-null: gravity sources read on the device (device-resident driver loop)
+    const SinkSrc* sk_dev;   // non-null: sink sources read on the device
 };
+
+// Centre of active cell (a, b, c) (0-based): x0 + (i - ng - 0.5) dx with
+// i = a + 1 + ng (src/gravity_bh.jl:63-65).
+__device__ __forceinline__ void cell_xyz(int a, int b, int c, double x0, double y0, double z0, double dx, double dy,
+                                         double dz, double& xc, double& yc, double& zc) {
+    xc = x0 + ((double)(a + 1) - 0.5) * dx;
+    yc = y0 + ((double)(b + 1) - 0.5) * dy;
+    zc = z0 + ((double)(c + 1) - 0.5) * dz;
+}
 
 // Several grids (mesh levels, patches of any size) updated by one launch:
 // level l's blocks are entries [start[l], start[l+1]) of one block list,

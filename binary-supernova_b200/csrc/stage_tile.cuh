@@ -348,6 +348,8 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
     sweep<P, TX, TY, TZ, NT, 2>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
 
     const double dt = A.dt_dev ? *A.dt_dev : A.dt;
+    const f64::BHSrc& BH = A.bh_dev ? *A.bh_dev : A.bh;     // kernel parameters are __grid_constant__
+    const f64::SinkSrc& SK = A.sk_dev ? *A.sk_dev : A.sk;
     const double cdt = A.stage == 2 ? 0.25 * dt : (A.stage == 3 ? (2.0 / 3.0) * dt : dt);
     double smax = 0.0;
 #pragma unroll
@@ -375,11 +377,11 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
         if (A.use_bh) {   // src/gpu_kernels.jl:199-230
             double vx = u1 / u0, vy = u2 / u0, vz = u3 / u0;
             double ax = 0.0, ay = 0.0, az = 0.0;
-            for (int nb = 0; nb < A.bh.n; ++nb) {
-                double ddx = xc - A.bh.px[nb], ddy = yc - A.bh.py[nb], ddz = zc - A.bh.pz[nb];
-                double r2 = sq(ddx) + sq(ddy) + sq(ddz) + sq(A.bh.eps[nb]);
+            for (int nb = 0; nb < BH.n; ++nb) {
+                double ddx = xc - BH.px[nb], ddy = yc - BH.py[nb], ddz = zc - BH.pz[nb];
+                double r2 = sq(ddx) + sq(ddy) + sq(ddz) + sq(BH.eps[nb]);
                 double r3 = r2 * sqrt(r2);
-                double fac = -A.bh.mass[nb] / r3;
+                double fac = -BH.mass[nb] / r3;
                 ax += fac * ddx; ay += fac * ddy; az += fac * ddz;
             }
             d[1] += u0 * ax; d[2] += u0 * ay; d[3] += u0 * az;
@@ -401,17 +403,17 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
             double vdotg = (u1 * gx + u2 * gy + u3 * gz) / u0;
             d[1] -= u0 * gx; d[2] -= u0 * gy; d[3] -= u0 * gz; d[4] -= u0 * vdotg;
         }
-        if (A.use_sink && u0 > A.sk.rho_min) {   // src/gpu_kernels.jl:238-284
-            for (int nb = 0; nb < A.sk.n; ++nb) {
-                double ddx = xc - A.sk.px[nb], ddy = yc - A.sk.py[nb], ddz = zc - A.sk.pz[nb];
+        if (A.use_sink && u0 > SK.rho_min) {   // src/gpu_kernels.jl:238-284
+            for (int nb = 0; nb < SK.n; ++nb) {
+                double ddx = xc - SK.px[nb], ddy = yc - SK.py[nb], ddz = zc - SK.pz[nb];
                 double rr = sqrt(sq(ddx) + sq(ddy) + sq(ddz));
-                if (rr < A.sk.rs[nb]) {
-                    double ts = A.sk.ts[nb];
+                if (rr < SK.rs[nb]) {
+                    double ts = SK.ts[nb];
                     d[0] -= u0 / ts;
-                    if (A.sk.torque_free) {
+                    if (SK.torque_free) {
                         double rx = ddx / rr, ry = ddy / rr, rz = ddz / rr;
                         double vx = u1 / u0, vy = u2 / u0, vz = u3 / u0;
-                        double vrx = vx - A.sk.vx[nb], vry = vy - A.sk.vy[nb], vrz = vz - A.sk.vz[nb];
+                        double vrx = vx - SK.vx[nb], vry = vy - SK.vy[nb], vrz = vz - SK.vz[nb];
                         double v_r = vrx * rx + vry * ry + vrz * rz;
                         double e_int = u4 / u0 - 0.5 * (sq(vx) + sq(vy) + sq(vz));
                         d[1] -= u0 * v_r * rx / ts;
@@ -468,7 +470,7 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
 
 // One launch per stage on one grid: CTA (x, y, z) owns block (x, y, z).
 template <class P, int TX, int TY, int TZ, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) stage_kernel(f64::StageArgs A) {
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__ f64::StageArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[NT / 32];
     __shared__ unsigned int nanflag;

@@ -249,6 +249,19 @@ bsn_status bsn_coupled_step_f64(bsn_ctx* ctx, double* U, bsn_bh* bhs, int nbh, d
                                 double gamma, double f_sink, double rho_floor, double P_floor,
                                 int torque_free, int self_gravity, double t_bh2_sink_on,
                                 double rho_sink_min, int evolve_orbit, double* Fgas_out);
+/* The driver loop around coupled_step! on the device: up to n_steps steps of
+ * dt = min(CFL dt, dt_max if > 0, t_end - t if t_end > 0) then coupled_step!,
+ * with the BHs, t and dt in device memory (gas forces, nbody_step!, source
+ * parameters and accrete! computed there) and each step one CUDA graph.
+ * bhs: host in/out.  precision: BSN_PREC_* stencils (sources, orbits and
+ * accretion FP64); FP32 transforms for self-gravity unless BSN_PREC_F64.
+ * *t_inout: start time in, final out; *steps_done (may be NULL). */
+bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs, int nbh, int nx, int ny, int nz,
+                                 double dx, double x0, double y0, double z0, double gamma, double cfl,
+                                 double dt_max, double f_sink, double rho_floor, double P_floor,
+                                 int torque_free, int self_gravity, double t_bh2_sink_on,
+                                 double rho_sink_min, int evolve_orbit, int precision, int n_steps,
+                                 double t_end, double* t_inout, int* steps_done);
 
 /* ---- src/fmr3d.jl ----------------------------------------------------------- */
 /* FMRGrid3D constructor's _prolong_all! (src/fmr3d.jl:131-151, 206-214) */

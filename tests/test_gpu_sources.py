@@ -181,3 +181,66 @@ def test_coupled_step_live_orbit(orc, bsn, self_gravity):
         for i in range(2):
             assert abs(bg[i].mass - bo[i].mass) <= 1e-13 * bo[i].mass
             assert np.allclose(list(bg[i].pos), list(bo[i].pos), rtol=0, atol=1e-13)
+
+
+def _reference_coupled_loop(orc, U, bo, dx, x0, steps, evolve, self_gravity, ton=0.0):
+    t = 0.0
+    for _ in range(steps):
+        dt = orc.cfl_dt_3d(U, dx, dx, dx, 4 / 3, 0.4)
+        orc.coupled_step(U, bo, 2, dt, t, dx, x0, x0, x0, 4 / 3, 1.0, 1e-8, 1e-10, True, self_gravity, ton, 2e-8,
+                         evolve_orbit=evolve)
+        t += dt
+    return t
+
+
+@pytest.mark.parametrize("ton", [0.0, 1e9])
+def test_coupled_run_steps_static_bhs_bitwise(orc, bsn, ton):
+    """The device-resident coupled loop (dt on the device, one graph per step)
+    against the reference driver loop: bit-identical state, BH masses and
+    velocities with the orbit frozen (accretion still changes them)."""
+    U, dx, x0, specs = binary_setup(orc, n=32)
+    Ud = dev(U)
+    bg, bo = _bhs(bsn, specs), orc.bh_array(_obhs(orc, specs))
+    t_ref = _reference_coupled_loop(orc, U, bo, dx, x0, 3, False, False, ton)
+    t, n = bsn.coupled_run_steps(Ud, bg, 32, 32, 32, dx, x0, x0, x0, 4 / 3, 0.4, n_steps=3, f_sink=1.0,
+                                 rho_floor=1e-8, P_floor=1e-10, torque_free=True, t_bh2_sink_on=ton,
+                                 rho_sink_min=2e-8, evolve_orbit=False)
+    assert n == 3 and t == t_ref
+    assert_bitwise(host(Ud), U, "coupled loop U")
+    for i in range(2):
+        assert bg[i].mass == bo[i].mass and list(bg[i].vel) == list(bo[i].vel) and list(bg[i].pos) == list(bo[i].pos)
+
+
+@pytest.mark.parametrize("self_gravity", [False, True])
+def test_coupled_run_steps_live_orbit(orc, bsn, self_gravity):
+    """Live N-body orbit on the device: within the whole-grid gas-force
+    summation's rounding of the reference driver loop (as the single step)."""
+    U, dx, x0, specs = binary_setup(orc, n=32)
+    Ud = dev(U)
+    bg, bo = _bhs(bsn, specs), orc.bh_array(_obhs(orc, specs))
+    t_ref = _reference_coupled_loop(orc, U, bo, dx, x0, 2, True, self_gravity)
+    t, n = bsn.coupled_run_steps(Ud, bg, 32, 32, 32, dx, x0, x0, x0, 4 / 3, 0.4, n_steps=2, f_sink=1.0,
+                                 rho_floor=1e-8, P_floor=1e-10, torque_free=True, self_gravity=self_gravity,
+                                 rho_sink_min=2e-8, evolve_orbit=True)
+    assert n == 2 and abs(t - t_ref) <= 1e-12 * t_ref
+    G = host(Ud)
+    for q in range(5):
+        assert np.abs(G[q] - U[q]).max() <= TOL * np.abs(U[q]).max(), q
+    for i in range(2):
+        assert abs(bg[i].mass - bo[i].mass) <= 1e-13 * bo[i].mass
+        assert np.allclose(list(bg[i].pos), list(bo[i].pos), rtol=0, atol=1e-13)
+
+
+def test_coupled_run_steps_t_end_and_fp32(orc, bsn):
+    """t_end stops the loop exactly; FP32 stencils stay close to FP64."""
+    U, dx, x0, specs = binary_setup(orc, n=32)
+    U64, U32 = dev(U), dev(U)
+    b64, b32 = _bhs(bsn, specs), _bhs(bsn, specs)
+    t_end = 2.5 * orc.cfl_dt_3d(U, dx, dx, dx, 4 / 3, 0.4)
+    kw = dict(n_steps=1000, t_end=t_end, f_sink=1.0, rho_floor=1e-8, P_floor=1e-10, rho_sink_min=2e-8)
+    t64, n64 = bsn.coupled_run_steps(U64, b64, 32, 32, 32, dx, x0, x0, x0, 4 / 3, 0.4, **kw)
+    t32, n32 = bsn.coupled_run_steps(U32, b32, 32, 32, 32, dx, x0, x0, x0, 4 / 3, 0.4, precision="f32", **kw)
+    assert t64 == t_end and t32 == t_end and n64 >= 3
+    a = (0,) + (slice(NG, -NG),) * 3
+    A, B = host(U32)[a], host(U64)[a]
+    assert np.abs(A - B).sum() / np.abs(B).sum() < 1e-5
