@@ -288,19 +288,34 @@ def coupled_step(U, bhs, dt, t, nx, ny, nz, dx, x0, y0, z0, gamma, f_sink, rho_f
 
 def coupled_run_steps(U, bhs, nx, ny, nz, dx, x0, y0, z0, gamma, cfl, *, n_steps, t=0.0, t_end=0.0, dt_max=0.0,
                       f_sink=1.0, rho_floor=0.0, P_floor=0.0, torque_free=True, self_gravity=False,
-                      t_bh2_sink_on=0.0, rho_sink_min=0.0, evolve_orbit=True, precision="f64"):
+                      t_bh2_sink_on=0.0, rho_sink_min=0.0, evolve_orbit=True, precision="f64", diag=None):
     """The coupled_step! driver loop on the device (one CUDA graph per step);
-    returns (t, steps) and updates `bhs` in place."""
+    returns (t, steps) and updates `bhs` in place.  diag: optional CUDA float64
+    tensor (cap, 12) receiving {t, dt, diagnostics(...)} after every step."""
     _check_state(U, nx, ny, nz)
+    if diag is not None and not (diag.is_cuda and diag.dtype == torch.float64 and diag.is_contiguous()
+                                 and diag.dim() == 2 and diag.shape[1] == 12):
+        raise TypeError("diag must be a contiguous CUDA float64 tensor of shape (cap, 12)")
     arr = _bh_array(bhs)
     tt = C.c_double(float(t))
     nd = C.c_int(0)
     _call("bsn_coupled_run_steps", context(), _ptr(U), arr, len(bhs), nx, ny, nz, float(dx), float(x0), float(y0),
           float(z0), float(gamma), float(cfl), float(dt_max), float(f_sink), float(rho_floor), float(P_floor),
           int(bool(torque_free)), int(bool(self_gravity)), float(t_bh2_sink_on), float(rho_sink_min),
-          int(bool(evolve_orbit)), PREC[precision], int(n_steps), float(t_end), C.byref(tt), C.byref(nd))
+          int(bool(evolve_orbit)), PREC[precision], int(n_steps), float(t_end), C.byref(tt), C.byref(nd),
+          _ptr(diag) if diag is not None else None, int(diag.shape[0]) if diag is not None else 0)
     _bh_writeback(bhs, arr)
     return tt.value, nd.value
+
+
+def diagnostics(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, bhs, gamma) -> np.ndarray:
+    """src/diagnostics.jl totals: (E_gas, KE_gas, Px, Py, Pz, Lx, Ly, Lz, M_bound, M_gas)."""
+    _check_state(U, nx, ny, nz)
+    arr = _bh_array(bhs)
+    out = (C.c_double * 10)()
+    _call("bsn_diagnostics_f64", context(), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz), float(x0),
+          float(y0), float(z0), arr, len(bhs), float(gamma), out)
+    return np.array(out[:])
 
 
 # ---------------------------------------------------------------------------
@@ -423,5 +438,5 @@ def set_profiling(on: bool):
     _call("bsn_ctx_set_profiling", context(), int(bool(on)))
 
 
-__all__ += ["euler3d_step_f32", "euler3d_step_learned", "run_steps", "fmr3d_run_steps", "coupled_run_steps", "tile_variants", "set_tile", "get_tile", "kernel_time",
+__all__ += ["euler3d_step_f32", "euler3d_step_learned", "run_steps", "fmr3d_run_steps", "coupled_run_steps", "diagnostics", "tile_variants", "set_tile", "get_tile", "kernel_time",
             "set_profiling", "PREC"]

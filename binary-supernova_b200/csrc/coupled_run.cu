@@ -10,6 +10,7 @@
 #include <cstring>
 
 #include "hydro_f64.cuh"
+#include "diagnostics.cuh"
 #include "poisson.cuh"
 #include "stage_launch.cuh"
 
@@ -265,7 +266,8 @@ struct State {
     int nx = 0, ny = 0, nz = 0, nbh = -1, prec = -1, variant = -1, sg = 0, torque_free = 0, evolve = 0;
     double dx = 0, x0 = 0, y0 = 0, z0 = 0, gamma = 0, cfl = 0, dt_max = 0, f_sink = 0, rho_floor = 0, P_floor = 0,
            t_on = 0, rho_min = 0, t_end = 0;
-    const void* ptrs[5] = {};
+    const void* ptrs[7] = {};
+    int diag_cap = 0;
     cudaStream_t cap = nullptr;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     void release() {
@@ -299,12 +301,15 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
                                             double dt_max, double f_sink, double rho_floor, double P_floor,
                                             int torque_free, int self_gravity, double t_bh2_sink_on,
                                             double rho_sink_min, int evolve_orbit, int precision, int n_steps,
-                                            double t_end, double* t_inout, int* steps_done) {
+                                            double t_end, double* t_inout, int* steps_done, double* diag_out,
+                                            int diag_cap) {
     if (!ctx) return BSN_ERR_ARG;
     BSN_TRY(check_dims(ctx, nx, ny, nz));
     if (!U || !t_inout || (nbh > 0 && !bhs)) return set_err(ctx, BSN_ERR_ARG, "null argument");
     if (nbh < 0 || nbh > MAXBH) return set_err(ctx, BSN_ERR_UNSUPPORTED, "at most %d black holes", MAXBH);
     if (n_steps < 0) return set_err(ctx, BSN_ERR_ARG, "n_steps < 0");
+    if (diag_out && diag_cap < 0) return set_err(ctx, BSN_ERR_ARG, "diag_cap < 0");
+    if (!diag_out) diag_cap = 0;
     if (precision != PREC_F64 && precision != PREC_F32 && precision != PREC_LEARNED)
         return set_err(ctx, BSN_ERR_ARG, "bad precision %d", precision);
     Geom G(nx, ny, nz);
@@ -315,6 +320,10 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
     Dev* r = (Dev*)slot(ctx, SLOT_CRUN, sizeof(Dev), &st); BSN_TRY(st);
     const int blocks = 148 * 4;
     double* part = (double*)slot(ctx, SLOT_CRED, sizeof(double) * 6 * blocks, &st); BSN_TRY(st);
+    double* dpart = nullptr;
+    if (diag_out) {
+        dpart = (double*)slot(ctx, SLOT_DIAGREC, sizeof(double) * 2 * diag::NDIAG * diag::BLOCKS, &st); BSN_TRY(st);
+    }
     double* phi = nullptr;
     if (self_gravity) {
         phi = (double*)slot(ctx, SLOT_PHI, sizeof(double) * (size_t)nx * ny * nz, &st); BSN_TRY(st);
@@ -345,14 +354,14 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
 
     if (!ctx->coupled_run_state) ctx->coupled_run_state = new State();
     State* S = (State*)ctx->coupled_run_state;
-    const void* ptrs[5] = {A, B, r, part, phi};
+    const void* ptrs[7] = {A, B, r, part, phi, diag_out, dpart};
     bool same = S->exec && S->U == U && S->nx == nx && S->ny == ny && S->nz == nz && S->nbh == nbh &&
                 S->prec == precision && S->variant == variant && S->sg == self_gravity &&
                 S->torque_free == torque_free && S->evolve == evolve_orbit && S->dx == dx && S->x0 == x0 &&
                 S->y0 == y0 && S->z0 == z0 && S->gamma == gamma && S->cfl == cfl && S->dt_max == dt_max &&
                 S->f_sink == f_sink && S->rho_floor == rho_floor && S->P_floor == P_floor &&
                 S->t_on == t_bh2_sink_on && S->rho_min == rho_sink_min && S->t_end == t_end &&
-                memcmp(S->ptrs, ptrs, sizeof(ptrs)) == 0;
+                S->diag_cap == diag_cap && memcmp(S->ptrs, ptrs, sizeof(ptrs)) == 0;
     if (!same) {
         S->release();
         if (!S->cap) BSN_CUDA(ctx, cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
@@ -404,7 +413,11 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
                 BSN_TRY(launch_check(ctx, "coupled_accrete_kernel"));
             }
             advance_kernel<<<1, 1, 0, ctx->stream>>>(r);
-            return launch_check(ctx, "coupled_advance_kernel");
+            BSN_TRY(launch_check(ctx, "coupled_advance_kernel"));
+            if (diag_out)   // the driver's diagnostics of the end-of-step state (BHs after accretion)
+                BSN_TRY(diag::launch(ctx, U, nx, ny, nz, dx, dx, dx, x0, y0, z0, r->bh, &r->nbh, nbh, gamma, dpart,
+                                     diag_out, &r->t, &r->dt, &r->steps, &r->done, diag_cap));
+            return BSN_OK;
         };
         bsn_status cst = body();
         cudaGraph_t graph = nullptr;
@@ -422,6 +435,7 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
         S->y0 = y0; S->z0 = z0; S->gamma = gamma; S->cfl = cfl; S->dt_max = dt_max; S->f_sink = f_sink;
         S->rho_floor = rho_floor; S->P_floor = P_floor; S->t_on = t_bh2_sink_on; S->rho_min = rho_sink_min;
         S->t_end = t_end;
+        S->diag_cap = diag_cap;
         memcpy(S->ptrs, ptrs, sizeof(ptrs));
     }
     BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps, t_end > 0.0, &r->done, S->ev,

@@ -255,13 +255,25 @@ bsn_status bsn_coupled_step_f64(bsn_ctx* ctx, double* U, bsn_bh* bhs, int nbh, d
  * parameters and accrete! computed there) and each step one CUDA graph.
  * bhs: host in/out.  precision: BSN_PREC_* stencils (sources, orbits and
  * accretion FP64); FP32 transforms for self-gravity unless BSN_PREC_F64.
- * *t_inout: start time in, final out; *steps_done (may be NULL). */
+ * *t_inout: start time in, final out; *steps_done (may be NULL).  diag_out
+ * (device, may be NULL): after every step k < diag_cap the record
+ * {t, dt, the 10 values of bsn_diagnostics_f64} at diag_out + 12 k, reduced
+ * on the device (no per-step copy to the host). */
 bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs, int nbh, int nx, int ny, int nz,
                                  double dx, double x0, double y0, double z0, double gamma, double cfl,
                                  double dt_max, double f_sink, double rho_floor, double P_floor,
                                  int torque_free, int self_gravity, double t_bh2_sink_on,
                                  double rho_sink_min, int evolve_orbit, int precision, int n_steps,
-                                 double t_end, double* t_inout, int* steps_done);
+                                 double t_end, double* t_inout, int* steps_done, double* diag_out,
+                                 int diag_cap);
+/* The driver's diagnostics (src/diagnostics.jl:21-175) in one device
+ * reduction: out[0] gas_energy_total, [1] gas_kinetic_total, [2..4]
+ * gas_momentum_total, [5..7] gas_angular_momentum_total, [8]
+ * bound_gas_mass(bhs, gamma), [9] the gas mass sum(rho) dV.  Whole-grid sums
+ * compensated (within about one rounding of the exact sum).  bhs: host. */
+bsn_status bsn_diagnostics_f64(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx,
+                               double dy, double dz, double x0, double y0, double z0,
+                               const bsn_bh* bhs, int nbh, double gamma, double out[10]);
 
 /* ---- src/fmr3d.jl ----------------------------------------------------------- */
 /* FMRGrid3D constructor's _prolong_all! (src/fmr3d.jl:131-151, 206-214) */

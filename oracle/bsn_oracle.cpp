@@ -1389,3 +1389,41 @@ extern "C" double orc_thermal_bomb(double* U, int nx, int ny, int nz, double dx,
             if (inside(i, j, k)) U[I(5, i, j, k)] += fac * U[I(1, i, j, k)];
     return M_bomb;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Diagnostics (src/diagnostics.jl): out[0] gas_energy_total (:21-26),
+ * out[1] gas_kinetic_total (:33-43), out[2..4] gas_momentum_total (:50-57),
+ * out[5..7] gas_angular_momentum_total (:65-87), out[8] bound_gas_mass
+ * (:127-175), out[9] gas mass sum rho dV.  The per-cell terms are the
+ * reference's; the whole-grid sums (Julia's `sum`, pairwise) are taken in
+ * long double so the restatement is within one rounding of the exact sum. */
+extern "C" void orc_diagnostics(const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                                double x0, double y0, double z0, const orc_bh* bhs, int nbh, double g,
+                                double out[10]) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    long double s[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = ng + 1; k <= ng + nz; ++k) for (int j = ng + 1; j <= ng + ny; ++j)
+        for (int i = ng + 1; i <= ng + nx; ++i) {
+            double r = U[I(1, i, j, k)], mx = U[I(2, i, j, k)], my = U[I(3, i, j, k)], mz = U[I(4, i, j, k)];
+            double E = U[I(5, i, j, k)];
+            double xc = x0 + ((double)(i - ng) - 0.5) * dx;
+            double yc = y0 + ((double)(j - ng) - 0.5) * dy;
+            double zc = z0 + ((double)(k - ng) - 0.5) * dz;
+            double rs = jmax(r, 1e-30);
+            double ke = 0.5 * (sq(mx) + sq(my) + sq(mz)) / rs;
+            s[0] += E; s[1] += ke; s[2] += mx; s[3] += my; s[4] += mz;
+            s[5] += yc * mz - zc * my; s[6] += zc * mx - xc * mz; s[7] += xc * my - yc * mx;
+            double P = jmax((g - 1.0) * (E - rs * ke), 0.0);
+            double eint = P / ((g - 1.0) * rs);
+            double phi = 0.0;
+            for (int b = 0; b < nbh; ++b)
+                phi -= bhs[b].mass / std::sqrt(sq(xc - bhs[b].pos[0]) + sq(yc - bhs[b].pos[1]) +
+                                               sq(zc - bhs[b].pos[2]) + sq(bhs[b].eps));
+            double etot = ke + eint + phi;
+            if (etot <= 0.0) s[8] += rs;
+            s[9] += r;
+        }
+    double dV = dx * dy * dz;
+    for (int q = 0; q < 10; ++q) out[q] = (double)s[q] * dV;
+}

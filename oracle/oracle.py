@@ -101,6 +101,7 @@ def _declare(L):
         "orc_lane_emden": (i, [d, d, P, P, P, i]),
         "orc_polytrope_ic_3d": (V, [P, i, i, i, d, d, d, d, d, d, d, d, d, d, d, d, d, d, d, P]),
         "orc_thermal_bomb": (d, [P, i, i, i] + [d] * 13),
+        "orc_diagnostics": (V, [P, i, i, i, d, d, d, d, d, d, C.POINTER(OrcBH), i, d, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -368,3 +369,12 @@ def sod_ic_3d(direction: str, n_normal=128, n_trans=4, gamma=1.4):
     U[(0,) + act] = np.broadcast_to(rho.reshape(shape), (nx, ny, nz))
     U[(4,) + act] = np.broadcast_to(E.reshape(shape), (nx, ny, nz))
     return U, (nx, ny, nz), (dx, dy, dz)
+
+
+def diagnostics(U, dx, dy, dz, x0, y0, z0, bhs, gamma):
+    """src/diagnostics.jl: (E_gas, KE_gas, Px, Py, Pz, Lx, Ly, Lz, M_bound, M_gas)."""
+    out = np.zeros(10)
+    arr = bh_array(bhs)
+    lib().orc_diagnostics(_p(U), *dims(U), dx, dy, dz, x0, y0, z0, arr, len(bhs), gamma,
+                          out.ctypes.data_as(_dp))
+    return out

@@ -244,3 +244,51 @@ def test_coupled_run_steps_t_end_and_fp32(orc, bsn):
     a = (0,) + (slice(NG, -NG),) * 3
     A, B = host(U32)[a], host(U64)[a]
     assert np.abs(A - B).sum() / np.abs(B).sum() < 1e-5
+
+
+def test_diagnostics_device_reduction(orc, bsn):
+    """bsn_diagnostics_f64 (one compensated device reduction) against the
+    oracle's restatement of src/diagnostics.jl, within 1e-13 of the sum of
+    magnitudes."""
+    U, dx, x0, specs = binary_setup(orc, n=32)
+    t = 0.0
+    bo = orc.bh_array(_obhs(orc, specs))
+    dt = orc.cfl_dt_3d(U, dx, dx, dx, 4 / 3, 0.4)
+    orc.coupled_step(U, bo, 2, dt, t, dx, x0, x0, x0, 4 / 3, 1.0, 1e-8, 1e-10, True, False, 0.0, 2e-8,
+                     evolve_orbit=True)   # a state with motion
+    obhs = [bo[i] for i in range(2)]
+    gbhs = [bsn.BlackHole(list(b.pos), list(b.vel), b.mass, b.eps, b.c_code, b.r_floor) for b in obhs]
+    ref = orc.diagnostics(U, dx, dx, dx, x0, x0, x0, obhs, 4 / 3)
+    got = bsn.diagnostics(dev(U), 32, 32, 32, dx, dx, dx, x0, x0, x0, gbhs, 4 / 3)
+    a = (slice(NG, -NG),) * 3
+    mag = np.abs(U[(4,) + a]).sum() + np.abs(U[(0,) + a]).sum() + np.abs(U[(1,) + a]).sum() + \
+        np.abs(U[(2,) + a]).sum() + np.abs(U[(3,) + a]).sum()
+    assert np.all(np.abs(got - ref) <= 1e-13 * mag * dx ** 3), (got, ref)
+    assert ref[8] > 0
+
+
+def test_coupled_run_steps_records_diagnostics(orc, bsn):
+    """The device loop's per-step records: {t, dt, diagnostics} equal to the
+    standalone reduction of the end state (same kernel), times and dts of the
+    reference loop."""
+    U, dx, x0, specs = binary_setup(orc, n=32)
+    Ud = dev(U)
+    bg = _bhs(bsn, specs)
+    rec = torch.zeros((4, 12), dtype=torch.float64, device="cuda")
+    t, n = bsn.coupled_run_steps(Ud, bg, 32, 32, 32, dx, x0, x0, x0, 4 / 3, 0.4, n_steps=3, f_sink=1.0,
+                                 rho_floor=1e-8, P_floor=1e-10, rho_sink_min=2e-8, evolve_orbit=False, diag=rec)
+    R = rec.cpu().numpy()
+    assert n == 3 and R[2, 0] == t and np.all(R[3] == 0.0)
+    assert np.all(R[:3, 1] > 0) and R[0, 0] == R[0, 1] and R[1, 0] == R[0, 0] + R[1, 1]
+    end = bsn.diagnostics(Ud, 32, 32, 32, dx, dx, dx, x0, x0, x0, bg, 4 / 3)
+    assert np.array_equal(R[2, 2:], end)
+    # the reference loop's times
+    bo = orc.bh_array(_obhs(orc, specs))
+    t_ref = 0.0
+    for k in range(3):
+        dt = orc.cfl_dt_3d(U, dx, dx, dx, 4 / 3, 0.4)
+        assert dt == R[k, 1]
+        orc.coupled_step(U, bo, 2, dt, t_ref, dx, x0, x0, x0, 4 / 3, 1.0, 1e-8, 1e-10, True, False, 0.0, 2e-8,
+                         evolve_orbit=False)
+        t_ref += dt
+    assert t_ref == t

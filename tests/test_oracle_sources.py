@@ -263,3 +263,40 @@ def test_fmr_gravity_momentum_and_infall(orc):
     r = np.sqrt(X ** 2 + Y ** 2 + Z ** 2)
     rad = (G.Uf[(1,) + af] * X + G.Uf[(2,) + af] * Y + G.Uf[(3,) + af] * Z) / np.maximum(r, 1e-300)
     assert rad.sum() * dxf ** 3 < 0.0
+
+
+def test_diagnostics_match_reference_formulas(orc):
+    """The oracle's src/diagnostics.jl restatement against numpy evaluations
+    of the reference's broadcast expressions (gas energy, kinetic energy,
+    momentum, angular momentum about the origin, bound mass with the BH
+    potential) on a random state with two BHs."""
+    from binary_ic import binary_setup
+    U, dx, x0, specs = binary_setup(orc, n=16)
+    rng = np.random.default_rng(3)
+    a = (slice(3, -3),) * 3
+    for q in (1, 2, 3):
+        U[(q,) + a] = rng.normal(0.0, 0.3, U[(q,) + a].shape) * U[(0,) + a]
+    bhs = [orc.make_bh(s["pos"], s["vel"], s["mass"], s["eps"], s["c_code"], s["r_floor"]) for s in specs]
+    g = 4 / 3
+    out = orc.diagnostics(U, dx, dx, dx, x0, x0, x0, bhs, g)
+    n = 16
+    c = x0 + (np.arange(1, n + 1) - 0.5) * dx
+    X, Y, Z = np.meshgrid(c, c, c, indexing="ij")
+    r, mx, my, mz, E = (U[(q,) + a] for q in range(5))
+    rs = np.maximum(r, 1e-30)
+    ke = 0.5 * (mx ** 2 + my ** 2 + mz ** 2) / rs
+    P = np.maximum((g - 1) * (E - rs * ke), 0.0)
+    phi = np.zeros_like(r)
+    for s in specs:
+        phi -= s["mass"] / np.sqrt((X - s["pos"][0]) ** 2 + (Y - s["pos"][1]) ** 2 + (Z - s["pos"][2]) ** 2
+                                   + s["eps"] ** 2)
+    bound = (ke + P / ((g - 1) * rs) + phi) <= 0
+    dV = dx ** 3
+    ref = [E.sum(), ke.sum(), mx.sum(), my.sum(), mz.sum(), (Y * mz - Z * my).sum(), (Z * mx - X * mz).sum(),
+           (X * my - Y * mx).sum(), rs[bound].sum(), r.sum()]
+    ref = np.array(ref) * dV
+    scale = np.array([abs(E).sum(), ke.sum(), abs(mx).sum(), abs(my).sum(), abs(mz).sum()] +
+                     [np.abs(X * my).sum() + np.abs(Y * mz).sum() + np.abs(Z * mx).sum()] * 3 +
+                     [rs.sum(), r.sum()]) * dV
+    assert 0 < bound.sum() < bound.size
+    assert np.all(np.abs(out - ref) <= 1e-13 * scale), (out, ref)
