@@ -270,6 +270,69 @@ def fmr_polytrope(bsn, torch, steps, warmup, log):
     return out
 
 
+def coupled_binary(bsn, torch, steps, warmup, log, n=128):
+    """Binary-BH supernova physics on a uniform grid: n=3 polytrope star
+    (M=10, R=1, G=1, gamma 4/3) at the origin with a thermal bomb E=1 in
+    r<0.1, two m=5 BH sinks on the circular orbit of separation 3 in z=0
+    (sink radius 4 cells, softening 2 cells), self-gravity, n^3 on [-4,4]^3.
+    Times `steps` steps of the device coupled loop (gas force, FP64 N-body
+    orbit, stages with BH gravity / self-gravity / sinks, accretion, per-step
+    diagnostics; one CUDA graph per step) for FP32 and FP64 stencils, and the
+    host-driven FP64 loop (cfl_dt_3d + coupled_step per step) beside them."""
+    import math
+    from bsn import ics
+    L, g = 4.0, 4.0 / 3.0
+    dx = 2 * L / n
+    kw = dict(rho_floor=1e-8, P_floor=1e-10)
+    U0 = bsn.state(n, n, n)
+    ics.polytrope_ic_3d(U0, n, n, n, dx, dx, dx, g, M_star=10.0, R_star=1.0, x0=-L, y0=-L, z0=-L, **kw)
+    ics.thermal_bomb(U0, n, n, n, dx, dx, dx, E_SN=1.0, r_bomb=0.1, x0=-L, y0=-L, z0=-L)
+    v = math.sqrt(10.0 / 3.0) / 2.0
+
+    def bhs():
+        return [bsn.BlackHole((1.5, 0.0, 0.0), (0.0, v, 0.0), 5.0, 2 * dx, 1e6, 4 * dx),
+                bsn.BlackHole((-1.5, 0.0, 0.0), (0.0, -v, 0.0), 5.0, 2 * dx, 1e6, 4 * dx)]
+
+    out = {"workload": f"binary BH supernova, uniform {n}^3 on [-4,4]^3, sinks + self-gravity", "steps": steps,
+           "unit": "cell-updates/s"}
+    common = dict(f_sink=1.0, torque_free=True, self_gravity=True, rho_sink_min=0.0, evolve_orbit=True, **kw)
+    for prec in ("f32", "f64"):
+        U, b = U0.clone(), bhs()
+        rec = torch.zeros((steps + warmup, 12), dtype=torch.float64, device="cuda")
+        t, _ = bsn.coupled_run_steps(U, b, n, n, n, dx, -L, -L, -L, g, 0.4, n_steps=warmup, precision=prec,
+                                     diag=rec, **common)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        bsn.coupled_run_steps(U, b, n, n, n, dx, -L, -L, -L, g, 0.4, n_steps=steps, t=t, precision=prec, diag=rec,
+                              **common)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[f"{prec}_device_loop_ms_per_step"] = ms
+        out[f"{prec}_device_loop_value"] = n ** 3 / (ms / 1e3)
+        log(f"binary BH {prec} device loop: {ms:.3f} ms/step")
+    U, b = U0.clone(), bhs()
+    t = 0.0
+    for k in range(warmup + steps):
+        if k == warmup:
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+        dt = bsn.cfl_dt_3d(U, n, n, n, dx, dx, dx, g, 0.4)
+        bsn.coupled_step(U, b, dt, t, n, n, n, dx, -L, -L, -L, g, 1.0, kw["rho_floor"], kw["P_floor"], True, True,
+                         0.0, 0.0)
+        t += dt
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    out["f64_host_loop_ms_per_step"] = ms
+    out["f64_host_loop_value"] = n ** 3 / (ms / 1e3)
+    out["speedup_f32_device_vs_f64_host_loop"] = ms / out["f32_device_loop_ms_per_step"]
+    log(f"binary BH f64 host loop: {ms:.3f} ms/step")
+    return out
+
+
 def run_bsn(args, rank, world):
     import numpy as np
     import torch
@@ -362,6 +425,7 @@ def run_bsn(args, rank, world):
     log(f"roofline: {kname} {t_stage * 1e3:.3f} ms per launch")
     acc = accuracy(bsn, torch, U0, n, dx, kw) if not args.no_accuracy else None
     fmr = fmr_polytrope(bsn, torch, max(5, min(args.steps, 20)), args.warmup, log) if not args.no_fmr else None
+    coupled = coupled_binary(bsn, torch, max(5, min(args.steps, 20)), args.warmup, log) if not args.no_fmr else None
 
     # e2e: host-buffer path -- pinned host state -> device, one CFL-limited
     # RK3 step through the public entry point, device -> host, every step
@@ -422,6 +486,7 @@ def run_bsn(args, rank, world):
             "compare": compare,
             "accuracy": acc,
             "fmr": fmr,
+            "coupled": coupled,
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_kind": hbm_kind,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "traffic_note": "DRAM read+write of one stage-1 launch, ncu at 128^3 scaled by cells",
@@ -449,7 +514,8 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the Sedov-to-t=0.05 accuracy runs of the three paths")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--no-fmr", action="store_true", help="skip the two-level FMR polytrope timing")
+    ap.add_argument("--no-fmr", action="store_true",
+                    help="skip the two-level FMR polytrope and binary-BH coupled-loop timings")
     ap.add_argument("--tile", type=int, default=-1,
                     help="force this stage-kernel tile variant for both precisions (default: autotune)")
     args = ap.parse_args()
