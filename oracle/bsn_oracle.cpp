@@ -1270,6 +1270,98 @@ extern "C" void orc_fmr3d_step(const orc_fmr* G, double dt_c, int self_gravity, 
     orc_apply_floors(Uc, ncx, ncy, ncz, rfl, Pfl, g);
 }
 
+/* N nested levels: the recursive generalisation of fmr3d_step! (src/fmr3d.jl
+ * :451-604; the reference has two levels, so this restatement is checked
+ * against orc_fmr3d_step at N = 2 and per operator).  pairs[k] couples level
+ * k (Uc) with level k+1 (Uf); pairs[k].Uf must be pairs[k+1].Uc.  A substep of
+ * level l: its RK3 (ghosts from the parent's interpolated state for l > 0, its
+ * own coarse registers toward its child, its boundary fluxes into the parent's
+ * fine registers), then ratio substeps of its child with ghosts from
+ * (1 - a) U_l^n + a U_l^{n+1}, restriction, Berger-Colella correction, floors.
+ * Self-gravity: density restricted up the chain, one isolated solve on level 0,
+ * trilinear Phi down the chain, frozen for the coarse step. */
+namespace {
+void fmrN_level(const orc_fmr* P, int np, int l, double dt, const double* Upar, FluxReg* fr_par,
+                std::vector<std::vector<double>>& phis, int sg) {
+    const orc_fmr* down = l < np ? &P[l] : nullptr;
+    const orc_fmr* up = l > 0 ? &P[l - 1] : nullptr;
+    double* U; int nx, ny, nz; double dx, dy, dz;
+    if (down) { U = down->Uc; nx = down->ncx; ny = down->ncy; nz = down->ncz; dx = down->dxc; dy = down->dyc; dz = down->dzc; }
+    else { U = up->Uf; nx = up->nfx; ny = up->nfy; nz = up->nfz; dx = up->dxf; dy = up->dyf; dz = up->dzf; }
+    const double g = P[0].gamma, rfl = P[0].rho_floor, Pfl = P[0].P_floor;
+    const double rk_w[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+    Idx I(nx, ny, nz);
+    long n = I.size();
+    StepScratch S(nx, ny, nz);
+    std::memcpy(S.Un.data(), U, sizeof(double) * n);
+    int nic = 0, njc = 0, nkc = 0;
+    if (down) { nic = down->ci_hi - down->ci_lo + 1; njc = down->cj_hi - down->cj_lo + 1; nkc = down->ck_hi - down->ck_lo + 1; }
+    FluxReg frc(nic, njc, nkc);
+    for (int stage = 0; stage < 3; ++stage) {
+        if (!up) {
+            orc_euler3d_rhs(S.dU.data(), S.Fx.data(), S.Fy.data(), S.Fz.data(), U, nx, ny, nz, dx, dy, dz, g,
+                            P[0].bc, rfl, Pfl, 1);
+        } else {
+            orc_prolong_fine_ghosts(U, Upar, up);
+            fine_rhs(S.dU.data(), S.Fx.data(), S.Fy.data(), S.Fz.data(), U, up);
+        }
+        if (down) accumulate_fr_coarse(frc, S.Fx.data(), S.Fy.data(), S.Fz.data(), rk_w[stage], dt, down);
+        if (up) accumulate_fr_fine(*fr_par, S.Fx.data(), S.Fy.data(), S.Fz.data(), rk_w[stage], dt, up);
+        if (sg) orc_sg_gradient(S.dU.data(), U, phis[l].data(), nx, ny, nz, dx, dy, dz);
+        if (stage == 0) combine1(U, S.Un.data(), S.dU.data(), dt, n);
+        else if (stage == 1) combine2(U, S.Un.data(), S.dU.data(), dt, n);
+        else combine3(U, S.Un.data(), S.dU.data(), dt, n);
+        orc_apply_floors(U, nx, ny, nz, rfl, Pfl, g);
+    }
+    if (!down) return;
+    const int r = down->ratio;
+    std::vector<double> Unp1(U, U + n), Ui(n);
+    FluxReg frf(nic, njc, nkc);
+    for (int sub = 0; sub < r; ++sub) {
+        double alpha = (double)sub / (double)r;
+        for (long t = 0; t < n; ++t) Ui[t] = (1.0 - alpha) * S.Un[t] + alpha * Unp1[t];
+        fmrN_level(P, np, l + 1, dt / (double)r, Ui.data(), &frf, phis, sg);
+    }
+    orc_restrict(U, down->Uf, down);
+    bc_correct(down, frc, frf);
+    orc_apply_floors(U, nx, ny, nz, rfl, Pfl, g);
+}
+}  // namespace
+
+extern "C" void orc_fmrN_step(const orc_fmr* P, int npairs, double dt0, int self_gravity, double G_grav) {
+    std::vector<std::vector<double>> phis(npairs + 1);
+    if (self_gravity) {
+        for (int k = npairs - 1; k >= 0; --k) orc_restrict_density_to_coarse(&P[k]);
+        const int ng = NG;
+        int nx = P[0].ncx, ny = P[0].ncy, nz = P[0].ncz;
+        Idx I0(nx, ny, nz);
+        std::vector<double> rho((long)nx * ny * nz);
+        for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i)
+            rho[i + (long)nx * (j + (long)ny * k)] = P[0].Uc[I0(1, ng + 1 + i, ng + 1 + j, ng + 1 + k)];
+        phis[0].resize((long)nx * ny * nz);
+        orc_solve_poisson_isolated(rho.data(), nx, ny, nz, P[0].dxc, P[0].dyc, P[0].dzc, phis[0].data());
+        for (int k = 0; k < npairs; ++k) {
+            phis[k + 1].resize((long)P[k].nfx * P[k].nfy * P[k].nfz);
+            orc_prolong_scalar_trilinear(phis[k + 1].data(), phis[k].data(), &P[k]);
+        }
+        if (G_grav != 1.0)
+            for (auto& ph : phis) for (auto& v : ph) v *= G_grav;
+    }
+    fmrN_level(P, npairs, 0, dt0, nullptr, nullptr, phis, self_gravity);
+}
+
+/* cfl_dt_fmr3d generalised: min over levels of (product of ratios above it) x dt_level */
+extern "C" double orc_cfl_dt_fmrN(const orc_fmr* P, int npairs, double cfl) {
+    double dt = orc_cfl_dt_3d(P[0].Uc, P[0].ncx, P[0].ncy, P[0].ncz, P[0].dxc, P[0].dyc, P[0].dzc, P[0].gamma, cfl);
+    int fac = 1;
+    for (int k = 0; k < npairs; ++k) {
+        fac *= P[k].ratio;
+        double dtk = orc_cfl_dt_3d(P[k].Uf, P[k].nfx, P[k].nfy, P[k].nfz, P[k].dxf, P[k].dyf, P[k].dzf, P[k].gamma, cfl);
+        dt = jmin(dt, (double)fac * dtk);
+    }
+    return dt;
+}
+
 /* src/fmr3d.jl:616-622 */
 extern "C" double orc_cfl_dt_fmr3d(const orc_fmr* G, double cfl) {
     double dtc = orc_cfl_dt_3d(G->Uc, G->ncx, G->ncy, G->ncz, G->dxc, G->dyc, G->dzc, G->gamma, cfl);

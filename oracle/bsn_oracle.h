@@ -120,6 +120,9 @@ void   orc_prolong_fine_ghosts(double* Uf, const double* Uc, const orc_fmr* G);
 void   orc_restrict(double* Uc, const double* Uf, const orc_fmr* G);
 void   orc_fmr3d_step(const orc_fmr* G, double dt_c, int self_gravity, double G_grav);
 double orc_cfl_dt_fmr3d(const orc_fmr* G, double cfl);
+/* N nested levels: pairs[k].Uf is pairs[k+1].Uc */
+void   orc_fmrN_step(const orc_fmr* pairs, int npairs, double dt0, int self_gravity, double G_grav);
+double orc_cfl_dt_fmrN(const orc_fmr* pairs, int npairs, double cfl);
 void   orc_restrict_density_to_coarse(const orc_fmr* G);
 void   orc_prolong_scalar_trilinear(double* phi_f, const double* phi_c, const orc_fmr* G);
 void   orc_solve_fmr_poisson(const orc_fmr* G, double* phi_c, double* phi_f);

@@ -95,6 +95,8 @@ def _declare(L):
         "orc_restrict": (V, [P, P, C.POINTER(OrcFMR)]),
         "orc_fmr3d_step": (V, [C.POINTER(OrcFMR), d, i, d]),
         "orc_cfl_dt_fmr3d": (d, [C.POINTER(OrcFMR), d]),
+        "orc_fmrN_step": (V, [C.POINTER(OrcFMR), i, d, i, d]),
+        "orc_cfl_dt_fmrN": (d, [C.POINTER(OrcFMR), i, d]),
         "orc_restrict_density_to_coarse": (V, [C.POINTER(OrcFMR)]),
         "orc_prolong_scalar_trilinear": (V, [P, P, C.POINTER(OrcFMR)]),
         "orc_solve_fmr_poisson": (V, [C.POINTER(OrcFMR), P, P]),
@@ -324,6 +326,30 @@ class FMRGrid:
         phif = np.zeros((s.nfx, s.nfy, s.nfz), order="F")
         lib().orc_solve_fmr_poisson(C.byref(s), _p(phic), _p(phif))
         return phic, phif
+
+
+class FMRHierarchy:
+    """N nested levels: a chain of FMRGrid pairs where pair k's fine level is
+    pair k+1's coarse level.  levels[0] is the base grid; each entry of
+    `boxes` is (ci_lo, ci_hi, cj_lo, cj_hi, ck_lo, ck_hi, ratio) in the
+    interior indices of the level above it."""
+
+    def __init__(self, U0, dx0, boxes, gamma, bc="outflow", rho_floor=0.0, P_floor=0.0):
+        self.pairs = []
+        Uc, dxc = U0, dx0
+        for (a, b, c, d_, e, f, r) in boxes:
+            g = FMRGrid(Uc, dxc, a, b, c, d_, e, f, r, gamma, bc=bc, rho_floor=rho_floor,
+                        P_floor=P_floor)
+            self.pairs.append(g)
+            Uc, dxc = g.Uf, dxc / r
+        self.levels = [U0] + [g.Uf for g in self.pairs]
+        self._arr = (OrcFMR * len(self.pairs))(*[g.s for g in self.pairs])
+
+    def step(self, dt0, self_gravity=False, G_grav=1.0):
+        lib().orc_fmrN_step(self._arr, len(self.pairs), dt0, int(self_gravity), G_grav)
+
+    def cfl_dt(self, cfl):
+        return lib().orc_cfl_dt_fmrN(self._arr, len(self.pairs), cfl)
 
 
 def lag5_weights(ratio):
