@@ -29,7 +29,8 @@ __all__ = [
     "cfl_dt_3d", "add_bh_gravity_source", "gas_force_on_bh", "add_sink_sources", "accrete", "r_sink", "t_sink",
     "nbody_step", "KeplerOrbit", "kepler_update", "solve_poisson_isolated", "add_self_gravity_source",
     "apply_sg_force_level", "coupled_step", "FMRGrid3D", "fmr3d_step", "cfl_dt_fmr3d", "solve_fmr_poisson",
-    "restrict_density_to_coarse",
+    "restrict_density_to_coarse", "FMRHierarchy3D", "fmr_nested_step", "cfl_dt_fmr_nested",
+    "fmr_nested_run_steps",
 ]
 
 # ---------------------------------------------------------------------------
@@ -366,6 +367,52 @@ def fmr3d_run_steps(G: FMRGrid3D, cfl, *, n_steps, t=0.0, t_end=0.0, precision="
     nd = C.c_int(0)
     _call("bsn_fmr3d_run_steps", context(), C.byref(G.s), float(cfl), PREC[precision], int(bool(self_gravity)),
           float(G_grav), int(n_steps), float(t_end), C.byref(tt), C.byref(nd))
+    return tt.value, nd.value
+
+
+class FMRHierarchy3D:
+    """Nested FMR levels over device arrays: a chain of FMRGrid3D pairs where
+    pair k's fine level is pair k+1's coarse level (the reference's two-level
+    FMRGrid3D, src/fmr3d.jl:109-151, applied pair by pair).  Each entry of
+    `boxes` is (ci_lo, ci_hi, cj_lo, cj_hi, ck_lo, ck_hi, ratio) in the
+    1-based active indices of the level above; levels[0] is U0."""
+
+    def __init__(self, U0, nx, ny, nz, dx0, boxes, gamma, *, bc="outflow", rho_floor=0.0, P_floor=0.0,
+                 init=True):
+        if not 1 <= len(boxes) <= 3:
+            raise ValueError("2 to 4 levels")
+        self.pairs = []
+        U, n, dx = U0, (nx, ny, nz), dx0
+        for (a, b, c, d, e, f, r) in boxes:
+            g = FMRGrid3D(U, *n, dx, a, b, c, d, e, f, r, gamma, bc=bc, rho_floor=rho_floor, P_floor=P_floor,
+                          init=init)
+            self.pairs.append(g)
+            U, n, dx = g.Uf, g.fine_dims, dx / r
+        self.levels = [U0] + [g.Uf for g in self.pairs]
+        self.dims = [(nx, ny, nz)] + [g.fine_dims for g in self.pairs]
+        self._arr = (bsn_fmr2 * len(self.pairs))(*[g.s for g in self.pairs])
+
+
+def fmr_nested_step(H: FMRHierarchy3D, dt0, *, self_gravity=False, G_grav=1.0):
+    _call("bsn_fmr_nested_step_f64", context(), H._arr, len(H.pairs), float(dt0), int(bool(self_gravity)),
+          float(G_grav))
+
+
+def cfl_dt_fmr_nested(H: FMRHierarchy3D, cfl) -> float:
+    out = C.c_double()
+    _call("bsn_cfl_dt_fmr_nested_f64", context(), H._arr, len(H.pairs), float(cfl), C.byref(out))
+    return out.value
+
+
+def fmr_nested_run_steps(H: FMRHierarchy3D, cfl, *, n_steps, t=0.0, t_end=0.0, precision="f64",
+                         self_gravity=False, G_grav=1.0):
+    """Up to n_steps CFL-limited nested steps on the device (one CUDA graph per
+    level-0 step; each chain of first substeps batched per RK3 stage);
+    returns (t, steps)."""
+    tt = C.c_double(float(t))
+    nd = C.c_int(0)
+    _call("bsn_fmr_nested_run_steps", context(), H._arr, len(H.pairs), float(cfl), PREC[precision],
+          int(bool(self_gravity)), float(G_grav), int(n_steps), float(t_end), C.byref(tt), C.byref(nd))
     return tt.value, nd.value
 
 

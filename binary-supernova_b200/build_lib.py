@@ -22,7 +22,7 @@ OUT = os.path.join(HERE, "bsn", "libbsn.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 BASE = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
-FP64_PARITY = {"hydro_f64.cu", "sources_f64.cu", "fmr_f64.cu", "poisson.cu", "context.cu", "cfl_noalloc.cu",
+FP64_PARITY = {"hydro_f64.cu", "sources_f64.cu", "fmr_f64.cu", "fmr_nlevel.cu", "poisson.cu", "context.cu", "cfl_noalloc.cu",
                "run_steps.cu", "autotune.cu", "coupled_run.cu", "diagnostics.cu"}
 # the FP32 fast path: contraction on, approximate division and square root
 FAST = {"stage_fast.cu", "learned.cu", "poisson_f32.cu"}

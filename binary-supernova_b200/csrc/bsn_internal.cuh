@@ -39,6 +39,7 @@ struct bsn_ctx {
     // graph-captured device time loop (run_steps.cu)
     void* run_state = nullptr;
     void* fmr_run_state = nullptr;   // fmr_f64.cu: graph of the device-resident FMR step
+    void* fmrN_state = nullptr;      // fmr_nlevel.cu: nested-level buffers and step graph
     void* coupled_run_state = nullptr;   // coupled_run.cu: graph of the device-resident coupled step
 };
 

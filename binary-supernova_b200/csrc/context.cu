@@ -98,6 +98,7 @@ void fft32_state_free(bsn_ctx* ctx);   // poisson_f32.cu
 void run_state_free(bsn_ctx* ctx);   // run_steps.cu
 void learned_state_free(bsn_ctx* ctx);   // learned.cu
 void fmr_run_state_free(bsn_ctx* ctx);   // fmr_f64.cu
+void fmrN_state_free(bsn_ctx* ctx);      // fmr_nlevel.cu
 void coupled_run_state_free(bsn_ctx* ctx);   // coupled_run.cu
 
 }  // namespace bsn
@@ -135,6 +136,7 @@ extern "C" bsn_status bsn_ctx_destroy(bsn_ctx* ctx) {
     run_state_free(ctx);
     learned_state_free(ctx);
     fmr_run_state_free(ctx);
+    fmrN_state_free(ctx);
     coupled_run_state_free(ctx);
     for (auto& r : ctx->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     delete ctx;

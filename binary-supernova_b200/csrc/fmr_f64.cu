@@ -13,19 +13,11 @@
 //   * the fine stage kernels write their boundary faces to a small buffer that
 //     one kernel folds into the fine registers in the reference's loop order,
 //     so the register sums are bit-identical.
+#include "fmr.cuh"
 #include "poisson.cuh"
-#include "stage_launch.cuh"
 
 namespace bsn {
 namespace fmr {
-
-constexpr int MAXR = 8;
-
-struct Geo {
-    int ncx, ncy, ncz, nfx, nfy, nfz, r;
-    int lo[3], hi[3];        // 1-based coarse active index range of the patch
-    double w[MAXR * 5];      // Lagrange-5 weights, w[s + r*j] (src/fmr3d.jl:32-46)
-};
 
 // src/fmr3d.jl:165-170 for a 0-based ghosted fine index g (Julia ig_f = g+1).
 __device__ __forceinline__ void coarse_stencil(int g, int c_lo, int r, int& ic0, int& s) {
@@ -131,10 +123,6 @@ __global__ void restrict_kernel(Geo G, double* Uc, const double* Uf, int qmax, c
 // Fine register accumulation (src/fmr3d.jl:331-369): one thread per coarse
 // register element adds its r^2 fine faces in the reference's loop order.
 // bnd[2D+side] holds fine faces (5, n1, n2) over the fine active transverse.
-struct Regs {
-    double* r[6];           // xlo, xhi, ylo, yhi, zlo, zhi: (5, t1, t2) coarse
-    const double* bnd[6];
-};
 // fac = weight * dt_f / r^2; with dtf_dev, (wt * *dtf_dev) / rr on the device.
 __global__ void fine_reg_kernel(Geo G, Regs R, double fac, const double* dtf_dev, double wt, double rr,
                                 const int* done) {
@@ -276,14 +264,14 @@ long long ghost_count(int nx, int ny, int nz) {
 }
 
 bsn_status prolong_ghosts(bsn_ctx* ctx, const Geo& G, const double* Ucn, const double* Ucnp1, double alpha,
-                          double* dst, const int* done = nullptr) {
+                          double* dst, const int* done) {
     long long n = ghost_count(G.nfx, G.nfy, G.nfz);
     prof_begin(ctx);
     prolong_ghosts_kernel<<<grid1d(n, 128), 128, 0, ctx->stream>>>(G, Ucn, Ucnp1, alpha, dst, done);
     return launch_check(ctx, "prolong_ghosts_kernel");
 }
 
-bsn_status restrict_(bsn_ctx* ctx, const Geo& G, double* Uc, const double* Uf, int qmax, const int* done = nullptr) {
+bsn_status restrict_(bsn_ctx* ctx, const Geo& G, double* Uc, const double* Uf, int qmax, const int* done) {
     long long n = (long long)(G.hi[0] - G.lo[0] + 1) * (G.hi[1] - G.lo[1] + 1) * (G.hi[2] - G.lo[2] + 1);
     prof_begin(ctx);
     restrict_kernel<<<grid1d(n, 128), 128, 0, ctx->stream>>>(G, Uc, Uf, qmax, done);
@@ -291,7 +279,7 @@ bsn_status restrict_(bsn_ctx* ctx, const Geo& G, double* Uc, const double* Uf, i
 }
 
 // solve_fmr_poisson (src/fmr_gravity.jl:119-133); fp32: FP32 transforms
-bsn_status fmr_poisson(bsn_ctx* ctx, const bsn_fmr2* g, const Geo& G, double* phic, double* phif, bool fp32 = false) {
+bsn_status fmr_poisson(bsn_ctx* ctx, const bsn_fmr2* g, const Geo& G, double* phic, double* phif, bool fp32) {
     BSN_TRY(restrict_(ctx, G, g->Uc, g->Uf, 1));
     if (fp32) BSN_TRY(poisson_from_state_f32(ctx, g->Uc, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, -1.0, phic));
     else BSN_TRY(poisson_from_state(ctx, g->Uc, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, -1.0, phic));

@@ -80,7 +80,7 @@ __device__ __forceinline__ void cell_xyz(int a, int b, int c, double x0, double 
 // gx/gy its blocks along x and y (filled by the launcher from the tile).
 // queue: a zeroed counter the CTAs draw blocks from (dynamic schedule);
 // null: CTA b takes blocks b, b + gridDim, ...
-constexpr int MAXLEV = 2;
+constexpr int MAXLEV = 4;
 struct StageBatch {
     StageArgs lv[MAXLEV];
     unsigned int* queue;

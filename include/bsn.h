@@ -307,6 +307,28 @@ bsn_status bsn_solve_fmr_poisson_f64(bsn_ctx* ctx, const bsn_fmr2* G, double* ph
 bsn_status bsn_fmr3d_run_steps(bsn_ctx* ctx, const bsn_fmr2* G, double cfl, int precision, int self_gravity,
                                double G_grav, int n_steps, double t_end, double* t_inout, int* steps_done);
 
+/* ---- nested FMR, N = npairs + 1 <= 4 levels.  The reference's fmr3d_step!
+ * (src/fmr3d.jl:451-604) couples two levels; these entries generalise it
+ * recursively: each level subcycles `ratio` times inside its parent's step
+ * with ghosts from the parent at a = s/ratio, registers and Berger-Colella
+ * correction per pair, self-gravity solved on level 0 and interpolated down
+ * the chain (src/fmr_gravity.jl pair by pair).  pairs[k] couples level k
+ * (Uc) with level k+1 (Uf); pairs[k].Uf must be pairs[k+1].Uc with matching
+ * extents and spacings.  gamma, bc and floors are taken from pairs[0].  At
+ * npairs = 1 they equal the two-level entries above. */
+bsn_status bsn_fmr_nested_step_f64(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, double dt0, int self_gravity,
+                             double G_grav);
+/* min over levels l of (ratio_0 ... ratio_{l-1}) * cfl / max signal speed of l */
+bsn_status bsn_cfl_dt_fmr_nested_f64(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, double cfl, double* dt_out);
+/* The nested driver loop on the device, one CUDA graph per level-0 step (as
+ * bsn_fmr3d_run_steps).  The first substeps of a chain of levels l..N-1 take
+ * their ghosts from their parents' states at the start of the parents'
+ * substeps, so each RK3 stage of such a chain is one persistent launch over
+ * all of its levels. */
+bsn_status bsn_fmr_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, double cfl, int precision,
+                              int self_gravity, double G_grav, int n_steps, double t_end, double* t_inout,
+                              int* steps_done);
+
 #ifdef __cplusplus
 }
 #endif
