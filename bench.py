@@ -270,6 +270,102 @@ def fmr_polytrope(bsn, torch, steps, warmup, log):
     return out
 
 
+def binary_nested(bsn, torch, steps, warmup, log, n=128):
+    """The binary-BH supernova on three nested FMR levels of n^3 (ratio 2) on
+    [-8,8]^3, [-4,4]^3, [-2,2]^3: n=3 polytrope star (M=10, R=1, G=1, gamma
+    4/3) with a thermal bomb E=1 in r<0.1 and two m=5 BH sinks at (+-1.5,0,0)
+    on their circular orbit (sink radius 4, softening 2 finest cells), every
+    level with its own initial state.  Times `steps` level-0 steps of the
+    device coupled loop on the nested levels (composite gas force, FP64
+    orbit, nested step with BH gravity / self-gravity / sinks on every level
+    and the chains of first substeps batched per RK3 stage, accretion,
+    diagnostics; one CUDA graph per step) with FP64, FP32 and learned
+    stencils.  cell-updates/s counts each level once per substep (7 n^3 per
+    level-0 step); the L1 of the finest level's density against FP64 is taken
+    at FP64's end time (the other paths rerun from the initial state to it)."""
+    import math
+    from bsn import ics
+    from bsn import learned as Lm
+    Lm.install(*Lm.load_params())
+    g, L = 4.0 / 3.0, 8.0
+    lo, hi = n // 4 + 1, 3 * n // 4
+    boxes = ((lo, hi, lo, hi, lo, hi, 2),) * 2
+    kw = dict(rho_floor=1e-8, P_floor=1e-10)
+    dx0 = 2 * L / n
+
+    def fill(U, dx, x0, bomb=True):
+        ics.polytrope_ic_3d(U, n, n, n, dx, dx, dx, g, M_star=10.0, R_star=1.0, x0=x0, y0=x0, z0=x0, **kw)
+        if bomb:
+            ics.thermal_bomb(U, n, n, n, dx, dx, dx, E_SN=1.0, r_bomb=0.1, x0=x0, y0=x0, z0=x0)
+
+    U0 = bsn.state(n, n, n)
+    # no level-0 cell centre lies within r < 0.1 at n = 128 (thermal_bomb! would
+    # raise); the covered centre of level 0 takes the finer levels' restriction
+    fill(U0, dx0, -L, bomb=2 * L / n < 0.1)
+    bsn.fill_ghost_3d_outflow(U0, n, n, n)
+    H0 = bsn.FMRHierarchy3D(U0, n, n, n, dx0, boxes, g, **kw)
+    x0, dx = -L, dx0
+    for k in range(2):
+        x0, dx = x0 + (lo - 1) * dx, dx / 2
+        fill(H0.levels[k + 1], dx, x0)
+        H0.pairs[k].prolong_fine_ghosts()
+    dxf = dx
+    init = [U.clone() for U in H0.levels]
+    del H0
+    v = math.sqrt(10.0 / 3.0) / 2.0
+    units = 7 * n ** 3
+    out = {"workload": f"binary BH supernova, 3 nested FMR levels {n}^3 (ratio 2) on [-8,8]^3/[-4,4]^3/[-2,2]^3, "
+                       "sinks + self-gravity", "steps": steps, "unit": "cell-updates/s", "units_per_step": units}
+    rho_f = {}
+
+    def fresh(prec, cap):
+        U = init[0].clone()
+        H = bsn.FMRHierarchy3D(U, n, n, n, dx0, boxes, g, init=False, **kw)
+        for Ud, Ui in zip(H.levels[1:], init[1:]):
+            Ud.copy_(Ui)
+        b = [bsn.BlackHole((1.5, 0.0, 0.0), (0.0, v, 0.0), 5.0, 2 * dxf, 1e6, 4 * dxf),
+             bsn.BlackHole((-1.5, 0.0, 0.0), (0.0, -v, 0.0), 5.0, 2 * dxf, 1e6, 4 * dxf)]
+        rec = torch.zeros((cap, 12), dtype=torch.float64, device="cuda")
+        common = dict(f_sink=1.0, torque_free=True, self_gravity=True, rho_sink_min=0.0, evolve_orbit=True,
+                      precision=prec, diag=rec)
+        return H, b, common
+
+    for prec in ("f64", "f32", "learned"):
+        H, b, common = fresh(prec, steps + warmup)
+        t, _ = bsn.coupled_nested_run_steps(H, b, -L, -L, -L, 0.4, n_steps=warmup, **common)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        t, _ = bsn.coupled_nested_run_steps(H, b, -L, -L, -L, 0.4, n_steps=steps, t=t, **common)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[f"{prec}_device_loop_ms_per_step"] = ms
+        out[f"{prec}_device_loop_value"] = units / (ms / 1e3)
+        log(f"binary BH nested {prec}: {ms:.3f} ms/step")
+        if prec == "f64":
+            t64 = t
+            rho_f[prec] = H.levels[2][0].clone()
+        del H
+    # accuracy at equal time: the reduced-precision paths rerun to FP64's end time
+    out["accuracy_t"] = t64
+    for prec in ("f32", "learned"):
+        H, b, common = fresh(prec, 1)
+        common["diag"] = None
+        _, k = bsn.coupled_nested_run_steps(H, b, -L, -L, -L, 0.4, n_steps=10 * (steps + warmup), t_end=t64,
+                                            **common)
+        out[f"{prec}_accuracy_steps"] = k
+        rho_f[prec] = H.levels[2][0].clone()
+        del H
+    a = (slice(3, -3),) * 3
+    ref = rho_f["f64"][a]
+    for prec in ("f32", "learned"):
+        out[f"{prec}_L1_rho_finest_vs_f64"] = float((rho_f[prec][a] - ref).abs().sum() / ref.abs().sum())
+    out["speedup_f32_vs_f64"] = out["f64_device_loop_ms_per_step"] / out["f32_device_loop_ms_per_step"]
+    out["speedup_learned_vs_f64"] = out["f64_device_loop_ms_per_step"] / out["learned_device_loop_ms_per_step"]
+    return out
+
+
 def coupled_binary(bsn, torch, steps, warmup, log, n=128):
     """Binary-BH supernova physics on a uniform grid: n=3 polytrope star
     (M=10, R=1, G=1, gamma 4/3) at the origin with a thermal bomb E=1 in
@@ -426,6 +522,7 @@ def run_bsn(args, rank, world):
     acc = accuracy(bsn, torch, U0, n, dx, kw) if not args.no_accuracy else None
     fmr = fmr_polytrope(bsn, torch, max(5, min(args.steps, 20)), args.warmup, log) if not args.no_fmr else None
     coupled = coupled_binary(bsn, torch, max(5, min(args.steps, 20)), args.warmup, log) if not args.no_fmr else None
+    nested = binary_nested(bsn, torch, max(5, min(args.steps, 20)), args.warmup, log) if not args.no_fmr else None
 
     # e2e: host-buffer path -- pinned host state -> device, one CFL-limited
     # RK3 step through the public entry point, device -> host, every step
@@ -487,6 +584,7 @@ def run_bsn(args, rank, world):
             "accuracy": acc,
             "fmr": fmr,
             "coupled": coupled,
+            "coupled_nested": nested,
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_kind": hbm_kind,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "traffic_note": "DRAM read+write of one stage-1 launch, ncu at 128^3 scaled by cells",

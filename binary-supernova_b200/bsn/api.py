@@ -30,7 +30,7 @@ __all__ = [
     "nbody_step", "KeplerOrbit", "kepler_update", "solve_poisson_isolated", "add_self_gravity_source",
     "apply_sg_force_level", "coupled_step", "FMRGrid3D", "fmr3d_step", "cfl_dt_fmr3d", "solve_fmr_poisson",
     "restrict_density_to_coarse", "FMRHierarchy3D", "fmr_nested_step", "cfl_dt_fmr_nested",
-    "fmr_nested_run_steps",
+    "fmr_nested_run_steps", "coupled_nested_run_steps",
 ]
 
 # ---------------------------------------------------------------------------
@@ -413,6 +413,28 @@ def fmr_nested_run_steps(H: FMRHierarchy3D, cfl, *, n_steps, t=0.0, t_end=0.0, p
     nd = C.c_int(0)
     _call("bsn_fmr_nested_run_steps", context(), H._arr, len(H.pairs), float(cfl), PREC[precision],
           int(bool(self_gravity)), float(G_grav), int(n_steps), float(t_end), C.byref(tt), C.byref(nd))
+    return tt.value, nd.value
+
+
+def coupled_nested_run_steps(H: FMRHierarchy3D, bhs, x0, y0, z0, cfl, *, n_steps, t=0.0, t_end=0.0,
+                             dt_max=0.0, f_sink=1.0, torque_free=True, self_gravity=False, t_bh2_sink_on=0.0,
+                             rho_sink_min=0.0, evolve_orbit=True, precision="f64", diag=None):
+    """The coupled_step! driver loop on nested FMR levels, on the device (one
+    CUDA graph per level-0 step); returns (t, steps) and updates `bhs` in
+    place.  x0, y0, z0: lower corner of level 0.  diag: optional CUDA float64
+    tensor (cap, 12) receiving {t, dt, diagnostics of level 0} per step."""
+    if diag is not None and not (diag.is_cuda and diag.dtype == torch.float64 and diag.is_contiguous()
+                                 and diag.dim() == 2 and diag.shape[1] == 12):
+        raise TypeError("diag must be a contiguous CUDA float64 tensor of shape (cap, 12)")
+    arr = _bh_array(bhs)
+    tt = C.c_double(float(t))
+    nd = C.c_int(0)
+    _call("bsn_coupled_nested_run_steps", context(), H._arr, len(H.pairs), arr, len(bhs), float(x0), float(y0),
+          float(z0), float(cfl), float(dt_max), float(f_sink), int(bool(torque_free)), int(bool(self_gravity)),
+          float(t_bh2_sink_on), float(rho_sink_min), int(bool(evolve_orbit)), PREC[precision], int(n_steps),
+          float(t_end), C.byref(tt), C.byref(nd), _ptr(diag) if diag is not None else None,
+          int(diag.shape[0]) if diag is not None else 0)
+    _bh_writeback(bhs, arr)
     return tt.value, nd.value
 
 

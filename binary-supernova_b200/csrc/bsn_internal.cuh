@@ -41,6 +41,7 @@ struct bsn_ctx {
     void* fmr_run_state = nullptr;   // fmr_f64.cu: graph of the device-resident FMR step
     void* fmrN_state = nullptr;      // fmr_nlevel.cu: nested-level buffers and step graph
     void* coupled_run_state = nullptr;   // coupled_run.cu: graph of the device-resident coupled step
+    void* coupled_nested_state = nullptr;   // coupled_run.cu: the coupled step on nested levels
 };
 
 namespace bsn {

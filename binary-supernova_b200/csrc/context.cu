@@ -100,6 +100,7 @@ void learned_state_free(bsn_ctx* ctx);   // learned.cu
 void fmr_run_state_free(bsn_ctx* ctx);   // fmr_f64.cu
 void fmrN_state_free(bsn_ctx* ctx);      // fmr_nlevel.cu
 void coupled_run_state_free(bsn_ctx* ctx);   // coupled_run.cu
+void coupled_nested_state_free(bsn_ctx* ctx);   // coupled_run.cu
 
 }  // namespace bsn
 
@@ -138,6 +139,7 @@ extern "C" bsn_status bsn_ctx_destroy(bsn_ctx* ctx) {
     fmr_run_state_free(ctx);
     fmrN_state_free(ctx);
     coupled_run_state_free(ctx);
+    coupled_nested_state_free(ctx);
     for (auto& r : ctx->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     delete ctx;
     return BSN_OK;

@@ -13,6 +13,7 @@
 #include "diagnostics.cuh"
 #include "poisson.cuh"
 #include "stage_launch.cuh"
+#include "fmr_nested.cuh"
 
 namespace bsn {
 namespace crun {
@@ -75,8 +76,14 @@ __device__ __forceinline__ DD dd_merge(DD a, DD b) {
     return s;
 }
 
+// active cells [lo, hi] (0-based, inclusive per axis) left out of a sum: the
+// region a finer level covers; lo > hi leaves nothing out
+struct Box {
+    int lo[3], hi[3];
+};
+
 __global__ void gas_force_kernel(const double* U, int nx, int ny, int nz, double dx, double dy, double dz, double x0,
-                                 double y0, double z0, const Dev* r, int i, double* part) {
+                                 double y0, double z0, const Dev* r, int i, double* part, Box skip) {
     if (r->done) return;
     const bsn_bh bh = r->bh[i];
     Geom G(nx, ny, nz);
@@ -85,6 +92,9 @@ __global__ void gas_force_kernel(const double* U, int nx, int ny, int nz, double
     long long n = (long long)nx * ny * nz;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         int a = (int)(t % nx); long long rr = t / nx; int b = (int)(rr % ny); int c = (int)(rr / ny);
+        if (a >= skip.lo[0] && a <= skip.hi[0] && b >= skip.lo[1] && b <= skip.hi[1] && c >= skip.lo[2] &&
+            c <= skip.hi[2])
+            continue;
         double xc, yc, zc;
         f64::cell_xyz(a, b, c, x0, y0, z0, dx, dy, dz, xc, yc, zc);
         double ddx = xc - bh.pos[0], ddy = yc - bh.pos[1], ddz = zc - bh.pos[2];
@@ -377,7 +387,8 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
             BSN_TRY(launch_check(ctx, "coupled_dt_kernel"));
             // gas force on every BH from the start-of-step state, then the orbit
             for (int i = 0; i < nbh; ++i) {
-                gas_force_kernel<<<blocks, 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dx, dx, x0, y0, z0, r, i, part);
+                gas_force_kernel<<<blocks, 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dx, dx, x0, y0, z0, r, i, part,
+                                                                  Box{{1, 1, 1}, {0, 0, 0}});
                 BSN_TRY(launch_check(ctx, "coupled_gas_force_kernel"));
                 gas_force_finish<<<1, 32, 0, ctx->stream>>>(part, blocks, r, i);
                 BSN_TRY(launch_check(ctx, "coupled_gas_force_finish"));
@@ -449,5 +460,207 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
     for (int i = 0; i < nbh; ++i) bhs[i] = d.bh[i];
     if (d.done == 2)
         return set_err(ctx, BSN_ERR_NONFINITE, "time step collapsed to 0 at t = %.17g (infinite signal speed)", d.t);
+    return BSN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The coupled driver loop on nested FMR levels (up to 4).  The reference runs
+// coupled_step! on one uniform grid; on nested levels each step is
+//   dt = min over levels of the nested CFL (capped by dt_max, clamped to t_end);
+//   gas force on every BH from the composite grid (each level's cells except
+//   those its child covers); the BH orbit over dt (nbody_step!, FP64);
+//   one nested step (fmr3d_step! generalised, fmr_nlevel.cu) whose stages on
+//   every level carry BH gravity, self-gravity (Phi frozen per level-0 step,
+//   src/fmr_gravity.jl) and sinks in the driver's order, the BHs frozen at
+//   their post-orbit state for the whole step;
+//   accrete! of every active sink from the finest level over dt;
+//   the driver's diagnostics of level 0 (which holds the restriction of the
+//   finer levels).
+// Time control (dt per level, t, done) lives in the nested plan's device
+// record and is mirrored into the coupled record read by the orbit,
+// source and accretion kernels.
+
+namespace bsn {
+namespace crun {
+
+__global__ void nested_sync_kernel(Dev* r, const fmr::NDev* n) {
+    r->dt = n->dt[0];
+    r->t = n->t;
+    r->done = n->done;
+    r->steps = n->steps;
+}
+
+}  // namespace crun
+
+void coupled_nested_state_free(bsn_ctx* ctx) {
+    fmr::nstate_destroy((fmr::NState*)ctx->coupled_nested_state);
+    ctx->coupled_nested_state = nullptr;
+}
+
+}  // namespace bsn
+
+extern "C" bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, bsn_bh* bhs,
+                                                   int nbh, double x0, double y0, double z0, double cfl,
+                                                   double dt_max, double f_sink, int torque_free, int self_gravity,
+                                                   double t_bh2_sink_on, double rho_sink_min, int evolve_orbit,
+                                                   int precision, int n_steps, double t_end, double* t_inout,
+                                                   int* steps_done, double* diag_out, int diag_cap) {
+    using namespace bsn::fmr;
+    if (!ctx) return BSN_ERR_ARG;
+    if (!t_inout || (nbh > 0 && !bhs)) return set_err(ctx, BSN_ERR_ARG, "null argument");
+    if (nbh < 0 || nbh > MAXBH) return set_err(ctx, BSN_ERR_UNSUPPORTED, "at most %d black holes", MAXBH);
+    if (n_steps < 0) return set_err(ctx, BSN_ERR_ARG, "n_steps < 0");
+    if (diag_out && diag_cap < 0) return set_err(ctx, BSN_ERR_ARG, "diag_cap < 0");
+    if (!diag_out) diag_cap = 0;
+    if (!ctx->coupled_nested_state) ctx->coupled_nested_state = new NState();
+    NState* S = (NState*)ctx->coupled_nested_state;
+    NPlan plan;
+    BSN_TRY(make_plan(ctx, pairs, npairs, precision, self_gravity, 1.0, S, plan));
+    const int nl = plan.nl;
+    bsn_status st;
+    Dev* r = (Dev*)slot(ctx, SLOT_CRUN, sizeof(Dev), &st); BSN_TRY(st);
+    const int blocks = 148 * 4;
+    double* part = (double*)slot(ctx, SLOT_CRED, sizeof(double) * 6 * blocks * nl, &st); BSN_TRY(st);
+    double* dpart = nullptr;
+    if (diag_out) {
+        dpart = (double*)slot(ctx, SLOT_DIAGREC, sizeof(double) * 2 * diag::NDIAG * diag::BLOCKS, &st); BSN_TRY(st);
+    }
+    // level origins: level k+1 starts at the lower face of level k's cell ci_lo
+    double ox[NMAXL], oy[NMAXL], oz[NMAXL];
+    ox[0] = x0; oy[0] = y0; oz[0] = z0;
+    for (int k = 0; k < npairs; ++k) {
+        ox[k + 1] = ox[k] + (double)(pairs[k].ci_lo - 1) * pairs[k].dxc;
+        oy[k + 1] = oy[k] + (double)(pairs[k].cj_lo - 1) * pairs[k].dyc;
+        oz[k + 1] = oz[k] + (double)(pairs[k].ck_lo - 1) * pairs[k].dzc;
+    }
+    for (int l = 0; l < nl; ++l) {
+        f64::StageArgs& a = plan.base[l];
+        a.x0 = ox[l]; a.y0 = oy[l]; a.z0 = oz[l];
+        if (nbh > 0) { a.use_bh = 1; a.bh_dev = &r->bsrc; a.use_sink = 1; a.sk_dev = &r->ssrc; }
+    }
+    if (self_gravity) {
+        const NLevel& v = plan.L[0];
+        if (precision == PREC_F64) BSN_TRY(poisson_prepare(ctx, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz));
+        else BSN_TRY(poisson_prepare_f32(ctx, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz));
+    }
+    int tiles[NMAXL] = {-1, -1, -1, -1};
+    for (int l = 0; l < nl; ++l) {
+        f64::StageArgs p = plan.base[l];
+        p.Uin = plan.L[l].U; p.dt_dev = nullptr; p.done_dev = nullptr; p.use_reg = 0; p.use_bnd = 0; p.Gh = nullptr;
+        p.use_bh = 0; p.use_sink = 0; p.bh_dev = nullptr; p.sk_dev = nullptr;
+        BSN_TRY(stage_autotune(ctx, precision, p, plan.L[l].A));
+        tiles[l] = ctx->tile_choice[std::make_tuple(precision, plan.L[l].nx, plan.L[l].ny, plan.L[l].nz)];
+    }
+    // BHs to the device through the pinned buffer, then both records initialised
+    double* h = (double*)pinned(ctx, sizeof(Dev) + sizeof(NDev) + 128, &st); BSN_TRY(st);
+    bsn_bh* hb = (bsn_bh*)h;
+    for (int i = 0; i < nbh; ++i) hb[i] = bhs[i];
+    bsn_bh* db = (bsn_bh*)part;
+    BSN_CUDA(ctx, cudaMemcpyAsync(db, hb, sizeof(bsn_bh) * (nbh > 0 ? nbh : 1), cudaMemcpyHostToDevice, ctx->stream));
+    init_kernel<<<1, 1, 0, ctx->stream>>>(r, *t_inout, db, nbh);
+    BSN_TRY(launch_check(ctx, "coupled_init_kernel"));
+    n_init_kernel<<<1, 1, 0, ctx->stream>>>(plan.d, *t_inout);
+    BSN_TRY(launch_check(ctx, "fmrN_init_kernel"));
+
+    const NLevel& fin = plan.L[nl - 1];
+    std::vector<double> extra = {(double)nbh, x0, y0, z0, dt_max, f_sink, (double)torque_free, t_bh2_sink_on,
+                                 rho_sink_min, (double)evolve_orbit, (double)diag_cap,
+                                 (double)(uintptr_t)r, (double)(uintptr_t)part, (double)(uintptr_t)diag_out,
+                                 (double)(uintptr_t)dpart};
+    bool same = S->exec && (int)S->key_pairs.size() == npairs &&
+                memcmp(S->key_pairs.data(), pairs, sizeof(bsn_fmr2) * npairs) == 0 && S->prec == precision &&
+                S->sg == self_gravity && S->cfl == cfl && S->t_end == t_end &&
+                memcmp(S->tiles, tiles, sizeof(tiles)) == 0 && S->key_base == S->arena.base && S->key_extra == extra;
+    if (!same) {
+        S->release();
+        if (!S->cap) BSN_CUDA(ctx, cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
+        bool prof = ctx->profiling;
+        ctx->profiling = false;
+        long long l0 = ctx->launches;
+        cudaStream_t user = ctx->stream;
+        ctx->stream = S->cap;
+        cudaError_t be = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (be != cudaSuccess) { ctx->stream = user; ctx->profiling = prof; return cuda_check(ctx, be, "cudaStreamBeginCapture"); }
+        auto body = [&]() -> bsn_status {
+            for (int l = 0; l < nl; ++l) {
+                const NLevel& v = plan.L[l];
+                BSN_TRY(f64_cfl_fold(ctx, v.U, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz, plan.gamma, &plan.d->sm[l],
+                                     &plan.d->nan[l]));
+            }
+            n_dt_kernel<<<1, 1, 0, ctx->stream>>>(plan.d, cfl, plan.R, t_end, dt_max);
+            BSN_TRY(launch_check(ctx, "fmrN_dt_kernel"));
+            nested_sync_kernel<<<1, 1, 0, ctx->stream>>>(r, plan.d);
+            BSN_TRY(launch_check(ctx, "coupled_nested_sync_kernel"));
+            // gas force on every BH from the composite of the levels
+            for (int i = 0; i < nbh; ++i) {
+                for (int l = 0; l < nl; ++l) {
+                    const NLevel& v = plan.L[l];
+                    Box skip{{1, 1, 1}, {0, 0, 0}};
+                    if (l < nl - 1)
+                        for (int d = 0; d < 3; ++d) {
+                            skip.lo[d] = plan.P[l].G.lo[d] - 1;
+                            skip.hi[d] = plan.P[l].G.hi[d] - 1;
+                        }
+                    gas_force_kernel<<<blocks, 256, 0, ctx->stream>>>(v.U, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz, ox[l],
+                                                                      oy[l], oz[l], r, i, part + 6 * blocks * l, skip);
+                    BSN_TRY(launch_check(ctx, "coupled_gas_force_kernel"));
+                }
+                gas_force_finish<<<1, 32, 0, ctx->stream>>>(part, blocks * nl, r, i);
+                BSN_TRY(launch_check(ctx, "coupled_gas_force_finish"));
+            }
+            if (evolve_orbit && nbh > 0) {
+                nbody_kernel<<<1, 32, 0, ctx->stream>>>(r);
+                BSN_TRY(launch_check(ctx, "coupled_nbody_kernel"));
+            }
+            fill_kernel<<<1, 32, 0, ctx->stream>>>(r, f_sink, torque_free, rho_sink_min, t_bh2_sink_on);
+            BSN_TRY(launch_check(ctx, "coupled_fill_kernel"));
+            BSN_TRY(plan.step());
+            for (int i = 0; i < nbh; ++i) {
+                accrete_kernel<<<1, 32, 0, ctx->stream>>>(fin.U, fin.nx, fin.ny, fin.nz, fin.dx, fin.dy, fin.dz,
+                                                          ox[nl - 1], oy[nl - 1], oz[nl - 1], r, i, f_sink,
+                                                          rho_sink_min);
+                BSN_TRY(launch_check(ctx, "coupled_accrete_kernel"));
+            }
+            n_advance_kernel<<<1, 1, 0, ctx->stream>>>(plan.d);
+            BSN_TRY(launch_check(ctx, "fmrN_advance_kernel"));
+            nested_sync_kernel<<<1, 1, 0, ctx->stream>>>(r, plan.d);
+            BSN_TRY(launch_check(ctx, "coupled_nested_sync_kernel"));
+            if (diag_out) {
+                const NLevel& v = plan.L[0];
+                BSN_TRY(diag::launch(ctx, v.U, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz, x0, y0, z0, r->bh, &r->nbh, nbh,
+                                     plan.gamma, dpart, diag_out, &r->t, &r->dt, &r->steps, &r->done, diag_cap));
+            }
+            return BSN_OK;
+        };
+        bsn_status cst = body();
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        ctx->stream = user;
+        ctx->profiling = prof;
+        S->kernels = (int)(ctx->launches - l0);
+        ctx->launches = l0;
+        if (cst != BSN_OK) { if (graph) cudaGraphDestroy(graph); return cst; }
+        BSN_CUDA(ctx, e);
+        S->graph = graph;
+        BSN_CUDA(ctx, cudaGraphInstantiate(&S->exec, graph, 0));
+        S->key_pairs.assign(pairs, pairs + npairs);
+        S->prec = precision; S->sg = self_gravity; S->G_grav = 1.0; S->cfl = cfl; S->t_end = t_end;
+        memcpy(S->tiles, tiles, sizeof(tiles));
+        S->key_base = S->arena.base;
+        S->key_extra = extra;
+    }
+    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps, t_end > 0.0, plan.done, S->ev,
+                         (volatile int*)((char*)h + sizeof(Dev) + sizeof(NDev))));
+    NDev* hn = (NDev*)((char*)h + sizeof(Dev));
+    BSN_CUDA(ctx, cudaMemcpyAsync(h, r, sizeof(Dev), cudaMemcpyDeviceToHost, ctx->stream));
+    BSN_CUDA(ctx, cudaMemcpyAsync(hn, plan.d, sizeof(NDev), cudaMemcpyDeviceToHost, ctx->stream));
+    BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    Dev d;
+    memcpy(&d, h, sizeof(Dev));
+    *t_inout = hn->t;
+    if (steps_done) *steps_done = hn->steps;
+    for (int i = 0; i < nbh; ++i) bhs[i] = d.bh[i];
+    if (hn->done == 2)
+        return set_err(ctx, BSN_ERR_NONFINITE, "time step collapsed to 0 at t = %.17g (infinite signal speed)", hn->t);
     return BSN_OK;
 }

@@ -19,28 +19,11 @@
 // substeps unwind deepest level first, each again batching its own chain.
 // For three levels of ratio 2 that is 6 stage launches per coarse step in place
 // of 21.
-#include "fmr.cuh"
+#include "fmr_nested.cuh"
 #include "poisson.cuh"
 
 namespace bsn {
 namespace fmr {
-
-constexpr int NMAXL = f64::MAXLEV;   // levels
-constexpr int NMAXQ = 64;            // batched stage launches per coarse step
-
-struct NDev {
-    double dt[NMAXL];                // substep dt of each level
-    double t;
-    unsigned long long sm[NMAXL];    // CFL maxima (double bits)
-    unsigned int nan[NMAXL];
-    int done, steps;
-    unsigned int queue[NMAXQ];       // block queues of the batched launches (zeroed every step)
-};
-
-struct Ratios {
-    int r[NMAXL];
-    int n;                           // levels
-};
 
 __device__ void n_set_level_dts(NDev* d, double dt0, const Ratios& R) {
     d->dt[0] = dt0;
@@ -61,8 +44,8 @@ __global__ void n_fixed_dt_kernel(NDev* d, double dt0, Ratios R) { n_set_level_d
 
 // cfl_dt_fmr3d over N levels: min over levels of (product of the ratios
 // above the level) x cfl / max speed (Inf for a NaN or zero maximum), then the
-// t_end clamp (src/fmr3d.jl:616-622).
-__global__ void n_dt_kernel(NDev* d, double cfl, Ratios R, double t_end) {
+// dt_max cap (> 0) and the t_end clamp (src/fmr3d.jl:616-622).
+__global__ void n_dt_kernel(NDev* d, double cfl, Ratios R, double t_end, double dt_max) {
     if (d->done) return;
     double dt = 0.0;
     int fac = 1;
@@ -74,6 +57,7 @@ __global__ void n_dt_kernel(NDev* d, double cfl, Ratios R, double t_end) {
         d->sm[l] = 0ull;
         d->nan[l] = 0u;
     }
+    if (dt_max > 0.0) dt = jmin(dt, dt_max);
     if (t_end > 0.0) {
         if (!(d->t < t_end)) { d->done = 1; return; }
         dt = jmin(dt, t_end - d->t);
@@ -88,70 +72,7 @@ __global__ void n_advance_kernel(NDev* d) {
     d->steps += 1;
 }
 
-struct NLevel {
-    double *U, *Ucn, *A, *B, *Gh, *phi;
-    int nx, ny, nz;
-    double dx, dy, dz;
-};
-
-struct NPair {
-    Geo G;
-    Regs Rc, Rf;
-    double* regs;                    // Rc and Rf, contiguous
-    long long nregs;                 // doubles in regs
-    long long nfine;                 // threads of fine_reg_kernel
-    long long ncorr;                 // threads of bc_correct_kernel
-};
-
-// Device buffers of all levels and pairs in one allocation, laid out from the
-// level sizes (the same sizes give the same pointers, so a captured graph
-// stays valid).
-struct NArena {
-    void* base = nullptr;
-    size_t bytes = 0;
-};
-
-struct NState {
-    NArena arena;
-    NDev* dev = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    int kernels = 0;
-    std::vector<bsn_fmr2> key_pairs;
-    int prec = -1, sg = 0;
-    double G_grav = 0, cfl = 0, t_end = 0;
-    int tiles[NMAXL] = {-1, -1, -1, -1};
-    void* key_base = nullptr;
-    cudaStream_t cap = nullptr;
-    cudaEvent_t ev[2] = {nullptr, nullptr};
-    void release() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        exec = nullptr;
-        graph = nullptr;
-    }
-};
-
-struct NPlan {
-    bsn_ctx* ctx = nullptr;
-    int nl = 0, prec = PREC_F64, sg = 0;
-    double G_grav = 1.0;
-    NLevel L[NMAXL];
-    NPair P[NMAXL - 1];
-    f64::StageArgs base[NMAXL];
-    Ratios R;
-    NDev* d = nullptr;
-    const int* done = nullptr;
-    int qn = 0;
-    double rho_floor = 0, P_floor = 0, gamma = 0;
-    int bc = 0;
-
-    bsn_status chain(int l, double alpha);
-    bsn_status gravity();
-    bsn_status step();
-};
-
-static const double kRkW[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+const double kRkW[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
 
 bsn_status NPlan::chain(int l, double alpha) {
     // substep starts of levels l..nl-1: saved states and fresh registers
@@ -245,7 +166,7 @@ bsn_status NPlan::step() {
 static size_t align_up(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // Validate the chain, lay out the arena and fill the plan.
-static bsn_status make_plan(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, int prec, int sg, double G_grav,
+bsn_status make_plan(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, int prec, int sg, double G_grav,
                             NState* S, NPlan& plan) {
     if (!pairs || npairs < 1 || npairs > NMAXL - 1)
         return set_err(ctx, BSN_ERR_ARG, "need 1..%d level pairs, got %d", NMAXL - 1, npairs);
@@ -450,7 +371,7 @@ bsn_status fmrN_run(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, double cfl,
                 BSN_TRY(f64_cfl_fold(ctx, v.U, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz, plan.gamma, &plan.d->sm[l],
                                      &plan.d->nan[l]));
             }
-            n_dt_kernel<<<1, 1, 0, ctx->stream>>>(plan.d, cfl, plan.R, t_end);
+            n_dt_kernel<<<1, 1, 0, ctx->stream>>>(plan.d, cfl, plan.R, t_end, 0.0);
             BSN_TRY(launch_check(ctx, "fmrN_dt_kernel"));
             BSN_TRY(plan.step());
             n_advance_kernel<<<1, 1, 0, ctx->stream>>>(plan.d);
@@ -487,15 +408,20 @@ bsn_status fmrN_run(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, double cfl,
 
 }  // namespace fmr
 
-void fmrN_state_free(bsn_ctx* ctx) {
-    if (!ctx->fmrN_state) return;
-    fmr::NState* S = (fmr::NState*)ctx->fmrN_state;
+namespace fmr {
+void nstate_destroy(NState* S) {
+    if (!S) return;
     S->release();
     if (S->arena.base) cudaFree(S->arena.base);
     if (S->cap) cudaStreamDestroy(S->cap);
     for (cudaEvent_t e : S->ev)
         if (e) cudaEventDestroy(e);
     delete S;
+}
+}  // namespace fmr
+
+void fmrN_state_free(bsn_ctx* ctx) {
+    fmr::nstate_destroy((fmr::NState*)ctx->fmrN_state);
     ctx->fmrN_state = nullptr;
 }
 

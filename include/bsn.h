@@ -266,6 +266,24 @@ bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs, int nbh, 
                                  double rho_sink_min, int evolve_orbit, int precision, int n_steps,
                                  double t_end, double* t_inout, int* steps_done, double* diag_out,
                                  int diag_cap);
+/* The same driver loop on nested FMR levels (no counterpart in the reference,
+ * whose coupled_step! runs on one uniform grid): per step dt = the nested CFL
+ * (bsn_cfl_dt_fmr_nested_f64, capped and clamped as above); the gas force on
+ * every BH from the composite of the levels (each level's cells except those
+ * its child covers); nbody_step!; one nested step (bsn_fmr_nested_step_f64)
+ * whose stages on every level carry BH gravity, self-gravity (Phi frozen per
+ * level-0 step, solved on level 0) and sinks in coupled_step!'s order, BHs
+ * frozen at their post-orbit state; accrete! from the finest level over dt.
+ * pairs: as bsn_fmr_nested_step_f64 (gamma, floors from pairs[0]); x0,y0,z0:
+ * lower corner of level 0 (each finer level starts at the lower face of its
+ * parent's cell ci_lo).  diag_out records are the diagnostics of level 0,
+ * which holds the restriction of the finer levels. */
+bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, bsn_bh* bhs, int nbh,
+                                        double x0, double y0, double z0, double cfl, double dt_max,
+                                        double f_sink, int torque_free, int self_gravity, double t_bh2_sink_on,
+                                        double rho_sink_min, int evolve_orbit, int precision, int n_steps,
+                                        double t_end, double* t_inout, int* steps_done, double* diag_out,
+                                        int diag_cap);
 /* The driver's diagnostics (src/diagnostics.jl:21-175) in one device
  * reduction: out[0] gas_energy_total, [1] gas_kinetic_total, [2..4]
  * gas_momentum_total, [5..7] gas_angular_momentum_total, [8]

@@ -1281,8 +1281,19 @@ extern "C" void orc_fmr3d_step(const orc_fmr* G, double dt_c, int self_gravity, 
  * Self-gravity: density restricted up the chain, one isolated solve on level 0,
  * trilinear Phi down the chain, frozen for the coarse step. */
 namespace {
+/* BH gravity and sinks on every level (the coupled step's stage sources in
+ * its order, scripts/run_sn50_fiducial.jl:756-818); x0/y0/z0 per level */
+struct NestedSrc {
+    orc_bh* bhs;
+    int nbh, nsink;
+    double f_sink;
+    int torque_free;
+    double rho_sink_min;
+    double x0[8], y0[8], z0[8];
+};
+
 void fmrN_level(const orc_fmr* P, int np, int l, double dt, const double* Upar, FluxReg* fr_par,
-                std::vector<std::vector<double>>& phis, int sg) {
+                std::vector<std::vector<double>>& phis, int sg, const NestedSrc* src) {
     const orc_fmr* down = l < np ? &P[l] : nullptr;
     const orc_fmr* up = l > 0 ? &P[l - 1] : nullptr;
     double* U; int nx, ny, nz; double dx, dy, dz;
@@ -1307,7 +1318,13 @@ void fmrN_level(const orc_fmr* P, int np, int l, double dt, const double* Upar, 
         }
         if (down) accumulate_fr_coarse(frc, S.Fx.data(), S.Fy.data(), S.Fz.data(), rk_w[stage], dt, down);
         if (up) accumulate_fr_fine(*fr_par, S.Fx.data(), S.Fy.data(), S.Fz.data(), rk_w[stage], dt, up);
+        if (src)
+            orc_add_bh_gravity_source(S.dU.data(), U, nx, ny, nz, dx, dy, dz, src->bhs, src->nbh, src->x0[l],
+                                      src->y0[l], src->z0[l]);
         if (sg) orc_sg_gradient(S.dU.data(), U, phis[l].data(), nx, ny, nz, dx, dy, dz);
+        if (src)
+            orc_add_sink_sources(S.dU.data(), U, nx, ny, nz, dx, dy, dz, src->bhs, src->nsink, src->x0[l],
+                                 src->y0[l], src->z0[l], src->f_sink, src->torque_free, src->rho_sink_min);
         if (stage == 0) combine1(U, S.Un.data(), S.dU.data(), dt, n);
         else if (stage == 1) combine2(U, S.Un.data(), S.dU.data(), dt, n);
         else combine3(U, S.Un.data(), S.dU.data(), dt, n);
@@ -1320,15 +1337,14 @@ void fmrN_level(const orc_fmr* P, int np, int l, double dt, const double* Upar, 
     for (int sub = 0; sub < r; ++sub) {
         double alpha = (double)sub / (double)r;
         for (long t = 0; t < n; ++t) Ui[t] = (1.0 - alpha) * S.Un[t] + alpha * Unp1[t];
-        fmrN_level(P, np, l + 1, dt / (double)r, Ui.data(), &frf, phis, sg);
+        fmrN_level(P, np, l + 1, dt / (double)r, Ui.data(), &frf, phis, sg, src);
     }
     orc_restrict(U, down->Uf, down);
     bc_correct(down, frc, frf);
     orc_apply_floors(U, nx, ny, nz, rfl, Pfl, g);
 }
-}  // namespace
 
-extern "C" void orc_fmrN_step(const orc_fmr* P, int npairs, double dt0, int self_gravity, double G_grav) {
+void fmrN_core(const orc_fmr* P, int npairs, double dt0, int self_gravity, double G_grav, const NestedSrc* src) {
     std::vector<std::vector<double>> phis(npairs + 1);
     if (self_gravity) {
         for (int k = npairs - 1; k >= 0; --k) orc_restrict_density_to_coarse(&P[k]);
@@ -1347,7 +1363,91 @@ extern "C" void orc_fmrN_step(const orc_fmr* P, int npairs, double dt0, int self
         if (G_grav != 1.0)
             for (auto& ph : phis) for (auto& v : ph) v *= G_grav;
     }
-    fmrN_level(P, npairs, 0, dt0, nullptr, nullptr, phis, self_gravity);
+    fmrN_level(P, npairs, 0, dt0, nullptr, nullptr, phis, self_gravity, src);
+}
+
+}  // namespace
+
+extern "C" void orc_fmrN_step(const orc_fmr* P, int npairs, double dt0, int self_gravity, double G_grav) {
+    fmrN_core(P, npairs, dt0, self_gravity, G_grav, nullptr);
+}
+
+/* origin (lower corner) of every level from level 0's; levels[k+1] starts at
+ * the lower face of coarse cell ci_lo of level k */
+static void level_origins(const orc_fmr* P, int npairs, double x0, double y0, double z0, double* xs, double* ys,
+                          double* zs) {
+    xs[0] = x0; ys[0] = y0; zs[0] = z0;
+    for (int k = 0; k < npairs; ++k) {
+        xs[k + 1] = xs[k] + (double)(P[k].ci_lo - 1) * P[k].dxc;
+        ys[k + 1] = ys[k] + (double)(P[k].cj_lo - 1) * P[k].dyc;
+        zs[k + 1] = zs[k] + (double)(P[k].ck_lo - 1) * P[k].dzc;
+    }
+}
+
+/* gas_force_on_bh (src/gravity_bh.jl:91-113) over the composite of nested
+ * levels: every level's active cells except those its child covers, levels
+ * in order, cells in (k, j, i) order */
+extern "C" void orc_gas_force_fmrN(const orc_fmr* P, int npairs, const orc_bh* bh, double x0, double y0, double z0,
+                                   double out[3]) {
+    double xs[8], ys[8], zs[8];
+    level_origins(P, npairs, x0, y0, z0, xs, ys, zs);
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    const int ng = NG;
+    for (int l = 0; l <= npairs; ++l) {
+        const double* U; int nx, ny, nz; double dx, dy, dz;
+        if (l < npairs) { U = P[l].Uc; nx = P[l].ncx; ny = P[l].ncy; nz = P[l].ncz; dx = P[l].dxc; dy = P[l].dyc; dz = P[l].dzc; }
+        else { U = P[l - 1].Uf; nx = P[l - 1].nfx; ny = P[l - 1].nfy; nz = P[l - 1].nfz; dx = P[l - 1].dxf; dy = P[l - 1].dyf; dz = P[l - 1].dzf; }
+        Idx I(nx, ny, nz);
+        double dV = dx * dy * dz;
+        for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i) {
+            if (l < npairs && i >= P[l].ci_lo && i <= P[l].ci_hi && j >= P[l].cj_lo && j <= P[l].cj_hi &&
+                k >= P[l].ck_lo && k <= P[l].ck_hi)
+                continue;
+            double xc = xs[l] + ((double)i - 0.5) * dx;
+            double yc = ys[l] + ((double)j - 0.5) * dy;
+            double zc = zs[l] + ((double)k - 0.5) * dz;
+            double ddx = xc - bh->pos[0], ddy = yc - bh->pos[1], ddz = zc - bh->pos[2];
+            double r2 = sq(ddx) + sq(ddy) + sq(ddz) + sq(bh->eps);
+            double r3 = r2 * std::sqrt(r2);
+            double fac = bh->mass / r3 * U[I(1, ng + i, ng + j, ng + k)] * dV;
+            Fx += fac * ddx; Fy += fac * ddy; Fz += fac * ddz;
+        }
+    }
+    out[0] = Fx; out[1] = Fy; out[2] = Fz;
+}
+
+/* coupled_step! (scripts/run_sn50_fiducial.jl:756-818) on nested levels: gas
+ * force on every BH from the composite, the BH orbit (nbody_step!) over dt0,
+ * one nested step with BH gravity and sinks on every level (BHs frozen at
+ * their post-orbit state for the whole level-0 step, Phi frozen as in
+ * fmr3d_step!), then accrete! of every active sink from the finest level
+ * over dt0. */
+extern "C" void orc_coupled_fmrN_step(const orc_fmr* P, int npairs, orc_bh* bhs, int nbh, double dt0, double t,
+                                      double x0, double y0, double z0, double f_sink, int torque_free,
+                                      int self_gravity, double t_bh2_sink_on, double rho_sink_min,
+                                      int evolve_orbit, double* Fgas) {
+    NestedSrc src;
+    src.bhs = bhs; src.nbh = nbh;
+    src.nsink = (t < t_bh2_sink_on) ? std::min(1, nbh) : nbh;
+    src.f_sink = f_sink; src.torque_free = torque_free; src.rho_sink_min = rho_sink_min;
+    level_origins(P, npairs, x0, y0, z0, src.x0, src.y0, src.z0);
+    for (int i = 0; i < nbh; ++i) {
+        orc_gas_force_fmrN(P, npairs, &bhs[i], x0, y0, z0, Fgas + 3 * i);
+        double* F = Fgas + 3 * i;
+        bool fin = std::isfinite(F[0]) && std::isfinite(F[1]) && std::isfinite(F[2]);
+        if (!fin || std::sqrt(sq(F[0]) + sq(F[1]) + sq(F[2])) > 1e3) { F[0] = F[1] = F[2] = 0.0; }
+    }
+    if (evolve_orbit) {
+        bool ok = true;
+        for (int i = 0; i < nbh; ++i)
+            for (int d = 0; d < 3; ++d) ok = ok && std::isfinite(bhs[i].pos[d]) && std::isfinite(bhs[i].vel[d]);
+        if (ok) orc_nbody_step(bhs, nbh, dt0, Fgas);
+    }
+    fmrN_core(P, npairs, dt0, self_gravity, 1.0, &src);
+    const orc_fmr& f = P[npairs - 1];
+    for (int i = 0; i < src.nsink; ++i)
+        orc_accrete(&bhs[i], f.Uf, f.nfx, f.nfy, f.nfz, f.dxf, f.dyf, f.dzf, src.x0[npairs], src.y0[npairs],
+                    src.z0[npairs], dt0, f_sink, rho_sink_min);
 }
 
 /* cfl_dt_fmr3d generalised: min over levels of (product of ratios above it) x dt_level */

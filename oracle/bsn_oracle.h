@@ -123,6 +123,15 @@ double orc_cfl_dt_fmr3d(const orc_fmr* G, double cfl);
 /* N nested levels: pairs[k].Uf is pairs[k+1].Uc */
 void   orc_fmrN_step(const orc_fmr* pairs, int npairs, double dt0, int self_gravity, double G_grav);
 double orc_cfl_dt_fmrN(const orc_fmr* pairs, int npairs, double cfl);
+/* gas_force_on_bh over the composite of nested levels (level 0 origin x0,y0,z0) */
+void   orc_gas_force_fmrN(const orc_fmr* pairs, int npairs, const orc_bh* bh, double x0, double y0, double z0,
+                          double out[3]);
+/* coupled_step! on nested levels: composite gas force, orbit, nested step
+ * with BH gravity / self-gravity / sinks on every level, accretion on the
+ * finest level */
+void   orc_coupled_fmrN_step(const orc_fmr* pairs, int npairs, orc_bh* bhs, int nbh, double dt0, double t,
+                             double x0, double y0, double z0, double f_sink, int torque_free, int self_gravity,
+                             double t_bh2_sink_on, double rho_sink_min, int evolve_orbit, double* Fgas);
 void   orc_restrict_density_to_coarse(const orc_fmr* G);
 void   orc_prolong_scalar_trilinear(double* phi_f, const double* phi_c, const orc_fmr* G);
 void   orc_solve_fmr_poisson(const orc_fmr* G, double* phi_c, double* phi_f);

@@ -97,6 +97,9 @@ def _declare(L):
         "orc_cfl_dt_fmr3d": (d, [C.POINTER(OrcFMR), d]),
         "orc_fmrN_step": (V, [C.POINTER(OrcFMR), i, d, i, d]),
         "orc_cfl_dt_fmrN": (d, [C.POINTER(OrcFMR), i, d]),
+        "orc_gas_force_fmrN": (V, [C.POINTER(OrcFMR), i, C.POINTER(OrcBH), d, d, d, P]),
+        "orc_coupled_fmrN_step": (V, [C.POINTER(OrcFMR), i, C.POINTER(OrcBH), i, d, d, d, d, d, d, i, i, d, d, i,
+                                      P]),
         "orc_restrict_density_to_coarse": (V, [C.POINTER(OrcFMR)]),
         "orc_prolong_scalar_trilinear": (V, [P, P, C.POINTER(OrcFMR)]),
         "orc_solve_fmr_poisson": (V, [C.POINTER(OrcFMR), P, P]),
@@ -350,6 +353,21 @@ class FMRHierarchy:
 
     def cfl_dt(self, cfl):
         return lib().orc_cfl_dt_fmrN(self._arr, len(self.pairs), cfl)
+
+    def gas_force(self, bh, x0, y0, z0):
+        out = np.zeros(3)
+        lib().orc_gas_force_fmrN(self._arr, len(self.pairs), C.byref(bh), x0, y0, z0, out.ctypes.data_as(_dp))
+        return out
+
+    def coupled_step(self, bhs_arr, nbh, dt0, t, x0, y0, z0, f_sink, torque_free, self_gravity, t_bh2_sink_on,
+                     rho_sink_min, evolve_orbit=True):
+        """coupled_step! on the nested levels (composite gas force, orbit,
+        nested step with sources on every level, accretion on the finest)."""
+        Fg = np.zeros(3 * max(nbh, 1))
+        lib().orc_coupled_fmrN_step(self._arr, len(self.pairs), bhs_arr, nbh, dt0, t, x0, y0, z0, f_sink,
+                                    int(torque_free), int(self_gravity), t_bh2_sink_on, rho_sink_min,
+                                    int(evolve_orbit), Fg.ctypes.data_as(_dp))
+        return Fg[: 3 * nbh].reshape(nbh, 3)
 
 
 def lag5_weights(ratio):

@@ -108,3 +108,37 @@ def test_three_level_covered_cells_are_restrictions(orc):
         mean = kids.mean(axis=(2, 4, 6))
         cov = Up[:, NG + ilo - 1:NG + ihi, NG + jlo - 1:NG + jhi, NG + klo - 1:NG + khi]
         assert np.allclose(cov, mean, rtol=1e-14, atol=0), k
+
+
+def test_nested_coupled_step_without_bhs_is_the_nested_step(orc):
+    from binary_ic import binary_nested_setup
+    H1, *_ = binary_nested_setup(orc)
+    H2, boxes, dx0, x0, _ = binary_nested_setup(orc)
+    for t in (0.0, 1.0):
+        dt = H1.cfl_dt(0.4)
+        H1.step(dt, self_gravity=True)
+        H2.coupled_step(orc.bh_array([]), 0, dt, t, x0, x0, x0, 1.0, True, True, 0.0, 0.0)
+    for A, B in zip(H1.levels, H2.levels):
+        assert np.array_equal(A, B)
+
+
+def test_nested_coupled_step_sinks_and_orbit(orc):
+    from binary_ic import binary_nested_setup
+    H, boxes, dx0, x0, specs = binary_nested_setup(orc)
+    bo = orc.bh_array([orc.make_bh(s["pos"], s["vel"], s["mass"], s["eps"], s["c_code"], s["r_floor"])
+                       for s in specs])
+    a = (0,) + (slice(NG, -NG),) * 3
+    t, M0, mb0 = 0.0, None, None
+    for k in range(3):
+        dt = H.cfl_dt(0.4)
+        Fg = H.coupled_step(bo, 2, dt, t, x0, x0, x0, 1.0, True, True, 0.0, 2e-8)
+        t += dt
+        if k == 0:   # level 0 holds the restriction of the finer levels' own states from here on
+            M0, mb0 = H.levels[0][a].sum() * dx0 ** 3, bo[0].mass + bo[1].mass
+    assert np.isfinite(Fg).all() and np.abs(Fg).max() > 0
+    # the sinks drained gas and the BHs gained it
+    assert bo[0].mass + bo[1].mass > mb0 > 10.0
+    assert H.levels[0][a].sum() * dx0 ** 3 < M0
+    # the orbit moved the BHs (counter-clockwise, mirror-symmetric pair)
+    assert bo[0].pos[1] > 0 and bo[1].pos[1] < 0
+    assert abs(bo[0].pos[0] + bo[1].pos[0]) < 1e-3 * abs(bo[0].pos[0])
