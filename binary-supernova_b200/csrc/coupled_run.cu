@@ -14,6 +14,7 @@
 #include "poisson.cuh"
 #include "stage_launch.cuh"
 #include "fmr_nested.cuh"
+#include "sums.cuh"
 
 namespace bsn {
 namespace crun {
@@ -61,20 +62,9 @@ __global__ void advance_kernel(Dev* r) {
 }
 
 // gas_force_on_bh partial sums for BH i (compensated, as f64::gas_force_kernel)
-struct DD { double hi, lo; };
-__device__ __forceinline__ void dd_add(DD& s, double x) {
-    double t = s.hi + x;
-    double bp = t - s.hi;
-    double e = (s.hi - (t - bp)) + (x - bp);
-    s.hi = t;
-    s.lo += e;
-}
-__device__ __forceinline__ DD dd_merge(DD a, DD b) {
-    DD s = a;
-    dd_add(s, b.hi);
-    s.lo += b.lo;
-    return s;
-}
+using sums::DD;
+using sums::dd_add;
+using sums::dd_merge;
 
 // active cells [lo, hi] (0-based, inclusive per axis) left out of a sum: the
 // region a finer level covers; lo > hi leaves nothing out
@@ -127,13 +117,10 @@ __global__ void gas_force_kernel(const double* U, int nx, int ny, int nz, double
 // total of BH i's partials, zeroed when non-finite or above 1e3 in norm (the
 // driver's guard, scripts/run_sn50_fiducial.jl:765-769)
 __global__ void gas_force_finish(const double* part, int nblocks, Dev* r, int i) {
-    if (r->done || threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (r->done || blockIdx.x != 0) return;
     double F[3];
-    for (int d = 0; d < 3; ++d) {
-        DD acc = {0.0, 0.0};
-        for (int b = 0; b < nblocks; ++b) acc = dd_merge(acc, DD{part[6 * b + 2 * d], part[6 * b + 2 * d + 1]});
-        F[d] = acc.hi + acc.lo;
-    }
+    sums::merge_partials3<256>(part, nblocks, F);
+    if (threadIdx.x != 0) return;
     bool fin = isfinite(F[0]) && isfinite(F[1]) && isfinite(F[2]);
     if (!fin || sqrt(F[0] * F[0] + F[1] * F[1] + F[2] * F[2]) > 1e3) F[0] = F[1] = F[2] = 0.0;
     for (int d = 0; d < 3; ++d) r->Fg[3 * i + d] = F[d];
@@ -227,7 +214,7 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? l
 // in the reference's (k, j, i) order over the sphere's index box, one thread
 __global__ void accrete_kernel(const double* U, int nx, int ny, int nz, double dx, double dy, double dz, double x0,
                                double y0, double z0, Dev* r, int i, double f_sink, double rho_min) {
-    if (r->done || threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (r->done || blockIdx.x != 0) return;
     if (i >= r->ssrc.n) return;
     bsn_bh& bh = r->bh[i];
     const double rs = r_sink(bh), ts = t_sink(bh, f_sink);
@@ -242,27 +229,16 @@ __global__ void accrete_kernel(const double* U, int nx, int ny, int nz, double d
     if (!isfinite(rs) || !isfinite(bh.pos[0]) || !isfinite(bh.pos[1]) || !isfinite(bh.pos[2])) {
         ilo = 0; ihi = nx - 1; jlo = 0; jhi = ny - 1; klo = 0; khi = nz - 1;
     }
-    Geom G(nx, ny, nz);
-    double dm = 0.0, dPx = 0.0, dPy = 0.0, dPz = 0.0;
-    for (int c = klo; c <= khi; ++c)
-        for (int b = jlo; b <= jhi; ++b)
-            for (int a = ilo; a <= ihi; ++a) {
-                double xc, yc, zc;
-                f64::cell_xyz(a, b, c, x0, y0, z0, dx, dy, dz, xc, yc, zc);
-                double rr = sqrt(sq(xc - bh.pos[0]) + sq(yc - bh.pos[1]) + sq(zc - bh.pos[2]));
-                if (rr >= rs) continue;
-                long long o = G.act(a, b, c);
-                if (U[o] <= rho_min) continue;
-                dm += U[o] * rate;
-                dPx += U[o + 1] * rate;
-                dPy += U[o + 2] * rate;
-                dPz += U[o + 3] * rate;
-            }
+    double v[4];
+    sums::sink_sums<256>(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, bh.pos[0], bh.pos[1], bh.pos[2], rs, rate, rho_min,
+                         ilo, ihi, jlo, jhi, klo, khi, v);
+    if (threadIdx.x != 0) return;
+    const double dm = v[0];
     if (dm > 0.0) {
         double M_new = bh.mass + dm;
-        bh.vel[0] = (bh.mass * bh.vel[0] + dPx) / M_new;
-        bh.vel[1] = (bh.mass * bh.vel[1] + dPy) / M_new;
-        bh.vel[2] = (bh.mass * bh.vel[2] + dPz) / M_new;
+        bh.vel[0] = (bh.mass * bh.vel[0] + v[1]) / M_new;
+        bh.vel[1] = (bh.mass * bh.vel[1] + v[2]) / M_new;
+        bh.vel[2] = (bh.mass * bh.vel[2] + v[3]) / M_new;
         bh.mass = M_new;
     }
 }
@@ -390,7 +366,7 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
                 gas_force_kernel<<<blocks, 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dx, dx, x0, y0, z0, r, i, part,
                                                                   Box{{1, 1, 1}, {0, 0, 0}});
                 BSN_TRY(launch_check(ctx, "coupled_gas_force_kernel"));
-                gas_force_finish<<<1, 32, 0, ctx->stream>>>(part, blocks, r, i);
+                gas_force_finish<<<1, 256, 0, ctx->stream>>>(part, blocks, r, i);
                 BSN_TRY(launch_check(ctx, "coupled_gas_force_finish"));
             }
             if (evolve_orbit && nbh > 0) {
@@ -419,7 +395,7 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
             }
             BSN_TRY(f64_ghost_combine(ctx, U, B, nullptr, nx, ny, nz, BSN_BC_OUTFLOW, 0.0, &r->dt, &r->done));
             for (int i = 0; i < nbh; ++i) {
-                accrete_kernel<<<1, 32, 0, ctx->stream>>>(U, nx, ny, nz, dx, dx, dx, x0, y0, z0, r, i, f_sink,
+                accrete_kernel<<<1, 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dx, dx, x0, y0, z0, r, i, f_sink,
                                                           rho_sink_min);
                 BSN_TRY(launch_check(ctx, "coupled_accrete_kernel"));
             }
@@ -605,7 +581,7 @@ extern "C" bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2*
                                                                       oy[l], oz[l], r, i, part + 6 * blocks * l, skip);
                     BSN_TRY(launch_check(ctx, "coupled_gas_force_kernel"));
                 }
-                gas_force_finish<<<1, 32, 0, ctx->stream>>>(part, blocks * nl, r, i);
+                gas_force_finish<<<1, 256, 0, ctx->stream>>>(part, blocks * nl, r, i);
                 BSN_TRY(launch_check(ctx, "coupled_gas_force_finish"));
             }
             if (evolve_orbit && nbh > 0) {
@@ -616,7 +592,7 @@ extern "C" bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2*
             BSN_TRY(launch_check(ctx, "coupled_fill_kernel"));
             BSN_TRY(plan.step());
             for (int i = 0; i < nbh; ++i) {
-                accrete_kernel<<<1, 32, 0, ctx->stream>>>(fin.U, fin.nx, fin.ny, fin.nz, fin.dx, fin.dy, fin.dz,
+                accrete_kernel<<<1, 256, 0, ctx->stream>>>(fin.U, fin.nx, fin.ny, fin.nz, fin.dx, fin.dy, fin.dz,
                                                           ox[nl - 1], oy[nl - 1], oz[nl - 1], r, i, f_sink,
                                                           rho_sink_min);
                 BSN_TRY(launch_check(ctx, "coupled_accrete_kernel"));

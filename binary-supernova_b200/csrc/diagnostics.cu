@@ -6,24 +6,14 @@
 // are compensated (two-sum), i.e. within about one rounding of the exact sum
 // (the reference's own `sum` is pairwise, so no summation order is "the" one).
 #include "diagnostics.cuh"
+#include "sums.cuh"
 
 namespace bsn {
 namespace diag {
 
-struct DD { double hi, lo; };
-__device__ __forceinline__ void dd_add(DD& s, double x) {
-    double t = s.hi + x;
-    double bp = t - s.hi;
-    double e = (s.hi - (t - bp)) + (x - bp);
-    s.hi = t;
-    s.lo += e;
-}
-__device__ __forceinline__ DD dd_merge(DD a, DD b) {
-    DD s = a;
-    dd_add(s, b.hi);
-    s.lo += b.lo;
-    return s;
-}
+using sums::DD;
+using sums::dd_add;
+using sums::dd_merge;
 
 __global__ void diag_kernel(const double* U, int nx, int ny, int nz, double dx, double dy, double dz, double x0,
                             double y0, double z0, const bsn_bh* bhs, const int* nbh_dev, int nbh, double g,

@@ -5,6 +5,7 @@
 
 #include "hydro_f64.cuh"
 #include "poisson.cuh"
+#include "sums.cuh"
 
 namespace bsn {
 namespace f64 {
@@ -97,20 +98,9 @@ __global__ void sg_gradient_kernel(double* dU, const double* U, const double* P,
 // Compensated (two-sum) accumulation: the parallel sum is accurate to about
 // one rounding of the exact sum, i.e. within the reference's own sequential
 // rounding error.
-struct DD { double hi, lo; };
-__device__ __forceinline__ void dd_add(DD& s, double x) {
-    double t = s.hi + x;
-    double bp = t - s.hi;
-    double e = (s.hi - (t - bp)) + (x - bp);
-    s.hi = t;
-    s.lo += e;
-}
-__device__ __forceinline__ DD dd_merge(DD a, DD b) {
-    DD s = a;
-    dd_add(s, b.hi);
-    s.lo += b.lo;
-    return s;
-}
+using sums::DD;
+using sums::dd_add;
+using sums::dd_merge;
 
 // gas_force_on_bh (src/gravity_bh.jl:91-113): out[3*blocks] partial (hi,lo).
 __global__ void gas_force_kernel(const double* U, int nx, int ny, int nz, double dx, double dy, double dz, double x0,
@@ -152,39 +142,21 @@ __global__ void gas_force_kernel(const double* U, int nx, int ny, int nz, double
 }
 
 __global__ void gas_force_finish(const double* part, int nblocks, double* out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    for (int d = 0; d < 3; ++d) {
-        DD acc = {0.0, 0.0};
-        for (int b = 0; b < nblocks; ++b) acc = dd_merge(acc, DD{part[6 * b + 2 * d], part[6 * b + 2 * d + 1]});
-        out[d] = acc.hi + acc.lo;
-    }
+    double F[3];
+    sums::merge_partials3<256>(part, nblocks, F);
+    if (threadIdx.x == 0) { out[0] = F[0]; out[1] = F[1]; out[2] = F[2]; }
 }
 
-// accrete! sums (src/sinks.jl:74-109) in the reference's exact loop order:
-// only cells inside the sink sphere contribute, so one thread walks the
-// (k,j,i) bounding box of the sphere in that order and reproduces the
-// sequential sum bit for bit.
+// accrete! sums (src/sinks.jl:74-109) in the reference's exact loop order
+// over the (k,j,i) bounding box of the sink sphere (sums::sink_sums), so the
+// sequential sum is reproduced bit for bit.
 __global__ void accrete_kernel(const double* U, int nx, int ny, int nz, double dx, double dy, double dz, double x0,
                                double y0, double z0, double px, double py, double pz, double rs, double rate,
                                double rho_min, int ilo, int ihi, int jlo, int jhi, int klo, int khi, double* out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    Geom G(nx, ny, nz);
-    double dm = 0.0, dPx = 0.0, dPy = 0.0, dPz = 0.0;
-    for (int c = klo; c <= khi; ++c)
-        for (int b = jlo; b <= jhi; ++b)
-            for (int a = ilo; a <= ihi; ++a) {
-                double xc, yc, zc;
-                cell_xyz(a, b, c, x0, y0, z0, dx, dy, dz, xc, yc, zc);
-                double r = sqrt(sq(xc - px) + sq(yc - py) + sq(zc - pz));
-                if (r >= rs) continue;
-                long long o = G.act(a, b, c);
-                if (U[o] <= rho_min) continue;
-                dm += U[o] * rate;
-                dPx += U[o + 1] * rate;
-                dPy += U[o + 2] * rate;
-                dPz += U[o + 3] * rate;
-            }
-    out[0] = dm; out[1] = dPx; out[2] = dPy; out[3] = dPz;
+    double v[4];
+    sums::sink_sums<256>(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, px, py, pz, rs, rate, rho_min, ilo, ihi, jlo, jhi,
+                         klo, khi, v);
+    if (threadIdx.x == 0) { out[0] = v[0]; out[1] = v[1]; out[2] = v[2]; out[3] = v[3]; }
 }
 
 }  // namespace f64
@@ -225,7 +197,7 @@ static bsn_status gas_force(bsn_ctx* ctx, const double* U, int nx, int ny, int n
     gas_force_kernel<<<blocks, 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, bh.pos[0], bh.pos[1],
                                                       bh.pos[2], bh.mass, bh.eps, part);
     BSN_TRY(launch_check(ctx, "gas_force_kernel"));
-    gas_force_finish<<<1, 32, 0, ctx->stream>>>(part, blocks, part + 6 * blocks);
+    gas_force_finish<<<1, 256, 0, ctx->stream>>>(part, blocks, part + 6 * blocks);
     BSN_TRY(launch_check(ctx, "gas_force_finish"));
     double* h = (double*)pinned(ctx, 64, &st); BSN_TRY(st);
     BSN_CUDA(ctx, cudaMemcpyAsync(h, part + 6 * blocks, 24, cudaMemcpyDeviceToHost, ctx->stream));
@@ -254,7 +226,7 @@ static bsn_status accrete(bsn_ctx* ctx, bsn_bh* bh, const double* U, int nx, int
     }
     bsn_status st;
     double* d = (double*)slot(ctx, SLOT_RED, 64, &st); BSN_TRY(st);
-    accrete_kernel<<<1, 32, 0, ctx->stream>>>(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, bh->pos[0], bh->pos[1],
+    accrete_kernel<<<1, 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, bh->pos[0], bh->pos[1],
                                               bh->pos[2], rs, rate, rho_min, ilo, ihi, jlo, jhi, klo, khi, d);
     BSN_TRY(launch_check(ctx, "accrete_kernel"));
     double* h = (double*)pinned(ctx, 64, &st); BSN_TRY(st);
