@@ -8,6 +8,12 @@ step, the loop the reference drivers run (cfl_dt_3d + euler3d_step!).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bsn|reference]
                   [--n 256] [--path learned|f32|f64] [--tile V] [--no-cpu]
                   [--no-accuracy] [--no-fmr]
+  python bench.py --workload binary_nested [--paths f64,f32,learned]
+                  [--steps K] [--warmup W]
+
+The second form times only the binary-BH supernova on three nested 128^3
+FMR levels (the coupled driver loop on the device) for the listed stencil
+paths and prints its JSON object.
 
 `value` is device-resident throughput over K steps (state in HBM).  `e2e`
 runs the same step through the public host-buffer path: the state is copied
@@ -270,7 +276,7 @@ def fmr_polytrope(bsn, torch, steps, warmup, log):
     return out
 
 
-def binary_nested(bsn, torch, steps, warmup, log, n=128):
+def binary_nested(bsn, torch, steps, warmup, log, n=128, paths=("f64", "f32", "learned")):
     """The binary-BH supernova on three nested FMR levels of n^3 (ratio 2) on
     [-8,8]^3, [-4,4]^3, [-2,2]^3: n=3 polytrope star (M=10, R=1, G=1, gamma
     4/3) with a thermal bomb E=1 in r<0.1 and two m=5 BH sinks at (+-1.5,0,0)
@@ -330,7 +336,8 @@ def binary_nested(bsn, torch, steps, warmup, log, n=128):
                       precision=prec, diag=rec)
         return H, b, common
 
-    for prec in ("f64", "f32", "learned"):
+    t64 = None
+    for prec in paths:
         H, b, common = fresh(prec, steps + warmup)
         t, _ = bsn.coupled_nested_run_steps(H, b, -L, -L, -L, 0.4, n_steps=warmup, **common)
         torch.cuda.synchronize()
@@ -348,8 +355,11 @@ def binary_nested(bsn, torch, steps, warmup, log, n=128):
             rho_f[prec] = H.levels[2][0].clone()
         del H
     # accuracy at equal time: the reduced-precision paths rerun to FP64's end time
+    if t64 is None:
+        return out
     out["accuracy_t"] = t64
-    for prec in ("f32", "learned"):
+    others = [p_ for p_ in paths if p_ != "f64"]
+    for prec in others:
         H, b, common = fresh(prec, 1)
         common["diag"] = None
         _, k = bsn.coupled_nested_run_steps(H, b, -L, -L, -L, 0.4, n_steps=10 * (steps + warmup), t_end=t64,
@@ -359,10 +369,9 @@ def binary_nested(bsn, torch, steps, warmup, log, n=128):
         del H
     a = (slice(3, -3),) * 3
     ref = rho_f["f64"][a]
-    for prec in ("f32", "learned"):
+    for prec in others:
         out[f"{prec}_L1_rho_finest_vs_f64"] = float((rho_f[prec][a] - ref).abs().sum() / ref.abs().sum())
-    out["speedup_f32_vs_f64"] = out["f64_device_loop_ms_per_step"] / out["f32_device_loop_ms_per_step"]
-    out["speedup_learned_vs_f64"] = out["f64_device_loop_ms_per_step"] / out["learned_device_loop_ms_per_step"]
+        out[f"speedup_{prec}_vs_f64"] = out["f64_device_loop_ms_per_step"] / out[f"{prec}_device_loop_ms_per_step"]
     return out
 
 
@@ -614,6 +623,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-fmr", action="store_true",
                     help="skip the two-level FMR polytrope and binary-BH coupled-loop timings")
+    ap.add_argument("--workload", default="sedov", choices=["sedov", "binary_nested"],
+                    help="binary_nested: time only the binary-BH supernova on three nested FMR levels")
+    ap.add_argument("--paths", default="f64,f32,learned",
+                    help="stencil paths of --workload binary_nested (comma-separated)")
     ap.add_argument("--tile", type=int, default=-1,
                     help="force this stage-kernel tile variant for both precisions (default: autotune)")
     args = ap.parse_args()
@@ -621,6 +634,13 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "binary_nested":
+        import torch
+        import bsn
+        paths = tuple(p_ for p_ in args.paths.split(",") if p_)
+        out = binary_nested(bsn, torch, args.steps, args.warmup, log, paths=paths)
+        print(json.dumps(out), flush=True)
         return
     if world > 1:
         import datetime
