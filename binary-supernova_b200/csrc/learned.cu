@@ -481,9 +481,50 @@ struct F32Learned {
                     f56 = 5.0f / 6.0f, k1312 = 13.0f / 12.0f;
         float L[5], Rv[5];
         unsigned need[2] = {0u, 0u};
+        // the smoothness test of field q from its stencil and indicators
+        auto test = [&](int q, float c0, float c1, float c2, float c3, float c4, float c5, float bA, float bB,
+                        float bC, float bD, float bE) {
+            // spreads about the common centre c2: left stencil c0..c4, right c1..c5
+            float m14 = fmaxf(fmaxf(fabsf(c1 - c2), fabsf(c3 - c2)), fabsf(c4 - c2));
+            float sL = fmaxf(m14, fabsf(c0 - c2)), sR = fmaxf(m14, fabsf(c5 - c2));
+            bool smL = fabsf(bA - bC) <= learned::THETA * (fminf(fminf(bA, bB), bC) + learned::BETA_EPS * sL * sL);
+            bool smR = fabsf(bB - bE) <= learned::THETA * (fminf(fminf(bB, bD), bE) + learned::BETA_EPS * sR * sR);
+            // spreads at FP32 rounding level of the centre value (or below
+            // WENO-Z's epsilon scale) carry no shape: WENO-Z stays.  This
+            // also keeps the network off the 1e-30-level precursor noise that
+            // upwind stencils leave ahead of a shock.
+            const float smin = fmaxf(learned::SPREAD_ABS, learned::SPREAD_REL_F32 * fabsf(c2));
+            need[0] |= (unsigned)(smL && sL > smin) << q;
+            need[1] |= (unsigned)(smR && sR > smin) << q;
+        };
+        // rho, m_x and m_y, m_z in packed pairs (f32x2), P alone
 #pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            const int col = q < 4 ? q : 5;
+        for (int q = 0; q < 4; q += 2) {
+            float v[6][2];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                v[i][0] = valid ? c[i][q] : 0.f;
+                v[i][1] = valid ? c[i][q + 1] : 0.f;
+            }
+            f32::f2 L2, R2, bA, bB, bC, bD, bE;
+            f32::weno5_lr2(f32::pk2(v[0][0], v[0][1]), f32::pk2(v[1][0], v[1][1]), f32::pk2(v[2][0], v[2][1]),
+                           f32::pk2(v[3][0], v[3][1]), f32::pk2(v[4][0], v[4][1]), f32::pk2(v[5][0], v[5][1]), L2,
+                           R2, bA, bB, bC, bD, bE);
+            f32::up2(L2, L[q], L[q + 1]);
+            f32::up2(R2, Rv[q], Rv[q + 1]);
+            if (quiet) continue;   // block-uniform
+            float A[2], B[2], C[2], Dd[2], E[2];
+            f32::up2(bA, A[0], A[1]);
+            f32::up2(bB, B[0], B[1]);
+            f32::up2(bC, C[0], C[1]);
+            f32::up2(bD, Dd[0], Dd[1]);
+            f32::up2(bE, E[0], E[1]);
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                test(q + h, v[0][h], v[1][h], v[2][h], v[3][h], v[4][h], v[5][h], A[h], B[h], C[h], Dd[h], E[h]);
+        }
+        {
+            const int q = 4, col = 5;
             float c0 = c[0][col], c1 = c[1][col], c2 = c[2][col], c3 = c[3][col], c4 = c[4][col], c5 = c[5][col];
             if (!valid) c0 = c1 = c2 = c3 = c4 = c5 = 0.f;
             float qA = t13 * c0 + m76 * c1 + e116 * c2;
@@ -502,19 +543,7 @@ struct F32Learned {
             float bE = fmaf(k1312 * s3, s3, 0.25f * e * e);
             L[q] = f32::wz(bA, bB, bC, 0.1f, 0.6f, 0.3f, qA, qB, qC);
             Rv[q] = f32::wz(bB, bD, bE, 0.3f, 0.6f, 0.1f, qB, qC, qD);
-            if (quiet) continue;   // block-uniform
-            // spreads about the common centre c2: left stencil c0..c4, right c1..c5
-            float m14 = fmaxf(fmaxf(fabsf(c1 - c2), fabsf(c3 - c2)), fabsf(c4 - c2));
-            float sL = fmaxf(m14, fabsf(c0 - c2)), sR = fmaxf(m14, fabsf(c5 - c2));
-            bool smL = fabsf(bA - bC) <= learned::THETA * (fminf(fminf(bA, bB), bC) + learned::BETA_EPS * sL * sL);
-            bool smR = fabsf(bB - bE) <= learned::THETA * (fminf(fminf(bB, bD), bE) + learned::BETA_EPS * sR * sR);
-            // spreads at FP32 rounding level of the centre value (or below
-            // WENO-Z's epsilon scale) carry no shape: WENO-Z stays.  This
-            // also keeps the network off the 1e-30-level precursor noise that
-            // upwind stencils leave ahead of a shock.
-            const float smin = fmaxf(learned::SPREAD_ABS, learned::SPREAD_REL_F32 * fabsf(c2));
-            need[0] |= (unsigned)(smL && sL > smin) << q;
-            need[1] |= (unsigned)(smR && sR > smin) << q;
+            if (!quiet) test(q, c0, c1, c2, c3, c4, c5, bA, bB, bC, bD, bE);
         }
         if (quiet) return finish<D>(c, k, L, Rv, F);
         // both sides' row counts in one prefix sum (8 bits each: at most 160 rows a side)

@@ -63,6 +63,100 @@ __device__ __forceinline__ void weno5_lr(float c0, float c1, float c2, float c3,
     R = wz(bB, bD, bE, 0.3f, 0.6f, 0.1f, qB, qC, qD);
 }
 
+// Two FP32 lanes in one 64-bit register pair.  sm_100's packed FP32
+// instructions (add/sub/mul/fma .f32x2) issue once for both lanes, each lane
+// rounding exactly as the scalar instruction would; the WENO5-Z arithmetic of
+// two reconstructed fields runs this way (divisions, min and abs per lane).
+struct f2 {
+    unsigned long long v;
+};
+__device__ __forceinline__ f2 pk2(float a, float b) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void up2(f2 x, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v)); }
+__device__ __forceinline__ f2 sp2(float a) { return pk2(a, a); }
+__device__ __forceinline__ f2 operator+(f2 a, f2 b) {
+    f2 d;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ f2 operator-(f2 a, f2 b) {
+    f2 d;
+    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ f2 operator*(f2 a, f2 b) {
+    f2 d;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+    f2 d;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return d;
+}
+
+// wz on two lanes: the same expressions as wz, lane by lane
+__device__ __forceinline__ f2 wz2(f2 b0, f2 b1, f2 b2, float d0, float d1, float d2, f2 q0, f2 q1, f2 q2) {
+    const float cap = 1e18f;
+    const f2 eps = sp2(1e-36f), one = sp2(1.0f);
+    f2 dt = b0 - b2;
+    f2 e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
+    float x, y, ex, ey;
+    up2(dt, x, y);
+    const float taux = fabsf(x), tauy = fabsf(y);
+    up2(e0, ex, ey);
+    f2 t0 = pk2(fminf(fdiv(taux, ex), cap), fminf(fdiv(tauy, ey), cap));
+    up2(e1, ex, ey);
+    f2 t1 = pk2(fminf(fdiv(taux, ex), cap), fminf(fdiv(tauy, ey), cap));
+    up2(e2, ex, ey);
+    f2 t2 = pk2(fminf(fdiv(taux, ex), cap), fminf(fdiv(tauy, ey), cap));
+    f2 a0 = sp2(d0) * fma2(t0, t0, one);
+    f2 a1 = sp2(d1) * fma2(t1, t1, one);
+    f2 a2 = sp2(d2) * fma2(t2, t2, one);
+    f2 num = fma2(a0, q0, fma2(a1, q1, a2 * q2));
+    f2 den = a0 + a1 + a2;
+    float nx, ny, dx, dy;
+    up2(num, nx, ny);
+    up2(den, dx, dy);
+    return pk2(fdiv(nx, dx), fdiv(ny, dy));
+}
+
+// weno5_lr on two fields at once (lane 0 and lane 1 of every argument); the
+// smoothness indicators bA..bE (left stencil: bA, bB, bC; right: bB, bD, bE)
+// are returned for callers that test them
+__device__ __forceinline__ void weno5_lr2(f2 c0, f2 c1, f2 c2, f2 c3, f2 c4, f2 c5, f2& L, f2& R, f2& bA, f2& bB,
+                                          f2& bC, f2& bD, f2& bE) {
+    const f2 t13 = sp2(1.0f / 3.0f), m76 = sp2(-7.0f / 6.0f), e116 = sp2(11.0f / 6.0f), m16 = sp2(-1.0f / 6.0f),
+             f56 = sp2(5.0f / 6.0f), k1312 = sp2(13.0f / 12.0f), m2 = sp2(-2.0f), m4 = sp2(-4.0f), p3 = sp2(3.0f),
+             q4 = sp2(0.25f);
+    f2 qA = fma2(e116, c2, fma2(m76, c1, t13 * c0));
+    f2 qB = fma2(t13, c3, fma2(f56, c2, m16 * c1));
+    f2 qC = fma2(m16, c4, fma2(f56, c3, t13 * c2));
+    f2 qD = fma2(t13, c5, fma2(m76, c4, e116 * c3));
+    f2 s0 = fma2(m2, c1, c0) + c2, s1 = fma2(m2, c2, c1) + c3, s2 = fma2(m2, c3, c2) + c4,
+       s3 = fma2(m2, c4, c3) + c5;
+    f2 a = fma2(p3, c2, fma2(m4, c1, c0));
+    f2 b = c1 - c3;
+    f2 c = fma2(m4, c3, p3 * c2) + c4;
+    f2 d = fma2(p3, c4, fma2(m4, c3, c2));
+    f2 e = fma2(m4, c4, p3 * c3) + c5;
+    bA = fma2(k1312 * s0, s0, q4 * a * a);
+    bB = fma2(k1312 * s1, s1, q4 * b * b);
+    f2 x2 = k1312 * s2 * s2;
+    bC = fma2(q4 * c, c, x2);
+    bD = fma2(q4 * d, d, x2);
+    bE = fma2(k1312 * s3, s3, q4 * e * e);
+    L = wz2(bA, bB, bC, 0.1f, 0.6f, 0.3f, qA, qB, qC);
+    R = wz2(bB, bD, bE, 0.3f, 0.6f, 0.1f, qB, qC, qD);
+}
+__device__ __forceinline__ void weno5_lr2(f2 c0, f2 c1, f2 c2, f2 c3, f2 c4, f2 c5, f2& L, f2& R) {
+    f2 bA, bB, bC, bD, bE;
+    weno5_lr2(c0, c1, c2, c3, c4, c5, L, R, bA, bB, bC, bD, bE);
+}
+
 __device__ __forceinline__ float cell_pressure(float r, float mx, float my, float mz, float E, float gm1) {
     r = fmaxf(r, 1e-30f);
     float KE = fdiv(0.5f * (mx * mx + my * my + mz * mz), r);
@@ -157,7 +251,13 @@ __device__ __forceinline__ void interface_flux(const float (&c)[6][6], float g, 
                                                float F[5]) {
     float L[5], R[5];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) weno5_lr(c[0][q], c[1][q], c[2][q], c[3][q], c[4][q], c[5][q], L[q], R[q]);
+    for (int q = 0; q < 4; q += 2) {
+        f2 L2, R2;
+        weno5_lr2(pk2(c[0][q], c[0][q + 1]), pk2(c[1][q], c[1][q + 1]), pk2(c[2][q], c[2][q + 1]),
+                  pk2(c[3][q], c[3][q + 1]), pk2(c[4][q], c[4][q + 1]), pk2(c[5][q], c[5][q + 1]), L2, R2);
+        up2(L2, L[q], L[q + 1]);
+        up2(R2, R[q], R[q + 1]);
+    }
     float PL, PR;
     weno5_lr(c[0][5], c[1][5], c[2][5], c[3][5], c[4][5], c[5][5], PL, PR);
     float PmaxL = fmaxf(fmaxf(fmaxf(fmaxf(c[0][5], c[1][5]), c[2][5]), c[3][5]), c[4][5]);
