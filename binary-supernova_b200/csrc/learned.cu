@@ -427,6 +427,9 @@ struct F32Learned {
     __device__ static float pressure(const float v[5], const Consts& k) {
         return f32::cell_pressure(v[0], v[1], v[2], v[3], v[4], k.gm1);
     }
+    __device__ static void floor(double (&v)[5], const f64::StageArgs& A) {
+        f32::floor_screened(v, A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+    }
     __device__ static void prologue(unsigned char* psm, const f64::StageArgs& A, int nt) {
         const unsigned char* src = (const unsigned char*)A.mlp;
         for (int i = threadIdx.x; i < 2 * learned::PK_BYTES; i += nt) psm[i] = src[i];

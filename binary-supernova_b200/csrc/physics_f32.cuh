@@ -13,6 +13,7 @@
 #pragma once
 
 #include "bsn_internal.cuh"
+#include "physics.cuh"
 
 namespace bsn {
 namespace f32 {
@@ -155,6 +156,22 @@ __device__ __forceinline__ void weno5_lr2(f2 c0, f2 c1, f2 c2, f2 c3, f2 c4, f2 
 __device__ __forceinline__ void weno5_lr2(f2 c0, f2 c1, f2 c2, f2 c3, f2 c4, f2 c5, f2& L, f2& R) {
     f2 bA, bB, bC, bD, bE;
     weno5_lr2(c0, c1, c2, c3, c4, c5, L, R, bA, bB, bC, bD, bE);
+}
+
+// f64::apply_floor with the FP64 pressure test skipped where an FP32
+// estimate shows the cell far above both floors.  E - KE in FP32 is within
+// ~1e-6 (|E| + KE) of its exact value, so a margin of 1e-5 (|E| + KE) above
+// P_floor / (gamma - 1) means the FP64 test would change nothing; any cell
+// below that margin, below the density floor or non-finite takes the FP64
+// floor itself, so the result is apply_floor's in every case.
+__device__ __forceinline__ void floor_screened(double (&v)[5], double rho_floor, double P_floor, double Pfl_gm1,
+                                               double gm1) {
+    if (v[0] >= rho_floor) {
+        const float r = (float)v[0], mx = (float)v[1], my = (float)v[2], mz = (float)v[3], E = (float)v[4];
+        const float KE = fdiv(0.5f * fmaf(mz, mz, fmaf(my, my, mx * mx)), r);
+        if (E - KE > (float)Pfl_gm1 + 1e-5f * (fabsf(E) + KE)) return;
+    }
+    f64::apply_floor(v[0], v[1], v[2], v[3], v[4], rho_floor, P_floor, Pfl_gm1, gm1);
 }
 
 __device__ __forceinline__ float cell_pressure(float r, float mx, float my, float mz, float E, float gm1) {

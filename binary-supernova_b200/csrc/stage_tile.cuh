@@ -47,6 +47,10 @@ struct F64Physics {
     __device__ static void prologue(unsigned char*, const f64::StageArgs&, int) {}
     struct Consts { double g, gm1; };
     __device__ static Consts consts(const f64::StageArgs& A) { return {A.g, A.gm1}; }
+    // apply_floors (src/gpu_kernels.jl:26-46) on one cell, as the reference
+    __device__ static void floor(double (&v)[5], const f64::StageArgs& A) {
+        f64::apply_floor(v[0], v[1], v[2], v[3], v[4], A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+    }
     __device__ static double pressure(const double v[5], const Consts& k) {
         return f64::cell_pressure(v[0], v[1], v[2], v[3], v[4], k.gm1);
     }
@@ -142,7 +146,7 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
             double v[5];
             bool act;
             load_cell(A, G, D, a, b, c, v, act);
-            if (act) f64::apply_floor(v[0], v[1], v[2], v[3], v[4], A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+            if (act) P::floor(v, A);
             real w[5];
 #pragma unroll
             for (int q = 0; q < 5; ++q) { w[q] = (real)v[q]; sC[q * S::NEXT + e] = w[q]; }
@@ -336,7 +340,7 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
             double v[5];
             bool act;
             load_cell(A, G, d, a, b, c, v, act);
-            if (act) f64::apply_floor(v[0], v[1], v[2], v[3], v[4], A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+            if (act) P::floor(v, A);
             real w[5];
 #pragma unroll
             for (int q = 0; q < 5; ++q) { w[q] = (real)v[q]; sC[q * S::NCROSS + e] = w[q]; }
@@ -367,8 +371,9 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
             u0 = (double)sC[0 * FS + e]; u1 = (double)sC[1 * FS + e]; u2 = (double)sC[2 * FS + e];
             u3 = (double)sC[3 * FS + e]; u4 = (double)sC[4 * FS + e];
         } else {
-            u0 = A.Uin[off]; u1 = A.Uin[off + 1]; u2 = A.Uin[off + 2]; u3 = A.Uin[off + 3]; u4 = A.Uin[off + 4];
-            f64::apply_floor(u0, u1, u2, u3, u4, A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+            double v[5] = {A.Uin[off], A.Uin[off + 1], A.Uin[off + 2], A.Uin[off + 3], A.Uin[off + 4]};
+            P::floor(v, A);
+            u0 = v[0]; u1 = v[1]; u2 = v[2]; u3 = v[3]; u4 = v[4];
         }
         double* d = acc[m];
         double xc = A.x0 + ((double)(a + 1) - 0.5) * A.dx;
@@ -446,7 +451,7 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
 #pragma unroll
             for (int q = 0; q < 5; ++q) w[q] = (1.0 / 3.0) * un[q] + (2.0 / 3.0) * uu[q] + cdt * d[q];
         }
-        f64::apply_floor(w[0], w[1], w[2], w[3], w[4], A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+        P::floor(w, A);
 #pragma unroll
         for (int q = 0; q < 5; ++q) A.Uout[off + q] = w[q];
         if (A.cfl_max) {
