@@ -259,6 +259,14 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
     return *reinterpret_cast<uint32_t*>(&h);
 }
 
+// max(lo, 0), max(hi, 0) rounded to BF16 and packed (lo in the low half),
+// one instruction: cvt.rn.relu.bf16x2.f32 puts its first source in the high half
+__device__ __forceinline__ uint32_t pack2_relu(float lo, float hi) {
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
+}
+
 __device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
     asm volatile(
         "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
@@ -291,7 +299,7 @@ __device__ __noinline__ void mlp_tiles(const unsigned char* pk, const uint32_t* 
         int r0 = tile * 16 + g, r1 = r0 + 8;
         const uint32_t a0 = rows[r0 * 4 + tg], a1 = rows[r1 * 4 + tg];
         __syncwarp();
-        // layer 1: 8 (5 used) -> 32
+        // layer 1: 8 (5 used) -> 32, bias as the accumulator's initial value
         float h[4][4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -299,13 +307,14 @@ __device__ __noinline__ void mlp_tiles(const unsigned char* pk, const uint32_t* 
             h[j][0] = c0; h[j][1] = c1; h[j][2] = c0; h[j][3] = c1;
             mma1688(h[j], a0, a1, W1[(8 * j + g) * 8 + tg]);
         }
+        // ReLU, BF16 and the A fragments of the next layer in one instruction per pair
         uint32_t a2[2][4];
 #pragma unroll
         for (int kk = 0; kk < 2; ++kk) {
-            a2[kk][0] = pack2(fmaxf(h[2 * kk][0], 0.f), fmaxf(h[2 * kk][1], 0.f));
-            a2[kk][1] = pack2(fmaxf(h[2 * kk][2], 0.f), fmaxf(h[2 * kk][3], 0.f));
-            a2[kk][2] = pack2(fmaxf(h[2 * kk + 1][0], 0.f), fmaxf(h[2 * kk + 1][1], 0.f));
-            a2[kk][3] = pack2(fmaxf(h[2 * kk + 1][2], 0.f), fmaxf(h[2 * kk + 1][3], 0.f));
+            a2[kk][0] = pack2_relu(h[2 * kk][0], h[2 * kk][1]);
+            a2[kk][1] = pack2_relu(h[2 * kk][2], h[2 * kk][3]);
+            a2[kk][2] = pack2_relu(h[2 * kk + 1][0], h[2 * kk + 1][1]);
+            a2[kk][3] = pack2_relu(h[2 * kk + 1][2], h[2 * kk + 1][3]);
         }
         // layer 2: 32 -> 32
 #pragma unroll
@@ -318,10 +327,10 @@ __device__ __noinline__ void mlp_tiles(const unsigned char* pk, const uint32_t* 
         }
 #pragma unroll
         for (int kk = 0; kk < 2; ++kk) {
-            a2[kk][0] = pack2(fmaxf(h[2 * kk][0], 0.f), fmaxf(h[2 * kk][1], 0.f));
-            a2[kk][1] = pack2(fmaxf(h[2 * kk][2], 0.f), fmaxf(h[2 * kk][3], 0.f));
-            a2[kk][2] = pack2(fmaxf(h[2 * kk + 1][0], 0.f), fmaxf(h[2 * kk + 1][1], 0.f));
-            a2[kk][3] = pack2(fmaxf(h[2 * kk + 1][2], 0.f), fmaxf(h[2 * kk + 1][3], 0.f));
+            a2[kk][0] = pack2_relu(h[2 * kk][0], h[2 * kk][1]);
+            a2[kk][1] = pack2_relu(h[2 * kk][2], h[2 * kk][3]);
+            a2[kk][2] = pack2_relu(h[2 * kk + 1][0], h[2 * kk + 1][1]);
+            a2[kk][3] = pack2_relu(h[2 * kk + 1][2], h[2 * kk + 1][3]);
         }
         // layer 3: 32 -> 8 (3 used)
         float o[4] = {B3[2 * tg], B3[2 * tg + 1], B3[2 * tg], B3[2 * tg + 1]};
@@ -409,7 +418,8 @@ struct F32Learned {
     using real = float;
     static constexpr bool kCenterFromSmem = false;
     static constexpr bool kWarpFaces = true;
-    static constexpr bool kCross = false;   // per-sweep staging: the row buffers need the shared memory
+    static constexpr bool kCross = true;    // the block and all halos staged once
+    static constexpr int kCols = 5;         // rho, m, P: the epilogue reloads the FP64 state
     // A sweep whose staged values all lie within a quarter of the network's
     // spread thresholds of the first one cannot hold a network row (every
     // stencil spread is at most twice that): its faces skip the fallback test.
@@ -431,33 +441,38 @@ struct F32Learned {
         f32::floor_screened(v, A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
     }
     __device__ static void prologue(unsigned char* psm, const f64::StageArgs& A, int nt) {
-        const unsigned char* src = (const unsigned char*)A.mlp;
-        for (int i = threadIdx.x; i < 2 * learned::PK_BYTES; i += nt) psm[i] = src[i];
+        static_assert(learned::PK_BYTES % 16 == 0, "16-byte copies of the packed parameters");
+        const uint4* src = (const uint4*)A.mlp;   // device allocation: 256-byte aligned
+        uint4* dst = (uint4*)psm;                 // policy_smem: 16-byte aligned
+        for (int i = threadIdx.x; i < 2 * learned::PK_BYTES / 16; i += nt) dst[i] = src[i];
     }
     // P clamp, face energy and HLLC of one interface from its reconstructed
-    // (rho, m, P) on both sides (same arithmetic as the FP32 path)
-    template <int D>
-    __device__ static void finish(const float (&c)[6][6], const Consts& k, const float (&L)[5], const float (&Rv)[5],
-                                  float F[5]) {
+    // (rho, m, P) on both sides (the FP32 path's arithmetic), with the sweep
+    // direction at run time (the warp path below is one function for all
+    // three sweeps)
+    __device__ static void finish_rt(const float (&c)[6][6], const Consts& k, const float (&L)[5], const float (&Rv)[5],
+                                     float (&F)[5], int D) {
         float PmaxL = fmaxf(fmaxf(fmaxf(fmaxf(c[0][5], c[1][5]), c[2][5]), c[3][5]), c[4][5]);
         float PmaxR = fmaxf(fmaxf(fmaxf(fmaxf(c[1][5], c[2][5]), c[3][5]), c[4][5]), c[5][5]);
         float PL = fminf(fmaxf(L[4], 0.0f), PmaxL);
         float PR = fminf(fmaxf(Rv[4], 0.0f), PmaxR);
         float EL = f32::EL_from_P(PL, L[0], L[1], L[2], L[3], k.inv_gm1);
         float ER = f32::EL_from_P(PR, Rv[0], Rv[1], Rv[2], Rv[3], k.inv_gm1);
+        // (normal, t1, t2) = (x, y, z), (y, x, z), (z, x, y)
+        const float nL = D == 0 ? L[1] : (D == 1 ? L[2] : L[3]);
+        const float aL = D == 0 ? L[2] : L[1];
+        const float bL = D == 2 ? L[2] : L[3];
+        const float nR = D == 0 ? Rv[1] : (D == 1 ? Rv[2] : Rv[3]);
+        const float aR = D == 0 ? Rv[2] : Rv[1];
+        const float bR = D == 2 ? Rv[2] : Rv[3];
         float Fr[5];
-        if (D == 0) {
-            f32::hllc_normal(L[0], L[1], L[2], L[3], EL, Rv[0], Rv[1], Rv[2], Rv[3], ER, k.g, k.gm1, k.gg, Fr);
-            F[0] = Fr[0]; F[1] = Fr[1]; F[2] = Fr[2]; F[3] = Fr[3]; F[4] = Fr[4];
-        } else if (D == 1) {
-            f32::hllc_normal(L[0], L[2], L[1], L[3], EL, Rv[0], Rv[2], Rv[1], Rv[3], ER, k.g, k.gm1, k.gg, Fr);
-            F[0] = Fr[0]; F[1] = Fr[2]; F[2] = Fr[1]; F[3] = Fr[3]; F[4] = Fr[4];
-        } else {
-            f32::hllc_normal(L[0], L[3], L[1], L[2], EL, Rv[0], Rv[3], Rv[1], Rv[2], ER, k.g, k.gm1, k.gg, Fr);
-            F[0] = Fr[0]; F[1] = Fr[2]; F[2] = Fr[3]; F[3] = Fr[1]; F[4] = Fr[4];
-        }
+        f32::hllc_normal(L[0], nL, aL, bL, EL, Rv[0], nR, aR, bR, ER, k.g, k.gm1, k.gg, Fr);
+        F[0] = Fr[0];
+        F[1] = D == 0 ? Fr[1] : Fr[2];
+        F[2] = D == 0 ? Fr[2] : (D == 1 ? Fr[1] : Fr[3]);
+        F[3] = D == 2 ? Fr[1] : Fr[3];
+        F[4] = Fr[4];
     }
-
     // One interface per lane; every lane of the warp calls this (valid or not).
     // c[cell][col]: cols 0-3 rho, m_x, m_y, m_z, col 4 E, col 5 P; the
     // reconstructed fields are rho, m and P (cols 0-3 and 5), as the
@@ -477,6 +492,16 @@ struct F32Learned {
     template <int D>
     __device__ static void warp_flux(const float (&c)[6][6], bool valid, const Consts& k, float F[5],
                                      unsigned char* psm, int warp, bool quiet) {
+        float Fo[5];
+        warp_flux_rt(c, valid, k, Fo, psm, warp, quiet, D);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) F[q] = Fo[q];
+    }
+    // One copy for all three sweeps, out of line: it runs only in sweeps
+    // whose staged values are not uniform, and keeping it out of the inlined
+    // sweep bodies keeps the hot code of the kernel small.
+    __device__ __noinline__ static void warp_flux_rt(const float (&c)[6][6], bool valid, const Consts& k,
+                                                     float (&F)[5], unsigned char* psm, int warp, bool quiet, int D) {
         const int lane = threadIdx.x & 31;
         uint32_t* R = (uint32_t*)(psm + 2 * learned::PK_BYTES + warp * 160 * 16);
         float* logit = (float*)R;
@@ -548,10 +573,10 @@ struct F32Learned {
             Rv[q] = f32::wz(bB, bD, bE, 0.3f, 0.6f, 0.1f, qB, qC, qD);
             if (!quiet) test(q, c0, c1, c2, c3, c4, c5, bA, bB, bC, bD, bE);
         }
-        if (quiet) return finish<D>(c, k, L, Rv, F);
+        if (quiet) return finish_rt(c, k, L, Rv, F, D);
         // both sides' row counts in one prefix sum (8 bits each: at most 160 rows a side)
         const int packed = __popc(need[0]) | (__popc(need[1]) << 8);
-        if (!__any_sync(0xffffffffu, packed != 0)) return finish<D>(c, k, L, Rv, F);   // warp-uniform
+        if (!__any_sync(0xffffffffu, packed != 0)) return finish_rt(c, k, L, Rv, F, D);   // warp-uniform
         int incl = packed;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -614,7 +639,7 @@ struct F32Learned {
             }
             __syncwarp();
         }
-        finish<D>(c, k, L, Rv, F);
+        finish_rt(c, k, L, Rv, F, D);
     }
     template <int D>
     // uniform sweeps (kQuiescentSkip): no network row can occur, plain FP32 WENO5-Z + HLLC

@@ -12,6 +12,7 @@ namespace tile {
 struct F32Physics {
     using real = float;
     static constexpr bool kCross = true;
+    static constexpr int kCols = 5;                  // rho, m, P: the epilogue reloads the FP64 state
     static constexpr bool kCenterFromSmem = false;  // smem holds FP32 copies: reload FP64 state
     static constexpr bool kWarpFaces = false;
     static constexpr bool kQuiescentSkip = false;

@@ -35,11 +35,19 @@ struct Shape {
     static constexpr int NCROSS = OZH + HZ;
 };
 
+// Staged columns.  The stencils read rho, m_x, m_y, m_z and the cell pressure
+// (c[s][0..3] and c[s][5]); E (c[s][4]) is staged only by policies whose
+// epilogue reads the block's state back from shared memory (kCols = 6: E at
+// column 4, P at 5).  With kCols = 5 the pressure sits in column 4.
+template <int COLS>
+__host__ __device__ constexpr int pcol() { return COLS - 1; }
+
 // Physics policies --------------------------------------------------------
 struct F64Physics {
     using real = double;
     static constexpr bool kCross = true;             // stage the block and all halos once
     static constexpr bool kCenterFromSmem = true;   // smem holds the floored FP64 state
+    static constexpr int kCols = 6;                 // staged columns: rho, m, E (read back by the epilogue), P
     static constexpr bool kWarpFaces = false;       // faces computed thread by thread
     static constexpr bool kQuiescentSkip = false;
     __device__ static bool same(double, double) { return true; }
@@ -120,7 +128,7 @@ __device__ __forceinline__ void cross_cell(int e, int a0, int b0, int c0, const 
 template <class P, int TX, int TY, int TZ, int NT, int D>
 __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::Consts& k, int a0, int b0, int c0,
                       typename P::real* sC, typename P::real* sF, unsigned char* psm,
-                      double (&acc)[Shape<TX, TY, TZ>::NCELL / NT][5]) {
+                      double (&acc)[Shape<TX, TY, TZ>::NCELL / NT][5], bool quiet_cross) {
     constexpr bool CROSS = P::kCross;
     using S = Shape<TX, TY, TZ>;
     using real = typename P::real;
@@ -149,8 +157,11 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
             if (act) P::floor(v, A);
             real w[5];
 #pragma unroll
-            for (int q = 0; q < 5; ++q) { w[q] = (real)v[q]; sC[q * S::NEXT + e] = w[q]; }
-            sC[5 * S::NEXT + e] = P::pressure(w, k);
+            for (int q = 0; q < 5; ++q) {
+                w[q] = (real)v[q];
+                if (q < 4 || P::kCols == 6) sC[q * S::NEXT + e] = w[q];
+            }
+            sC[pcol<P::kCols>() * S::NEXT + e] = P::pressure(w, k);
         }
         // policies with per-stencil work that only non-uniform data can need
         // (the learned weights' fallback test) learn here whether every staged
@@ -160,9 +171,9 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
             bool varied = false;
             for (int e = tid; e < NE; e += NT) {
 #pragma unroll
-                for (int q = 0; q < 6; ++q) {
-                    if (q == 4) continue;   // E is not reconstructed
-                    varied |= !P::same(sC[q * S::NEXT + e], sC[q * S::NEXT]);
+                for (int q = 0; q < 5; ++q) {   // rho, m, P (E is not reconstructed)
+                    const int col = q < 4 ? q : pcol<P::kCols>();
+                    varied |= !P::same(sC[col * S::NEXT + e], sC[col * S::NEXT]);
                 }
             }
             quiet = !__syncthreads_or(varied);
@@ -170,6 +181,7 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
             __syncthreads();
         }
     }
+    if constexpr (CROSS) quiet = quiet_cross;
     constexpr int SD = (D == 0) ? 1 : (D == 1 ? LX : LX * LY);
     constexpr int FSTR = CROSS ? S::NCROSS : S::NEXT;   // field stride of the staged values
     // staged index of stencil cell s (0..5, cells fd-3 .. fd+2 along D) of face (fx, fy, fz)
@@ -250,7 +262,10 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
             for (int s = 0; s < 6; ++s) {
                 const int e = sidx(fx, fy, fz, s);
 #pragma unroll
-                for (int q = 0; q < 6; ++q) c[s][q] = sC[q * FSTR + e];
+                for (int q = 0; q < 6; ++q) {
+                    const int col = q < 4 ? q : (q == 5 ? pcol<P::kCols>() : 4);
+                    c[s][q] = (q == 4 && P::kCols == 5) ? (real)0 : sC[col * FSTR + e];
+                }
             }
             real F[5];
             P::template flux<D>(c, k, F);
@@ -273,7 +288,10 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
                 for (int s = 0; s < 6; ++s) {
                     const int e = valid ? sidx(fx, fy, fz, s) : 0;
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) c[s][q] = valid ? sC[q * FSTR + e] : (real)0;
+                    for (int q = 0; q < 6; ++q) {
+                        const int col = q < 4 ? q : (q == 5 ? pcol<P::kCols>() : 4);
+                        c[s][q] = (valid && (q != 4 || P::kCols == 6)) ? sC[col * FSTR + e] : (real)0;
+                    }
                 }
                 real F[5];
                 P::template warp_flux<D>(c, valid, k, F, psm, warp, quiet);
@@ -307,7 +325,7 @@ template <class P, int TX, int TY, int TZ>
 __device__ __forceinline__ unsigned char* policy_smem(unsigned char* smem_raw) {
     using S = Shape<TX, TY, TZ>;
     constexpr int NST = P::kCross ? S::NCROSS : S::NEXT;
-    return smem_raw + ((sizeof(typename P::real) * (6 * NST + 5 * S::NFACE) + 15) / 16) * 16;
+    return smem_raw + ((sizeof(typename P::real) * (P::kCols * NST + 5 * S::NFACE) + 15) / 16) * 16;
 }
 
 // One RK3 stage (or euler3d_rhs!) of the TX x TY x TZ block at active
@@ -322,7 +340,7 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
     static_assert(S::NCELL % NT == 0, "cells must divide evenly among threads");
     constexpr int CPT = S::NCELL / NT;
     real* sC = reinterpret_cast<real*>(smem_raw);
-    real* sF = sC + 6 * (P::kCross ? S::NCROSS : S::NEXT);
+    real* sF = sC + P::kCols * (P::kCross ? S::NCROSS : S::NEXT);
 
     Geom G(A.nx, A.ny, A.nz);
     const int tid = threadIdx.x;
@@ -343,13 +361,39 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
             if (act) P::floor(v, A);
             real w[5];
 #pragma unroll
-            for (int q = 0; q < 5; ++q) { w[q] = (real)v[q]; sC[q * S::NCROSS + e] = w[q]; }
-            sC[5 * S::NCROSS + e] = P::pressure(w, k);
+            for (int q = 0; q < 5; ++q) {
+                w[q] = (real)v[q];
+                if (q < 4 || P::kCols == 6) sC[q * S::NCROSS + e] = w[q];
+            }
+            sC[pcol<P::kCols>() * S::NCROSS + e] = P::pressure(w, k);
         }
     }
-    sweep<P, TX, TY, TZ, NT, 0>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
-    sweep<P, TX, TY, TZ, NT, 1>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
-    sweep<P, TX, TY, TZ, NT, 2>(A, G, k, a0, b0, c0, sC, sF, psm, acc);
+    // policies with per-stencil work that only non-uniform data can need (the
+    // learned weights' fallback test) learn here, per sweep, whether every
+    // value the sweep's stencils read (the block and that sweep's halos)
+    // equals the block's first cell within the policy's margin
+    bool quiet[3] = {false, false, false};
+    if constexpr (P::kCross && P::kQuiescentSkip) {
+        __syncthreads();
+        unsigned varied = 0u;   // bit 0: block, bits 1-3: x, y, z halos
+        for (int e = tid; e < S::NCROSS; e += NT) {
+            bool v = false;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const int col = q < 4 ? q : pcol<P::kCols>();
+                v |= !P::same(sC[col * S::NCROSS + e], sC[col * S::NCROSS]);
+            }
+            if (v) varied |= e < S::OXL ? 1u : (e < S::OYL ? 2u : (e < S::OZL ? 4u : 8u));
+        }
+        const bool vb = __syncthreads_or(varied & 1u), vx = __syncthreads_or(varied & 2u),
+                   vy = __syncthreads_or(varied & 4u), vz = __syncthreads_or(varied & 8u);
+        quiet[0] = !(vb || vx);
+        quiet[1] = !(vb || vy);
+        quiet[2] = !(vb || vz);
+    }
+    sweep<P, TX, TY, TZ, NT, 0>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[0]);
+    sweep<P, TX, TY, TZ, NT, 1>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[1]);
+    sweep<P, TX, TY, TZ, NT, 2>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[2]);
 
     const double dt = A.dt_dev ? *A.dt_dev : A.dt;
     const f64::BHSrc& BH = A.bh_dev ? *A.bh_dev : A.bh;     // kernel parameters are __grid_constant__
@@ -518,7 +562,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_batch(const __grid_cons
 template <class P, int TX, int TY, int TZ>
 constexpr int smem_bytes() {
     using S = Shape<TX, TY, TZ>;
-    return (6 * (P::kCross ? S::NCROSS : S::NEXT) + 5 * S::NFACE) * (int)sizeof(typename P::real) + 16;
+    return (P::kCols * (P::kCross ? S::NCROSS : S::NEXT) + 5 * S::NFACE) * (int)sizeof(typename P::real) + 16;
 }
 
 // Host: launch stage_kernel_batch for the levels in B with a persistent grid
