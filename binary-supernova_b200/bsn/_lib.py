@@ -96,6 +96,10 @@ SIGNATURES = {
     "bsn_coupled_run_steps": (_I, [_V, _P, _BH, _I, _I, _I, _I, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _I, _I,
                                    _D, _D, _I, _I, _I, _D, _dp, C.POINTER(C.c_int), _P, _I]),
     "bsn_diagnostics_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _BH, _I, _D, _dp]),
+    "bsn_rotating_frame_source_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _D]),
+    "bsn_relax_damping_source_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _D, _D]),
+    "bsn_relax_ic": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _BH, _I, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D,
+                          _I, _I, _I, _dp, C.POINTER(C.c_int), _dp]),
     "bsn_coupled_nested_run_steps": (_I, [_V, _FMR, _I, _BH, _I, _D, _D, _D, _D, _D, _D, _I, _I, _D, _D, _I, _I,
                                           _I, _D, _dp, C.POINTER(C.c_int), _P, _I]),
     "bsn_fmr_prolong_all_f64": (_I, [_V, _FMR]),

@@ -30,7 +30,8 @@ __all__ = [
     "nbody_step", "KeplerOrbit", "kepler_update", "solve_poisson_isolated", "add_self_gravity_source",
     "apply_sg_force_level", "coupled_step", "FMRGrid3D", "fmr3d_step", "cfl_dt_fmr3d", "solve_fmr_poisson",
     "restrict_density_to_coarse", "FMRHierarchy3D", "fmr_nested_step", "cfl_dt_fmr_nested",
-    "fmr_nested_run_steps", "coupled_nested_run_steps",
+    "fmr_nested_run_steps", "coupled_nested_run_steps", "rotating_frame_source", "relax_damping_source",
+    "relax_ic",
 ]
 
 # ---------------------------------------------------------------------------
@@ -307,6 +308,38 @@ def coupled_run_steps(U, bhs, nx, ny, nz, dx, x0, y0, z0, gamma, cfl, *, n_steps
           _ptr(diag) if diag is not None else None, int(diag.shape[0]) if diag is not None else 0)
     _bh_writeback(bhs, arr)
     return tt.value, nd.value
+
+
+def rotating_frame_source(dU, U, nx, ny, nz, dx, dy, dz, x0, y0, z0, Omega):
+    """rotating_frame_source! (src/relax_ic.jl:150-176)."""
+    _check_state(U, nx, ny, nz)
+    _check_state(dU, nx, ny, nz, "dU")
+    _call("bsn_rotating_frame_source_f64", context(), _ptr(dU), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz),
+          float(x0), float(y0), float(z0), float(Omega))
+
+
+def relax_damping_source(dU, U, nx, ny, nz, dx, dy, dz, x0, y0, z0, t_damp, *, Omega=0.0):
+    """relax_damping_source! (src/relax_ic.jl:59-120)."""
+    _check_state(U, nx, ny, nz)
+    _check_state(dU, nx, ny, nz, "dU")
+    _call("bsn_relax_damping_source_f64", context(), _ptr(dU), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz),
+          float(x0), float(y0), float(z0), float(t_damp), float(Omega))
+
+
+def relax_ic(U, nx, ny, nz, dx, dy, dz, gamma, *, bhs=(), x0=0.0, y0=0.0, z0=0.0, t_damp=0.1, t_max=2.0, cfl=0.4,
+             rho_floor=1e-10, P_floor=1e-10, KE_tol=0.01, Omega=0.0, self_gravity=False, precision="f64",
+             max_steps=1000000):
+    """relax_ic! (src/relax_ic.jl:200-330) on the device; returns (t, n_steps, KE_ratio)."""
+    _check_state(U, nx, ny, nz)
+    arr = _bh_array(list(bhs))
+    t = C.c_double(0.0)
+    n = C.c_int(0)
+    kr = C.c_double(0.0)
+    _call("bsn_relax_ic", context(), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz), float(gamma), arr,
+          len(bhs), float(x0), float(y0), float(z0), float(t_damp), float(t_max), float(cfl), float(rho_floor),
+          float(P_floor), float(KE_tol), float(Omega), int(bool(self_gravity)), PREC[precision], int(max_steps),
+          C.byref(t), C.byref(n), C.byref(kr))
+    return t.value, n.value, kr.value
 
 
 def diagnostics(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, bhs, gamma) -> np.ndarray:

@@ -23,7 +23,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 BASE = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 FP64_PARITY = {"hydro_f64.cu", "sources_f64.cu", "fmr_f64.cu", "fmr_nlevel.cu", "poisson.cu", "context.cu", "cfl_noalloc.cu",
-               "run_steps.cu", "autotune.cu", "coupled_run.cu", "diagnostics.cu"}
+               "run_steps.cu", "autotune.cu", "coupled_run.cu", "diagnostics.cu", "relax.cu"}
 # the FP32 fast path: contraction on, approximate division and square root
 FAST = {"stage_fast.cu", "learned.cu", "poisson_f32.cu"}
 FAST_FLAGS = ["--ftz=true", "--prec-div=false", "--prec-sqrt=false", "--fmad=true"]

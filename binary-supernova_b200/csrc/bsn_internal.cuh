@@ -42,6 +42,7 @@ struct bsn_ctx {
     void* fmrN_state = nullptr;      // fmr_nlevel.cu: nested-level buffers and step graph
     void* coupled_run_state = nullptr;   // coupled_run.cu: graph of the device-resident coupled step
     void* coupled_nested_state = nullptr;   // coupled_run.cu: the coupled step on nested levels
+    void* relax_state = nullptr;     // relax.cu: graph of the device-resident relaxation step
 };
 
 namespace bsn {
@@ -49,7 +50,8 @@ namespace bsn {
 enum Slot {
     SLOT_A = 0, SLOT_B, SLOT_UN, SLOT_RED, SLOT_FFT0, SLOT_FFT1, SLOT_PHI, SLOT_RHO,
     SLOT_FMR_UCN, SLOT_FMR_UCNP1, SLOT_FMR_GH, SLOT_FMR_FA, SLOT_FMR_FB, SLOT_FMR_REG,
-    SLOT_FMR_BF, SLOT_PHI2, SLOT_RUN, SLOT_FMR_RUN, SLOT_CRUN, SLOT_CRED, SLOT_DIAG, SLOT_DIAGREC, SLOT_COUNT
+    SLOT_FMR_BF, SLOT_PHI2, SLOT_RUN, SLOT_FMR_RUN, SLOT_CRUN, SLOT_CRED, SLOT_DIAG, SLOT_DIAGREC, SLOT_RELAX,
+    SLOT_COUNT
 };
 
 bsn_status set_err(bsn_ctx* ctx, bsn_status code, const char* fmt, ...);

@@ -196,6 +196,40 @@ __device__ __forceinline__ void apply_floor(double& r, double& mx, double& my, d
     }
 }
 
+// rotating_frame_source! (src/relax_ic.jl:150-176) on one cell's RHS d[5]:
+// centrifugal rho Omega^2 (x, y) plus Coriolis 2 Omega (m_y, -m_x) on the
+// momentum, rho v . a_centrifugal on the energy, in the reference's
+// expression order.
+__device__ __forceinline__ void rot_frame_src(double* d, double u0, double u1, double u2, double xc, double yc,
+                                              double om) {
+    const double O2 = om * om;
+    d[1] = d[1] + (O2 * u0 * xc + 2.0 * om * u2);
+    d[2] = d[2] + (O2 * u0 * yc - 2.0 * om * u1);
+    d[4] = d[4] + O2 * (xc * u1 + yc * u2);
+}
+
+// relax_damping_source! (src/relax_ic.jl:59-120) on one cell's RHS d[5]:
+// momentum damped toward the co-rotation velocity (-Omega y, Omega x, 0) over
+// t_damp, the energy by the work of that force (inv_td = 1 / t_damp).
+__device__ __forceinline__ void damp_src(double* d, double u0, double u1, double u2, double u3, double xc, double yc,
+                                         double inv_td, double t_damp, double om) {
+    const double rs = jmax(u0, 1e-30);
+    if (om == 0.0) {
+        d[1] = d[1] - u1 * inv_td;
+        d[2] = d[2] - u2 * inv_td;
+        d[3] = d[3] - u3 * inv_td;
+        d[4] = d[4] - (u1 * u1 + u2 * u2 + u3 * u3) / (rs * t_damp);
+    } else {
+        const double vx = u1 / rs, vy = u2 / rs, vz = u3 / rs;
+        const double vrotx = -om * yc, vroty = om * xc;
+        const double vrx = vx - vrotx, vry = vy - vroty;
+        d[1] = d[1] - rs * vrx * inv_td;
+        d[2] = d[2] - rs * vry * inv_td;
+        d[3] = d[3] - u3 * inv_td;
+        d[4] = d[4] - rs * (vx * vrx + vy * vry + vz * vz) * inv_td;
+    }
+}
+
 // CFL speed of one cell (src/gpu_kernels.jl:174-191).
 __device__ __forceinline__ double cfl_speed(double U0, double U1, double U2, double U3, double U4, double g,
                                             double gm1, double idx, double idy, double idz) {

@@ -36,6 +36,24 @@ __global__ void bh_gravity_kernel(double* dU, const double* U, int nx, int ny, i
     dU[o + 4] += rho * (vx * ax + vy * ay + vz * az);
 }
 
+// rotating_frame_source! / relax_damping_source! (src/relax_ic.jl:59-176) as
+// standalone passes over the active cells (the stage kernel applies the same
+// per-cell functions in its epilogue)
+__global__ void relax_src_kernel(double* dU, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                                 double x0, double y0, double z0, int rot, double omega, double inv_td, double t_damp) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nx * ny * nz) return;
+    int a = (int)(t % nx); long long r = t / nx; int b = (int)(r % ny); int c = (int)(r / ny);
+    Geom G(nx, ny, nz);
+    long long o = G.act(a, b, c);
+    double xc, yc, zc;
+    cell_xyz(a, b, c, x0, y0, z0, dx, dy, dz, xc, yc, zc);
+    double d[5] = {dU[o], dU[o + 1], dU[o + 2], dU[o + 3], dU[o + 4]};
+    if (rot) rot_frame_src(d, U[o], U[o + 1], U[o + 2], xc, yc, omega);
+    else damp_src(d, U[o], U[o + 1], U[o + 2], U[o + 3], xc, yc, inv_td, t_damp, omega);
+    for (int q = 1; q < 5; ++q) dU[o + q] = d[q];
+}
+
 // add_sink_sources! (src/gpu_kernels.jl:238-284)
 __global__ void sink_kernel(double* dU, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
                             double x0, double y0, double z0, SinkSrc sk) {
@@ -275,6 +293,30 @@ extern "C" bsn_status bsn_add_bh_gravity_source_f64(bsn_ctx* ctx, double* dU, co
     bh_gravity_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(dU, U, nx, ny, nz, dx, dy, dz,
                                                                                        x0, y0, z0, s);
     return launch_check(ctx, "bh_gravity_kernel");
+}
+
+extern "C" bsn_status bsn_rotating_frame_source_f64(bsn_ctx* ctx, double* dU, const double* U, int nx, int ny,
+                                                    int nz, double dx, double dy, double dz, double x0, double y0,
+                                                    double z0, double Omega) {
+    if (!ctx) return BSN_ERR_ARG;
+    BSN_TRY(check_dims(ctx, nx, ny, nz));
+    if (!dU || !U) return set_err(ctx, BSN_ERR_ARG, "null array");
+    relax_src_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(dU, U, nx, ny, nz, dx, dy, dz, x0,
+                                                                                      y0, z0, 1, Omega, 0.0, 0.0);
+    return launch_check(ctx, "relax_src_kernel");
+}
+
+extern "C" bsn_status bsn_relax_damping_source_f64(bsn_ctx* ctx, double* dU, const double* U, int nx, int ny, int nz,
+                                                   double dx, double dy, double dz, double x0, double y0, double z0,
+                                                   double t_damp, double Omega) {
+    if (!ctx) return BSN_ERR_ARG;
+    BSN_TRY(check_dims(ctx, nx, ny, nz));
+    if (!dU || !U) return set_err(ctx, BSN_ERR_ARG, "null array");
+    if (!(t_damp > 0.0)) return set_err(ctx, BSN_ERR_ARG, "t_damp must be positive");
+    relax_src_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(dU, U, nx, ny, nz, dx, dy, dz, x0,
+                                                                                      y0, z0, 0, Omega, 1.0 / t_damp,
+                                                                                      t_damp);
+    return launch_check(ctx, "relax_src_kernel");
 }
 
 extern "C" bsn_status bsn_add_sink_sources_f64(bsn_ctx* ctx, double* dU, const double* U, int nx, int ny, int nz,

@@ -64,6 +64,10 @@ struct StageArgs {
     const void* mlp;         // learned stencil path: packed network parameters
     const BHSrc* bh_dev;     // non-null: gravity sources read on the device (device-resident driver loop)
     const SinkSrc* sk_dev;   // non-null: sink sources read on the device
+    // relaxation sources (src/relax_ic.jl): rotating frame at rot_omega,
+    // velocity damping over damp_t (damp_inv_td = 1 / damp_t) toward rotation at damp_omega
+    int use_rot, use_damp;
+    double rot_omega, damp_t, damp_inv_td, damp_omega;
 };
 
 // Centre of active cell (a, b, c) (0-based): x0 + (i - ng - 0.5) dx with

@@ -475,6 +475,8 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
                 }
             }
         }
+        if (A.use_rot) f64::rot_frame_src(d, u0, u1, u2, xc, yc, A.rot_omega);   // src/relax_ic.jl:150-176
+        if (A.use_damp) f64::damp_src(d, u0, u1, u2, u3, xc, yc, A.damp_inv_td, A.damp_t, A.damp_omega);
         if (A.mode == 1) {
 #pragma unroll
             for (int q = 0; q < 5; ++q) A.dU[off + q] = d[q];

@@ -240,6 +240,30 @@ bsn_status bsn_sg_gradient_f64(bsn_ctx* ctx, double* dU, const double* U, const 
 bsn_status bsn_add_self_gravity_source_f64(bsn_ctx* ctx, double* dU, const double* U,
                                            int nx, int ny, int nz, double dx, double dy, double dz);
 
+/* ---- src/relax_ic.jl ------------------------------------------------------ */
+/* rotating_frame_source! (src/relax_ic.jl:150-176): centrifugal and Coriolis
+ * terms of a frame rotating at Omega about z through the origin, added to dU. */
+bsn_status bsn_rotating_frame_source_f64(bsn_ctx* ctx, double* dU, const double* U, int nx, int ny, int nz,
+                                         double dx, double dy, double dz, double x0, double y0, double z0,
+                                         double Omega);
+/* relax_damping_source! (src/relax_ic.jl:59-120): velocity damping over t_damp
+ * toward the co-rotation velocity (-Omega y, Omega x, 0), added to dU. */
+bsn_status bsn_relax_damping_source_f64(bsn_ctx* ctx, double* dU, const double* U, int nx, int ny, int nz,
+                                        double dx, double dy, double dz, double x0, double y0, double z0,
+                                        double t_damp, double Omega);
+/* relax_ic! (src/relax_ic.jl:200-330) on the device: SSP-RK3 with the hydro
+ * RHS, BH gravity (bhs, host, held fixed), self-gravity per stage when
+ * self_gravity != 0, the rotating frame when Omega != 0 and damping toward
+ * rest, until t_max, KE/E_thermal < KE_tol, or the ratio turns back up 10 %
+ * past its post-peak minimum; at most max_steps steps.  dt, t and the stop
+ * rule stay on the device, one CUDA graph per step.  precision: BSN_PREC_*
+ * stencils.  Outputs (may be NULL): final t, steps taken, last KE ratio. */
+bsn_status bsn_relax_ic(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                        double gamma, const bsn_bh* bhs, int nbh, double x0, double y0, double z0,
+                        double t_damp, double t_max, double cfl, double rho_floor, double P_floor,
+                        double KE_tol, double Omega, int self_gravity, int precision, int max_steps,
+                        double* t_out, int* n_steps_out, double* ke_ratio_out);
+
 /* ---- driver stage order: coupled_step! (scripts/run_sn50_fiducial.jl:756-818)
  * BH forces, optional nbody_step! (evolve_orbit), three fused RK3 stages with
  * BH gravity, optional self-gravity and sinks, then accrete!.  bhs is host

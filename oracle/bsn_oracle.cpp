@@ -1619,3 +1619,105 @@ extern "C" void orc_diagnostics(const double* U, int nx, int ny, int nz, double 
     double dV = dx * dy * dz;
     for (int q = 0; q < 10; ++q) out[q] = (double)s[q] * dV;
 }
+
+/* ------------------------------------------------------------------------- */
+/* src/relax_ic.jl:150-176 rotating_frame_source!: centrifugal Omega^2 (x, y)
+ * and Coriolis (2 Omega m_y, -2 Omega m_x) on the momentum, rho v .
+ * a_centrifugal on the energy; cell centres x0 + (i - 0.5) dx. */
+extern "C" void orc_rotating_frame_source(double* dU, const double* U, int nx, int ny, int nz, double dx, double dy,
+                                          double dz, double x0, double y0, double z0, double Om) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    const double O2 = Om * Om;
+    for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i) {
+        const double xc = x0 + ((double)i - 0.5) * dx, yc = y0 + ((double)j - 0.5) * dy;
+        const double rho = U[I(1, ng + i, ng + j, ng + k)], mx = U[I(2, ng + i, ng + j, ng + k)],
+                     my = U[I(3, ng + i, ng + j, ng + k)];
+        double& d2 = dU[I(2, ng + i, ng + j, ng + k)];
+        double& d3 = dU[I(3, ng + i, ng + j, ng + k)];
+        double& d5 = dU[I(5, ng + i, ng + j, ng + k)];
+        d2 = d2 + (O2 * rho * xc + 2.0 * Om * my);
+        d3 = d3 + (O2 * rho * yc - 2.0 * Om * mx);
+        d5 = d5 + O2 * (xc * mx + yc * my);
+    }
+}
+
+/* src/relax_ic.jl:59-120 relax_damping_source!: damping of the momentum over
+ * t_damp toward the co-rotation velocity (-Omega y, Omega x, 0) and of the
+ * energy by that force's work. */
+extern "C" void orc_relax_damping_source(double* dU, const double* U, int nx, int ny, int nz, double dx, double dy,
+                                         double dz, double x0, double y0, double z0, double t_damp, double Om) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    const double inv_td = 1.0 / t_damp;
+    for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i) {
+        const double rho = U[I(1, ng + i, ng + j, ng + k)], mx = U[I(2, ng + i, ng + j, ng + k)],
+                     my = U[I(3, ng + i, ng + j, ng + k)], mz = U[I(4, ng + i, ng + j, ng + k)];
+        double& d2 = dU[I(2, ng + i, ng + j, ng + k)];
+        double& d3 = dU[I(3, ng + i, ng + j, ng + k)];
+        double& d4 = dU[I(4, ng + i, ng + j, ng + k)];
+        double& d5 = dU[I(5, ng + i, ng + j, ng + k)];
+        const double rs = jmax(rho, 1e-30);
+        if (Om == 0.0) {
+            d2 = d2 - mx * inv_td;
+            d3 = d3 - my * inv_td;
+            d4 = d4 - mz * inv_td;
+            d5 = d5 - (mx * mx + my * my + mz * mz) / (rs * t_damp);
+        } else {
+            const double xc = x0 + ((double)i - 0.5) * dx, yc = y0 + ((double)j - 0.5) * dy;
+            const double vx = mx / rs, vy = my / rs, vz = mz / rs;
+            const double vrotx = -Om * yc, vroty = Om * xc;
+            const double vrx = vx - vrotx, vry = vy - vroty;
+            d2 = d2 - rs * vrx * inv_td;
+            d3 = d3 - rs * vry * inv_td;
+            d4 = d4 - mz * inv_td;
+            d5 = d5 - rs * (vx * vrx + vy * vry + vz * vz) * inv_td;
+        }
+    }
+}
+
+/* src/relax_ic.jl:200-330 relax_ic!: SSP-RK3 with hydro, BH gravity (fixed
+ * BHs), optional self-gravity, rotating frame (Omega != 0) and damping toward
+ * rest (the driver passes Omega = 0 to the damping), until t_max, KE/E_th <
+ * KE_tol or the ratio turns back up 10 % past its post-peak minimum; at most
+ * max_steps steps.  out: {t, n_steps, KE_ratio}. */
+extern "C" void orc_relax_ic(double* U, int nx, int ny, int nz, double dx, double dy, double dz, double g,
+                             const orc_bh* bhs, int nbh, double x0, double y0, double z0, double t_damp,
+                             double t_max, double cfl, double rho_floor, double P_floor, double KE_tol, double Om,
+                             int self_gravity, int max_steps, double out[3]) {
+    Idx I(nx, ny, nz);
+    const long n = I.size();
+    StepScratch S(nx, ny, nz);
+    double t = 0.0, KE_ratio = INFINITY, ke_peak = 0.0, ke_valley = INFINITY;
+    bool descended = false;
+    int n_steps = 0;
+    while (t < t_max && KE_ratio > KE_tol && n_steps < max_steps) {
+        double dt = jmin(orc_cfl_dt_3d(U, nx, ny, nz, dx, dy, dz, g, cfl), t_max - t);
+        std::memcpy(S.Un.data(), U, sizeof(double) * n);
+        for (int stage = 0; stage < 3; ++stage) {
+            orc_euler3d_rhs(S.dU.data(), S.Fx.data(), S.Fy.data(), S.Fz.data(), U, nx, ny, nz, dx, dy, dz, g, 0,
+                            rho_floor, P_floor, 1);
+            if (nbh > 0) orc_add_bh_gravity_source(S.dU.data(), U, nx, ny, nz, dx, dy, dz, bhs, nbh, x0, y0, z0);
+            if (self_gravity) orc_add_self_gravity_source(S.dU.data(), U, nx, ny, nz, dx, dy, dz);
+            if (Om != 0.0) orc_rotating_frame_source(S.dU.data(), U, nx, ny, nz, dx, dy, dz, x0, y0, z0, Om);
+            orc_relax_damping_source(S.dU.data(), U, nx, ny, nz, dx, dy, dz, x0, y0, z0, t_damp, 0.0);
+            if (stage == 0) combine1(U, S.Un.data(), S.dU.data(), dt, n);
+            else if (stage == 1) combine2(U, S.Un.data(), S.dU.data(), dt, n);
+            else combine3(U, S.Un.data(), S.dU.data(), dt, n);
+            orc_apply_floors(U, nx, ny, nz, rho_floor, P_floor, g);
+        }
+        t += dt;
+        n_steps += 1;
+        double tot[10];
+        orc_diagnostics(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, nullptr, 0, g, tot);
+        const double KE = tot[1], E_th = jmax(tot[0] - KE, 0.0);
+        KE_ratio = E_th > 0.0 ? KE / E_th : 0.0;
+        ke_peak = jmax(ke_peak, KE_ratio);
+        if (!descended) descended = KE_ratio < 0.9 * ke_peak;
+        if (descended) {
+            ke_valley = jmin(ke_valley, KE_ratio);
+            if (KE_ratio > 1.1 * ke_valley) break;
+        }
+    }
+    out[0] = t; out[1] = (double)n_steps; out[2] = KE_ratio;
+}

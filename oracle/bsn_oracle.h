@@ -120,6 +120,15 @@ void   orc_prolong_fine_ghosts(double* Uf, const double* Uc, const orc_fmr* G);
 void   orc_restrict(double* Uc, const double* Uf, const orc_fmr* G);
 void   orc_fmr3d_step(const orc_fmr* G, double dt_c, int self_gravity, double G_grav);
 double orc_cfl_dt_fmr3d(const orc_fmr* G, double cfl);
+/* relax_ic.jl */
+void   orc_rotating_frame_source(double* dU, const double* U, int nx, int ny, int nz, double dx, double dy,
+                                 double dz, double x0, double y0, double z0, double Om);
+void   orc_relax_damping_source(double* dU, const double* U, int nx, int ny, int nz, double dx, double dy,
+                                double dz, double x0, double y0, double z0, double t_damp, double Om);
+void   orc_relax_ic(double* U, int nx, int ny, int nz, double dx, double dy, double dz, double g,
+                    const orc_bh* bhs, int nbh, double x0, double y0, double z0, double t_damp, double t_max,
+                    double cfl, double rho_floor, double P_floor, double KE_tol, double Om, int self_gravity,
+                    int max_steps, double out[3]);
 /* N nested levels: pairs[k].Uf is pairs[k+1].Uc */
 void   orc_fmrN_step(const orc_fmr* pairs, int npairs, double dt0, int self_gravity, double G_grav);
 double orc_cfl_dt_fmrN(const orc_fmr* pairs, int npairs, double cfl);

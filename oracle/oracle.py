@@ -98,6 +98,9 @@ def _declare(L):
         "orc_fmrN_step": (V, [C.POINTER(OrcFMR), i, d, i, d]),
         "orc_cfl_dt_fmrN": (d, [C.POINTER(OrcFMR), i, d]),
         "orc_gas_force_fmrN": (V, [C.POINTER(OrcFMR), i, C.POINTER(OrcBH), d, d, d, P]),
+        "orc_rotating_frame_source": (V, [P, P, i, i, i, d, d, d, d, d, d, d]),
+        "orc_relax_damping_source": (V, [P, P, i, i, i, d, d, d, d, d, d, d, d]),
+        "orc_relax_ic": (V, [P, i, i, i, d, d, d, d, C.POINTER(OrcBH), i, d, d, d, d, d, d, d, d, d, d, i, i, P]),
         "orc_coupled_fmrN_step": (V, [C.POINTER(OrcFMR), i, C.POINTER(OrcBH), i, d, d, d, d, d, d, i, i, d, d, i,
                                       P]),
         "orc_restrict_density_to_coarse": (V, [C.POINTER(OrcFMR)]),
@@ -269,6 +272,24 @@ def sg_gradient(dU, U, phi, dx, dy, dz):
 
 def add_self_gravity_source(dU, U, dx, dy, dz):
     lib().orc_add_self_gravity_source(_p(dU), _p(U), *dims(U), dx, dy, dz)
+
+
+def rotating_frame_source(dU, U, dx, dy, dz, x0, y0, z0, Omega):
+    lib().orc_rotating_frame_source(_p(dU), _p(U), *dims(U), dx, dy, dz, x0, y0, z0, Omega)
+
+
+def relax_damping_source(dU, U, dx, dy, dz, x0, y0, z0, t_damp, Omega=0.0):
+    lib().orc_relax_damping_source(_p(dU), _p(U), *dims(U), dx, dy, dz, x0, y0, z0, t_damp, Omega)
+
+
+def relax_ic(U, dx, dy, dz, gamma, bhs=(), x0=0.0, y0=0.0, z0=0.0, t_damp=0.1, t_max=2.0, cfl=0.4,
+             rho_floor=1e-10, P_floor=1e-10, KE_tol=0.01, Omega=0.0, self_gravity=False, max_steps=1000000):
+    """relax_ic! (src/relax_ic.jl:200-330); returns (t, n_steps, KE_ratio)."""
+    arr = bh_array(list(bhs))
+    out = np.zeros(3)
+    lib().orc_relax_ic(_p(U), *dims(U), dx, dy, dz, gamma, arr, len(bhs), x0, y0, z0, t_damp, t_max, cfl,
+                       rho_floor, P_floor, KE_tol, Omega, int(self_gravity), int(max_steps), out.ctypes.data_as(_dp))
+    return float(out[0]), int(out[1]), float(out[2])
 
 
 def coupled_step(U, bhs_arr, nbh, dt, t, dx, x0, y0, z0, gamma, f_sink, rho_floor, P_floor,
