@@ -497,11 +497,13 @@ struct F32Learned {
 #pragma unroll
         for (int q = 0; q < 5; ++q) F[q] = Fo[q];
     }
-    // One copy for all three sweeps, out of line: it runs only in sweeps
-    // whose staged values are not uniform, and keeping it out of the inlined
-    // sweep bodies keeps the hot code of the kernel small.
-    __device__ __noinline__ static void warp_flux_rt(const float (&c)[6][6], bool valid, const Consts& k,
-                                                     float (&F)[5], unsigned char* psm, int warp, bool quiet, int D) {
+    // Inlined into each sweep with D a compile-time constant: an out-of-line
+    // copy shrinks the kernel's code but passes the stencil and the caller's
+    // live registers through local memory on every call, which costs more
+    // than it saves where most sweeps are non-uniform (inside a star).
+    __device__ __forceinline__ static void warp_flux_rt(const float (&c)[6][6], bool valid, const Consts& k,
+                                                        float (&F)[5], unsigned char* psm, int warp, bool quiet,
+                                                        int D) {
         const int lane = threadIdx.x & 31;
         uint32_t* R = (uint32_t*)(psm + 2 * learned::PK_BYTES + warp * 160 * 16);
         float* logit = (float*)R;
