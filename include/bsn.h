@@ -161,7 +161,7 @@ bsn_status bsn_ctx_set_tile(bsn_ctx* ctx, int precision, int variant);
 bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int ny, int nz, int out[5]);
 
 /* ---- learned WENO weights (no counterpart in the reference; plain WENO5-Z of
- * src/weno5.jl:14-61 is its judge).  Two networks, for the left- and the
+ * src/weno5.jl:14-61 is its yardstick).  Two networks, for the left- and the
  * right-biased reconstruction, each 5 -> 32 -> 32 -> 3 (ReLU, softmax), map
  * a normalised 5-point stencil u_i = (v_i - v_c)/max|v_j - v_c| to the three
  * weights.  A reconstruction uses the network only where the smoothness

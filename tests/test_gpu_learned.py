@@ -1,5 +1,5 @@
 """GPU tests of the learned WENO weights (no reference counterpart; plain
-WENO5-Z is the judge):
+WENO5-Z is the yardstick):
 
 * the hand-written training kernels' loss and gradient agree with a numpy
   FP64 forward/backward (tests/mlp_ref.py) to 1e-4 relative;
