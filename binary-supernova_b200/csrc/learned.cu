@@ -440,6 +440,9 @@ struct F32Learned {
     __device__ static void floor(double (&v)[5], const f64::StageArgs& A) {
         f32::floor_screened(v, A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
     }
+    __device__ static void stage(double (&v)[5], bool act, const f64::StageArgs& A, float (&w)[5]) {
+        f32::stage_floored(v, act, A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1, w);
+    }
     __device__ static void prologue(unsigned char* psm, const f64::StageArgs& A, int nt) {
         static_assert(learned::PK_BYTES % 16 == 0, "16-byte copies of the packed parameters");
         const uint4* src = (const uint4*)A.mlp;   // device allocation: 256-byte aligned

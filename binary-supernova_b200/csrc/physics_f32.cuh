@@ -164,14 +164,29 @@ __device__ __forceinline__ void weno5_lr2(f2 c0, f2 c1, f2 c2, f2 c3, f2 c4, f2 
 // P_floor / (gamma - 1) means the FP64 test would change nothing; any cell
 // below that margin, below the density floor or non-finite takes the FP64
 // floor itself, so the result is apply_floor's in every case.
+// true when the FP32 copy w of a cell (density v0 in FP64) shows it clear of
+// both floors by that margin
+__device__ __forceinline__ bool floor_clear(const float (&w)[5], double v0, double rho_floor, double Pfl_gm1) {
+    if (!(v0 >= rho_floor)) return false;
+    const float KE = fdiv(0.5f * fmaf(w[3], w[3], fmaf(w[2], w[2], w[1] * w[1])), w[0]);
+    return w[4] - KE > (float)Pfl_gm1 + 1e-5f * (fabsf(w[4]) + KE);
+}
 __device__ __forceinline__ void floor_screened(double (&v)[5], double rho_floor, double P_floor, double Pfl_gm1,
                                                double gm1) {
-    if (v[0] >= rho_floor) {
-        const float r = (float)v[0], mx = (float)v[1], my = (float)v[2], mz = (float)v[3], E = (float)v[4];
-        const float KE = fdiv(0.5f * fmaf(mz, mz, fmaf(my, my, mx * mx)), r);
-        if (E - KE > (float)Pfl_gm1 + 1e-5f * (fabsf(E) + KE)) return;
-    }
+    const float w[5] = {(float)v[0], (float)v[1], (float)v[2], (float)v[3], (float)v[4]};
+    if (floor_clear(w, v[0], rho_floor, Pfl_gm1)) return;
     f64::apply_floor(v[0], v[1], v[2], v[3], v[4], rho_floor, P_floor, Pfl_gm1, gm1);
+}
+// A staged cell: the FP32 copy w of the floored state v (floors on active
+// cells only), converting once where the cell is clear of the floors.
+__device__ __forceinline__ void stage_floored(double (&v)[5], bool act, double rho_floor, double P_floor,
+                                              double Pfl_gm1, double gm1, float (&w)[5]) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) w[q] = (float)v[q];
+    if (!act || floor_clear(w, v[0], rho_floor, Pfl_gm1)) return;
+    f64::apply_floor(v[0], v[1], v[2], v[3], v[4], rho_floor, P_floor, Pfl_gm1, gm1);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) w[q] = (float)v[q];
 }
 
 __device__ __forceinline__ float cell_pressure(float r, float mx, float my, float mz, float E, float gm1) {

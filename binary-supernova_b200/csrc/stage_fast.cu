@@ -30,6 +30,9 @@ struct F32Physics {
     __device__ static void floor(double (&v)[5], const f64::StageArgs& A) {
         f32::floor_screened(v, A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
     }
+    __device__ static void stage(double (&v)[5], bool act, const f64::StageArgs& A, float (&w)[5]) {
+        f32::stage_floored(v, act, A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1, w);
+    }
     template <int D>
     __device__ static void flux(const float (&c)[6][6], const Consts& k, float F[5]) {
         f32::interface_flux<D>(c, k.g, k.gm1, k.inv_gm1, k.gg, F);

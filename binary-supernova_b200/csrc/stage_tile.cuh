@@ -59,6 +59,12 @@ struct F64Physics {
     __device__ static void floor(double (&v)[5], const f64::StageArgs& A) {
         f64::apply_floor(v[0], v[1], v[2], v[3], v[4], A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
     }
+    // a staged cell: floors on active cells, the staged copy
+    __device__ static void stage(double (&v)[5], bool act, const f64::StageArgs& A, double (&w)[5]) {
+        if (act) floor(v, A);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) w[q] = v[q];
+    }
     __device__ static double pressure(const double v[5], const Consts& k) {
         return f64::cell_pressure(v[0], v[1], v[2], v[3], v[4], k.gm1);
     }
@@ -154,13 +160,11 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
             double v[5];
             bool act;
             load_cell(A, G, D, a, b, c, v, act);
-            if (act) P::floor(v, A);
             real w[5];
+            P::stage(v, act, A, w);
 #pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                w[q] = (real)v[q];
+            for (int q = 0; q < 5; ++q)
                 if (q < 4 || P::kCols == 6) sC[q * S::NEXT + e] = w[q];
-            }
             sC[pcol<P::kCols>() * S::NEXT + e] = P::pressure(w, k);
         }
         // policies with per-stencil work that only non-uniform data can need
@@ -358,13 +362,11 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
             double v[5];
             bool act;
             load_cell(A, G, d, a, b, c, v, act);
-            if (act) P::floor(v, A);
             real w[5];
+            P::stage(v, act, A, w);
 #pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                w[q] = (real)v[q];
+            for (int q = 0; q < 5; ++q)
                 if (q < 4 || P::kCols == 6) sC[q * S::NCROSS + e] = w[q];
-            }
             sC[pcol<P::kCols>() * S::NCROSS + e] = P::pressure(w, k);
         }
     }
