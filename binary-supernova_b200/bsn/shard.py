@@ -1,0 +1,208 @@
+"""Z-slab domain decomposition of the uniform-grid update across ranks (one
+process per GPU; torch.distributed over NCCL between GPUs, gloo on CPU).
+
+Rank r of W holds z-planes [r nz, (r + 1) nz) of an nx x ny x (W nz) grid,
+with the usual three ghost planes on every side.  One SSP-RK3 step is the
+reference's euler3d_step! (src/euler3d.jl:220-260) with a halo exchange in
+front of every right-hand side:
+
+  1. fill the slab's ghosts by the boundary condition (x, then y, then z);
+  2. replace the z ghost planes that face a neighbouring rank by that rank's
+     three boundary planes (send/recv), floored as the reference floors them
+     before its fluxes where they are active cells of the global grid (their
+     x/y ghost columns are the copies its ghost fill made; across a periodic
+     wrap they are its ghost planes, filled before the floors, and stay raw);
+  3. euler3d_rhs! without its own ghost fill (it floors the slab's active
+     cells and computes the fluxes with the ghosts as they stand);
+  4. the stage combination and floors of euler3d_step!.
+
+The active cells of every slab are then bit-identical to the same cells of
+the undivided grid (FP64), and dt = min over ranks of each slab's
+cfl_dt_3d equals the undivided grid's (IEEE division is monotone).  The
+exchange per stage is 3 planes x 5 variables x (nx+6)(ny+6) words each way.
+
+The operations of steps 1, 3 and 4 come from an `ops` object (`DeviceOps`:
+this library's C ABI on CUDA tensors), so the exchange logic is the same
+whatever computes the stages.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import torch
+
+NG = 3
+
+
+@dataclass
+class Slab:
+    """This rank's part of the global z range and its neighbours (None at an
+    outflow boundary; periodic z wraps around)."""
+    nx: int
+    ny: int
+    nz: int           # planes held by this rank
+    rank: int
+    world: int
+    bc: str = "outflow"
+
+    @classmethod
+    def split(cls, nx, ny, nz_global, rank, world, bc="outflow"):
+        if world < 1 or not 0 <= rank < world:
+            raise ValueError(f"rank {rank} of {world}")
+        if nz_global % world:
+            raise ValueError(f"{nz_global} z-planes do not split evenly over {world} ranks")
+        nz = nz_global // world
+        if nz < NG:
+            raise ValueError(f"{nz} planes per rank: at least {NG} are needed for the 3-plane halo")
+        if bc not in ("outflow", "periodic"):
+            raise ValueError(f"unknown boundary condition {bc!r}")
+        return cls(nx, ny, nz, rank, world, bc)
+
+    @property
+    def k0(self) -> int:
+        """first global active plane of this slab"""
+        return self.rank * self.nz
+
+    @property
+    def lo(self):
+        if self.rank > 0:
+            return self.rank - 1
+        return self.world - 1 if (self.bc == "periodic" and self.world > 1) else None
+
+    @property
+    def hi(self):
+        if self.rank < self.world - 1:
+            return self.rank + 1
+        return 0 if (self.bc == "periodic" and self.world > 1) else None
+
+
+def _zmajor(U):
+    """(Z, Y, X, 5) C-contiguous view of a state array in the reference layout
+    (a torch tensor, or a Fortran-ordered numpy array)."""
+    if isinstance(U, torch.Tensor):
+        V = U.permute(3, 2, 1, 0)
+    else:
+        V = torch.from_numpy(U.T)
+    assert V.is_contiguous()
+    return V
+
+
+def exchange(U, slab: Slab, ops, group=None, rho_floor=0.0, P_floor=0.0, gamma=1.4):
+    """Step 2 above: the z ghost planes facing other ranks from those ranks'
+    boundary planes, floored."""
+    if slab.world == 1:
+        return
+    import torch.distributed as dist
+    V = _zmajor(U)
+    nz = slab.nz
+    ops_list, recv = [], []
+    # tag 0: my top planes go up (to hi's bottom ghosts); tag 1: my bottom planes go down
+    # planes from an interior neighbour are active cells of the global grid and
+    # are floored; across the periodic wrap they are the global grid's ghost
+    # planes, which the reference fills (unfloored) before it floors
+    if slab.hi is not None:
+        ops_list.append(dist.P2POp(dist.isend, V[nz:nz + NG].clone(), slab.hi, group, tag=0))
+        buf = torch.empty_like(V[NG + nz:])
+        ops_list.append(dist.P2POp(dist.irecv, buf, slab.hi, group, tag=1))
+        recv.append((slice(NG + nz, 2 * NG + nz), buf, slab.rank < slab.world - 1))
+    if slab.lo is not None:
+        ops_list.append(dist.P2POp(dist.isend, V[NG:2 * NG].clone(), slab.lo, group, tag=1))
+        buf = torch.empty_like(V[:NG])
+        ops_list.append(dist.P2POp(dist.irecv, buf, slab.lo, group, tag=0))
+        recv.append((slice(0, NG), buf, slab.rank > 0))
+    for req in dist.batch_isend_irecv(ops_list):
+        req.wait()
+    for sl, buf, interior in recv:
+        V[sl] = ops.floor_planes(buf, slab.nx, slab.ny, rho_floor, P_floor, gamma) if interior else buf
+
+
+def _allreduce_min(x: float, ops, group, world):
+    if world == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=ops.device)
+    dist.all_reduce(t, op=dist.ReduceOp.MIN, group=group)
+    return float(t.item())
+
+
+def cfl_dt(U, slab: Slab, dx, dy, dz, gamma, cfl, ops, group=None) -> float:
+    """cfl_dt_3d of the global grid: the min over ranks."""
+    return _allreduce_min(ops.cfl(U, slab.nx, slab.ny, slab.nz, dx, dy, dz, gamma, cfl), ops, group, slab.world)
+
+
+def euler3d_step(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group=None, rho_floor=0.0, P_floor=0.0):
+    """euler3d_step! (src/euler3d.jl:220-260) on this rank's slab, with the
+    halo exchange before every right-hand side."""
+    nx, ny, nz = slab.nx, slab.ny, slab.nz
+    Un = ops.copy(U)
+    dU = ops.zeros_like(U)
+    for stage in range(3):
+        ops.fill(U, nx, ny, nz, slab.bc)
+        exchange(U, slab, ops, group, rho_floor, P_floor, gamma)
+        ops.rhs(dU, U, nx, ny, nz, dx, dy, dz, gamma, slab.bc, rho_floor, P_floor)
+        if stage == 0:
+            ops.assign(U, Un + dt * dU)
+        elif stage == 1:
+            ops.assign(U, 0.75 * Un + 0.25 * U + (0.25 * dt) * dU)
+        else:
+            ops.assign(U, (1.0 / 3.0) * Un + (2.0 / 3.0) * U + ((2.0 / 3.0) * dt) * dU)
+        ops.floors(U, nx, ny, nz, rho_floor, P_floor, gamma)
+
+
+def run_steps(U, slab: Slab, dx, dy, dz, gamma, cfl, ops, *, n_steps, t=0.0, t_end=0.0, group=None,
+              rho_floor=0.0, P_floor=0.0):
+    """The driver loop `dt = cfl_dt_3d; dt = min(dt, t_end - t); euler3d_step!;
+    t += dt` over the slabs (every rank takes the same dts); returns (t, steps)."""
+    steps = 0
+    while steps < n_steps and (t_end <= 0.0 or t < t_end):
+        dt = cfl_dt(U, slab, dx, dy, dz, gamma, cfl, ops, group)
+        if t_end > 0.0:
+            dt = min(dt, t_end - t)
+        if not dt > 0.0:
+            raise FloatingPointError(f"time step collapsed to {dt} at t = {t}")
+        euler3d_step(U, slab, dx, dy, dz, dt, gamma, ops, group, rho_floor, P_floor)
+        t += dt
+        steps += 1
+    return t, steps
+
+
+class DeviceOps:
+    """The slab operations on CUDA tensors through this library's C ABI."""
+
+    def __init__(self, device="cuda"):
+        from . import api
+        self.api = api
+        self.device = torch.device(device)
+
+    @staticmethod
+    def copy(U):
+        return U.clone()
+
+    @staticmethod
+    def zeros_like(U):
+        return torch.zeros_like(U)
+
+    @staticmethod
+    def assign(U, V):
+        U.copy_(V)
+
+    def fill(self, U, nx, ny, nz, bc):
+        (self.api.fill_ghost_3d_outflow if bc == "outflow" else self.api.fill_ghost_3d_periodic)(U, nx, ny, nz)
+
+    def rhs(self, dU, U, nx, ny, nz, dx, dy, dz, gamma, bc, rho_floor, P_floor):
+        self.api.euler3d_rhs(dU, None, None, None, U, nx, ny, nz, dx, dy, dz, gamma, bc=bc, rho_floor=rho_floor,
+                             P_floor=P_floor, fill_ghosts=False)
+
+    def floors(self, U, nx, ny, nz, rho_floor, P_floor, gamma):
+        self.api.apply_floors_3d(U, nx, ny, nz, rho_floor, P_floor, gamma)
+
+    def cfl(self, U, nx, ny, nz, dx, dy, dz, gamma, cfl):
+        return self.api.cfl_dt_3d(U, nx, ny, nz, dx, dy, dz, gamma, cfl)
+
+    def floor_planes(self, planes, nx, ny, rho_floor, P_floor, gamma):
+        """apply_floors_3d! on the active (i, j) cells of NG received z-planes
+        ((NG, Y, X, 5) C-contiguous), through a ghosted scratch array."""
+        G = self.api.state(nx, ny, NG, device=planes.device)
+        _zmajor(G)[NG:2 * NG] = planes
+        self.api.apply_floors_3d(G, nx, ny, NG, rho_floor, P_floor, gamma)
+        return _zmajor(G)[NG:2 * NG]

@@ -1,0 +1,147 @@
+"""The z-slab decomposition (bsn/shard.py) on CPU: two or four gloo ranks, each
+stepping its slab of the grid with the oracle's right-hand side, ghost fill
+and floors, exchanging halos through torch.distributed; the active cells of
+every slab must be bit-identical to the oracle's undivided euler3d_step!
+(src/euler3d.jl:220-260) driver loop, and every rank must take the same dts."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+NG = 3
+
+
+class OracleOps:
+    """The slab operations on Fortran-ordered numpy arrays through the oracle
+    (test infrastructure: it checks the exchange logic, not a product path)."""
+
+    def __init__(self, orc, dx):
+        import torch
+        self.orc = orc
+        self.device = torch.device("cpu")
+
+    @staticmethod
+    def copy(U):
+        return U.copy(order="F")
+
+    @staticmethod
+    def zeros_like(U):
+        return np.zeros_like(U, order="F")
+
+    @staticmethod
+    def assign(U, V):
+        U[...] = V
+
+    def fill(self, U, nx, ny, nz, bc):
+        (self.orc.fill_ghost_3d_outflow if bc == "outflow" else self.orc.fill_ghost_3d_periodic)(U)
+
+    def rhs(self, dU, U, nx, ny, nz, dx, dy, dz, gamma, bc, rho_floor, P_floor):
+        Fx, Fy, Fz = self.orc.flux_arrays(nx, ny, nz)
+        self.orc.euler3d_rhs(dU, Fx, Fy, Fz, U, dx, dy, dz, gamma, bc=bc, rho_floor=rho_floor, P_floor=P_floor,
+                             fill_ghosts=False)
+
+    def floors(self, U, nx, ny, nz, rho_floor, P_floor, gamma):
+        self.orc.apply_floors_3d(U, rho_floor, P_floor, gamma)
+
+    def cfl(self, U, nx, ny, nz, dx, dy, dz, gamma, cfl):
+        return self.orc.cfl_dt_3d(U, dx, dy, dz, gamma, cfl)
+
+    def floor_planes(self, planes, nx, ny, rho_floor, P_floor, gamma):
+        import torch
+        G = self.orc.state(nx, ny, NG)
+        torch.from_numpy(G.T)[NG:2 * NG] = planes
+        self.orc.apply_floors_3d(G, rho_floor, P_floor, gamma)
+        return torch.from_numpy(G.T)[NG:2 * NG].clone()
+
+
+def _initial(orc, n, nzg, seed, bc):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from gpu_util import random_state
+    U = random_state(n, n, nzg, seed=seed, gamma=1.4, vacuum=True)
+    (orc.fill_ghost_3d_outflow if bc == "outflow" else orc.fill_ghost_3d_periodic)(U)
+    return U
+
+
+def _worker(rank, world, port, bc, q, use_loop=False):
+    try:
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        import torch.distributed as dist
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        sys.path.insert(0, os.path.join(ROOT, "binary-supernova_b200"))
+        import oracle as orc
+        from bsn import shard
+        dist.init_process_group("gloo", rank=rank, world_size=world)
+        n, nzg, dx, g = 10, 16, 0.1, 1.4
+        kw = dict(rho_floor=1e-6, P_floor=1e-5)
+        U = _initial(orc, n, nzg, 7, bc)
+        ref = U.copy(order="F")
+        slab = shard.Slab.split(n, n, nzg, rank, world, bc)
+        k0 = slab.k0
+        Us = orc.state(n, n, slab.nz)
+        Us[...] = U[:, :, :, k0:k0 + slab.nz + 2 * NG]
+        ops = OracleOps(orc, dx)
+        if use_loop:
+            t, steps = shard.run_steps(Us, slab, dx, dx, dx, g, 0.4, ops, n_steps=3, **kw)
+            t_ref = 0.0
+            for _ in range(3):
+                dt_ref = orc.cfl_dt_3d(ref, dx, dx, dx, g, 0.4)
+                orc.euler3d_step(ref, dx, dx, dx, dt_ref, g, bc=bc, **kw)
+                t_ref += dt_ref
+            assert (t, steps) == (t_ref, 3), (rank, t, t_ref)
+        else:
+            for _ in range(3):
+                dt = shard.cfl_dt(Us, slab, dx, dx, dx, g, 0.4, ops)
+                shard.euler3d_step(Us, slab, dx, dx, dx, dt, g, ops, **kw)
+                # the undivided reference loop
+                dt_ref = orc.cfl_dt_3d(ref, dx, dx, dx, g, 0.4)
+                orc.euler3d_step(ref, dx, dx, dx, dt_ref, g, bc=bc, **kw)
+                assert dt == dt_ref, (rank, dt, dt_ref)
+        a = (slice(None), slice(NG, NG + n), slice(NG, NG + n))
+        mine = Us[a + (slice(NG, NG + slab.nz),)]
+        theirs = ref[a + (slice(NG + k0, NG + k0 + slab.nz),)]
+        same = (mine == theirs) | (np.isnan(mine) & np.isnan(theirs))
+        q.put((rank, bool(same.all()), int((~same).sum())))
+        dist.destroy_process_group()
+    except Exception as e:   # report to the parent instead of hanging it
+        q.put((rank, False, repr(e)))
+
+
+@pytest.mark.parametrize("world,bc,loop", [(2, "outflow", False), (2, "periodic", False), (4, "periodic", True)])
+def test_slabs_match_the_undivided_step(world, bc, loop):
+    import multiprocessing as mp
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, bc, q, loop)) for r in range(world)]
+    for p in procs:
+        p.start()
+    try:
+        res = [q.get(timeout=240) for _ in procs]
+    finally:
+        for p in procs:   # a rank left waiting on a failed peer is ended here
+            p.join(timeout=30)
+            if p.is_alive():
+                p.terminate()
+                p.join(timeout=10)
+    for rank, ok, info in sorted(res):
+        assert ok, (rank, info)
+
+
+def test_split_checks():
+    sys.path.insert(0, os.path.join(ROOT, "binary-supernova_b200"))
+    from bsn import shard
+    s = shard.Slab.split(8, 8, 16, 1, 4, "periodic")
+    assert (s.nz, s.k0, s.lo, s.hi) == (4, 4, 0, 2)
+    s = shard.Slab.split(8, 8, 16, 3, 4, "periodic")
+    assert s.hi == 0
+    s = shard.Slab.split(8, 8, 16, 0, 4)
+    assert s.lo is None and s.hi == 1
+    with pytest.raises(ValueError):
+        shard.Slab.split(8, 8, 15, 0, 2)
+    with pytest.raises(ValueError):
+        shard.Slab.split(8, 8, 8, 0, 4)   # 2 planes per rank < the 3-plane halo
