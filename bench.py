@@ -42,6 +42,7 @@ GAMMA = 5.0 / 3.0
 CFL = 0.4
 T_MID = 0.025     # start of the timed steps (Sedov run to t = 0.05)
 T_END = 0.05
+METRIC = "cell-updates/s per RK3 step (Sedov 3D, WENO5-Z+HLLC+SSP-RK3)"   # both arms
 
 
 _T0 = time.time()
@@ -163,7 +164,7 @@ def run_reference(args, rank, world):
         cpu_reference_rate(args.n, threads, nz, 1)
     rate, el, _ = cpu_reference_rate(args.n, threads, nz, args.steps)
     line = {
-        "impl": "reference", "metric": "cell-updates/s per RK3 step (Sedov 3D, FP64)", "value": rate,
+        "impl": "reference", "metric": METRIC, "value": rate,
         "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (Sedov initial condition)",
@@ -580,7 +581,7 @@ def run_bsn(args, rank, world):
             compare[f"{p_}_ms_per_step"] = m_ / args.steps
             compare[f"speedup_vs_{p_}"] = value / v_
         line = {
-            "metric": "cell-updates/s per RK3 step (Sedov 3D, WENO5-Z+HLLC+SSP-RK3)",
+            "metric": METRIC,
             "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if prec == "f64" else ("f32+bf16" if prec == "learned" else "f32"), "data": "synthetic (Sedov initial condition, sedov_ic_3d!)",
