@@ -233,30 +233,62 @@ __global__ void adam_kernel(float* P, float* grad, float* m, float* v, float sca
 }
 
 // ---------------------------------------------------------------------------
-// BF16 tensor-core inference.  Packed parameters (per side): W1b[32][16],
-// W2b[32][32], W3b[8][32] as BF16 (row = output unit, zero padded), then
-// b1[32], b2[32], b3[8] as FP32.
-constexpr int PK_W1 = 0, PK_W2 = PK_W1 + 32 * 16 * 2, PK_W3 = PK_W2 + 32 * 32 * 2, PK_B1 = PK_W3 + 8 * 32 * 2,
+// BF16 tensor-core inference.  Packed parameters (per side), in the order the
+// MMA fragments of lane (g, tg) = (lane / 4, lane % 4) read them, so that each
+// lane loads a fragment set with one 16-byte shared-memory load:
+//   F1[lane][j]      layer-1 B fragment of output block j (m16n8k8: one word)
+//   F2[lane][j][i]   layer-2 B fragments of block j, i = (k-step, half)
+//   F3[lane][i]      layer-3 B fragments, i = (k-step, half)
+//   FB1[tg][j][h], FB2[tg][j][h], FB3[tg][h]   the lane's bias pairs (FP32)
+// A word holds two BF16 values (the lower k in the low half); rows are output
+// units, zero padded (inputs 5 -> 8 for layer 1, outputs 3 -> 8 for layer 3).
+constexpr int PK_F1 = 0, PK_F2 = PK_F1 + 32 * 4 * 4, PK_F3 = PK_F2 + 32 * 16 * 4, PK_B1 = PK_F3 + 32 * 4 * 4,
               PK_B2 = PK_B1 + 32 * 4, PK_B3 = PK_B2 + 32 * 4, PK_BYTES = PK_B3 + 8 * 4;   // bytes per side
-
-__global__ void pack_kernel(const float* P, unsigned char* out) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    __nv_bfloat16* W1 = (__nv_bfloat16*)(out + PK_W1);
-    __nv_bfloat16* W2 = (__nv_bfloat16*)(out + PK_W2);
-    __nv_bfloat16* W3 = (__nv_bfloat16*)(out + PK_W3);
-    float* B1 = (float*)(out + PK_B1);
-    float* B2 = (float*)(out + PK_B2);
-    float* B3 = (float*)(out + PK_B3);
-    if (i < 32 * 16) { int n = i / 16, k = i % 16; W1[i] = __float2bfloat16(k < NIN ? P[OFF_W1 + n * NIN + k] : 0.f); }
-    if (i < 32 * 32) W2[i] = __float2bfloat16(P[OFF_W2 + i]);
-    if (i < 8 * 32) { int n = i / 32, k = i % 32; W3[i] = __float2bfloat16(n < NOUT ? P[OFF_W3 + n * NH + k] : 0.f); }
-    if (i < 32) { B1[i] = P[OFF_B1 + i]; B2[i] = P[OFF_B2 + i]; }
-    if (i < 8) B3[i] = i < NOUT ? P[OFF_B3 + i] : 0.f;
-}
+static_assert(PK_F2 % 16 == 0 && PK_F3 % 16 == 0 && PK_B1 % 16 == 0 && PK_B2 % 16 == 0 && PK_B3 % 16 == 0 &&
+                  PK_BYTES % 16 == 0, "16-byte fragment loads");
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
     __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<uint32_t*>(&h);
+}
+
+// layer weights (row n = output unit, column k = input) with the zero padding
+__device__ __forceinline__ float w1_at(const float* P, int n, int k) { return k < NIN ? P[OFF_W1 + n * NIN + k] : 0.f; }
+__device__ __forceinline__ float w2_at(const float* P, int n, int k) { return P[OFF_W2 + n * NH + k]; }
+__device__ __forceinline__ float w3_at(const float* P, int n, int k) { return n < NOUT ? P[OFF_W3 + n * NH + k] : 0.f; }
+
+__global__ void pack_kernel(const float* P, unsigned char* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t* F1 = (uint32_t*)(out + PK_F1);
+    uint32_t* F2 = (uint32_t*)(out + PK_F2);
+    uint32_t* F3 = (uint32_t*)(out + PK_F3);
+    float* B1 = (float*)(out + PK_B1);
+    float* B2 = (float*)(out + PK_B2);
+    float* B3 = (float*)(out + PK_B3);
+    // word w of a row covers k = 2w, 2w + 1; the lane's fragment words are
+    // w = tg (layer 1) and w = tg, tg + 4, tg + 8, tg + 12 (k-steps 0 and 1)
+    if (i < 32 * 4) {
+        const int lane = i / 4, j = i % 4, g = lane / 4, tg = lane % 4, n = 8 * j + g;
+        F1[i] = pack2(w1_at(P, n, 2 * tg), w1_at(P, n, 2 * tg + 1));
+    }
+    if (i < 32 * 16) {
+        const int lane = i / 16, j = (i / 4) % 4, q = i % 4, g = lane / 4, tg = lane % 4, n = 8 * j + g;
+        const int w = tg + 4 * q;
+        F2[i] = pack2(w2_at(P, n, 2 * w), w2_at(P, n, 2 * w + 1));
+    }
+    if (i < 32 * 4) {
+        const int lane = i / 4, q = i % 4, g = lane / 4, tg = lane % 4, w = tg + 4 * q;
+        F3[i] = pack2(w3_at(P, g, 2 * w), w3_at(P, g, 2 * w + 1));
+    }
+    if (i < 32) {
+        const int tg = i / 8, j = (i / 2) % 4, h = i % 2, n = 8 * j + 2 * tg + h;
+        B1[i] = P[OFF_B1 + n];
+        B2[i] = P[OFF_B2 + n];
+    }
+    if (i < 8) {
+        const int tg = i / 2, h = i % 2, n = 2 * tg + h;
+        B3[i] = n < NOUT ? P[OFF_B3 + n] : 0.f;
+    }
 }
 
 // max(lo, 0), max(hi, 0) rounded to BF16 and packed (lo in the low half),
@@ -289,23 +321,27 @@ __device__ __forceinline__ void mma1688(float (&c)[4], uint32_t a0, uint32_t a1,
 // stored, and tile t's logits land below tile t+1's rows).
 __device__ __noinline__ void mlp_tiles(const unsigned char* pk, const uint32_t* rows, float* out, int ntiles) {
     const int lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
-    const uint32_t* W1 = (const uint32_t*)(pk + PK_W1);   // row n: 8 words
-    const uint32_t* W2 = (const uint32_t*)(pk + PK_W2);   // row n: 16 words
-    const uint32_t* W3 = (const uint32_t*)(pk + PK_W3);   // row n: 16 words
-    const float* B1 = (const float*)(pk + PK_B1);
-    const float* B2 = (const float*)(pk + PK_B2);
-    const float* B3 = (const float*)(pk + PK_B3);
+    const uint4* F1 = (const uint4*)(pk + PK_F1) + lane;          // words j = 0..3
+    const uint4* F2 = (const uint4*)(pk + PK_F2) + 4 * lane;      // per j: (k-step 0: lo, hi, k-step 1: lo, hi)
+    const uint4* F3 = (const uint4*)(pk + PK_F3) + lane;
+    const float4* B1 = (const float4*)(pk + PK_B1) + 2 * tg;      // (j, h) pairs, j = 0..3
+    const float4* B2 = (const float4*)(pk + PK_B2) + 2 * tg;
+    const float2* B3 = (const float2*)(pk + PK_B3) + tg;
     for (int tile = 0; tile < ntiles; ++tile) {
         int r0 = tile * 16 + g, r1 = r0 + 8;
         const uint32_t a0 = rows[r0 * 4 + tg], a1 = rows[r1 * 4 + tg];
         __syncwarp();
         // layer 1: 8 (5 used) -> 32, bias as the accumulator's initial value
+        const uint4 w1 = *F1;
+        const float4 b1a = B1[0], b1b = B1[1];
+        const float b1[8] = {b1a.x, b1a.y, b1a.z, b1a.w, b1b.x, b1b.y, b1b.z, b1b.w};
+        const uint32_t w1s[4] = {w1.x, w1.y, w1.z, w1.w};
         float h[4][4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            float c0 = B1[8 * j + 2 * tg], c1 = B1[8 * j + 2 * tg + 1];
+            const float c0 = b1[2 * j], c1 = b1[2 * j + 1];
             h[j][0] = c0; h[j][1] = c1; h[j][2] = c0; h[j][3] = c1;
-            mma1688(h[j], a0, a1, W1[(8 * j + g) * 8 + tg]);
+            mma1688(h[j], a0, a1, w1s[j]);
         }
         // ReLU, BF16 and the A fragments of the next layer in one instruction per pair
         uint32_t a2[2][4];
@@ -317,13 +353,15 @@ __device__ __noinline__ void mlp_tiles(const unsigned char* pk, const uint32_t* 
             a2[kk][3] = pack2_relu(h[2 * kk + 1][2], h[2 * kk + 1][3]);
         }
         // layer 2: 32 -> 32
+        const float4 b2a = B2[0], b2b = B2[1];
+        const float b2[8] = {b2a.x, b2a.y, b2a.z, b2a.w, b2b.x, b2b.y, b2b.z, b2b.w};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            float c0 = B2[8 * j + 2 * tg], c1 = B2[8 * j + 2 * tg + 1];
+            const uint4 w2 = F2[j];
+            const float c0 = b2[2 * j], c1 = b2[2 * j + 1];
             h[j][0] = c0; h[j][1] = c1; h[j][2] = c0; h[j][3] = c1;
-#pragma unroll
-            for (int kk = 0; kk < 2; ++kk)
-                mma16816(h[j], a2[kk], W2[(8 * j + g) * 16 + 8 * kk + tg], W2[(8 * j + g) * 16 + 8 * kk + 4 + tg]);
+            mma16816(h[j], a2[0], w2.x, w2.y);
+            mma16816(h[j], a2[1], w2.z, w2.w);
         }
 #pragma unroll
         for (int kk = 0; kk < 2; ++kk) {
@@ -333,9 +371,11 @@ __device__ __noinline__ void mlp_tiles(const unsigned char* pk, const uint32_t* 
             a2[kk][3] = pack2_relu(h[2 * kk + 1][2], h[2 * kk + 1][3]);
         }
         // layer 3: 32 -> 8 (3 used)
-        float o[4] = {B3[2 * tg], B3[2 * tg + 1], B3[2 * tg], B3[2 * tg + 1]};
-#pragma unroll
-        for (int kk = 0; kk < 2; ++kk) mma16816(o, a2[kk], W3[g * 16 + 8 * kk + tg], W3[g * 16 + 8 * kk + 4 + tg]);
+        const uint4 w3 = *F3;
+        const float2 b3 = *B3;
+        float o[4] = {b3.x, b3.y, b3.x, b3.y};
+        mma16816(o, a2[0], w3.x, w3.y);
+        mma16816(o, a2[1], w3.z, w3.w);
         __syncwarp();
         if (tg == 0) {
             out[4 * r0 + 0] = o[0]; out[4 * r0 + 1] = o[1];
