@@ -6,7 +6,7 @@ The grid is a uniform flow with a random blob (shock and near-vacuum cells
 included) in its far corner.  A step only reads nine cells around each cell,
 so the corner's 24^3 active cells must come out exactly as the oracle's step
 (src/euler3d.jl:220-260) of a 24^3 grid holding the same corner; the CFL
-maximum over 4.5e8 cells must equal the small grid's.  Needs ~80 GB free on
+maximum over 4.4e8 cells must equal the small grid's.  Needs ~80 GB free on
 the device (the state, two stage buffers and the autotuner's scratch)."""
 import numpy as np
 import pytest
