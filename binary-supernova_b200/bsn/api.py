@@ -28,6 +28,7 @@ __all__ = [
     "fill_ghost_3d_outflow", "fill_ghost_3d_periodic", "apply_floors_3d", "euler3d_rhs", "euler3d_step",
     "cfl_dt_3d", "add_bh_gravity_source", "gas_force_on_bh", "add_sink_sources", "accrete", "r_sink", "t_sink",
     "nbody_step", "KeplerOrbit", "kepler_update", "solve_poisson_isolated", "add_self_gravity_source",
+    "poisson_slab_forward", "poisson_slab_zconv", "poisson_slab_inverse",
     "apply_sg_force_level", "coupled_step", "FMRGrid3D", "fmr3d_step", "cfl_dt_fmr3d", "solve_fmr_poisson",
     "restrict_density_to_coarse", "FMRHierarchy3D", "fmr_nested_step", "cfl_dt_fmr_nested",
     "fmr_nested_run_steps", "coupled_nested_run_steps", "rotating_frame_source", "relax_damping_source",
@@ -75,6 +76,13 @@ def _ptr(t) -> C.c_void_p | None:
         return None
     if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64):
         raise TypeError("expected a CUDA float64 tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _cptr(t) -> C.c_void_p:
+    """a CUDA complex128 tensor as interleaved doubles"""
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.complex128):
+        raise TypeError("expected a CUDA complex128 tensor")
     return C.c_void_p(t.data_ptr())
 
 
@@ -257,6 +265,35 @@ def solve_poisson_isolated(rho, nx, ny, nz, dx, dy, dz, *, precision="f64") -> t
     phi = active_grid(nx, ny, nz, device=rho.device)
     name = {"f64": "bsn_solve_poisson_isolated_f64", "f32": "bsn_solve_poisson_isolated_f32"}[precision]
     _call(name, context(), _ptr(rho), nx, ny, nz, float(dx), float(dy), float(dz), _ptr(phi))
+    return phi
+
+
+def poisson_slab_forward(rho, nx, ny, nzl) -> torch.Tensor:
+    """x and y transforms of a slab of nzl density planes (rho column-major
+    (nx, ny, nzl)): complex128 W2 of shape (nzl, 2ny, nx+1)."""
+    _check_grid(rho, nx, ny, nzl, "rho")
+    W2 = torch.empty((nzl, 2 * ny, nx + 1), dtype=torch.complex128, device=rho.device)
+    _call("bsn_poisson_slab_forward_f64", context(), _ptr(rho), nx, ny, nzl, _cptr(W2))
+    return W2
+
+
+def poisson_slab_zconv(T, nx, ny, nz, ky0, dx, dy, dz):
+    """z transform, Green's function of the global nx x ny x nz grid and
+    inverse z transform of T (complex128 (nz, nky, nx+1), ky = ky0 + kyl), in place."""
+    if T.dtype != torch.complex128 or T.dim() != 3 or T.shape[0] != nz or T.shape[2] != nx + 1 \
+            or not T.is_contiguous():
+        raise ValueError(f"T must be contiguous complex128 (nz, nky, nx+1), got {tuple(T.shape)} {T.dtype}")
+    _call("bsn_poisson_slab_zconv_f64", context(), _cptr(T), nx, ny, nz, int(ky0), int(T.shape[1]), float(dx),
+          float(dy), float(dz))
+
+
+def poisson_slab_inverse(W2, nx, ny, nzl) -> torch.Tensor:
+    """y and x inverse transforms of W2 (complex128 (nzl, 2ny, nx+1)): the
+    slab's potential, column-major (nx, ny, nzl)."""
+    if W2.dtype != torch.complex128 or tuple(W2.shape) != (nzl, 2 * ny, nx + 1) or not W2.is_contiguous():
+        raise ValueError(f"W2 must be contiguous complex128 {(nzl, 2 * ny, nx + 1)}, got {tuple(W2.shape)}")
+    phi = active_grid(nx, ny, nzl, device=W2.device)
+    _call("bsn_poisson_slab_inverse_f64", context(), _cptr(W2), nx, ny, nzl, _ptr(phi))
     return phi
 
 

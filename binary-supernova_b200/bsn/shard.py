@@ -24,6 +24,11 @@ exchange per stage is 3 planes x 5 variables x (nx+6)(ny+6) words each way.
 The operations of steps 1, 3 and 4 come from an `ops` object (`DeviceOps`:
 this library's C ABI on CUDA tensors), so the exchange logic is the same
 whatever computes the stages.
+
+`poisson_isolated` is the self-gravity solve on the same slabs: local x/y
+transforms, an all-to-all transpose to z lines, the z convolution with the
+global grid's Green's function, and the transpose back; on the device it is
+bit-identical to the undivided bsn_solve_poisson_isolated_f64.
 """
 from __future__ import annotations
 
@@ -166,6 +171,86 @@ def run_steps(U, slab: Slab, dx, dy, dz, gamma, cfl, ops, *, n_steps, t=0.0, t_e
     return t, steps
 
 
+# ---------------------------------------------------------------------------
+# solve_poisson_isolated (src/self_gravity.jl:35-76) over z-slabs
+#
+# The zero-padded convolution transforms x and y within each z-plane, so a
+# rank does those for its own planes; the z transform needs whole z lines, so
+# the spectrum is transposed (one all-to-all): rank r receives every rank's
+# planes for its share [b_r, b_{r+1}) of the 2ny y frequencies, convolves
+# those lines with the Green's function of the global grid, and a second
+# all-to-all returns each rank's planes.  Per rank and solve the exchange is
+# 2 x (nx+1) x 2ny x nzl complex doubles each way (minus the share it keeps).
+
+
+def ky_shares(ny: int, world: int):
+    """[b_r, b_{r+1}) of the 2ny y frequencies that rank r convolves along z."""
+    N2 = 2 * ny
+    return [(r * N2 // world, (r + 1) * N2 // world) for r in range(world)]
+
+
+class SlabPoisson:
+    """The three local phases of the distributed solve for one rank; the
+    caller moves the pieces between them (`poisson_isolated` does it with
+    all-to-alls, a one-device emulation by hand)."""
+
+    def __init__(self, slab: Slab, dx, dy, dz, ops):
+        self.slab, self.dx, self.dy, self.dz, self.ops = slab, dx, dy, dz, ops
+        self.ky = ky_shares(slab.ny, slab.world)
+        self.nkx = slab.nx + 1
+
+    def forward(self, rho):
+        """x, y transforms of this slab's density; the piece for each rank r
+        is its ky share of the slab's planes, (nzl, nky_r, nx+1)."""
+        s = self.slab
+        W2 = self.ops.poisson_forward(rho, s.nx, s.ny, s.nz)
+        return [W2[:, a:b].contiguous() for a, b in self.ky]
+
+    def forward_shapes(self):
+        a, b = self.ky[self.slab.rank]
+        return [(self.slab.nz, b - a, self.nkx)] * self.slab.world
+
+    def lines(self, recv):
+        """z convolution of this rank's ky share over all planes (recv[s]:
+        rank s's planes, in z order); the piece for each rank is its planes."""
+        s = self.slab
+        T = torch.cat(recv, 0).contiguous()
+        self.ops.poisson_zconv(T, s.nx, s.ny, s.nz * s.world, self.ky[s.rank][0], self.dx, self.dy, self.dz)
+        return [T[r * s.nz:(r + 1) * s.nz] for r in range(s.world)]
+
+    def back_shapes(self):
+        return [(self.slab.nz, b - a, self.nkx) for a, b in self.ky]
+
+    def inverse(self, recv):
+        """y, x inverse transforms of this slab's planes (recv[r]: rank r's ky
+        share): the slab's potential (nx, ny, nzl)."""
+        s = self.slab
+        return self.ops.poisson_inverse(torch.cat(recv, 1).contiguous(), s.nx, s.ny, s.nz)
+
+
+def _all_to_all(pieces, shapes, group):
+    """pieces[r] goes to rank r; returns what each rank sent here, shaped."""
+    import torch.distributed as dist
+    send = torch.cat([torch.view_as_real(p).reshape(-1) for p in pieces])
+    out = [2 * a * b * c for a, b, c in shapes]
+    recv = torch.empty(sum(out), dtype=torch.float64, device=send.device)
+    dist.all_to_all_single(recv, send, output_split_sizes=out, input_split_sizes=[2 * p.numel() for p in pieces],
+                           group=group)
+    return [torch.view_as_complex(c.view(*sh, 2)) for c, sh in zip(recv.split(out), shapes)]
+
+
+def poisson_isolated(rho, slab: Slab, dx, dy, dz, ops, group=None):
+    """solve_poisson_isolated of the global nx x ny x (world nz) grid from this
+    rank's density planes rho (nx, ny, nz); returns this rank's planes of phi.
+    nx, ny and the global nz are powers of two (the isolated solve's FFTs)."""
+    P = SlabPoisson(slab, dx, dy, dz, ops)
+    if slab.world == 1:
+        return P.inverse(P.lines(P.forward(rho)))
+    recv = _all_to_all(P.forward(rho), P.forward_shapes(), group)
+    recv = _all_to_all(P.lines(recv), P.back_shapes(), group)
+    return P.inverse(recv)
+
+
 class DeviceOps:
     """The slab operations on CUDA tensors through this library's C ABI."""
 
@@ -198,6 +283,15 @@ class DeviceOps:
 
     def cfl(self, U, nx, ny, nz, dx, dy, dz, gamma, cfl):
         return self.api.cfl_dt_3d(U, nx, ny, nz, dx, dy, dz, gamma, cfl)
+
+    def poisson_forward(self, rho, nx, ny, nzl):
+        return self.api.poisson_slab_forward(rho, nx, ny, nzl)
+
+    def poisson_zconv(self, T, nx, ny, nz, ky0, dx, dy, dz):
+        self.api.poisson_slab_zconv(T, nx, ny, nz, ky0, dx, dy, dz)
+
+    def poisson_inverse(self, W2, nx, ny, nzl):
+        return self.api.poisson_slab_inverse(W2, nx, ny, nzl)
 
     def floor_planes(self, planes, nx, ny, rho_floor, P_floor, gamma):
         """apply_floors_3d! on the active (i, j) cells of NG received z-planes

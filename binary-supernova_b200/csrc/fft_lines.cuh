@@ -171,10 +171,12 @@ __global__ void axis_kernel(AxisIO<C> io, const C* tw, int logn, int lines, int 
 }
 
 // z forward (DIF) * Khat (bit-reversed order) * z inverse (DIT), in place in
-// W2[kx + (nx+1)*(ky + N2*z)], z < nz in and out.
+// W2[kx + (nx+1)*(kyl + nky*z)] for ky = ky0 + kyl (the whole ky range
+// ky0 = 0, nky = N2 on one GPU; a rank's share of it after the transpose of
+// a z-slab decomposition), z < nz in and out.
 template <class C>
 __global__ void z_conv_kernel(C* W2, const typename Cx<C>::R* khat, int nx, int N2, int ny, int nz, int logn,
-                              int lines, const C* tw) {
+                              int lines, const C* tw, int ky0, int nky) {
     using R = typename Cx<C>::R;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
@@ -184,16 +186,16 @@ __global__ void z_conv_kernel(C* W2, const typename Cx<C>::R* khat, int nx, int 
     load_twiddles(stw, tw, logn);
     int nkx = nx + 1;
     int nbx = (nkx + lines - 1) / lines;
-    int ky = blockIdx.x / nbx;
+    const int kyl = blockIdx.x / nbx, ky = ky0 + kyl;
     int kx0 = (blockIdx.x % nbx) * lines;
-    long long plane = (long long)nkx * N2;
+    long long plane = (long long)nkx * nky;
     for (int t = threadIdx.x; t < lines * N; t += blockDim.x) s[t] = Cx<C>::mk(R(0), R(0));
     __syncthreads();
     for (int t = threadIdx.x; t < lines * nz; t += blockDim.x) {
         int l = t % lines, z = t / lines;
         int kx = kx0 + l;
         if (kx >= nkx) continue;
-        s[l * N + z] = W2[kx + (long long)nkx * ky + plane * z];
+        s[l * N + z] = W2[kx + (long long)nkx * kyl + plane * z];
     }
     fft_dif(s, stw, lines, logn, false);
     int kyf = ky <= ny ? ky : N2 - ky;
@@ -211,7 +213,7 @@ __global__ void z_conv_kernel(C* W2, const typename Cx<C>::R* khat, int nx, int 
         int l = t % lines, z = t / lines;
         int kx = kx0 + l;
         if (kx >= nkx) continue;
-        W2[kx + (long long)nkx * ky + plane * z] = s[l * N + z];
+        W2[kx + (long long)nkx * kyl + plane * z] = s[l * N + z];
     }
 }
 
@@ -255,9 +257,9 @@ inline int fft_ilog2(int v) {
     return l;
 }
 
+// dynamic shared memory limit of the four line kernels, once per device
 template <class C>
-bsn_status solve_lines(bsn_ctx* ctx, const RhoSrc& src, const typename Cx<C>::R* K, const C* t1, const C* t2,
-                       const C* t3, C* W1, C* W2, double* phi, int smem_complex, int nt) {
+bsn_status line_attrs(bsn_ctx* ctx, int smem_complex) {
     static bool attr[64] = {false};
     const int dev = ctx->device & 63;
     if (!attr[dev]) {
@@ -268,6 +270,13 @@ bsn_status solve_lines(bsn_ctx* ctx, const RhoSrc& src, const typename Cx<C>::R*
             BSN_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         attr[dev] = true;
     }
+    return BSN_OK;
+}
+
+template <class C>
+bsn_status solve_lines(bsn_ctx* ctx, const RhoSrc& src, const typename Cx<C>::R* K, const C* t1, const C* t2,
+                       const C* t3, C* W1, C* W2, double* phi, int smem_complex, int nt) {
+    BSN_TRY(line_attrs<C>(ctx, smem_complex));
     const int nx = src.nx, ny = src.ny, nz = src.nz;
     const int N1 = 2 * nx, N2 = 2 * ny, N3 = 2 * nz;
     auto lines_for = [&](int N) { return std::max(1, std::min(64, smem_complex / N)); };
@@ -285,8 +294,73 @@ bsn_status solve_lines(bsn_ctx* ctx, const RhoSrc& src, const typename Cx<C>::R*
     int nbx3 = (nx + 1 + l3 - 1) / l3;
     prof_begin(ctx);
     z_conv_kernel<C><<<(unsigned)(nbx3 * N2), nt, smem_for(N3, l3), ctx->stream>>>(W2, K, nx, N2, ny, nz,
-                                                                                    fft_ilog2(N3), l3, t3);
+                                                                                    fft_ilog2(N3), l3, t3, 0, N2);
     BSN_TRY(launch_check(ctx, "z_conv_kernel"));
+    AxisIO<C> y2{W2, W1, nx + 1, nz, nx + 1, nx + 1, (long long)(nx + 1) * N2, (long long)(nx + 1) * ny, N2, ny};
+    prof_begin(ctx);
+    axis_kernel<C><<<(unsigned)(nbx2 * nz), nt, smem_for(N2, l2), ctx->stream>>>(y2, t2, fft_ilog2(N2), l2, 1);
+    BSN_TRY(launch_check(ctx, "fft_y_kernel"));
+    prof_begin(ctx);
+    inv_x_kernel<C><<<grid1d(rows, l1), nt, smem_for(N1, l1), ctx->stream>>>(W1, phi, nx, ny, nz, fft_ilog2(N1), l1,
+                                                                              t1);
+    return launch_check(ctx, "inv_x_kernel");
+}
+
+// The solve split at the z transform, for a z-slab decomposition (one rank
+// per slab of nzl planes; the kernels and their per-line arithmetic are those
+// of solve_lines, so the assembled potential is bit-identical to it).
+// Forward: x and y transforms of the slab's nzl density planes into
+// W2[kx + (nx+1)*(ky + N2*z)], z < nzl (W1: (nx+1) ny nzl scratch).
+template <class C>
+bsn_status slab_forward_lines(bsn_ctx* ctx, const RhoSrc& src, const C* t1, const C* t2, C* W1, C* W2,
+                              int smem_complex, int nt) {
+    BSN_TRY(line_attrs<C>(ctx, smem_complex));
+    const int nx = src.nx, ny = src.ny, nz = src.nz;
+    const int N1 = 2 * nx, N2 = 2 * ny;
+    auto lines_for = [&](int N) { return std::max(1, std::min(64, smem_complex / N)); };
+    auto smem_for = [&](int N, int lines) { return sizeof(C) * ((size_t)lines * N + N / 2); };
+    int l1 = lines_for(N1), l2 = lines_for(N2);
+    long long rows = (long long)ny * nz;
+    prof_begin(ctx);
+    fwd_x_kernel<C><<<grid1d(rows, l1), nt, smem_for(N1, l1), ctx->stream>>>(src, W1, t1, fft_ilog2(N1), l1);
+    BSN_TRY(launch_check(ctx, "fwd_x_kernel"));
+    int nbx2 = (nx + 1 + l2 - 1) / l2;
+    AxisIO<C> y1{W1, W2, nx + 1, nz, nx + 1, nx + 1, (long long)(nx + 1) * ny, (long long)(nx + 1) * N2, ny, N2};
+    prof_begin(ctx);
+    axis_kernel<C><<<(unsigned)(nbx2 * nz), nt, smem_for(N2, l2), ctx->stream>>>(y1, t2, fft_ilog2(N2), l2, 0);
+    return launch_check(ctx, "fft_y_kernel");
+}
+
+// z lines of the global grid (nz planes) for ky in [ky0, ky0 + nky), in place
+// in T[kx + (nx+1)*(kyl + nky*z)].
+template <class C>
+bsn_status slab_zconv_lines(bsn_ctx* ctx, C* T, const typename Cx<C>::R* K, const C* t3, int nx, int ny, int nz,
+                            int ky0, int nky, int smem_complex, int nt) {
+    BSN_TRY(line_attrs<C>(ctx, smem_complex));
+    const int N2 = 2 * ny, N3 = 2 * nz;
+    auto lines_for = [&](int N) { return std::max(1, std::min(64, smem_complex / N)); };
+    auto smem_for = [&](int N, int lines) { return sizeof(C) * ((size_t)lines * N + N / 2); };
+    int l3 = lines_for(N3);
+    int nbx3 = (nx + 1 + l3 - 1) / l3;
+    if (nky < 1) return BSN_OK;
+    prof_begin(ctx);
+    z_conv_kernel<C><<<(unsigned)(nbx3 * nky), nt, smem_for(N3, l3), ctx->stream>>>(T, K, nx, N2, ny, nz,
+                                                                                     fft_ilog2(N3), l3, t3, ky0, nky);
+    return launch_check(ctx, "z_conv_kernel");
+}
+
+// Inverse: y and x transforms of the slab's W2 (z < nzl) into its nzl planes
+// of Phi (W1: (nx+1) ny nzl scratch; W2 is left as it was).
+template <class C>
+bsn_status slab_inverse_lines(bsn_ctx* ctx, const C* W2, const C* t1, const C* t2, C* W1, double* phi, int nx,
+                              int ny, int nz, int smem_complex, int nt) {
+    BSN_TRY(line_attrs<C>(ctx, smem_complex));
+    const int N1 = 2 * nx, N2 = 2 * ny;
+    auto lines_for = [&](int N) { return std::max(1, std::min(64, smem_complex / N)); };
+    auto smem_for = [&](int N, int lines) { return sizeof(C) * ((size_t)lines * N + N / 2); };
+    int l1 = lines_for(N1), l2 = lines_for(N2);
+    long long rows = (long long)ny * nz;
+    int nbx2 = (nx + 1 + l2 - 1) / l2;
     AxisIO<C> y2{W2, W1, nx + 1, nz, nx + 1, nx + 1, (long long)(nx + 1) * N2, (long long)(nx + 1) * ny, N2, ny};
     prof_begin(ctx);
     axis_kernel<C><<<(unsigned)(nbx2 * nz), nt, smem_for(N2, l2), ctx->stream>>>(y2, t2, fft_ilog2(N2), l2, 1);

@@ -308,3 +308,64 @@ extern "C" bsn_status bsn_solve_poisson_isolated_f64(bsn_ctx* ctx, const double*
     BSN_TRY(check_dims(ctx, nx, ny, nz));
     return poisson_solve(ctx, rho, nx, ny, nz, dx, dy, dz, phi);
 }
+
+// ---- z-slab decomposition of solve_poisson_isolated -------------------------
+// A rank holding planes [z0, z0 + nzl) of the density runs slab_forward on
+// them, sends W2's ky range of every rank to that rank (an all-to-all), runs
+// slab_zconv on the z lines of its own ky range (all nz planes, in z order),
+// sends each rank's z range back and runs slab_inverse on its planes.  W2 and
+// T are interleaved complex doubles: W2[kx + (nx+1)*(ky + 2ny*z)], z < nzl;
+// T[kx + (nx+1)*(kyl + nky*z)], z < nz.
+
+static bsn_status slab_check(bsn_ctx* ctx, int nx, int ny, int nz) {
+    if (!ctx) return BSN_ERR_ARG;
+    if (!fft::pow2(nx) || !fft::pow2(ny) || nx < 2 || ny < 2 || nz < 1)
+        return set_err(ctx, BSN_ERR_UNSUPPORTED, "slab FFT needs power-of-two nx, ny >= 2 and nz >= 1 (got %d,%d,%d)",
+                       nx, ny, nz);
+    if (2 * std::max(nx, ny) > fft::SMEM_COMPLEX) return set_err(ctx, BSN_ERR_UNSUPPORTED, "FFT length above %d",
+                                                                 fft::SMEM_COMPLEX);
+    return BSN_OK;
+}
+
+extern "C" bsn_status bsn_poisson_slab_forward_f64(bsn_ctx* ctx, const double* rho, int nx, int ny, int nzl,
+                                                   double* W2) {
+    BSN_TRY(slab_check(ctx, nx, ny, nzl));
+    if (!rho || !W2) return set_err(ctx, BSN_ERR_ARG, "rho and W2 must be non-null");
+    const double2 *t1, *t2;
+    BSN_TRY(fft::twiddles(ctx, 2 * nx, &t1));
+    BSN_TRY(fft::twiddles(ctx, 2 * ny, &t2));
+    bsn_status st;
+    double2* W1 = (double2*)slot(ctx, SLOT_FFT0, sizeof(double2) * (size_t)(nx + 1) * ny * nzl, &st); BSN_TRY(st);
+    fft::RhoSrc src{rho, nullptr, nx, ny, nzl, -1.0};
+    return fft::slab_forward_lines<double2>(ctx, src, t1, t2, W1, (double2*)W2, fft::SMEM_COMPLEX, fft::NT);
+}
+
+extern "C" bsn_status bsn_poisson_slab_zconv_f64(bsn_ctx* ctx, double* T, int nx, int ny, int nz, int ky0, int nky,
+                                                 double dx, double dy, double dz) {
+    BSN_TRY(slab_check(ctx, nx, ny, nz));
+    if (!fft::pow2(nz) || nz < 2 || 2 * nz > fft::SMEM_COMPLEX)
+        return set_err(ctx, BSN_ERR_UNSUPPORTED, "global nz must be a power of two in [2, %d] (got %d)",
+                       fft::SMEM_COMPLEX / 2, nz);
+    if (ky0 < 0 || nky < 0 || ky0 + nky > 2 * ny)
+        return set_err(ctx, BSN_ERR_ARG, "ky range [%d, %d) outside [0, %d)", ky0, ky0 + nky, 2 * ny);
+    if (nky > 0 && !T) return set_err(ctx, BSN_ERR_ARG, "T must be non-null");
+    BSN_TRY(fft::set_smem(ctx));
+    const double* K;
+    BSN_TRY(fft::khat(ctx, nx, ny, nz, dx, dy, dz, &K));
+    const double2* t3;
+    BSN_TRY(fft::twiddles(ctx, 2 * nz, &t3));
+    return fft::slab_zconv_lines<double2>(ctx, (double2*)T, K, t3, nx, ny, nz, ky0, nky, fft::SMEM_COMPLEX, fft::NT);
+}
+
+extern "C" bsn_status bsn_poisson_slab_inverse_f64(bsn_ctx* ctx, const double* W2, int nx, int ny, int nzl,
+                                                   double* phi) {
+    BSN_TRY(slab_check(ctx, nx, ny, nzl));
+    if (!W2 || !phi) return set_err(ctx, BSN_ERR_ARG, "W2 and phi must be non-null");
+    const double2 *t1, *t2;
+    BSN_TRY(fft::twiddles(ctx, 2 * nx, &t1));
+    BSN_TRY(fft::twiddles(ctx, 2 * ny, &t2));
+    bsn_status st;
+    double2* W1 = (double2*)slot(ctx, SLOT_FFT0, sizeof(double2) * (size_t)(nx + 1) * ny * nzl, &st); BSN_TRY(st);
+    return fft::slab_inverse_lines<double2>(ctx, (const double2*)W2, t1, t2, W1, phi, nx, ny, nzl, fft::SMEM_COMPLEX,
+                                            fft::NT);
+}

@@ -233,6 +233,22 @@ bsn_status bsn_solve_poisson_isolated_f64(bsn_ctx* ctx, const double* rho, int n
  * rho in and phi out, FP32 spectra and Green's function. */
 bsn_status bsn_solve_poisson_isolated_f32(bsn_ctx* ctx, const double* rho, int nx, int ny, int nz,
                                           double dx, double dy, double dz, double* phi);
+/* solve_poisson_isolated of an nx x ny x nz grid split into z-slabs, one per
+ * rank (no reference counterpart: the reference solves on one device).  The
+ * three calls are the solve cut at its z transform; between them the caller
+ * moves data between ranks (an all-to-all), and the assembled potential is
+ * bit-identical to bsn_solve_poisson_isolated_f64.  W2, T: interleaved
+ * complex doubles, W2[kx + (nx+1)*(ky + 2ny*z)] for the slab's nzl planes,
+ * T[kx + (nx+1)*(kyl + nky*z)] for ky = ky0 + kyl and all nz planes; rho, phi
+ * (nx, ny, nzl).  nx, ny (and the global nz) powers of two.
+ * slab_forward: x, y transforms of the slab's density planes into W2.
+ * slab_zconv: z transform, Green's function of the global grid, inverse z
+ *   transform of the lines of T, in place.
+ * slab_inverse: y, x inverse transforms of W2 into the slab's potential. */
+bsn_status bsn_poisson_slab_forward_f64(bsn_ctx* ctx, const double* rho, int nx, int ny, int nzl, double* W2);
+bsn_status bsn_poisson_slab_zconv_f64(bsn_ctx* ctx, double* T, int nx, int ny, int nz, int ky0, int nky,
+                                      double dx, double dy, double dz);
+bsn_status bsn_poisson_slab_inverse_f64(bsn_ctx* ctx, const double* W2, int nx, int ny, int nzl, double* phi);
 /* _apply_sg_force_level! (src/fmr_gravity.jl:146-156; src/gpu_kernels.jl:291-319) */
 bsn_status bsn_sg_gradient_f64(bsn_ctx* ctx, double* dU, const double* U, const double* phi,
                                int nx, int ny, int nz, double dx, double dy, double dz);

@@ -132,6 +132,113 @@ def test_slabs_match_the_undivided_step(world, bc, loop):
         assert ok, (rank, info)
 
 
+class FFTOps:
+    """The three phases of the slab Poisson solve with torch.fft on CPU tensors
+    (test infrastructure: it checks the transposes, not a product path).
+    Green's function and normalisation of src/self_gravity.jl:35-76."""
+
+    def __init__(self):
+        import torch
+        self.torch = torch
+        self.device = torch.device("cpu")
+
+    def poisson_forward(self, rho, nx, ny, nzl):
+        fft = self.torch.fft
+        A = fft.fft(rho, n=2 * nx, dim=0)[:nx + 1]
+        return fft.fft(A, n=2 * ny, dim=1).permute(2, 1, 0).contiguous()        # (nzl, 2ny, nx+1)
+
+    def _khat(self, nx, ny, nz, dx, dy, dz):
+        torch = self.torch
+        f = lambda n, d: torch.tensor([(m if m < n else m - 2 * n) * d for m in range(2 * n)], dtype=torch.float64)
+        X, Y, Z = torch.meshgrid(f(nx, dx), f(ny, dy), f(nz, dz), indexing="ij")
+        eps2 = (dx * dy * dz) ** (2.0 / 3.0)
+        K = -1.0 / torch.sqrt(X * X + Y * Y + Z * Z + eps2)
+        return (dx * dy * dz) * torch.fft.fftn(K).real.permute(2, 1, 0)         # (2nz, 2ny, 2nx)
+
+    def poisson_zconv(self, T, nx, ny, nz, ky0, dx, dy, dz):
+        fft = self.torch.fft
+        Kh = self._khat(nx, ny, nz, dx, dy, dz)[:, ky0:ky0 + T.shape[1], :nx + 1]
+        T[...] = fft.ifft(fft.fft(T, n=2 * nz, dim=0) * Kh, dim=0)[:nz]
+
+    def poisson_inverse(self, W2, nx, ny, nzl):
+        fft = self.torch.fft
+        Y = fft.ifft(W2, dim=1)[:, :ny]
+        return fft.irfft(Y, n=2 * nx, dim=2)[:, :, :nx].permute(2, 1, 0)        # (nx, ny, nzl)
+
+
+def _density(n, nzg):
+    import torch
+    g = torch.Generator().manual_seed(5)
+    x = torch.linspace(-1, 1, n, dtype=torch.float64)
+    z = torch.linspace(-1, 1, nzg, dtype=torch.float64)
+    X, Y, Z = torch.meshgrid(x, x, z, indexing="ij")
+    return torch.exp(-4 * (X ** 2 + 2 * Y ** 2 + 3 * Z ** 2)) + 0.05 * torch.rand((n, n, nzg), generator=g,
+                                                                                  dtype=torch.float64)
+
+
+def _poisson_worker(rank, world, port, q):
+    try:
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        import torch
+        import torch.distributed as dist
+        sys.path.insert(0, os.path.join(ROOT, "binary-supernova_b200"))
+        from bsn import shard
+        dist.init_process_group("gloo", rank=rank, world_size=world)
+        n, nzg, d = 8, 16, (0.1, 0.12, 0.09)
+        rho = _density(n, nzg)
+        slab = shard.Slab.split(n, n, nzg, rank, world)
+        mine = shard.poisson_isolated(rho[:, :, slab.k0:slab.k0 + slab.nz], slab, *d, FFTOps())
+        whole = shard.poisson_isolated(rho, shard.Slab.split(n, n, nzg, 0, 1), *d, FFTOps())
+        ref = whole[:, :, slab.k0:slab.k0 + slab.nz]
+        err = float((mine - ref).abs().max() / ref.abs().max())
+        q.put((rank, err < 1e-13, err))
+        dist.destroy_process_group()
+    except Exception as e:   # report to the parent instead of hanging it
+        q.put((rank, False, repr(e)))
+
+
+def _spawn(target, world, extra=()):
+    import multiprocessing as mp
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=target, args=(r, world, port, q) + tuple(extra)) for r in range(world)]
+    for p in procs:
+        p.start()
+    try:
+        res = [q.get(timeout=240) for _ in procs]
+    finally:
+        for p in procs:   # a rank left waiting on a failed peer is ended here
+            p.join(timeout=30)
+            if p.is_alive():
+                p.terminate()
+                p.join(timeout=10)
+    return sorted(res)
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_slab_poisson_matches_the_undivided_solve(world):
+    for rank, ok, info in _spawn(_poisson_worker, world):
+        assert ok, (rank, info)
+
+
+def test_slab_poisson_phases_match_the_oracle(orc):
+    """The FFT phases the distributed test uses, undivided, against the
+    oracle's solve_poisson_isolated."""
+    sys.path.insert(0, os.path.join(ROOT, "binary-supernova_b200"))
+    from bsn import shard
+    n, nzg, d = 8, 16, (0.1, 0.12, 0.09)
+    rho = _density(n, nzg)
+    phi = shard.poisson_isolated(rho, shard.Slab.split(n, n, nzg, 0, 1), *d, FFTOps()).numpy()
+    want = orc.solve_poisson_isolated(rho.numpy(), *d)
+    assert np.abs(phi - want).max() <= 1e-12 * np.abs(want).max()
+    assert shard.ky_shares(8, 4) == [(0, 4), (4, 8), (8, 12), (12, 16)]
+    assert shard.ky_shares(2, 8)[0] == (0, 0)   # more ranks than y frequencies: some convolve nothing
+
+
 def test_split_checks():
     sys.path.insert(0, os.path.join(ROOT, "binary-supernova_b200"))
     from bsn import shard
