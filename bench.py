@@ -439,6 +439,29 @@ def coupled_binary(bsn, torch, steps, warmup, log, n=128):
     return out
 
 
+# Algorithmic floating-point operations per active cell per RK3 step of the
+# reference scheme (every +, -, *, /, sqrt and comparison of euler3d_step!
+# counted once; 3647 add, 4426 mul, 768 div, 18 sqrt, 1163 cmp), counted by
+# `python oracle/count_flops.py` on the Sedov 128^3 state at t = 0.025, the
+# timed workload's state at half the resolution (Sod 64^3: 10111).
+FLOPS_PER_CELL_STEP = 10023.4
+
+
+def fp_pipe(prec, ms, ms_other, cell_steps, peak):
+    """FP-pipe fraction of every path's whole step: FLOPS_PER_CELL_STEP per
+    cell-step over the measured FMA peak of its arithmetic (FP64; FP32 with
+    the better of scalar and packed f32x2 FMA)."""
+    out = {"flops_per_cell_step": FLOPS_PER_CELL_STEP, "unit": "TFLOP/s",
+           "peaks_measured": {k: round(v, 2) for k, v in peak.items()},
+           "note": "operations of the reference scheme (oracle count), not instructions issued: a division "
+                   "or square root counts one but costs several pipe operations"}
+    for p_, m_ in [(prec, ms)] + list(ms_other.items()):
+        a = FLOPS_PER_CELL_STEP * cell_steps / (m_ / 1e3) / 1e12
+        pk = peak["f64"] if p_ == "f64" else max(peak["f32"], peak["f32x2"])
+        out[p_] = {"achieved": a, "peak": pk, "frac": a / pk}
+    return out
+
+
 def run_bsn(args, rank, world):
     import numpy as np
     import torch
@@ -529,6 +552,10 @@ def run_bsn(args, rank, world):
     del Up
 
     log(f"roofline: {kname} {t_stage * 1e3:.3f} ms per launch")
+    # FP-pipe fraction of each path over its whole step: the reference scheme's
+    # operations per cell-step against this GPU's measured FMA throughput
+    peak_fp = {k_: bsn.fp_peak(k_) for k_ in ("f64", "f32", "f32x2")}
+    log("measured FMA peaks (TFLOP/s): " + ", ".join(f"{k_} {v_:.1f}" for k_, v_ in peak_fp.items()))
     acc = accuracy(bsn, torch, U0, n, dx, kw) if not args.no_accuracy else None
     fmr = fmr_polytrope(bsn, torch, max(5, min(args.steps, 20)), args.warmup, log) if not args.no_fmr else None
     coupled = coupled_binary(bsn, torch, max(5, min(args.steps, 20)), args.warmup, log) if not args.no_fmr else None
@@ -601,6 +628,7 @@ def run_bsn(args, rank, world):
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": t_stage * 1e3,
                          "note": "the fused stencil kernel is FP-pipe bound (FP32/FP64), not HBM bound; "
                                  "HBM fraction of the algorithmic 40 words/cell-step"},
+            "fp_pipe": fp_pipe(prec, ms, ms_other, ncell * world * args.steps, peak_fp),
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "steps": k_e2e},

@@ -61,6 +61,7 @@ SIGNATURES = {
     "bsn_ctx_launch_count": (_LL, [_V]),
     "bsn_ctx_set_profiling": (_I, [_V, _I]),
     "bsn_ctx_kernel_stats": (_I, [_V, C.c_char_p, _dp, C.POINTER(C.c_longlong)]),
+    "bsn_fp_peak": (_I, [_V, _I, _dp]),
     "bsn_fill_ghost_3d_f64": (_I, [_V, _P, _I, _I, _I, _I]),
     "bsn_apply_floors_3d_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D]),
     "bsn_euler3d_rhs_f64": (_I, [_V, _P, _P, _P, _P, _P, _I, _I, _I, _D, _D, _D, _D, _I, _D, _D, _I]),

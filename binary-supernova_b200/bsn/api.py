@@ -573,9 +573,16 @@ def kernel_time(name: str):
     return tot.value, cnt.value
 
 
+def fp_peak(precision="f64") -> float:
+    """Measured FMA throughput in TFLOP/s: "f64", "f32" or "f32x2" (packed)."""
+    out = C.c_double()
+    _call("bsn_fp_peak", context(), {"f64": 0, "f32": 1, "f32x2": 2}[precision], C.byref(out))
+    return out.value
+
+
 def set_profiling(on: bool):
     _call("bsn_ctx_set_profiling", context(), int(bool(on)))
 
 
 __all__ += ["euler3d_step_f32", "euler3d_step_learned", "run_steps", "fmr3d_run_steps", "coupled_run_steps", "diagnostics", "tile_variants", "set_tile", "get_tile", "kernel_time",
-            "set_profiling", "PREC"]
+            "set_profiling", "fp_peak", "PREC"]

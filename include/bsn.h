@@ -89,6 +89,10 @@ long long   bsn_ctx_launch_count(const bsn_ctx* ctx);
  * disabling clears the records; stats sum every recorded launch of `name`. */
 bsn_status  bsn_ctx_set_profiling(bsn_ctx* ctx, int on);
 bsn_status  bsn_ctx_kernel_stats(bsn_ctx* ctx, const char* name, double* total_ms, long long* count);
+/* Measured multiply-add throughput of the context's GPU in TFLOP/s (one FMA =
+ * 2 flops): precision 0 FP64, 1 FP32, 2 FP32 packed (f32x2 FMA).  The
+ * denominators of the stencil kernels' FP-pipe fraction; synchronises. */
+bsn_status  bsn_fp_peak(bsn_ctx* ctx, int precision, double* tflops);
 
 /* ---- src/euler3d.jl ------------------------------------------------------ */
 /* fill_ghost_3d_outflow! / fill_ghost_3d_periodic! (src/euler3d.jl:33-62) */

@@ -19,445 +19,8 @@
 #include <omp.h>
 #endif
 
-namespace {
+#include "hydro.inc"
 
-const int NG = 3;   /* src/BinarySupernova.jl:8 */
-
-/* Julia Base.max/min/clamp for Float64: NaN-propagating, max(+0,-0)=+0,
- * min(+0,-0)=-0; clamp(x,lo,hi) = x>hi ? hi : x<lo ? lo : x. */
-inline double jmax(double x, double y) {
-    if (x != x || y != y) return x + y;
-    if (x > y) return x;
-    if (y > x) return y;
-    return std::signbit(x) ? y : x;
-}
-inline double jmin(double x, double y) {
-    if (x != x || y != y) return x + y;
-    if (x < y) return x;
-    if (y < x) return y;
-    return std::signbit(x) ? x : y;
-}
-inline double jclamp(double x, double lo, double hi) { return x > hi ? hi : (x < lo ? lo : x); }
-inline double sq(double x) { return x * x; }
-
-/* Julia 1-based indexing helpers for U[q,i,j,k] with extents (5,NXT,NYT,NZT). */
-struct Idx {
-    long nxt, nyt, nzt;
-    Idx(int nx, int ny, int nz) : nxt(nx + 2 * NG), nyt(ny + 2 * NG), nzt(nz + 2 * NG) {}
-    inline long operator()(int q, int i, int j, int k) const {
-        return (long)(q - 1) + 5L * ((long)(i - 1) + nxt * ((long)(j - 1) + nyt * (long)(k - 1)));
-    }
-    long size() const { return 5L * nxt * nyt * nzt; }
-};
-struct FIdx {   /* (5, ex, ey, ez) general */
-    long ex, ey, ez;
-    FIdx(long a, long b, long c) : ex(a), ey(b), ez(c) {}
-    inline long operator()(int q, int i, int j, int k) const {
-        return (long)(q - 1) + 5L * ((long)(i - 1) + ex * ((long)(j - 1) + ey * (long)(k - 1)));
-    }
-    long size() const { return 5L * ex * ey * ez; }
-};
-
-int g_threads = 0;
-
-}  // namespace
-
-extern "C" void orc_set_threads(int n) {
-    g_threads = n;
-#ifdef _OPENMP
-    if (n > 0) omp_set_num_threads(n);
-#endif
-}
-
-/* ------------------------------------------------------------------------- */
-/* src/weno5.jl:14-21 */
-extern "C" void orc_wenoz_weights(double b0, double b1, double b2, double d0, double d1, double d2,
-                                  double out[3]) {
-    const double eps = 1e-36;
-    double tau5 = std::fabs(b0 - b2);
-    double a0 = d0 * (1.0 + sq(tau5 / (eps + b0)));
-    double a1 = d1 * (1.0 + sq(tau5 / (eps + b1)));
-    double a2 = d2 * (1.0 + sq(tau5 / (eps + b2)));
-    double asum = a0 + a1 + a2;
-    out[0] = a0 / asum; out[1] = a1 / asum; out[2] = a2 / asum;
-}
-
-/* src/weno5.jl:25-41 */
-extern "C" double orc_weno5_left(double vm2, double vm1, double v0, double vp1, double vp2) {
-    double q0 = (1.0 / 3.0) * vm2 + (-7.0 / 6.0) * vm1 + (11.0 / 6.0) * v0;
-    double q1 = (-1.0 / 6.0) * vm1 + (5.0 / 6.0) * v0 + (1.0 / 3.0) * vp1;
-    double q2 = (1.0 / 3.0) * v0 + (5.0 / 6.0) * vp1 + (-1.0 / 6.0) * vp2;
-    double b0 = (13.0 / 12.0) * sq(vm2 - 2.0 * vm1 + v0) + (1.0 / 4.0) * sq(vm2 - 4.0 * vm1 + 3.0 * v0);
-    double b1 = (13.0 / 12.0) * sq(vm1 - 2.0 * v0 + vp1) + (1.0 / 4.0) * sq(vm1 - vp1);
-    double b2 = (13.0 / 12.0) * sq(v0 - 2.0 * vp1 + vp2) + (1.0 / 4.0) * sq(3.0 * v0 - 4.0 * vp1 + vp2);
-    double w[3];
-    orc_wenoz_weights(b0, b1, b2, 1.0 / 10.0, 6.0 / 10.0, 3.0 / 10.0, w);
-    return w[0] * q0 + w[1] * q1 + w[2] * q2;
-}
-
-/* src/weno5.jl:45-61 */
-extern "C" double orc_weno5_right(double vm1, double v0, double vp1, double vp2, double vp3) {
-    double q0 = (-1.0 / 6.0) * vm1 + (5.0 / 6.0) * v0 + (1.0 / 3.0) * vp1;
-    double q1 = (1.0 / 3.0) * v0 + (5.0 / 6.0) * vp1 + (-1.0 / 6.0) * vp2;
-    double q2 = (11.0 / 6.0) * vp1 + (-7.0 / 6.0) * vp2 + (1.0 / 3.0) * vp3;
-    double b0 = (13.0 / 12.0) * sq(vm1 - 2.0 * v0 + vp1) + (1.0 / 4.0) * sq(vm1 - vp1);
-    double b1 = (13.0 / 12.0) * sq(v0 - 2.0 * vp1 + vp2) + (1.0 / 4.0) * sq(v0 - 4.0 * vp1 + 3.0 * vp2);
-    double b2 = (13.0 / 12.0) * sq(vp1 - 2.0 * vp2 + vp3) + (1.0 / 4.0) * sq(3.0 * vp1 - 4.0 * vp2 + vp3);
-    double w[3];
-    orc_wenoz_weights(b0, b1, b2, 3.0 / 10.0, 6.0 / 10.0, 1.0 / 10.0, w);
-    return w[0] * q0 + w[1] * q1 + w[2] * q2;
-}
-
-/* ------------------------------------------------------------------------- */
-/* src/hllc.jl:17-165  (_hllc_normal) */
-static void hllc_normal(double rL, double mnL, double mt1L, double mt2L, double EL,
-                        double rR, double mnR, double mt1R, double mt2R, double ER,
-                        double g, double F[5]) {
-    if (rL <= 0.0) { rL = 1e-30; mnL = 0.0; mt1L = 0.0; mt2L = 0.0; EL = 0.0; }
-    else           { rL = jmax(rL, 1e-30); }
-    if (rR <= 0.0) { rR = 1e-30; mnR = 0.0; mt1R = 0.0; mt2R = 0.0; ER = 0.0; }
-    else           { rR = jmax(rR, 1e-30); }
-
-    double m2L = sq(mnL) + sq(mt1L) + sq(mt2L);
-    if (m2L > sq(rL) * 1e4) {
-        double s = rL * 100.0 / std::sqrt(m2L);
-        mnL *= s; mt1L *= s; mt2L *= s;
-    }
-    double m2R = sq(mnR) + sq(mt1R) + sq(mt2R);
-    if (m2R > sq(rR) * 1e4) {
-        double s = rR * 100.0 / std::sqrt(m2R);
-        mnR *= s; mt1R *= s; mt2R *= s;
-    }
-
-    double KE_L = jmin(0.5 * (sq(mnL) + sq(mt1L) + sq(mt2L)) / rL, 0.5 * rL * 1e4);
-    double KE_R = jmin(0.5 * (sq(mnR) + sq(mt1R) + sq(mt2R)) / rR, 0.5 * rR * 1e4);
-    EL = jmax(EL, KE_L);
-    ER = jmax(ER, KE_R);
-
-    double vnL = mnL / rL, vt1L = mt1L / rL, vt2L = mt2L / rL;
-    double vnR = mnR / rR, vt1R = mt1R / rR, vt2R = mt2R / rR;
-
-    double pL = (g - 1.0) * (EL - KE_L);
-    double pR = (g - 1.0) * (ER - KE_R);
-    double csL = std::sqrt(g * pL / rL);
-    double csR = std::sqrt(g * pR / rR);
-
-    double SL, SR;
-    if (pL > 0.0 && pR > 0.0) {
-        double r_avg = 0.5 * (rL + rR);
-        double cs_avg = 0.5 * (csL + csR);
-        double p_star = jmax(0.0, 0.5 * (pL + pR) - 0.5 * (vnR - vnL) * r_avg * cs_avg);
-        double qL = p_star > pL ? std::sqrt(1.0 + (g + 1.0) / (2.0 * g) * (p_star / pL - 1.0)) : 1.0;
-        double qR = p_star > pR ? std::sqrt(1.0 + (g + 1.0) / (2.0 * g) * (p_star / pR - 1.0)) : 1.0;
-        SL = vnL - csL * qL;
-        SR = vnR + csR * qR;
-    } else {
-        SL = jmin(vnL - csL, vnR - csR);
-        SR = jmax(vnL + csL, vnR + csR);
-    }
-
-    double denom = rL * (SL - vnL) - rR * (SR - vnR);
-    if (std::fabs(denom) < 1e-100) { F[0] = F[1] = F[2] = F[3] = F[4] = 0.0; return; }
-    double S_star = (pR - pL + rL * vnL * (SL - vnL) - rR * vnR * (SR - vnR)) / denom;
-
-    double FrL = mnL;
-    double FmnL = rL * sq(vnL) + pL;
-    double Fmt1L = mt1L * vnL;
-    double Fmt2L = mt2L * vnL;
-    double FEL = (EL + pL) * vnL;
-    if (SL >= 0.0) { F[0] = FrL; F[1] = FmnL; F[2] = Fmt1L; F[3] = Fmt2L; F[4] = FEL; return; }
-
-    double FrR = mnR;
-    double FmnR = rR * sq(vnR) + pR;
-    double Fmt1R = mt1R * vnR;
-    double Fmt2R = mt2R * vnR;
-    double FER = (ER + pR) * vnR;
-    if (SR <= 0.0) { F[0] = FrR; F[1] = FmnR; F[2] = Fmt1R; F[3] = Fmt2R; F[4] = FER; return; }
-
-    if (jmax(rL, rR) > 3.0 * jmin(rL, rR)) {
-        double inv_dS = 1.0 / (SR - SL);
-        F[0] = (SR * FrL - SL * FrR + SL * SR * (rR - rL)) * inv_dS;
-        F[1] = (SR * FmnL - SL * FmnR + SL * SR * (mnR - mnL)) * inv_dS;
-        F[2] = (SR * Fmt1L - SL * Fmt1R + SL * SR * (mt1R - mt1L)) * inv_dS;
-        F[3] = (SR * Fmt2L - SL * Fmt2R + SL * SR * (mt2R - mt2L)) * inv_dS;
-        F[4] = (SR * FEL - SL * FER + SL * SR * (ER - EL)) * inv_dS;
-        return;
-    }
-
-    if (S_star >= 0.0) {
-        double denom_L = rL * (SL - vnL);
-        double chi = denom_L / (SL - S_star);
-        double rsL = chi, mnsL = chi * S_star, mt1sL = chi * vt1L, mt2sL = chi * vt2L;
-        double EsL = std::fabs(denom_L) > 1e-100
-                         ? chi * (EL / rL + (S_star - vnL) * (S_star + pL / denom_L)) : 0.0;
-        F[0] = FrL + SL * (rsL - rL);
-        F[1] = FmnL + SL * (mnsL - mnL);
-        F[2] = Fmt1L + SL * (mt1sL - mt1L);
-        F[3] = Fmt2L + SL * (mt2sL - mt2L);
-        F[4] = FEL + SL * (EsL - EL);
-    } else {
-        double denom_R = rR * (SR - vnR);
-        double chi = denom_R / (SR - S_star);
-        double rsR = chi, mnsR = chi * S_star, mt1sR = chi * vt1R, mt2sR = chi * vt2R;
-        double EsR = std::fabs(denom_R) > 1e-100
-                         ? chi * (ER / rR + (S_star - vnR) * (S_star + pR / denom_R)) : 0.0;
-        F[0] = FrR + SR * (rsR - rR);
-        F[1] = FmnR + SR * (mnsR - mnR);
-        F[2] = Fmt1R + SR * (mt1sR - mt1R);
-        F[3] = Fmt2R + SR * (mt2sR - mt2R);
-        F[4] = FER + SR * (EsR - ER);
-    }
-}
-
-/* src/hllc.jl:176-208: x/y/z rotations */
-extern "C" void orc_hllc_flux(int dir, const double* L, const double* R, double g, double out[5]) {
-    double F[5];
-    if (dir == 0) {
-        hllc_normal(L[0], L[1], L[2], L[3], L[4], R[0], R[1], R[2], R[3], R[4], g, F);
-        out[0] = F[0]; out[1] = F[1]; out[2] = F[2]; out[3] = F[3]; out[4] = F[4];
-    } else if (dir == 1) {
-        hllc_normal(L[0], L[2], L[1], L[3], L[4], R[0], R[2], R[1], R[3], R[4], g, F);
-        out[0] = F[0]; out[1] = F[2]; out[2] = F[1]; out[3] = F[3]; out[4] = F[4];
-    } else {
-        hllc_normal(L[0], L[3], L[1], L[2], L[4], R[0], R[3], R[1], R[2], R[4], g, F);
-        out[0] = F[0]; out[1] = F[2]; out[2] = F[3]; out[3] = F[1]; out[4] = F[4];
-    }
-}
-
-/* ------------------------------------------------------------------------- */
-/* src/euler3d.jl:33-44 (x faces, then y, then z) */
-extern "C" void orc_fill_ghost_outflow(double* U, int nx, int ny, int nz) {
-    Idx I(nx, ny, nz);
-    const int ng = NG;
-    for (int k = 1; k <= I.nzt; ++k) for (int j = 1; j <= I.nyt; ++j) for (int q = 1; q <= 5; ++q) {
-        for (int i = 1; i <= ng; ++i) U[I(q, i, j, k)] = U[I(q, ng + 1, j, k)];
-        for (int i = ng + nx + 1; i <= ng + nx + ng; ++i) U[I(q, i, j, k)] = U[I(q, ng + nx, j, k)];
-    }
-    for (int k = 1; k <= I.nzt; ++k) for (int i = 1; i <= I.nxt; ++i) for (int q = 1; q <= 5; ++q) {
-        for (int j = 1; j <= ng; ++j) U[I(q, i, j, k)] = U[I(q, i, ng + 1, k)];
-        for (int j = ng + ny + 1; j <= ng + ny + ng; ++j) U[I(q, i, j, k)] = U[I(q, i, ng + ny, k)];
-    }
-    for (int j = 1; j <= I.nyt; ++j) for (int i = 1; i <= I.nxt; ++i) for (int q = 1; q <= 5; ++q) {
-        for (int k = 1; k <= ng; ++k) U[I(q, i, j, k)] = U[I(q, i, j, ng + 1)];
-        for (int k = ng + nz + 1; k <= ng + nz + ng; ++k) U[I(q, i, j, k)] = U[I(q, i, j, ng + nz)];
-    }
-}
-
-/* src/euler3d.jl:51-62 */
-extern "C" void orc_fill_ghost_periodic(double* U, int nx, int ny, int nz) {
-    Idx I(nx, ny, nz);
-    const int ng = NG;
-    for (int k = 1; k <= I.nzt; ++k) for (int j = 1; j <= I.nyt; ++j) for (int q = 1; q <= 5; ++q) {
-        for (int t = 0; t < ng; ++t) U[I(q, 1 + t, j, k)] = U[I(q, nx + 1 + t, j, k)];
-        for (int t = 0; t < ng; ++t) U[I(q, ng + nx + 1 + t, j, k)] = U[I(q, ng + 1 + t, j, k)];
-    }
-    for (int k = 1; k <= I.nzt; ++k) for (int i = 1; i <= I.nxt; ++i) for (int q = 1; q <= 5; ++q) {
-        for (int t = 0; t < ng; ++t) U[I(q, i, 1 + t, k)] = U[I(q, i, ny + 1 + t, k)];
-        for (int t = 0; t < ng; ++t) U[I(q, i, ng + ny + 1 + t, k)] = U[I(q, i, ng + 1 + t, k)];
-    }
-    for (int j = 1; j <= I.nyt; ++j) for (int i = 1; i <= I.nxt; ++i) for (int q = 1; q <= 5; ++q) {
-        for (int t = 0; t < ng; ++t) U[I(q, i, j, 1 + t)] = U[I(q, i, j, nz + 1 + t)];
-        for (int t = 0; t < ng; ++t) U[I(q, i, j, ng + nz + 1 + t)] = U[I(q, i, j, ng + 1 + t)];
-    }
-}
-
-/* src/gpu_kernels.jl:26-46 via src/euler3d.jl:73-80 */
-extern "C" void orc_apply_floors(double* U, int nx, int ny, int nz, double rho_floor, double P_floor,
-                                 double g) {
-    Idx I(nx, ny, nz);
-    const int ng = NG;
-#pragma omp parallel for schedule(static)
-    for (int kk = 1; kk <= nz; ++kk)
-        for (int jj = 1; jj <= ny; ++jj)
-            for (int ii = 1; ii <= nx; ++ii) {
-                int i = ii + ng, j = jj + ng, k = kk + ng;
-                double r = U[I(1, i, j, k)];
-                if (r < rho_floor) {
-                    U[I(1, i, j, k)] = rho_floor;
-                    U[I(2, i, j, k)] = 0.0;
-                    U[I(3, i, j, k)] = 0.0;
-                    U[I(4, i, j, k)] = 0.0;
-                    U[I(5, i, j, k)] = P_floor / (g - 1.0);
-                } else {
-                    double KE = 0.5 * (sq(U[I(2, i, j, k)]) + sq(U[I(3, i, j, k)]) + sq(U[I(4, i, j, k)])) / r;
-                    double P = (g - 1.0) * (U[I(5, i, j, k)] - KE);
-                    if (P < P_floor) U[I(5, i, j, k)] = P_floor / (g - 1.0) + KE;
-                }
-            }
-}
-
-/* src/euler3d.jl:86-90 */
-static inline double cell_pressure(double r, double mx, double my, double mz, double E, double g) {
-    r = jmax(r, 1e-30);
-    double KE = 0.5 * (sq(mx) + sq(my) + sq(mz)) / r;
-    return jmax((g - 1.0) * (E - KE), 0.0);
-}
-/* src/euler3d.jl:99-106 */
-static inline double EL_from_P(double PL, double rL, double mxL, double myL, double mzL, double g) {
-    double r_pos = jmax(rL, 1e-30);
-    double m2 = sq(mxL) + sq(myL) + sq(mzL);
-    double KE_raw = 0.5 * m2 / r_pos;
-    double KE = jmin(KE_raw, 0.5 * r_pos * 1e4);
-    return PL / (g - 1.0) + KE;
-}
-
-/* src/gpu_kernels.jl:51-154: one interface.  c[s][q] = U[q, cell s] for the
- * six cells i-2..i+3 along the sweep direction. */
-static inline void interface_flux(int dir, const double c[6][5], double g, double out[5]) {
-    double L[5], R[5];
-    for (int q = 0; q < 4; ++q) {
-        L[q] = orc_weno5_left(c[0][q], c[1][q], c[2][q], c[3][q], c[4][q]);
-        R[q] = orc_weno5_right(c[1][q], c[2][q], c[3][q], c[4][q], c[5][q]);
-    }
-    double p[6];
-    for (int s = 0; s < 6; ++s) p[s] = cell_pressure(c[s][0], c[s][1], c[s][2], c[s][3], c[s][4], g);
-    double PmaxL = jmax(jmax(jmax(jmax(p[0], p[1]), p[2]), p[3]), p[4]);
-    double PmaxR = jmax(jmax(jmax(jmax(p[1], p[2]), p[3]), p[4]), p[5]);
-    double PL = jclamp(orc_weno5_left(p[0], p[1], p[2], p[3], p[4]), 0.0, PmaxL);
-    double PR = jclamp(orc_weno5_right(p[1], p[2], p[3], p[4], p[5]), 0.0, PmaxR);
-    L[4] = EL_from_P(PL, L[0], L[1], L[2], L[3], g);
-    R[4] = EL_from_P(PR, R[0], R[1], R[2], R[3], g);
-    orc_hllc_flux(dir, L, R, g, out);
-}
-
-/* src/gpu_kernels.jl:51-154 via src/euler3d.jl:109-130.  F has the reference
- * shape for the given direction; only interfaces are written. */
-extern "C" void orc_weno_fluxes(int dir, double* F, const double* U, int nx, int ny, int nz, double g) {
-    Idx I(nx, ny, nz);
-    const int ng = NG;
-    FIdx FI(I.nxt + (dir == 0), I.nyt + (dir == 1), I.nzt + (dir == 2));
-    int ex = nx + (dir == 0), ey = ny + (dir == 1), ez = nz + (dir == 2);
-#pragma omp parallel for schedule(static)
-    for (int kk = 1; kk <= ez; ++kk)
-        for (int jj = 1; jj <= ey; ++jj)
-            for (int ii = 1; ii <= ex; ++ii) {
-                int i = ii + ng - (dir == 0), j = jj + ng - (dir == 1), k = kk + ng - (dir == 2);
-                double c[6][5];
-                for (int s = 0; s < 6; ++s) {
-                    int o = s - 2;
-                    int ci = i + (dir == 0 ? o : 0), cj = j + (dir == 1 ? o : 0), ck = k + (dir == 2 ? o : 0);
-                    for (int q = 0; q < 5; ++q) c[s][q] = U[I(q + 1, ci, cj, ck)];
-                }
-                double out[5];
-                interface_flux(dir, c, g, out);
-                for (int q = 0; q < 5; ++q) F[FI(q + 1, i, j, k)] = out[q];
-            }
-}
-
-/* src/gpu_kernels.jl:159-169 via src/euler3d.jl:135-145 (dU zeroed first) */
-extern "C" void orc_flux_divergence(double* dU, const double* Fx, const double* Fy, const double* Fz,
-                                    int nx, int ny, int nz, double dx, double dy, double dz) {
-    Idx I(nx, ny, nz);
-    const int ng = NG;
-    FIdx X(I.nxt + 1, I.nyt, I.nzt), Y(I.nxt, I.nyt + 1, I.nzt), Z(I.nxt, I.nyt, I.nzt + 1);
-    std::memset(dU, 0, sizeof(double) * I.size());
-    double inv_dx = 1.0 / dx, inv_dy = 1.0 / dy, inv_dz = 1.0 / dz;
-#pragma omp parallel for schedule(static)
-    for (int kk = 1; kk <= nz; ++kk)
-        for (int jj = 1; jj <= ny; ++jj)
-            for (int ii = 1; ii <= nx; ++ii) {
-                int i = ii + ng, j = jj + ng, k = kk + ng;
-                for (int q = 1; q <= 5; ++q)
-                    dU[I(q, i, j, k)] = -(Fx[X(q, i, j, k)] - Fx[X(q, i - 1, j, k)]) * inv_dx -
-                                        (Fy[Y(q, i, j, k)] - Fy[Y(q, i, j - 1, k)]) * inv_dy -
-                                        (Fz[Z(q, i, j, k)] - Fz[Z(q, i, j, k - 1)]) * inv_dz;
-            }
-}
-
-/* src/gpu_kernels.jl:174-191 + src/euler3d.jl:157-169 */
-extern "C" double orc_cfl_dt_3d(const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
-                                double g, double cfl) {
-    Idx I(nx, ny, nz);
-    const int ng = NG;
-    double inv_dx = 1.0 / dx, inv_dy = 1.0 / dy, inv_dz = 1.0 / dz;
-    double smax = -INFINITY;
-    bool any_nan = false;
-    for (int kk = 1; kk <= nz; ++kk)
-        for (int jj = 1; jj <= ny; ++jj)
-            for (int ii = 1; ii <= nx; ++ii) {
-                int i = ii + ng, j = jj + ng, k = kk + ng;
-                double r = jmax(U[I(1, i, j, k)], 1e-30);
-                double vx = U[I(2, i, j, k)] / r, vy = U[I(3, i, j, k)] / r, vz = U[I(4, i, j, k)] / r;
-                double KE = 0.5 * (sq(vx) + sq(vy) + sq(vz));
-                double P = jmax((g - 1.0) * (U[I(5, i, j, k)] / r - KE) * r, 0.0);
-                double cs = std::sqrt(g * P / r);
-                double s = jmax(jmax((std::fabs(vx) + cs) * inv_dx, (std::fabs(vy) + cs) * inv_dy),
-                                (std::fabs(vz) + cs) * inv_dz);
-                if (s != s) any_nan = true;
-                smax = jmax(smax, s);
-            }
-    /* maximum() propagates NaN and `NaN > 0.0` is false, so the reference
-     * returns Inf for a state holding a NaN. */
-    if (any_nan) return INFINITY;
-    return smax > 0.0 ? cfl / smax : INFINITY;
-}
-
-/* src/euler3d.jl:182-205 */
-extern "C" void orc_euler3d_rhs(double* dU, double* Fx, double* Fy, double* Fz, double* U,
-                                int nx, int ny, int nz, double dx, double dy, double dz, double g,
-                                int bc, double rho_floor, double P_floor, int fill_ghosts) {
-    Idx I(nx, ny, nz);
-    if (fill_ghosts) {
-        if (bc == 1) orc_fill_ghost_periodic(U, nx, ny, nz);
-        else         orc_fill_ghost_outflow(U, nx, ny, nz);
-    }
-    orc_apply_floors(U, nx, ny, nz, rho_floor, P_floor, g);
-    std::memset(Fx, 0, sizeof(double) * 5L * (I.nxt + 1) * I.nyt * I.nzt);
-    std::memset(Fy, 0, sizeof(double) * 5L * I.nxt * (I.nyt + 1) * I.nzt);
-    std::memset(Fz, 0, sizeof(double) * 5L * I.nxt * I.nyt * (I.nzt + 1));
-    orc_weno_fluxes(0, Fx, U, nx, ny, nz, g);
-    orc_weno_fluxes(1, Fy, U, nx, ny, nz, g);
-    orc_weno_fluxes(2, Fz, U, nx, ny, nz, g);
-    orc_flux_divergence(dU, Fx, Fy, Fz, nx, ny, nz, dx, dy, dz);
-}
-
-namespace {
-struct StepScratch {
-    std::vector<double> Fx, Fy, Fz, dU, Un;
-    StepScratch(int nx, int ny, int nz) {
-        Idx I(nx, ny, nz);
-        Fx.resize(5L * (I.nxt + 1) * I.nyt * I.nzt);
-        Fy.resize(5L * I.nxt * (I.nyt + 1) * I.nzt);
-        Fz.resize(5L * I.nxt * I.nyt * (I.nzt + 1));
-        dU.resize(I.size());
-        Un.resize(I.size());
-    }
-};
-/* stage combines, src/euler3d.jl:244,250,256 (whole array incl. ghosts) */
-void combine1(double* U, const double* Un, const double* dU, double dt, long n) {
-#pragma omp parallel for schedule(static)
-    for (long t = 0; t < n; ++t) U[t] = Un[t] + dt * dU[t];
-}
-void combine2(double* U, const double* Un, const double* dU, double dt, long n) {
-#pragma omp parallel for schedule(static)
-    for (long t = 0; t < n; ++t) U[t] = 0.75 * Un[t] + 0.25 * U[t] + 0.25 * dt * dU[t];
-}
-void combine3(double* U, const double* Un, const double* dU, double dt, long n) {
-#pragma omp parallel for schedule(static)
-    for (long t = 0; t < n; ++t) U[t] = (1.0 / 3.0) * Un[t] + (2.0 / 3.0) * U[t] + (2.0 / 3.0) * dt * dU[t];
-}
-}  // namespace
-
-/* src/euler3d.jl:220-260 */
-extern "C" void orc_euler3d_step(double* U, int nx, int ny, int nz, double dx, double dy, double dz,
-                                 double dt, double g, int bc, double rho_floor, double P_floor) {
-    Idx I(nx, ny, nz);
-    StepScratch S(nx, ny, nz);
-    long n = I.size();
-    std::memcpy(S.Un.data(), U, sizeof(double) * n);
-    orc_euler3d_rhs(S.dU.data(), S.Fx.data(), S.Fy.data(), S.Fz.data(), U, nx, ny, nz, dx, dy, dz, g, bc,
-                    rho_floor, P_floor, 1);
-    combine1(U, S.Un.data(), S.dU.data(), dt, n);
-    orc_apply_floors(U, nx, ny, nz, rho_floor, P_floor, g);
-    orc_euler3d_rhs(S.dU.data(), S.Fx.data(), S.Fy.data(), S.Fz.data(), U, nx, ny, nz, dx, dy, dz, g, bc,
-                    rho_floor, P_floor, 1);
-    combine2(U, S.Un.data(), S.dU.data(), dt, n);
-    orc_apply_floors(U, nx, ny, nz, rho_floor, P_floor, g);
-    orc_euler3d_rhs(S.dU.data(), S.Fx.data(), S.Fy.data(), S.Fz.data(), U, nx, ny, nz, dx, dy, dz, g, bc,
-                    rho_floor, P_floor, 1);
-    combine3(U, S.Un.data(), S.dU.data(), dt, n);
-    orc_apply_floors(U, nx, ny, nz, rho_floor, P_floor, g);
-}
 
 /* src/euler3d.jl:275-316 */
 extern "C" void orc_sedov_ic_3d(double* U, int nx, int ny, int nz, double dx, double dy, double dz, double g,

@@ -191,6 +191,31 @@ def cfl_dt_3d(U, dx, dy, dz, gamma, cfl):
     return lib().orc_cfl_dt_3d(_p(U), *dims(U), dx, dy, dz, gamma, cfl)
 
 
+_flops_lib = None
+FLOP_KINDS = ("add", "mul", "div", "sqrt", "cmp")
+
+
+def count_step_flops(U, dx, dy, dz, dt, gamma, bc="outflow", rho_floor=0.0, P_floor=0.0) -> dict:
+    """euler3d_step! on U (in place, the oracle's arithmetic) through the
+    counting build (oracle/flops.cpp); returns the operations it took:
+    add (+ and -), mul, div, sqrt, cmp, one each, and their total."""
+    global _flops_lib
+    if _flops_lib is None:
+        path = os.path.join(_HERE, "build", "libbsn_oracle_flops.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        d, i = C.c_double, C.c_int
+        L.orc_count_step.restype = None
+        L.orc_count_step.argtypes = [_dp, i, i, i, d, d, d, d, d, i, d, d, C.c_ulonglong * 5]
+        _flops_lib = L
+    out = (C.c_ulonglong * 5)()
+    _flops_lib.orc_count_step(_p(U), *dims(U), dx, dy, dz, dt, gamma, BC[bc], rho_floor, P_floor, out)
+    r = dict(zip(FLOP_KINDS, (int(v) for v in out)))
+    r["total"] = sum(out)
+    return r
+
+
 def sedov_ic_3d(U, dx, dy, dz, gamma, E_blast=1.0, r_inject=None, rho_bg=1.0, P_floor=1e-5,
                 x_offset=0.0, y_offset=0.0, z_offset=0.0):
     lib().orc_sedov_ic_3d(_p(U), *dims(U), dx, dy, dz, gamma, E_blast,
