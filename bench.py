@@ -376,6 +376,40 @@ def binary_nested(bsn, torch, steps, warmup, log, n=128, paths=("f64", "f32", "l
     return out
 
 
+def poisson_solves(bsn, torch, peak_fp, hbm, log, n=128, reps=20):
+    """The isolated Poisson solve on an n^3 grid ((2n)^3 zero-padded; the
+    self-gravity solve of the FMR and binary-BH workloads), FP64 and FP32
+    transforms, against the standard R2C/C2R solve's figures: 3 passes x
+    read+write of (2n)^3/2 complex doubles plus the Green's function read,
+    and 5 M log2 M flops per complex transform of M = (2n)^3 points (half of
+    that for a real one; one forward and one inverse per solve)."""
+    M = (2 * n) ** 3
+    alg_bytes = 3 * 2 * M / 2 * 16 + (n + 1) ** 3 * 8
+    flops = 2 * 0.5 * 5 * M * math.log2(M)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    rho = bsn.active_grid(n, n, n)   # column-major (nx, ny, nz)
+    rho.copy_(torch.rand((n, n, n), device="cuda", dtype=torch.float64, generator=g) + 0.1)
+    out = {"workload": f"isolated Poisson solve {n}^3 ({2 * n}^3 padded)", "alg_bytes_per_solve": alg_bytes,
+           "flops_per_solve": flops}
+    for prec in ("f64", "f32"):
+        for _ in range(3):
+            bsn.solve_poisson_isolated(rho, n, n, n, 0.01, 0.01, 0.01, precision=prec)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            bsn.solve_poisson_isolated(rho, n, n, n, 0.01, 0.01, 0.01, precision=prec)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = alg_bytes / (ms / 1e3) / 1e9
+        tf = flops / (ms / 1e3) / 1e12
+        pk = peak_fp["f64"] if prec == "f64" else max(peak_fp["f32"], peak_fp["f32x2"])
+        out[prec] = {"ms_per_solve": ms, "GB/s": gbs, "hbm_frac": gbs / hbm, "TFLOP/s": tf, "fp_frac": tf / pk}
+        log(f"Poisson {n}^3 {prec}: {ms:.3f} ms per solve")
+    return out
+
+
 def coupled_binary(bsn, torch, steps, warmup, log, n=128):
     """Binary-BH supernova physics on a uniform grid: n=3 polytrope star
     (M=10, R=1, G=1, gamma 4/3) at the origin with a thermal bomb E=1 in
@@ -560,6 +594,7 @@ def run_bsn(args, rank, world):
     fmr = fmr_polytrope(bsn, torch, max(5, min(args.steps, 20)), args.warmup, log) if not args.no_fmr else None
     coupled = coupled_binary(bsn, torch, max(5, min(args.steps, 20)), args.warmup, log) if not args.no_fmr else None
     nested = binary_nested(bsn, torch, max(5, min(args.steps, 20)), args.warmup, log) if not args.no_fmr else None
+    poisson = poisson_solves(bsn, torch, peak_fp, hbm, log) if not args.no_fmr else None
 
     # e2e: host-buffer path -- pinned host state -> device, one CFL-limited
     # RK3 step through the public entry point, device -> host, every step
@@ -622,6 +657,7 @@ def run_bsn(args, rank, world):
             "fmr": fmr,
             "coupled": coupled,
             "coupled_nested": nested,
+            "poisson": poisson,
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_kind": hbm_kind,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "traffic_note": "DRAM read+write of one stage-1 launch, ncu at 128^3 scaled by cells",

@@ -235,9 +235,10 @@ __global__ void adam_kernel(float* P, float* grad, float* m, float* v, float sca
 // ---------------------------------------------------------------------------
 // BF16 tensor-core inference.  Packed parameters (per side), in the order the
 // MMA fragments of lane (g, tg) = (lane / 4, lane % 4) read them, so that each
-// lane loads a fragment set with one 16-byte shared-memory load:
+// lane loads a fragment set with one 16-byte shared-memory load and the 32
+// lanes of a load read consecutive 16-byte words (no bank conflicts):
 //   F1[lane][j]      layer-1 B fragment of output block j (m16n8k8: one word)
-//   F2[lane][j][i]   layer-2 B fragments of block j, i = (k-step, half)
+//   F2[j][lane][i]   layer-2 B fragments of block j, i = (k-step, half)
 //   F3[lane][i]      layer-3 B fragments, i = (k-step, half)
 //   FB1[tg][j][h], FB2[tg][j][h], FB3[tg][h]   the lane's bias pairs (FP32)
 // A word holds two BF16 values (the lower k in the low half); rows are output
@@ -272,7 +273,7 @@ __global__ void pack_kernel(const float* P, unsigned char* out) {
         F1[i] = pack2(w1_at(P, n, 2 * tg), w1_at(P, n, 2 * tg + 1));
     }
     if (i < 32 * 16) {
-        const int lane = i / 16, j = (i / 4) % 4, q = i % 4, g = lane / 4, tg = lane % 4, n = 8 * j + g;
+        const int j = i / 128, lane = (i / 4) % 32, q = i % 4, g = lane / 4, tg = lane % 4, n = 8 * j + g;
         const int w = tg + 4 * q;
         F2[i] = pack2(w2_at(P, n, 2 * w), w2_at(P, n, 2 * w + 1));
     }
@@ -299,19 +300,25 @@ __device__ __forceinline__ uint32_t pack2_relu(float lo, float hi) {
     return d;
 }
 
+// D = A B + C (m16n8k16, BF16 in, FP32 accumulate); C may be other registers
+// than D (a bias as the initial accumulator without copying it first)
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1, float c0,
+                                         float c1, float c2, float c3) {
+    asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%10,%11,%12,%13};\n"
+        : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1), "f"(c0), "f"(c1), "f"(c2), "f"(c3));
+}
 __device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    mma16816(c, a, b0, b1, c[0], c[1], c[2], c[3]);
 }
 
-__device__ __forceinline__ void mma1688(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a0), "r"(a1), "r"(b0));
+// D = A B + C (m16n8k8)
+__device__ __forceinline__ void mma1688(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0, float c0, float c1,
+                                        float c2, float c3) {
+    asm("mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%7,%8,%9,%10};\n"
+        : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+        : "r"(a0), "r"(a1), "r"(b0), "f"(c0), "f"(c1), "f"(c2), "f"(c3));
 }
 
 // Warp-collective MLP over `ntiles` tiles of 16 rows.  rows: BF16 inputs,
@@ -322,7 +329,7 @@ __device__ __forceinline__ void mma1688(float (&c)[4], uint32_t a0, uint32_t a1,
 __device__ __noinline__ void mlp_tiles(const unsigned char* pk, const uint32_t* rows, float* out, int ntiles) {
     const int lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
     const uint4* F1 = (const uint4*)(pk + PK_F1) + lane;          // words j = 0..3
-    const uint4* F2 = (const uint4*)(pk + PK_F2) + 4 * lane;      // per j: (k-step 0: lo, hi, k-step 1: lo, hi)
+    const uint4* F2 = (const uint4*)(pk + PK_F2) + lane;          // F2[32 j]: (k-step 0: lo, hi, k-step 1: lo, hi)
     const uint4* F3 = (const uint4*)(pk + PK_F3) + lane;
     const float4* B1 = (const float4*)(pk + PK_B1) + 2 * tg;      // (j, h) pairs, j = 0..3
     const float4* B2 = (const float4*)(pk + PK_B2) + 2 * tg;
@@ -338,11 +345,7 @@ __device__ __noinline__ void mlp_tiles(const unsigned char* pk, const uint32_t* 
         const uint32_t w1s[4] = {w1.x, w1.y, w1.z, w1.w};
         float h[4][4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const float c0 = b1[2 * j], c1 = b1[2 * j + 1];
-            h[j][0] = c0; h[j][1] = c1; h[j][2] = c0; h[j][3] = c1;
-            mma1688(h[j], a0, a1, w1s[j]);
-        }
+        for (int j = 0; j < 4; ++j) mma1688(h[j], a0, a1, w1s[j], b1[2 * j], b1[2 * j + 1], b1[2 * j], b1[2 * j + 1]);
         // ReLU, BF16 and the A fragments of the next layer in one instruction per pair
         uint32_t a2[2][4];
 #pragma unroll
@@ -357,10 +360,8 @@ __device__ __noinline__ void mlp_tiles(const unsigned char* pk, const uint32_t* 
         const float b2[8] = {b2a.x, b2a.y, b2a.z, b2a.w, b2b.x, b2b.y, b2b.z, b2b.w};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const uint4 w2 = F2[j];
-            const float c0 = b2[2 * j], c1 = b2[2 * j + 1];
-            h[j][0] = c0; h[j][1] = c1; h[j][2] = c0; h[j][3] = c1;
-            mma16816(h[j], a2[0], w2.x, w2.y);
+            const uint4 w2 = F2[32 * j];
+            mma16816(h[j], a2[0], w2.x, w2.y, b2[2 * j], b2[2 * j + 1], b2[2 * j], b2[2 * j + 1]);
             mma16816(h[j], a2[1], w2.z, w2.w);
         }
 #pragma unroll
@@ -373,8 +374,8 @@ __device__ __noinline__ void mlp_tiles(const unsigned char* pk, const uint32_t* 
         // layer 3: 32 -> 8 (3 used)
         const uint4 w3 = *F3;
         const float2 b3 = *B3;
-        float o[4] = {b3.x, b3.y, b3.x, b3.y};
-        mma16816(o, a2[0], w3.x, w3.y);
+        float o[4];
+        mma16816(o, a2[0], w3.x, w3.y, b3.x, b3.y, b3.x, b3.y);
         mma16816(o, a2[1], w3.z, w3.w);
         __syncwarp();
         if (tg == 0) {
