@@ -29,6 +29,11 @@ static bsn_status launch_batch_variant(bsn_ctx* ctx, int prec, int idx, const f6
 static bool prec_ok(int p) { return p == PREC_F64 || p == PREC_F32 || p == PREC_LEARNED; }
 
 bsn_status stage_autotune(bsn_ctx* ctx, int prec, const f64::StageArgs& probe, double* scratch) {
+    if (prec == PREC_LEARNED) {   // the split learned stage's block list, allocated before any capture
+        bsn_status st;
+        slot(ctx, SLOT_SPLIT, learned_split_bytes(probe.nx, probe.ny, probe.nz), &st);
+        BSN_TRY(st);
+    }
     auto key = std::make_tuple(prec, probe.nx, probe.ny, probe.nz);
     if (ctx->tile_choice.count(key)) return BSN_OK;
     int nv = variant_count(prec);

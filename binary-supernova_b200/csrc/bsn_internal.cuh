@@ -51,6 +51,7 @@ enum Slot {
     SLOT_A = 0, SLOT_B, SLOT_UN, SLOT_RED, SLOT_FFT0, SLOT_FFT1, SLOT_PHI, SLOT_RHO,
     SLOT_FMR_UCN, SLOT_FMR_UCNP1, SLOT_FMR_GH, SLOT_FMR_FA, SLOT_FMR_FB, SLOT_FMR_REG,
     SLOT_FMR_BF, SLOT_PHI2, SLOT_RUN, SLOT_FMR_RUN, SLOT_CRUN, SLOT_CRED, SLOT_DIAG, SLOT_DIAGREC, SLOT_RELAX,
+    SLOT_SPLIT,
     SLOT_COUNT
 };
 

@@ -12,12 +12,14 @@
 // stencil kernel.  Built with the fast-path flags (FMA, approximate div/sqrt).
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
 #include "hydro_f64.cuh"
 #include "learned.cuh"
 #include "physics_f32.cuh"
+#include "stage_f32.cuh"
 #include "stage_launch.cuh"
 #include "stage_tile.cuh"
 
@@ -465,6 +467,7 @@ struct F32Learned {
     // spread thresholds of the first one cannot hold a network row (every
     // stencil spread is at most twice that): its faces skip the fallback test.
     static constexpr bool kQuiescentSkip = true;
+    static constexpr bool kScreen = false;
     __device__ static bool same(float v, float ref) {
         return fabsf(v - ref) <= fmaxf(0.25f * learned::SPREAD_ABS, 0.125f * learned::SPREAD_REL_F32 * fabsf(ref));
     }
@@ -694,31 +697,72 @@ struct F32Learned {
     }
 };
 
+// The screening launch of the learned stage: the FP32 path's plain stencils
+// for every block whose three sweeps are uniform by F32Learned's test (no
+// network row can occur there, so the learned stage computes the same
+// fluxes), listing the other blocks for the learned launch.
+struct F32Screen : F32Physics {
+    static constexpr bool kQuiescentSkip = true;
+    static constexpr bool kScreen = true;
+    __device__ static bool same(float v, float ref) { return F32Learned::same(v, ref); }
+};
+
 }  // namespace tile
 
 namespace {
 const TileVariant kLearnedVariants[] = {{8, 8, 8, 256, 2}, {16, 8, 4, 256, 2}, {8, 8, 8, 256, 3}, {8, 8, 4, 128, 6},
                                         {16, 16, 4, 256, 2}, {16, 8, 8, 256, 2}};
 
+// One learned stage as two launches on the context's stream: the screening
+// launch over every block, then the learned launch over the blocks it listed
+// (a persistent grid); 95-97 % of the Sedov blocks take the first.
 template <int TX, int TY, int TZ, int NT, int MINB>
-bsn_status launch_learned(bsn_ctx* ctx, const f64::StageArgs& A) {
-    auto fn = tile::stage_kernel<tile::F32Learned, TX, TY, TZ, NT, MINB>;
-    constexpr int smem = tile::smem_bytes<tile::F32Learned, TX, TY, TZ>() + tile::F32Learned::kExtraSmem(NT) + 16;
-    static bool attr_done[64] = {false};
+bsn_status launch_learned(bsn_ctx* ctx, const f64::StageArgs& A0) {
+    auto fs = tile::stage_kernel<tile::F32Screen, TX, TY, TZ, NT, MINB>;
+    auto fl = tile::stage_kernel_list<tile::F32Learned, TX, TY, TZ, NT, MINB>;
+    constexpr int smem_s = tile::smem_bytes<tile::F32Screen, TX, TY, TZ>();
+    constexpr int smem_l = tile::smem_bytes<tile::F32Learned, TX, TY, TZ>() + tile::F32Learned::kExtraSmem(NT) + 16;
+    static int occ[64] = {0}, sms[64] = {0};
     int dev = ctx->device & 63;
-    if (!attr_done[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (!occ[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(fs, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_s);
+        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaFuncSetAttribute(stage_kernel_learned_screen)");
+        e = cudaFuncSetAttribute(fl, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_l);
         if (e != cudaSuccess) return cuda_check(ctx, e, "cudaFuncSetAttribute(stage_kernel_learned)");
-        attr_done[dev] = true;
+        int o = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fl, NT, smem_l);
+        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, ctx->device);
+        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaDeviceGetAttribute");
+        occ[dev] = o < 1 ? 1 : o;
     }
-    dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + TZ - 1) / TZ);
+    dim3 grid((A0.nx + TX - 1) / TX, (A0.ny + TY - 1) / TY, (A0.nz + TZ - 1) / TZ);
+    const long long nblk = (long long)grid.x * grid.y * grid.z;
+    bsn_status st;
+    // sized for every variant before any graph capture (stage_autotune), so this never allocates while capturing
+    unsigned int* cnt = (unsigned int*)slot(ctx, SLOT_SPLIT, learned_split_bytes(A0.nx, A0.ny, A0.nz), &st);
+    BSN_TRY(st);
+    f64::StageArgs A = A0;
+    A.split_count = cnt;
+    A.split_list = (int*)(cnt + 4);
+    BSN_CUDA(ctx, cudaMemsetAsync(cnt, 0, sizeof(unsigned int), ctx->stream));
     prof_begin(ctx);
-    fn<<<grid, NT, smem, ctx->stream>>>(A);
+    fs<<<grid, NT, smem_s, ctx->stream>>>(A);
+    BSN_TRY(launch_check(ctx, "stage_kernel_learned_screen"));
+    const long long pgrid = std::min<long long>(nblk, (long long)occ[dev] * sms[dev]);
+    prof_begin(ctx);
+    fl<<<(unsigned)pgrid, NT, smem_l, ctx->stream>>>(A);
     return launch_check(ctx, "stage_kernel_learned");
 }
 }  // namespace
 
 int learned_variant_count() { return (int)(sizeof(kLearnedVariants) / sizeof(kLearnedVariants[0])); }
+size_t learned_split_bytes(int nx, int ny, int nz) {
+    long long mx = 0;
+    for (const TileVariant& t : kLearnedVariants)
+        mx = std::max(mx, (long long)((nx + t.tx - 1) / t.tx) * ((ny + t.ty - 1) / t.ty) * ((nz + t.tz - 1) / t.tz));
+    return 16 + sizeof(int) * (size_t)mx;
+}
 TileVariant learned_variant(int idx) { return kLearnedVariants[idx]; }
 bsn_status learned_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A0) {
     learned::State* S = (learned::State*)ctx->learned_state;

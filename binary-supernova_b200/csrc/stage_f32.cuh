@@ -1,0 +1,46 @@
+// stage_f32.cuh -- the FP32-stencil physics policy of the fused stage kernel
+// (the fast path): FP32 staging, WENO5-Z, pressures and HLLC; FP64 state,
+// floors, divergence, sources, RK3 combine and CFL.  Included by the
+// translation units built with the fast-path flags (stage_fast.cu, and
+// learned.cu for the screening launch of the learned stage).
+#pragma once
+
+#include "physics_f32.cuh"
+#include "stage_tile.cuh"
+
+namespace bsn {
+namespace tile {
+
+struct F32Physics {
+    using real = float;
+    static constexpr bool kCross = true;
+    static constexpr int kCols = 5;                  // rho, m, P: the epilogue reloads the FP64 state
+    static constexpr bool kCenterFromSmem = false;  // smem holds FP32 copies: reload FP64 state
+    static constexpr bool kWarpFaces = false;
+    static constexpr bool kQuiescentSkip = false;
+    static constexpr bool kScreen = false;
+    __device__ static bool same(float, float) { return true; }
+    static constexpr int kExtraSmem(int) { return 0; }
+    __device__ static void prologue(unsigned char*, const f64::StageArgs&, int) {}
+    struct Consts { float g, gm1, inv_gm1, gg; };
+    __device__ static Consts consts(const f64::StageArgs& A) {
+        float g = (float)A.g;
+        return {g, (float)A.gm1, 1.0f / (float)A.gm1, (g + 1.0f) / (2.0f * g)};
+    }
+    __device__ static float pressure(const float v[5], const Consts& k) {
+        return f32::cell_pressure(v[0], v[1], v[2], v[3], v[4], k.gm1);
+    }
+    __device__ static void floor(double (&v)[5], const f64::StageArgs& A) {
+        f32::floor_screened(v, A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+    }
+    __device__ static void stage(double (&v)[5], bool act, const f64::StageArgs& A, float (&w)[5]) {
+        f32::stage_floored(v, act, A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1, w);
+    }
+    template <int D>
+    __device__ static void flux(const float (&c)[6][6], const Consts& k, float F[5]) {
+        f32::interface_flux<D>(c, k.g, k.gm1, k.inv_gm1, k.gg, F);
+    }
+};
+
+}  // namespace tile
+}  // namespace bsn

@@ -62,6 +62,11 @@ struct StageArgs {
     const double* dt_dev;    // non-null: dt read on the device (graph-captured time loop)
     const int* done_dev;     // non-null and *done_dev != 0: the device time loop has finished
     const void* mlp;         // learned stencil path: packed network parameters
+    // learned stage split in two launches: the screening launch (plain FP32
+    // stencils) does every block whose three sweeps are uniform and lists the
+    // others here; the learned launch then does the listed blocks
+    int* split_list;              // block index bx + gx (by + gy bz)
+    unsigned int* split_count;
     const BHSrc* bh_dev;     // non-null: gravity sources read on the device (device-resident driver loop)
     const SinkSrc* sk_dev;   // non-null: sink sources read on the device
     // relaxation sources (src/relax_ic.jl): rotating frame at rot_omega,

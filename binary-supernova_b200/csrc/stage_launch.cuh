@@ -12,6 +12,10 @@ struct TileVariant {
     int tx, ty, tz, nt, minb;   // block tile, threads per CTA, min CTAs per SM (register cap)
 };
 
+// Bytes of the split learned stage's block list (count + one index per
+// block) for the tile variant with the most blocks on an nx x ny x nz grid.
+size_t learned_split_bytes(int nx, int ny, int nz);
+
 // per-precision variant tables (hydro_f64.cu: FP64, stage_fast.cu: FP32)
 int f64_variant_count();
 TileVariant f64_variant(int idx);

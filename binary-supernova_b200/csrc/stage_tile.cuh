@@ -50,6 +50,7 @@ struct F64Physics {
     static constexpr int kCols = 6;                 // staged columns: rho, m, E (read back by the epilogue), P
     static constexpr bool kWarpFaces = false;       // faces computed thread by thread
     static constexpr bool kQuiescentSkip = false;
+    static constexpr bool kScreen = false;          // screening launch of a split stage
     __device__ static bool same(double, double) { return true; }
     static constexpr int kExtraSmem(int) { return 0; }
     __device__ static void prologue(unsigned char*, const f64::StageArgs&, int) {}
@@ -392,6 +393,18 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
         quiet[0] = !(vb || vx);
         quiet[1] = !(vb || vy);
         quiet[2] = !(vb || vz);
+        if constexpr (P::kScreen) {
+            // a block with a non-uniform sweep is left to the split stage's
+            // other launch: listed, nothing written here (the test is uniform
+            // over the CTA, so every thread returns)
+            if (!(quiet[0] && quiet[1] && quiet[2])) {
+                if (tid == 0) {
+                    const int gx = (A.nx + TX - 1) / TX, gy = (A.ny + TY - 1) / TY;
+                    A.split_list[atomicAdd(A.split_count, 1u)] = a0 / TX + gx * (b0 / TY + gy * (c0 / TZ));
+                }
+                return;
+            }
+        }
     }
     sweep<P, TX, TY, TZ, NT, 0>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[0]);
     sweep<P, TX, TY, TZ, NT, 1>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[1]);
@@ -530,6 +543,25 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
     if (A.done_dev && *A.done_dev) return;   // device time loop already reached t_end
     P::prologue(policy_smem<P, TX, TY, TZ>(smem_raw), A, NT);   // visible after the first barrier
     stage_block<P, TX, TY, TZ, NT>(A, blockIdx.x * TX, blockIdx.y * TY, blockIdx.z * TZ, smem_raw, red, nanflag);
+}
+
+// The listed blocks of a split stage (written by its screening launch, which
+// runs first on the same stream), walked by a persistent grid.
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel_list(const __grid_constant__ f64::StageArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[NT / 32];
+    __shared__ unsigned int nanflag;
+    if (A.done_dev && *A.done_dev) return;
+    const int n = (int)*A.split_count;
+    if ((int)blockIdx.x >= n) return;
+    P::prologue(policy_smem<P, TX, TY, TZ>(smem_raw), A, NT);   // visible after the first barrier
+    const int gx = (A.nx + TX - 1) / TX, gy = (A.ny + TY - 1) / TY;
+    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+        const int b = A.split_list[t];
+        stage_block<P, TX, TY, TZ, NT>(A, (b % gx) * TX, ((b / gx) % gy) * TY, (b / (gx * gy)) * TZ, smem_raw, red,
+                                       nanflag);
+    }
 }
 
 // Several grids (mesh levels or patches of any size) in one launch: their
