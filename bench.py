@@ -579,9 +579,9 @@ def run_bsn(args, rank, world):
     bsn.set_profiling(False)
     t_stage = tot / max(cnt, 1) / 1e3
     alg_bytes = 40 * 8 * ncell / 3.0     # 40 FP64 state words per cell per RK3 step, 3 stage launches
-    # DRAM bytes of one stage-1 launch from an ncu capture at 128^3 (t = 0.025), scaled by the
-    # cell count (profiles/stage_kernel_*_sedov128_ncu.md); None where no capture exists
-    traffic_128 = {"learned": 141.6e6, "f32": 133.7e6, "f64": 133.1e6}.get(prec)
+    # DRAM bytes of one stage-1 launch (learned: its screening and learned launches) from an ncu
+    # capture at 128^3 (t = 0.025), scaled by the cell count (profiles/stage_kernel_*_sedov128_ncu.md)
+    traffic_128 = {"learned": 134.1e6, "f32": 133.7e6, "f64": 133.1e6}.get(prec)
     traffic = traffic_128 * ncell / 128 ** 3 if traffic_128 else None
     hbm, hbm_kind = peaks()
     achieved = alg_bytes / t_stage / 1e9
