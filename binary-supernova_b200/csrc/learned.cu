@@ -713,11 +713,32 @@ namespace {
 const TileVariant kLearnedVariants[] = {{8, 8, 8, 256, 2}, {16, 8, 4, 256, 2}, {8, 8, 8, 256, 3}, {8, 8, 4, 128, 6},
                                         {16, 16, 4, 256, 2}, {16, 8, 8, 256, 2}};
 
+// One learned stage over every block in one launch (FMR levels and the
+// coupled loops, whose grids are mostly non-uniform).
+template <int TX, int TY, int TZ, int NT, int MINB>
+bsn_status launch_learned_whole(bsn_ctx* ctx, const f64::StageArgs& A) {
+    auto fn = tile::stage_kernel<tile::F32Learned, TX, TY, TZ, NT, MINB>;
+    constexpr int smem = tile::smem_bytes<tile::F32Learned, TX, TY, TZ>() + tile::F32Learned::kExtraSmem(NT) + 16;
+    static bool attr_done[64] = {false};
+    int dev = ctx->device & 63;
+    if (!attr_done[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaFuncSetAttribute(stage_kernel_learned)");
+        attr_done[dev] = true;
+    }
+    dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + TZ - 1) / TZ);
+    prof_begin(ctx);
+    fn<<<grid, NT, smem, ctx->stream>>>(A);
+    return launch_check(ctx, "stage_kernel_learned");
+}
+
 // One learned stage as two launches on the context's stream: the screening
 // launch over every block, then the learned launch over the blocks it listed
-// (a persistent grid); 95-97 % of the Sedov blocks take the first.
+// (a persistent grid); 95-97 % of the Sedov blocks take the first.  Used where
+// the caller asks for it (A.learned_split: the uniform-grid entry points).
 template <int TX, int TY, int TZ, int NT, int MINB>
 bsn_status launch_learned(bsn_ctx* ctx, const f64::StageArgs& A0) {
+    if (!A0.learned_split) return launch_learned_whole<TX, TY, TZ, NT, MINB>(ctx, A0);
     auto fs = tile::stage_kernel<tile::F32Screen, TX, TY, TZ, NT, MINB>;
     auto fl = tile::stage_kernel_list<tile::F32Learned, TX, TY, TZ, NT, MINB>;
     constexpr int smem_s = tile::smem_bytes<tile::F32Screen, TX, TY, TZ>();

@@ -171,6 +171,7 @@ extern "C" bsn_status bsn_euler3d_step_learned(bsn_ctx* ctx, double* U, int nx, 
     BSN_TRY(check_step_args(ctx, U, nx, ny, nz, bc, PREC_LEARNED));
     f64::StageArgs A;
     stage_args_init(A, nx, ny, nz, dx, dy, dz, gamma, bc, rho_floor, P_floor);
+    A.learned_split = 1;
     return rk3_prec(ctx, A, U, dt, PREC_LEARNED);
 }
 
@@ -191,6 +192,7 @@ extern "C" bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int
     f64::StageArgs base;
     stage_args_init(base, nx, ny, nz, dx, dy, dz, gamma, bc, rho_floor, P_floor);
     base.Uin = U; base.Un = U;
+    base.learned_split = 1;   // a uniform grid: mostly uniform blocks away from the flow's features
     // autotune before any capture (it launches and times kernels)
     {
         double* scratch = (double*)slot(ctx, SLOT_UN, bytes, &st); BSN_TRY(st);

@@ -65,6 +65,7 @@ struct StageArgs {
     // learned stage split in two launches: the screening launch (plain FP32
     // stencils) does every block whose three sweeps are uniform and lists the
     // others here; the learned launch then does the listed blocks
+    int learned_split;            // learned stages split (uniform-grid entry points; off elsewhere)
     int* split_list;              // block index bx + gx (by + gy bz)
     unsigned int* split_count;
     const BHSrc* bh_dev;     // non-null: gravity sources read on the device (device-resident driver loop)
