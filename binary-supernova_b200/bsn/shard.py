@@ -251,6 +251,55 @@ def poisson_isolated(rho, slab: Slab, dx, dy, dz, ops, group=None):
     return P.inverse(recv)
 
 
+def _phi_neighbours(phi, slab: Slab, group):
+    """The plane of Phi next to this slab on each side ((Y, X) tensors; None
+    at the global z boundaries: the isolated solve does not wrap)."""
+    if slab.world == 1:
+        return None, None
+    import torch.distributed as dist
+    P = phi.permute(2, 1, 0)   # (Z, Y, X) view of the column-major (nx, ny, nzl) array
+    lo = slab.rank - 1 if slab.rank > 0 else None
+    hi = slab.rank + 1 if slab.rank < slab.world - 1 else None
+    ops_list, got = [], {}
+    if hi is not None:
+        ops_list.append(dist.P2POp(dist.isend, P[-1].contiguous(), hi, group, tag=2))
+        got["hi"] = torch.empty_like(P[0].contiguous())
+        ops_list.append(dist.P2POp(dist.irecv, got["hi"], hi, group, tag=3))
+    if lo is not None:
+        ops_list.append(dist.P2POp(dist.isend, P[0].contiguous(), lo, group, tag=3))
+        got["lo"] = torch.empty_like(P[0].contiguous())
+        ops_list.append(dist.P2POp(dist.irecv, got["lo"], lo, group, tag=2))
+    for req in dist.batch_isend_irecv(ops_list):
+        req.wait()
+    return got.get("lo"), got.get("hi")
+
+
+def sg_source(dU, U, phi, slab: Slab, dx, dy, dz, ops, lo=None, hi=None):
+    """The self-gravity source (src/self_gravity.jl:93-115 after the solve;
+    src/gpu_kernels.jl:291-319) on this slab's cells from its planes of Phi and
+    the neighbours' planes lo / hi (None at a global boundary, where the
+    reference's one-sided difference applies).  Computed on the slab extended
+    by those planes, so every cell takes the undivided grid's arithmetic."""
+    nx, ny, nz = slab.nx, slab.ny, slab.nz
+    a, b = (lo is not None), (hi is not None)
+    if not (a or b):
+        ops.sg_gradient(dU, U, phi, nx, ny, nz, dx, dy, dz)
+        return
+    nze = nz + a + b
+    Ue, dUe, phie = ops.extend(U, dU, phi, nx, ny, nz, a, b, lo, hi)
+    ops.sg_gradient(dUe, Ue, phie, nx, ny, nze, dx, dy, dz)
+    ops.assign(dU, ops.shrink(dUe, dU, nz, a))
+
+
+def add_self_gravity_source(dU, U, slab: Slab, dx, dy, dz, ops, group=None):
+    """add_self_gravity_source! (src/self_gravity.jl:93-115) of the global grid
+    on this rank's slab: Phi from the distributed solve of the slabs' active
+    densities, one plane of Phi from each neighbour, the source added to dU."""
+    phi = poisson_isolated(ops.active_rho(U, slab.nx, slab.ny, slab.nz), slab, dx, dy, dz, ops, group)
+    lo, hi = _phi_neighbours(phi, slab, group)
+    sg_source(dU, U, phi, slab, dx, dy, dz, ops, lo, hi)
+
+
 class DeviceOps:
     """The slab operations on CUDA tensors through this library's C ABI."""
 
@@ -292,6 +341,38 @@ class DeviceOps:
 
     def poisson_inverse(self, W2, nx, ny, nzl):
         return self.api.poisson_slab_inverse(W2, nx, ny, nzl)
+
+    def active_rho(self, U, nx, ny, nz):
+        rho = self.api.active_grid(nx, ny, nz, device=U.device)
+        rho.copy_(U[0, NG:NG + nx, NG:NG + ny, NG:NG + nz])
+        return rho
+
+    def sg_gradient(self, dU, U, phi, nx, ny, nz, dx, dy, dz):
+        self.api.apply_sg_force_level(dU, U, phi, nx, ny, nz, dx, dy, dz)
+
+    def extend(self, U, dU, phi, nx, ny, nz, a, b, lo, hi):
+        """U, dU and Phi of the slab with `a` plane(s) below and `b` above:
+        dU and U copied (U's ghost planes supply the extra cells' state, which
+        only feeds their own discarded source), Phi from the neighbours."""
+        nze = nz + a + b
+        Ue = self.api.state(nx, ny, nze, device=U.device)
+        dUe = self.api.state(nx, ny, nze, device=U.device)
+        _zmajor(Ue)[NG:NG + nze] = _zmajor(U)[NG - a:NG + nz + b]
+        _zmajor(dUe)[NG + a:NG + a + nz] = _zmajor(dU)[NG:NG + nz]
+        phie = self.api.active_grid(nx, ny, nze, device=U.device)
+        P = phie.permute(2, 1, 0)
+        if a:
+            P[0] = lo
+        P[a:a + nz] = phi.permute(2, 1, 0)
+        if b:
+            P[a + nz] = hi
+        return Ue, dUe, phie
+
+    @staticmethod
+    def shrink(dUe, dU, nz, a):
+        out = dU.clone()
+        _zmajor(out)[NG:NG + nz] = _zmajor(dUe)[NG + a:NG + a + nz]
+        return out
 
     def floor_planes(self, planes, nx, ny, rho_floor, P_floor, gamma):
         """apply_floors_3d! on the active (i, j) cells of NG received z-planes

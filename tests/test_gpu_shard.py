@@ -65,3 +65,39 @@ def test_slab_poisson_bitwise_to_the_undivided_solve(orc, world):
     phi = [P[r].inverse([lines[s][r] for s in range(world)]) for r in range(world)]
     got = torch.cat(phi, 2)
     assert torch.equal(got, ref)
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_slab_self_gravity_source_bitwise(orc, world):
+    """The self-gravity source on slabs (distributed Phi, one plane of Phi from
+    each neighbour, the gradient on the slab extended by those planes), ranks
+    emulated one after another in one process: bit-identical to the undivided
+    bsn_add_self_gravity_source_f64 on every slab's cells."""
+    import bsn
+    from bsn import shard
+    n, nz, d = 16, 32, (0.05, 0.07, 0.03)
+    U = random_state(n, n, nz, seed=13, gamma=5 / 3)
+    orc.fill_ghost_3d_outflow(U)
+    Ud = dev(U)
+    dU_ref = torch.zeros_like(Ud)
+    bsn.add_self_gravity_source(dU_ref, Ud, n, n, nz, *d)
+    ops = shard.DeviceOps()
+    slabs = [shard.Slab.split(n, n, nz, r, world) for r in range(world)]
+    P = [shard.SlabPoisson(s, *d, ops) for s in slabs]
+    nzl = nz // world
+    Us = []
+    for s in slabs:
+        V = bsn.state(n, n, nzl)
+        shard._zmajor(V)[...] = shard._zmajor(Ud)[s.k0:s.k0 + nzl + 2 * NG]
+        Us.append(V)
+    sent = [P[r].forward(ops.active_rho(Us[r], n, n, nzl)) for r in range(world)]
+    lines = [P[r].lines([sent[s][r] for s in range(world)]) for r in range(world)]
+    phi = [P[r].inverse([lines[s][r] for s in range(world)]) for r in range(world)]
+    for r, s in enumerate(slabs):
+        lo = phi[r - 1].permute(2, 1, 0)[-1] if r > 0 else None
+        hi = phi[r + 1].permute(2, 1, 0)[0] if r < world - 1 else None
+        dUs = torch.zeros_like(Us[r])
+        shard.sg_source(dUs, Us[r], phi[r], s, *d, ops, lo, hi)
+        got = dUs[:, NG:NG + n, NG:NG + n, NG:NG + nzl]
+        want = dU_ref[:, NG:NG + n, NG:NG + n, NG + s.k0:NG + s.k0 + nzl]
+        assert torch.equal(got, want), (r, float((got - want).abs().max()))

@@ -252,3 +252,81 @@ def test_split_checks():
         shard.Slab.split(8, 8, 15, 0, 2)
     with pytest.raises(ValueError):
         shard.Slab.split(8, 8, 8, 0, 4)   # 2 planes per rank < the 3-plane halo
+
+
+class SGOps(OracleOps, FFTOps):
+    """Oracle arithmetic for the self-gravity source on slabs (numpy state
+    arrays), torch.fft phases for the distributed solve."""
+
+    def __init__(self, orc):
+        OracleOps.__init__(self, orc, None)
+        FFTOps.__init__(self)
+
+    def active_rho(self, U, nx, ny, nz):
+        import torch
+        return torch.from_numpy(np.asfortranarray(U[0, NG:NG + nx, NG:NG + ny, NG:NG + nz]))
+
+    def sg_gradient(self, dU, U, phi, nx, ny, nz, dx, dy, dz):
+        self.orc.sg_gradient(dU, U, np.asfortranarray(np.asarray(phi)), dx, dy, dz)
+
+    def extend(self, U, dU, phi, nx, ny, nz, a, b, lo, hi):
+        nze = nz + a + b
+        Ue, dUe = self.orc.state(nx, ny, nze), self.orc.state(nx, ny, nze)
+        Ue[:, :, :, NG:NG + nze] = U[:, :, :, NG - a:NG + nz + b]
+        dUe[:, :, :, NG + a:NG + a + nz] = dU[:, :, :, NG:NG + nz]
+        phie = np.zeros((nx, ny, nze), order="F")
+        if a:
+            phie[:, :, 0] = np.asarray(lo).T
+        phie[:, :, a:a + nz] = np.asarray(phi)
+        if b:
+            phie[:, :, a + nz] = np.asarray(hi).T
+        return Ue, dUe, phie
+
+    @staticmethod
+    def shrink(dUe, dU, nz, a):
+        out = dU.copy(order="F")
+        out[:, :, :, NG:NG + nz] = dUe[:, :, :, NG + a:NG + a + nz]
+        return out
+
+
+def _sg_worker(rank, world, port, q):
+    try:
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        import torch.distributed as dist
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        sys.path.insert(0, os.path.join(ROOT, "binary-supernova_b200"))
+        import oracle as orc
+        from bsn import shard
+        dist.init_process_group("gloo", rank=rank, world_size=world)
+        n, nzg, d = 8, 16, (0.1, 0.12, 0.09)
+        U = _initial(orc, n, nzg, 9, "outflow")
+        ops = SGOps(orc)
+        # the undivided grid through the same phases (world 1), and the oracle's own source
+        whole = shard.Slab.split(n, n, nzg, 0, 1)
+        dU_ref = np.zeros_like(U, order="F")
+        shard.add_self_gravity_source(dU_ref, U, whole, *d, ops)
+        dU_orc = np.zeros_like(U, order="F")
+        orc.add_self_gravity_source(dU_orc, U, *d)
+        slab = shard.Slab.split(n, n, nzg, rank, world)
+        k0 = slab.k0
+        Us = orc.state(n, n, slab.nz)
+        Us[...] = U[:, :, :, k0:k0 + slab.nz + 2 * NG]
+        dUs = np.zeros_like(Us, order="F")
+        shard.add_self_gravity_source(dUs, Us, slab, *d, ops)
+        a = (slice(None), slice(NG, NG + n), slice(NG, NG + n))
+        mine = dUs[a + (slice(NG, NG + slab.nz),)]
+        ref = dU_ref[a + (slice(NG + k0, NG + k0 + slab.nz),)]
+        orc_ref = dU_orc[a + (slice(NG + k0, NG + k0 + slab.nz),)]
+        scale = np.abs(dU_orc).max()
+        err = float(np.abs(mine - ref).max() / scale)
+        err_orc = float(np.abs(mine - orc_ref).max() / scale)
+        q.put((rank, err < 1e-13 and err_orc < 1e-11, (err, err_orc)))
+        dist.destroy_process_group()
+    except Exception as e:   # report to the parent instead of hanging it
+        q.put((rank, False, repr(e)))
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_slab_self_gravity_source_matches_the_undivided_source(world):
+    for rank, ok, info in _spawn(_sg_worker, world):
+        assert ok, (rank, info)
