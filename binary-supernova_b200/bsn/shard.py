@@ -135,9 +135,12 @@ def cfl_dt(U, slab: Slab, dx, dy, dz, gamma, cfl, ops, group=None) -> float:
     return _allreduce_min(ops.cfl(U, slab.nx, slab.ny, slab.nz, dx, dy, dz, gamma, cfl), ops, group, slab.world)
 
 
-def euler3d_step(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group=None, rho_floor=0.0, P_floor=0.0):
+def euler3d_step(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group=None, rho_floor=0.0, P_floor=0.0,
+                 self_gravity=False):
     """euler3d_step! (src/euler3d.jl:220-260) on this rank's slab, with the
-    halo exchange before every right-hand side."""
+    halo exchange before every right-hand side; with self_gravity, the
+    self-gravity source of the global grid after each right-hand side, as
+    coupled_step! adds it (scripts/run_sn50_fiducial.jl:756-818, no BHs)."""
     nx, ny, nz = slab.nx, slab.ny, slab.nz
     Un = ops.copy(U)
     dU = ops.zeros_like(U)
@@ -145,6 +148,8 @@ def euler3d_step(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group=None, rho_floo
         ops.fill(U, nx, ny, nz, slab.bc)
         exchange(U, slab, ops, group, rho_floor, P_floor, gamma)
         ops.rhs(dU, U, nx, ny, nz, dx, dy, dz, gamma, slab.bc, rho_floor, P_floor)
+        if self_gravity:
+            add_self_gravity_source(dU, U, slab, dx, dy, dz, ops, group)
         if stage == 0:
             ops.assign(U, Un + dt * dU)
         elif stage == 1:
@@ -155,7 +160,7 @@ def euler3d_step(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group=None, rho_floo
 
 
 def run_steps(U, slab: Slab, dx, dy, dz, gamma, cfl, ops, *, n_steps, t=0.0, t_end=0.0, group=None,
-              rho_floor=0.0, P_floor=0.0):
+              rho_floor=0.0, P_floor=0.0, self_gravity=False):
     """The driver loop `dt = cfl_dt_3d; dt = min(dt, t_end - t); euler3d_step!;
     t += dt` over the slabs (every rank takes the same dts); returns (t, steps)."""
     steps = 0
@@ -165,7 +170,7 @@ def run_steps(U, slab: Slab, dx, dy, dz, gamma, cfl, ops, *, n_steps, t=0.0, t_e
             dt = min(dt, t_end - t)
         if not dt > 0.0:
             raise FloatingPointError(f"time step collapsed to {dt} at t = {t}")
-        euler3d_step(U, slab, dx, dy, dz, dt, gamma, ops, group, rho_floor, P_floor)
+        euler3d_step(U, slab, dx, dy, dz, dt, gamma, ops, group, rho_floor, P_floor, self_gravity)
         t += dt
         steps += 1
     return t, steps

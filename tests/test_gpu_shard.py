@@ -101,3 +101,25 @@ def test_slab_self_gravity_source_bitwise(orc, world):
         got = dUs[:, NG:NG + n, NG:NG + n, NG:NG + nzl]
         want = dU_ref[:, NG:NG + n, NG:NG + n, NG + s.k0:NG + s.k0 + nzl]
         assert torch.equal(got, want), (r, float((got - want).abs().max()))
+
+
+def test_single_slab_self_gravity_step_matches_coupled_step(orc):
+    """The sharded step with self-gravity on one rank (device operations,
+    the distributed solve's phases) against the oracle's coupled_step! with
+    no BHs: the FFTs differ by rounding only."""
+    from bsn import shard
+    n, nz, dx, g = 16, 16, 0.1, 5 / 3
+    kw = dict(rho_floor=1e-8, P_floor=1e-8)
+    U = random_state(n, n, nz, seed=19, gamma=g, jumps=False)
+    orc.fill_ghost_3d_outflow(U)
+    Ud = dev(U)
+    slab = shard.Slab.split(n, n, nz, 0, 1)
+    none = (orc.OrcBH * 1)()
+    for _ in range(2):
+        shard.euler3d_step(Ud, slab, dx, dx, dx, 1e-3, g, shard.DeviceOps(), self_gravity=True, **kw)
+        orc.coupled_step(U, none, 0, 1e-3, 0.0, dx, 0.0, 0.0, 0.0, g, 1.0, kw["rho_floor"], kw["P_floor"],
+                         True, True, 0.0, 0.0, evolve_orbit=False)
+    got = host(Ud)
+    a = (slice(NG, -NG),) * 3
+    for q in range(5):
+        assert np.abs(got[(q,) + a] - U[(q,) + a]).max() <= 1e-11 * np.abs(U[q]).max(), q
