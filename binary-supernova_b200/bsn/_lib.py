@@ -94,6 +94,7 @@ SIGNATURES = {
     "bsn_poisson_slab_zconv_f64": (_I, [_V, _P, _I, _I, _I, _I, _I, _D, _D, _D]),
     "bsn_poisson_slab_inverse_f64": (_I, [_V, _P, _I, _I, _I, _P]),
     "bsn_sg_gradient_f64": (_I, [_V, _P, _P, _P, _I, _I, _I, _D, _D, _D]),
+    "bsn_sg_gradient_slab_f64": (_I, [_V, _P, _P, _P, _P, _P, _I, _I, _I, _D, _D, _D]),
     "bsn_add_self_gravity_source_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D]),
     "bsn_coupled_step_f64": (_I, [_V, _P, _BH, _I, _D, _D, _I, _I, _I, _D, _D, _D, _D, _D, _D, _D, _D,
                                   _I, _I, _D, _D, _I, _dp]),

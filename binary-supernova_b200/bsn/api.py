@@ -29,7 +29,7 @@ __all__ = [
     "cfl_dt_3d", "add_bh_gravity_source", "gas_force_on_bh", "add_sink_sources", "accrete", "r_sink", "t_sink",
     "nbody_step", "KeplerOrbit", "kepler_update", "solve_poisson_isolated", "add_self_gravity_source",
     "poisson_slab_forward", "poisson_slab_zconv", "poisson_slab_inverse",
-    "apply_sg_force_level", "coupled_step", "FMRGrid3D", "fmr3d_step", "cfl_dt_fmr3d", "solve_fmr_poisson",
+    "apply_sg_force_level", "apply_sg_force_slab", "coupled_step", "FMRGrid3D", "fmr3d_step", "cfl_dt_fmr3d", "solve_fmr_poisson",
     "restrict_density_to_coarse", "FMRHierarchy3D", "fmr_nested_step", "cfl_dt_fmr_nested",
     "fmr_nested_run_steps", "coupled_nested_run_steps", "rotating_frame_source", "relax_damping_source",
     "relax_ic",
@@ -302,6 +302,18 @@ def apply_sg_force_level(dU, U, phi, nx, ny, nz, dx, dy, dz):
     _check_grid(phi, nx, ny, nz, "phi")
     _call("bsn_sg_gradient_f64", context(), _ptr(dU), _ptr(U), _ptr(phi), nx, ny, nz, float(dx), float(dy),
           float(dz))
+
+
+def apply_sg_force_slab(dU, U, phi, nx, ny, nz, dx, dy, dz, phi_lo=None, phi_hi=None):
+    """_apply_sg_force_level! on a z-slab of a larger grid: phi_lo / phi_hi
+    are the (nx, ny) planes of Phi just below / above the slab (None at the
+    larger grid's own z boundary)."""
+    _check_grid(phi, nx, ny, nz, "phi")
+    for p in (phi_lo, phi_hi):
+        if p is not None and not (p.is_contiguous() and p.numel() == nx * ny):
+            raise ValueError("neighbour planes of Phi must be contiguous (nx, ny) arrays")
+    _call("bsn_sg_gradient_slab_f64", context(), _ptr(dU), _ptr(U), _ptr(phi), _ptr(phi_lo), _ptr(phi_hi), nx, ny,
+          nz, float(dx), float(dy), float(dz))
 
 
 def add_self_gravity_source(dU, U, nx, ny, nz, dx, dy, dz):

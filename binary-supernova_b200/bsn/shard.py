@@ -140,7 +140,11 @@ def euler3d_step(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group=None, rho_floo
     """euler3d_step! (src/euler3d.jl:220-260) on this rank's slab, with the
     halo exchange before every right-hand side; with self_gravity, the
     self-gravity source of the global grid after each right-hand side, as
-    coupled_step! adds it (scripts/run_sn50_fiducial.jl:756-818, no BHs)."""
+    coupled_step! adds it (scripts/run_sn50_fiducial.jl:756-818, no BHs).
+    Self-gravity needs outflow boundaries: the isolated solve does not wrap,
+    and the reference runs it only with outflow (coupled_step!)."""
+    if self_gravity and slab.bc != "outflow":
+        raise ValueError("self_gravity needs bc='outflow': the isolated Poisson solve has no periodic form")
     nx, ny, nz = slab.nx, slab.ny, slab.nz
     Un = ops.copy(U)
     dU = ops.zeros_like(U)
@@ -163,6 +167,8 @@ def run_steps(U, slab: Slab, dx, dy, dz, gamma, cfl, ops, *, n_steps, t=0.0, t_e
               rho_floor=0.0, P_floor=0.0, self_gravity=False):
     """The driver loop `dt = cfl_dt_3d; dt = min(dt, t_end - t); euler3d_step!;
     t += dt` over the slabs (every rank takes the same dts); returns (t, steps)."""
+    if self_gravity and slab.bc != "outflow":
+        raise ValueError("self_gravity needs bc='outflow': the isolated Poisson solve has no periodic form")
     steps = 0
     while steps < n_steps and (t_end <= 0.0 or t < t_end):
         dt = cfl_dt(U, slab, dx, dy, dz, gamma, cfl, ops, group)
@@ -283,17 +289,16 @@ def sg_source(dU, U, phi, slab: Slab, dx, dy, dz, ops, lo=None, hi=None):
     """The self-gravity source (src/self_gravity.jl:93-115 after the solve;
     src/gpu_kernels.jl:291-319) on this slab's cells from its planes of Phi and
     the neighbours' planes lo / hi (None at a global boundary, where the
-    reference's one-sided difference applies).  Computed on the slab extended
-    by those planes, so every cell takes the undivided grid's arithmetic."""
+    reference's one-sided difference applies).  Every cell takes the
+    undivided grid's arithmetic: interior slab faces the central difference
+    with the neighbour's plane, global boundaries the one-sided one."""
     nx, ny, nz = slab.nx, slab.ny, slab.nz
-    a, b = (lo is not None), (hi is not None)
-    if not (a or b):
+    if lo is None and hi is None:
         ops.sg_gradient(dU, U, phi, nx, ny, nz, dx, dy, dz)
         return
-    nze = nz + a + b
-    Ue, dUe, phie = ops.extend(U, dU, phi, nx, ny, nz, a, b, lo, hi)
-    ops.sg_gradient(dUe, Ue, phie, nx, ny, nze, dx, dy, dz)
-    ops.assign(dU, ops.shrink(dUe, dU, nz, a))
+    # the slab's edge planes take the central z difference with the
+    # neighbours' planes, in place (no extended copy of the state)
+    ops.sg_gradient_slab(dU, U, phi, nx, ny, nz, dx, dy, dz, lo, hi)
 
 
 def add_self_gravity_source(dU, U, slab: Slab, dx, dy, dz, ops, group=None):
@@ -355,29 +360,10 @@ class DeviceOps:
     def sg_gradient(self, dU, U, phi, nx, ny, nz, dx, dy, dz):
         self.api.apply_sg_force_level(dU, U, phi, nx, ny, nz, dx, dy, dz)
 
-    def extend(self, U, dU, phi, nx, ny, nz, a, b, lo, hi):
-        """U, dU and Phi of the slab with `a` plane(s) below and `b` above:
-        dU and U copied (U's ghost planes supply the extra cells' state, which
-        only feeds their own discarded source), Phi from the neighbours."""
-        nze = nz + a + b
-        Ue = self.api.state(nx, ny, nze, device=U.device)
-        dUe = self.api.state(nx, ny, nze, device=U.device)
-        _zmajor(Ue)[NG:NG + nze] = _zmajor(U)[NG - a:NG + nz + b]
-        _zmajor(dUe)[NG + a:NG + a + nz] = _zmajor(dU)[NG:NG + nz]
-        phie = self.api.active_grid(nx, ny, nze, device=U.device)
-        P = phie.permute(2, 1, 0)
-        if a:
-            P[0] = lo
-        P[a:a + nz] = phi.permute(2, 1, 0)
-        if b:
-            P[a + nz] = hi
-        return Ue, dUe, phie
-
-    @staticmethod
-    def shrink(dUe, dU, nz, a):
-        out = dU.clone()
-        _zmajor(out)[NG:NG + nz] = _zmajor(dUe)[NG + a:NG + a + nz]
-        return out
+    def sg_gradient_slab(self, dU, U, phi, nx, ny, nz, dx, dy, dz, lo, hi):
+        self.api.apply_sg_force_slab(dU, U, phi, nx, ny, nz, dx, dy, dz,
+                                     None if lo is None else lo.contiguous(),
+                                     None if hi is None else hi.contiguous())
 
     def floor_planes(self, planes, nx, ny, rho_floor, P_floor, gamma):
         """apply_floors_3d! on the active (i, j) cells of NG received z-planes

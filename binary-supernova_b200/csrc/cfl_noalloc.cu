@@ -12,10 +12,19 @@
 //     so grids of at most 134,217,728 active cells (512^3) are accepted; larger
 //     grids are rejected with BSN_ERR_UNSUPPORTED before anything is launched;
 //   * the array occupies 512 KiB on every GPU that loads the library, until
-//     the process exits;
+//     the process exits.  The library is built without relocatable device
+//     code, so this file is a module of its own, and under CUDA's lazy module
+//     loading (the default since CUDA 12.2) the driver reserves the array on
+//     a device only when this file's module is first used there: at the first
+//     call of this entry point on that device.  A caller whose pool will
+//     later reserve the whole device should make one warm-up call at start-up,
+//     before the pool takes its memory, or run with CUDA_MODULE_LOADING=EAGER;
 //   * the first call on a device looks the array's device address up
-//     (cudaGetSymbolAddress, with that device current) and caches it; this
-//     first call should come before any stream capture;
+//     (cudaGetSymbolAddress, with that device current) and caches it per
+//     device; this first call should come before any stream capture.  The
+//     device is the context's: a call made while another device is current
+//     is rejected with BSN_ERR_ARG, since the context's stream and the array
+//     of the current device would then belong to different GPUs;
 //   * every call shares the array and overwrites the slots it reads, so calls
 //     that overlap on the GPU (different streams, threads or contexts of one
 //     process) race; serialise them;
@@ -92,9 +101,16 @@ __global__ void cfl_final_kernel(unsigned long long* partial, int nblocks, unsig
 std::mutex g_setup_mutex;
 unsigned long long* g_scratch_ptr[64] = {nullptr};
 
-bsn_status scratch_for_current_device(bsn_ctx* ctx, unsigned long long** out) {
+// The array of the context's device.  cudaGetSymbolAddress answers for the
+// current device, so the current device must be the context's.
+bsn_status scratch_for_context_device(bsn_ctx* ctx, unsigned long long** out) {
     int dev = -1;
     BSN_TRY(cuda_check(ctx, cudaGetDevice(&dev), "cudaGetDevice"));
+    if (dev != ctx->device)
+        return set_err(ctx, BSN_ERR_ARG,
+                       "bsn_cfl_dt_3d_f64_noalloc: current device %d is not the context's device %d; make the "
+                       "context's device current first",
+                       dev, ctx->device);
     if (dev < 0 || dev >= 64) return set_err(ctx, BSN_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_scratch_ptr[dev]) {
@@ -114,6 +130,7 @@ using namespace bsn::noalloc;
 
 extern "C" bsn_status bsn_cfl_dt_3d_f64_noalloc(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx,
                                                 double dy, double dz, double gamma, double cfl, double* dt_out) {
+    if (!ctx) return BSN_ERR_ARG;
     BSN_TRY(check_dims(ctx, nx, ny, nz));
     if (!U || !dt_out) return set_err(ctx, BSN_ERR_ARG, "U and dt_out must be non-null");
     const long long n = (long long)nx * ny * nz;
@@ -123,7 +140,7 @@ extern "C" bsn_status bsn_cfl_dt_3d_f64_noalloc(bsn_ctx* ctx, const double* U, i
                        "cells (512^3); use bsn_cfl_dt_3d_f64",
                        n, kMaxCells);
     unsigned long long* scratch = nullptr;
-    BSN_TRY(scratch_for_current_device(ctx, &scratch));
+    BSN_TRY(scratch_for_context_device(ctx, &scratch));
     const int nblocks = (int)((n + kCellsPerBlock - 1) / kCellsPerBlock);
     // every partial slot [0, nblocks) and the result slot are written before
     // they are read in this call, so nothing needs clearing

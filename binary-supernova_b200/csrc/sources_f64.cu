@@ -89,9 +89,13 @@ __global__ void sink_kernel(double* dU, const double* U, int nx, int ny, int nz,
     }
 }
 
-// _sg_gradient_kernel! (src/gpu_kernels.jl:291-319)
+// _sg_gradient_kernel! (src/gpu_kernels.jl:291-319).  Plo / Phi (may be
+// null): the plane of Phi just below / above the grid, when the grid is a
+// z-slab of a larger one; the slab's edge planes then take the central
+// difference the larger grid's cells take there.
 __global__ void sg_gradient_kernel(double* dU, const double* U, const double* P, int nx, int ny, int nz,
-                                   double i2x, double i2y, double i2z) {
+                                   double i2x, double i2y, double i2z, const double* Plo = nullptr,
+                                   const double* Phi = nullptr) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)nx * ny * nz) return;
     int a = (int)(t % nx); long long r = t / nx; int b = (int)(r % ny); int c = (int)(r / ny);
@@ -105,7 +109,13 @@ __global__ void sg_gradient_kernel(double* dU, const double* U, const double* P,
     long long sy = nx, sz = (long long)nx * ny;
     double gx = (P[ip + sy * b + sz * c] - P[im + sy * b + sz * c]) * fx;
     double gy = (P[a + sy * jp + sz * c] - P[a + sy * jm + sz * c]) * fy;
-    double gz = (P[a + sy * b + sz * kp] - P[a + sy * b + sz * km]) * fz;
+    double pzp = P[a + sy * b + sz * kp], pzm = P[a + sy * b + sz * km];
+    // with a neighbour plane the slab is part of a grid of >= 2 planes, where
+    // every plane's z difference spans two distinct planes
+    if (Plo || Phi) fz = i2z;
+    if (c == nz - 1 && Phi) pzp = Phi[a + sy * b];
+    if (c == 0 && Plo) pzm = Plo[a + sy * b];
+    double gz = (pzp - pzm) * fz;
     double vdotg = (rvx * gx + rvy * gy + rvz * gz) / rho;
     dU[o + 1] -= rho * gx;
     dU[o + 2] -= rho * gy;
@@ -354,6 +364,16 @@ extern "C" bsn_status bsn_sg_gradient_f64(bsn_ctx* ctx, double* dU, const double
     if (!dU || !U || !phi) return set_err(ctx, BSN_ERR_ARG, "null array");
     sg_gradient_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(dU, U, phi, nx, ny, nz, 0.5 / dx,
                                                                                         0.5 / dy, 0.5 / dz);
+    return launch_check(ctx, "sg_gradient_kernel");
+}
+
+extern "C" bsn_status bsn_sg_gradient_slab_f64(bsn_ctx* ctx, double* dU, const double* U, const double* phi,
+                                               const double* phi_lo, const double* phi_hi, int nx, int ny, int nz,
+                                               double dx, double dy, double dz) {
+    BSN_TRY(check_dims(ctx, nx, ny, nz));
+    if (!dU || !U || !phi) return set_err(ctx, BSN_ERR_ARG, "null array");
+    sg_gradient_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(
+        dU, U, phi, nx, ny, nz, 0.5 / dx, 0.5 / dy, 0.5 / dz, phi_lo, phi_hi);
     return launch_check(ctx, "sg_gradient_kernel");
 }
 

@@ -120,10 +120,14 @@ bsn_status bsn_cfl_dt_3d_f64(bsn_ctx* ctx, const double* U, int nx, int ny, int 
  * device-memory pool, or a job that sizes all its memory at start-up).  Its
  * scratch is a file-scope static device array of 512 KiB held on every GPU
  * that loads the library until exit; grids above 512^3 = 134,217,728 active
- * cells are rejected with BSN_ERR_UNSUPPORTED.  The first call on a device
- * looks up the array's address with that device current; this first call
- * should come before any stream capture.  All calls share the array: calls
- * that overlap on the GPU race.  The success path allocates nothing. */
+ * cells are rejected with BSN_ERR_UNSUPPORTED.  Under CUDA's lazy module
+ * loading the driver reserves the array on a device at the first call there:
+ * make one warm-up call at start-up, before a pool takes the device's memory
+ * (or set CUDA_MODULE_LOADING=EAGER).  The first call on a device looks up
+ * the array's address with that device current; this first call should come
+ * before any stream capture.  The context's device must be current
+ * (BSN_ERR_ARG otherwise).  All calls share the array: calls that overlap on
+ * the GPU race.  The success path allocates nothing. */
 bsn_status bsn_cfl_dt_3d_f64_noalloc(bsn_ctx* ctx, const double* U, int nx, int ny, int nz,
                                      double dx, double dy, double dz, double gamma, double cfl,
                                      double* dt_out);
@@ -256,6 +260,14 @@ bsn_status bsn_poisson_slab_inverse_f64(bsn_ctx* ctx, const double* W2, int nx, 
 /* _apply_sg_force_level! (src/fmr_gravity.jl:146-156; src/gpu_kernels.jl:291-319) */
 bsn_status bsn_sg_gradient_f64(bsn_ctx* ctx, double* dU, const double* U, const double* phi,
                                int nx, int ny, int nz, double dx, double dy, double dz);
+/* _apply_sg_force_level! on a z-slab of a larger grid (src/gpu_kernels.jl:
+ * 291-319 applied to the larger grid): phi_lo / phi_hi (device, nx*ny, may be
+ * NULL) are the planes of Phi just below / above the slab, so the slab's edge
+ * planes take the central z difference of the larger grid's cells; NULL at the
+ * larger grid's own boundary keeps the reference's one-sided difference. */
+bsn_status bsn_sg_gradient_slab_f64(bsn_ctx* ctx, double* dU, const double* U, const double* phi,
+                                    const double* phi_lo, const double* phi_hi, int nx, int ny, int nz,
+                                    double dx, double dy, double dz);
 /* add_self_gravity_source! (src/self_gravity.jl:93-115) */
 bsn_status bsn_add_self_gravity_source_f64(bsn_ctx* ctx, double* dU, const double* U,
                                            int nx, int ny, int nz, double dx, double dy, double dz);

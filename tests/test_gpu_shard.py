@@ -70,7 +70,7 @@ def test_slab_poisson_bitwise_to_the_undivided_solve(orc, world):
 @pytest.mark.parametrize("world", [2, 4])
 def test_slab_self_gravity_source_bitwise(orc, world):
     """The self-gravity source on slabs (distributed Phi, one plane of Phi from
-    each neighbour, the gradient on the slab extended by those planes), ranks
+    each neighbour, the gradient taking those planes at the slab's edges), ranks
     emulated one after another in one process: bit-identical to the undivided
     bsn_add_self_gravity_source_f64 on every slab's cells."""
     import bsn

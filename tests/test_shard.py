@@ -252,6 +252,13 @@ def test_split_checks():
         shard.Slab.split(8, 8, 15, 0, 2)
     with pytest.raises(ValueError):
         shard.Slab.split(8, 8, 8, 0, 4)   # 2 planes per rank < the 3-plane halo
+    # self-gravity's isolated solve does not wrap: periodic slabs are refused
+    # before any state or operation is touched
+    per = shard.Slab.split(8, 8, 16, 0, 2, "periodic")
+    with pytest.raises(ValueError):
+        shard.euler3d_step(None, per, 1.0, 1.0, 1.0, 1e-3, 1.4, None, self_gravity=True)
+    with pytest.raises(ValueError):
+        shard.run_steps(None, per, 1.0, 1.0, 1.0, 1.4, 0.4, None, n_steps=1, self_gravity=True)
 
 
 class SGOps(OracleOps, FFTOps):
@@ -287,6 +294,14 @@ class SGOps(OracleOps, FFTOps):
         out = dU.copy(order="F")
         out[:, :, :, NG:NG + nz] = dUe[:, :, :, NG + a:NG + a + nz]
         return out
+
+    def sg_gradient_slab(self, dU, U, phi, nx, ny, nz, dx, dy, dz, lo, hi):
+        """The oracle's gradient on the slab extended by the neighbour planes:
+        the undivided grid's arithmetic on the slab's cells."""
+        a, b = int(lo is not None), int(hi is not None)
+        Ue, dUe, phie = self.extend(U, dU, phi, nx, ny, nz, a, b, lo, hi)
+        self.sg_gradient(dUe, Ue, phie, nx, ny, nz + a + b, dx, dy, dz)
+        self.assign(dU, self.shrink(dUe, dU, nz, a))
 
 
 def _sg_worker(rank, world, port, q):

@@ -46,6 +46,33 @@ def test_noalloc_cfl_matches_regular_entry_two_calls_in_a_row():
         assert first == ref and second == ref
 
 
+def test_noalloc_cfl_reserves_no_device_memory():
+    # A fresh context has no workspace yet.  After one warm-up call (which,
+    # under lazy module loading, lets the driver place the static array),
+    # further calls must leave the device's free memory unchanged: no
+    # cudaMalloc, and no workspace slot created behind the caller's back.
+    import bsn
+    from bsn._lib import load
+    L = load()
+    bsn.context()
+    torch.cuda.set_device(0)
+    U = dev(random_state(32, 24, 16, seed=15))
+    torch.cuda.synchronize()
+    ctx = C.c_void_p()
+    assert L.bsn_ctx_create(C.byref(ctx), 0, C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+    try:
+        n, d = (32, 24, 16), (0.1, 0.1, 0.1)
+        warm = _dt(L, "bsn_cfl_dt_3d_f64_noalloc", ctx, U, n, d)
+        free_before, _ = torch.cuda.mem_get_info()
+        got = [_dt(L, "bsn_cfl_dt_3d_f64_noalloc", ctx, U, n, d) for _ in range(4)]
+        free_after, _ = torch.cuda.mem_get_info()
+        assert free_after == free_before, (free_before, free_after)
+        assert all(g == warm for g in got)
+        assert got[0] == _dt(L, "bsn_cfl_dt_3d_f64", ctx, U, n, d)
+    finally:
+        L.bsn_ctx_destroy(ctx)
+
+
 def test_noalloc_cfl_nan_state_gives_inf_like_the_reference():
     ctx, L = _ctx_and_lib()
     U = random_state(16, 8, 8, seed=13)
