@@ -13,6 +13,8 @@ sequentially in the reference's loop order i fastest, then j, then k):
 * lane_emden       src/stellar_ic.jl:34-63
 * polytrope_ic_3d  src/stellar_ic.jl:87-178 (polytrope_ic_3d!)
 * thermal_bomb     src/stellar_ic.jl:210-253 (thermal_bomb!)
+* apply_stellar_rotation  scripts/run_sn50_fiducial.jl:421-446
+                   (apply_stellar_rotation!, the rigid-rotation overlay)
 """
 from __future__ import annotations
 
@@ -229,3 +231,31 @@ def thermal_bomb(U, nx, ny, nz, dx, dy, dz, *, E_SN, r_bomb, r_bomb_inner=0.0, x
     H[(4,) + a] = np.where(sel, E + fac * rho, E)
     _store(U, H)
     return M_bomb
+
+
+def apply_stellar_rotation(U, nx, ny, nz, dx, gamma, Omega, *, v_star_y=0.0, x_star=0.0, y_star=0.0, rho_thresh,
+                           x0=0.0, y0=0.0):
+    """apply_stellar_rotation! (scripts/run_sn50_fiducial.jl:421-446): the
+    gas of every active cell with rho > rho_thresh takes the velocity
+    v = (0, v_star_y, 0) + Omega z x (r - r_star); its internal energy
+    (U[4] holds only internal energy before the overlay) is kept and the
+    kinetic energy added.  x0, y0: lower corner of the grid; dx the cell width
+    the reference uses on both axes."""
+    H = _read(U, nx, ny, nz)
+    a = (slice(NG, NG + nx), slice(NG, NG + ny), slice(NG, NG + nz))
+    rho = H[(0,) + a]
+    sel = rho > rho_thresh
+    xc = x0 + (np.arange(1, nx + 1, dtype=np.float64) - 0.5) * dx - x_star
+    yc = y0 + (np.arange(1, ny + 1, dtype=np.float64) - 0.5) * dx - y_star
+    shape = (nx, ny, nz)
+    vx = np.broadcast_to(-Omega * yc[None, :, None], shape)
+    vy = np.broadcast_to(v_star_y + Omega * xc[:, None, None], shape)
+    vz = np.zeros(shape)
+    P_int = H[(4,) + a] * (gamma - 1.0)
+    ke = ((vx * vx + vy * vy) + vz * vz)
+    m = {1: rho * vx, 2: rho * vy, 3: rho * vz}
+    for q in (1, 2, 3):
+        H[(q,) + a] = np.where(sel, m[q], H[(q,) + a])
+    H[(4,) + a] = np.where(sel, P_int / (gamma - 1.0) + 0.5 * rho * ke, H[(4,) + a])
+    if H is not U:
+        _store(U, H)

@@ -22,12 +22,16 @@ def binary_setup(orc, n=32, L=4.0, r_bomb=0.5, gamma=4.0 / 3.0, rho_floor=1e-8, 
     return U, dx, -L, bhs
 
 
-def binary_nested_setup(orc, n=16, L=4.0, sep=1.0, r_bomb=0.5, gamma=4.0 / 3.0, rho_floor=1e-8, P_floor=1e-10):
+def binary_nested_setup(orc, n=16, L=4.0, sep=1.0, r_bomb=0.5, gamma=4.0 / 3.0, rho_floor=1e-8, P_floor=1e-10,
+                        sink_cells=3):
     """Three nested levels of n^3 (ratio 2, each covering the middle half of
     its parent: [-L,L]^3, [-L/2,L/2]^3, [-L/4,L/4]^3), each with its own
     polytrope + thermal bomb initial state at its resolution and ghosts from
-    its parent; two m=5 BHs at (+-sep/2, 0, 0) with sink radius 3 and
-    softening 2 finest cells.  Returns (hierarchy, dx0, x0, bh specs)."""
+    its parent; two m=5 BHs at (+-sep/2, 0, 0) with sink radius `sink_cells`
+    and softening 2 finest cells.  A level none of whose cell centres lies
+    within r_bomb gets no bomb (thermal_bomb! would find no gas there; the
+    covered centre of that level takes the finer levels' restriction).  Returns (hierarchy,
+    dx0, x0, bh specs)."""
     dx0 = 2 * L / n
     lo, hi = n // 4 + 1, 3 * n // 4
     boxes = ((lo, hi, lo, hi, lo, hi, 2),) * 2
@@ -36,7 +40,8 @@ def binary_nested_setup(orc, n=16, L=4.0, sep=1.0, r_bomb=0.5, gamma=4.0 / 3.0, 
     def fill(U, dx, x0):
         orc.polytrope_ic_3d(U, dx, dx, dx, gamma, 10.0, 1.0, x0=x0, y0=x0, z0=x0, rho_floor=rho_floor,
                             P_floor=P_floor)
-        orc.thermal_bomb(U, dx, dx, dx, 1.0, r_bomb, x0=x0, y0=x0, z0=x0)
+        if math.sqrt(3.0) * dx / 2 < r_bomb:   # the cell centres nearest the origin
+            orc.thermal_bomb(U, dx, dx, dx, 1.0, r_bomb, x0=x0, y0=x0, z0=x0)
 
     fill(U0, dx0, -L)
     orc.fill_ghost_3d_outflow(U0)
@@ -50,5 +55,5 @@ def binary_nested_setup(orc, n=16, L=4.0, sep=1.0, r_bomb=0.5, gamma=4.0 / 3.0, 
     v = math.sqrt(10.0 / sep) / 2.0
     bhs = [dict(pos=(sep / 2, 0.0, 0.0), vel=(0.0, v, 0.0)), dict(pos=(-sep / 2, 0.0, 0.0), vel=(0.0, -v, 0.0))]
     for b in bhs:
-        b.update(mass=5.0, eps=2 * dx, c_code=1e6, r_floor=3 * dx)
+        b.update(mass=5.0, eps=2 * dx, c_code=1e6, r_floor=sink_cells * dx)
     return H, boxes, dx0, -L, bhs

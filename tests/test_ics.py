@@ -58,3 +58,31 @@ def test_bomb_without_gas_raises():
     B = np.zeros((5, 14, 14, 14), order="F")
     with pytest.raises(ValueError):
         ics.thermal_bomb(B, 8, 8, 8, 0.1, 0.1, 0.1, E_SN=1.0, r_bomb=0.2)
+
+
+def test_stellar_rotation_overlay(orc):
+    """apply_stellar_rotation! (scripts/run_sn50_fiducial.jl:421-446) as the
+    reference's cell loop, written out here in plain Python at a small size:
+    the vectorised overlay must produce the same bits."""
+    n, g, dx, x0 = 12, 2.0, 4.0 / 12, -2.0
+    A = orc.state(n, n + 2, n + 1)
+    orc.polytrope_ic_3d(A, dx, dx, dx, g, 1.0, 1.2, x0=x0, y0=x0, z0=x0, rho_floor=1e-8, P_floor=1e-10)
+    B = A.copy(order="F")
+    Om, vsy, xs, ys, thr = 0.5657, 0.1, 0.05, -0.02, 2e-8
+    NG = 3
+    for k in range(NG, NG + n + 1):
+        for j in range(NG, NG + n + 2):
+            for i in range(NG, NG + n):
+                rho = A[0, i, j, k]
+                if rho <= thr:
+                    continue
+                xc = x0 + (i + 1 - NG - 0.5) * dx - xs
+                yc = x0 + (j + 1 - NG - 0.5) * dx - ys
+                vx, vy, vz = -Om * yc, vsy + Om * xc, 0.0
+                P = A[4, i, j, k] * (g - 1.0)
+                A[1, i, j, k], A[2, i, j, k], A[3, i, j, k] = rho * vx, rho * vy, rho * vz
+                A[4, i, j, k] = P / (g - 1.0) + 0.5 * rho * (vx * vx + vy * vy + vz * vz)
+    ics.apply_stellar_rotation(B, n, n + 2, n + 1, dx, g, Om, v_star_y=vsy, x_star=xs, y_star=ys, rho_thresh=thr,
+                               x0=x0, y0=x0)
+    assert (A[0] > thr).sum() > 100
+    _eq(A, B)
