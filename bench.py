@@ -9,11 +9,18 @@ step, the loop the reference drivers run (cfl_dt_3d + euler3d_step!).
                   [--n 256] [--path learned|f32|f64] [--tile V] [--no-cpu]
                   [--no-accuracy] [--no-fmr]
   python bench.py --workload binary_nested [--paths f64,f32,learned]
-                  [--steps K] [--warmup W]
+                  [--steps K] [--warmup W] [--full]
+  python bench.py --workload polytrope_fmr [--omega 0.2] [--steps K]
+                  [--warmup W] [--full]
 
-The second form times only the binary-BH supernova on three nested 128^3
+The other forms time only the binary-BH supernova on three nested 128^3
 FMR levels (the coupled driver loop on the device) for the listed stencil
-paths and prints its JSON object.
+paths, or only the self-gravitating polytrope on two 128^3 FMR levels, and
+print their JSON object; --full runs the workload's stated length from its
+initial state (1000 / 200 steps).  Both report the FP64 mass budget of the
+driver loop (gas mass against the ledger of floors, outflow, sink drain and
+accretion) where the loop has sinks, and the L1 density and energy
+differences of the reduced-precision paths against FP64 at equal time.
 
 `value` is device-resident throughput over K steps (state in HBM).  `e2e`
 runs the same step through the public host-buffer path: the state is copied
@@ -51,6 +58,24 @@ _T0 = time.time()
 def log(msg):
     """Progress on stderr (the JSON line is the only stdout output)."""
     print(f"[bench {time.time() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
+def mass_closure(rec_last, M_start, MBH_start, MBH_end):
+    """The mass budget of a driver-loop call from its last diagnostics record
+    (bsn.DIAG_FIELDS: the gas mass and the FP64 ledger since the call began):
+    the gas-side residual |M_gas - (M_start + floors_in - outflow - drained)|
+    and the whole residual with the BHs and the reference's drain / credit
+    split, both relative to the mass at the start."""
+    import bsn
+    f = {k: float(rec_last[i]) for i, k in enumerate(bsn.DIAG_FIELDS)}
+    gas = f["M_gas"] - (M_start + f["floors_in"] - f["outflow"] - f["drained"])
+    total = (f["M_gas"] + MBH_end - M_start - MBH_start - f["floors_in"] + f["outflow"]
+             - (f["accreted"] - f["drained"]))
+    return {"M_gas_start": M_start, "M_gas_end": f["M_gas"], "M_bh_start": MBH_start, "M_bh_end": MBH_end,
+            "floors_in": f["floors_in"], "outflow": f["outflow"], "drained": f["drained"],
+            "accreted": f["accreted"], "gas_residual_rel": abs(gas) / M_start,
+            "total_residual_rel": abs(total) / (M_start + MBH_start),
+            "accreted_minus_drained": f["accreted"] - f["drained"]}
 
 
 def peaks():
@@ -133,18 +158,27 @@ def sedov_host(n, cpu_leg=False):
     return U, dx
 
 
-def cpu_reference_rate(n, threads, nz_sample, steps, min_seconds=0.0, max_steps=64):
-    """Oracle (CPU restatement of the reference path) on a z-slab sample of
-    the Sedov n^3 workload: cell-updates/s with `threads` OpenMP threads,
-    over `steps` RK3 steps, continued until `min_seconds` have elapsed (at
-    most `max_steps`).  Returns (rate, seconds, steps)."""
+CPU_SLAB = 32      # z-planes of the CPU sample (both CPU legs)
+
+
+def cpu_slab(U, n, nz_sample):
+    """nz_sample z-planes through the blast centre of a ghosted Sedov state,
+    as a grid of its own (ghost planes included, F-ordered)."""
     import numpy as np
+    k0 = NG + n // 2 - nz_sample // 2
+    return np.asfortranarray(U[:, :, :, k0 - NG:k0 + nz_sample + NG])
+
+
+def cpu_reference_rate(S, n, dx, threads, steps, min_seconds=0.0, max_steps=64):
+    """Oracle (CPU restatement of the reference path) on a z-slab sample S of
+    the Sedov n^3 workload, stepped in place: cell-updates/s with `threads`
+    OpenMP threads, over `steps` RK3 steps (cfl_dt_3d + euler3d_step!),
+    continued until `min_seconds` have elapsed (at most `max_steps`).
+    Returns (rate, seconds, steps)."""
     import oracle
     oracle.build()
     oracle.set_threads(threads)
-    U, dx = sedov_host(n, cpu_leg=True)
-    k0 = NG + n // 2 - nz_sample // 2
-    S = np.asfortranarray(U[:, :, :, k0 - NG:k0 + nz_sample + NG])
+    nz_sample = S.shape[3] - 2 * NG
     t0 = time.perf_counter()
     k = 0
     while k < steps or (time.perf_counter() - t0 < min_seconds and k < max_steps):
@@ -155,23 +189,51 @@ def cpu_reference_rate(n, threads, nz_sample, steps, min_seconds=0.0, max_steps=
     return n * n * nz_sample * k / el, el, k
 
 
+def sedov_mid_state(n):
+    """The Sedov n^3 state at t = T_MID, the state the GPU arm's timed steps
+    start from, on the host.  It is made by the library's FP64 device loop,
+    which is bit-identical to the oracle's own loop (FP64 parity tests up to
+    the workload's sizes): the oracle would need tens of minutes of host time
+    to reach it.  Without a GPU: the initial state (and t = 0)."""
+    U0, dx = sedov_host(n, cpu_leg=True)
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return U0, dx, 0.0
+        import bsn
+        Ud = torch.from_numpy(U0).cuda()
+        t, _ = bsn.run_steps(Ud, n, n, n, dx, dx, dx, GAMMA, CFL, n_steps=1_000_000, t=0.0, t_end=T_MID,
+                             precision="f64", rho_floor=1e-6, P_floor=1e-6)
+        return Ud.cpu().numpy(), dx, t
+    except ImportError:
+        return U0, dx, 0.0
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    nz = max(4, min(args.n, int(os.environ.get("BSN_REF_SLAB", "16"))))
-    for _ in range(args.warmup):
-        cpu_reference_rate(args.n, threads, nz, 1)
-    rate, el, _ = cpu_reference_rate(args.n, threads, nz, args.steps)
+    nz = max(4, min(args.n, CPU_SLAB))
+    U, dx, t0 = sedov_mid_state(args.n)
+    log(f"reference arm: Sedov {args.n}^3 state at t={t0:.4g}; oracle on a {nz}-plane slab, {threads} threads")
+    S = cpu_slab(U, args.n, nz)
+    del U
+    if args.warmup:
+        cpu_reference_rate(S.copy(order="F"), args.n, dx, threads, args.warmup)
+    rate, el, _ = cpu_reference_rate(S, args.n, dx, threads, args.steps)
+    sample = (f"{args.steps} RK3 steps (cfl_dt_3d + euler3d_step!) of a {args.n}x{args.n}x{nz} z-slab through "
+              f"the blast centre of Sedov {args.n}^3 at t={t0:.4g}")
     line = {
         "impl": "reference", "metric": METRIC, "value": rate,
         "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (Sedov initial condition)",
-        "config": {"workload": f"sedov{args.n}^3", "path": "reference CPU restatement (oracle), FP64",
-                   "sample": f"{args.n}x{args.n}x{nz} z-slab through the blast centre per step"},
+        "dtype": "f64", "data": "synthetic (Sedov initial condition, sedov_ic_3d!, run to the timed state)",
+        "config": {"workload": f"sedov{args.n}^3", "grid": [args.n, args.n, args.n],
+                   "path": "reference CPU restatement (oracle), FP64", "threads": threads,
+                   "timed_from": f"Sedov state at t={t0:.4g} (FP64 run from the initial condition)",
+                   "sample": sample},
         "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} RK3 steps of a {args.n}x{args.n}x{nz} slab of Sedov {args.n}^3"},
+                         "sample": sample},
         "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -220,14 +282,19 @@ def accuracy(bsn, torch, U0, n, dx, kw, t_end=T_END):
     return out
 
 
-def fmr_polytrope(bsn, torch, steps, warmup, log):
+def fmr_polytrope(bsn, torch, steps, warmup, log, omega_frac=0.0, host_loop=True):
     """Two-level FMR self-gravitating n=1 polytrope (M=1, R=0.5, G=1) in a
     rho=1e-8 atmosphere: 128^3 base on [-2,2]^3, 128^3 fine on [-1,1]^3
-    (ratio 2), isolated FFT Poisson every step.  Times `steps` steps of the
+    (ratio 2), isolated FFT Poisson every step, optionally in rigid rotation
+    at omega_frac of breakup (the driver's overlay,
+    scripts/run_sn50_fiducial.jl:421-446).  Times `steps` steps of the
     device loop (one graph per step, coarse step + first subcycle batched)
     for FP32 and FP64 stencils, and the FP64 host-driven loop (cfl_dt_fmr3d +
-    fmr3d_step per step, one launch per level and stage) beside them.
+    fmr3d_step per step, one launch per level and stage) beside them; then
+    reruns the FP32 path from the initial state to the FP64 run's end time
+    for the L1 density and energy differences on both levels.
     cell-updates/s counts the fine level once per subcycle."""
+    import math
     from bsn import ics
     nc, ratio, gam = 128, 2, 2.0
     dxc = 4.0 / nc
@@ -236,6 +303,9 @@ def fmr_polytrope(bsn, torch, steps, warmup, log):
     U0 = bsn.state(nc, nc, nc)
     ics.polytrope_ic_3d(U0, nc, nc, nc, dxc, dxc, dxc, gam, M_star=1.0, R_star=0.5, x0=-2.0, y0=-2.0, z0=-2.0,
                         **kw)
+    if omega_frac:
+        ics.apply_stellar_rotation(U0, nc, nc, nc, dxc, gam, omega_frac * math.sqrt(1.0 / 0.5 ** 3),
+                                   rho_thresh=2.0 * kw["rho_floor"], x0=-2.0, y0=-2.0)
     bsn.fill_ghost_3d_outflow(U0, nc, nc, nc)
     nf = (hi - lo + 1) * ratio
     units = nc ** 3 + ratio * nf ** 3
@@ -243,22 +313,43 @@ def fmr_polytrope(bsn, torch, steps, warmup, log):
     def grid():
         return bsn.FMRGrid3D(U0.clone(), nc, nc, nc, dxc, lo, hi, lo, hi, lo, hi, ratio, gam, **kw)
 
-    out = {"workload": "polytrope FMR 128^3 + 128^3 (ratio 2), self-gravity", "steps": steps,
-           "unit": "cell-updates/s", "units_per_step": units}
+    out = {"workload": "polytrope FMR 128^3 + 128^3 (ratio 2), self-gravity"
+                       + (f", rigid rotation {omega_frac} of breakup" if omega_frac else ""),
+           "steps": steps, "warmup": warmup, "unit": "cell-updates/s", "units_per_step": units}
+    end = {}
     for prec in ("f32", "f64"):
         G = grid()
-        t, _ = bsn.fmr3d_run_steps(G, 0.4, n_steps=warmup, precision=prec, self_gravity=True)
+        t = 0.0
+        if warmup:
+            t, _ = bsn.fmr3d_run_steps(G, 0.4, n_steps=warmup, precision=prec, self_gravity=True)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        bsn.fmr3d_run_steps(G, 0.4, n_steps=steps, t=t, precision=prec, self_gravity=True)
+        t, _ = bsn.fmr3d_run_steps(G, 0.4, n_steps=steps, t=t, precision=prec, self_gravity=True)
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
         out[f"{prec}_batched_ms_per_step"] = ms
         out[f"{prec}_batched_value"] = units / (ms / 1e3)
+        out[f"{prec}_end_time"] = t
         log(f"FMR polytrope {prec} batched: {ms:.3f} ms/step")
+        if prec == "f64":
+            end["f64"] = (G.Uc.clone(), G.Uf.clone())
         del G
+    # FP32 against FP64 at the FP64 run's end time
+    G = grid()
+    t64 = out["f64_end_time"]
+    _, k = bsn.fmr3d_run_steps(G, 0.4, n_steps=100 * (steps + warmup), t_end=t64, precision="f32", self_gravity=True)
+    a = (slice(3, -3),) * 3
+    for lev, A, B in (("coarse", G.Uc, end["f64"][0]), ("fine", G.Uf, end["f64"][1])):
+        for q, nm in ((0, "rho"), (4, "E")):
+            ref = B[q][a]
+            out[f"f32_L1_{nm}_{lev}_vs_f64"] = float((A[q][a] - ref).abs().sum() / ref.abs().sum())
+    out["accuracy_t"] = t64
+    out["f32_accuracy_steps"] = k
+    del G, end
+    if not host_loop:
+        return out
     G = grid()
     for _ in range(warmup):
         bsn.fmr3d_step(G, bsn.cfl_dt_fmr3d(G, 0.4), self_gravity=True)
@@ -316,6 +407,10 @@ def binary_nested(bsn, torch, steps, warmup, log, n=128, paths=("f64", "f32", "l
         x0, dx = x0 + (lo - 1) * dx, dx / 2
         fill(H0.levels[k + 1], dx, x0)
         H0.pairs[k].prolong_fine_ghosts()
+    # every level holds the restriction of the finer ones (the invariant the
+    # step keeps), so level 0's mass is the composite grid's from the start
+    H0.pairs[1].restrict()
+    H0.pairs[0].restrict()
     dxf = dx
     init = [U.clone() for U in H0.levels]
     del H0
@@ -332,28 +427,38 @@ def binary_nested(bsn, torch, steps, warmup, log, n=128, paths=("f64", "f32", "l
             Ud.copy_(Ui)
         b = [bsn.BlackHole((1.5, 0.0, 0.0), (0.0, v, 0.0), 5.0, 2 * dxf, 1e6, 4 * dxf),
              bsn.BlackHole((-1.5, 0.0, 0.0), (0.0, -v, 0.0), 5.0, 2 * dxf, 1e6, 4 * dxf)]
-        rec = torch.zeros((cap, 12), dtype=torch.float64, device="cuda")
+        rec = torch.zeros((cap, bsn.DIAG_RECORD), dtype=torch.float64, device="cuda")
         common = dict(f_sink=1.0, torque_free=True, self_gravity=True, rho_sink_min=0.0, evolve_orbit=True,
                       precision=prec, diag=rec)
         return H, b, common
 
     t64 = None
+    E_f = {}
     for prec in paths:
         H, b, common = fresh(prec, steps + warmup)
-        t, _ = bsn.coupled_nested_run_steps(H, b, -L, -L, -L, 0.4, n_steps=warmup, **common)
+        t = 0.0
+        if warmup:
+            t, _ = bsn.coupled_nested_run_steps(H, b, -L, -L, -L, 0.4, n_steps=warmup, **common)
+        M_start = float(bsn.diagnostics(H.levels[0], n, n, n, dx0, dx0, dx0, -L, -L, -L, b, g)[9])
+        MBH_start = sum(bh.mass for bh in b)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        t, _ = bsn.coupled_nested_run_steps(H, b, -L, -L, -L, 0.4, n_steps=steps, t=t, **common)
+        t, k = bsn.coupled_nested_run_steps(H, b, -L, -L, -L, 0.4, n_steps=steps, t=t, **common)
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
         out[f"{prec}_device_loop_ms_per_step"] = ms
         out[f"{prec}_device_loop_value"] = units / (ms / 1e3)
-        log(f"binary BH nested {prec}: {ms:.3f} ms/step")
+        out[f"{prec}_end_time"] = t
+        out[f"{prec}_mass_closure"] = mass_closure(common["diag"][k - 1].cpu().numpy(), M_start, MBH_start,
+                                                   sum(bh.mass for bh in b))
+        log(f"binary BH nested {prec}: {ms:.3f} ms/step, mass closure "
+            f"{out[f'{prec}_mass_closure']['gas_residual_rel']:.2e}")
         if prec == "f64":
             t64 = t
             rho_f[prec] = H.levels[2][0].clone()
+            E_f[prec] = H.levels[2][4].clone()
         del H
     # accuracy at equal time: the reduced-precision paths rerun to FP64's end time
     if t64 is None:
@@ -367,11 +472,14 @@ def binary_nested(bsn, torch, steps, warmup, log, n=128, paths=("f64", "f32", "l
                                             **common)
         out[f"{prec}_accuracy_steps"] = k
         rho_f[prec] = H.levels[2][0].clone()
+        E_f[prec] = H.levels[2][4].clone()
         del H
     a = (slice(3, -3),) * 3
     ref = rho_f["f64"][a]
+    refE = E_f["f64"][a]
     for prec in others:
         out[f"{prec}_L1_rho_finest_vs_f64"] = float((rho_f[prec][a] - ref).abs().sum() / ref.abs().sum())
+        out[f"{prec}_L1_E_finest_vs_f64"] = float((E_f[prec][a] - refE).abs().sum() / refE.abs().sum())
         out[f"speedup_{prec}_vs_f64"] = out["f64_device_loop_ms_per_step"] / out[f"{prec}_device_loop_ms_per_step"]
     return out
 
@@ -438,9 +546,11 @@ def coupled_binary(bsn, torch, steps, warmup, log, n=128):
     common = dict(f_sink=1.0, torque_free=True, self_gravity=True, rho_sink_min=0.0, evolve_orbit=True, **kw)
     for prec in ("f32", "f64"):
         U, b = U0.clone(), bhs()
-        rec = torch.zeros((steps + warmup, 12), dtype=torch.float64, device="cuda")
+        rec = torch.zeros((steps + warmup, bsn.DIAG_RECORD), dtype=torch.float64, device="cuda")
         t, _ = bsn.coupled_run_steps(U, b, n, n, n, dx, -L, -L, -L, g, 0.4, n_steps=warmup, precision=prec,
                                      diag=rec, **common)
+        M_start = float(bsn.diagnostics(U, n, n, n, dx, dx, dx, -L, -L, -L, b, g)[9])
+        MBH_start = sum(bh.mass for bh in b)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -451,7 +561,10 @@ def coupled_binary(bsn, torch, steps, warmup, log, n=128):
         ms = e0.elapsed_time(e1) / steps
         out[f"{prec}_device_loop_ms_per_step"] = ms
         out[f"{prec}_device_loop_value"] = n ** 3 / (ms / 1e3)
-        log(f"binary BH {prec} device loop: {ms:.3f} ms/step")
+        out[f"{prec}_mass_closure"] = mass_closure(rec[steps - 1].cpu().numpy(), M_start, MBH_start,
+                                                   sum(bh.mass for bh in b))
+        log(f"binary BH {prec} device loop: {ms:.3f} ms/step, mass closure "
+            f"{out[f'{prec}_mass_closure']['gas_residual_rel']:.2e}")
     U, b = U0.clone(), bhs()
     t = 0.0
     for k in range(warmup + steps):
@@ -629,11 +742,13 @@ def run_bsn(args, rank, world):
 
     cpu = None
     if rank == 0 and not args.no_cpu:
+        # the same sample as the reference arm: the timed state's slab, all threads
         threads = os.cpu_count() or 1
-        nz = min(n, 32)
-        rate, el, k = cpu_reference_rate(n, threads, nz, 1, min_seconds=12.0)
+        nz = max(4, min(n, CPU_SLAB))
+        rate, el, k = cpu_reference_rate(cpu_slab(U_mid, n, nz), n, dx, threads, 1, min_seconds=12.0)
         cpu = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-               "sample": f"{k} RK3 steps (oracle, FP64) of a {n}x{n}x{nz} z-slab of Sedov {n}^3, {el:.1f} s"}
+               "sample": f"{k} RK3 steps (cfl_dt_3d + euler3d_step!, oracle, FP64) of a {n}x{n}x{nz} z-slab "
+                         f"through the blast centre of Sedov {n}^3 at t={t_mid:.4g}, {el:.1f} s"}
     if rank == 0:
         desc = {"f32": "FP32 stencils/fluxes, FP64 state and RK3 accumulation",
                 "f64": "FP64, bit-identical to the reference CPU path",
@@ -691,8 +806,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-fmr", action="store_true",
                     help="skip the two-level FMR polytrope and binary-BH coupled-loop timings")
-    ap.add_argument("--workload", default="sedov", choices=["sedov", "binary_nested"],
-                    help="binary_nested: time only the binary-BH supernova on three nested FMR levels")
+    ap.add_argument("--workload", default="sedov", choices=["sedov", "binary_nested", "polytrope_fmr"],
+                    help="binary_nested: time only the binary-BH supernova on three nested FMR levels; "
+                         "polytrope_fmr: only the two-level self-gravitating polytrope")
+    ap.add_argument("--full", action="store_true",
+                    help="with --workload: run the workload's stated length from its initial state (polytrope "
+                         "200 steps, binary 1000 steps, no warm-up) instead of --steps")
+    ap.add_argument("--omega", type=float, default=0.0,
+                    help="--workload polytrope_fmr: rigid rotation as a fraction of breakup (e.g. 0.2)")
     ap.add_argument("--paths", default="f64,f32,learned",
                     help="stencil paths of --workload binary_nested (comma-separated)")
     ap.add_argument("--tile", type=int, default=-1,
@@ -703,11 +824,17 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.workload == "binary_nested":
+    if args.workload in ("binary_nested", "polytrope_fmr"):
         import torch
         import bsn
-        paths = tuple(p_ for p_ in args.paths.split(",") if p_)
-        out = binary_nested(bsn, torch, args.steps, args.warmup, log, paths=paths)
+        if args.workload == "binary_nested":
+            paths = tuple(p_ for p_ in args.paths.split(",") if p_)
+            steps, warmup = (1000, 0) if args.full else (args.steps, args.warmup)
+            out = binary_nested(bsn, torch, steps, warmup, log, paths=paths)
+        else:
+            steps, warmup = (200, 0) if args.full else (args.steps, args.warmup)
+            out = fmr_polytrope(bsn, torch, steps, warmup, log, omega_frac=args.omega, host_loop=not args.full)
+        out["full_length"] = bool(args.full)
         print(json.dumps(out), flush=True)
         return
     if world > 1:

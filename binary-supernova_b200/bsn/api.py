@@ -32,7 +32,7 @@ __all__ = [
     "apply_sg_force_level", "apply_sg_force_slab", "coupled_step", "FMRGrid3D", "fmr3d_step", "cfl_dt_fmr3d", "solve_fmr_poisson",
     "restrict_density_to_coarse", "FMRHierarchy3D", "fmr_nested_step", "cfl_dt_fmr_nested",
     "fmr_nested_run_steps", "coupled_nested_run_steps", "rotating_frame_source", "relax_damping_source",
-    "relax_ic",
+    "relax_ic", "DIAG_FIELDS", "DIAG_RECORD",
 ]
 
 # ---------------------------------------------------------------------------
@@ -337,16 +337,37 @@ def coupled_step(U, bhs, dt, t, nx, ny, nz, dx, x0, y0, z0, gamma, f_sink, rho_f
     return np.array(Fg[: 3 * len(bhs)]).reshape(len(bhs), 3)
 
 
+# The per-step record of the device driver loops (coupled_run_steps,
+# coupled_nested_run_steps): t, dt, the driver's diagnostics, and the mass
+# ledger since the start of the call -- mass added by the floors, mass that
+# left through the domain boundary, mass the sink sources drained from the
+# gas, mass accrete! credited to the BHs.  The gas mass closes as
+#   M_gas(t) = M_gas(0) + floors_in - outflow - drained
+# and the BHs gain `accreted`, which accrete! takes from the end-of-step
+# state while the sources drain the gas stage by stage (src/sinks.jl:74-109
+# against src/gpu_kernels.jl:238-284): accreted - drained is the reference's
+# own bookkeeping difference, not a loss of the update.
+DIAG_FIELDS = ("t", "dt", "E_gas", "KE_gas", "Px", "Py", "Pz", "Lx", "Ly", "Lz", "M_bound", "M_gas",
+               "floors_in", "outflow", "drained", "accreted")
+DIAG_RECORD = len(DIAG_FIELDS)
+
+
+def _check_diag(diag):
+    if diag is not None and not (diag.is_cuda and diag.dtype == torch.float64 and diag.is_contiguous()
+                                 and diag.dim() == 2 and diag.shape[1] == DIAG_RECORD):
+        raise TypeError(f"diag must be a contiguous CUDA float64 tensor of shape (cap, {DIAG_RECORD})")
+
+
 def coupled_run_steps(U, bhs, nx, ny, nz, dx, x0, y0, z0, gamma, cfl, *, n_steps, t=0.0, t_end=0.0, dt_max=0.0,
                       f_sink=1.0, rho_floor=0.0, P_floor=0.0, torque_free=True, self_gravity=False,
                       t_bh2_sink_on=0.0, rho_sink_min=0.0, evolve_orbit=True, precision="f64", diag=None):
     """The coupled_step! driver loop on the device (one CUDA graph per step);
     returns (t, steps) and updates `bhs` in place.  diag: optional CUDA float64
-    tensor (cap, 12) receiving {t, dt, diagnostics(...)} after every step."""
+    tensor (cap, DIAG_RECORD) receiving after every step the record
+    {t, dt, diagnostics(...) [10 values], mass ledger [4 values]} (see
+    DIAG_FIELDS; the ledger totals count from the start of this call)."""
     _check_state(U, nx, ny, nz)
-    if diag is not None and not (diag.is_cuda and diag.dtype == torch.float64 and diag.is_contiguous()
-                                 and diag.dim() == 2 and diag.shape[1] == 12):
-        raise TypeError("diag must be a contiguous CUDA float64 tensor of shape (cap, 12)")
+    _check_diag(diag)
     arr = _bh_array(bhs)
     tt = C.c_double(float(t))
     nd = C.c_int(0)
@@ -504,10 +525,9 @@ def coupled_nested_run_steps(H: FMRHierarchy3D, bhs, x0, y0, z0, cfl, *, n_steps
     """The coupled_step! driver loop on nested FMR levels, on the device (one
     CUDA graph per level-0 step); returns (t, steps) and updates `bhs` in
     place.  x0, y0, z0: lower corner of level 0.  diag: optional CUDA float64
-    tensor (cap, 12) receiving {t, dt, diagnostics of level 0} per step."""
-    if diag is not None and not (diag.is_cuda and diag.dtype == torch.float64 and diag.is_contiguous()
-                                 and diag.dim() == 2 and diag.shape[1] == 12):
-        raise TypeError("diag must be a contiguous CUDA float64 tensor of shape (cap, 12)")
+    tensor (cap, DIAG_RECORD) receiving per step {t, dt, diagnostics of level 0,
+    mass ledger of the composite grid} (see DIAG_FIELDS)."""
+    _check_diag(diag)
     arr = _bh_array(bhs)
     tt = C.c_double(float(t))
     nd = C.c_int(0)

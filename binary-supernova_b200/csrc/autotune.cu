@@ -54,6 +54,7 @@ bsn_status stage_autotune(bsn_ctx* ctx, int prec, const f64::StageArgs& probe, d
     a.F[0] = a.F[1] = a.F[2] = nullptr;
     a.dt_dev = nullptr;
     a.done_dev = nullptr;
+    a.ledger = nullptr;
     cudaEvent_t e0, e1;
     BSN_CUDA(ctx, cudaEventCreate(&e0));
     BSN_CUDA(ctx, cudaEventCreate(&e1));

@@ -31,12 +31,21 @@ struct Dev {
     double Fg[3 * MAXBH];
     f64::BHSrc bsrc;
     f64::SinkSrc ssrc;
+    // mass ledger: per-stage sums of the step being taken, per level (the
+    // stage kernels add, f64_ledger_fold clears), and the totals since the
+    // start of the call (f64::LEDT_*)
+    double led[f64::MAXLEV][3][f64::LED_TERMS];
+    double led_tot[f64::LEDT_COUNT];
 };
 
 __global__ void init_kernel(Dev* r, double t, const bsn_bh* bhs, int nbh) {
     r->dt = 0.0; r->t = t; r->smax = 0ull; r->nanflag = 0u; r->done = 0; r->steps = 0; r->nbh = nbh;
     for (int i = 0; i < nbh; ++i) r->bh[i] = bhs[i];
     for (int i = 0; i < 3 * MAXBH; ++i) r->Fg[i] = 0.0;
+    for (int l = 0; l < f64::MAXLEV; ++l)
+        for (int s = 0; s < 3; ++s)
+            for (int q = 0; q < f64::LED_TERMS; ++q) r->led[l][s][q] = 0.0;
+    for (int q = 0; q < f64::LEDT_COUNT; ++q) r->led_tot[q] = 0.0;
 }
 
 // dt = cfl / max speed (Inf for NaN or zero), capped by dt_max > 0, clamped to t_end > 0.
@@ -235,6 +244,7 @@ __global__ void accrete_kernel(const double* U, int nx, int ny, int nz, double d
     if (threadIdx.x != 0) return;
     const double dm = v[0];
     if (dm > 0.0) {
+        r->led_tot[f64::LEDT_ACCRETED] += dm;
         double M_new = bh.mass + dm;
         bh.vel[0] = (bh.mass * bh.vel[0] + v[1]) / M_new;
         bh.vel[1] = (bh.mass * bh.vel[1] + v[2]) / M_new;
@@ -391,8 +401,11 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
                     a.phi = phi; a.use_sg = 1;
                 }
                 if (s == 2) { a.cfl_max = &r->smax; a.cfl_nan = &r->nanflag; }
+                a.ledger = &r->led[0][s][0];
+                a.led_bnd = 1;
                 BSN_TRY(stage_launch(ctx, precision, a));
             }
+            BSN_TRY(f64_ledger_fold(ctx, &r->led[0][0][0], r->led_tot, &r->dt, &r->done));
             BSN_TRY(f64_ghost_combine(ctx, U, B, nullptr, nx, ny, nz, BSN_BC_OUTFLOW, 0.0, &r->dt, &r->done));
             for (int i = 0; i < nbh; ++i) {
                 accrete_kernel<<<1, 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dx, dx, x0, y0, z0, r, i, f_sink,
@@ -403,7 +416,7 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
             BSN_TRY(launch_check(ctx, "coupled_advance_kernel"));
             if (diag_out)   // the driver's diagnostics of the end-of-step state (BHs after accretion)
                 BSN_TRY(diag::launch(ctx, U, nx, ny, nz, dx, dx, dx, x0, y0, z0, r->bh, &r->nbh, nbh, gamma, dpart,
-                                     diag_out, &r->t, &r->dt, &r->steps, &r->done, diag_cap));
+                                     diag_out, &r->t, &r->dt, &r->steps, &r->done, diag_cap, r->led_tot));
             return BSN_OK;
         };
         bsn_status cst = body();
@@ -513,7 +526,9 @@ extern "C" bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2*
         f64::StageArgs& a = plan.base[l];
         a.x0 = ox[l]; a.y0 = oy[l]; a.z0 = oz[l];
         if (nbh > 0) { a.use_bh = 1; a.bh_dev = &r->bsrc; a.use_sink = 1; a.sk_dev = &r->ssrc; }
+        plan.led_raw[l] = &r->led[l][0][0];
     }
+    plan.led_tot = r->led_tot;
     if (self_gravity) {
         const NLevel& v = plan.L[0];
         if (precision == PREC_F64) BSN_TRY(poisson_prepare(ctx, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz));
@@ -604,7 +619,8 @@ extern "C" bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2*
             if (diag_out) {
                 const NLevel& v = plan.L[0];
                 BSN_TRY(diag::launch(ctx, v.U, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz, x0, y0, z0, r->bh, &r->nbh, nbh,
-                                     plan.gamma, dpart, diag_out, &r->t, &r->dt, &r->steps, &r->done, diag_cap));
+                                     plan.gamma, dpart, diag_out, &r->t, &r->dt, &r->steps, &r->done, diag_cap,
+                                     r->led_tot));
             }
             return BSN_OK;
         };

@@ -71,7 +71,7 @@ __global__ void diag_kernel(const double* U, int nx, int ny, int nz, double dx, 
 // totals times dV -> out[0..NDIAG); with the device loop's counters, the
 // record {t, dt, totals} at index steps - 1 when it is below cap.
 __global__ void diag_finish(const double* part, int nblocks, double dV, double* out, const double* t,
-                            const double* dt, const int* steps, const int* done, int cap) {
+                            const double* dt, const int* steps, const int* done, int cap, const double* ledger) {
     if (done && *done) return;
     const int q = threadIdx.x;
     if (q >= NDIAG || blockIdx.x != 0) return;
@@ -81,20 +81,21 @@ __global__ void diag_finish(const double* part, int nblocks, double dV, double* 
     if (!steps) { out[q] = v; return; }
     const int k = *steps - 1;
     if (k < 0 || k >= cap) return;
-    double* rec = out + (long long)(NDIAG + 2) * k;
+    double* rec = out + (long long)NREC * k;
     if (q == 0) { rec[0] = *t; rec[1] = *dt; }
     rec[2 + q] = v;
+    if (q < f64::LEDT_COUNT) rec[2 + NDIAG + q] = ledger ? ledger[q] : 0.0;
 }
 
 bsn_status launch(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx, double dy, double dz, double x0,
                   double y0, double z0, const bsn_bh* bhs_dev, const int* nbh_dev, int nbh, double gamma,
                   double* part, double* out, const double* t, const double* dt, const int* steps, const int* done,
-                  int cap) {
+                  int cap, const double* ledger) {
     prof_begin(ctx);
     diag_kernel<<<BLOCKS, 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, bhs_dev, nbh_dev, nbh, gamma,
                                                  done, part);
     BSN_TRY(launch_check(ctx, "diag_kernel"));
-    diag_finish<<<1, 32, 0, ctx->stream>>>(part, BLOCKS, dx * dy * dz, out, t, dt, steps, done, cap);
+    diag_finish<<<1, 32, 0, ctx->stream>>>(part, BLOCKS, dx * dy * dz, out, t, dt, steps, done, cap, ledger);
     return launch_check(ctx, "diag_finish");
 }
 

@@ -81,7 +81,14 @@ struct NPlan {
     int qn = 0;
     double rho_floor = 0, P_floor = 0, gamma = 0;
     int bc = 0;
+    // optional mass ledger of the composite grid: per level the per-stage
+    // sums of the substep being taken (3 x LED_TERMS doubles, device), and
+    // the cumulative totals (LEDT_COUNT doubles, device).  Each level counts
+    // its cells outside its child's region; level 0 also its boundary faces.
+    double* led_raw[NMAXL] = {nullptr, nullptr, nullptr, nullptr};
+    double* led_tot = nullptr;
 
+    LedBox covered(int l) const;    // level l's cells that level l+1 covers (none for the finest)
     bsn_status chain(int l, double alpha);
     bsn_status gravity();
     bsn_status step();

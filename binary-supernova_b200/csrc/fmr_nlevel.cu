@@ -74,6 +74,16 @@ __global__ void n_advance_kernel(NDev* d) {
 
 const double kRkW[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
 
+LedBox NPlan::covered(int l) const {
+    LedBox b;
+    if (l < nl - 1)
+        for (int d = 0; d < 3; ++d) {
+            b.lo[d] = P[l].G.lo[d] - 1;
+            b.hi[d] = P[l].G.hi[d];
+        }
+    return b;
+}
+
 bsn_status NPlan::chain(int l, double alpha) {
     // substep starts of levels l..nl-1: saved states and fresh registers
     for (int k = l; k < nl - 1; ++k) {
@@ -101,6 +111,12 @@ bsn_status NPlan::chain(int l, double alpha) {
             a.Uin = in[s]; a.Un = L[k].U; a.Uout = out[s];
             set_stage(a, s + 1, 0.0);
             a.reg.wt = kRkW[s];
+            if (led_raw[k]) {
+                a.ledger = led_raw[k] + f64::LED_TERMS * s;
+                a.led_bnd = k == 0;
+                const LedBox cv = covered(k);
+                for (int d = 0; d < 3; ++d) { a.led_skip_lo[d] = cv.lo[d]; a.led_skip_hi[d] = cv.hi[d]; }
+            }
         }
         if (nb == 1) {
             BSN_TRY(stage_launch(ctx, prec, B.lv[0]));
@@ -118,6 +134,8 @@ bsn_status NPlan::chain(int l, double alpha) {
         }
     }
     for (int k = l; k < nl; ++k)
+        if (led_raw[k]) BSN_TRY(f64_ledger_fold(ctx, led_raw[k], led_tot, &d->dt[k], done));
+    for (int k = l; k < nl; ++k)
         BSN_TRY(f64_ghost_combine(ctx, L[k].U, k == 0 ? L[0].B : nullptr, k == 0 ? nullptr : L[k].Gh, L[k].nx,
                                   L[k].ny, L[k].nz, bc, 0.0, &d->dt[k], done));
     // unwind: the remaining substeps of each child, deepest first, then
@@ -129,7 +147,9 @@ bsn_status NPlan::chain(int l, double alpha) {
         bc_correct_kernel<<<grid1d(P[k].ncorr, 128), 128, 0, ctx->stream>>>(
             P[k].G, P[k].Rc, P[k].Rf, L[k].U, 1.0 / L[k].dx, 1.0 / L[k].dy, 1.0 / L[k].dz, done);
         BSN_TRY(launch_check(ctx, "bc_correct_kernel"));
-        BSN_TRY(f64_floors(ctx, L[k].U, L[k].nx, L[k].ny, L[k].nz, rho_floor, P_floor, gamma, done));
+        BSN_TRY(f64_floors(ctx, L[k].U, L[k].nx, L[k].ny, L[k].nz, rho_floor, P_floor, gamma, done,
+                           led_tot ? led_tot + f64::LEDT_FLOORS : nullptr, covered(k),
+                           L[k].dx * L[k].dy * L[k].dz));
     }
     return BSN_OK;
 }

@@ -80,8 +80,11 @@ __global__ void ghost_combine_kernel(double* U, const double* S, const double* G
     for (int q = 0; q < 5; ++q) U[dst + q] = (1.0 / 3.0) * U[dst + q] + (2.0 / 3.0) * src[so + q] + cz;
 }
 
+// led (may be null): the floors' change of rho dV on the cells outside the
+// half-open box [lo, hi) is added there (mass ledger).
 __global__ void floors_kernel(double* U, int nx, int ny, int nz, double rho_floor, double P_floor, double Pfl_gm1,
-                              double gm1, const int* done) {
+                              double gm1, const int* done, double* led = nullptr, LedBox skip = LedBox{},
+                              double dV = 0.0) {
     if (done && *done) return;
     Geom G(nx, ny, nz);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -92,9 +95,31 @@ __global__ void floors_kernel(double* U, int nx, int ny, int nz, double rho_floo
     double v[5];
 #pragma unroll
     for (int q = 0; q < 5; ++q) v[q] = U[o + q];
+    const double rho0 = v[0];
     apply_floor(v[0], v[1], v[2], v[3], v[4], rho_floor, P_floor, Pfl_gm1, gm1);
 #pragma unroll
     for (int q = 0; q < 5; ++q) U[o + q] = v[q];
+    if (led && v[0] != rho0 && !skip.has(a, b, c)) atomicAdd(led, (v[0] - rho0) * dV);
+}
+
+// Mass ledger of one SSP-RK3 step (or substep) from its per-stage sums raw[3]
+// [LED_TERMS] (stage_tile.cuh): a change to stage s's result reaches the
+// step's result with the weight the later combines give it -- the stage-1
+// right-hand side and result 0.25 * 2/3, stage 2's 2/3, stage 3's 1 (times
+// dt for the right-hand sides, whose stage coefficients are dt, dt/4 and
+// 2dt/3) -- and the input floors of stages 2 and 3 the weights of the stage
+// results they alter.  Adds into tot[LEDT_*] and clears raw.
+__global__ void ledger_fold_kernel(double* raw, double* tot, const double* dt_dev, const int* done) {
+    if ((done && *done) || threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double dt = *dt_dev, c1 = 0.25 * (2.0 / 3.0), c3 = 2.0 / 3.0;
+    double(*r)[f64::LED_TERMS] = reinterpret_cast<double(*)[f64::LED_TERMS]>(raw);
+    using namespace f64;
+    tot[LEDT_FLOORS] += ((c1 * r[0][LED_POST] + c1 * r[1][LED_PRE]) + (c3 * r[1][LED_POST] + c3 * r[2][LED_PRE])) +
+                        r[2][LED_POST];
+    tot[LEDT_OUTFLOW] -= dt * ((c1 * r[0][LED_BND] + c1 * r[1][LED_BND]) + c3 * r[2][LED_BND]);
+    tot[LEDT_DRAINED] += dt * ((c1 * r[0][LED_DRAIN] + c1 * r[1][LED_DRAIN]) + c3 * r[2][LED_DRAIN]);
+    for (int s = 0; s < 3; ++s)
+        for (int q = 0; q < LED_TERMS; ++q) r[s][q] = 0.0;
 }
 
 // cfl_dt_3d speeds folded into a device max (src/gpu_kernels.jl:174-191).
@@ -144,12 +169,17 @@ bsn_status f64_fill_ghosts(bsn_ctx* ctx, double* U, int nx, int ny, int nz, int 
 }
 
 bsn_status f64_floors(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double rho_floor, double P_floor, double gamma,
-                      const int* done_dev) {
+                      const int* done_dev, double* led, LedBox skip, double dV) {
     double gm1 = gamma - 1.0;
     prof_begin(ctx);
-    floors_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(U, nx, ny, nz, rho_floor, P_floor,
-                                                                                   P_floor / gm1, gm1, done_dev);
+    floors_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(
+        U, nx, ny, nz, rho_floor, P_floor, P_floor / gm1, gm1, done_dev, led, skip, dV);
     return launch_check(ctx, "floors_kernel");
+}
+
+bsn_status f64_ledger_fold(bsn_ctx* ctx, double* raw, double* tot, const double* dt_dev, const int* done_dev) {
+    ledger_fold_kernel<<<1, 32, 0, ctx->stream>>>(raw, tot, dt_dev, done_dev);
+    return launch_check(ctx, "ledger_fold_kernel");
 }
 
 bsn_status f64_ghost_combine(bsn_ctx* ctx, double* U, const double* S, const double* Gh, int nx, int ny, int nz,

@@ -12,8 +12,20 @@ namespace bsn {
 
 bsn_status check_dims(bsn_ctx* ctx, int nx, int ny, int nz);
 bsn_status f64_fill_ghosts(bsn_ctx* ctx, double* U, int nx, int ny, int nz, int bc);
+// Cells of a half-open box [lo, hi) of active indices (lo = hi: none).
+struct LedBox {
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    __host__ __device__ bool has(int a, int b, int c) const {
+        return a >= lo[0] && a < hi[0] && b >= lo[1] && b < hi[1] && c >= lo[2] && c < hi[2];
+    }
+};
+// apply_floors_3d! on the active cells; with led, the floors' change of the
+// mass outside `skip` (rho dV, dV the cell volume) is added to *led.
 bsn_status f64_floors(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double rho_floor, double P_floor, double gamma,
-                      const int* done_dev = nullptr);
+                      const int* done_dev = nullptr, double* led = nullptr, LedBox skip = LedBox{}, double dV = 0.0);
+// Fold one RK3 step's per-stage mass-ledger sums raw[3][LED_TERMS] into the
+// cumulative totals tot[LEDT_COUNT] with the step's dt (hydro_f64.cu).
+bsn_status f64_ledger_fold(bsn_ctx* ctx, double* raw, double* tot, const double* dt_dev, const int* done_dev);
 bsn_status f64_ghost_combine(bsn_ctx* ctx, double* U, const double* S, const double* Gh, int nx, int ny, int nz,
                              int bc, double dt, const double* dt_dev = nullptr, const int* done_dev = nullptr);
 void stage_args_init(f64::StageArgs& A, int nx, int ny, int nz, double dx, double dy, double dz, double gamma, int bc,

@@ -74,7 +74,24 @@ struct StageArgs {
     // velocity damping over damp_t (damp_inv_td = 1 / damp_t) toward rotation at damp_omega
     int use_rot, use_damp;
     double rot_omega, damp_t, damp_inv_td, damp_omega;
+    // mass ledger (null: off).  Four sums of rho dV for this stage, added
+    // with atomics: [LED_BND] mass flux into the grid through its own
+    // boundary faces per unit time (counted when led_bnd != 0, i.e. the grid's
+    // boundary is the domain's), [LED_DRAIN] the sink drain rho / t_sink per
+    // unit time, [LED_POST] the change made by the floors after the combine,
+    // [LED_PRE] the change the floors made to the stage input where the
+    // combine uses it (stages 2 and 3).  Cells in [led_skip_lo, led_skip_hi)
+    // (a finer level's region, overwritten by its restriction) are not counted.
+    double* ledger;
+    int led_bnd;
+    int led_skip_lo[3], led_skip_hi[3];
 };
+
+enum { LED_BND = 0, LED_DRAIN = 1, LED_POST = 2, LED_PRE = 3, LED_TERMS = 4 };
+// cumulative mass-ledger totals of a driver loop (rho dV): mass added by the
+// floors, mass that left through the domain boundary, mass the sink sources
+// drained from the gas, mass the sinks' accrete! credited to the BHs
+enum { LEDT_FLOORS = 0, LEDT_OUTFLOW = 1, LEDT_DRAINED = 2, LEDT_ACCRETED = 3, LEDT_COUNT = 4 };
 
 // Centre of active cell (a, b, c) (0-based): x0 + (i - ng - 0.5) dx with
 // i = a + 1 + ng (src/gravity_bh.jl:63-65).

@@ -135,7 +135,7 @@ __device__ __forceinline__ void cross_cell(int e, int a0, int b0, int c0, const 
 template <class P, int TX, int TY, int TZ, int NT, int D>
 __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::Consts& k, int a0, int b0, int c0,
                       typename P::real* sC, typename P::real* sF, unsigned char* psm,
-                      double (&acc)[Shape<TX, TY, TZ>::NCELL / NT][5], bool quiet_cross) {
+                      double (&acc)[Shape<TX, TY, TZ>::NCELL / NT][5], bool quiet_cross, double* sled) {
     constexpr bool CROSS = P::kCross;
     using S = Shape<TX, TY, TZ>;
     using real = typename P::real;
@@ -238,6 +238,11 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
                 }
             }
         }
+        if (A.ledger && A.led_bnd && (gd == 0 || gd == n[D])) {   // mass through the grid's boundary
+            // per unit volume, as the divergence sees it (the flush multiplies by dV)
+            const double inv = (D == 0) ? A.idx : (D == 1 ? A.idy : A.idz);
+            atomicAdd(&sled[f64::LED_BND], (gd == 0 ? (double)F[0] : -(double)F[0]) * inv);
+        }
         if (A.use_bnd && (gd == 0 || gd == n[D])) {
             int ta = (D == 0) ? gb : ga, tb = (D == 2) ? gb : gc;
             int n1 = (D == 0) ? G.ny : G.nx;
@@ -333,6 +338,13 @@ __device__ __forceinline__ unsigned char* policy_smem(unsigned char* smem_raw) {
     return smem_raw + ((sizeof(typename P::real) * (P::kCols * NST + 5 * S::NFACE) + 15) / 16) * 16;
 }
 
+// Whether active cell (a, b, c) counts in the mass ledger: outside the
+// region a finer level covers (half-open [led_skip_lo, led_skip_hi)).
+__device__ __forceinline__ bool led_counted(const f64::StageArgs& A, int a, int b, int c) {
+    return !(a >= A.led_skip_lo[0] && a < A.led_skip_hi[0] && b >= A.led_skip_lo[1] && b < A.led_skip_hi[1] &&
+             c >= A.led_skip_lo[2] && c < A.led_skip_hi[2]);
+}
+
 // One RK3 stage (or euler3d_rhs!) of the TX x TY x TZ block at active
 // origin (a0, b0, c0): three sweeps, sources, combine, floors, CFL fold.
 // Starts with a barrier (the first sweep's), so a CTA may call it for one
@@ -353,6 +365,8 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
     const typename P::Consts k = P::consts(A);
     unsigned char* psm = policy_smem<P, TX, TY, TZ>(smem_raw);
     double acc[CPT][5];
+    __shared__ double sled[f64::LED_TERMS];   // this block's mass-ledger sums (A.ledger)
+    if (A.ledger && tid < f64::LED_TERMS) sled[tid] = 0.0;   // ordered before use by the staging barriers
     if constexpr (P::kCross) {
         // the block and the halos of all three sweeps, staged once (floors in
         // FP64 on active cells, ghosts raw, pressure once per cell)
@@ -406,9 +420,9 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
             }
         }
     }
-    sweep<P, TX, TY, TZ, NT, 0>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[0]);
-    sweep<P, TX, TY, TZ, NT, 1>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[1]);
-    sweep<P, TX, TY, TZ, NT, 2>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[2]);
+    sweep<P, TX, TY, TZ, NT, 0>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[0], sled);
+    sweep<P, TX, TY, TZ, NT, 1>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[1], sled);
+    sweep<P, TX, TY, TZ, NT, 2>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[2], sled);
 
     const double dt = A.dt_dev ? *A.dt_dev : A.dt;
     const f64::BHSrc& BH = A.bh_dev ? *A.bh_dev : A.bh;     // kernel parameters are __grid_constant__
@@ -474,6 +488,7 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
                 if (rr < SK.rs[nb]) {
                     double ts = SK.ts[nb];
                     d[0] -= u0 / ts;
+                    if (A.ledger && led_counted(A, a, b, c)) atomicAdd(&sled[f64::LED_DRAIN], u0 / ts);
                     if (SK.torque_free) {
                         double rx = ddx / rr, ry = ddy / rr, rz = ddz / rr;
                         double vx = u1 / u0, vy = u2 / u0, vz = u3 / u0;
@@ -512,7 +527,17 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
 #pragma unroll
             for (int q = 0; q < 5; ++q) w[q] = (1.0 / 3.0) * un[q] + (2.0 / 3.0) * uu[q] + cdt * d[q];
         }
-        P::floor(w, A);
+        if (A.ledger && led_counted(A, a, b, c)) {
+            const double w0 = w[0];
+            P::floor(w, A);
+            if (w[0] != w0) atomicAdd(&sled[f64::LED_POST], w[0] - w0);
+            if (A.stage > 1) {   // the input's floors reach the combine in stages 2 and 3
+                const double raw = A.Uin[off];
+                if (u0 != raw) atomicAdd(&sled[f64::LED_PRE], u0 - raw);
+            }
+        } else {
+            P::floor(w, A);
+        }
 #pragma unroll
         for (int q = 0; q < 5; ++q) A.Uout[off + q] = w[q];
         if (A.cfl_max) {
@@ -531,6 +556,10 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
             atomicMax(A.cfl_max, (unsigned long long)__double_as_longlong(m));
             if (nanflag) atomicOr(A.cfl_nan, 1u);
         }
+    }
+    if (A.ledger) {
+        __syncthreads();   // every cell's and face's contribution is in sled
+        if (tid < f64::LED_TERMS && sled[tid] != 0.0) atomicAdd(&A.ledger[tid], sled[tid] * (A.dx * A.dy * A.dz));
     }
 }
 

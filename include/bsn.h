@@ -312,9 +312,17 @@ bsn_status bsn_coupled_step_f64(bsn_ctx* ctx, double* U, bsn_bh* bhs, int nbh, d
  * bhs: host in/out.  precision: BSN_PREC_* stencils (sources, orbits and
  * accretion FP64); FP32 transforms for self-gravity unless BSN_PREC_F64.
  * *t_inout: start time in, final out; *steps_done (may be NULL).  diag_out
- * (device, may be NULL): after every step k < diag_cap the record
- * {t, dt, the 10 values of bsn_diagnostics_f64} at diag_out + 12 k, reduced
- * on the device (no per-step copy to the host). */
+ * (device, may be NULL): after every step k < diag_cap the record of
+ * BSN_DIAG_RECORD doubles {t, dt, the 10 values of bsn_diagnostics_f64, the
+ * mass ledger} at diag_out + BSN_DIAG_RECORD k, reduced on the device (no
+ * per-step copy to the host).  The mass ledger, FP64 totals since the start
+ * of the call: [12] mass the floors added, [13] mass that left through the
+ * domain boundary, [14] mass the sink sources drained from the gas, [15]
+ * mass accrete! credited to the BHs; the gas mass [11] closes as
+ * M_gas(0) + [12] - [13] - [14].  [15] - [14] is the reference's own
+ * difference between accrete! (end-of-step state, src/sinks.jl:74-109) and
+ * the stage drain (src/gpu_kernels.jl:238-284). */
+enum { BSN_DIAG_RECORD = 16 };
 bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs, int nbh, int nx, int ny, int nz,
                                  double dx, double x0, double y0, double z0, double gamma, double cfl,
                                  double dt_max, double f_sink, double rho_floor, double P_floor,
@@ -333,7 +341,10 @@ bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs, int nbh, 
  * pairs: as bsn_fmr_nested_step_f64 (gamma, floors from pairs[0]); x0,y0,z0:
  * lower corner of level 0 (each finer level starts at the lower face of its
  * parent's cell ci_lo).  diag_out records are the diagnostics of level 0,
- * which holds the restriction of the finer levels. */
+ * which holds the restriction of the finer levels, with the mass ledger of
+ * the composite grid (each level counts the cells its child does not cover;
+ * level 0 the domain boundary).  Start from levels that hold the restriction
+ * of their children for the ledger to close from the first step. */
 bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, bsn_bh* bhs, int nbh,
                                         double x0, double y0, double z0, double cfl, double dt_max,
                                         double f_sink, int torque_free, int self_gravity, double t_bh2_sink_on,

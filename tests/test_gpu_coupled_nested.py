@@ -91,7 +91,7 @@ def test_nested_coupled_t_end_diagnostics_and_fp32(orc, bsn):
     # five steps in all
     t_end = H.cfl_dt(0.4) + 4e-4
     kw = dict(n_steps=1000, t_end=t_end, f_sink=1.0, rho_sink_min=2e-8, self_gravity=True)
-    rec = torch.zeros((8, 12), dtype=torch.float64, device="cuda")
+    rec = torch.zeros((8, bsn.DIAG_RECORD), dtype=torch.float64, device="cuda")
     t64, n64 = bsn.coupled_nested_run_steps(H64, b64, x0, x0, x0, 0.4, diag=rec, **kw)
     t32, n32 = bsn.coupled_nested_run_steps(H32, b32, x0, x0, x0, 0.4, precision="f32", **kw)
     assert t64 == t_end and t32 == t_end and n64 >= 3
@@ -99,7 +99,7 @@ def test_nested_coupled_t_end_diagnostics_and_fp32(orc, bsn):
     n0 = H64.dims[0][0]
     dx0 = 8.0 / n0
     end = bsn.diagnostics(H64.levels[0], n0, n0, n0, dx0, dx0, dx0, x0, x0, x0, b64, 4 / 3)
-    assert R[n64 - 1, 0] == t64 and np.array_equal(R[n64 - 1, 2:], end) and np.all(R[n64:] == 0.0)
+    assert R[n64 - 1, 0] == t64 and np.array_equal(R[n64 - 1, 2:12], end) and np.all(R[n64:] == 0.0)
     a = (0,) + (slice(NG, -NG),) * 3
     for A, B in zip(H32.levels, H64.levels):
         A, B = host(A)[a], host(B)[a]

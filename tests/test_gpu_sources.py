@@ -274,14 +274,14 @@ def test_coupled_run_steps_records_diagnostics(orc, bsn):
     U, dx, x0, specs = binary_setup(orc, n=32)
     Ud = dev(U)
     bg = _bhs(bsn, specs)
-    rec = torch.zeros((4, 12), dtype=torch.float64, device="cuda")
+    rec = torch.zeros((4, bsn.DIAG_RECORD), dtype=torch.float64, device="cuda")
     t, n = bsn.coupled_run_steps(Ud, bg, 32, 32, 32, dx, x0, x0, x0, 4 / 3, 0.4, n_steps=3, f_sink=1.0,
                                  rho_floor=1e-8, P_floor=1e-10, rho_sink_min=2e-8, evolve_orbit=False, diag=rec)
     R = rec.cpu().numpy()
     assert n == 3 and R[2, 0] == t and np.all(R[3] == 0.0)
     assert np.all(R[:3, 1] > 0) and R[0, 0] == R[0, 1] and R[1, 0] == R[0, 0] + R[1, 1]
     end = bsn.diagnostics(Ud, 32, 32, 32, dx, dx, dx, x0, x0, x0, bg, 4 / 3)
-    assert np.array_equal(R[2, 2:], end)
+    assert np.array_equal(R[2, 2:12], end)
     # the reference loop's times
     bo = orc.bh_array(_obhs(orc, specs))
     t_ref = 0.0
