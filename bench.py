@@ -663,6 +663,8 @@ def run_bsn(args, rank, world):
     if "learned" in (prec,) + tuple(others):
         from bsn import learned as LW
         LW.install(*LW.load_params())
+    if args.no_tma:
+        bsn.set_tma(False)
     if args.tile >= 0:
         for p_ in ("f32", "f64", "learned"):
             bsn.set_tile(p_, min(args.tile, bsn.tile_variants(p_) - 1))
@@ -686,6 +688,10 @@ def run_bsn(args, rank, world):
     for _ in range(3):
         step_fn(Up, n, n, n, dx, dx, dx, dt0, GAMMA, **kw)
     tot, cnt = bsn.kernel_time(kname)
+    if prec != "learned":   # the stage kernel with TMA staging, where the grid allows it
+        t_, c_ = bsn.kernel_time(kname + "_tma")
+        if c_:
+            tot, cnt, kname = tot + t_, cnt + c_, kname + "_tma"
     if prec == "learned":   # a learned stage is a screening launch plus the learned launch
         tot += bsn.kernel_time("stage_kernel_learned_screen")[0]
         kname = "stage_kernel_learned_screen + stage_kernel_learned"
@@ -768,6 +774,7 @@ def run_bsn(args, rank, world):
             "config": {"workload": f"sedov{n}^3", "grid": [n, n, n], "path": desc[prec],
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "tile": list(tile), "time_loop": "device-resident dt, one CUDA graph per step",
+                       "staging": "TMA tensor copies" if bsn.get_tile_tma(n, n, n, prec) else "per-thread loads",
                        "timed_from": f"Sedov state at t={T_MID} (FP64 run from the initial condition)",
                        "l2": f"state {Ud.numel() * 8 / 1e6:.0f} MB per array > 126 MB L2 (no flush needed)"},
             "compare": compare,
@@ -816,6 +823,8 @@ def main():
                     help="--workload polytrope_fmr: rigid rotation as a fraction of breakup (e.g. 0.2)")
     ap.add_argument("--paths", default="f64,f32,learned",
                     help="stencil paths of --workload binary_nested (comma-separated)")
+    ap.add_argument("--no-tma", action="store_true",
+                    help="stage the stencil tiles with the plain per-thread loader instead of TMA copies")
     ap.add_argument("--tile", type=int, default=-1,
                     help="force this stage-kernel tile variant for both precisions (default: autotune)")
     args = ap.parse_args()

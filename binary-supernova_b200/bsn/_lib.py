@@ -79,6 +79,9 @@ SIGNATURES = {
     "bsn_learned_train": (_I, [_V, _P, _LL, _P, _I, _I, C.c_float, C.c_ulonglong, _dp]),
     "bsn_learned_set_params": (_I, [_V, _P, _P]),
     "bsn_learned_eval": (_I, [_V, _P, _LL, _P, _P, _I]),
+    "bsn_ctx_set_tma": (_I, [_V, _I]),
+    "bsn_ctx_get_tma": (_I, [_V]),
+    "bsn_ctx_get_tile_tma": (_I, [_V, _I, _I, _I, _I]),
     "bsn_tile_variant_count": (_I, [_I]),
     "bsn_ctx_set_tile": (_I, [_V, _I, _I]),
     "bsn_ctx_get_tile": (_I, [_V, _I, _I, _I, _I, C.POINTER(C.c_int)]),

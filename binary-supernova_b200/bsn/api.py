@@ -32,7 +32,7 @@ __all__ = [
     "apply_sg_force_level", "apply_sg_force_slab", "coupled_step", "FMRGrid3D", "fmr3d_step", "cfl_dt_fmr3d", "solve_fmr_poisson",
     "restrict_density_to_coarse", "FMRHierarchy3D", "fmr_nested_step", "cfl_dt_fmr_nested",
     "fmr_nested_run_steps", "coupled_nested_run_steps", "rotating_frame_source", "relax_damping_source",
-    "relax_ic", "DIAG_FIELDS", "DIAG_RECORD",
+    "relax_ic", "DIAG_FIELDS", "DIAG_RECORD", "set_tma", "get_tma", "get_tile_tma",
 ]
 
 # ---------------------------------------------------------------------------
@@ -586,6 +586,22 @@ def run_steps(U, nx, ny, nz, dx, dy, dz, gamma, cfl, *, n_steps, t=0.0, t_end=0.
 
 def tile_variants(precision="f64") -> int:
     return int(load().bsn_tile_variant_count(PREC[precision]))
+
+
+def set_tma(on=True):
+    """Stage the fused kernel's block and halos with TMA tensor copies (the
+    default where the grid allows) or with the plain per-thread loader."""
+    _call("bsn_ctx_set_tma", context(), int(bool(on)))
+
+
+def get_tma() -> bool:
+    return bool(load().bsn_ctx_get_tma(context()))
+
+
+def get_tile_tma(nx, ny, nz, precision="f64"):
+    """Whether the tile chosen for this grid is TMA-staged (None: not chosen yet)."""
+    r = load().bsn_ctx_get_tile_tma(context(), PREC[precision], nx, ny, nz)
+    return None if r < 0 else bool(r)
 
 
 def set_tile(precision="f64", variant=-1):

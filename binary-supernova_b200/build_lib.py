@@ -5,7 +5,8 @@ Usage: python build_lib.py [--force] [--verbose]
 Every translation unit is compiled for sm_100a only.  The FP64 parity path
 (files listed in FP64_PARITY) is compiled with -fmad=false so that no
 multiply-add is contracted and results match the reference's CPU arithmetic
-bit for bit; the FP32 fast path keeps contraction on.
+bit for bit; the FP32 stencil units are built the same way with their
+multiply-adds written out, the FP32 FFTs keep contraction on.
 """
 from __future__ import annotations
 
@@ -23,10 +24,15 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 BASE = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 FP64_PARITY = {"hydro_f64.cu", "sources_f64.cu", "fmr_f64.cu", "fmr_nlevel.cu", "poisson.cu", "context.cu", "cfl_noalloc.cu",
-               "run_steps.cu", "autotune.cu", "coupled_run.cu", "diagnostics.cu", "relax.cu"}
-# the FP32 fast path: contraction on, approximate division and square root
+               "run_steps.cu", "autotune.cu", "coupled_run.cu", "diagnostics.cu", "relax.cu", "tma_host.cu"}
+# the FP32 fast path: approximate division and square root.  The stencil
+# units write every multiply-add out (fmaf, fma.rn.f32x2) and are built
+# without contraction, so their results do not depend on the compiler's
+# contraction choices (each tile variant gives the same bits); the FP32 FFTs
+# keep contraction on.
 FAST = {"stage_fast.cu", "learned.cu", "poisson_f32.cu"}
 FAST_FLAGS = ["--ftz=true", "--prec-div=false", "--prec-sqrt=false", "--fmad=true"]
+EXPLICIT_FMA = {"stage_fast.cu", "learned.cu"}
 
 
 def sources():
@@ -49,6 +55,8 @@ def _compile(src: str, force: bool, verbose: bool):
         flags += ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]
     elif src in FAST:
         flags += FAST_FLAGS
+        if src in EXPLICIT_FMA:
+            flags[-1] = "--fmad=false"
     cmd = [NVCC] + ARCH + flags + ["-c", srcp, "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

@@ -1,10 +1,14 @@
-// autotune.cu -- picks the tile shape of the fused stage kernel per grid.
+// autotune.cu -- picks the tile shape of the fused stage kernel per grid,
+// and whether its block is staged by TMA copies or by the plain loader.
 //
 // On the first stage of a new (precision, nx, ny, nz) the autotuner launches
 // every tile variant on stage-1 work (reading the caller's state, writing a
-// scratch array), times two launches of each with CUDA events after one
-// warm-up, and keeps the fastest for the life of the context.  FP64 variants
-// give bit-identical results, so the choice never changes a result.
+// scratch array), with each staging the grid allows, times two launches of
+// each with CUDA events after one warm-up, and keeps the fastest for the life
+// of the context.  Every variant and staging gives bit-identical results (FP64
+// by the reference's arithmetic, FP32 by its written-out multiply-adds), so
+// the choice never changes a result.  The choice is stored as a code: the
+// variant index plus kTmaBit when the TMA form won.
 #include "hydro_f64.cuh"
 #include "stage_launch.cuh"
 
@@ -16,10 +20,24 @@ static int variant_count(int prec) {
 static TileVariant variant(int prec, int idx) {
     return prec == PREC_F64 ? f64_variant(idx) : (prec == PREC_F32 ? f32_variant(idx) : learned_variant(idx));
 }
-static bsn_status launch_variant(bsn_ctx* ctx, int prec, int idx, const f64::StageArgs& A) {
-    if (prec == PREC_F64) return f64_launch_variant(ctx, idx, A);
-    if (prec == PREC_F32) return f32_launch_variant(ctx, idx, A);
-    return learned_launch_variant(ctx, idx, A);
+constexpr int kTmaBit = 256;   // tile-choice code: variant index | kTmaBit when TMA staging is chosen
+
+// One launch of variant `code & 255`, TMA-staged where the code asks for it
+// (and the grid allows it); ctx->tma_used_last tells whether it was.
+static bsn_status launch_variant(bsn_ctx* ctx, int prec, int code, const f64::StageArgs& A) {
+    const int idx = code & (kTmaBit - 1);
+    ctx->tma_now = (code & kTmaBit) ? 1 : 0;
+    ctx->tma_used_last = 0;
+    bsn_status st = prec == PREC_F64 ? f64_launch_variant(ctx, idx, A)
+                    : prec == PREC_F32 ? f32_launch_variant(ctx, idx, A)
+                                       : learned_launch_variant(ctx, idx, A);
+    ctx->tma_now = 0;
+    return st;
+}
+// the code of a forced variant: TMA wherever the context allows it
+static int forced_code(bsn_ctx* ctx, int prec) {
+    const int v = ctx->forced_tile[prec] >= 0 ? ctx->forced_tile[prec] : 0;
+    return v | (ctx->tma_on ? kTmaBit : 0);
 }
 static bsn_status launch_batch_variant(bsn_ctx* ctx, int prec, int idx, const f64::StageBatch& B) {
     if (prec == PREC_F64) return f64_launch_batch_variant(ctx, idx, B);
@@ -37,8 +55,8 @@ bsn_status stage_autotune(bsn_ctx* ctx, int prec, const f64::StageArgs& probe, d
     auto key = std::make_tuple(prec, probe.nx, probe.ny, probe.nz);
     if (ctx->tile_choice.count(key)) return BSN_OK;
     int nv = variant_count(prec);
-    if (ctx->forced_tile[prec] >= 0 || nv == 1) {
-        ctx->tile_choice[key] = ctx->forced_tile[prec] >= 0 ? ctx->forced_tile[prec] : 0;
+    if (ctx->forced_tile[prec] >= 0) {
+        ctx->tile_choice[key] = forced_code(ctx, prec);
         return BSN_OK;
     }
     f64::StageArgs a = probe;
@@ -64,19 +82,23 @@ bsn_status stage_autotune(bsn_ctx* ctx, int prec, const f64::StageArgs& probe, d
     ctx->profiling = false;
     bsn_status st = BSN_OK;
     for (int v = 0; v < nv && st == BSN_OK; ++v) {
-        st = launch_variant(ctx, prec, v, a);   // warm-up (sets smem attributes)
-        if (st != BSN_OK) break;
-        float ms = 1e30f;
-        for (int r = 0; r < 2 && st == BSN_OK; ++r) {
-            cudaEventRecord(e0, ctx->stream);
-            st = launch_variant(ctx, prec, v, a);
-            cudaEventRecord(e1, ctx->stream);
-            cudaEventSynchronize(e1);
-            float t = 0.f;
-            cudaEventElapsedTime(&t, e0, e1);
-            ms = t < ms ? t : ms;
+        for (int tma = 0; tma < (ctx->tma_on ? 2 : 1) && st == BSN_OK; ++tma) {
+            const int code = v | (tma ? kTmaBit : 0);
+            st = launch_variant(ctx, prec, code, a);   // warm-up (sets smem attributes)
+            if (st != BSN_OK) break;
+            if (tma && !ctx->tma_used_last) break;      // the grid does not allow TMA staging of this tile
+            float ms = 1e30f;
+            for (int r = 0; r < 2 && st == BSN_OK; ++r) {
+                cudaEventRecord(e0, ctx->stream);
+                st = launch_variant(ctx, prec, code, a);
+                cudaEventRecord(e1, ctx->stream);
+                st = st != BSN_OK ? st : cuda_check(ctx, cudaEventSynchronize(e1), "cudaEventSynchronize(autotune)");
+                float t = 0.f;
+                cudaEventElapsedTime(&t, e0, e1);
+                ms = t < ms ? t : ms;
+            }
+            if (ms < best_ms) { best_ms = ms; best = code; }
         }
-        if (ms < best_ms) { best_ms = ms; best = v; }
     }
     ctx->profiling = prof;
     cudaEventDestroy(e0);
@@ -92,10 +114,8 @@ bsn_status stage_launch(bsn_ctx* ctx, int prec, const f64::StageArgs& A) {
     if (it == ctx->tile_choice.end()) {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         cudaStreamIsCapturing(ctx->stream, &cs);
-        if (ctx->forced_tile[prec] >= 0 || cs != cudaStreamCaptureStatusNone) {
-            int v = ctx->forced_tile[prec] >= 0 ? ctx->forced_tile[prec] : 0;
-            return launch_variant(ctx, prec, v, A);
-        }
+        if (ctx->forced_tile[prec] >= 0 || cs != cudaStreamCaptureStatusNone)
+            return launch_variant(ctx, prec, forced_code(ctx, prec), A);
         Geom G(A.nx, A.ny, A.nz);
         bsn_status st;
         double* scratch = (double*)slot(ctx, SLOT_UN, sizeof(double) * (size_t)G.nelem(), &st);
@@ -111,7 +131,7 @@ bsn_status stage_launch(bsn_ctx* ctx, int prec, const f64::StageArgs& A) {
 static bsn_status choose(bsn_ctx* ctx, int prec, const f64::StageArgs& A, int& v) {
     auto key = std::make_tuple(prec, A.nx, A.ny, A.nz);
     auto it = ctx->tile_choice.find(key);
-    if (it != ctx->tile_choice.end()) { v = it->second; return BSN_OK; }
+    if (it != ctx->tile_choice.end()) { v = it->second & (kTmaBit - 1); return BSN_OK; }
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(ctx->stream, &cs);
     if (ctx->forced_tile[prec] >= 0 || cs != cudaStreamCaptureStatusNone) {
@@ -123,7 +143,7 @@ static bsn_status choose(bsn_ctx* ctx, int prec, const f64::StageArgs& A, int& v
     double* scratch = (double*)slot(ctx, SLOT_UN, sizeof(double) * (size_t)G.nelem(), &st);
     BSN_TRY(st);
     BSN_TRY(stage_autotune(ctx, prec, A, scratch));
-    v = ctx->tile_choice[key];
+    v = ctx->tile_choice[key] & (kTmaBit - 1);   // several grids in one launch: the plain loader
     return BSN_OK;
 }
 
@@ -153,9 +173,16 @@ extern "C" bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int 
     auto it = ctx->tile_choice.find(std::make_tuple(precision, nx, ny, nz));
     if (it == ctx->tile_choice.end()) return set_err(ctx, BSN_ERR_ARG, "no tile chosen yet for this grid");
     if (!prec_ok(precision)) return set_err(ctx, BSN_ERR_ARG, "bad precision %d", precision);
-    TileVariant v = variant(precision, it->second);
+    TileVariant v = variant(precision, it->second & (kTmaBit - 1));
     out[0] = v.tx; out[1] = v.ty; out[2] = v.tz; out[3] = v.nt; out[4] = v.minb;
     return BSN_OK;
+}
+
+extern "C" int bsn_ctx_get_tile_tma(bsn_ctx* ctx, int precision, int nx, int ny, int nz) {
+    if (!ctx) return -1;
+    auto it = ctx->tile_choice.find(std::make_tuple(precision, nx, ny, nz));
+    if (it == ctx->tile_choice.end()) return -1;
+    return (it->second & kTmaBit) ? 1 : 0;
 }
 
 extern "C" int bsn_tile_variant_count(int precision) {

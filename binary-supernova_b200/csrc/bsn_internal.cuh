@@ -43,6 +43,12 @@ struct bsn_ctx {
     void* coupled_run_state = nullptr;   // coupled_run.cu: graph of the device-resident coupled step
     void* coupled_nested_state = nullptr;   // coupled_run.cu: the coupled step on nested levels
     void* relax_state = nullptr;     // relax.cu: graph of the device-resident relaxation step
+    // TMA staging of the stage kernels (tma_host.cu): on unless switched off
+    // with bsn_ctx_set_tma; tma_err is the device word a timed-out copy wait sets
+    int tma_on = 1;
+    unsigned int* tma_err = nullptr;
+    int tma_now = 0;                 // the launch being made may use TMA staging (autotune.cu)
+    int tma_used_last = 0;           // the last stage launch used it
 };
 
 namespace bsn {
@@ -63,6 +69,10 @@ bsn_status launch_check(bsn_ctx* ctx, const char* what);
 void prof_begin(bsn_ctx* ctx);
 void* slot(bsn_ctx* ctx, int s, size_t bytes, bsn_status* st);
 void* pinned(bsn_ctx* ctx, size_t bytes, bsn_status* st);
+namespace tma {
+void init_ctx(bsn_ctx* ctx);             // tma_host.cu: error word of the context's device
+bsn_status check_error(bsn_ctx* ctx);    // BSN_ERR_TIMEOUT if a staging copy wait ran out (synchronises)
+}  // namespace tma
 
 #define BSN_TRY(expr)                         \
     do {                                      \

@@ -122,6 +122,7 @@ extern "C" bsn_status bsn_ctx_create(bsn_ctx** out, int device, void* stream) {
     c->stream = (cudaStream_t)stream;
     c->slot_ptr.assign(SLOT_COUNT, nullptr);
     c->slot_bytes.assign(SLOT_COUNT, 0);
+    tma::init_ctx(c);
     *out = c;
     return BSN_OK;
 }
@@ -155,7 +156,8 @@ extern "C" bsn_status bsn_ctx_set_stream(bsn_ctx* ctx, void* stream) {
 
 extern "C" bsn_status bsn_ctx_synchronize(bsn_ctx* ctx) {
     if (!ctx) return BSN_ERR_ARG;
-    return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+    BSN_TRY(cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"));
+    return tma::check_error(ctx);
 }
 
 extern "C" const char* bsn_last_error(const bsn_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }

@@ -211,19 +211,11 @@ const TileVariant kF64Variants[] = {{8, 8, 8, 256, 2}, {8, 8, 4, 128, 4}, {16, 8
 
 template <int TX, int TY, int TZ, int NT, int MINB>
 bsn_status launch_f64(bsn_ctx* ctx, const StageArgs& A) {
-    auto fn = tile::stage_kernel<tile::F64Physics, TX, TY, TZ, NT, MINB>;
-    constexpr int smem = tile::smem_bytes<tile::F64Physics, TX, TY, TZ>();
-    static bool attr_done[64] = {false};
-    int dev = ctx->device & 63;
-    if (!attr_done[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaFuncSetAttribute(stage_kernel)");
-        attr_done[dev] = true;
-    }
-    dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + TZ - 1) / TZ);
-    prof_begin(ctx);
-    fn<<<grid, NT, smem, ctx->stream>>>(A);
-    return launch_check(ctx, "stage_kernel");
+    bool tma_used = false;
+    BSN_TRY((tile::launch_tma<tile::F64Physics, TX, TY, TZ, NT, MINB>(ctx, A, "stage_kernel_tma", &tma_used)));
+    if (tma_used) return BSN_OK;
+    return tile::launch_plain<tile::F64Physics, TX, TY, TZ, NT, MINB>(
+        ctx, A, tile::smem_bytes<tile::F64Physics, TX, TY, TZ>(), "stage_kernel");
 }
 }  // namespace
 

@@ -564,8 +564,8 @@ struct F32Learned {
             // spreads about the common centre c2: left stencil c0..c4, right c1..c5
             float m14 = fmaxf(fmaxf(fabsf(c1 - c2), fabsf(c3 - c2)), fabsf(c4 - c2));
             float sL = fmaxf(m14, fabsf(c0 - c2)), sR = fmaxf(m14, fabsf(c5 - c2));
-            bool smL = fabsf(bA - bC) <= learned::THETA * (fminf(fminf(bA, bB), bC) + learned::BETA_EPS * sL * sL);
-            bool smR = fabsf(bB - bE) <= learned::THETA * (fminf(fminf(bB, bD), bE) + learned::BETA_EPS * sR * sR);
+            bool smL = fabsf(bA - bC) <= learned::THETA * fmaf(learned::BETA_EPS * sL, sL, fminf(fminf(bA, bB), bC));
+            bool smR = fabsf(bB - bE) <= learned::THETA * fmaf(learned::BETA_EPS * sR, sR, fminf(fminf(bB, bD), bE));
             // spreads at FP32 rounding level of the centre value (or below
             // WENO-Z's epsilon scale) carry no shape: WENO-Z stays.  This
             // also keeps the network off the 1e-30-level precursor noise that
@@ -604,14 +604,15 @@ struct F32Learned {
             const int q = 4, col = 5;
             float c0 = c[0][col], c1 = c[1][col], c2 = c[2][col], c3 = c[3][col], c4 = c[4][col], c5 = c[5][col];
             if (!valid) c0 = c1 = c2 = c3 = c4 = c5 = 0.f;
-            float qA = t13 * c0 + m76 * c1 + e116 * c2;
-            float qB = m16 * c1 + f56 * c2 + t13 * c3;
-            float qC = t13 * c2 + f56 * c3 + m16 * c4;
-            float qD = e116 * c3 + m76 * c4 + t13 * c5;
-            float s0 = c0 - 2.0f * c1 + c2, s1 = c1 - 2.0f * c2 + c3, s2 = c2 - 2.0f * c3 + c4,
-                  s3 = c3 - 2.0f * c4 + c5;
-            float a = c0 - 4.0f * c1 + 3.0f * c2, b = c1 - c3, cc = 3.0f * c2 - 4.0f * c3 + c4,
-                  d = c2 - 4.0f * c3 + 3.0f * c4, e = 3.0f * c3 - 4.0f * c4 + c5;
+            // f32::weno5_lr's operations, keeping the indicators for the test
+            float qA = fmaf(e116, c2, fmaf(m76, c1, t13 * c0));
+            float qB = fmaf(t13, c3, fmaf(f56, c2, m16 * c1));
+            float qC = fmaf(m16, c4, fmaf(f56, c3, t13 * c2));
+            float qD = fmaf(t13, c5, fmaf(m76, c4, e116 * c3));
+            float s0 = fmaf(-2.0f, c1, c0) + c2, s1 = fmaf(-2.0f, c2, c1) + c3, s2 = fmaf(-2.0f, c3, c2) + c4,
+                  s3 = fmaf(-2.0f, c4, c3) + c5;
+            float a = fmaf(3.0f, c2, fmaf(-4.0f, c1, c0)), b = c1 - c3, cc = fmaf(-4.0f, c3, 3.0f * c2) + c4,
+                  d = fmaf(3.0f, c4, fmaf(-4.0f, c3, c2)), e = fmaf(-4.0f, c4, 3.0f * c3) + c5;
             float bA = fmaf(k1312 * s0, s0, 0.25f * a * a);
             float bB = fmaf(k1312 * s1, s1, 0.25f * b * b);
             float x2 = k1312 * s2 * s2;
@@ -674,15 +675,15 @@ struct F32Learned {
                 const float v0 = c[side][col], v1 = c[side + 1][col], v2 = c[side + 2][col], v3 = c[side + 3][col],
                             v4 = c[side + 4][col];
                 float qa, qb, qc;
-                if (side == 0) {
-                    qa = t13 * v0 + m76 * v1 + e116 * v2;
-                    qb = m16 * v1 + f56 * v2 + t13 * v3;
-                    qc = t13 * v2 + f56 * v3 + m16 * v4;
+                if (side == 0) {   // the candidate polynomials of weno5_lr (qA, qB, qC)
+                    qa = fmaf(e116, v2, fmaf(m76, v1, t13 * v0));
+                    qb = fmaf(t13, v3, fmaf(f56, v2, m16 * v1));
+                    qc = fmaf(m16, v4, fmaf(f56, v3, t13 * v2));
                     L[q] = fmaf(w[0], qa, fmaf(w[1], qb, w[2] * qc));
-                } else {
-                    qa = m16 * v0 + f56 * v1 + t13 * v2;
-                    qb = t13 * v1 + f56 * v2 + m16 * v3;
-                    qc = e116 * v2 + m76 * v3 + t13 * v4;
+                } else {           // (qB, qC, qD)
+                    qa = fmaf(t13, v2, fmaf(f56, v1, m16 * v0));
+                    qb = fmaf(m16, v3, fmaf(f56, v2, t13 * v1));
+                    qc = fmaf(t13, v4, fmaf(m76, v3, e116 * v2));
                     Rv[q] = fmaf(w[0], qa, fmaf(w[1], qb, w[2] * qc));
                 }
             }
@@ -717,19 +718,8 @@ const TileVariant kLearnedVariants[] = {{8, 8, 8, 256, 2}, {16, 8, 4, 256, 2}, {
 // coupled loops, whose grids are mostly non-uniform).
 template <int TX, int TY, int TZ, int NT, int MINB>
 bsn_status launch_learned_whole(bsn_ctx* ctx, const f64::StageArgs& A) {
-    auto fn = tile::stage_kernel<tile::F32Learned, TX, TY, TZ, NT, MINB>;
     constexpr int smem = tile::smem_bytes<tile::F32Learned, TX, TY, TZ>() + tile::F32Learned::kExtraSmem(NT) + 16;
-    static bool attr_done[64] = {false};
-    int dev = ctx->device & 63;
-    if (!attr_done[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaFuncSetAttribute(stage_kernel_learned)");
-        attr_done[dev] = true;
-    }
-    dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + TZ - 1) / TZ);
-    prof_begin(ctx);
-    fn<<<grid, NT, smem, ctx->stream>>>(A);
-    return launch_check(ctx, "stage_kernel_learned");
+    return tile::launch_plain<tile::F32Learned, TX, TY, TZ, NT, MINB>(ctx, A, smem, "stage_kernel_learned");
 }
 
 // One learned stage as two launches on the context's stream: the screening
@@ -767,6 +757,7 @@ bsn_status launch_learned(bsn_ctx* ctx, const f64::StageArgs& A0) {
     A.split_count = cnt;
     A.split_list = (int*)(cnt + 4);
     BSN_CUDA(ctx, cudaMemsetAsync(cnt, 0, sizeof(unsigned int), ctx->stream));
+    // the screening launch stages with the plain loader (its TMA form is not used)
     prof_begin(ctx);
     fs<<<grid, NT, smem_s, ctx->stream>>>(A);
     BSN_TRY(launch_check(ctx, "stage_kernel_learned_screen"));

@@ -1,9 +1,12 @@
 // physics_f32.cuh -- FP32 stencil physics of the fast path.
 //
 // Same method as the reference (WENO5-Z of rho, m, P with the P clamp, face
-// energy from P, HLLC with its guards), evaluated in FP32 with contraction to
-// FMA and approximate reciprocals/square roots (the translation unit is built
-// with --ftz=true --prec-div=false --prec-sqrt=false).  FP32-specific guards:
+// energy from P, HLLC with its guards), evaluated in FP32 with approximate
+// reciprocals/square roots (the translation units are built with --ftz=true
+// --prec-div=false --prec-sqrt=false).  Every fused multiply-add is written
+// out (fmaf, fma.rn.f32x2) and the units are built with --fmad=false, so no
+// result depends on the compiler's contraction choices: each tile variant,
+// and TMA or plain staging, gives the same bits.  FP32-specific guards:
 //   * WENO-Z: tau/(eps+beta) is clamped to 1e18 before squaring, so the
 //     weights cannot overflow to Inf/Inf when beta ~ 0 and tau != 0 (with the
 //     reference's eps = 1e-36 the unclamped square overflows FP32);
@@ -44,16 +47,18 @@ __device__ __forceinline__ void weno5_lr(float c0, float c1, float c2, float c3,
                                          float& R) {
     const float t13 = 1.0f / 3.0f, m76 = -7.0f / 6.0f, e116 = 11.0f / 6.0f, m16 = -1.0f / 6.0f, f56 = 5.0f / 6.0f;
     const float k1312 = 13.0f / 12.0f;
-    float qA = t13 * c0 + m76 * c1 + e116 * c2;
-    float qB = m16 * c1 + f56 * c2 + t13 * c3;
-    float qC = t13 * c2 + f56 * c3 + m16 * c4;
-    float qD = e116 * c3 + m76 * c4 + t13 * c5;
-    float s0 = c0 - 2.0f * c1 + c2, s1 = c1 - 2.0f * c2 + c3, s2 = c2 - 2.0f * c3 + c4, s3 = c3 - 2.0f * c4 + c5;
-    float a = c0 - 4.0f * c1 + 3.0f * c2;
+    // the same operations, multiply-adds and order as the two-lane weno5_lr2
+    float qA = fmaf(e116, c2, fmaf(m76, c1, t13 * c0));
+    float qB = fmaf(t13, c3, fmaf(f56, c2, m16 * c1));
+    float qC = fmaf(m16, c4, fmaf(f56, c3, t13 * c2));
+    float qD = fmaf(t13, c5, fmaf(m76, c4, e116 * c3));
+    float s0 = fmaf(-2.0f, c1, c0) + c2, s1 = fmaf(-2.0f, c2, c1) + c3, s2 = fmaf(-2.0f, c3, c2) + c4,
+          s3 = fmaf(-2.0f, c4, c3) + c5;
+    float a = fmaf(3.0f, c2, fmaf(-4.0f, c1, c0));
     float b = c1 - c3;
-    float c = 3.0f * c2 - 4.0f * c3 + c4;
-    float d = c2 - 4.0f * c3 + 3.0f * c4;
-    float e = 3.0f * c3 - 4.0f * c4 + c5;
+    float c = fmaf(-4.0f, c3, 3.0f * c2) + c4;
+    float d = fmaf(3.0f, c4, fmaf(-4.0f, c3, c2));
+    float e = fmaf(-4.0f, c4, 3.0f * c3) + c5;
     float bA = fmaf(k1312 * s0, s0, 0.25f * a * a);
     float bB = fmaf(k1312 * s1, s1, 0.25f * b * b);
     float x2 = k1312 * s2 * s2;
@@ -169,7 +174,7 @@ __device__ __forceinline__ void weno5_lr2(f2 c0, f2 c1, f2 c2, f2 c3, f2 c4, f2 
 __device__ __forceinline__ bool floor_clear(const float (&w)[5], double v0, double rho_floor, double Pfl_gm1) {
     if (!(v0 >= rho_floor)) return false;
     const float KE = fdiv(0.5f * fmaf(w[3], w[3], fmaf(w[2], w[2], w[1] * w[1])), w[0]);
-    return w[4] - KE > (float)Pfl_gm1 + 1e-5f * (fabsf(w[4]) + KE);
+    return w[4] - KE > fmaf(1e-5f, fabsf(w[4]) + KE, (float)Pfl_gm1);
 }
 __device__ __forceinline__ void floor_screened(double (&v)[5], double rho_floor, double P_floor, double Pfl_gm1,
                                                double gm1) {
@@ -191,13 +196,13 @@ __device__ __forceinline__ void stage_floored(double (&v)[5], bool act, double r
 
 __device__ __forceinline__ float cell_pressure(float r, float mx, float my, float mz, float E, float gm1) {
     r = fmaxf(r, 1e-30f);
-    float KE = fdiv(0.5f * (mx * mx + my * my + mz * mz), r);
+    float KE = fdiv(0.5f * fmaf(mz, mz, fmaf(my, my, mx * mx)), r);
     return fmaxf(gm1 * (E - KE), 0.0f);
 }
 
 __device__ __forceinline__ float EL_from_P(float PL, float rL, float mx, float my, float mz, float inv_gm1) {
     float rp = fmaxf(rL, 1e-30f);
-    float KE = fminf(fdiv(0.5f * (mx * mx + my * my + mz * mz), rp), 0.5f * rp * 1e4f);
+    float KE = fminf(fdiv(0.5f * fmaf(mz, mz, fmaf(my, my, mx * mx)), rp), 0.5f * rp * 1e4f);
     return fmaf(PL, inv_gm1, KE);
 }
 
@@ -209,17 +214,17 @@ __device__ __forceinline__ void hllc_normal(float rL, float mnL, float mt1L, flo
     if (rR <= 0.0f) { rR = 1e-30f; mnR = 0.0f; mt1R = 0.0f; mt2R = 0.0f; ER = 0.0f; }
     rL = fmaxf(rL, 1e-30f);
     rR = fmaxf(rR, 1e-30f);
-    float m2L = mnL * mnL + mt1L * mt1L + mt2L * mt2L;
+    float m2L = fmaf(mt2L, mt2L, fmaf(mt1L, mt1L, mnL * mnL));
     if (m2L > rL * rL * 1e4f) {
         float s = rL * 100.0f * rsqrtf(m2L);
         mnL *= s; mt1L *= s; mt2L *= s;
-        m2L = mnL * mnL + mt1L * mt1L + mt2L * mt2L;
+        m2L = fmaf(mt2L, mt2L, fmaf(mt1L, mt1L, mnL * mnL));
     }
-    float m2R = mnR * mnR + mt1R * mt1R + mt2R * mt2R;
+    float m2R = fmaf(mt2R, mt2R, fmaf(mt1R, mt1R, mnR * mnR));
     if (m2R > rR * rR * 1e4f) {
         float s = rR * 100.0f * rsqrtf(m2R);
         mnR *= s; mt1R *= s; mt2R *= s;
-        m2R = mnR * mnR + mt1R * mt1R + mt2R * mt2R;
+        m2R = fmaf(mt2R, mt2R, fmaf(mt1R, mt1R, mnR * mnR));
     }
     float iL = fdiv(1.0f, rL), iR = fdiv(1.0f, rR);
     float KE_L = fminf(0.5f * m2L * iL, 0.5f * rL * 1e4f);
@@ -233,11 +238,11 @@ __device__ __forceinline__ void hllc_normal(float rL, float mnL, float mt1L, flo
     float SL, SR;
     if (pL > 0.0f && pR > 0.0f) {
         float r_avg = 0.5f * (rL + rR), cs_avg = 0.5f * (csL + csR);
-        float p_star = fmaxf(0.0f, 0.5f * (pL + pR) - 0.5f * (vnR - vnL) * r_avg * cs_avg);
+        float p_star = fmaxf(0.0f, fmaf(-0.5f * (vnR - vnL) * r_avg, cs_avg, 0.5f * (pL + pR)));
         float qL = p_star > pL ? sqrtf(fmaf(gg, fdiv(p_star, pL) - 1.0f, 1.0f)) : 1.0f;
         float qR = p_star > pR ? sqrtf(fmaf(gg, fdiv(p_star, pR) - 1.0f, 1.0f)) : 1.0f;
-        SL = vnL - csL * qL;
-        SR = vnR + csR * qR;
+        SL = fmaf(-csL, qL, vnL);
+        SR = fmaf(csR, qR, vnR);
     } else {
         SL = fminf(vnL - csL, vnR - csR);
         SR = fmaxf(vnL + csL, vnR + csR);
@@ -245,36 +250,36 @@ __device__ __forceinline__ void hllc_normal(float rL, float mnL, float mt1L, flo
     float dL = rL * (SL - vnL), dR = rR * (SR - vnR);
     float denom = dL - dR;
     if (fabsf(denom) < 1e-36f) { F[0] = F[1] = F[2] = F[3] = F[4] = 0.0f; return; }
-    float S_star = fdiv(pR - pL + mnL * (SL - vnL) - mnR * (SR - vnR), denom);
+    float S_star = fdiv(fmaf(-mnR, SR - vnR, fmaf(mnL, SL - vnL, pR - pL)), denom);
     float FrL = mnL, FmnL = fmaf(mnL, vnL, pL), Fmt1L = mt1L * vnL, Fmt2L = mt2L * vnL, FEL = (EL + pL) * vnL;
     if (SL >= 0.0f) { F[0] = FrL; F[1] = FmnL; F[2] = Fmt1L; F[3] = Fmt2L; F[4] = FEL; return; }
     float FrR = mnR, FmnR = fmaf(mnR, vnR, pR), Fmt1R = mt1R * vnR, Fmt2R = mt2R * vnR, FER = (ER + pR) * vnR;
     if (SR <= 0.0f) { F[0] = FrR; F[1] = FmnR; F[2] = Fmt1R; F[3] = Fmt2R; F[4] = FER; return; }
     if (fmaxf(rL, rR) > 3.0f * fminf(rL, rR)) {
         float inv = fdiv(1.0f, SR - SL), SLSR = SL * SR;
-        F[0] = (SR * FrL - SL * FrR + SLSR * (rR - rL)) * inv;
-        F[1] = (SR * FmnL - SL * FmnR + SLSR * (mnR - mnL)) * inv;
-        F[2] = (SR * Fmt1L - SL * Fmt1R + SLSR * (mt1R - mt1L)) * inv;
-        F[3] = (SR * Fmt2L - SL * Fmt2R + SLSR * (mt2R - mt2L)) * inv;
-        F[4] = (SR * FEL - SL * FER + SLSR * (ER - EL)) * inv;
+        F[0] = fmaf(SLSR, rR - rL, fmaf(-SL, FrR, SR * FrL)) * inv;
+        F[1] = fmaf(SLSR, mnR - mnL, fmaf(-SL, FmnR, SR * FmnL)) * inv;
+        F[2] = fmaf(SLSR, mt1R - mt1L, fmaf(-SL, Fmt1R, SR * Fmt1L)) * inv;
+        F[3] = fmaf(SLSR, mt2R - mt2L, fmaf(-SL, Fmt2R, SR * Fmt2L)) * inv;
+        F[4] = fmaf(SLSR, ER - EL, fmaf(-SL, FER, SR * FEL)) * inv;
         return;
     }
     if (S_star >= 0.0f) {
         float chi = fdiv(dL, SL - S_star);
-        float EsL = fabsf(dL) > 1e-36f ? chi * (EL * iL + (S_star - vnL) * (S_star + fdiv(pL, dL))) : 0.0f;
-        F[0] = FrL + SL * (chi - rL);
-        F[1] = FmnL + SL * (chi * S_star - mnL);
-        F[2] = Fmt1L + SL * (chi * vt1L - mt1L);
-        F[3] = Fmt2L + SL * (chi * vt2L - mt2L);
-        F[4] = FEL + SL * (EsL - EL);
+        float EsL = fabsf(dL) > 1e-36f ? chi * fmaf(S_star - vnL, S_star + fdiv(pL, dL), EL * iL) : 0.0f;
+        F[0] = fmaf(SL, chi - rL, FrL);
+        F[1] = fmaf(SL, fmaf(chi, S_star, -mnL), FmnL);
+        F[2] = fmaf(SL, fmaf(chi, vt1L, -mt1L), Fmt1L);
+        F[3] = fmaf(SL, fmaf(chi, vt2L, -mt2L), Fmt2L);
+        F[4] = fmaf(SL, EsL - EL, FEL);
     } else {
         float chi = fdiv(dR, SR - S_star);
-        float EsR = fabsf(dR) > 1e-36f ? chi * (ER * iR + (S_star - vnR) * (S_star + fdiv(pR, dR))) : 0.0f;
-        F[0] = FrR + SR * (chi - rR);
-        F[1] = FmnR + SR * (chi * S_star - mnR);
-        F[2] = Fmt1R + SR * (chi * vt1R - mt1R);
-        F[3] = Fmt2R + SR * (chi * vt2R - mt2R);
-        F[4] = FER + SR * (EsR - ER);
+        float EsR = fabsf(dR) > 1e-36f ? chi * fmaf(S_star - vnR, S_star + fdiv(pR, dR), ER * iR) : 0.0f;
+        F[0] = fmaf(SR, chi - rR, FrR);
+        F[1] = fmaf(SR, fmaf(chi, S_star, -mnR), FmnR);
+        F[2] = fmaf(SR, fmaf(chi, vt1R, -mt1R), Fmt1R);
+        F[3] = fmaf(SR, fmaf(chi, vt2R, -mt2R), Fmt2R);
+        F[4] = fmaf(SR, EsR - ER, FER);
     }
 }
 

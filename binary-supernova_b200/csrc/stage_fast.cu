@@ -16,19 +16,11 @@ const TileVariant kF32Variants[] = {{8, 8, 8, 256, 3}, {16, 8, 4, 256, 3}, {8, 8
 
 template <int TX, int TY, int TZ, int NT, int MINB>
 bsn_status launch_f32(bsn_ctx* ctx, const f64::StageArgs& A) {
-    auto fn = tile::stage_kernel<tile::F32Physics, TX, TY, TZ, NT, MINB>;
-    constexpr int smem = tile::smem_bytes<tile::F32Physics, TX, TY, TZ>();
-    static bool attr_done[64] = {false};
-    int dev = ctx->device & 63;
-    if (!attr_done[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaFuncSetAttribute(stage_kernel_f32)");
-        attr_done[dev] = true;
-    }
-    dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + TZ - 1) / TZ);
-    prof_begin(ctx);
-    fn<<<grid, NT, smem, ctx->stream>>>(A);
-    return launch_check(ctx, "stage_kernel_f32");
+    bool tma_used = false;
+    BSN_TRY((tile::launch_tma<tile::F32Physics, TX, TY, TZ, NT, MINB>(ctx, A, "stage_kernel_f32_tma", &tma_used)));
+    if (tma_used) return BSN_OK;
+    return tile::launch_plain<tile::F32Physics, TX, TY, TZ, NT, MINB>(
+        ctx, A, tile::smem_bytes<tile::F32Physics, TX, TY, TZ>(), "stage_kernel_f32");
 }
 }  // namespace
 

@@ -16,6 +16,7 @@
 #pragma once
 
 #include "stage_f64.cuh"
+#include "tma.cuh"
 
 namespace bsn {
 namespace tile {
@@ -132,7 +133,7 @@ __device__ __forceinline__ void cross_cell(int e, int a0, int b0, int c0, const 
     }
 }
 
-template <class P, int TX, int TY, int TZ, int NT, int D>
+template <class P, int TX, int TY, int TZ, int NT, int D, bool LED>
 __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::Consts& k, int a0, int b0, int c0,
                       typename P::real* sC, typename P::real* sF, unsigned char* psm,
                       double (&acc)[Shape<TX, TY, TZ>::NCELL / NT][5], bool quiet_cross, double* sled) {
@@ -238,7 +239,7 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
                 }
             }
         }
-        if (A.ledger && A.led_bnd && (gd == 0 || gd == n[D])) {   // mass through the grid's boundary
+        if (LED && A.ledger && A.led_bnd && (gd == 0 || gd == n[D])) {   // mass through the grid's boundary
             // per unit volume, as the divergence sees it (the flush multiplies by dV)
             const double inv = (D == 0) ? A.idx : (D == 1 ? A.idy : A.idz);
             atomicAdd(&sled[f64::LED_BND], (gd == 0 ? (double)F[0] : -(double)F[0]) * inv);
@@ -345,13 +346,155 @@ __device__ __forceinline__ bool led_counted(const f64::StageArgs& A, int a, int 
              c >= A.led_skip_lo[2] && c < A.led_skip_hi[2]);
 }
 
+// TMA staging state of a CTA (stage_kernel_tma): the tensor maps, the two
+// raw buffers, their mbarriers and the parity each barrier completes next.
+struct TmaCtx {
+    const tma::Maps* M;
+    double* raw[2];
+    uint64_t* bar;
+    uint32_t ph[2];
+};
+
+// Raw-buffer placement of a tile: inside the face buffer when it is free
+// (it is during staging) and large enough, else after the policy's smem.
+// Copies of kChunkCap bytes where the dynamic smem still fits MINB CTAs per
+// SM, else copies small enough for both buffers to sit in the face buffer.
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+struct TmaSmem {
+    using S = Shape<TX, TY, TZ>;
+    static constexpr int FACE_OFF = (int)sizeof(typename P::real) * P::kCols * S::NCROSS;
+    static constexpr int FACE_BYTES = (int)sizeof(typename P::real) * 5 * S::NFACE;
+    static constexpr int APPEND_OFF = (int)(((sizeof(typename P::real) * (P::kCols * S::NCROSS + 5 * S::NFACE) + 16) +
+                                             127) / 128 * 128);
+    static constexpr int in_faces(int rawb) { return FACE_BYTES >= 2 * rawb ? 2 : (FACE_BYTES >= rawb ? 1 : 0); }
+    static constexpr int bytes_for(int rawb) { return APPEND_OFF + (2 - in_faces(rawb)) * rawb; }
+    static constexpr int BUDGET = 233472 / MINB - 2048;   // per-CTA smem that keeps MINB CTAs on an SM
+    static constexpr int CAP = bytes_for(tma::Chunks<TX, TY, TZ, tma::kChunkCap>::RAWB) <= BUDGET
+                                   ? tma::kChunkCap
+                                   : FACE_BYTES / 2 / 128 * 128;
+    using C = tma::Chunks<TX, TY, TZ, CAP>;
+    static constexpr int IN_FACES = in_faces(C::RAWB);
+    static constexpr int BYTES = bytes_for(C::RAWB);   // dynamic smem of the TMA kernel
+    static_assert(FACE_OFF % 128 == 0, "face buffer must start on a 128-byte boundary for TMA copies");
+    // raw buffer 0 always lies in the face buffer (the layouts this path is
+    // verified with); a tile whose copies fit only after the face buffer
+    // keeps the plain loader
+    static constexpr bool OK = IN_FACES >= 1;
+};
+
+// The cross region of block (a0, b0, c0) staged by TMA copies: each copy's
+// cells converted as the plain loader converts them (P::stage, pressure),
+// cells outside the active domain through the boundary map instead.  Returns
+// false on every thread when a copy did not arrive within the wait bound
+// (the error word is set and the copies in flight are waited for, bounded).
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+__device__ bool stage_cross_tma(const f64::StageArgs& A, TmaCtx& T, const Geom& G, const typename P::Consts& k,
+                                int a0, int b0, int c0, typename P::real* sC) {
+    using S = Shape<TX, TY, TZ>;
+    using C = typename TmaSmem<P, TX, TY, TZ, NT, MINB>::C;
+    using real = typename P::real;
+    const int tid = threadIdx.x;
+    const tma::Maps& M = *T.M;
+    const int n[3] = {G.nx, G.ny, G.nz};
+    auto issue = [&](int c, int b) {   // thread 0: copy c into buffer b
+        uint32_t bytes;
+        const CUtensorMap* map;
+        int x, y, z;
+        if (c < C::NA) {
+            map = &M.a; bytes = C::BA; x = 5 * a0;
+            y = b0 + 3 + (c % C::NAY) * C::AY; z = c0 + 3 + (c / C::NAY) * C::AZ;
+        } else if (c < C::NA + C::NY) {
+            const int r = c - C::NA, hi = r >= C::NY / 2, p = hi ? r - C::NY / 2 : r;
+            map = &M.y; bytes = C::BY; x = 5 * (a0 + 2); y = hi ? b0 + TY + 3 : b0; z = c0 + 3 + p * C::YZ;
+        } else {
+            const int r = c - C::NA - C::NY, hi = r >= C::NZ / 2, p = hi ? r - C::NZ / 2 : r;
+            map = &M.z; bytes = C::BZ; x = 5 * (a0 + 2); y = b0 + 3 + p * C::ZY; z = hi ? c0 + TZ + 3 : c0;
+        }
+        tma::fence_proxy_async();   // earlier generic accesses of the buffer before the copy's writes
+        tma::mbar_expect_tx(&T.bar[b], bytes);
+        tma::load_3d(T.raw[b], map, &T.bar[b], x, y, z);
+    };
+    // one staged cell: from the copy (src, 5 doubles) when it lies in the
+    // active domain along axis d, else through the boundary map
+    auto put = [&](int e, int a, int b, int c, int d, const double* src) {
+        const int p = d == 0 ? a : (d == 1 ? b : c);
+        double v[5];
+        bool act = true;
+        if (p >= 0 && p < n[d]) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) v[q] = src[q];
+        } else {
+            load_cell(A, G, d, a, b, c, v, act);
+        }
+        real w[5];
+        P::stage(v, act, A, w);
+#pragma unroll
+        for (int q = 0; q < 5; ++q)
+            if (q < 4 || P::kCols == 6) sC[q * S::NCROSS + e] = w[q];
+        sC[pcol<P::kCols>() * S::NCROSS + e] = P::pressure(w, k);
+    };
+    if (tid == 0) {
+        issue(0, 0);
+        if (C::N > 1) issue(1, 1);
+    }
+    for (int c = 0; c < C::N; ++c) {
+        const int b = c & 1;
+        const bool got = tma::mbar_wait_bounded(&T.bar[b], T.ph[b]);
+        const double* raw = T.raw[b];
+        if (got) {
+            if (c < C::NA) {   // block rows with their x halos: AY rows x AZ planes
+                const int j0 = (c % C::NAY) * C::AY, k0 = (c / C::NAY) * C::AZ;
+                for (int t = tid; t < (TX + 6) * C::AY * C::AZ; t += NT) {
+                    const int ib = t % (TX + 6), r = t / (TX + 6), jb = r % C::AY, kb = r / C::AY;
+                    const int j = j0 + jb, kk = k0 + kb;
+                    const int e = ib < 3 ? S::OXL + ib + 3 * (j + TY * kk)
+                                         : (ib >= TX + 3 ? S::OXH + (ib - TX - 3) + 3 * (j + TY * kk)
+                                                         : (ib - 3) + TX * (j + TY * kk));
+                    put(e, a0 - 3 + ib, b0 + j, c0 + kk, 0, raw + 5 * ib + C::RA * (jb + C::AY * kb));
+                }
+            } else if (c < C::NA + C::NY) {   // y halo rows
+                const int r = c - C::NA, hi = r >= C::NY / 2, p = hi ? r - C::NY / 2 : r;
+                for (int t = tid; t < TX * 3 * C::YZ; t += NT) {
+                    const int i = t % TX, r2 = t / TX, h = r2 % 3, kb = r2 / 3, kk = p * C::YZ + kb;
+                    const int e = (hi ? S::OYH : S::OYL) + i + TX * (h + 3 * kk);
+                    put(e, a0 + i, hi ? b0 + TY + h : b0 - 3 + h, c0 + kk, 1, raw + 5 * (i + 1) + C::RH * (h + 3 * kb));
+                }
+            } else {   // z halo planes
+                const int r = c - C::NA - C::NY, hi = r >= C::NZ / 2, p = hi ? r - C::NZ / 2 : r;
+                for (int t = tid; t < TX * C::ZY * 3; t += NT) {
+                    const int i = t % TX, r2 = t / TX, jb = r2 % C::ZY, h = r2 / C::ZY, j = p * C::ZY + jb;
+                    const int e = (hi ? S::OZH : S::OZL) + i + TX * (j + TY * h);
+                    put(e, a0 + i, b0 + j, hi ? c0 + TZ + h : c0 - 3 + h, 2,
+                        raw + 5 * (i + 1) + C::RH * (jb + C::ZY * h));
+                }
+            }
+        }
+        // every thread is done with buffer b; one decision for the whole CTA
+        const bool ok = __syncthreads_and(got);
+        if (!ok) {
+            if (tid == 0) {
+                if (M.err) atomicOr(M.err, 1u);
+                // the copies still in flight: this one and the other buffer's
+                tma::mbar_wait_bounded(&T.bar[b], T.ph[b]);
+                if (c + 1 < C::N) tma::mbar_wait_bounded(&T.bar[b ^ 1], T.ph[b ^ 1]);
+            }
+            __syncthreads();
+            return false;
+        }
+        T.ph[b] ^= 1u;
+        if (tid == 0 && c + 2 < C::N) issue(c + 2, b);
+    }
+    return true;
+}
+
 // One RK3 stage (or euler3d_rhs!) of the TX x TY x TZ block at active
 // origin (a0, b0, c0): three sweeps, sources, combine, floors, CFL fold.
 // Starts with a barrier (the first sweep's), so a CTA may call it for one
 // block after another.
-template <class P, int TX, int TY, int TZ, int NT>
-__device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int b0, int c0,
-                                            unsigned char* smem_raw, double* red, unsigned int& nanflag) {
+template <class P, int TX, int TY, int TZ, int NT, int MINB = 1, bool LED = false>
+__device__ __forceinline__ bool stage_block(const f64::StageArgs& A, int a0, int b0, int c0,
+                                            unsigned char* smem_raw, double* red, unsigned int& nanflag,
+                                            TmaCtx* T = nullptr) {
     using S = Shape<TX, TY, TZ>;
     using real = typename P::real;
     static_assert(S::NCELL % NT == 0, "cells must divide evenly among threads");
@@ -365,24 +508,30 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
     const typename P::Consts k = P::consts(A);
     unsigned char* psm = policy_smem<P, TX, TY, TZ>(smem_raw);
     double acc[CPT][5];
-    __shared__ double sled[f64::LED_TERMS];   // this block's mass-ledger sums (A.ledger)
-    if (A.ledger && tid < f64::LED_TERMS) sled[tid] = 0.0;   // ordered before use by the staging barriers
+    // this block's mass-ledger sums (LED kernels with A.ledger set; the other
+    // kernels carry no ledger code at all)
+    __shared__ double sled[LED ? f64::LED_TERMS : 1];
+    if (LED && A.ledger && tid < f64::LED_TERMS) sled[tid] = 0.0;   // ordered before use by the staging barriers
     if constexpr (P::kCross) {
         // the block and the halos of all three sweeps, staged once (floors in
         // FP64 on active cells, ghosts raw, pressure once per cell)
         __syncthreads();   // the previous block of a persistent CTA is done with smem
-        for (int e = tid; e < S::NCROSS; e += NT) {
-            int a, b, c, d;
-            cross_cell<TX, TY, TZ>(e, a0, b0, c0, G, a, b, c, d);
-            double v[5];
-            bool act;
-            load_cell(A, G, d, a, b, c, v, act);
-            real w[5];
-            P::stage(v, act, A, w);
+        if (T) {
+            if (!stage_cross_tma<P, TX, TY, TZ, NT, MINB>(A, *T, G, k, a0, b0, c0, sC)) return false;
+        } else {
+            for (int e = tid; e < S::NCROSS; e += NT) {
+                int a, b, c, d;
+                cross_cell<TX, TY, TZ>(e, a0, b0, c0, G, a, b, c, d);
+                double v[5];
+                bool act;
+                load_cell(A, G, d, a, b, c, v, act);
+                real w[5];
+                P::stage(v, act, A, w);
 #pragma unroll
-            for (int q = 0; q < 5; ++q)
-                if (q < 4 || P::kCols == 6) sC[q * S::NCROSS + e] = w[q];
-            sC[pcol<P::kCols>() * S::NCROSS + e] = P::pressure(w, k);
+                for (int q = 0; q < 5; ++q)
+                    if (q < 4 || P::kCols == 6) sC[q * S::NCROSS + e] = w[q];
+                sC[pcol<P::kCols>() * S::NCROSS + e] = P::pressure(w, k);
+            }
         }
     }
     // policies with per-stencil work that only non-uniform data can need (the
@@ -416,13 +565,13 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
                     const int gx = (A.nx + TX - 1) / TX, gy = (A.ny + TY - 1) / TY;
                     A.split_list[atomicAdd(A.split_count, 1u)] = a0 / TX + gx * (b0 / TY + gy * (c0 / TZ));
                 }
-                return;
+                return true;
             }
         }
     }
-    sweep<P, TX, TY, TZ, NT, 0>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[0], sled);
-    sweep<P, TX, TY, TZ, NT, 1>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[1], sled);
-    sweep<P, TX, TY, TZ, NT, 2>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[2], sled);
+    sweep<P, TX, TY, TZ, NT, 0, LED>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[0], sled);
+    sweep<P, TX, TY, TZ, NT, 1, LED>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[1], sled);
+    sweep<P, TX, TY, TZ, NT, 2, LED>(A, G, k, a0, b0, c0, sC, sF, psm, acc, quiet[2], sled);
 
     const double dt = A.dt_dev ? *A.dt_dev : A.dt;
     const f64::BHSrc& BH = A.bh_dev ? *A.bh_dev : A.bh;     // kernel parameters are __grid_constant__
@@ -488,7 +637,7 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
                 if (rr < SK.rs[nb]) {
                     double ts = SK.ts[nb];
                     d[0] -= u0 / ts;
-                    if (A.ledger && led_counted(A, a, b, c)) atomicAdd(&sled[f64::LED_DRAIN], u0 / ts);
+                    if (LED && A.ledger && led_counted(A, a, b, c)) atomicAdd(&sled[f64::LED_DRAIN], u0 / ts);
                     if (SK.torque_free) {
                         double rx = ddx / rr, ry = ddy / rr, rz = ddz / rr;
                         double vx = u1 / u0, vy = u2 / u0, vz = u3 / u0;
@@ -527,16 +676,14 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
 #pragma unroll
             for (int q = 0; q < 5; ++q) w[q] = (1.0 / 3.0) * un[q] + (2.0 / 3.0) * uu[q] + cdt * d[q];
         }
-        if (A.ledger && led_counted(A, a, b, c)) {
-            const double w0 = w[0];
-            P::floor(w, A);
+        const double w0 = w[0];
+        P::floor(w, A);
+        if (LED && A.ledger && led_counted(A, a, b, c)) {
             if (w[0] != w0) atomicAdd(&sled[f64::LED_POST], w[0] - w0);
             if (A.stage > 1) {   // the input's floors reach the combine in stages 2 and 3
                 const double raw = A.Uin[off];
                 if (u0 != raw) atomicAdd(&sled[f64::LED_PRE], u0 - raw);
             }
-        } else {
-            P::floor(w, A);
         }
 #pragma unroll
         for (int q = 0; q < 5; ++q) A.Uout[off + q] = w[q];
@@ -557,21 +704,58 @@ __device__ __forceinline__ void stage_block(const f64::StageArgs& A, int a0, int
             if (nanflag) atomicOr(A.cfl_nan, 1u);
         }
     }
-    if (A.ledger) {
+    if (LED && A.ledger) {
         __syncthreads();   // every cell's and face's contribution is in sled
         if (tid < f64::LED_TERMS && sled[tid] != 0.0) atomicAdd(&A.ledger[tid], sled[tid] * (A.dx * A.dy * A.dz));
     }
+    return true;
 }
 
 // One launch per stage on one grid: CTA (x, y, z) owns block (x, y, z).
-template <class P, int TX, int TY, int TZ, int NT, int MINB>
+// LED: the instantiation that keeps the mass ledger (A.ledger) -- the driver
+// loops' launches; the others compile no ledger code.
+template <class P, int TX, int TY, int TZ, int NT, int MINB, bool LED = false>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__ f64::StageArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[NT / 32];
     __shared__ unsigned int nanflag;
     if (A.done_dev && *A.done_dev) return;   // device time loop already reached t_end
     P::prologue(policy_smem<P, TX, TY, TZ>(smem_raw), A, NT);   // visible after the first barrier
-    stage_block<P, TX, TY, TZ, NT>(A, blockIdx.x * TX, blockIdx.y * TY, blockIdx.z * TZ, smem_raw, red, nanflag);
+    stage_block<P, TX, TY, TZ, NT, MINB, LED>(A, blockIdx.x * TX, blockIdx.y * TY, blockIdx.z * TZ, smem_raw, red,
+                                              nanflag);
+}
+
+// stage_kernel with the cross region staged by TMA copies (tma.cuh): one
+// block per CTA, as stage_kernel.  Launched only where build_maps accepted
+// the grid (uniform grid, tile dividing it, even nx, no ghost buffer).
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    stage_kernel_tma(const __grid_constant__ f64::StageArgs A, const __grid_constant__ tma::Maps M) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ double red[NT / 32];
+    __shared__ unsigned int nanflag;
+    __shared__ __align__(8) uint64_t bar[2];
+    if (A.done_dev && *A.done_dev) return;
+    using TS = TmaSmem<P, TX, TY, TZ, NT, MINB>;
+    using C = typename TS::C;
+    P::prologue(policy_smem<P, TX, TY, TZ>(smem_raw), A, NT);
+    if (threadIdx.x == 0) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+    unsigned char* face = smem_raw + TS::FACE_OFF;
+    unsigned char* app = smem_raw + TS::APPEND_OFF;
+    TmaCtx T;
+    T.M = &M;
+    T.raw[0] = reinterpret_cast<double*>(TS::IN_FACES >= 1 ? face : app);
+    T.raw[1] = reinterpret_cast<double*>(TS::IN_FACES == 2 ? face + C::RAWB
+                                                             : (TS::IN_FACES == 1 ? app : app + C::RAWB));
+    T.bar = bar;
+    T.ph[0] = T.ph[1] = 0u;
+    stage_block<P, TX, TY, TZ, NT, MINB>(A, blockIdx.x * TX, blockIdx.y * TY, blockIdx.z * TZ, smem_raw, red, nanflag,
+                                         &T);
 }
 
 // The listed blocks of a split stage (written by its screening launch, which
@@ -599,7 +783,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_list(const __grid_const
 // blocks from an atomic queue when one is given.  Each level keeps its own
 // arguments (states, dt, flux registers, boundary capture), so every block
 // computes exactly what its level's own launch would.
-template <class P, int TX, int TY, int TZ, int NT, int MINB>
+template <class P, int TX, int TY, int TZ, int NT, int MINB, bool LED = false>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel_batch(const __grid_constant__ f64::StageBatch B) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[NT / 32];
@@ -619,8 +803,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel_batch(const __grid_cons
         while (l + 1 < B.nlev && t >= B.start[l + 1]) ++l;
         const f64::StageArgs& A = B.lv[l];
         const int r = t - B.start[l], gx = B.gx[l], gy = B.gy[l];
-        stage_block<P, TX, TY, TZ, NT>(A, (r % gx) * TX, ((r / gx) % gy) * TY, (r / (gx * gy)) * TZ, smem_raw, red,
-                                       nanflag);
+        stage_block<P, TX, TY, TZ, NT, MINB, LED>(A, (r % gx) * TX, ((r / gx) % gy) * TY, (r / (gx * gy)) * TZ,
+                                                  smem_raw, red, nanflag);
     }
 }
 
@@ -632,9 +816,9 @@ constexpr int smem_bytes() {
 
 // Host: launch stage_kernel_batch for the levels in B with a persistent grid
 // (at most as many CTAs as fit on the device at once).
-template <class P, int TX, int TY, int TZ, int NT, int MINB>
-bsn_status launch_batch(bsn_ctx* ctx, f64::StageBatch B, int smem, const char* name) {
-    auto fn = stage_kernel_batch<P, TX, TY, TZ, NT, MINB>;
+template <class P, int TX, int TY, int TZ, int NT, int MINB, bool LED>
+bsn_status launch_batch_led(bsn_ctx* ctx, f64::StageBatch B, int smem, const char* name) {
+    auto fn = stage_kernel_batch<P, TX, TY, TZ, NT, MINB, LED>;
     static int occ[64] = {0}, sms[64] = {0};
     const int dev = ctx->device & 63;
     if (!occ[dev]) {
@@ -662,6 +846,65 @@ bsn_status launch_batch(bsn_ctx* ctx, f64::StageBatch B, int smem, const char* n
     long long grid = std::min<long long>(total, (long long)occ[dev] * sms[dev]);
     prof_begin(ctx);
     fn<<<(unsigned)grid, NT, smem, ctx->stream>>>(B);
+    return launch_check(ctx, name);
+}
+
+// the ledger instantiation when any level keeps a mass ledger
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+bsn_status launch_batch(bsn_ctx* ctx, const f64::StageBatch& B, int smem, const char* name) {
+    bool led = false;
+    for (int l = 0; l < B.nlev && l < f64::MAXLEV; ++l) led = led || B.lv[l].ledger;
+    return led ? launch_batch_led<P, TX, TY, TZ, NT, MINB, true>(ctx, B, smem, name)
+               : launch_batch_led<P, TX, TY, TZ, NT, MINB, false>(ctx, B, smem, name);
+}
+
+// Host: one stage on one grid through stage_kernel (the ledger
+// instantiation when A keeps a mass ledger); smem is the dynamic smem.
+template <class P, int TX, int TY, int TZ, int NT, int MINB, bool LED>
+bsn_status launch_plain_led(bsn_ctx* ctx, const f64::StageArgs& A, int smem, const char* name) {
+    auto fn = stage_kernel<P, TX, TY, TZ, NT, MINB, LED>;
+    static bool attr_done[64] = {false};
+    const int dev = ctx->device & 63;
+    if (!attr_done[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaFuncSetAttribute(stage_kernel)");
+        attr_done[dev] = true;
+    }
+    dim3 grid((A.nx + TX - 1) / TX, (A.ny + TY - 1) / TY, (A.nz + TZ - 1) / TZ);
+    prof_begin(ctx);
+    fn<<<grid, NT, smem, ctx->stream>>>(A);
+    return launch_check(ctx, name);
+}
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+bsn_status launch_plain(bsn_ctx* ctx, const f64::StageArgs& A, int smem, const char* name) {
+    return A.ledger ? launch_plain_led<P, TX, TY, TZ, NT, MINB, true>(ctx, A, smem, name)
+                    : launch_plain_led<P, TX, TY, TZ, NT, MINB, false>(ctx, A, smem, name);
+}
+
+// Host: one stage on one grid through stage_kernel_tma when the grid
+// qualifies (tma::build_maps); *used tells whether it was launched.
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+bsn_status launch_tma(bsn_ctx* ctx, const f64::StageArgs& A, const char* name, bool* used) {
+    using TS = TmaSmem<P, TX, TY, TZ, NT, MINB>;
+    using C = typename TS::C;
+    *used = false;
+    if constexpr (!TS::OK) return BSN_OK;
+    if (A.ledger) return BSN_OK;   // the TMA kernel keeps no mass ledger
+    tma::Maps M;
+    if (!tma::build_maps(ctx, A, TX, TY, TZ, C::AY, C::AZ, C::YZ, C::ZY, M)) return BSN_OK;
+    auto fn = stage_kernel_tma<P, TX, TY, TZ, NT, MINB>;
+    static bool attr_done[64] = {false};
+    const int dev = ctx->device & 63;
+    if (!attr_done[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, TS::BYTES);
+        if (e != cudaSuccess) return cuda_check(ctx, e, "cudaFuncSetAttribute(stage_kernel_tma)");
+        attr_done[dev] = true;
+    }
+    dim3 grid(A.nx / TX, A.ny / TY, A.nz / TZ);
+    prof_begin(ctx);
+    fn<<<grid, NT, TS::BYTES, ctx->stream>>>(A, M);
+    *used = true;
+    ctx->tma_used_last = 1;
     return launch_check(ctx, name);
 }
 

@@ -164,6 +164,21 @@ bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double
  * bsn_ctx_set_tile forces variant `variant` (-1: autotune again);
  * bsn_ctx_get_tile reports the choice for a grid as {tx, ty, tz, threads,
  * minimum CTAs per SM the kernel's registers are capped for}. */
+/* Staging of the fused stage kernel's block and halos by TMA tensor copies
+ * (cp.async.bulk.tensor into shared memory; possible where the tile divides
+ * the grid, nx is even and no ghost buffer is involved) beside the plain
+ * per-thread loader.  With on != 0 (the default) the autotuner times both
+ * stagings of every tile variant and keeps the faster, and a forced variant
+ * (bsn_ctx_set_tile) uses TMA wherever possible; on = 0 keeps the plain
+ * loader.  Results are the same either way; the switch releases the
+ * context's captured step graphs.  bsn_ctx_get_tma reports the setting,
+ * bsn_ctx_get_tile_tma whether a grid's chosen tile is TMA-staged (1), not
+ * (0) or not chosen yet (-1).  A staging copy that does not arrive within the
+ * kernel's wait bound sets an error word, reported as BSN_ERR_TIMEOUT by the
+ * next bsn_ctx_synchronize or device time loop. */
+bsn_status bsn_ctx_set_tma(bsn_ctx* ctx, int on);
+int        bsn_ctx_get_tma(const bsn_ctx* ctx);
+int        bsn_ctx_get_tile_tma(bsn_ctx* ctx, int precision, int nx, int ny, int nz);
 int        bsn_tile_variant_count(int precision);
 bsn_status bsn_ctx_set_tile(bsn_ctx* ctx, int precision, int variant);
 bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int ny, int nz, int out[5]);
