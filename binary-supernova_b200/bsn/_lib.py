@@ -80,6 +80,8 @@ SIGNATURES = {
     "bsn_learned_set_params": (_I, [_V, _P, _P]),
     "bsn_learned_eval": (_I, [_V, _P, _LL, _P, _P, _I]),
     "bsn_ctx_set_tma": (_I, [_V, _I]),
+    "bsn_ctx_set_stiff_guard": (_I, [_V, _I]),
+    "bsn_euler3d_rhs_f32": (_I, [_V, _P, _P, _P, _P, _P, _I, _I, _I, _D, _D, _D, _D, _I, _D, _D, _I]),
     "bsn_ctx_get_tma": (_I, [_V]),
     "bsn_ctx_get_tile_tma": (_I, [_V, _I, _I, _I, _I]),
     "bsn_tile_variant_count": (_I, [_I]),

@@ -32,7 +32,7 @@ __all__ = [
     "apply_sg_force_level", "apply_sg_force_slab", "coupled_step", "FMRGrid3D", "fmr3d_step", "cfl_dt_fmr3d", "solve_fmr_poisson",
     "restrict_density_to_coarse", "FMRHierarchy3D", "fmr_nested_step", "cfl_dt_fmr_nested",
     "fmr_nested_run_steps", "coupled_nested_run_steps", "rotating_frame_source", "relax_damping_source",
-    "relax_ic", "DIAG_FIELDS", "DIAG_RECORD", "set_tma", "get_tma", "get_tile_tma",
+    "relax_ic", "DIAG_FIELDS", "DIAG_RECORD", "set_tma", "get_tma", "get_tile_tma", "set_stiff_guard",
 ]
 
 # ---------------------------------------------------------------------------
@@ -171,6 +171,17 @@ def euler3d_rhs(dU, Fx, Fy, Fz, U, nx, ny, nz, dx, dy, dz, gamma, *, bc="outflow
     _check_state(U, nx, ny, nz)
     _check_state(dU, nx, ny, nz, "dU")
     _call("bsn_euler3d_rhs_f64", context(), _ptr(dU), _ptr(Fx), _ptr(Fy), _ptr(Fz), _ptr(U), nx, ny, nz,
+          float(dx), float(dy), float(dz), float(gamma), BC[bc], float(rho_floor), float(P_floor), int(fill_ghosts))
+
+
+def euler3d_rhs_f32(dU, Fx, Fy, Fz, U, nx, ny, nz, dx, dy, dz, gamma, *, bc="outflow", rho_floor=0.0, P_floor=0.0,
+                    fill_ghosts=True):
+    """euler3d_rhs! with the FP32 stencils (src/euler3d.jl:182-205): face
+    fluxes from the FP32 reconstruction and HLLC (stiff faces in FP64 when the
+    context's stiff guard is on), stored as FP32 values; divergence in FP64."""
+    _check_state(U, nx, ny, nz)
+    _check_state(dU, nx, ny, nz, "dU")
+    _call("bsn_euler3d_rhs_f32", context(), _ptr(dU), _ptr(Fx), _ptr(Fy), _ptr(Fz), _ptr(U), nx, ny, nz,
           float(dx), float(dy), float(dz), float(gamma), BC[bc], float(rho_floor), float(P_floor), int(fill_ghosts))
 
 
@@ -594,6 +605,13 @@ def set_tma(on=True):
     _call("bsn_ctx_set_tma", context(), int(bool(on)))
 
 
+def set_stiff_guard(on=True):
+    """Uniform-grid FP32 steps: compute faces whose density stencil spans more
+    than three decades in FP64 (always on in the driver, FMR and relaxation
+    loops)."""
+    _call("bsn_ctx_set_stiff_guard", context(), int(bool(on)))
+
+
 def get_tma() -> bool:
     return bool(load().bsn_ctx_get_tma(context()))
 
@@ -632,5 +650,5 @@ def set_profiling(on: bool):
     _call("bsn_ctx_set_profiling", context(), int(bool(on)))
 
 
-__all__ += ["euler3d_step_f32", "euler3d_step_learned", "run_steps", "fmr3d_run_steps", "coupled_run_steps", "diagnostics", "tile_variants", "set_tile", "get_tile", "kernel_time",
+__all__ += ["euler3d_rhs_f32", "euler3d_step_f32", "euler3d_step_learned", "run_steps", "fmr3d_run_steps", "coupled_run_steps", "diagnostics", "tile_variants", "set_tile", "get_tile", "kernel_time",
             "set_profiling", "fp_peak", "PREC"]

@@ -48,6 +48,7 @@ struct bsn_ctx {
     int tma_on = 1;
     unsigned int* tma_err = nullptr;
     int tma_now = 0;                 // the launch being made may use TMA staging (autotune.cu)
+    int stiff_guard = 0;             // uniform-grid FP32 steps: stiff faces in FP64 (bsn_ctx_set_stiff_guard)
     int tma_used_last = 0;           // the last stage launch used it
 };
 

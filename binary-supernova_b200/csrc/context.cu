@@ -154,6 +154,14 @@ extern "C" bsn_status bsn_ctx_set_stream(bsn_ctx* ctx, void* stream) {
     return BSN_OK;
 }
 
+extern "C" bsn_status bsn_ctx_set_stiff_guard(bsn_ctx* ctx, int on) {
+    if (!ctx) return BSN_ERR_ARG;
+    BSN_TRY(cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"));
+    ctx->stiff_guard = on ? 1 : 0;
+    bsn::run_state_free(ctx);   // the device time loop's graph holds the kernels chosen before
+    return BSN_OK;
+}
+
 extern "C" bsn_status bsn_ctx_synchronize(bsn_ctx* ctx) {
     if (!ctx) return BSN_ERR_ARG;
     BSN_TRY(cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"));

@@ -331,6 +331,7 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
     stage_args_init(base, nx, ny, nz, dx, dx, dx, gamma, BSN_BC_OUTFLOW, rho_floor, P_floor);
     base.x0 = x0; base.y0 = y0; base.z0 = z0;
     base.Uin = U; base.Un = U;
+    base.stiff_guard = 1;   // near-vacuum cells beside the sinks: stiff FP32 faces in FP64
     {
         double* scratch = (double*)slot(ctx, SLOT_UN, bytes, &st); BSN_TRY(st);
         BSN_TRY(stage_autotune(ctx, precision, base, scratch));
@@ -527,6 +528,7 @@ extern "C" bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2*
         a.x0 = ox[l]; a.y0 = oy[l]; a.z0 = oz[l];
         if (nbh > 0) { a.use_bh = 1; a.bh_dev = &r->bsrc; a.use_sink = 1; a.sk_dev = &r->ssrc; }
         plan.led_raw[l] = &r->led[l][0][0];
+        a.stiff_guard = 1;
     }
     plan.led_tot = r->led_tot;
     if (self_gravity) {

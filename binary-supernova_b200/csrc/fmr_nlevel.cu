@@ -289,6 +289,7 @@ bsn_status make_plan(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, int prec, 
         f64::StageArgs& a = plan.base[l];
         const NLevel& v = plan.L[l];
         stage_args_init(a, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz, plan.gamma, plan.bc, plan.rho_floor, plan.P_floor);
+        a.stiff_guard = 1;   // floor atmospheres beside dense gas: stiff FP32 faces in FP64
         if (l < plan.nl - 1) {
             const Geo& G = plan.P[l].G;
             a.use_reg = 1;

@@ -458,6 +458,7 @@ struct State {
 namespace tile {
 
 struct F32Learned {
+    static constexpr bool kStiffFallback = false;   // the warp path reconstructs all faces in FP32
     using real = float;
     static constexpr bool kCenterFromSmem = false;
     static constexpr bool kWarpFaces = true;

@@ -493,6 +493,7 @@ extern "C" bsn_status bsn_coupled_step_f64(bsn_ctx* ctx, double* U, bsn_bh* bhs,
     }
     f64::StageArgs A;
     stage_args_init(A, nx, ny, nz, dx, dx, dx, gamma, BSN_BC_OUTFLOW, rho_floor, P_floor);
+    A.stiff_guard = 1;
     A.x0 = x0; A.y0 = y0; A.z0 = z0;
     if (nbh > 0) {
         BSN_TRY(fill_bh(ctx, bhs, nbh, A.bh));

@@ -13,6 +13,7 @@ namespace tile {
 
 struct F32Physics {
     using real = float;
+    static constexpr bool kStiffFallback = false;
     static constexpr bool kCross = true;
     static constexpr int kCols = 5;                  // rho, m, P: the epilogue reloads the FP64 state
     static constexpr bool kCenterFromSmem = false;  // smem holds FP32 copies: reload FP64 state
@@ -40,6 +41,15 @@ struct F32Physics {
     __device__ static void flux(const float (&c)[6][6], const Consts& k, float F[5]) {
         f32::interface_flux<D>(c, k.g, k.gm1, k.inv_gm1, k.gg, F);
     }
+};
+
+// The FP32 policy with stiff faces in FP64: a face whose density stencil
+// spans more than three decades is computed from the FP64 state by the FP64
+// path's arithmetic (stage_tile.cuh face_flux_f64).  Launched where
+// A.stiff_guard is set: the driver loops with sinks, the FMR and relaxation
+// loops (near-vacuum cells beside dense gas), or any grid on request.
+struct F32Guarded : F32Physics {
+    static constexpr bool kStiffFallback = true;
 };
 
 }  // namespace tile

@@ -85,6 +85,9 @@ struct StageArgs {
     double* ledger;
     int led_bnd;
     int led_skip_lo[3], led_skip_hi[3];
+    // FP32 path: compute faces whose density stencil spans more than three
+    // decades in FP64 (the F32Guarded policy)
+    int stiff_guard;
 };
 
 enum { LED_BND = 0, LED_DRAIN = 1, LED_POST = 2, LED_PRE = 3, LED_TERMS = 4 };

@@ -14,13 +14,29 @@ namespace {
 const TileVariant kF32Variants[] = {{8, 8, 8, 256, 3}, {16, 8, 4, 256, 3}, {8, 8, 4, 128, 6}, {16, 8, 8, 256, 2},
                                      {16, 16, 4, 256, 2}};
 
+template <class P, int TX, int TY, int TZ, int NT, int MINB>
+bsn_status launch_f32_policy(bsn_ctx* ctx, const f64::StageArgs& A) {
+    bool tma_used = false;
+    BSN_TRY((tile::launch_tma<P, TX, TY, TZ, NT, MINB>(ctx, A, "stage_kernel_f32_tma", &tma_used)));
+    if (tma_used) return BSN_OK;
+    return tile::launch_plain<P, TX, TY, TZ, NT, MINB>(ctx, A, tile::smem_bytes<P, TX, TY, TZ>(), "stage_kernel_f32");
+}
 template <int TX, int TY, int TZ, int NT, int MINB>
 bsn_status launch_f32(bsn_ctx* ctx, const f64::StageArgs& A) {
-    bool tma_used = false;
-    BSN_TRY((tile::launch_tma<tile::F32Physics, TX, TY, TZ, NT, MINB>(ctx, A, "stage_kernel_f32_tma", &tma_used)));
-    if (tma_used) return BSN_OK;
-    return tile::launch_plain<tile::F32Physics, TX, TY, TZ, NT, MINB>(
-        ctx, A, tile::smem_bytes<tile::F32Physics, TX, TY, TZ>(), "stage_kernel_f32");
+    return A.stiff_guard ? launch_f32_policy<tile::F32Guarded, TX, TY, TZ, NT, MINB>(ctx, A)
+                         : launch_f32_policy<tile::F32Physics, TX, TY, TZ, NT, MINB>(ctx, A);
+}
+template <class P>
+bsn_status launch_f32_batch(bsn_ctx* ctx, int idx, const f64::StageBatch& B) {
+    const char* nm = "stage_kernel_batch_f32";
+    switch (idx) {
+        case 0: return tile::launch_batch<P, 8, 8, 8, 256, 3>(ctx, B, tile::smem_bytes<P, 8, 8, 8>(), nm);
+        case 1: return tile::launch_batch<P, 16, 8, 4, 256, 3>(ctx, B, tile::smem_bytes<P, 16, 8, 4>(), nm);
+        case 2: return tile::launch_batch<P, 8, 8, 4, 128, 6>(ctx, B, tile::smem_bytes<P, 8, 8, 4>(), nm);
+        case 3: return tile::launch_batch<P, 16, 8, 8, 256, 2>(ctx, B, tile::smem_bytes<P, 16, 8, 8>(), nm);
+        case 4: return tile::launch_batch<P, 16, 16, 4, 256, 2>(ctx, B, tile::smem_bytes<P, 16, 16, 4>(), nm);
+        default: return set_err(ctx, BSN_ERR_ARG, "no FP32 tile variant %d", idx);
+    }
 }
 }  // namespace
 
@@ -38,16 +54,9 @@ bsn_status f32_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A) {
 }
 
 bsn_status f32_launch_batch_variant(bsn_ctx* ctx, int idx, const f64::StageBatch& B) {
-    using P = tile::F32Physics;
-    const char* nm = "stage_kernel_batch_f32";
-    switch (idx) {
-        case 0: return tile::launch_batch<P, 8, 8, 8, 256, 3>(ctx, B, tile::smem_bytes<P, 8, 8, 8>(), nm);
-        case 1: return tile::launch_batch<P, 16, 8, 4, 256, 3>(ctx, B, tile::smem_bytes<P, 16, 8, 4>(), nm);
-        case 2: return tile::launch_batch<P, 8, 8, 4, 128, 6>(ctx, B, tile::smem_bytes<P, 8, 8, 4>(), nm);
-        case 3: return tile::launch_batch<P, 16, 8, 8, 256, 2>(ctx, B, tile::smem_bytes<P, 16, 8, 8>(), nm);
-        case 4: return tile::launch_batch<P, 16, 16, 4, 256, 2>(ctx, B, tile::smem_bytes<P, 16, 16, 4>(), nm);
-        default: return set_err(ctx, BSN_ERR_ARG, "no FP32 tile variant %d", idx);
-    }
+    bool guard = false;
+    for (int l = 0; l < B.nlev && l < f64::MAXLEV; ++l) guard = guard || B.lv[l].stiff_guard;
+    return guard ? launch_f32_batch<tile::F32Guarded>(ctx, idx, B) : launch_f32_batch<tile::F32Physics>(ctx, idx, B);
 }
 
 }  // namespace bsn

@@ -46,6 +46,7 @@ __host__ __device__ constexpr int pcol() { return COLS - 1; }
 // Physics policies --------------------------------------------------------
 struct F64Physics {
     using real = double;
+    static constexpr bool kStiffFallback = false;   // (already FP64)
     static constexpr bool kCross = true;             // stage the block and all halos once
     static constexpr bool kCenterFromSmem = true;   // smem holds the floored FP64 state
     static constexpr int kCols = 6;                 // staged columns: rho, m, E (read back by the epilogue), P
@@ -131,6 +132,43 @@ __device__ __forceinline__ void cross_cell(int e, int a0, int b0, int c0, const 
         int i = r % TX, rr = r / TX, j = rr % TY, h = rr / TY;
         a = a0 + i; b = b0 + j; c = hi ? c0 + TZ + h : c0 - 3 + h; d = 2;
     }
+}
+
+// Density contrast of a face's six-cell stencil above which a reduced-
+// precision policy computes that face in FP64: where min rho < 1e-3 max rho
+// the face states reconstructed on the thin side carry the rounding of the
+// dense side's values (FP32: 1e-7 of them), i.e. relative errors of 1e-4 and
+// more in the thin cell, whose velocity m / rho then runs away beside sinks.
+constexpr float kStiffContrast = 1e-3f;
+
+__device__ __forceinline__ bool stiff_stencil(const float (&c)[6][6]) {
+    float lo = c[0][0], hi = c[0][0];
+#pragma unroll
+    for (int s = 1; s < 6; ++s) { lo = fminf(lo, c[s][0]); hi = fmaxf(hi, c[s][0]); }
+    return lo < kStiffContrast * hi;
+}
+
+// The FP64 flux of the face between active cells p_D - 1 and p_D along D
+// (p: the face's cell on the high side), from the FP64 state as the FP64
+// path stages it (boundary map, floors on active cells, pressure once):
+// the same operations, so the same bits as the FP64 path's flux there.
+template <int D>
+__device__ __noinline__ void face_flux_f64(const f64::StageArgs& A, int a, int b, int c, double F[5]) {
+    Geom G(A.nx, A.ny, A.nz);
+    double cs[6][6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        int p[3] = {a, b, c};
+        p[D] += s - 3;
+        double v[5];
+        bool act;
+        load_cell(A, G, D, p[0], p[1], p[2], v, act);
+        if (act) f64::apply_floor(v[0], v[1], v[2], v[3], v[4], A.rho_floor, A.P_floor, A.Pfl_gm1, A.gm1);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) cs[s][q] = v[q];
+        cs[s][5] = f64::cell_pressure(v[0], v[1], v[2], v[3], v[4], A.gm1);
+    }
+    f64::interface_flux<D>(cs, A.g, A.gm1, F);
 }
 
 template <class P, int TX, int TY, int TZ, int NT, int D, bool LED>
@@ -263,9 +301,14 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
         }
         return valid;
     };
-    // thread-per-face loop (the plain stencil physics)
+    // thread-per-face loop (the plain stencil physics); faces whose density
+    // stencil is stiff (kStiffFallback policies) are left to a second pass
+    // that computes them in FP64, so the main loop keeps its registers
     auto plain_faces = [&]() {
-        for (int f = tid; f < NF; f += NT) {
+        static_assert(NF <= 32 * NT, "one bit per face of a thread");
+        unsigned stiff = 0u;
+        int it = 0;
+        for (int f = tid; f < NF; f += NT, ++it) {
             int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
             if (!face_valid(fx, fy, fz)) continue;
             real c[6][6];
@@ -278,9 +321,24 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
                     c[s][q] = (q == 4 && P::kCols == 5) ? (real)0 : sC[col * FSTR + e];
                 }
             }
+            if constexpr (P::kStiffFallback) {
+                if (stiff_stencil(c)) { stiff |= 1u << it; continue; }
+            }
             real F[5];
             P::template flux<D>(c, k, F);
             emit(f, fx, fy, fz, F);
+        }
+        if constexpr (P::kStiffFallback) {
+            for (; stiff; stiff &= stiff - 1u) {
+                const int f = tid + NT * (__ffs(stiff) - 1);
+                const int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
+                double F64[5];
+                face_flux_f64<D>(A, o[0] + fx, o[1] + fy, o[2] + fz, F64);
+                real F[5];
+#pragma unroll
+                for (int q = 0; q < 5; ++q) F[q] = (real)F64[q];
+                emit(f, fx, fy, fz, F);
+            }
         }
     };
     if constexpr (P::kWarpFaces) {

@@ -141,6 +141,24 @@ enum { BSN_PREC_F64 = 0,     /* stencils in FP64, bit-identical to the reference
                                 divergence, sources and RK3 accumulation in FP64 */
        BSN_PREC_LEARNED = 2  /* as BSN_PREC_F32, with the WENO-Z weights of smooth
                                 stencils from the learned network (see below) */ };
+/* FP32 stencils meet near-vacuum cells beside dense gas (a sink's
+ * surroundings, a floor atmosphere): where a face's six-cell density stencil
+ * spans more than three decades, FP32 rounding of the dense side's values is
+ * 1e-4 and more of the thin cell's, and its velocity m / rho can run away.
+ * Such faces are computed in FP64 by the FP64 path's arithmetic in the
+ * driver loops with sinks, the FMR and the relaxation loops; the uniform-grid
+ * FP32 steps (bsn_euler3d_step_f32, bsn_run_steps) do it when on != 0 here
+ * (default off: a few percent of the step).  Releases the context's
+ * captured time-loop graph. */
+bsn_status bsn_ctx_set_stiff_guard(bsn_ctx* ctx, int on);
+/* euler3d_rhs! with FP32 stencils (BSN_PREC_F32): the same semantics as
+ * bsn_euler3d_rhs_f64 (mutates U: ghost fill, floors; fills the optional
+ * Fx/Fy/Fz and dU), the face fluxes from the FP32 reconstruction and HLLC
+ * (or, with the stiff guard, in FP64 where the density stencil spans more than
+ * three decades), stored as FP32 values, the divergence in FP64. */
+bsn_status bsn_euler3d_rhs_f32(bsn_ctx* ctx, double* dU, double* Fx, double* Fy, double* Fz, double* U,
+                               int nx, int ny, int nz, double dx, double dy, double dz, double gamma, int bc,
+                               double rho_floor, double P_floor, int fill_ghosts);
 /* euler3d_step! with FP32 stencils (BSN_PREC_F32); same arguments. */
 bsn_status bsn_euler3d_step_f32(bsn_ctx* ctx, double* U, int nx, int ny, int nz,
                                 double dx, double dy, double dz, double dt, double gamma,

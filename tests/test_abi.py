@@ -45,6 +45,15 @@ def test_python_binding_covers_header():
     assert sorted(SIGNATURES) == declared()
 
 
+def test_every_public_api_function_is_exported():
+    import ast
+    import bsn.api as api
+    tree = ast.parse(open(api.__file__).read())
+    public = [n.name for n in tree.body
+              if isinstance(n, (ast.FunctionDef, ast.ClassDef)) and not n.name.startswith("_")]
+    assert [n for n in public if n not in api.__all__] == []
+
+
 def test_host_orbit_entry_points_without_gpu(lib):
     # bsn_nbody_step / bsn_kepler_* are host FP64 code paths of the library
     import bsn._lib as B

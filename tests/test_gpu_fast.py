@@ -11,6 +11,7 @@ the FP32-stencil fast path.
   t = 0.1 and on one random-state step.
 """
 import numpy as np
+import torch
 import pytest
 
 from gpu_util import NG, assert_bitwise, dev, host, random_state
@@ -146,3 +147,45 @@ def test_poisson_fp32_transforms_close_to_fp64(bsn, dims):
     p32 = bsn.solve_poisson_isolated(rho, nx, ny, nz, h, h, h, precision="f32")
     err = (p32 - p64).abs().max().item() / p64.abs().max().item()
     assert 0 < err < 1e-5, err
+
+
+def test_fp32_step_takes_fp64_fluxes_at_stiff_faces(orc, bsn):
+    """Faces whose six-cell density stencil spans more than three decades are
+    computed in FP64 by the FP32 path when the stiff guard is on (FP32
+    rounding of the dense side's values would be 1e-4 and more of the thin
+    cell's).  On a 3-D checkerboard of O(1) and 1e-4 densities every face of
+    every axis is stiff, so the guarded FP32 face fluxes are the FP64 fluxes
+    rounded to FP32 (relative error <= 2^-24 per face, 1e-7 of the axis's
+    largest flux taken here), while unguarded FP32 stencils miss them by far
+    more.  Fluxes rather than a step are compared: the checkerboard's step
+    switches WENO/HLLC branches on 1e-12 perturbations, so its increments
+    are not a conditioned measure of the face arithmetic."""
+    n, d, g = (16, 16, 16), (0.05, 0.05, 0.05), 5 / 3
+    U = random_state(*n, seed=91, gamma=g, jumps=False)
+    a = (slice(3, -3),) * 3
+    i, j, k = np.meshgrid(*(np.arange(m) for m in n), indexing="ij")
+    scale = np.where((i + j + k) % 2 == 1, 1e-4, 1.0)
+    for q in range(5):
+        U[(q,) + a] = U[(q,) + a] * scale
+    orc.fill_ghost_3d_outflow(U)
+    flux = {}
+    for name, guard in (("f64", None), ("guarded", True), ("plain", False)):
+        Ud = dev(U)
+        dUd = torch.zeros_like(Ud)
+        F = [torch.zeros_like(dev(f)) for f in orc.flux_arrays(*n)]
+        if guard is None:
+            bsn.euler3d_rhs(dUd, *F, Ud, *n, *d, g, rho_floor=1e-10, P_floor=1e-14)
+        else:
+            bsn.set_stiff_guard(guard)
+            try:
+                bsn.euler3d_rhs_f32(dUd, *F, Ud, *n, *d, g, rho_floor=1e-10, P_floor=1e-14)
+            finally:
+                bsn.set_stiff_guard(False)
+        flux[name] = [host(f) for f in F]
+    err = {}
+    for name in ("guarded", "plain"):
+        err[name] = max(float(np.abs(f - r)[q].max() / np.abs(r[q]).max())
+                        for f, r in zip(flux[name], flux["f64"]) for q in range(5))
+    print("face fluxes vs FP64, max relative: guarded %.2e, plain FP32 %.2e" % (err["guarded"], err["plain"]))
+    assert err["guarded"] < 1e-7, err
+    assert err["plain"] > 100 * err["guarded"], err
