@@ -813,9 +813,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-fmr", action="store_true",
                     help="skip the two-level FMR polytrope and binary-BH coupled-loop timings")
-    ap.add_argument("--workload", default="sedov", choices=["sedov", "binary_nested", "polytrope_fmr"],
+    ap.add_argument("--workload", default="sedov", choices=["sedov", "binary_nested", "polytrope_fmr", "poisson"],
                     help="binary_nested: time only the binary-BH supernova on three nested FMR levels; "
-                         "polytrope_fmr: only the two-level self-gravitating polytrope")
+                         "polytrope_fmr: only the two-level self-gravitating polytrope; "
+                         "poisson: only the isolated Poisson solve at 128^3, --steps solves per precision")
     ap.add_argument("--full", action="store_true",
                     help="with --workload: run the workload's stated length from its initial state (polytrope "
                          "200 steps, binary 1000 steps, no warm-up) instead of --steps")
@@ -832,6 +833,13 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "poisson":
+        import torch
+        import bsn
+        peak_fp = {k_: bsn.fp_peak(k_) for k_ in ("f64", "f32", "f32x2")}
+        out = poisson_solves(bsn, torch, peak_fp, peaks()[0], log, reps=max(1, args.steps))
+        print(json.dumps(out), flush=True)
         return
     if args.workload in ("binary_nested", "polytrope_fmr"):
         import torch

@@ -92,6 +92,15 @@ SIGNATURES = {
     "bsn_add_sink_sources_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D, _BH, _I, _D, _D, _D, _D, _I, _D]),
     "bsn_accrete_f64": (_I, [_V, _BH, _P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _D, _D, _D]),
     "bsn_nbody_step": (_I, [_BH, _I, _D, _dp]),
+    "bsn_add_bh_gravity_source_slab_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D, _BH, _I, _D, _D, _D, _I]),
+    "bsn_add_sink_sources_slab_f64": (_I, [_V, _P, _P, _I, _I, _I, _D, _D, _D, _BH, _I, _D, _D, _D, _D, _I, _D,
+                                           _I]),
+    "bsn_gas_force_on_bh_slab_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _BH, _D, _D, _D, _I, _dp]),
+    "bsn_merge_force_pairs": (_I, [_dp, _I, _dp]),
+    "bsn_sink_box": (_I, [_BH, _I, _I, _I, _D, _D, _D, _D, _D, _D, C.POINTER(C.c_int)]),
+    "bsn_sink_terms_slab_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _I, _BH, _D, _D, _D,
+                                     C.POINTER(C.c_int), _dp, _LL, C.POINTER(C.c_longlong)]),
+    "bsn_accrete_from_terms": (_I, [_BH, _dp, _LL]),
     "bsn_kepler_init": (_I, [_BH, _dp, _dp, _D, _dp]),
     "bsn_kepler_update": (_I, [_BH, _dp, _D]),
     "bsn_solve_poisson_isolated_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _P]),

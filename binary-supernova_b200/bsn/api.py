@@ -228,6 +228,72 @@ def accrete(bh, U, nx, ny, nz, dx, dy, dz, x0, y0, z0, dt, *, f_sink=1.0, rho_si
           float(x0), float(y0), float(z0), float(dt), float(f_sink), float(rho_sink_min))
 
 
+def add_bh_gravity_source_slab(dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0, k0):
+    """add_bh_gravity_source! on a z-slab whose first active plane is global plane k0."""
+    arr = _bh_array(bhs)
+    _call("bsn_add_bh_gravity_source_slab_f64", context(), _ptr(dU), _ptr(U), nx, ny, nz, float(dx), float(dy),
+          float(dz), arr, len(bhs), float(x0), float(y0), float(z0), int(k0))
+
+
+def add_sink_sources_slab(dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0, k0, *, f_sink=1.0, torque_free=True,
+                          rho_sink_min=0.0):
+    """add_sink_sources! on a z-slab whose first active plane is global plane k0."""
+    arr = _bh_array(bhs)
+    _call("bsn_add_sink_sources_slab_f64", context(), _ptr(dU), _ptr(U), nx, ny, nz, float(dx), float(dy),
+          float(dz), arr, len(bhs), float(x0), float(y0), float(z0), float(f_sink), int(bool(torque_free)),
+          float(rho_sink_min), int(k0))
+
+
+def gas_force_pairs_slab(U, nx, ny, nz, dx, dy, dz, bh, x0, y0, z0, k0) -> np.ndarray:
+    """The slab's compensated gas_force_on_bh partial sums: (hi, lo) per component, shape (6,)."""
+    out = (C.c_double * 6)()
+    _call("bsn_gas_force_on_bh_slab_f64", context(), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz),
+          C.byref(bh), float(x0), float(y0), float(z0), int(k0), out)
+    return np.array(out[:])
+
+
+def merge_force_pairs(pairs) -> np.ndarray:
+    """Merge per-slab (hi, lo) pairs (rows in rank order) into the force (host)."""
+    P = np.ascontiguousarray(np.asarray(pairs, dtype=np.float64).reshape(-1, 6))
+    out = (C.c_double * 3)()
+    rc = load().bsn_merge_force_pairs(P.ctypes.data_as(C.POINTER(C.c_double)), P.shape[0], out)
+    if rc != 0:
+        raise BSNError(rc, "merge_force_pairs")
+    return np.array(out[:])
+
+
+def sink_box(bh, nx, ny, nz, dx, dy, dz, x0, y0, z0):
+    """The global active box {ilo, ihi, jlo, jhi, klo, khi} that holds the sink sphere (host)."""
+    b = (C.c_int * 6)()
+    rc = load().bsn_sink_box(C.byref(bh), nx, ny, nz, float(dx), float(dy), float(dz), float(x0), float(y0),
+                             float(z0), b)
+    if rc != 0:
+        raise BSNError(rc, "sink_box")
+    return tuple(b[:])
+
+
+def sink_terms_slab(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, k0, bh, dt, box, *, f_sink=1.0, rho_sink_min=0.0):
+    """accrete!'s terms over this slab's part of the global box, (n, 4) host array in (k, j, i) order."""
+    ilo, ihi, jlo, jhi, klo, khi = box
+    kl, kh = max(klo, k0), min(khi, k0 + nz - 1)
+    cap = max(0, ihi - ilo + 1) * max(0, jhi - jlo + 1) * max(0, kh - kl + 1)
+    out = np.zeros((max(cap, 1), 4))
+    n = C.c_longlong(0)
+    b = (C.c_int * 6)(*box)
+    _call("bsn_sink_terms_slab_f64", context(), _ptr(U), nx, ny, nz, float(dx), float(dy), float(dz), float(x0),
+          float(y0), float(z0), int(k0), C.byref(bh), float(dt), float(f_sink), float(rho_sink_min), b,
+          out.ctypes.data_as(C.POINTER(C.c_double)), cap, C.byref(n))
+    return out[:n.value]
+
+
+def accrete_from_terms(bh, terms):
+    """The end of accrete! from the global (k, j, i)-ordered term list (host)."""
+    T = np.ascontiguousarray(np.asarray(terms, dtype=np.float64).reshape(-1, 4))
+    rc = load().bsn_accrete_from_terms(C.byref(bh), T.ctypes.data_as(C.POINTER(C.c_double)), T.shape[0])
+    if rc != 0:
+        raise BSNError(rc, "accrete_from_terms")
+
+
 def nbody_step(bhs, dt, F_gas):
     arr = _bh_array(bhs)
     F = np.ascontiguousarray(np.asarray(F_gas, dtype=np.float64).reshape(-1))
@@ -650,5 +716,6 @@ def set_profiling(on: bool):
     _call("bsn_ctx_set_profiling", context(), int(bool(on)))
 
 
-__all__ += ["euler3d_rhs_f32", "euler3d_step_f32", "euler3d_step_learned", "run_steps", "fmr3d_run_steps", "coupled_run_steps", "diagnostics", "tile_variants", "set_tile", "get_tile", "kernel_time",
+__all__ += ["add_bh_gravity_source_slab", "add_sink_sources_slab", "gas_force_pairs_slab", "merge_force_pairs",
+            "sink_box", "sink_terms_slab", "accrete_from_terms", "euler3d_rhs_f32", "euler3d_step_f32", "euler3d_step_learned", "run_steps", "fmr3d_run_steps", "coupled_run_steps", "diagnostics", "tile_variants", "set_tile", "get_tile", "kernel_time",
             "set_profiling", "fp_peak", "PREC"]

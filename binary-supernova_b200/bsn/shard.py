@@ -29,6 +29,13 @@ whatever computes the stages.
 transforms, an all-to-all transpose to z lines, the z convolution with the
 global grid's Green's function, and the transpose back; on the device it is
 bit-identical to the undivided bsn_solve_poisson_isolated_f64.
+
+`coupled_step` is the production step (coupled_step!,
+scripts/run_sn50_fiducial.jl:756-818) on the slabs: BH gravity and the sink
+sources per cell with the global plane index, the gas force on the BHs as an
+all-gather of the ranks' compensated partial sums merged in rank order, and
+accrete! as an ordered gather of the sink sphere's cell terms; with the orbit
+frozen it is the undivided step bit for bit.
 """
 from __future__ import annotations
 
@@ -145,6 +152,18 @@ def euler3d_step(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group=None, rho_floo
     and the reference runs it only with outflow (coupled_step!)."""
     if self_gravity and slab.bc != "outflow":
         raise ValueError("self_gravity needs bc='outflow': the isolated Poisson solve has no periodic form")
+
+    def sources(dU, U):
+        if self_gravity:
+            add_self_gravity_source(dU, U, slab, dx, dy, dz, ops, group)
+
+    _rk3(U, slab, dx, dy, dz, dt, gamma, ops, group, rho_floor, P_floor, sources)
+
+
+def _rk3(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group, rho_floor, P_floor, sources):
+    """The three stages of euler3d_step! on the slab: ghosts, halo exchange,
+    euler3d_rhs!, then sources(dU, U) (the source terms coupled_step! adds
+    after the right-hand side), the stage combination and floors."""
     nx, ny, nz = slab.nx, slab.ny, slab.nz
     Un = ops.copy(U)
     dU = ops.zeros_like(U)
@@ -152,8 +171,7 @@ def euler3d_step(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group=None, rho_floo
         ops.fill(U, nx, ny, nz, slab.bc)
         exchange(U, slab, ops, group, rho_floor, P_floor, gamma)
         ops.rhs(dU, U, nx, ny, nz, dx, dy, dz, gamma, slab.bc, rho_floor, P_floor)
-        if self_gravity:
-            add_self_gravity_source(dU, U, slab, dx, dy, dz, ops, group)
+        sources(dU, U)
         if stage == 0:
             ops.assign(U, Un + dt * dU)
         elif stage == 1:
@@ -161,6 +179,104 @@ def euler3d_step(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group=None, rho_floo
         else:
             ops.assign(U, (1.0 / 3.0) * Un + (2.0 / 3.0) * U + ((2.0 / 3.0) * dt) * dU)
         ops.floors(U, nx, ny, nz, rho_floor, P_floor, gamma)
+
+
+# ---------------------------------------------------------------------------
+# coupled_step! (scripts/run_sn50_fiducial.jl:756-818) over z-slabs
+#
+# The per-cell sources (BH gravity, sinks) take the global cell index (k0),
+# so they are the undivided grid's bit for bit.  The two grid sums become
+# collectives: gas_force_on_bh is each rank's compensated partial sum,
+# gathered and merged in rank order (the same force on every rank, within
+# the whole-grid sum's rounding of the reference's sequential sum), and
+# accrete! gathers the terms of the sink sphere's cells from the ranks whose
+# slab meets it, in the reference's (k, j, i) order, and adds them in that
+# order on every rank (the undivided accrete! bit for bit).
+
+
+def _gather_rows(x, world, group, device):
+    """all-gather of one float64 vector per rank -> (world, len) numpy, rank order."""
+    import numpy as np
+    if world == 1:
+        return np.asarray(x, dtype=np.float64).reshape(1, -1)
+    import torch.distributed as dist
+    t = torch.as_tensor(np.ascontiguousarray(x, dtype=np.float64), device=device)
+    out = [torch.empty_like(t) for _ in range(world)]
+    dist.all_gather(out, t, group=group)
+    return torch.stack(out).cpu().numpy()
+
+
+def gas_force(U, slab: Slab, bh, dx, dy, dz, x0, y0, z0, ops, group=None):
+    """gas_force_on_bh (src/gravity_bh.jl:91-113) of the global grid on every rank."""
+    from . import api
+    pairs = ops.gas_force_pairs(U, slab.nx, slab.ny, slab.nz, dx, dy, dz, bh, x0, y0, z0, slab.k0)
+    return api.merge_force_pairs(_gather_rows(pairs, slab.world, group, ops.device))
+
+
+def _slab_box_cells(box, slab: Slab, rank):
+    ilo, ihi, jlo, jhi, klo, khi = box
+    k0 = rank * slab.nz
+    kl, kh = max(klo, k0), min(khi, k0 + slab.nz - 1)
+    return max(0, ihi - ilo + 1) * max(0, jhi - jlo + 1) * max(0, kh - kl + 1)
+
+
+def accrete(bh, U, slab: Slab, dx, dy, dz, x0, y0, z0, dt, ops, group=None, *, f_sink=1.0, rho_sink_min=0.0):
+    """accrete! (src/sinks.jl:74-109) of the global grid: the terms of the
+    sink box's cells, gathered from the ranks in rank order (each rank's
+    count follows from the box, so only the ranks whose slab meets it send
+    anything), added in the reference's order on every rank."""
+    import numpy as np
+    from . import api
+    box = api.sink_box(bh, slab.nx, slab.ny, slab.nz * slab.world, dx, dy, dz, x0, y0, z0)
+    counts = [_slab_box_cells(box, slab, r) for r in range(slab.world)]
+    terms = ops.sink_terms(U, slab.nx, slab.ny, slab.nz, dx, dy, dz, x0, y0, z0, slab.k0, bh, dt, box, f_sink,
+                           rho_sink_min)
+    assert terms.shape == (counts[slab.rank], 4)
+    if slab.world > 1 and max(counts) > 0:
+        pad = np.zeros((max(counts), 4))
+        pad[:len(terms)] = terms
+        rows = _gather_rows(pad.reshape(-1), slab.world, group, ops.device).reshape(slab.world, -1, 4)
+        terms = np.concatenate([rows[r, :counts[r]] for r in range(slab.world)])
+    api.accrete_from_terms(bh, terms)
+
+
+def coupled_step(U, bhs, slab: Slab, dt, t, dx, x0, y0, z0, gamma, ops, group=None, *, f_sink=1.0,
+                 rho_floor=0.0, P_floor=0.0, torque_free=True, self_gravity=False, t_bh2_sink_on=0.0,
+                 rho_sink_min=0.0, evolve_orbit=True):
+    """coupled_step! (scripts/run_sn50_fiducial.jl:756-818) on this rank's slab
+    of the global grid (cubic cells dx, outflow boundaries): the gas force on
+    every BH with the driver's non-finite / 1e3 guard, nbody_step!, the three
+    stages with BH gravity, optional self-gravity and the sinks (only the first
+    BH's before t_bh2_sink_on), then accrete! of the active sinks.  `bhs`
+    (bsn_bh, the same on every rank) is updated in place; returns F_gas."""
+    import math
+    import numpy as np
+    from . import api
+    if slab.bc != "outflow":
+        raise ValueError("coupled_step runs with bc='outflow'")
+    nbh = len(bhs)
+    nsink = min(1, nbh) if t < t_bh2_sink_on else nbh
+    F = np.zeros((nbh, 3))
+    for i, bh in enumerate(bhs):
+        f = gas_force(U, slab, bh, dx, dx, dx, x0, y0, z0, ops, group)
+        fin = all(math.isfinite(v) for v in f)
+        if fin and not math.sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]) > 1e3:
+            F[i] = f
+    if evolve_orbit and nbh > 0 and all(math.isfinite(v) for b in bhs for v in (*b.pos, *b.vel)):
+        api.nbody_step(bhs, dt, F)
+    nx, ny, nz = slab.nx, slab.ny, slab.nz
+
+    def sources(dU, U):
+        ops.bh_gravity(dU, U, nx, ny, nz, dx, dx, dx, bhs, x0, y0, z0, slab.k0)
+        if self_gravity:
+            add_self_gravity_source(dU, U, slab, dx, dx, dx, ops, group)
+        ops.sink_sources(dU, U, nx, ny, nz, dx, dx, dx, bhs[:nsink], x0, y0, z0, slab.k0, f_sink, torque_free,
+                         rho_sink_min)
+
+    _rk3(U, slab, dx, dx, dx, dt, gamma, ops, group, rho_floor, P_floor, sources)
+    for i in range(nsink):
+        accrete(bhs[i], U, slab, dx, dx, dx, x0, y0, z0, dt, ops, group, f_sink=f_sink, rho_sink_min=rho_sink_min)
+    return F
 
 
 def run_steps(U, slab: Slab, dx, dy, dz, gamma, cfl, ops, *, n_steps, t=0.0, t_end=0.0, group=None,
@@ -364,6 +480,20 @@ class DeviceOps:
         self.api.apply_sg_force_slab(dU, U, phi, nx, ny, nz, dx, dy, dz,
                                      None if lo is None else lo.contiguous(),
                                      None if hi is None else hi.contiguous())
+
+    def bh_gravity(self, dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0, k0):
+        self.api.add_bh_gravity_source_slab(dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0, k0)
+
+    def sink_sources(self, dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0, k0, f_sink, torque_free, rho_sink_min):
+        self.api.add_sink_sources_slab(dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0, k0, f_sink=f_sink,
+                                       torque_free=torque_free, rho_sink_min=rho_sink_min)
+
+    def gas_force_pairs(self, U, nx, ny, nz, dx, dy, dz, bh, x0, y0, z0, k0):
+        return self.api.gas_force_pairs_slab(U, nx, ny, nz, dx, dy, dz, bh, x0, y0, z0, k0)
+
+    def sink_terms(self, U, nx, ny, nz, dx, dy, dz, x0, y0, z0, k0, bh, dt, box, f_sink, rho_sink_min):
+        return self.api.sink_terms_slab(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, k0, bh, dt, box, f_sink=f_sink,
+                                        rho_sink_min=rho_sink_min)
 
     def floor_planes(self, planes, nx, ny, rho_floor, P_floor, gamma):
         """apply_floors_3d! on the active (i, j) cells of NG received z-planes

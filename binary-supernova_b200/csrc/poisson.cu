@@ -17,9 +17,10 @@
 //     so no bit reversal is needed between them) and keeps only the n output
 //     planes the solution needs; the full padded spectrum never reaches HBM;
 //   * inverse y and x passes produce only the first octant.
-// Every transform is an in-shared-memory radix-2 FFT over a batch of lines
-// whose neighbouring elements are contiguous in HBM, so loads and stores are
-// coalesced for all three axes.
+// The solve's transforms are register-resident self-sorting FFTs over
+// batches of lines (fft_lines.cuh) whose neighbouring elements are contiguous
+// in HBM, so loads and stores are coalesced for all three axes; Khat's
+// one-off transforms are radix-2 FFTs in shared memory.
 #include <cmath>
 #include <map>
 
@@ -226,7 +227,7 @@ bsn_status solve(bsn_ctx* ctx, RhoSrc src, double dx, double dy, double dz, doub
     bsn_status st;
     double2* W1 = (double2*)slot(ctx, SLOT_FFT0, sizeof(double2) * w1, &st); BSN_TRY(st);
     double2* W2 = (double2*)slot(ctx, SLOT_FFT1, sizeof(double2) * w2, &st); BSN_TRY(st);
-    return solve_lines<double2>(ctx, src, K, t1, t2, t3, W1, W2, phi, SMEM_COMPLEX, NT);
+    return solve_lines<double2>(ctx, src, K, t1, t2, t3, W1, W2, phi);
 }
 
 }  // namespace fft
@@ -337,7 +338,7 @@ extern "C" bsn_status bsn_poisson_slab_forward_f64(bsn_ctx* ctx, const double* r
     bsn_status st;
     double2* W1 = (double2*)slot(ctx, SLOT_FFT0, sizeof(double2) * (size_t)(nx + 1) * ny * nzl, &st); BSN_TRY(st);
     fft::RhoSrc src{rho, nullptr, nx, ny, nzl, -1.0};
-    return fft::slab_forward_lines<double2>(ctx, src, t1, t2, W1, (double2*)W2, fft::SMEM_COMPLEX, fft::NT);
+    return fft::slab_forward_lines<double2>(ctx, src, t1, t2, W1, (double2*)W2);
 }
 
 extern "C" bsn_status bsn_poisson_slab_zconv_f64(bsn_ctx* ctx, double* T, int nx, int ny, int nz, int ky0, int nky,
@@ -354,7 +355,7 @@ extern "C" bsn_status bsn_poisson_slab_zconv_f64(bsn_ctx* ctx, double* T, int nx
     BSN_TRY(fft::khat(ctx, nx, ny, nz, dx, dy, dz, &K));
     const double2* t3;
     BSN_TRY(fft::twiddles(ctx, 2 * nz, &t3));
-    return fft::slab_zconv_lines<double2>(ctx, (double2*)T, K, t3, nx, ny, nz, ky0, nky, fft::SMEM_COMPLEX, fft::NT);
+    return fft::slab_zconv_lines<double2>(ctx, (double2*)T, K, t3, nx, ny, nz, ky0, nky);
 }
 
 extern "C" bsn_status bsn_poisson_slab_inverse_f64(bsn_ctx* ctx, const double* W2, int nx, int ny, int nzl,
@@ -366,6 +367,5 @@ extern "C" bsn_status bsn_poisson_slab_inverse_f64(bsn_ctx* ctx, const double* W
     BSN_TRY(fft::twiddles(ctx, 2 * ny, &t2));
     bsn_status st;
     double2* W1 = (double2*)slot(ctx, SLOT_FFT0, sizeof(double2) * (size_t)(nx + 1) * ny * nzl, &st); BSN_TRY(st);
-    return fft::slab_inverse_lines<double2>(ctx, (const double2*)W2, t1, t2, W1, phi, nx, ny, nzl, fft::SMEM_COMPLEX,
-                                            fft::NT);
+    return fft::slab_inverse_lines<double2>(ctx, (const double2*)W2, t1, t2, W1, phi, nx, ny, nzl);
 }

@@ -12,8 +12,7 @@
 namespace bsn {
 namespace fft32 {
 
-constexpr int NT = 256;
-constexpr int SMEM_COMPLEX = 8192;   // complex floats of line storage per CTA (64 KiB)
+constexpr int MAX_LEN = 4096;   // longest padded line of the transforms (fft_lines.cuh)
 
 struct State {
     std::map<int, float2*> tw;
@@ -81,8 +80,8 @@ bsn_status prepare(bsn_ctx* ctx, int nx, int ny, int nz, double dx, double dy, d
     if (nx < 2 || ny < 2 || nz < 2 || (nx & (nx - 1)) || (ny & (ny - 1)) || (nz & (nz - 1)))
         return set_err(ctx, BSN_ERR_UNSUPPORTED, "FFT Poisson solve needs power-of-two sizes >= 2 (got %d,%d,%d)",
                        nx, ny, nz);
-    if (2 * std::max(nx, std::max(ny, nz)) > SMEM_COMPLEX)
-        return set_err(ctx, BSN_ERR_UNSUPPORTED, "FFT length above %d", SMEM_COMPLEX);
+    if (2 * std::max(nx, std::max(ny, nz)) > MAX_LEN)
+        return set_err(ctx, BSN_ERR_UNSUPPORTED, "FFT length above %d", MAX_LEN);
     BSN_TRY(khat(ctx, nx, ny, nz, dx, dy, dz, K));
     BSN_TRY(twiddles(ctx, 2 * nx, &tw[0]));
     BSN_TRY(twiddles(ctx, 2 * ny, &tw[1]));
@@ -98,7 +97,7 @@ bsn_status solve(bsn_ctx* ctx, const fft::RhoSrc& src, double dx, double dy, dou
     const float2* tw[3];
     float2 *W1, *W2;
     BSN_TRY(prepare(ctx, src.nx, src.ny, src.nz, dx, dy, dz, &K, tw, &W1, &W2));
-    return fft::solve_lines<float2>(ctx, src, K, tw[0], tw[1], tw[2], W1, W2, phi, SMEM_COMPLEX, NT);
+    return fft::solve_lines<float2>(ctx, src, K, tw[0], tw[1], tw[2], W1, W2, phi);
 }
 
 }  // namespace fft32

@@ -1,6 +1,7 @@
 // sources_f64.cu -- BH gravity, sinks, self-gravity gradient, gas->BH force,
 // accretion, host FP64 orbits and the coupled-step driver (FP64 parity path).
 #include <cmath>
+#include <algorithm>
 #include <cstring>
 
 #include "hydro_f64.cuh"
@@ -12,15 +13,18 @@ namespace f64 {
 
 
 // add_bh_gravity_source! (src/gpu_kernels.jl:199-230)
+// k0: global index of the grid's first active plane when it is a z-slab of a
+// larger grid (0 otherwise); cell centres use the global index, so a slab's
+// cells take the undivided grid's arithmetic.
 __global__ void bh_gravity_kernel(double* dU, const double* U, int nx, int ny, int nz, double dx, double dy,
-                                  double dz, double x0, double y0, double z0, BHSrc bh) {
+                                  double dz, double x0, double y0, double z0, BHSrc bh, int k0) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)nx * ny * nz) return;
     int a = (int)(t % nx); long long r = t / nx; int b = (int)(r % ny); int c = (int)(r / ny);
     Geom G(nx, ny, nz);
     long long o = G.act(a, b, c);
     double xc, yc, zc;
-    cell_xyz(a, b, c, x0, y0, z0, dx, dy, dz, xc, yc, zc);
+    cell_xyz(a, b, c + k0, x0, y0, z0, dx, dy, dz, xc, yc, zc);
     double rho = U[o], vx = U[o + 1] / rho, vy = U[o + 2] / rho, vz = U[o + 3] / rho;
     double ax = 0.0, ay = 0.0, az = 0.0;
     for (int n = 0; n < bh.n; ++n) {
@@ -56,14 +60,14 @@ __global__ void relax_src_kernel(double* dU, const double* U, int nx, int ny, in
 
 // add_sink_sources! (src/gpu_kernels.jl:238-284)
 __global__ void sink_kernel(double* dU, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
-                            double x0, double y0, double z0, SinkSrc sk) {
+                            double x0, double y0, double z0, SinkSrc sk, int k0) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)nx * ny * nz) return;
     int a = (int)(t % nx); long long r = t / nx; int b = (int)(r % ny); int c = (int)(r / ny);
     Geom G(nx, ny, nz);
     long long o = G.act(a, b, c);
     double xc, yc, zc;
-    cell_xyz(a, b, c, x0, y0, z0, dx, dy, dz, xc, yc, zc);
+    cell_xyz(a, b, c + k0, x0, y0, z0, dx, dy, dz, xc, yc, zc);
     double rho = U[o], mx = U[o + 1], my = U[o + 2], mz = U[o + 3], E = U[o + 4];
     if (!(rho > sk.rho_min)) return;
     for (int n = 0; n < sk.n; ++n) {
@@ -133,7 +137,7 @@ using sums::dd_merge;
 // gas_force_on_bh (src/gravity_bh.jl:91-113): out[3*blocks] partial (hi,lo).
 __global__ void gas_force_kernel(const double* U, int nx, int ny, int nz, double dx, double dy, double dz, double x0,
                                  double y0, double z0, double px, double py, double pz, double mass, double eps,
-                                 double* part) {
+                                 double* part, int k0) {
     Geom G(nx, ny, nz);
     double dV = dx * dy * dz;
     DD s[3] = {{0, 0}, {0, 0}, {0, 0}};
@@ -141,7 +145,7 @@ __global__ void gas_force_kernel(const double* U, int nx, int ny, int nz, double
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         int a = (int)(t % nx); long long r = t / nx; int b = (int)(r % ny); int c = (int)(r / ny);
         double xc, yc, zc;
-        cell_xyz(a, b, c, x0, y0, z0, dx, dy, dz, xc, yc, zc);
+        cell_xyz(a, b, c + k0, x0, y0, z0, dx, dy, dz, xc, yc, zc);
         double ddx = xc - px, ddy = yc - py, ddz = zc - pz;
         double r2 = sq(ddx) + sq(ddy) + sq(ddz) + sq(eps);
         double r3 = r2 * sqrt(r2);
@@ -169,10 +173,45 @@ __global__ void gas_force_kernel(const double* U, int nx, int ny, int nz, double
     }
 }
 
-__global__ void gas_force_finish(const double* part, int nblocks, double* out) {
+__global__ void gas_force_finish(const double* part, int nblocks, double* out, int as_pairs) {
+    if (as_pairs) {   // the compensated (hi, lo) pairs of the grid, for a merge over slabs
+        double F[6];
+        sums::merge_partials3_dd<256>(part, nblocks, F);
+        if (threadIdx.x == 0)
+            for (int d = 0; d < 6; ++d) out[d] = F[d];
+        return;
+    }
     double F[3];
     sums::merge_partials3<256>(part, nblocks, F);
     if (threadIdx.x == 0) { out[0] = F[0]; out[1] = F[1]; out[2] = F[2]; }
+}
+
+// accrete!'s per-cell terms (src/sinks.jl:74-109) over the global active box
+// [ilo,ihi] x [jlo,jhi] x [klo,khi] restricted to this grid's planes (global
+// k0 .. k0 + nz - 1), in the reference's (k, j, i) order: {rho, mx, my, mz} *
+// rate inside the sink sphere where rho > rho_min, zeros elsewhere (adding
+// +0.0 leaves the sequential sums as skipping the cell does).
+__global__ void sink_terms_kernel(const double* U, int nx, int ny, int nz, double dx, double dy, double dz, double x0,
+                                  double y0, double z0, int k0, double px, double py, double pz, double rs,
+                                  double rate, double rho_min, int ilo, int ihi, int jlo, int jhi, int klo, int khi,
+                                  double* out) {
+    const long long nI = ihi - ilo + 1, nJ = jhi - jlo + 1, nK = khi - klo + 1;
+    const long long total = nI * nJ * nK;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    int a = ilo + (int)(t % nI);
+    long long rr = t / nI;
+    int b = jlo + (int)(rr % nJ), kg = klo + (int)(rr / nJ);
+    double xc, yc, zc;
+    cell_xyz(a, b, kg, x0, y0, z0, dx, dy, dz, xc, yc, zc);
+    double r = sqrt(sq(xc - px) + sq(yc - py) + sq(zc - pz));
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (!(r >= rs)) {
+        long long o = Geom(nx, ny, nz).act(a, b, kg - k0);
+        if (!(U[o] <= rho_min))
+            for (int q = 0; q < 4; ++q) v[q] = U[o + q] * rate;
+    }
+    for (int q = 0; q < 4; ++q) out[4 * t + q] = v[q];
 }
 
 // accrete! sums (src/sinks.jl:74-109) in the reference's exact loop order
@@ -217,41 +256,64 @@ static bsn_status fill_sink(bsn_ctx* ctx, const bsn_bh* bhs, int nbh, double f_s
     return BSN_OK;
 }
 
+// out[3] = the force, or with pairs != 0 out[6] = its compensated (hi, lo)
+// pairs per component; k0 as bh_gravity_kernel's.
 static bsn_status gas_force(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
-                            const bsn_bh& bh, double x0, double y0, double z0, double out[3]) {
+                            const bsn_bh& bh, double x0, double y0, double z0, double* out, int k0 = 0,
+                            int pairs = 0) {
     const int blocks = 148 * 4;
     bsn_status st;
     double* part = (double*)slot(ctx, SLOT_RED, sizeof(double) * (6 * blocks + 8), &st); BSN_TRY(st);
     gas_force_kernel<<<blocks, 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, bh.pos[0], bh.pos[1],
-                                                      bh.pos[2], bh.mass, bh.eps, part);
+                                                      bh.pos[2], bh.mass, bh.eps, part, k0);
     BSN_TRY(launch_check(ctx, "gas_force_kernel"));
-    gas_force_finish<<<1, 256, 0, ctx->stream>>>(part, blocks, part + 6 * blocks);
+    gas_force_finish<<<1, 256, 0, ctx->stream>>>(part, blocks, part + 6 * blocks, pairs);
     BSN_TRY(launch_check(ctx, "gas_force_finish"));
     double* h = (double*)pinned(ctx, 64, &st); BSN_TRY(st);
-    BSN_CUDA(ctx, cudaMemcpyAsync(h, part + 6 * blocks, 24, cudaMemcpyDeviceToHost, ctx->stream));
+    const int nout = pairs ? 6 : 3;
+    BSN_CUDA(ctx, cudaMemcpyAsync(h, part + 6 * blocks, 8 * nout, cudaMemcpyDeviceToHost, ctx->stream));
     BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    out[0] = h[0]; out[1] = h[1]; out[2] = h[2];
+    for (int d = 0; d < nout; ++d) out[d] = h[d];
     return BSN_OK;
 }
 
 static int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// Conservative active-index box [b0,b1] x [b2,b3] x [b4,b5] (0-based,
+// inclusive) of the sink sphere |x - p| < r_sink on an nx x ny x nz grid; the
+// whole grid for a non-finite sink geometry (the reference then selects no
+// cell by r >= rs, which is false for NaN, so every cell's NaN enters its sums).
+static void sink_box(const bsn_bh& bh, double rs, int nx, int ny, int nz, double dx, double dy, double dz, double x0,
+                     double y0, double z0, int b[6]) {
+    auto lo = [](double p, double r, double o, double h) { return (int)std::floor((p - r - o) / h) - 2; };
+    auto hi = [](double p, double r, double o, double h) { return (int)std::ceil((p + r - o) / h) + 2; };
+    b[0] = clampi(lo(bh.pos[0], rs, x0, dx), 0, nx - 1); b[1] = clampi(hi(bh.pos[0], rs, x0, dx), 0, nx - 1);
+    b[2] = clampi(lo(bh.pos[1], rs, y0, dy), 0, ny - 1); b[3] = clampi(hi(bh.pos[1], rs, y0, dy), 0, ny - 1);
+    b[4] = clampi(lo(bh.pos[2], rs, z0, dz), 0, nz - 1); b[5] = clampi(hi(bh.pos[2], rs, z0, dz), 0, nz - 1);
+    if (!std::isfinite(rs) || !std::isfinite(bh.pos[0]) || !std::isfinite(bh.pos[1]) || !std::isfinite(bh.pos[2])) {
+        b[0] = 0; b[1] = nx - 1; b[2] = 0; b[3] = ny - 1; b[4] = 0; b[5] = nz - 1;
+    }
+}
+
+// The end of accrete! (src/sinks.jl:96-107) from its sums.
+static void accrete_update(bsn_bh* bh, double dm, double dPx, double dPy, double dPz) {
+    if (dm > 0.0) {
+        double M_new = bh->mass + dm;
+        bh->vel[0] = (bh->mass * bh->vel[0] + dPx) / M_new;
+        bh->vel[1] = (bh->mass * bh->vel[1] + dPy) / M_new;
+        bh->vel[2] = (bh->mass * bh->vel[2] + dPz) / M_new;
+        bh->mass = M_new;
+    }
+}
 
 static bsn_status accrete(bsn_ctx* ctx, bsn_bh* bh, const double* U, int nx, int ny, int nz, double dx, double dy,
                           double dz, double x0, double y0, double z0, double dt, double f_sink, double rho_min) {
     double rs = bh_r_sink(*bh), ts = bh_t_sink(*bh, f_sink);
     double dV = dx * dy * dz;
     double rate = dV / ts * dt;
-    // conservative active-index box of the sphere |x - p| < rs
-    auto lo = [](double p, double r, double o, double h) { return (int)std::floor((p - r - o) / h) - 2; };
-    auto hi = [](double p, double r, double o, double h) { return (int)std::ceil((p + r - o) / h) + 2; };
-    int ilo = clampi(lo(bh->pos[0], rs, x0, dx), 0, nx - 1), ihi = clampi(hi(bh->pos[0], rs, x0, dx), 0, nx - 1);
-    int jlo = clampi(lo(bh->pos[1], rs, y0, dy), 0, ny - 1), jhi = clampi(hi(bh->pos[1], rs, y0, dy), 0, ny - 1);
-    int klo = clampi(lo(bh->pos[2], rs, z0, dz), 0, nz - 1), khi = clampi(hi(bh->pos[2], rs, z0, dz), 0, nz - 1);
-    if (!std::isfinite(rs) || !std::isfinite(bh->pos[0]) || !std::isfinite(bh->pos[1]) || !std::isfinite(bh->pos[2])) {
-        // non-finite sink geometry selects no cell in the reference either (r >= rs is false for NaN,
-        // so the reference would sum NaNs); fall back to the whole grid to keep its exact behaviour
-        ilo = 0; ihi = nx - 1; jlo = 0; jhi = ny - 1; klo = 0; khi = nz - 1;
-    }
+    int b[6];
+    sink_box(*bh, rs, nx, ny, nz, dx, dy, dz, x0, y0, z0, b);
+    const int ilo = b[0], ihi = b[1], jlo = b[2], jhi = b[3], klo = b[4], khi = b[5];
     bsn_status st;
     double* d = (double*)slot(ctx, SLOT_RED, 64, &st); BSN_TRY(st);
     accrete_kernel<<<1, 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, bh->pos[0], bh->pos[1],
@@ -260,14 +322,7 @@ static bsn_status accrete(bsn_ctx* ctx, bsn_bh* bh, const double* U, int nx, int
     double* h = (double*)pinned(ctx, 64, &st); BSN_TRY(st);
     BSN_CUDA(ctx, cudaMemcpyAsync(h, d, 32, cudaMemcpyDeviceToHost, ctx->stream));
     BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    double dm = h[0];
-    if (dm > 0.0) {
-        double M_new = bh->mass + dm;
-        bh->vel[0] = (bh->mass * bh->vel[0] + h[1]) / M_new;
-        bh->vel[1] = (bh->mass * bh->vel[1] + h[2]) / M_new;
-        bh->vel[2] = (bh->mass * bh->vel[2] + h[3]) / M_new;
-        bh->mass = M_new;
-    }
+    accrete_update(bh, h[0], h[1], h[2], h[3]);
     return BSN_OK;
 }
 
@@ -301,7 +356,7 @@ extern "C" bsn_status bsn_add_bh_gravity_source_f64(bsn_ctx* ctx, double* dU, co
     BHSrc s;
     BSN_TRY(fill_bh(ctx, bhs, nbh, s));
     bh_gravity_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(dU, U, nx, ny, nz, dx, dy, dz,
-                                                                                       x0, y0, z0, s);
+                                                                                       x0, y0, z0, s, 0);
     return launch_check(ctx, "bh_gravity_kernel");
 }
 
@@ -338,7 +393,7 @@ extern "C" bsn_status bsn_add_sink_sources_f64(bsn_ctx* ctx, double* dU, const d
     SinkSrc s;
     BSN_TRY(fill_sink(ctx, bhs, nbh, f_sink, torque_free, rho_sink_min, s));
     sink_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(dU, U, nx, ny, nz, dx, dy, dz, x0, y0,
-                                                                                 z0, s);
+                                                                                 z0, s, 0);
     return launch_check(ctx, "sink_kernel");
 }
 
@@ -356,6 +411,105 @@ extern "C" bsn_status bsn_accrete_f64(bsn_ctx* ctx, bsn_bh* bh, const double* U,
     BSN_TRY(check_dims(ctx, nx, ny, nz));
     if (!U || !bh) return set_err(ctx, BSN_ERR_ARG, "null argument");
     return accrete(ctx, bh, U, nx, ny, nz, dx, dy, dz, x0, y0, z0, dt, f_sink, rho_sink_min);
+}
+
+// ---- the sources on a z-slab of a larger grid (k0: its first global plane) ----
+
+extern "C" bsn_status bsn_add_bh_gravity_source_slab_f64(bsn_ctx* ctx, double* dU, const double* U, int nx, int ny,
+                                                         int nz, double dx, double dy, double dz, const bsn_bh* bhs,
+                                                         int nbh, double x0, double y0, double z0, int k0) {
+    BSN_TRY(check_dims(ctx, nx, ny, nz));
+    if (!dU || !U) return set_err(ctx, BSN_ERR_ARG, "null array");
+    if (k0 < 0) return set_err(ctx, BSN_ERR_ARG, "k0 = %d", k0);
+    BHSrc s;
+    BSN_TRY(fill_bh(ctx, bhs, nbh, s));
+    bh_gravity_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(dU, U, nx, ny, nz, dx, dy, dz,
+                                                                                       x0, y0, z0, s, k0);
+    return launch_check(ctx, "bh_gravity_kernel");
+}
+
+extern "C" bsn_status bsn_add_sink_sources_slab_f64(bsn_ctx* ctx, double* dU, const double* U, int nx, int ny, int nz,
+                                                    double dx, double dy, double dz, const bsn_bh* bhs, int nbh,
+                                                    double x0, double y0, double z0, double f_sink, int torque_free,
+                                                    double rho_sink_min, int k0) {
+    BSN_TRY(check_dims(ctx, nx, ny, nz));
+    if (!dU || !U) return set_err(ctx, BSN_ERR_ARG, "null array");
+    if (k0 < 0) return set_err(ctx, BSN_ERR_ARG, "k0 = %d", k0);
+    SinkSrc s;
+    BSN_TRY(fill_sink(ctx, bhs, nbh, f_sink, torque_free, rho_sink_min, s));
+    sink_kernel<<<grid1d((long long)nx * ny * nz, 256), 256, 0, ctx->stream>>>(dU, U, nx, ny, nz, dx, dy, dz, x0, y0,
+                                                                                 z0, s, k0);
+    return launch_check(ctx, "sink_kernel");
+}
+
+extern "C" bsn_status bsn_gas_force_on_bh_slab_f64(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx,
+                                                   double dy, double dz, const bsn_bh* bh, double x0, double y0,
+                                                   double z0, int k0, double out[6]) {
+    BSN_TRY(check_dims(ctx, nx, ny, nz));
+    if (!U || !bh || !out) return set_err(ctx, BSN_ERR_ARG, "null argument");
+    if (k0 < 0) return set_err(ctx, BSN_ERR_ARG, "k0 = %d", k0);
+    return gas_force(ctx, U, nx, ny, nz, dx, dy, dz, *bh, x0, y0, z0, out, k0, 1);
+}
+
+extern "C" bsn_status bsn_merge_force_pairs(const double* pairs, int nparts, double out[3]) {
+    if (!pairs || !out || nparts < 0) return BSN_ERR_ARG;
+    for (int d = 0; d < 3; ++d) {
+        // the two-sum merge of the device reduction (sums.cuh dd_merge), in part order
+        double hi = 0.0, lo = 0.0;
+        for (int p = 0; p < nparts; ++p) {
+            const double x = pairs[6 * p + 2 * d], t = hi + x, bp = t - hi;
+            lo += (hi - (t - bp)) + (x - bp);
+            hi = t;
+            lo += pairs[6 * p + 2 * d + 1];
+        }
+        out[d] = hi + lo;
+    }
+    return BSN_OK;
+}
+
+extern "C" bsn_status bsn_sink_box(const bsn_bh* bh, int nx, int ny, int nz, double dx, double dy, double dz,
+                                   double x0, double y0, double z0, int box[6]) {
+    if (!bh || !box || nx < 1 || ny < 1 || nz < 1) return BSN_ERR_ARG;
+    sink_box(*bh, bh_r_sink(*bh), nx, ny, nz, dx, dy, dz, x0, y0, z0, box);
+    return BSN_OK;
+}
+
+extern "C" bsn_status bsn_sink_terms_slab_f64(bsn_ctx* ctx, const double* U, int nx, int ny, int nz, double dx,
+                                              double dy, double dz, double x0, double y0, double z0, int k0,
+                                              const bsn_bh* bh, double dt, double f_sink, double rho_sink_min,
+                                              const int box[6], double* terms, long long cap, long long* count) {
+    BSN_TRY(check_dims(ctx, nx, ny, nz));
+    if (!U || !bh || !box || !count || (cap > 0 && !terms)) return set_err(ctx, BSN_ERR_ARG, "null argument");
+    if (k0 < 0) return set_err(ctx, BSN_ERR_ARG, "k0 = %d", k0);
+    const int klo = std::max(box[4], k0), khi = std::min(box[5], k0 + nz - 1);
+    if (box[0] < 0 || box[1] >= nx || box[2] < 0 || box[3] >= ny)
+        return set_err(ctx, BSN_ERR_ARG, "sink box outside the grid's x/y range");
+    const long long n = (box[1] >= box[0] && box[3] >= box[2] && khi >= klo)
+                            ? (long long)(box[1] - box[0] + 1) * (box[3] - box[2] + 1) * (khi - klo + 1) : 0;
+    *count = n;
+    if (n == 0) return BSN_OK;
+    if (n > cap) return set_err(ctx, BSN_ERR_ARG, "%lld sink cells, room for %lld", n, cap);
+    const double rs = bh_r_sink(*bh), ts = bh_t_sink(*bh, f_sink);
+    const double rate = dx * dy * dz / ts * dt;
+    bsn_status st;
+    double* d = (double*)slot(ctx, SLOT_RED, sizeof(double) * 4 * (size_t)n, &st); BSN_TRY(st);
+    sink_terms_kernel<<<grid1d(n, 256), 256, 0, ctx->stream>>>(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, k0,
+                                                                bh->pos[0], bh->pos[1], bh->pos[2], rs, rate,
+                                                                rho_sink_min, box[0], box[1], box[2], box[3], klo,
+                                                                khi, d);
+    BSN_TRY(launch_check(ctx, "sink_terms_kernel"));
+    BSN_CUDA(ctx, cudaMemcpyAsync(terms, d, sizeof(double) * 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return BSN_OK;
+}
+
+extern "C" bsn_status bsn_accrete_from_terms(bsn_bh* bh, const double* terms, long long n) {
+    if (!bh || (n > 0 && !terms) || n < 0) return BSN_ERR_ARG;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (long long c = 0; c < n; ++c)
+        for (int q = 0; q < 4; ++q) s[q] += terms[4 * c + q];
+    accrete_update(bh, s[0], s[1], s[2], s[3]);
+    return BSN_OK;
 }
 
 extern "C" bsn_status bsn_sg_gradient_f64(bsn_ctx* ctx, double* dU, const double* U, const double* phi, int nx, int ny,

@@ -27,9 +27,9 @@ __device__ __forceinline__ DD dd_merge(DD a, DD b) {
 // Merge nblocks partial DD triples part[6 b + 2 d], part[6 b + 2 d + 1]
 // (d = 0..2) with all NT threads of one block in a fixed order (thread t takes
 // b = t, t + NT, ...; then a fixed shuffle tree and the warps in order), so
-// the result does not depend on scheduling.  Thread 0 gets out[d] = hi + lo.
+// the result does not depend on scheduling.  Thread 0 gets the merged pairs.
 template <int NT>
-__device__ void merge_partials3(const double* part, int nblocks, double out[3]) {
+__device__ void merge_partials3_pairs(const double* part, int nblocks, DD out[3]) {
     static_assert(NT % 32 == 0 && NT <= 1024, "block of whole warps");
     DD s[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
     for (int b = threadIdx.x; b < nblocks; b += NT)
@@ -47,8 +47,26 @@ __device__ void merge_partials3(const double* part, int nblocks, double out[3]) 
         for (int d = 0; d < 3; ++d) {
             DD acc = red[d][0];
             for (int w = 1; w < NT / 32; ++w) acc = dd_merge(acc, red[d][w]);
-            out[d] = acc.hi + acc.lo;
+            out[d] = acc;
         }
+}
+
+// As merge_partials3_pairs; thread 0 gets out[d] = hi + lo.
+template <int NT>
+__device__ void merge_partials3(const double* part, int nblocks, double out[3]) {
+    DD s[3];
+    merge_partials3_pairs<NT>(part, nblocks, s);
+    if (threadIdx.x == 0)
+        for (int d = 0; d < 3; ++d) out[d] = s[d].hi + s[d].lo;
+}
+
+// As merge_partials3_pairs; thread 0 gets out[2 d] = hi, out[2 d + 1] = lo.
+template <int NT>
+__device__ void merge_partials3_dd(const double* part, int nblocks, double out[6]) {
+    DD s[3];
+    merge_partials3_pairs<NT>(part, nblocks, s);
+    if (threadIdx.x == 0)
+        for (int d = 0; d < 3; ++d) { out[2 * d] = s[d].hi; out[2 * d + 1] = s[d].lo; }
 }
 
 // accrete! sums over the active-index box [ilo,ihi] x [jlo,jhi] x [klo,khi]:

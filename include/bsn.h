@@ -257,6 +257,43 @@ bsn_status bsn_add_sink_sources_f64(bsn_ctx* ctx, double* dU, const double* U,
 bsn_status bsn_accrete_f64(bsn_ctx* ctx, bsn_bh* bh, const double* U, int nx, int ny, int nz,
                            double dx, double dy, double dz, double x0, double y0, double z0,
                            double dt, double f_sink, double rho_sink_min);
+/* The same sources on a z-slab of a larger grid (one rank's planes of a
+ * z-decomposed grid; the reference runs on one device and has no slab form):
+ * k0 is the global index of the slab's first active plane, and cell centres
+ * are z0 + (k0 + k + 0.5) dz with the global index, so every cell takes the
+ * undivided grid's arithmetic bit for bit.  gas_force_on_bh's slab form gives
+ * the slab's compensated partial sums as (hi, lo) pairs per component
+ * (out[6]); bsn_merge_force_pairs merges the ranks' pairs in rank order (the
+ * same two-sum merge as the device reduction) into the force. */
+bsn_status bsn_add_bh_gravity_source_slab_f64(bsn_ctx* ctx, double* dU, const double* U,
+                                              int nx, int ny, int nz, double dx, double dy, double dz,
+                                              const bsn_bh* bhs, int nbh, double x0, double y0, double z0, int k0);
+bsn_status bsn_add_sink_sources_slab_f64(bsn_ctx* ctx, double* dU, const double* U,
+                                         int nx, int ny, int nz, double dx, double dy, double dz,
+                                         const bsn_bh* bhs, int nbh, double x0, double y0, double z0,
+                                         double f_sink, int torque_free, double rho_sink_min, int k0);
+bsn_status bsn_gas_force_on_bh_slab_f64(bsn_ctx* ctx, const double* U, int nx, int ny, int nz,
+                                        double dx, double dy, double dz, const bsn_bh* bh,
+                                        double x0, double y0, double z0, int k0, double out[6]);
+bsn_status bsn_merge_force_pairs(const double* pairs, int nparts, double out[3]);
+/* accrete! (src/sinks.jl:74-109) over slabs, in three parts whose result is
+ * the undivided accrete! bit for bit: bsn_sink_box gives the global active
+ * box (0-based inclusive {ilo,ihi,jlo,jhi,klo,khi}) that holds the sink
+ * sphere on the global nx x ny x nz grid (host); each rank's
+ * bsn_sink_terms_slab_f64 writes the terms the reference's sums add for the
+ * cells of that box in its planes, in the reference's (k, j, i) order, into
+ * the host buffer terms (4 doubles per cell: rho, mx, my, mz times
+ * dV / t_sink * dt, zeros outside the sphere or at rho <= rho_sink_min;
+ * *count cells, at most cap); the ranks' term lists concatenated in rank
+ * order are the global list, and bsn_accrete_from_terms adds them in order
+ * and updates the BH (host). */
+bsn_status bsn_sink_box(const bsn_bh* bh, int nx, int ny, int nz, double dx, double dy, double dz,
+                        double x0, double y0, double z0, int box[6]);
+bsn_status bsn_sink_terms_slab_f64(bsn_ctx* ctx, const double* U, int nx, int ny, int nz,
+                                   double dx, double dy, double dz, double x0, double y0, double z0, int k0,
+                                   const bsn_bh* bh, double dt, double f_sink, double rho_sink_min,
+                                   const int box[6], double* terms, long long cap, long long* count);
+bsn_status bsn_accrete_from_terms(bsn_bh* bh, const double* terms, long long n);
 /* nbody_step! (src/nbody.jl:74-104), host FP64.  F_gas is nbh*3 host doubles. */
 bsn_status bsn_nbody_step(bsn_bh* bhs, int nbh, double dt, const double* F_gas);
 /* KeplerOrbit(bhs; com, nhat, Omega) (src/kepler_orbit.jl:63-111), host FP64.

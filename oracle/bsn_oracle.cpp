@@ -65,10 +65,13 @@ extern "C" double orc_t_sink(const orc_bh* bh, double f_sink) {
     return f_sink * rs / v_ff;
 }
 
-/* src/gpu_kernels.jl:199-230 via src/gravity_bh.jl:58-78 */
-extern "C" void orc_add_bh_gravity_source(double* dU, const double* U, int nx, int ny, int nz,
-                                          double dx, double dy, double dz, const orc_bh* bhs, int nbh,
-                                          double x0, double y0, double z0) {
+/* src/gpu_kernels.jl:199-230 via src/gravity_bh.jl:58-78.  The _slab forms
+ * take a z-slab of a larger grid whose first active plane is global plane
+ * kofs (0-based): cell centres use the global index, z0 + (kofs + kk - 0.5) dz,
+ * so every cell takes the undivided grid's arithmetic. */
+extern "C" void orc_add_bh_gravity_source_slab(double* dU, const double* U, int nx, int ny, int nz,
+                                               double dx, double dy, double dz, const orc_bh* bhs, int nbh,
+                                               double x0, double y0, double z0, int kofs) {
     Idx I(nx, ny, nz);
     const int ng = NG;
 #pragma omp parallel for schedule(static)
@@ -78,7 +81,7 @@ extern "C" void orc_add_bh_gravity_source(double* dU, const double* U, int nx, i
                 int i = ii + ng, j = jj + ng, k = kk + ng;
                 double xc = x0 + ((double)ii - 0.5) * dx;
                 double yc = y0 + ((double)jj - 0.5) * dy;
-                double zc = z0 + ((double)kk - 0.5) * dz;
+                double zc = z0 + ((double)(kofs + kk) - 0.5) * dz;
                 double r = U[I(1, i, j, k)];
                 double vx = U[I(2, i, j, k)] / r, vy = U[I(3, i, j, k)] / r, vz = U[I(4, i, j, k)] / r;
                 double ax = 0.0, ay = 0.0, az = 0.0;
@@ -96,9 +99,16 @@ extern "C" void orc_add_bh_gravity_source(double* dU, const double* U, int nx, i
             }
 }
 
-/* src/gravity_bh.jl:91-113 */
-extern "C" void orc_gas_force_on_bh(const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
-                                    const orc_bh* bh, double x0, double y0, double z0, double out[3]) {
+extern "C" void orc_add_bh_gravity_source(double* dU, const double* U, int nx, int ny, int nz,
+                                          double dx, double dy, double dz, const orc_bh* bhs, int nbh,
+                                          double x0, double y0, double z0) {
+    orc_add_bh_gravity_source_slab(dU, U, nx, ny, nz, dx, dy, dz, bhs, nbh, x0, y0, z0, 0);
+}
+
+/* src/gravity_bh.jl:91-113 (the _slab form: see orc_add_bh_gravity_source_slab) */
+extern "C" void orc_gas_force_on_bh_slab(const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                                         const orc_bh* bh, double x0, double y0, double z0, int kofs,
+                                         double out[3]) {
     Idx I(nx, ny, nz);
     const int ng = NG;
     double dV = dx * dy * dz;
@@ -106,7 +116,7 @@ extern "C" void orc_gas_force_on_bh(const double* U, int nx, int ny, int nz, dou
     for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i) {
         double xc = x0 + ((double)i - 0.5) * dx;
         double yc = y0 + ((double)j - 0.5) * dy;
-        double zc = z0 + ((double)k - 0.5) * dz;
+        double zc = z0 + ((double)(kofs + k) - 0.5) * dz;
         double ddx = xc - bh->pos[0], ddy = yc - bh->pos[1], ddz = zc - bh->pos[2];
         double r2 = sq(ddx) + sq(ddy) + sq(ddz) + sq(bh->eps);
         double r3 = r2 * std::sqrt(r2);
@@ -116,11 +126,17 @@ extern "C" void orc_gas_force_on_bh(const double* U, int nx, int ny, int nz, dou
     out[0] = Fx; out[1] = Fy; out[2] = Fz;
 }
 
-/* src/gpu_kernels.jl:238-284 via src/sinks.jl:32-59 */
-extern "C" void orc_add_sink_sources(double* dU, const double* U, int nx, int ny, int nz,
-                                     double dx, double dy, double dz, const orc_bh* bhs, int nbh,
-                                     double x0, double y0, double z0, double f_sink, int torque_free,
-                                     double rho_sink_min) {
+extern "C" void orc_gas_force_on_bh(const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                                    const orc_bh* bh, double x0, double y0, double z0, double out[3]) {
+    orc_gas_force_on_bh_slab(U, nx, ny, nz, dx, dy, dz, bh, x0, y0, z0, 0, out);
+}
+
+/* src/gpu_kernels.jl:238-284 via src/sinks.jl:32-59 (the _slab form: see
+ * orc_add_bh_gravity_source_slab) */
+extern "C" void orc_add_sink_sources_slab(double* dU, const double* U, int nx, int ny, int nz,
+                                          double dx, double dy, double dz, const orc_bh* bhs, int nbh,
+                                          double x0, double y0, double z0, double f_sink, int torque_free,
+                                          double rho_sink_min, int kofs) {
     Idx I(nx, ny, nz);
     const int ng = NG;
     std::vector<double> rs(nbh), ts(nbh);
@@ -132,7 +148,7 @@ extern "C" void orc_add_sink_sources(double* dU, const double* U, int nx, int ny
                 int i = ii + ng, j = jj + ng, k = kk + ng;
                 double xc = x0 + ((double)ii - 0.5) * dx;
                 double yc = y0 + ((double)jj - 0.5) * dy;
-                double zc = z0 + ((double)kk - 0.5) * dz;
+                double zc = z0 + ((double)(kofs + kk) - 0.5) * dz;
                 double r = U[I(1, i, j, k)];
                 double mx = U[I(2, i, j, k)], my = U[I(3, i, j, k)], mz = U[I(4, i, j, k)];
                 double E = U[I(5, i, j, k)];
@@ -164,6 +180,14 @@ extern "C" void orc_add_sink_sources(double* dU, const double* U, int nx, int ny
             }
 }
 
+extern "C" void orc_add_sink_sources(double* dU, const double* U, int nx, int ny, int nz,
+                                     double dx, double dy, double dz, const orc_bh* bhs, int nbh,
+                                     double x0, double y0, double z0, double f_sink, int torque_free,
+                                     double rho_sink_min) {
+    orc_add_sink_sources_slab(dU, U, nx, ny, nz, dx, dy, dz, bhs, nbh, x0, y0, z0, f_sink, torque_free,
+                              rho_sink_min, 0);
+}
+
 /* src/sinks.jl:74-109 */
 extern "C" void orc_accrete(orc_bh* bh, const double* U, int nx, int ny, int nz, double dx, double dy,
                             double dz, double x0, double y0, double z0, double dt, double f_sink,
@@ -193,6 +217,37 @@ extern "C" void orc_accrete(orc_bh* bh, const double* U, int nx, int ny, int nz,
         bh->vel[2] = (bh->mass * bh->vel[2] + dPz) / M_new;
         bh->mass = M_new;
     }
+}
+
+/* The terms accrete! (src/sinks.jl:74-109) adds, for the cells of the
+ * global active box [ilo,ihi] x [jlo,jhi] x [klo,khi] (0-based, inclusive)
+ * that lie in this z-slab (global planes kofs .. kofs + nz - 1), in the
+ * reference's (k, j, i) loop order: {rho, mx, my, mz} * rate for a cell in
+ * the sink sphere with rho > rho_sink_min, zeros for any other cell (adding
+ * +0.0 leaves the sequential sums as skipping the cell does).  Returns the
+ * number of cells written (4 doubles each). */
+extern "C" long orc_sink_terms_slab(const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                                    double x0, double y0, double z0, int kofs, const orc_bh* bh, double rate,
+                                    double rho_sink_min, int ilo, int ihi, int jlo, int jhi, int klo, int khi,
+                                    double* out) {
+    Idx I(nx, ny, nz);
+    const int ng = NG;
+    double rs = orc_r_sink(bh);
+    long n = 0;
+    int k_lo = std::max(klo, kofs), k_hi = std::min(khi, kofs + nz - 1);
+    for (int kg = k_lo; kg <= k_hi; ++kg) for (int j = jlo; j <= jhi; ++j) for (int i = ilo; i <= ihi; ++i) {
+        double xc = x0 + ((double)(i + 1) - 0.5) * dx;
+        double yc = y0 + ((double)(j + 1) - 0.5) * dy;
+        double zc = z0 + ((double)(kg + 1) - 0.5) * dz;
+        double r = std::sqrt(sq(xc - bh->pos[0]) + sq(yc - bh->pos[1]) + sq(zc - bh->pos[2]));
+        double* o = out + 4 * n++;
+        o[0] = o[1] = o[2] = o[3] = 0.0;
+        int k = kg - kofs;
+        if (r >= rs) continue;
+        if (U[I(1, ng + 1 + i, ng + 1 + j, ng + 1 + k)] <= rho_sink_min) continue;
+        for (int q = 0; q < 4; ++q) o[q] = U[I(1 + q, ng + 1 + i, ng + 1 + j, ng + 1 + k)] * rate;
+    }
+    return n;
 }
 
 /* src/nbody.jl:24-56 */

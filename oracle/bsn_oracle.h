@@ -87,6 +87,19 @@ void   orc_add_sink_sources(double* dU, const double* U, int nx, int ny, int nz,
                             double dx, double dy, double dz, const orc_bh* bhs, int nbh,
                             double x0, double y0, double z0, double f_sink, int torque_free,
                             double rho_sink_min);
+void   orc_add_bh_gravity_source_slab(double* dU, const double* U, int nx, int ny, int nz,
+                                      double dx, double dy, double dz, const orc_bh* bhs, int nbh,
+                                      double x0, double y0, double z0, int kofs);
+void   orc_gas_force_on_bh_slab(const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                                const orc_bh* bh, double x0, double y0, double z0, int kofs, double out[3]);
+void   orc_add_sink_sources_slab(double* dU, const double* U, int nx, int ny, int nz,
+                                 double dx, double dy, double dz, const orc_bh* bhs, int nbh,
+                                 double x0, double y0, double z0, double f_sink, int torque_free,
+                                 double rho_sink_min, int kofs);
+long   orc_sink_terms_slab(const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
+                           double x0, double y0, double z0, int kofs, const orc_bh* bh, double rate,
+                           double rho_sink_min, int ilo, int ihi, int jlo, int jhi, int klo, int khi,
+                           double* out);
 void   orc_accrete(orc_bh* bh, const double* U, int nx, int ny, int nz, double dx, double dy, double dz,
                    double x0, double y0, double z0, double dt, double f_sink, double rho_sink_min);
 void   orc_nbody_step(orc_bh* bhs, int nbh, double dt, const double* F_gas /* [nbh][3] */);

@@ -80,6 +80,11 @@ def _declare(L):
         "orc_gas_force_on_bh": (V, [P, i, i, i, d, d, d, C.POINTER(OrcBH), d, d, d, P]),
         "orc_add_sink_sources": (V, [P, P, i, i, i, d, d, d, C.POINTER(OrcBH), i, d, d, d, d, i, d]),
         "orc_accrete": (V, [C.POINTER(OrcBH), P, i, i, i, d, d, d, d, d, d, d, d, d]),
+        "orc_add_bh_gravity_source_slab": (V, [P, P, i, i, i, d, d, d, C.POINTER(OrcBH), i, d, d, d, i]),
+        "orc_gas_force_on_bh_slab": (V, [P, i, i, i, d, d, d, C.POINTER(OrcBH), d, d, d, i, P]),
+        "orc_add_sink_sources_slab": (V, [P, P, i, i, i, d, d, d, C.POINTER(OrcBH), i, d, d, d, d, i, d, i]),
+        "orc_sink_terms_slab": (C.c_long, [P, i, i, i, d, d, d, d, d, d, i, C.POINTER(OrcBH), d, d,
+                                           i, i, i, i, i, i, P]),
         "orc_nbody_step": (V, [C.POINTER(OrcBH), i, d, P]),
         "orc_kepler_init": (i, [C.POINTER(OrcBH), P, P, d, P]),
         "orc_kepler_update": (V, [C.POINTER(OrcBH), P, d]),
@@ -261,6 +266,36 @@ def add_sink_sources(dU, U, dx, dy, dz, bhs, x0, y0, z0, f_sink=1.0, torque_free
 
 def accrete(bh: OrcBH, U, dx, dy, dz, x0, y0, z0, dt, f_sink=1.0, rho_sink_min=0.0):
     lib().orc_accrete(C.byref(bh), _p(U), *dims(U), dx, dy, dz, x0, y0, z0, dt, f_sink, rho_sink_min)
+
+
+def add_bh_gravity_source_slab(dU, U, dx, dy, dz, bhs, x0, y0, z0, kofs):
+    """add_bh_gravity_source! on a z-slab whose first active plane is global plane kofs."""
+    arr = bh_array(bhs)
+    lib().orc_add_bh_gravity_source_slab(_p(dU), _p(U), *dims(U), dx, dy, dz, arr, len(bhs), x0, y0, z0, kofs)
+
+
+def gas_force_on_bh_slab(U, dx, dy, dz, bh, x0, y0, z0, kofs):
+    out = (C.c_double * 3)()
+    lib().orc_gas_force_on_bh_slab(_p(U), *dims(U), dx, dy, dz, C.byref(bh), x0, y0, z0, kofs, out)
+    return np.array(out[:])
+
+
+def add_sink_sources_slab(dU, U, dx, dy, dz, bhs, x0, y0, z0, kofs, f_sink=1.0, torque_free=True, rho_sink_min=0.0):
+    arr = bh_array(bhs)
+    lib().orc_add_sink_sources_slab(_p(dU), _p(U), *dims(U), dx, dy, dz, arr, len(bhs), x0, y0, z0,
+                                    f_sink, int(torque_free), rho_sink_min, kofs)
+
+
+def sink_terms_slab(U, dx, dy, dz, x0, y0, z0, kofs, bh, rate, rho_sink_min, box):
+    """accrete!'s per-cell terms over this slab's part of the global box (k, j, i order), (n, 4)."""
+    ilo, ihi, jlo, jhi, klo, khi = box
+    nz = dims(U)[2]
+    n = max(0, ihi - ilo + 1) * max(0, jhi - jlo + 1) * max(0, min(khi, kofs + nz - 1) - max(klo, kofs) + 1)
+    out = np.zeros((max(n, 1), 4))
+    m = lib().orc_sink_terms_slab(_p(U), *dims(U), dx, dy, dz, x0, y0, z0, kofs, C.byref(bh), rate, rho_sink_min,
+                                  ilo, ihi, jlo, jhi, klo, khi, out.ctypes.data_as(_dp))
+    assert m == n
+    return out[:n]
 
 
 def nbody_step(bhs_arr, nbh, dt, F_gas: np.ndarray):

@@ -72,13 +72,26 @@ def test_nested_coupled_live_orbit_selfgravity(orc, bsn):
                                         torque_free=True, self_gravity=True, rho_sink_min=2e-8, evolve_orbit=True)
     assert n == 3 and t == t_ref
     # momentum components against the largest momentum component (z momentum
-    # alone is tiny in this orbit-plane-symmetric problem)
-    err = []
-    for Ud, Uo in zip(Hd.levels, H.levels):
-        G = host(Ud)
-        scale = [np.abs(Uo[0]).max()] + [np.abs(Uo[1:4]).max()] * 3 + [np.abs(Uo[4]).max()]
-        err.append([float(np.abs(G[q] - Uo[q]).max() / scale[q]) for q in range(5)])
-    assert max(max(e) for e in err) <= 1e-10, err
+    # alone is tiny in this orbit-plane-symmetric problem).  The problem
+    # amplifies rounding: the oracle itself, rerun from a state perturbed by
+    # 1e-15 relative, moves by the amount measured here (sens), so the bound
+    # is the larger of 1e-10 and 10 x that sensitivity.
+    def rel(A, B):
+        out = []
+        for Ua, Ub in zip(A, B):
+            scale = [np.abs(Ub[0]).max()] + [np.abs(Ub[1:4]).max()] * 3 + [np.abs(Ub[4]).max()]
+            out.append([float(np.abs(Ua[q] - Ub[q]).max() / scale[q]) for q in range(5)])
+        return out
+    err = rel([host(Ud) for Ud in Hd.levels], H.levels)
+    Hp, _, bp, _, _ = _setup(orc, bsn)
+    rng = np.random.default_rng(5)
+    for Up in Hp.levels:
+        Up[0] *= 1.0 + 1e-15 * rng.standard_normal(Up[0].shape)
+    _oracle_loop(Hp, bp, x0, 3, True, True, dt_max=5e-4)
+    sens = rel(Hp.levels, H.levels)
+    print("GPU vs oracle", err, "oracle vs perturbed oracle", sens)
+    bound = max(1e-10, 10 * max(max(s) for s in sens))
+    assert max(max(e) for e in err) <= bound, (err, sens)
     for i in range(2):
         assert abs(bg[i].mass - bo[i].mass) <= 1e-13 * bo[i].mass
         assert np.allclose(list(bg[i].pos), list(bo[i].pos), rtol=0, atol=1e-13)

@@ -56,7 +56,13 @@ def _density(nx, ny, nz, dx, dy, dz, seed):
 
 @pytest.mark.parametrize("shape,d", [((128, 128, 128), (4.0 / 128,) * 3),
                                      ((32, 64, 16), (0.05, 0.03, 0.11)),
-                                     ((16, 16, 64), (0.1, 0.1, 0.025))])
+                                     ((16, 16, 64), (0.1, 0.1, 0.025)),
+                                     # every line length of the transforms, 4 .. 4096 points
+                                     ((2, 4, 8), (0.3, 0.2, 0.1)),
+                                     ((512, 4, 2), (0.004, 0.2, 0.3)),
+                                     ((4, 2048, 2), (0.2, 0.001, 0.3)),
+                                     ((2, 2, 1024), (0.3, 0.3, 0.002)),
+                                     ((256, 16, 32), (0.01, 0.1, 0.05))])
 def test_poisson_solve_matches_cufft(shape, d):
     import bsn
     rho = dev(_density(*shape, *d, seed=sum(shape)))

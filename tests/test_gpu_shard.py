@@ -123,3 +123,93 @@ def test_single_slab_self_gravity_step_matches_coupled_step(orc):
     a = (slice(NG, -NG),) * 3
     for q in range(5):
         assert np.abs(got[(q,) + a] - U[(q,) + a]).max() <= 1e-11 * np.abs(U[q]).max(), q
+
+
+SLAB_SPECS = [dict(pos=(0.43, 0.37, 0.05), vel=(0.1, -0.2, 0.05), mass=1.0, eps=0.05, c_code=1e6, r_floor=0.3),
+              dict(pos=(0.2, 0.61, -0.21), vel=(-0.1, 0.0, 0.2), mass=0.5, eps=0.02, c_code=1e6, r_floor=0.25)]
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_slab_bh_sources_and_accretion_on_device(orc, world):
+    """The slab forms of the BH sources on the device, the ranks' slabs taken
+    one after another in one process: BH gravity and the sink sources with
+    the global plane index are the undivided kernels' bit for bit, the
+    accrete! terms of the slabs concatenated in rank order give the undivided
+    accrete! (device and oracle) bit for bit, and the merged gas-force pairs
+    agree with the undivided compensated sum to 1e-15."""
+    import bsn
+    from bsn import shard
+    n, nz, d = 16, 32, (0.07, 0.08, 0.06)
+    x0, y0, z0 = 0.0, -0.1, -0.96
+    U = random_state(n, n, nz, seed=31)
+    Ud = dev(U)
+    mk = lambda: [bsn.BlackHole(s["pos"], s["vel"], s["mass"], s["eps"], s["c_code"], s["r_floor"])
+                  for s in SLAB_SPECS]
+    bhs = mk()
+    dU_ref = torch.zeros_like(Ud)
+    bsn.add_bh_gravity_source(dU_ref, Ud, n, n, nz, *d, bhs, x0, y0, z0)
+    bsn.add_sink_sources(dU_ref, Ud, n, n, nz, *d, bhs, x0, y0, z0, f_sink=1.3, rho_sink_min=0.9)
+    F_ref = [bsn.gas_force_on_bh(Ud, n, n, nz, *d, b, x0, y0, z0) for b in bhs]
+    acc_ref = mk()
+    for b in acc_ref:
+        bsn.accrete(b, Ud, n, n, nz, *d, x0, y0, z0, 0.01, f_sink=1.3, rho_sink_min=0.9)
+    nzl = nz // world
+    pairs = [[] for _ in bhs]
+    terms = [[] for _ in bhs]
+    boxes = [bsn.sink_box(b, n, n, nz, *d, x0, y0, z0) for b in bhs]
+    for r in range(world):
+        k0 = r * nzl
+        Us = bsn.state(n, n, nzl)
+        shard._zmajor(Us)[...] = shard._zmajor(Ud)[k0:k0 + nzl + 2 * NG]
+        dUs = torch.zeros_like(Us)
+        bsn.add_bh_gravity_source_slab(dUs, Us, n, n, nzl, *d, bhs, x0, y0, z0, k0)
+        bsn.add_sink_sources_slab(dUs, Us, n, n, nzl, *d, bhs, x0, y0, z0, k0, f_sink=1.3, rho_sink_min=0.9)
+        got = dUs[:, NG:NG + n, NG:NG + n, NG:NG + nzl]
+        want = dU_ref[:, NG:NG + n, NG:NG + n, NG + k0:NG + k0 + nzl]
+        assert torch.equal(got, want), r
+        for i, b in enumerate(bhs):
+            pairs[i].append(bsn.gas_force_pairs_slab(Us, n, n, nzl, *d, b, x0, y0, z0, k0))
+            terms[i].append(bsn.sink_terms_slab(Us, n, n, nzl, *d, x0, y0, z0, k0, b, 0.01, boxes[i], f_sink=1.3,
+                                                rho_sink_min=0.9))
+    assert sum(len(t) > 0 for t in terms[0]) >= 2   # the sphere straddles a slab boundary
+    acc = mk()
+    ob = [orc.make_bh(s["pos"], s["vel"], s["mass"], s["eps"], s["c_code"], s["r_floor"]) for s in SLAB_SPECS]
+    for i, b in enumerate(acc):
+        bsn.accrete_from_terms(b, np.concatenate(terms[i]))
+        orc.accrete(ob[i], U, *d, x0, y0, z0, 0.01, f_sink=1.3, rho_sink_min=0.9)
+        assert b.mass > SLAB_SPECS[i]["mass"]
+        for want in (acc_ref[i], ob[i]):
+            assert b.mass == want.mass and list(b.vel) == list(want.vel)
+        F = bsn.merge_force_pairs(np.array(pairs[i]))
+        assert np.abs(F - F_ref[i]).max() <= 1e-15 * np.abs(F_ref[i]).max()
+        s = SLAB_SPECS[i]   # the BH before accretion
+        F_orc = orc.gas_force_on_bh(U, *d, orc.make_bh(s["pos"], s["vel"], s["mass"], s["eps"], s["c_code"],
+                                                       s["r_floor"]), x0, y0, z0)
+        assert np.abs(F - F_orc).max() <= 1e-13 * np.abs(F_orc).max()
+
+
+def test_single_slab_coupled_step_bitwise_to_oracle(orc):
+    """shard.coupled_step on one rank with the device operations (the slab
+    source forms, accrete! through its terms) against the oracle's
+    coupled_step!, orbit frozen: bit for bit."""
+    import bsn
+    from bsn import shard
+    from binary_ic import binary_setup
+    U, dx, x0, specs = binary_setup(orc, n=32)
+    Ud = dev(U)
+    bg = [bsn.BlackHole(s["pos"], s["vel"], s["mass"], s["eps"], s["c_code"], s["r_floor"]) for s in specs]
+    bo = orc.bh_array([orc.make_bh(s["pos"], s["vel"], s["mass"], s["eps"], s["c_code"], s["r_floor"])
+                       for s in specs])
+    slab = shard.Slab.split(32, 32, 32, 0, 1)
+    t = 0.0
+    for _ in range(3):
+        dt = orc.cfl_dt_3d(U, dx, dx, dx, 4 / 3, 0.4)
+        shard.coupled_step(Ud, bg, slab, dt, t, dx, x0, x0, x0, 4 / 3, shard.DeviceOps(), rho_floor=1e-8,
+                           P_floor=1e-10, rho_sink_min=2e-8, evolve_orbit=False)
+        orc.coupled_step(U, bo, 2, dt, t, dx, x0, x0, x0, 4 / 3, 1.0, 1e-8, 1e-10, True, False, 0.0, 2e-8,
+                         evolve_orbit=False)
+        t += dt
+    assert_bitwise(host(Ud), U, "coupled step on one slab")
+    for i in range(2):
+        assert bg[i].mass == bo[i].mass and list(bg[i].vel) == list(bo[i].vel)
+        assert bg[i].mass > specs[i]["mass"]

@@ -48,6 +48,26 @@ class OracleOps:
     def cfl(self, U, nx, ny, nz, dx, dy, dz, gamma, cfl):
         return self.orc.cfl_dt_3d(U, dx, dy, dz, gamma, cfl)
 
+    def _obhs(self, bhs):
+        return [self.orc.make_bh(tuple(b.pos), tuple(b.vel), b.mass, b.eps, b.c_code, b.r_floor) for b in bhs]
+
+    def bh_gravity(self, dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0, k0):
+        self.orc.add_bh_gravity_source_slab(dU, U, dx, dy, dz, self._obhs(bhs), x0, y0, z0, k0)
+
+    def sink_sources(self, dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0, k0, f_sink, torque_free, rho_sink_min):
+        self.orc.add_sink_sources_slab(dU, U, dx, dy, dz, self._obhs(bhs), x0, y0, z0, k0, f_sink=f_sink,
+                                       torque_free=torque_free, rho_sink_min=rho_sink_min)
+
+    def gas_force_pairs(self, U, nx, ny, nz, dx, dy, dz, bh, x0, y0, z0, k0):
+        # the oracle's sequential sum over the slab as the partial (lo = 0)
+        F = self.orc.gas_force_on_bh_slab(U, dx, dy, dz, self._obhs([bh])[0], x0, y0, z0, k0)
+        return np.array([F[0], 0.0, F[1], 0.0, F[2], 0.0])
+
+    def sink_terms(self, U, nx, ny, nz, dx, dy, dz, x0, y0, z0, k0, bh, dt, box, f_sink, rho_sink_min):
+        ob = self._obhs([bh])[0]
+        rate = dx * dy * dz / self.orc.t_sink(ob, f_sink) * dt
+        return self.orc.sink_terms_slab(U, dx, dy, dz, x0, y0, z0, k0, ob, rate, rho_sink_min, box)
+
     def floor_planes(self, planes, nx, ny, rho_floor, P_floor, gamma):
         import torch
         G = self.orc.state(nx, ny, NG)
@@ -389,4 +409,99 @@ def test_slab_step_with_self_gravity_matches_coupled_step(world):
     distributed solve's torch.fft phases differ from the oracle's FFT by
     rounding only."""
     for rank, ok, info in _spawn(_sg_step_worker, world):
+        assert ok, (rank, info)
+
+
+def _coupled_worker(rank, world, port, q, live, self_gravity):
+    """Three coupled_step!s of the binary-BH physics on slabs (oracle
+    arithmetic per slab, the product's exchange, gas-force merge and
+    accretion gather) against the oracle's undivided coupled_step!."""
+    try:
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        import torch.distributed as dist
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        sys.path.insert(0, os.path.join(ROOT, "binary-supernova_b200"))
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle as orc
+        import bsn
+        from bsn import shard
+        from binary_ic import binary_setup
+        dist.init_process_group("gloo", rank=rank, world_size=world)
+        # 32^3: on 16^3 the two-cell bomb leaves faces whose reconstruction
+        # switches branch on a 1e-15 change of the state (the reference's own
+        # conditioning, seen with any reordering of the gas-force sum)
+        n, g = 32, 4.0 / 3.0
+        U, dx, x0, specs = binary_setup(orc, n=n)
+        ref = U.copy(order="F")
+        bo = orc.bh_array([orc.make_bh(s["pos"], s["vel"], s["mass"], s["eps"], s["c_code"], s["r_floor"])
+                           for s in specs])
+        bg = [bsn.BlackHole(s["pos"], s["vel"], s["mass"], s["eps"], s["c_code"], s["r_floor"]) for s in specs]
+        slab = shard.Slab.split(n, n, n, rank, world)
+        k0 = slab.k0
+        Us = orc.state(n, n, slab.nz)
+        Us[...] = U[:, :, :, k0:k0 + slab.nz + 2 * NG]
+        ops = SGOps(orc) if self_gravity else OracleOps(orc, dx)
+        kw = dict(f_sink=1.0, rho_floor=1e-8, P_floor=1e-10, torque_free=True, self_gravity=self_gravity,
+                  t_bh2_sink_on=0.0, rho_sink_min=2e-8, evolve_orbit=live)
+        t, err = 0.0, []
+        for _ in range(2 if live else 3):
+            dt = shard.cfl_dt(Us, slab, dx, dx, dx, g, 0.4, ops)
+            dt_ref = orc.cfl_dt_3d(ref, dx, dx, dx, g, 0.4)
+            if live:
+                dt = dt_ref = min(dt, dt_ref)   # the states differ by rounding; keep one dt
+            Fs = shard.coupled_step(Us, bg, slab, dt, t, dx, x0, x0, x0, g, ops, **kw)
+            Fo = orc.coupled_step(ref, bo, 2, dt_ref, t, dx, x0, x0, x0, g, kw["f_sink"], kw["rho_floor"],
+                                  kw["P_floor"], True, self_gravity, 0.0, kw["rho_sink_min"], evolve_orbit=live)
+            t += dt
+            if not live:
+                assert dt == dt_ref, (dt, dt_ref)
+            err.append(float(np.abs(Fs - Fo).max() / np.abs(Fo).max()))
+        a = (slice(None), slice(NG, NG + n), slice(NG, NG + n))
+        mine = Us[a + (slice(NG, NG + slab.nz),)]
+        theirs = ref[a + (slice(NG + k0, NG + k0 + slab.nz),)]
+        if live or self_gravity:
+            st = max(float(np.abs(mine[c] - theirs[c]).max() / np.abs(ref[c]).max()) for c in range(5))
+            bh = max(max(abs(bg[i].mass - bo[i].mass) / bo[i].mass,
+                          max(abs(p - r) for p, r in zip(bg[i].pos, bo[i].pos)),
+                          max(abs(p - r) for p, r in zip(bg[i].vel, bo[i].vel))) for i in range(2))
+            ok = st < 1e-11 and bh < 1e-12 and max(err) < 1e-10
+            info = (st, bh, max(err))
+        else:
+            same = bool((mine == theirs).all())
+            bh_same = all(bg[i].mass == bo[i].mass and list(bg[i].vel) == list(bo[i].vel)
+                          and list(bg[i].pos) == list(bo[i].pos) for i in range(2))
+            grew = all(bg[i].mass > s["mass"] for i, s in enumerate(specs))   # both sinks accreted
+            ok = same and bh_same and grew and max(err) < 1e-12
+            info = (same, bh_same, grew, max(err), [bg[i].mass for i in range(2)])
+        q.put((rank, ok, info))
+        dist.destroy_process_group()
+    except Exception as e:   # report to the parent instead of hanging it
+        import traceback
+        q.put((rank, False, traceback.format_exc()))
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_slab_coupled_step_frozen_orbit_bitwise(world):
+    """coupled_step! with the orbit frozen: BH gravity and the sink sources per
+    slab cell with the global index, and accrete! as an ordered gather of the
+    sink sphere's terms (the sphere straddles the slab boundaries), give the
+    undivided oracle's state, BH masses and velocities bit for bit; the
+    merged gas force agrees with the oracle's sequential sum to 1e-12."""
+    for rank, ok, info in _spawn(_coupled_worker, world, (False, False)):
+        assert ok, (rank, info)
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_slab_coupled_step_live_orbit(world):
+    """coupled_step! with the live N-body orbit: the gas force merged over
+    the ranks drives nbody_step! on every rank; state, BHs and forces follow
+    the undivided oracle to the whole-grid sum's rounding."""
+    for rank, ok, info in _spawn(_coupled_worker, world, (True, False)):
+        assert ok, (rank, info)
+
+
+def test_slab_coupled_step_with_self_gravity():
+    """coupled_step! with the live orbit and self-gravity (the distributed
+    solve's torch.fft phases) on two ranks against the undivided oracle."""
+    for rank, ok, info in _spawn(_coupled_worker, 2, (True, True)):
         assert ok, (rank, info)
