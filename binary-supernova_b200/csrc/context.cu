@@ -158,7 +158,11 @@ extern "C" bsn_status bsn_ctx_set_stiff_guard(bsn_ctx* ctx, int on) {
     if (!ctx) return BSN_ERR_ARG;
     BSN_TRY(cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"));
     ctx->stiff_guard = on ? 1 : 0;
-    bsn::run_state_free(ctx);   // the device time loop's graph holds the kernels chosen before
+    // the captured time-loop graphs hold the kernels chosen before
+    bsn::run_state_free(ctx);
+    bsn::fmr_run_state_free(ctx);
+    bsn::fmrN_state_free(ctx);
+    bsn::relax_state_free(ctx);
     return BSN_OK;
 }
 

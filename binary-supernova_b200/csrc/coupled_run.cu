@@ -505,7 +505,7 @@ extern "C" bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2*
     if (!ctx->coupled_nested_state) ctx->coupled_nested_state = new NState();
     NState* S = (NState*)ctx->coupled_nested_state;
     NPlan plan;
-    BSN_TRY(make_plan(ctx, pairs, npairs, precision, self_gravity, 1.0, S, plan));
+    BSN_TRY(make_plan(ctx, pairs, npairs, precision, self_gravity, 1.0, 1, S, plan));
     const int nl = plan.nl;
     bsn_status st;
     Dev* r = (Dev*)slot(ctx, SLOT_CRUN, sizeof(Dev), &st); BSN_TRY(st);

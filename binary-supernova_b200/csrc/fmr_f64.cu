@@ -348,7 +348,7 @@ bsn_status fmr3d_step(bsn_ctx* ctx, const bsn_fmr2* g, double dt_c, int self_gra
     {
         f64::StageArgs base;
         stage_args_init(base, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, g->gamma, g->bc, g->rho_floor,
-                        g->P_floor); base.stiff_guard = 1;
+                        g->P_floor); base.stiff_guard = ctx->stiff_guard;
         base.use_reg = 1;
         for (int i = 0; i < 6; ++i) base.reg.reg[i] = R.c.r[i];
         for (int d = 0; d < 3; ++d) {
@@ -375,7 +375,7 @@ bsn_status fmr3d_step(bsn_ctx* ctx, const bsn_fmr2* g, double dt_c, int self_gra
     double* Af = (double*)slot(ctx, SLOT_FMR_FA, sizeof(double) * F.nelem(), &st); BSN_TRY(st);
     double* Bf = (double*)slot(ctx, SLOT_FMR_FB, sizeof(double) * F.nelem(), &st); BSN_TRY(st);
     f64::StageArgs fb;
-    stage_args_init(fb, g->nfx, g->nfy, g->nfz, g->dxf, g->dyf, g->dzf, g->gamma, g->bc, g->rho_floor, g->P_floor); fb.stiff_guard = 1;
+    stage_args_init(fb, g->nfx, g->nfy, g->nfz, g->dxf, g->dyf, g->dzf, g->gamma, g->bc, g->rho_floor, g->P_floor); fb.stiff_guard = ctx->stiff_guard;
     fb.Gh = Gh;
     fb.use_bnd = 1;
     for (int i = 0; i < 6; ++i) fb.bnd.f[i] = const_cast<double*>(R.f.bnd[i]);
@@ -526,7 +526,7 @@ bsn_status fmr3d_run(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int prec, int 
     // level arguments (as fmr3d_step), dt and done on the device
     const double rk_w[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
     f64::StageArgs cb, fb;
-    stage_args_init(cb, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, g->gamma, g->bc, g->rho_floor, g->P_floor); cb.stiff_guard = 1;
+    stage_args_init(cb, g->ncx, g->ncy, g->ncz, g->dxc, g->dyc, g->dzc, g->gamma, g->bc, g->rho_floor, g->P_floor); cb.stiff_guard = ctx->stiff_guard;
     cb.use_reg = 1;
     for (int i = 0; i < 6; ++i) cb.reg.reg[i] = R.c.r[i];
     for (int d = 0; d < 3; ++d) {
@@ -538,7 +538,7 @@ bsn_status fmr3d_run(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int prec, int 
     if (self_gravity) { cb.use_sg = 1; cb.phi = phic; }
     cb.dt_dev = &rd->dt;
     cb.done_dev = &rd->done;
-    stage_args_init(fb, g->nfx, g->nfy, g->nfz, g->dxf, g->dyf, g->dzf, g->gamma, g->bc, g->rho_floor, g->P_floor); fb.stiff_guard = 1;
+    stage_args_init(fb, g->nfx, g->nfy, g->nfz, g->dxf, g->dyf, g->dzf, g->gamma, g->bc, g->rho_floor, g->P_floor); fb.stiff_guard = ctx->stiff_guard;
     fb.Gh = Gh;
     fb.use_bnd = 1;
     for (int i = 0; i < 6; ++i) fb.bnd.f[i] = const_cast<double*>(R.f.bnd[i]);

@@ -99,7 +99,7 @@ struct NPlan {
 // arguments per level (registers toward the child, boundary faces toward the
 // parent, ghosts from the parent, Phi with self-gravity, dt read on the
 // device).  Callers may add sources to plan.base[l] before plan.step().
-bsn_status make_plan(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, int prec, int sg, double G_grav, NState* S,
+bsn_status make_plan(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, int prec, int sg, double G_grav, int guard, NState* S,
                      NPlan& plan);
 
 // graphs, stream, events and arena of a state, then the state itself

@@ -186,7 +186,7 @@ bsn_status NPlan::step() {
 static size_t align_up(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // Validate the chain, lay out the arena and fill the plan.
-bsn_status make_plan(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, int prec, int sg, double G_grav,
+bsn_status make_plan(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, int prec, int sg, double G_grav, int guard,
                             NState* S, NPlan& plan) {
     if (!pairs || npairs < 1 || npairs > NMAXL - 1)
         return set_err(ctx, BSN_ERR_ARG, "need 1..%d level pairs, got %d", NMAXL - 1, npairs);
@@ -289,7 +289,7 @@ bsn_status make_plan(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, int prec, 
         f64::StageArgs& a = plan.base[l];
         const NLevel& v = plan.L[l];
         stage_args_init(a, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz, plan.gamma, plan.bc, plan.rho_floor, plan.P_floor);
-        a.stiff_guard = 1;   // floor atmospheres beside dense gas: stiff FP32 faces in FP64
+        a.stiff_guard = guard;   // FP32 faces of stiff stencils in FP64 (sinks beside dense gas)
         if (l < plan.nl - 1) {
             const Geo& G = plan.P[l].G;
             a.use_reg = 1;
@@ -322,7 +322,7 @@ static NState* nstate(bsn_ctx* ctx) {
 bsn_status fmrN_step(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, double dt0, int sg, double G_grav) {
     NState* S = nstate(ctx);
     NPlan plan;
-    BSN_TRY(make_plan(ctx, pairs, npairs, PREC_F64, sg, G_grav, S, plan));
+    BSN_TRY(make_plan(ctx, pairs, npairs, PREC_F64, sg, G_grav, ctx->stiff_guard, S, plan));
     n_init_kernel<<<1, 1, 0, ctx->stream>>>(plan.d, 0.0);
     BSN_TRY(launch_check(ctx, "fmrN_init_kernel"));
     n_fixed_dt_kernel<<<1, 1, 0, ctx->stream>>>(plan.d, dt0, plan.R);
@@ -355,7 +355,7 @@ bsn_status fmrN_run(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, double cfl,
     if (n_steps < 0 || !t_inout) return set_err(ctx, BSN_ERR_ARG, "bad n_steps or null t_inout");
     NState* S = nstate(ctx);
     NPlan plan;
-    BSN_TRY(make_plan(ctx, pairs, npairs, prec, sg, G_grav, S, plan));
+    BSN_TRY(make_plan(ctx, pairs, npairs, prec, sg, G_grav, ctx->stiff_guard, S, plan));
     if (sg) {
         const NLevel& v = plan.L[0];
         if (prec == PREC_F64) BSN_TRY(poisson_prepare(ctx, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz));

@@ -129,7 +129,7 @@ extern "C" bsn_status bsn_relax_ic(bsn_ctx* ctx, double* U, int nx, int ny, int 
     // Omega = 0 to relax_damping_source!)
     f64::StageArgs base;
     stage_args_init(base, nx, ny, nz, dx, dy, dz, gamma, BSN_BC_OUTFLOW, rho_floor, P_floor);
-    base.stiff_guard = 1;
+    base.stiff_guard = ctx->stiff_guard;
     base.x0 = x0; base.y0 = y0; base.z0 = z0;
     if (nbh > 0) {
         base.use_bh = 1;

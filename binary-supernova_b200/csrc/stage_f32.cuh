@@ -46,8 +46,8 @@ struct F32Physics {
 // The FP32 policy with stiff faces in FP64: a face whose density stencil
 // spans more than three decades is computed from the FP64 state by the FP64
 // path's arithmetic (stage_tile.cuh face_flux_f64).  Launched where
-// A.stiff_guard is set: the driver loops with sinks, the FMR and relaxation
-// loops (near-vacuum cells beside dense gas), or any grid on request.
+// A.stiff_guard is set: the coupled driver loops with sinks (near-vacuum
+// cells beside dense gas), or any loop on request.
 struct F32Guarded : F32Physics {
     static constexpr bool kStiffFallback = true;
 };

@@ -144,12 +144,15 @@ enum { BSN_PREC_F64 = 0,     /* stencils in FP64, bit-identical to the reference
 /* FP32 stencils meet near-vacuum cells beside dense gas (a sink's
  * surroundings, a floor atmosphere): where a face's six-cell density stencil
  * spans more than three decades, FP32 rounding of the dense side's values is
- * 1e-4 and more of the thin cell's, and its velocity m / rho can run away.
+ * 1e-4 and more of the thin cell's, and its velocity m / rho can run away
+ * (seen beside the sinks, where the drain empties cells next to dense gas).
  * Such faces are computed in FP64 by the FP64 path's arithmetic in the
- * driver loops with sinks, the FMR and the relaxation loops; the uniform-grid
- * FP32 steps (bsn_euler3d_step_f32, bsn_run_steps) do it when on != 0 here
- * (default off: a few percent of the step).  Releases the context's
- * captured time-loop graph. */
+ * coupled driver loops with sinks (uniform and nested, bsn_coupled_step_f64)
+ * always; the other FP32 loops and steps (bsn_euler3d_step_f32,
+ * bsn_run_steps, the FMR and relaxation loops) do it when on != 0 here
+ * (default off: a star's surface in a floor atmosphere is a shell of stiff
+ * faces, which doubles the FP32 polytrope FMR step).  Releases the context's
+ * captured time-loop graphs. */
 bsn_status bsn_ctx_set_stiff_guard(bsn_ctx* ctx, int on);
 /* euler3d_rhs! with FP32 stencils (BSN_PREC_F32): the same semantics as
  * bsn_euler3d_rhs_f64 (mutates U: ghost fill, floors; fills the optional
