@@ -368,7 +368,7 @@ def fmr_polytrope(bsn, torch, steps, warmup, log, omega_frac=0.0, host_loop=True
     return out
 
 
-def binary_nested(bsn, torch, steps, warmup, log, n=128, paths=("f64", "f32", "learned")):
+def binary_nested(bsn, torch, steps, warmup, log, n=128, paths=("f64", "f32", "learned"), perturbed=False):
     """The binary-BH supernova on three nested FMR levels of n^3 (ratio 2) on
     [-8,8]^3, [-4,4]^3, [-2,2]^3: n=3 polytrope star (M=10, R=1, G=1, gamma
     4/3) with a thermal bomb E=1 in r<0.1 and two m=5 BH sinks at (+-1.5,0,0)
@@ -474,13 +474,30 @@ def binary_nested(bsn, torch, steps, warmup, log, n=128, paths=("f64", "f32", "l
         rho_f[prec] = H.levels[2][0].clone()
         E_f[prec] = H.levels[2][4].clone()
         del H
+    if perturbed:
+        # the problem's own conditioning: FP64 again from an initial density
+        # perturbed by 1e-15 relative, to the same time
+        H, b, common = fresh("f64", 1)
+        common["diag"] = None
+        gen = torch.Generator(device="cuda").manual_seed(7)
+        for U in H.levels:
+            U[0].mul_(1.0 + 1e-15 * torch.randn(U[0].shape, device="cuda", dtype=torch.float64, generator=gen))
+        _, k = bsn.coupled_nested_run_steps(H, b, -L, -L, -L, 0.4, n_steps=10 * (steps + warmup), t_end=t64,
+                                            **common)
+        out["f64_perturbed_accuracy_steps"] = k
+        rho_f["f64_perturbed"] = H.levels[2][0].clone()
+        E_f["f64_perturbed"] = H.levels[2][4].clone()
+        others = others + ["f64_perturbed"]
+        del H
     a = (slice(3, -3),) * 3
     ref = rho_f["f64"][a]
     refE = E_f["f64"][a]
     for prec in others:
         out[f"{prec}_L1_rho_finest_vs_f64"] = float((rho_f[prec][a] - ref).abs().sum() / ref.abs().sum())
         out[f"{prec}_L1_E_finest_vs_f64"] = float((E_f[prec][a] - refE).abs().sum() / refE.abs().sum())
-        out[f"speedup_{prec}_vs_f64"] = out["f64_device_loop_ms_per_step"] / out[f"{prec}_device_loop_ms_per_step"]
+        if f"{prec}_device_loop_ms_per_step" in out:
+            out[f"speedup_{prec}_vs_f64"] = (out["f64_device_loop_ms_per_step"]
+                                             / out[f"{prec}_device_loop_ms_per_step"])
     return out
 
 
@@ -847,7 +864,7 @@ def main():
         if args.workload == "binary_nested":
             paths = tuple(p_ for p_ in args.paths.split(",") if p_)
             steps, warmup = (1000, 0) if args.full else (args.steps, args.warmup)
-            out = binary_nested(bsn, torch, steps, warmup, log, paths=paths)
+            out = binary_nested(bsn, torch, steps, warmup, log, paths=paths, perturbed=args.full)
         else:
             steps, warmup = (200, 0) if args.full else (args.steps, args.warmup)
             out = fmr_polytrope(bsn, torch, steps, warmup, log, omega_frac=args.omega, host_loop=not args.full)

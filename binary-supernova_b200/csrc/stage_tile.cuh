@@ -302,13 +302,18 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
         return valid;
     };
     // thread-per-face loop (the plain stencil physics); faces whose density
-    // stencil is stiff (kStiffFallback policies) are left to a second pass
-    // that computes them in FP64, so the main loop keeps its registers
+    // stencil is stiff (kStiffFallback policies) are listed for a second pass
+    // that computes them in FP64, so the main loop keeps its registers, and
+    // the listed faces are spread over all threads of the block (they
+    // cluster: a star's surface, a sink's surroundings)
+    __shared__ int s_nstiff;
+    __shared__ int s_stiff[P::kStiffFallback ? NF : 1];
     auto plain_faces = [&]() {
-        static_assert(NF <= 32 * NT, "one bit per face of a thread");
-        unsigned stiff = 0u;
-        int it = 0;
-        for (int f = tid; f < NF; f += NT, ++it) {
+        if constexpr (P::kStiffFallback) {
+            if (tid == 0) s_nstiff = 0;
+            __syncthreads();
+        }
+        for (int f = tid; f < NF; f += NT) {
             int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
             if (!face_valid(fx, fy, fz)) continue;
             real c[6][6];
@@ -322,15 +327,17 @@ __device__ void sweep(const f64::StageArgs& A, const Geom& G, const typename P::
                 }
             }
             if constexpr (P::kStiffFallback) {
-                if (stiff_stencil(c)) { stiff |= 1u << it; continue; }
+                if (stiff_stencil(c)) { s_stiff[atomicAdd(&s_nstiff, 1)] = f; continue; }
             }
             real F[5];
             P::template flux<D>(c, k, F);
             emit(f, fx, fy, fz, F);
         }
         if constexpr (P::kStiffFallback) {
-            for (; stiff; stiff &= stiff - 1u) {
-                const int f = tid + NT * (__ffs(stiff) - 1);
+            __syncthreads();
+            const int nst = s_nstiff;   // read by every thread before the next sweep resets it
+            for (int i = tid; i < nst; i += NT) {
+                const int f = s_stiff[i];
                 const int fx = f % FX, r = f / FX, fy = r % FY, fz = r / FY;
                 double F64[5];
                 face_flux_f64<D>(A, o[0] + fx, o[1] + fy, o[2] + fz, F64);
