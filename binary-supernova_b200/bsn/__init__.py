@@ -9,3 +9,7 @@ sm_100a kernels through the C ABI of include/bsn.h.  There is no CPU path.
 """
 from .api import *  # noqa: F401,F403
 from .api import __all__  # noqa: F401
+from .h5io import *  # noqa: F401,F403,E402
+from .h5io import __all__ as _h5io_all  # noqa: E402
+
+__all__ = list(__all__) + list(_h5io_all)

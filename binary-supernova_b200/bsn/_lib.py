@@ -45,6 +45,17 @@ class bsn_fmr2(C.Structure):
                 ("gamma", C.c_double), ("bc", C.c_int), ("rho_floor", C.c_double), ("P_floor", C.c_double)]
 
 
+class bsn_ckpt_meta(C.Structure):
+    _fields_ = [("t", C.c_double), ("step", C.c_longlong), ("dt_last", C.c_double), ("t_snap", C.c_double),
+                ("t_bh2_sink_on", C.c_double)]
+
+
+class bsn_grid_meta(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
+                ("dz", C.c_double), ("gamma", C.c_double), ("x0", C.c_double), ("y0", C.c_double),
+                ("z0", C.c_double), ("rho_floor", C.c_double), ("P_floor", C.c_double)]
+
+
 _V, _I, _D, _P, _LL = C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_longlong
 _dp = C.POINTER(C.c_double)
 _BH = C.POINTER(bsn_bh)
@@ -101,6 +112,23 @@ SIGNATURES = {
     "bsn_sink_terms_slab_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _I, _BH, _D, _D, _D,
                                      C.POINTER(C.c_int), _dp, _LL, C.POINTER(C.c_longlong)]),
     "bsn_accrete_from_terms": (_I, [_BH, _dp, _LL]),
+    "bsn_save_checkpoint_uniform": (_I, [_V, C.c_char_p, _P, _I, _BH, _I, C.POINTER(bsn_grid_meta),
+                                         C.POINTER(bsn_ckpt_meta)]),
+    "bsn_save_checkpoint_uniform_async": (_I, [_V, C.c_char_p, _P, _BH, _I, C.POINTER(bsn_grid_meta),
+                                               C.POINTER(bsn_ckpt_meta)]),
+    "bsn_checkpoint_wait": (_I, [_V]),
+    "bsn_load_checkpoint_uniform": (_I, [_V, C.c_char_p, _P, _I, _BH, _I, C.POINTER(C.c_int),
+                                         C.POINTER(bsn_grid_meta), C.POINTER(bsn_ckpt_meta)]),
+    "bsn_save_checkpoint_fmr": (_I, [_V, C.c_char_p, _FMR, _I, _BH, _I, _D, _LL, _D]),
+    "bsn_load_checkpoint_fmr": (_I, [_V, C.c_char_p, _FMR, _I, _BH, _I, C.POINTER(C.c_int), _dp,
+                                     C.POINTER(C.c_longlong), _dp]),
+    "bsn_write_snapshot": (_I, [_V, C.c_char_p, _P, _I, _I, _I, _I, _D, _D, _D, _D, _D]),
+    "bsn_read_snapshot": (_I, [C.c_char_p, _dp, _LL, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                               _dp, _dp, _dp, _dp, _dp]),
+    "bsn_trajectory_init": (_I, [C.c_char_p, _I]),
+    "bsn_trajectory_append": (_I, [C.c_char_p, _D, _BH, _I]),
+    "bsn_trajectory_read": (_I, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp, _dp, _dp, _dp,
+                                 _LL]),
     "bsn_kepler_init": (_I, [_BH, _dp, _dp, _D, _dp]),
     "bsn_kepler_update": (_I, [_BH, _dp, _D]),
     "bsn_solve_poisson_isolated_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _P]),

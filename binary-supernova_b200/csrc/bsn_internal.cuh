@@ -50,6 +50,7 @@ struct bsn_ctx {
     int tma_now = 0;                 // the launch being made may use TMA staging (autotune.cu)
     int stiff_guard = 0;             // uniform-grid FP32 steps: stiff faces in FP64 (bsn_ctx_set_stiff_guard)
     int tma_used_last = 0;           // the last stage launch used it
+    void* ckpt_state = nullptr;      // h5io.cu: asynchronous checkpoint buffers and writer thread
 };
 
 namespace bsn {

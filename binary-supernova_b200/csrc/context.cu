@@ -102,6 +102,7 @@ void fmrN_state_free(bsn_ctx* ctx);      // fmr_nlevel.cu
 void coupled_run_state_free(bsn_ctx* ctx);   // coupled_run.cu
 void coupled_nested_state_free(bsn_ctx* ctx);   // coupled_run.cu
 void relax_state_free(bsn_ctx* ctx);     // relax.cu
+void ckpt_state_free(bsn_ctx* ctx);      // h5io.cu
 
 }  // namespace bsn
 
@@ -143,6 +144,7 @@ extern "C" bsn_status bsn_ctx_destroy(bsn_ctx* ctx) {
     coupled_run_state_free(ctx);
     coupled_nested_state_free(ctx);
     relax_state_free(ctx);
+    ckpt_state_free(ctx);
     for (auto& r : ctx->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     delete ctx;
     return BSN_OK;

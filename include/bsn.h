@@ -43,7 +43,8 @@ enum {
     BSN_ERR_TIMEOUT = 3,    /* a bounded device-side wait expired */
     BSN_ERR_NONFINITE = 4,  /* a NaN/Inf was detected where the reference would throw */
     BSN_ERR_UNSUPPORTED = 5,/* size/feature outside what this build supports */
-    BSN_ERR_NOMEM = 6       /* workspace allocation failed */
+    BSN_ERR_NOMEM = 6,      /* workspace allocation failed */
+    BSN_ERR_IO = 7          /* a checkpoint / snapshot file could not be written or read */
 };
 
 enum { BSN_BC_OUTFLOW = 0, BSN_BC_PERIODIC = 1 };
@@ -486,6 +487,69 @@ bsn_status bsn_cfl_dt_fmr_nested_f64(bsn_ctx* ctx, const bsn_fmr2* pairs, int np
 bsn_status bsn_fmr_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, double cfl, int precision,
                               int self_gravity, double G_grav, int n_steps, double t_end, double* t_inout,
                               int* steps_done);
+
+/* ---- src/checkpoint.jl, src/io.jl: HDF5 checkpoints, snapshots, trajectories
+ * The files are written by the library's own HDF5 writer (no HDF5 library is
+ * linked): version-2 superblock and object headers, compact groups,
+ * attributes in the object headers, contiguous little-endian float64 / int64
+ * datasets, null-terminated ASCII string attributes; array dimensions in
+ * HDF5 order, i.e. reversed from the reference's column-major shapes with
+ * the same bytes (the way HDF5.jl stores a Julia array).  The readers take
+ * the files this library writes.  Group, dataset and attribute names, shapes
+ * and meanings are the reference's. */
+typedef struct {   /* the /manifest scalars of a uniform checkpoint */
+    double t; long long step; double dt_last, t_snap, t_bh2_sink_on;
+} bsn_ckpt_meta;
+typedef struct {   /* the /grid attributes of a uniform checkpoint */
+    int nx, ny, nz; double dx, dy, dz, gamma, x0, y0, z0, rho_floor, P_floor;
+} bsn_grid_meta;
+/* save_checkpoint_uniform (src/checkpoint.jl:222-265): U the ghosted state
+ * (device memory when on_device != 0, else host), bhs host.  Returns when the
+ * file is written. */
+bsn_status bsn_save_checkpoint_uniform(bsn_ctx* ctx, const char* path, const double* U, int on_device,
+                                       const bsn_bh* bhs, int nbh, const bsn_grid_meta* grid,
+                                       const bsn_ckpt_meta* meta);
+/* The same checkpoint without stopping the run: a device copy of U ordered on
+ * the context's stream (work enqueued after the call may change U), then a
+ * copy to pinned host memory on a copy stream and the file write on a host
+ * thread.  bsn_checkpoint_wait joins it and returns its status; a second
+ * asynchronous checkpoint on the context first waits for the previous one. */
+bsn_status bsn_save_checkpoint_uniform_async(bsn_ctx* ctx, const char* path, const double* U_dev,
+                                             const bsn_bh* bhs, int nbh, const bsn_grid_meta* grid,
+                                             const bsn_ckpt_meta* meta);
+bsn_status bsn_checkpoint_wait(bsn_ctx* ctx);
+/* load_checkpoint_uniform (src/checkpoint.jl:277-318).  With U = NULL only
+ * grid, meta and *nbh are read (to size the arrays); then U (device or host,
+ * 5 (nx+6)(ny+6)(nz+6) doubles) and bhs (room for cap_bh) are filled.  Rejects
+ * a checkpoint whose format_version is not 1 or whose kind is not "uniform". */
+bsn_status bsn_load_checkpoint_uniform(bsn_ctx* ctx, const char* path, double* U, int on_device, bsn_bh* bhs,
+                                       int cap_bh, int* nbh, bsn_grid_meta* grid, bsn_ckpt_meta* meta);
+/* save_checkpoint / load_checkpoint of a two-level FMR grid
+ * (src/checkpoint.jl:39-165): G's level arrays on the device (on_device != 0)
+ * or host.  load fills G's geometry, gamma, bc and floors from the file; with
+ * G->Uc / G->Uf non-NULL it also reads the level states into them (the fine
+ * level as saved, not re-prolonged). */
+bsn_status bsn_save_checkpoint_fmr(bsn_ctx* ctx, const char* path, const bsn_fmr2* G, int on_device,
+                                   const bsn_bh* bhs, int nbh, double t, long long step, double dt_last);
+bsn_status bsn_load_checkpoint_fmr(bsn_ctx* ctx, const char* path, bsn_fmr2* G, int on_device, bsn_bh* bhs,
+                                   int cap_bh, int* nbh, double* t, long long* step, double* dt_last);
+/* write_snapshot / read_snapshot (src/io.jl:29-83): /gas/{rho,rhovx,rhovy,
+ * rhovz,E} of the active cells and root attributes t, nx, ny, nz, dx, dy, dz,
+ * gamma.  read_snapshot fills U_active[q, i, j, k] (5 nx ny nz doubles, host;
+ * NULL to read the attributes only). */
+bsn_status bsn_write_snapshot(bsn_ctx* ctx, const char* path, const double* U, int on_device, int nx, int ny,
+                              int nz, double dx, double dy, double dz, double t, double gamma);
+bsn_status bsn_read_snapshot(const char* path, double* U_active, long long cap, int* nx, int* ny, int* nz,
+                             double* dx, double* dy, double* dz, double* t, double* gamma);
+/* init_trajectory_file / append_trajectory / read_trajectory (src/io.jl:96-
+ * 180): /time and /bh{i}/{mass, rsink, pos, vel}; the reference extends
+ * chunked datasets, here each append rewrites the file one record longer.
+ * read fills t[N], mass/rsink[b*N + r], pos/vel[(b*N + r)*3 + d] (room for
+ * cap dumps; t = NULL reads the counts only). */
+bsn_status bsn_trajectory_init(const char* path, int n_bh);
+bsn_status bsn_trajectory_append(const char* path, double t, const bsn_bh* bhs, int nbh);
+bsn_status bsn_trajectory_read(const char* path, int* n_dumps, int* n_bh, double* t, double* mass, double* pos,
+                               double* vel, double* rsink, long long cap);
 
 #ifdef __cplusplus
 }
