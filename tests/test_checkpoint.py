@@ -235,3 +235,91 @@ def test_trajectory_records(bsn, tmp_path):
     raw, root = walk(p)
     assert set(root[2]) == {"time", "bh1", "bh2"}
     assert root[2]["bh1"][2]["pos"][2] == [3, 3]        # Julia (N, 3)
+
+
+# ---- the reference's own checkpoint tests (test/test_checkpoint.jl), restated
+
+
+def _fmr_host(bsn, U_c, U_f):
+    """bsn_fmr2 over host arrays: 8^3 coarse, dx 1/8, refined box 4:5 in every
+    axis at ratio 4 (8^3 fine), gamma 5/3, outflow, floors 1e-12."""
+    from bsn._lib import bsn_fmr2
+    import ctypes as C
+    return bsn_fmr2(C.c_void_p(U_c.ctypes.data), 8, 8, 8, 1 / 8, 1 / 8, 1 / 8, C.c_void_p(U_f.ctypes.data), 8, 8, 8,
+                    1 / 32, 1 / 32, 1 / 32, 4, 4, 5, 4, 5, 4, 5, 5 / 3, 0, 1e-12, 1e-12)
+
+
+def test_reference_checkpoint_round_trip_fmr_grid_and_bhs(bsn, tmp_path):
+    """"Checkpoint round-trip: FMR grid + BHs" (test/test_checkpoint.jl:4-67)
+    and "Checkpoint with empty BH list" (:69-82): every field bit for bit,
+    the fine level as saved."""
+    import ctypes as C
+    g = 5 / 3
+    Uc = np.zeros((5, 14, 14, 14), order="F")
+    for k in range(NG, NG + 8):
+        for j in range(NG, NG + 8):
+            for i in range(NG, NG + 8):
+                xc, yc, zc = ((i - NG + 0.5) / 8 - 0.5, (j - NG + 0.5) / 8 - 0.5, (k - NG + 0.5) / 8 - 0.5)
+                Uc[0, i, j, k] = 1.0 + 0.1 * (xc * xc + yc * yc + zc * zc)
+                Uc[4, i, j, k] = 1.0 / (g - 1.0)
+    Uf = np.asfortranarray(np.random.default_rng(8).random((5, 14, 14, 14)) * 1.01)
+    G = _fmr_host(bsn, Uc, Uf)
+    bhs = [bsn.BlackHole((-0.5, 0.0, 0.0), (0.0, -0.5, 0.0), 0.5, 1e-3, 1431.6, 1e-3),
+           bsn.BlackHole((0.5, 0.1, 0.0), (0.0, 0.5, 0.0), 0.5, 1e-3, 1431.6, 1e-3)]
+    L = bsn._lib.load()
+    p = str(tmp_path / "ckpt.h5").encode()
+    assert L.bsn_save_checkpoint_fmr(None, p, C.byref(G), 0, bsn.api._bh_array(bhs), 2, 0.25, 42, 0.001) == 0
+    Vc, Vf = np.zeros_like(Uc, order="F"), np.zeros_like(Uf, order="F")
+    H = _fmr_host(bsn, Vc, Vf)
+    for f in ("ratio", "ci_lo", "gamma", "rho_floor", "ncx", "nfx", "dxc", "dxf"):
+        setattr(H, f, 0)
+    arr = (bsn._lib.bsn_bh * 2)()
+    nb, t, step, dtl = C.c_int(), C.c_double(), C.c_longlong(), C.c_double()
+    assert L.bsn_load_checkpoint_fmr(None, p, C.byref(H), 0, arr, 2, C.byref(nb), C.byref(t), C.byref(step),
+                                     C.byref(dtl)) == 0
+    assert (t.value, step.value, dtl.value, nb.value) == (0.25, 42, 0.001, 2)
+    for f, _ in G._fields_:
+        if f not in ("Uc", "Uf"):
+            assert getattr(H, f) == getattr(G, f), f
+    assert np.array_equal(Vc, Uc) and np.array_equal(Vf, Uf)
+    for b, b2 in zip(bhs, arr):
+        assert list(b2.pos) == list(b.pos) and list(b2.vel) == list(b.vel)
+        assert (b2.mass, b2.eps, b2.c_code, b2.r_floor) == (b.mass, b.eps, b.c_code, b.r_floor)
+    # empty BH list, default t / step
+    q = str(tmp_path / "ckpt_empty.h5").encode()
+    assert L.bsn_save_checkpoint_fmr(None, q, C.byref(G), 0, None, 0, 0.0, 0, 0.0) == 0
+    assert L.bsn_load_checkpoint_fmr(None, q, C.byref(H), 0, arr, 2, C.byref(nb), C.byref(t), C.byref(step),
+                                     C.byref(dtl)) == 0
+    assert (nb.value, t.value, step.value) == (0, 0.0, 0)
+    # the two checkpoint kinds are not cross-loadable (test/test_checkpoint.jl:139-140)
+    with pytest.raises(bsn.BSNError):
+        bsn.load_checkpoint_uniform(q.decode(), device="cpu")
+
+
+def test_reference_uniform_checkpoint_round_trip(bsn, tmp_path):
+    """"Uniform checkpoint round-trip: U + BHs + meta" (test/test_checkpoint.jl:86-141)."""
+    import ctypes as C
+    nx = ny = nz = 6
+    U = np.asfortranarray((0.5 + 1.0e-3 * np.arange(1, 5 * 12 ** 3 + 1)).reshape((5, 12, 12, 12), order="F"))
+    bhs = [bsn.BlackHole((-0.3, 0.0, 0.0), (0.0, -0.7, 0.0), 0.6, 2e-3, 1431.6, 2e-3),
+           bsn.BlackHole((0.3, 0.05, -0.1), (0.01, 0.7, 0.0), 0.4, 2e-3, 1431.6, 2e-3)]
+    p = tmp_path / "ckpt_uniform.h5"
+    bsn.save_checkpoint_uniform(p, U, bhs, t=7.5, step=12345, dt_last=2.5e-3, t_snap=8.0, t_bh2_sink_on=5.0,
+                                nx=nx, ny=ny, nz=nz, dx=0.2, dy=0.2, dz=0.2, gamma=4 / 3, x0=-1.0, y0=-1.0, z0=-1.0,
+                                rho_floor=3e-4, P_floor=1e-5)
+    U2, bhs2, grid, meta = bsn.load_checkpoint_uniform(p, device="cpu")
+    assert U2.shape == U.shape and np.array_equal(U2, U)
+    assert (meta["t"], meta["step"], meta["dt_last"], meta["t_snap"], meta["t_bh2_sink_on"]) == \
+        (7.5, 12345, 2.5e-3, 8.0, 5.0)
+    assert meta["format_version"] == 1
+    assert (grid["nx"], grid["ny"], grid["nz"], grid["dx"], grid["gamma"]) == (6, 6, 6, 0.2, 4 / 3)
+    assert (grid["x0"], grid["y0"], grid["z0"], grid["rho_floor"], grid["P_floor"]) == (-1.0, -1.0, -1.0, 3e-4, 1e-5)
+    for b, b2 in zip(bhs, bhs2):
+        assert list(b2.pos) == list(b.pos) and list(b2.vel) == list(b.vel)
+        assert (b2.mass, b2.eps, b2.c_code, b2.r_floor) == (b.mass, b.eps, b.c_code, b.r_floor)
+    # the FMR loader on a uniform file fails
+    L = bsn._lib.load()
+    H = _fmr_host(bsn, np.zeros((5, 14, 14, 14), order="F"), np.zeros((5, 14, 14, 14), order="F"))
+    nb, t, step, dtl = C.c_int(), C.c_double(), C.c_longlong(), C.c_double()
+    assert L.bsn_load_checkpoint_fmr(None, str(p).encode(), C.byref(H), 0, None, 0, C.byref(nb), C.byref(t),
+                                     C.byref(step), C.byref(dtl)) == 7
