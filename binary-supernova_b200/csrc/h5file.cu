@@ -249,7 +249,21 @@ void emit(const Group& g, const Plan& P, Buf& o) {
 
 }  // namespace
 
+namespace {
+bool names_fit(const Group& g) {
+    for (const Group& c : g.groups)
+        if (c.name.empty() || c.name.size() > 255 || !names_fit(c)) return false;
+    for (const Dataset& d : g.dsets)
+        if (d.name.empty() || d.name.size() > 255) return false;
+    return true;
+}
+}  // namespace
+
 bool write_file(const std::string& path, const Group& root, std::string* err) {
+    if (!names_fit(root)) {
+        if (err) *err = "group and dataset names must be 1..255 bytes";
+        return false;
+    }
     Plan P;
     assign(root, P);
     const uint64_t meta_end = P.next;
@@ -386,6 +400,10 @@ bool Reader::parse_object(uint64_t addr, RGroup* g, RDataset* d, bool* is_datase
     for (int i = 0; i < w; ++i) chunk |= (uint64_t)wb[i] << (8 * i);
     off += (uint64_t)w;
     const uint64_t hdr_len = off - addr;
+    if (chunk > eof_ || off + chunk + 4 > eof_) {
+        if (err) *err = "object header at " + std::to_string(addr) + " runs past the end of the file";
+        return false;
+    }
     std::vector<uint8_t> all(hdr_len + chunk + 4);
     if (!read_at(addr, all.data(), all.size())) { if (err) *err = "truncated object header"; return false; }
     uint32_t ck = 0;
@@ -433,8 +451,10 @@ bool Reader::parse_object(uint64_t addr, RGroup* g, RDataset* d, bool* is_datase
             if (!m.need(pad(nsz))) break;
             std::string name((const char*)m.p, nsz ? nsz - 1 : 0);
             m.p += pad(nsz);
+            if (!m.need(pad(tsz))) break;
             Cur t{m.p, m.p + tsz};
             m.skip(pad(tsz));
+            if (!m.need(pad(ssz))) break;
             Cur s{m.p, m.p + ssz};
             m.skip(pad(ssz));
             Kind k;

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
@@ -160,279 +161,327 @@ using namespace bsn;
 extern "C" bsn_status bsn_save_checkpoint_uniform(bsn_ctx* ctx, const char* path, const double* U, int on_device,
                                                   const bsn_bh* bhs, int nbh, const bsn_grid_meta* g,
                                                   const bsn_ckpt_meta* m) {
-    if (!path || !U || !g || !m || nbh < 0 || (nbh > 0 && !bhs) || !valid_grid(*g) || (on_device && !ctx))
-        return ctx ? set_err(ctx, BSN_ERR_ARG, "invalid checkpoint arguments") : BSN_ERR_ARG;
-    std::vector<double> tmp;
-    const double* h = nullptr;
-    BSN_TRY(fetch(ctx, U, on_device, state_elems(g->nx, g->ny, g->nz), tmp, &h));
-    std::string err;
-    if (!write_uniform(path, h, bhs, nbh, *g, *m, &err)) return io_err(ctx, err);
-    return BSN_OK;
+    try {
+        if (!path || !U || !g || !m || nbh < 0 || (nbh > 0 && !bhs) || !valid_grid(*g) || (on_device && !ctx))
+            return ctx ? set_err(ctx, BSN_ERR_ARG, "invalid checkpoint arguments") : BSN_ERR_ARG;
+        std::vector<double> tmp;
+        const double* h = nullptr;
+        BSN_TRY(fetch(ctx, U, on_device, state_elems(g->nx, g->ny, g->nz), tmp, &h));
+        std::string err;
+        if (!write_uniform(path, h, bhs, nbh, *g, *m, &err)) return io_err(ctx, err);
+        return BSN_OK;
+    } catch (const std::bad_alloc&) {
+        return ctx ? set_err(ctx, BSN_ERR_NOMEM, "host memory exhausted") : BSN_ERR_NOMEM;
+    } catch (...) {
+        return ctx ? set_err(ctx, BSN_ERR_IO, "unexpected error") : BSN_ERR_IO;
+    }
 }
 
 extern "C" bsn_status bsn_save_checkpoint_uniform_async(bsn_ctx* ctx, const char* path, const double* U,
                                                         const bsn_bh* bhs, int nbh, const bsn_grid_meta* g,
                                                         const bsn_ckpt_meta* m) {
-    if (!ctx) return BSN_ERR_ARG;
-    if (!path || !U || !g || !m || nbh < 0 || (nbh > 0 && !bhs) || !valid_grid(*g))
-        return set_err(ctx, BSN_ERR_ARG, "invalid checkpoint arguments");
-    BSN_TRY(bsn_checkpoint_wait(ctx));   // one checkpoint in flight per context
-    CkptState* S = ckpt(ctx);
-    const size_t bytes = sizeof(double) * (size_t)state_elems(g->nx, g->ny, g->nz);
-    if (S->bytes < bytes) {
-        if (S->snap) cudaFree(S->snap);
-        if (S->host) cudaFreeHost(S->host);
-        S->snap = nullptr; S->host = nullptr; S->bytes = 0;
-        BSN_CUDA(ctx, cudaMalloc(&S->snap, bytes));
-        BSN_CUDA(ctx, cudaMallocHost(&S->host, bytes));
-        S->bytes = bytes;
-    }
-    if (!S->copy) {
-        BSN_CUDA(ctx, cudaStreamCreateWithFlags(&S->copy, cudaStreamNonBlocking));
-        BSN_CUDA(ctx, cudaEventCreateWithFlags(&S->snapped, cudaEventDisableTiming));
-        BSN_CUDA(ctx, cudaEventCreateWithFlags(&S->copied, cudaEventDisableTiming));
-    }
-    // the snapshot is ordered on the caller's stream: later work there may change U at once
-    BSN_CUDA(ctx, cudaMemcpyAsync(S->snap, U, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-    BSN_CUDA(ctx, cudaEventRecord(S->snapped, ctx->stream));
-    BSN_CUDA(ctx, cudaStreamWaitEvent(S->copy, S->snapped, 0));
-    BSN_CUDA(ctx, cudaMemcpyAsync(S->host, S->snap, bytes, cudaMemcpyDeviceToHost, S->copy));
-    BSN_CUDA(ctx, cudaEventRecord(S->copied, S->copy));
-    std::vector<bsn_bh> b(bhs, bhs + nbh);
-    const bsn_grid_meta gm = *g;
-    const bsn_ckpt_meta mm = *m;
-    const std::string p = path;
-    S->device = ctx->device;
-    S->active = true;
-    S->result = BSN_OK;
-    S->err.clear();
-    S->th = std::thread([S, b, gm, mm, p]() {
-        cudaSetDevice(S->device);
-        if (cudaEventSynchronize(S->copied) != cudaSuccess) {
-            S->result = BSN_ERR_CUDA;
-            S->err = "checkpoint copy failed";
-            return;
+    try {
+        if (!ctx) return BSN_ERR_ARG;
+        if (!path || !U || !g || !m || nbh < 0 || (nbh > 0 && !bhs) || !valid_grid(*g))
+            return set_err(ctx, BSN_ERR_ARG, "invalid checkpoint arguments");
+        BSN_TRY(bsn_checkpoint_wait(ctx));   // one checkpoint in flight per context
+        CkptState* S = ckpt(ctx);
+        const size_t bytes = sizeof(double) * (size_t)state_elems(g->nx, g->ny, g->nz);
+        if (S->bytes < bytes) {
+            if (S->snap) cudaFree(S->snap);
+            if (S->host) cudaFreeHost(S->host);
+            S->snap = nullptr; S->host = nullptr; S->bytes = 0;
+            BSN_CUDA(ctx, cudaMalloc(&S->snap, bytes));
+            BSN_CUDA(ctx, cudaMallocHost(&S->host, bytes));
+            S->bytes = bytes;
         }
-        std::string err;
-        if (!write_uniform(p, S->host, b.data(), (int)b.size(), gm, mm, &err)) {
-            S->result = BSN_ERR_IO;
-            S->err = err;
+        if (!S->copy) {
+            BSN_CUDA(ctx, cudaStreamCreateWithFlags(&S->copy, cudaStreamNonBlocking));
+            BSN_CUDA(ctx, cudaEventCreateWithFlags(&S->snapped, cudaEventDisableTiming));
+            BSN_CUDA(ctx, cudaEventCreateWithFlags(&S->copied, cudaEventDisableTiming));
         }
-    });
-    return BSN_OK;
+        // the snapshot is ordered on the caller's stream: later work there may change U at once
+        BSN_CUDA(ctx, cudaMemcpyAsync(S->snap, U, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        BSN_CUDA(ctx, cudaEventRecord(S->snapped, ctx->stream));
+        BSN_CUDA(ctx, cudaStreamWaitEvent(S->copy, S->snapped, 0));
+        BSN_CUDA(ctx, cudaMemcpyAsync(S->host, S->snap, bytes, cudaMemcpyDeviceToHost, S->copy));
+        BSN_CUDA(ctx, cudaEventRecord(S->copied, S->copy));
+        std::vector<bsn_bh> b(bhs, bhs + nbh);
+        const bsn_grid_meta gm = *g;
+        const bsn_ckpt_meta mm = *m;
+        const std::string p = path;
+        S->device = ctx->device;
+        S->active = true;
+        S->result = BSN_OK;
+        S->err.clear();
+        S->th = std::thread([S, b, gm, mm, p]() {
+            cudaSetDevice(S->device);
+            if (cudaEventSynchronize(S->copied) != cudaSuccess) {
+                S->result = BSN_ERR_CUDA;
+                S->err = "checkpoint copy failed";
+                return;
+            }
+            std::string err;
+            if (!write_uniform(p, S->host, b.data(), (int)b.size(), gm, mm, &err)) {
+                S->result = BSN_ERR_IO;
+                S->err = err;
+            }
+        });
+        return BSN_OK;
+    } catch (const std::bad_alloc&) {
+        return ctx ? set_err(ctx, BSN_ERR_NOMEM, "host memory exhausted") : BSN_ERR_NOMEM;
+    } catch (...) {
+        return ctx ? set_err(ctx, BSN_ERR_IO, "unexpected error") : BSN_ERR_IO;
+    }
 }
 
 extern "C" bsn_status bsn_checkpoint_wait(bsn_ctx* ctx) {
-    if (!ctx) return BSN_ERR_ARG;
-    if (!ctx->ckpt_state) return BSN_OK;
-    CkptState* S = (CkptState*)ctx->ckpt_state;
-    if (!S->active) return BSN_OK;
-    if (S->th.joinable()) S->th.join();
-    S->active = false;
-    if (S->result != BSN_OK) return set_err(ctx, S->result, "asynchronous checkpoint: %s", S->err.c_str());
-    return BSN_OK;
+    try {
+        if (!ctx) return BSN_ERR_ARG;
+        if (!ctx->ckpt_state) return BSN_OK;
+        CkptState* S = (CkptState*)ctx->ckpt_state;
+        if (!S->active) return BSN_OK;
+        if (S->th.joinable()) S->th.join();
+        S->active = false;
+        if (S->result != BSN_OK) return set_err(ctx, S->result, "asynchronous checkpoint: %s", S->err.c_str());
+        return BSN_OK;
+    } catch (const std::bad_alloc&) {
+        return ctx ? set_err(ctx, BSN_ERR_NOMEM, "host memory exhausted") : BSN_ERR_NOMEM;
+    } catch (...) {
+        return ctx ? set_err(ctx, BSN_ERR_IO, "unexpected error") : BSN_ERR_IO;
+    }
 }
 
 extern "C" bsn_status bsn_load_checkpoint_uniform(bsn_ctx* ctx, const char* path, double* U, int on_device,
                                                   bsn_bh* bhs, int cap_bh, int* nbh, bsn_grid_meta* g,
                                                   bsn_ckpt_meta* m) {
-    if (!path || !nbh || !g || !m || (U && on_device && !ctx)) return ctx ? set_err(ctx, BSN_ERR_ARG, "null argument") : BSN_ERR_ARG;
-    h5::Reader R;
-    std::string err;
-    if (!R.open(path, &err)) return io_err(ctx, err);
-    const h5::RGroup* man = R.group("manifest");
-    const h5::RGroup* gr = R.group("grid");
-    int64_t fv = 0, step = 0, nx = 0, ny = 0, nz = 0;
-    std::string kind;
-    if (!man || !gr || !h5::get_i64(man->attrs, "format_version", &fv))
-        return io_err(ctx, std::string(path) + ": no checkpoint manifest");
-    if (fv != FORMAT_VERSION) return io_err(ctx, "checkpoint format_version " + std::to_string(fv) + ", expected 1");
-    if (!h5::get_str(man->attrs, "kind", &kind) || kind != "uniform")
-        return io_err(ctx, std::string(path) + " is not a uniform-grid checkpoint (kind != \"uniform\")");
-    bool ok = h5::get_f64(man->attrs, "t", &m->t) && h5::get_i64(man->attrs, "step", &step) &&
-              h5::get_f64(man->attrs, "dt_last", &m->dt_last) && h5::get_f64(man->attrs, "t_snap", &m->t_snap) &&
-              h5::get_f64(man->attrs, "t_bh2_sink_on", &m->t_bh2_sink_on) &&
-              h5::get_i64(gr->attrs, "nx", &nx) && h5::get_i64(gr->attrs, "ny", &ny) && h5::get_i64(gr->attrs, "nz", &nz) &&
-              h5::get_f64(gr->attrs, "dx", &g->dx) && h5::get_f64(gr->attrs, "dy", &g->dy) &&
-              h5::get_f64(gr->attrs, "dz", &g->dz) && h5::get_f64(gr->attrs, "gamma", &g->gamma) &&
-              h5::get_f64(gr->attrs, "x0", &g->x0) && h5::get_f64(gr->attrs, "y0", &g->y0) &&
-              h5::get_f64(gr->attrs, "z0", &g->z0) && h5::get_f64(gr->attrs, "rho_floor", &g->rho_floor) &&
-              h5::get_f64(gr->attrs, "P_floor", &g->P_floor);
-    if (!ok) return io_err(ctx, std::string(path) + ": checkpoint attributes missing");
-    m->step = step;
-    g->nx = (int)nx; g->ny = (int)ny; g->nz = (int)nz;
-    if (!read_bhs(R, bhs, cap_bh, nbh, &err)) return io_err(ctx, err);
-    if (!U) return BSN_OK;
-    const h5::RDataset* d = R.dataset("grid/U");
-    if (!d || d->kind != h5::F64 || d->dims != state_dims(g->nx, g->ny, g->nz))
-        return io_err(ctx, std::string(path) + ": /grid/U does not match the grid");
-    const size_t bytes = sizeof(double) * (size_t)state_elems(g->nx, g->ny, g->nz);
-    if (!on_device) return R.read_data(*d, U, bytes, &err) ? BSN_OK : io_err(ctx, err);
-    std::vector<double> h(bytes / 8);
-    if (!R.read_data(*d, h.data(), bytes, &err)) return io_err(ctx, err);
-    BSN_CUDA(ctx, cudaMemcpyAsync(U, h.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
-    BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return BSN_OK;
+    try {
+        if (!path || !nbh || !g || !m || (U && on_device && !ctx)) return ctx ? set_err(ctx, BSN_ERR_ARG, "null argument") : BSN_ERR_ARG;
+        h5::Reader R;
+        std::string err;
+        if (!R.open(path, &err)) return io_err(ctx, err);
+        const h5::RGroup* man = R.group("manifest");
+        const h5::RGroup* gr = R.group("grid");
+        int64_t fv = 0, step = 0, nx = 0, ny = 0, nz = 0;
+        std::string kind;
+        if (!man || !gr || !h5::get_i64(man->attrs, "format_version", &fv))
+            return io_err(ctx, std::string(path) + ": no checkpoint manifest");
+        if (fv != FORMAT_VERSION) return io_err(ctx, "checkpoint format_version " + std::to_string(fv) + ", expected 1");
+        if (!h5::get_str(man->attrs, "kind", &kind) || kind != "uniform")
+            return io_err(ctx, std::string(path) + " is not a uniform-grid checkpoint (kind != \"uniform\")");
+        bool ok = h5::get_f64(man->attrs, "t", &m->t) && h5::get_i64(man->attrs, "step", &step) &&
+                  h5::get_f64(man->attrs, "dt_last", &m->dt_last) && h5::get_f64(man->attrs, "t_snap", &m->t_snap) &&
+                  h5::get_f64(man->attrs, "t_bh2_sink_on", &m->t_bh2_sink_on) &&
+                  h5::get_i64(gr->attrs, "nx", &nx) && h5::get_i64(gr->attrs, "ny", &ny) && h5::get_i64(gr->attrs, "nz", &nz) &&
+                  h5::get_f64(gr->attrs, "dx", &g->dx) && h5::get_f64(gr->attrs, "dy", &g->dy) &&
+                  h5::get_f64(gr->attrs, "dz", &g->dz) && h5::get_f64(gr->attrs, "gamma", &g->gamma) &&
+                  h5::get_f64(gr->attrs, "x0", &g->x0) && h5::get_f64(gr->attrs, "y0", &g->y0) &&
+                  h5::get_f64(gr->attrs, "z0", &g->z0) && h5::get_f64(gr->attrs, "rho_floor", &g->rho_floor) &&
+                  h5::get_f64(gr->attrs, "P_floor", &g->P_floor);
+        if (!ok) return io_err(ctx, std::string(path) + ": checkpoint attributes missing");
+        m->step = step;
+        g->nx = (int)nx; g->ny = (int)ny; g->nz = (int)nz;
+        if (!read_bhs(R, bhs, cap_bh, nbh, &err)) return io_err(ctx, err);
+        if (!U) return BSN_OK;
+        const h5::RDataset* d = R.dataset("grid/U");
+        if (!d || d->kind != h5::F64 || d->dims != state_dims(g->nx, g->ny, g->nz))
+            return io_err(ctx, std::string(path) + ": /grid/U does not match the grid");
+        const size_t bytes = sizeof(double) * (size_t)state_elems(g->nx, g->ny, g->nz);
+        if (!on_device) return R.read_data(*d, U, bytes, &err) ? BSN_OK : io_err(ctx, err);
+        std::vector<double> h(bytes / 8);
+        if (!R.read_data(*d, h.data(), bytes, &err)) return io_err(ctx, err);
+        BSN_CUDA(ctx, cudaMemcpyAsync(U, h.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+        BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        return BSN_OK;
+    } catch (const std::bad_alloc&) {
+        return ctx ? set_err(ctx, BSN_ERR_NOMEM, "host memory exhausted") : BSN_ERR_NOMEM;
+    } catch (...) {
+        return ctx ? set_err(ctx, BSN_ERR_IO, "unexpected error") : BSN_ERR_IO;
+    }
 }
 
 // ---- two-level FMR checkpoint (src/checkpoint.jl:39-119) ---------------------
 
 extern "C" bsn_status bsn_save_checkpoint_fmr(bsn_ctx* ctx, const char* path, const bsn_fmr2* G, int on_device,
                                               const bsn_bh* bhs, int nbh, double t, long long step, double dt_last) {
-    if (!path || !G || !G->Uc || !G->Uf || nbh < 0 || (nbh > 0 && !bhs) || (on_device && !ctx))
-        return ctx ? set_err(ctx, BSN_ERR_ARG, "invalid checkpoint arguments") : BSN_ERR_ARG;
-    std::vector<double> tc, tf;
-    const double *hc = nullptr, *hf = nullptr;
-    BSN_TRY(fetch(ctx, G->Uc, on_device, state_elems(G->ncx, G->ncy, G->ncz), tc, &hc));
-    BSN_TRY(fetch(ctx, G->Uf, on_device, state_elems(G->nfx, G->nfy, G->nfz), tf, &hf));
-    h5::Group root, man, grid;
-    man.name = "manifest";
-    man.attrs = {h5::attr_i64("format_version", FORMAT_VERSION), h5::attr_f64("t", t), h5::attr_i64("step", step),
-                 h5::attr_f64("dt_last", dt_last)};
-    grid.name = "grid";
-    grid.attrs = {h5::attr_i64("ratio", G->ratio), h5::attr_f64("gamma", G->gamma),
-                  h5::attr_str("bc", G->bc == BSN_BC_PERIODIC ? "periodic" : "outflow"),
-                  h5::attr_f64("rho_floor", G->rho_floor), h5::attr_f64("P_floor", G->P_floor),
-                  h5::attr_i64("ci_lo", G->ci_lo), h5::attr_i64("ci_hi", G->ci_hi),
-                  h5::attr_i64("cj_lo", G->cj_lo), h5::attr_i64("cj_hi", G->cj_hi),
-                  h5::attr_i64("ck_lo", G->ck_lo), h5::attr_i64("ck_hi", G->ck_hi)};
-    auto level = [](const char* name, int nx, int ny, int nz, double dx, double dy, double dz, const double* U) {
-        h5::Group l;
-        l.name = name;
-        l.attrs = {h5::attr_i64("nx", nx), h5::attr_i64("ny", ny), h5::attr_i64("nz", nz), h5::attr_f64("dx", dx),
-                   h5::attr_f64("dy", dy), h5::attr_f64("dz", dz)};
-        h5::Dataset u;
-        u.name = "U"; u.kind = h5::F64; u.dims = state_dims(nx, ny, nz); u.data = U;
-        l.dsets.push_back(u);
-        return l;
-    };
-    grid.groups = {level("coarse", G->ncx, G->ncy, G->ncz, G->dxc, G->dyc, G->dzc, hc),
-                   level("fine", G->nfx, G->nfy, G->nfz, G->dxf, G->dyf, G->dzf, hf)};
-    BHArrays A;
-    root.groups = {man, grid, bh_group(bhs, nbh, A)};
-    std::string err;
-    if (!h5::write_file(path, root, &err)) return io_err(ctx, err);
-    return BSN_OK;
+    try {
+        if (!path || !G || !G->Uc || !G->Uf || nbh < 0 || (nbh > 0 && !bhs) || (on_device && !ctx))
+            return ctx ? set_err(ctx, BSN_ERR_ARG, "invalid checkpoint arguments") : BSN_ERR_ARG;
+        std::vector<double> tc, tf;
+        const double *hc = nullptr, *hf = nullptr;
+        BSN_TRY(fetch(ctx, G->Uc, on_device, state_elems(G->ncx, G->ncy, G->ncz), tc, &hc));
+        BSN_TRY(fetch(ctx, G->Uf, on_device, state_elems(G->nfx, G->nfy, G->nfz), tf, &hf));
+        h5::Group root, man, grid;
+        man.name = "manifest";
+        man.attrs = {h5::attr_i64("format_version", FORMAT_VERSION), h5::attr_f64("t", t), h5::attr_i64("step", step),
+                     h5::attr_f64("dt_last", dt_last)};
+        grid.name = "grid";
+        grid.attrs = {h5::attr_i64("ratio", G->ratio), h5::attr_f64("gamma", G->gamma),
+                      h5::attr_str("bc", G->bc == BSN_BC_PERIODIC ? "periodic" : "outflow"),
+                      h5::attr_f64("rho_floor", G->rho_floor), h5::attr_f64("P_floor", G->P_floor),
+                      h5::attr_i64("ci_lo", G->ci_lo), h5::attr_i64("ci_hi", G->ci_hi),
+                      h5::attr_i64("cj_lo", G->cj_lo), h5::attr_i64("cj_hi", G->cj_hi),
+                      h5::attr_i64("ck_lo", G->ck_lo), h5::attr_i64("ck_hi", G->ck_hi)};
+        auto level = [](const char* name, int nx, int ny, int nz, double dx, double dy, double dz, const double* U) {
+            h5::Group l;
+            l.name = name;
+            l.attrs = {h5::attr_i64("nx", nx), h5::attr_i64("ny", ny), h5::attr_i64("nz", nz), h5::attr_f64("dx", dx),
+                       h5::attr_f64("dy", dy), h5::attr_f64("dz", dz)};
+            h5::Dataset u;
+            u.name = "U"; u.kind = h5::F64; u.dims = state_dims(nx, ny, nz); u.data = U;
+            l.dsets.push_back(u);
+            return l;
+        };
+        grid.groups = {level("coarse", G->ncx, G->ncy, G->ncz, G->dxc, G->dyc, G->dzc, hc),
+                       level("fine", G->nfx, G->nfy, G->nfz, G->dxf, G->dyf, G->dzf, hf)};
+        BHArrays A;
+        root.groups = {man, grid, bh_group(bhs, nbh, A)};
+        std::string err;
+        if (!h5::write_file(path, root, &err)) return io_err(ctx, err);
+        return BSN_OK;
+    } catch (const std::bad_alloc&) {
+        return ctx ? set_err(ctx, BSN_ERR_NOMEM, "host memory exhausted") : BSN_ERR_NOMEM;
+    } catch (...) {
+        return ctx ? set_err(ctx, BSN_ERR_IO, "unexpected error") : BSN_ERR_IO;
+    }
 }
 
 extern "C" bsn_status bsn_load_checkpoint_fmr(bsn_ctx* ctx, const char* path, bsn_fmr2* G, int on_device,
                                               bsn_bh* bhs, int cap_bh, int* nbh, double* t, long long* step,
                                               double* dt_last) {
-    if (!path || !G || !nbh || !t || !step || !dt_last || (on_device && (G->Uc || G->Uf) && !ctx))
-        return ctx ? set_err(ctx, BSN_ERR_ARG, "null argument") : BSN_ERR_ARG;
-    h5::Reader R;
-    std::string err;
-    if (!R.open(path, &err)) return io_err(ctx, err);
-    const h5::RGroup *man = R.group("manifest"), *gr = R.group("grid");
-    const h5::RGroup *co = R.group("grid/coarse"), *fi = R.group("grid/fine");
-    int64_t fv = 0, st = 0, v[7];
-    std::string bc;
-    if (!man || !gr || !co || !fi || !h5::get_i64(man->attrs, "format_version", &fv))
-        return io_err(ctx, std::string(path) + ": no FMR checkpoint manifest");
-    if (fv != FORMAT_VERSION) return io_err(ctx, "checkpoint format_version " + std::to_string(fv) + ", expected 1");
-    const char* keys[7] = {"ratio", "ci_lo", "ci_hi", "cj_lo", "cj_hi", "ck_lo", "ck_hi"};
-    bool ok = h5::get_f64(man->attrs, "t", t) && h5::get_i64(man->attrs, "step", &st) &&
-              h5::get_f64(man->attrs, "dt_last", dt_last) && h5::get_f64(gr->attrs, "gamma", &G->gamma) &&
-              h5::get_str(gr->attrs, "bc", &bc) && h5::get_f64(gr->attrs, "rho_floor", &G->rho_floor) &&
-              h5::get_f64(gr->attrs, "P_floor", &G->P_floor);
-    for (int i = 0; i < 7; ++i) ok = ok && h5::get_i64(gr->attrs, keys[i], &v[i]);
-    int64_t c3[3], f3[3];
-    ok = ok && h5::get_i64(co->attrs, "nx", &c3[0]) && h5::get_i64(co->attrs, "ny", &c3[1]) &&
-         h5::get_i64(co->attrs, "nz", &c3[2]) && h5::get_i64(fi->attrs, "nx", &f3[0]) &&
-         h5::get_i64(fi->attrs, "ny", &f3[1]) && h5::get_i64(fi->attrs, "nz", &f3[2]) &&
-         h5::get_f64(co->attrs, "dx", &G->dxc) && h5::get_f64(co->attrs, "dy", &G->dyc) &&
-         h5::get_f64(co->attrs, "dz", &G->dzc) && h5::get_f64(fi->attrs, "dx", &G->dxf) &&
-         h5::get_f64(fi->attrs, "dy", &G->dyf) && h5::get_f64(fi->attrs, "dz", &G->dzf);
-    if (!ok) return io_err(ctx, std::string(path) + ": checkpoint attributes missing");
-    *step = st;
-    G->ratio = (int)v[0]; G->ci_lo = (int)v[1]; G->ci_hi = (int)v[2]; G->cj_lo = (int)v[3]; G->cj_hi = (int)v[4];
-    G->ck_lo = (int)v[5]; G->ck_hi = (int)v[6];
-    G->bc = bc == "periodic" ? BSN_BC_PERIODIC : BSN_BC_OUTFLOW;
-    G->ncx = (int)c3[0]; G->ncy = (int)c3[1]; G->ncz = (int)c3[2];
-    G->nfx = (int)f3[0]; G->nfy = (int)f3[1]; G->nfz = (int)f3[2];
-    if (!read_bhs(R, bhs, cap_bh, nbh, &err)) return io_err(ctx, err);
-    struct { const char* p; double* U; int nx, ny, nz; } lv[2] = {{"grid/coarse/U", G->Uc, G->ncx, G->ncy, G->ncz},
-                                                                 {"grid/fine/U", G->Uf, G->nfx, G->nfy, G->nfz}};
-    for (auto& l : lv) {
-        if (!l.U) continue;
-        const h5::RDataset* d = R.dataset(l.p);
-        if (!d || d->kind != h5::F64 || d->dims != state_dims(l.nx, l.ny, l.nz))
-            return io_err(ctx, std::string(path) + ": /" + l.p + " does not match its level");
-        const size_t bytes = sizeof(double) * (size_t)state_elems(l.nx, l.ny, l.nz);
-        if (!on_device) {
-            if (!R.read_data(*d, l.U, bytes, &err)) return io_err(ctx, err);
-            continue;
+    try {
+        if (!path || !G || !nbh || !t || !step || !dt_last || (on_device && (G->Uc || G->Uf) && !ctx))
+            return ctx ? set_err(ctx, BSN_ERR_ARG, "null argument") : BSN_ERR_ARG;
+        h5::Reader R;
+        std::string err;
+        if (!R.open(path, &err)) return io_err(ctx, err);
+        const h5::RGroup *man = R.group("manifest"), *gr = R.group("grid");
+        const h5::RGroup *co = R.group("grid/coarse"), *fi = R.group("grid/fine");
+        int64_t fv = 0, st = 0, v[7];
+        std::string bc;
+        if (!man || !gr || !co || !fi || !h5::get_i64(man->attrs, "format_version", &fv))
+            return io_err(ctx, std::string(path) + ": no FMR checkpoint manifest");
+        if (fv != FORMAT_VERSION) return io_err(ctx, "checkpoint format_version " + std::to_string(fv) + ", expected 1");
+        const char* keys[7] = {"ratio", "ci_lo", "ci_hi", "cj_lo", "cj_hi", "ck_lo", "ck_hi"};
+        bool ok = h5::get_f64(man->attrs, "t", t) && h5::get_i64(man->attrs, "step", &st) &&
+                  h5::get_f64(man->attrs, "dt_last", dt_last) && h5::get_f64(gr->attrs, "gamma", &G->gamma) &&
+                  h5::get_str(gr->attrs, "bc", &bc) && h5::get_f64(gr->attrs, "rho_floor", &G->rho_floor) &&
+                  h5::get_f64(gr->attrs, "P_floor", &G->P_floor);
+        for (int i = 0; i < 7; ++i) ok = ok && h5::get_i64(gr->attrs, keys[i], &v[i]);
+        int64_t c3[3], f3[3];
+        ok = ok && h5::get_i64(co->attrs, "nx", &c3[0]) && h5::get_i64(co->attrs, "ny", &c3[1]) &&
+             h5::get_i64(co->attrs, "nz", &c3[2]) && h5::get_i64(fi->attrs, "nx", &f3[0]) &&
+             h5::get_i64(fi->attrs, "ny", &f3[1]) && h5::get_i64(fi->attrs, "nz", &f3[2]) &&
+             h5::get_f64(co->attrs, "dx", &G->dxc) && h5::get_f64(co->attrs, "dy", &G->dyc) &&
+             h5::get_f64(co->attrs, "dz", &G->dzc) && h5::get_f64(fi->attrs, "dx", &G->dxf) &&
+             h5::get_f64(fi->attrs, "dy", &G->dyf) && h5::get_f64(fi->attrs, "dz", &G->dzf);
+        if (!ok) return io_err(ctx, std::string(path) + ": checkpoint attributes missing");
+        *step = st;
+        G->ratio = (int)v[0]; G->ci_lo = (int)v[1]; G->ci_hi = (int)v[2]; G->cj_lo = (int)v[3]; G->cj_hi = (int)v[4];
+        G->ck_lo = (int)v[5]; G->ck_hi = (int)v[6];
+        G->bc = bc == "periodic" ? BSN_BC_PERIODIC : BSN_BC_OUTFLOW;
+        G->ncx = (int)c3[0]; G->ncy = (int)c3[1]; G->ncz = (int)c3[2];
+        G->nfx = (int)f3[0]; G->nfy = (int)f3[1]; G->nfz = (int)f3[2];
+        if (!read_bhs(R, bhs, cap_bh, nbh, &err)) return io_err(ctx, err);
+        struct { const char* p; double* U; int nx, ny, nz; } lv[2] = {{"grid/coarse/U", G->Uc, G->ncx, G->ncy, G->ncz},
+                                                                     {"grid/fine/U", G->Uf, G->nfx, G->nfy, G->nfz}};
+        for (auto& l : lv) {
+            if (!l.U) continue;
+            const h5::RDataset* d = R.dataset(l.p);
+            if (!d || d->kind != h5::F64 || d->dims != state_dims(l.nx, l.ny, l.nz))
+                return io_err(ctx, std::string(path) + ": /" + l.p + " does not match its level");
+            const size_t bytes = sizeof(double) * (size_t)state_elems(l.nx, l.ny, l.nz);
+            if (!on_device) {
+                if (!R.read_data(*d, l.U, bytes, &err)) return io_err(ctx, err);
+                continue;
+            }
+            std::vector<double> h(bytes / 8);
+            if (!R.read_data(*d, h.data(), bytes, &err)) return io_err(ctx, err);
+            BSN_CUDA(ctx, cudaMemcpyAsync(l.U, h.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+            BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         }
-        std::vector<double> h(bytes / 8);
-        if (!R.read_data(*d, h.data(), bytes, &err)) return io_err(ctx, err);
-        BSN_CUDA(ctx, cudaMemcpyAsync(l.U, h.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
-        BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        return BSN_OK;
+    } catch (const std::bad_alloc&) {
+        return ctx ? set_err(ctx, BSN_ERR_NOMEM, "host memory exhausted") : BSN_ERR_NOMEM;
+    } catch (...) {
+        return ctx ? set_err(ctx, BSN_ERR_IO, "unexpected error") : BSN_ERR_IO;
     }
-    return BSN_OK;
 }
 
 // ---- snapshots (src/io.jl:29-83) ----------------------------------------------
 
 extern "C" bsn_status bsn_write_snapshot(bsn_ctx* ctx, const char* path, const double* U, int on_device, int nx,
                                          int ny, int nz, double dx, double dy, double dz, double t, double gamma) {
-    if (!path || !U || nx < 1 || ny < 1 || nz < 1 || (on_device && !ctx))
-        return ctx ? set_err(ctx, BSN_ERR_ARG, "invalid snapshot arguments") : BSN_ERR_ARG;
-    std::vector<double> tmp;
-    const double* h = nullptr;
-    BSN_TRY(fetch(ctx, U, on_device, state_elems(nx, ny, nz), tmp, &h));
-    // the five active-cell fields, each (nx, ny, nz) column-major
-    const size_t nc = (size_t)nx * ny * nz;
-    std::vector<double> F(5 * nc);
-    const long long X = nx + 2 * BSN_NG, Y = ny + 2 * BSN_NG;
-    for (int k = 0; k < nz; ++k)
-        for (int j = 0; j < ny; ++j)
-            for (int i = 0; i < nx; ++i) {
-                const double* c = h + 5 * ((i + BSN_NG) + X * ((j + BSN_NG) + Y * (long long)(k + BSN_NG)));
-                const size_t o = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k);
-                for (int q = 0; q < 5; ++q) F[q * nc + o] = c[q];
-            }
-    h5::Group root, gas;
-    gas.name = "gas";
-    const char* names[5] = {"rho", "rhovx", "rhovy", "rhovz", "E"};
-    for (int q = 0; q < 5; ++q) {
-        h5::Dataset d;
-        d.name = names[q]; d.kind = h5::F64; d.dims = {(uint64_t)nz, (uint64_t)ny, (uint64_t)nx};
-        d.data = F.data() + q * nc;
-        gas.dsets.push_back(d);
+    try {
+        if (!path || !U || nx < 1 || ny < 1 || nz < 1 || (on_device && !ctx))
+            return ctx ? set_err(ctx, BSN_ERR_ARG, "invalid snapshot arguments") : BSN_ERR_ARG;
+        std::vector<double> tmp;
+        const double* h = nullptr;
+        BSN_TRY(fetch(ctx, U, on_device, state_elems(nx, ny, nz), tmp, &h));
+        // the five active-cell fields, each (nx, ny, nz) column-major
+        const size_t nc = (size_t)nx * ny * nz;
+        std::vector<double> F(5 * nc);
+        const long long X = nx + 2 * BSN_NG, Y = ny + 2 * BSN_NG;
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const double* c = h + 5 * ((i + BSN_NG) + X * ((j + BSN_NG) + Y * (long long)(k + BSN_NG)));
+                    const size_t o = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k);
+                    for (int q = 0; q < 5; ++q) F[q * nc + o] = c[q];
+                }
+        h5::Group root, gas;
+        gas.name = "gas";
+        const char* names[5] = {"rho", "rhovx", "rhovy", "rhovz", "E"};
+        for (int q = 0; q < 5; ++q) {
+            h5::Dataset d;
+            d.name = names[q]; d.kind = h5::F64; d.dims = {(uint64_t)nz, (uint64_t)ny, (uint64_t)nx};
+            d.data = F.data() + q * nc;
+            gas.dsets.push_back(d);
+        }
+        root.groups = {gas};
+        root.attrs = {h5::attr_f64("t", t), h5::attr_i64("nx", nx), h5::attr_i64("ny", ny), h5::attr_i64("nz", nz),
+                      h5::attr_f64("dx", dx), h5::attr_f64("dy", dy), h5::attr_f64("dz", dz),
+                      h5::attr_f64("gamma", gamma)};
+        std::string err;
+        if (!h5::write_file(path, root, &err)) return io_err(ctx, err);
+        return BSN_OK;
+    } catch (const std::bad_alloc&) {
+        return ctx ? set_err(ctx, BSN_ERR_NOMEM, "host memory exhausted") : BSN_ERR_NOMEM;
+    } catch (...) {
+        return ctx ? set_err(ctx, BSN_ERR_IO, "unexpected error") : BSN_ERR_IO;
     }
-    root.groups = {gas};
-    root.attrs = {h5::attr_f64("t", t), h5::attr_i64("nx", nx), h5::attr_i64("ny", ny), h5::attr_i64("nz", nz),
-                  h5::attr_f64("dx", dx), h5::attr_f64("dy", dy), h5::attr_f64("dz", dz),
-                  h5::attr_f64("gamma", gamma)};
-    std::string err;
-    if (!h5::write_file(path, root, &err)) return io_err(ctx, err);
-    return BSN_OK;
 }
 
 extern "C" bsn_status bsn_read_snapshot(const char* path, double* U_active, long long cap, int* nx, int* ny, int* nz,
                                         double* dx, double* dy, double* dz, double* t, double* gamma) {
-    if (!path || !nx || !ny || !nz || !dx || !dy || !dz || !t || !gamma) return BSN_ERR_ARG;
-    h5::Reader R;
-    std::string err;
-    if (!R.open(path, &err)) return BSN_ERR_IO;
-    const auto& a = R.root().attrs;
-    int64_t n3[3];
-    if (!h5::get_i64(a, "nx", &n3[0]) || !h5::get_i64(a, "ny", &n3[1]) || !h5::get_i64(a, "nz", &n3[2]) ||
-        !h5::get_f64(a, "dx", dx) || !h5::get_f64(a, "dy", dy) || !h5::get_f64(a, "dz", dz) ||
-        !h5::get_f64(a, "t", t) || !h5::get_f64(a, "gamma", gamma))
+    try {
+        if (!path || !nx || !ny || !nz || !dx || !dy || !dz || !t || !gamma) return BSN_ERR_ARG;
+        h5::Reader R;
+        std::string err;
+        if (!R.open(path, &err)) return BSN_ERR_IO;
+        const auto& a = R.root().attrs;
+        int64_t n3[3];
+        if (!h5::get_i64(a, "nx", &n3[0]) || !h5::get_i64(a, "ny", &n3[1]) || !h5::get_i64(a, "nz", &n3[2]) ||
+            !h5::get_f64(a, "dx", dx) || !h5::get_f64(a, "dy", dy) || !h5::get_f64(a, "dz", dz) ||
+            !h5::get_f64(a, "t", t) || !h5::get_f64(a, "gamma", gamma))
+            return BSN_ERR_IO;
+        *nx = (int)n3[0]; *ny = (int)n3[1]; *nz = (int)n3[2];
+        if (!U_active) return BSN_OK;
+        const size_t nc = (size_t)n3[0] * n3[1] * n3[2];
+        if ((long long)(5 * nc) > cap) return BSN_ERR_ARG;
+        const char* names[5] = {"gas/rho", "gas/rhovx", "gas/rhovy", "gas/rhovz", "gas/E"};
+        std::vector<double> f(nc);
+        for (int q = 0; q < 5; ++q) {
+            const h5::RDataset* d = R.dataset(names[q]);
+            if (!d || d->kind != h5::F64 || d->count() != nc || !R.read_data(*d, f.data(), 8 * nc, &err)) return BSN_ERR_IO;
+            for (size_t o = 0; o < nc; ++o) U_active[5 * o + q] = f[o];   // U_active[q, i, j, k]
+        }
+        return BSN_OK;
+    } catch (const std::bad_alloc&) {
+        return BSN_ERR_NOMEM;
+    } catch (...) {
         return BSN_ERR_IO;
-    *nx = (int)n3[0]; *ny = (int)n3[1]; *nz = (int)n3[2];
-    if (!U_active) return BSN_OK;
-    const size_t nc = (size_t)n3[0] * n3[1] * n3[2];
-    if ((long long)(5 * nc) > cap) return BSN_ERR_ARG;
-    const char* names[5] = {"gas/rho", "gas/rhovx", "gas/rhovy", "gas/rhovz", "gas/E"};
-    std::vector<double> f(nc);
-    for (int q = 0; q < 5; ++q) {
-        const h5::RDataset* d = R.dataset(names[q]);
-        if (!d || d->kind != h5::F64 || d->count() != nc || !R.read_data(*d, f.data(), 8 * nc, &err)) return BSN_ERR_IO;
-        for (size_t o = 0; o < nc; ++o) U_active[5 * o + q] = f[o];   // U_active[q, i, j, k]
     }
-    return BSN_OK;
 }
 
 // ---- BH trajectories (src/io.jl:96-180) -----------------------------------------
@@ -497,59 +546,77 @@ bool traj_read(const std::string& path, Traj& T, std::string* err) {
 }  // namespace
 
 extern "C" bsn_status bsn_trajectory_init(const char* path, int n_bh) {
-    if (!path || n_bh < 0) return BSN_ERR_ARG;
-    Traj T;
-    T.bh.resize((size_t)n_bh);
-    std::string err;
-    return traj_write(path, T, &err) ? BSN_OK : BSN_ERR_IO;
+    try {
+        if (!path || n_bh < 0) return BSN_ERR_ARG;
+        Traj T;
+        T.bh.resize((size_t)n_bh);
+        std::string err;
+        return traj_write(path, T, &err) ? BSN_OK : BSN_ERR_IO;
+    } catch (const std::bad_alloc&) {
+        return BSN_ERR_NOMEM;
+    } catch (...) {
+        return BSN_ERR_IO;
+    }
 }
 
 extern "C" bsn_status bsn_trajectory_append(const char* path, double t, const bsn_bh* bhs, int nbh) {
-    if (!path || nbh < 0 || (nbh > 0 && !bhs)) return BSN_ERR_ARG;
-    Traj T;
-    std::string err;
-    if (!traj_read(path, T, &err)) return BSN_ERR_IO;
-    if ((int)T.bh.size() != nbh) return BSN_ERR_ARG;
-    const size_t N = T.t.size();
-    T.t.push_back(t);
-    for (int i = 0; i < nbh; ++i) {
-        Traj::B& b = T.bh[i];
-        b.mass.push_back(bhs[i].mass);
-        b.rsink.push_back(jmax(6.0 * bhs[i].mass / sq(bhs[i].c_code), bhs[i].r_floor));   // r_sink(bh)
-        // (N+1, 3) column-major: insert the new row's entry at the end of each column
-        std::vector<double> p(3 * (N + 1)), v(3 * (N + 1));
-        for (int d = 0; d < 3; ++d) {
-            for (size_t r = 0; r < N; ++r) { p[d * (N + 1) + r] = b.pos[d * N + r]; v[d * (N + 1) + r] = b.vel[d * N + r]; }
-            p[d * (N + 1) + N] = bhs[i].pos[d];
-            v[d * (N + 1) + N] = bhs[i].vel[d];
+    try {
+        if (!path || nbh < 0 || (nbh > 0 && !bhs)) return BSN_ERR_ARG;
+        Traj T;
+        std::string err;
+        if (!traj_read(path, T, &err)) return BSN_ERR_IO;
+        if ((int)T.bh.size() != nbh) return BSN_ERR_ARG;
+        const size_t N = T.t.size();
+        T.t.push_back(t);
+        for (int i = 0; i < nbh; ++i) {
+            Traj::B& b = T.bh[i];
+            b.mass.push_back(bhs[i].mass);
+            b.rsink.push_back(jmax(6.0 * bhs[i].mass / sq(bhs[i].c_code), bhs[i].r_floor));   // r_sink(bh)
+            // (N+1, 3) column-major: insert the new row's entry at the end of each column
+            std::vector<double> p(3 * (N + 1)), v(3 * (N + 1));
+            for (int d = 0; d < 3; ++d) {
+                for (size_t r = 0; r < N; ++r) { p[d * (N + 1) + r] = b.pos[d * N + r]; v[d * (N + 1) + r] = b.vel[d * N + r]; }
+                p[d * (N + 1) + N] = bhs[i].pos[d];
+                v[d * (N + 1) + N] = bhs[i].vel[d];
+            }
+            b.pos.swap(p);
+            b.vel.swap(v);
         }
-        b.pos.swap(p);
-        b.vel.swap(v);
+        return traj_write(path, T, &err) ? BSN_OK : BSN_ERR_IO;
+    } catch (const std::bad_alloc&) {
+        return BSN_ERR_NOMEM;
+    } catch (...) {
+        return BSN_ERR_IO;
     }
-    return traj_write(path, T, &err) ? BSN_OK : BSN_ERR_IO;
 }
 
 extern "C" bsn_status bsn_trajectory_read(const char* path, int* n_dumps, int* n_bh, double* t, double* mass,
                                           double* pos, double* vel, double* rsink, long long cap) {
-    if (!path || !n_dumps || !n_bh) return BSN_ERR_ARG;
-    Traj T;
-    std::string err;
-    if (!traj_read(path, T, &err)) return BSN_ERR_IO;
-    const long long N = (long long)T.t.size(), nb = (long long)T.bh.size();
-    *n_dumps = (int)N;
-    *n_bh = (int)nb;
-    if (!t) return BSN_OK;
-    if (N > cap) return BSN_ERR_ARG;
-    // t[N]; mass/rsink[b][N]; pos/vel[b][N][3] (row per dump)
-    for (long long r = 0; r < N; ++r) t[r] = T.t[r];
-    for (long long b = 0; b < nb; ++b)
-        for (long long r = 0; r < N; ++r) {
-            if (mass) mass[b * N + r] = T.bh[b].mass[r];
-            if (rsink) rsink[b * N + r] = T.bh[b].rsink[r];
-            for (int d = 0; d < 3; ++d) {
-                if (pos) pos[(b * N + r) * 3 + d] = T.bh[b].pos[d * N + r];
-                if (vel) vel[(b * N + r) * 3 + d] = T.bh[b].vel[d * N + r];
+    try {
+        if (!path || !n_dumps || !n_bh) return BSN_ERR_ARG;
+        Traj T;
+        std::string err;
+        if (!traj_read(path, T, &err)) return BSN_ERR_IO;
+        const long long N = (long long)T.t.size(), nb = (long long)T.bh.size();
+        *n_dumps = (int)N;
+        *n_bh = (int)nb;
+        if (!t) return BSN_OK;
+        if (N > cap) return BSN_ERR_ARG;
+        // t[N]; mass/rsink[b][N]; pos/vel[b][N][3] (row per dump)
+        for (long long r = 0; r < N; ++r) t[r] = T.t[r];
+        for (long long b = 0; b < nb; ++b)
+            for (long long r = 0; r < N; ++r) {
+                if (mass) mass[b * N + r] = T.bh[b].mass[r];
+                if (rsink) rsink[b * N + r] = T.bh[b].rsink[r];
+                for (int d = 0; d < 3; ++d) {
+                    if (pos) pos[(b * N + r) * 3 + d] = T.bh[b].pos[d * N + r];
+                    if (vel) vel[(b * N + r) * 3 + d] = T.bh[b].vel[d * N + r];
+                }
             }
-        }
-    return BSN_OK;
+        return BSN_OK;
+    } catch (const std::bad_alloc&) {
+        return BSN_ERR_NOMEM;
+    } catch (...) {
+        return BSN_ERR_IO;
+    }
 }
