@@ -209,6 +209,68 @@ def sedov_mid_state(n):
         return U0, dx, 0.0
 
 
+def slab_sedov(args, rank, world, log):
+    """Sedov n^3 at t = T_MID split into z-slabs over the ranks (bsn.shard:
+    ghost fill, halo exchange over torch.distributed, one fused stage launch
+    per RK3 stage, dt as the min over ranks), K steps timed with CUDA events
+    (max over ranks); beside it on rank 0 of a one-rank run, the device time
+    loop (bsn_run_steps) on the whole grid.  Strong scaling: the grid is the
+    same whatever the rank count."""
+    import torch
+    import bsn
+    from bsn import shard
+    n = args.n
+    # the package's initial condition, run to T_MID by the device loop on every rank
+    Uh, dx = sedov_host(n)
+    Ud0 = torch.from_numpy(Uh).cuda()
+    t0, _ = bsn.run_steps(Ud0, n, n, n, dx, dx, dx, GAMMA, CFL, n_steps=1_000_000, t=0.0, t_end=T_MID,
+                          precision="f64", rho_floor=1e-6, P_floor=1e-6)
+    U0 = Ud0.cpu().numpy()
+    del Ud0
+    slab = shard.Slab.split(n, n, n, rank, world)
+    k0, nzl = slab.k0, slab.nz
+    out = {"workload": f"sedov{n}^3 z-slabs", "ranks": world, "planes_per_rank": nzl, "steps": args.steps}
+    kw = dict(rho_floor=1e-6, P_floor=1e-6)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    ops = shard.DeviceOps()
+    for prec in ("f64", "f32"):
+        U = bsn.state(n, n, nzl)
+        shard._zmajor(U)[...] = torch.from_numpy(U0.T[k0:k0 + nzl + 2 * NG].copy()).cuda()
+        t = t0
+        for _ in range(max(1, args.warmup)):
+            t, _ = shard.run_steps(U, slab, dx, dx, dx, GAMMA, CFL, ops, n_steps=1, t=t, precision=prec, **kw)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        t, k = shard.run_steps(U, slab, dx, dx, dx, GAMMA, CFL, ops, n_steps=args.steps, t=t, precision=prec, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        if dist:
+            tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        out[f"{prec}_slab_ms_per_step"] = ms
+        out[f"{prec}_slab_value"] = n ** 3 / (ms / 1e3)
+        log(f"slab Sedov {n}^3 {prec}, {world} rank(s): {ms:.3f} ms/step")
+        if world == 1:
+            Ud = torch.from_numpy(U0).cuda()
+            tt_, _ = bsn.run_steps(Ud, n, n, n, dx, dx, dx, GAMMA, CFL, n_steps=args.warmup, t=t0, precision=prec,
+                                   **kw)
+            torch.cuda.synchronize()
+            e0.record()
+            bsn.run_steps(Ud, n, n, n, dx, dx, dx, GAMMA, CFL, n_steps=args.steps, t=tt_, precision=prec, **kw)
+            e1.record()
+            torch.cuda.synchronize()
+            out[f"{prec}_device_loop_ms_per_step"] = e0.elapsed_time(e1) / args.steps
+        del U
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -830,10 +892,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-fmr", action="store_true",
                     help="skip the two-level FMR polytrope and binary-BH coupled-loop timings")
-    ap.add_argument("--workload", default="sedov", choices=["sedov", "binary_nested", "polytrope_fmr", "poisson"],
+    ap.add_argument("--workload", default="sedov", choices=["sedov", "binary_nested", "polytrope_fmr", "poisson", "slab"],
                     help="binary_nested: time only the binary-BH supernova on three nested FMR levels; "
                          "polytrope_fmr: only the two-level self-gravitating polytrope; "
-                         "poisson: only the isolated Poisson solve at 128^3, --steps solves per precision")
+                         "poisson: only the isolated Poisson solve at 128^3, --steps solves per precision; "
+                         "slab: Sedov --n^3 split into z-slabs over the torchrun ranks (bsn.shard)")
     ap.add_argument("--full", action="store_true",
                     help="with --workload: run the workload's stated length from its initial state (polytrope "
                          "200 steps, binary 1000 steps, no warm-up) instead of --steps")
@@ -878,6 +941,11 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
+        if args.workload == "slab":
+            out = slab_sedov(args, rank, world, log)
+            if rank == 0:
+                print(json.dumps(out), flush=True)
+            return
         run_bsn(args, rank, world)
     finally:
         if world > 1:

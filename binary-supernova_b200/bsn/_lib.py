@@ -56,6 +56,13 @@ class bsn_grid_meta(C.Structure):
                 ("z0", C.c_double), ("rho_floor", C.c_double), ("P_floor", C.c_double)]
 
 
+class bsn_stage_sources(C.Structure):
+    _fields_ = [("bhs", C.POINTER(bsn_bh)), ("nbh", C.c_int), ("nsink", C.c_int), ("f_sink", C.c_double),
+                ("torque_free", C.c_int), ("rho_sink_min", C.c_double), ("x0", C.c_double), ("y0", C.c_double),
+                ("z0", C.c_double), ("k0", C.c_int), ("phi", C.c_void_p), ("phi_lo", C.c_void_p),
+                ("phi_hi", C.c_void_p)]
+
+
 _V, _I, _D, _P, _LL = C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_longlong
 _dp = C.POINTER(C.c_double)
 _BH = C.POINTER(bsn_bh)
@@ -112,6 +119,8 @@ SIGNATURES = {
     "bsn_sink_terms_slab_f64": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _I, _BH, _D, _D, _D,
                                      C.POINTER(C.c_int), _dp, _LL, C.POINTER(C.c_longlong)]),
     "bsn_accrete_from_terms": (_I, [_BH, _dp, _LL]),
+    "bsn_euler3d_stage": (_I, [_V, _P, _P, _P, _I, _I, _I, _D, _D, _D, _D, _D, _I, _D, _D, _I,
+                               C.POINTER(bsn_stage_sources)]),
     "bsn_save_checkpoint_uniform": (_I, [_V, C.c_char_p, _P, _I, _BH, _I, C.POINTER(bsn_grid_meta),
                                          C.POINTER(bsn_ckpt_meta)]),
     "bsn_save_checkpoint_uniform_async": (_I, [_V, C.c_char_p, _P, _BH, _I, C.POINTER(bsn_grid_meta),

@@ -18,7 +18,7 @@ from typing import Sequence
 import numpy as np
 import torch
 
-from ._lib import BSNError, bsn_bh, bsn_fmr2, load
+from ._lib import BSNError, bsn_bh, bsn_fmr2, bsn_stage_sources, load
 
 NG = 3
 BC = {"outflow": 0, "periodic": 1}
@@ -284,6 +284,28 @@ def sink_terms_slab(U, nx, ny, nz, dx, dy, dz, x0, y0, z0, k0, bh, dt, box, *, f
           float(y0), float(z0), int(k0), C.byref(bh), float(dt), float(f_sink), float(rho_sink_min), b,
           out.ctypes.data_as(C.POINTER(C.c_double)), cap, C.byref(n))
     return out[:n.value]
+
+
+def euler3d_stage(Uout, Uin, Un, nx, ny, nz, dx, dy, dz, dt, gamma, stage, *, rho_floor=0.0, P_floor=0.0,
+                  precision="f64", bhs=(), nsink=0, f_sink=1.0, torque_free=True, rho_sink_min=0.0, x0=0.0,
+                  y0=0.0, z0=0.0, k0=0, phi=None, phi_lo=None, phi_hi=None):
+    """One SSP-RK3 stage (1, 2 or 3) of euler3d_step! / coupled_step! in one
+    fused launch, with Uin's ghost cells as the caller left them; Uout must
+    differ from Uin, and stage 1 takes Un = Uin.  Sources: BH gravity of
+    `bhs`, the sinks of bhs[:nsink], the self-gravity gradient of `phi` (the
+    potential of Uin's floored density) with the neighbouring slabs' planes
+    phi_lo / phi_hi; k0 is the slab's first global plane."""
+    for a, name in ((Uout, "Uout"), (Uin, "Uin"), (Un, "Un")):
+        _check_state(a, nx, ny, nz, name)
+    arr = _bh_array(bhs)
+    src = bsn_stage_sources(arr, len(bhs), int(nsink), float(f_sink), int(bool(torque_free)), float(rho_sink_min),
+                            float(x0), float(y0), float(z0), int(k0),
+                            None if phi is None else phi.data_ptr(),
+                            None if phi_lo is None else phi_lo.data_ptr(),
+                            None if phi_hi is None else phi_hi.data_ptr())
+    _call("bsn_euler3d_stage", context(), _ptr(Uout), _ptr(Uin), _ptr(Un), nx, ny, nz, float(dx), float(dy),
+          float(dz), float(dt), float(gamma), int(stage), float(rho_floor), float(P_floor), PREC[precision],
+          C.byref(src))
 
 
 def accrete_from_terms(bh, terms):
@@ -716,6 +738,6 @@ def set_profiling(on: bool):
     _call("bsn_ctx_set_profiling", context(), int(bool(on)))
 
 
-__all__ += ["add_bh_gravity_source_slab", "add_sink_sources_slab", "gas_force_pairs_slab", "merge_force_pairs",
+__all__ += ["euler3d_stage", "add_bh_gravity_source_slab", "add_sink_sources_slab", "gas_force_pairs_slab", "merge_force_pairs",
             "sink_box", "sink_terms_slab", "accrete_from_terms", "euler3d_rhs_f32", "euler3d_step_f32", "euler3d_step_learned", "run_steps", "fmr3d_run_steps", "coupled_run_steps", "diagnostics", "tile_variants", "set_tile", "get_tile", "kernel_time",
             "set_profiling", "fp_peak", "PREC"]

@@ -143,7 +143,7 @@ def cfl_dt(U, slab: Slab, dx, dy, dz, gamma, cfl, ops, group=None) -> float:
 
 
 def euler3d_step(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group=None, rho_floor=0.0, P_floor=0.0,
-                 self_gravity=False):
+                 self_gravity=False, precision="f64"):
     """euler3d_step! (src/euler3d.jl:220-260) on this rank's slab, with the
     halo exchange before every right-hand side; with self_gravity, the
     self-gravity source of the global grid after each right-hand side, as
@@ -152,33 +152,43 @@ def euler3d_step(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group=None, rho_floo
     and the reference runs it only with outflow (coupled_step!)."""
     if self_gravity and slab.bc != "outflow":
         raise ValueError("self_gravity needs bc='outflow': the isolated Poisson solve has no periodic form")
-
-    def sources(dU, U):
-        if self_gravity:
-            add_self_gravity_source(dU, U, slab, dx, dy, dz, ops, group)
-
-    _rk3(U, slab, dx, dy, dz, dt, gamma, ops, group, rho_floor, P_floor, sources)
+    _rk3(U, slab, dx, dy, dz, dt, gamma, ops, group, rho_floor, P_floor, None, self_gravity, precision)
 
 
-def _rk3(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group, rho_floor, P_floor, sources):
-    """The three stages of euler3d_step! on the slab: ghosts, halo exchange,
-    euler3d_rhs!, then sources(dU, U) (the source terms coupled_step! adds
-    after the right-hand side), the stage combination and floors."""
+class StageSources:
+    """The sources coupled_step! adds after each right-hand side on a slab:
+    BH gravity of `bhs`, the sinks of bhs[:nsink], and (filled per stage by
+    _rk3) the self-gravity potential with its neighbouring planes."""
+
+    def __init__(self, bhs=(), nsink=0, f_sink=1.0, torque_free=True, rho_sink_min=0.0, x0=0.0, y0=0.0, z0=0.0):
+        self.bhs, self.nsink, self.f_sink, self.torque_free = list(bhs), nsink, f_sink, torque_free
+        self.rho_sink_min, self.x0, self.y0, self.z0 = rho_sink_min, x0, y0, z0
+        self.phi = self.phi_lo = self.phi_hi = None
+
+
+def _rk3(U, slab: Slab, dx, dy, dz, dt, gamma, ops, group, rho_floor, P_floor, src, self_gravity, precision):
+    """The three stages of euler3d_step! on the slab, each one `ops.stage`
+    (on the device: one fused launch) after the ghost fill and the halo
+    exchange of its input; the stage inputs and outputs alternate (a copy of
+    U) -> A -> B -> U, with U^n = U in every combination.  With self-gravity the potential of the stage input's floored
+    density (the density euler3d_rhs! leaves before add_self_gravity_source!)
+    is solved over the slabs first."""
     nx, ny, nz = slab.nx, slab.ny, slab.nz
-    Un = ops.copy(U)
-    dU = ops.zeros_like(U)
-    for stage in range(3):
-        ops.fill(U, nx, ny, nz, slab.bc)
-        exchange(U, slab, ops, group, rho_floor, P_floor, gamma)
-        ops.rhs(dU, U, nx, ny, nz, dx, dy, dz, gamma, slab.bc, rho_floor, P_floor)
-        sources(dU, U)
-        if stage == 0:
-            ops.assign(U, Un + dt * dU)
-        elif stage == 1:
-            ops.assign(U, 0.75 * Un + 0.25 * U + (0.25 * dt) * dU)
-        else:
-            ops.assign(U, (1.0 / 3.0) * Un + (2.0 / 3.0) * U + ((2.0 / 3.0) * dt) * dU)
-        ops.floors(U, nx, ny, nz, rho_floor, P_floor, gamma)
+    # stage 1 reads a copy of U, whose ghosts the fill and the exchange may
+    # change: U^n's own ghost cells enter the final combination unchanged
+    C, A, B = ops.copy(U), ops.zeros_like(U), ops.zeros_like(U)
+    ins, outs = (C, A, B), (A, B, U)
+    if self_gravity and src is None:
+        src = StageSources()
+    for s in range(3):
+        Uin = ins[s]
+        ops.fill(Uin, nx, ny, nz, slab.bc)
+        exchange(Uin, slab, ops, group, rho_floor, P_floor, gamma)
+        if self_gravity:
+            rho = ops.active_rho_floored(Uin, nx, ny, nz, rho_floor)
+            src.phi = poisson_isolated(rho, slab, dx, dy, dz, ops, group)
+            src.phi_lo, src.phi_hi = _phi_neighbours(src.phi, slab, group)
+        ops.stage(outs[s], Uin, U, s + 1, slab, dx, dy, dz, dt, gamma, rho_floor, P_floor, src, precision)
 
 
 # ---------------------------------------------------------------------------
@@ -242,7 +252,7 @@ def accrete(bh, U, slab: Slab, dx, dy, dz, x0, y0, z0, dt, ops, group=None, *, f
 
 def coupled_step(U, bhs, slab: Slab, dt, t, dx, x0, y0, z0, gamma, ops, group=None, *, f_sink=1.0,
                  rho_floor=0.0, P_floor=0.0, torque_free=True, self_gravity=False, t_bh2_sink_on=0.0,
-                 rho_sink_min=0.0, evolve_orbit=True):
+                 rho_sink_min=0.0, evolve_orbit=True, precision="f64"):
     """coupled_step! (scripts/run_sn50_fiducial.jl:756-818) on this rank's slab
     of the global grid (cubic cells dx, outflow boundaries): the gas force on
     every BH with the driver's non-finite / 1e3 guard, nbody_step!, the three
@@ -264,23 +274,15 @@ def coupled_step(U, bhs, slab: Slab, dt, t, dx, x0, y0, z0, gamma, ops, group=No
             F[i] = f
     if evolve_orbit and nbh > 0 and all(math.isfinite(v) for b in bhs for v in (*b.pos, *b.vel)):
         api.nbody_step(bhs, dt, F)
-    nx, ny, nz = slab.nx, slab.ny, slab.nz
-
-    def sources(dU, U):
-        ops.bh_gravity(dU, U, nx, ny, nz, dx, dx, dx, bhs, x0, y0, z0, slab.k0)
-        if self_gravity:
-            add_self_gravity_source(dU, U, slab, dx, dx, dx, ops, group)
-        ops.sink_sources(dU, U, nx, ny, nz, dx, dx, dx, bhs[:nsink], x0, y0, z0, slab.k0, f_sink, torque_free,
-                         rho_sink_min)
-
-    _rk3(U, slab, dx, dx, dx, dt, gamma, ops, group, rho_floor, P_floor, sources)
+    src = StageSources(bhs, nsink, f_sink, torque_free, rho_sink_min, x0, y0, z0)
+    _rk3(U, slab, dx, dx, dx, dt, gamma, ops, group, rho_floor, P_floor, src, self_gravity, precision)
     for i in range(nsink):
         accrete(bhs[i], U, slab, dx, dx, dx, x0, y0, z0, dt, ops, group, f_sink=f_sink, rho_sink_min=rho_sink_min)
     return F
 
 
 def run_steps(U, slab: Slab, dx, dy, dz, gamma, cfl, ops, *, n_steps, t=0.0, t_end=0.0, group=None,
-              rho_floor=0.0, P_floor=0.0, self_gravity=False):
+              rho_floor=0.0, P_floor=0.0, self_gravity=False, precision="f64"):
     """The driver loop `dt = cfl_dt_3d; dt = min(dt, t_end - t); euler3d_step!;
     t += dt` over the slabs (every rank takes the same dts); returns (t, steps)."""
     if self_gravity and slab.bc != "outflow":
@@ -292,7 +294,7 @@ def run_steps(U, slab: Slab, dx, dy, dz, gamma, cfl, ops, *, n_steps, t=0.0, t_e
             dt = min(dt, t_end - t)
         if not dt > 0.0:
             raise FloatingPointError(f"time step collapsed to {dt} at t = {t}")
-        euler3d_step(U, slab, dx, dy, dz, dt, gamma, ops, group, rho_floor, P_floor, self_gravity)
+        euler3d_step(U, slab, dx, dy, dz, dt, gamma, ops, group, rho_floor, P_floor, self_gravity, precision)
         t += dt
         steps += 1
     return t, steps
@@ -480,6 +482,23 @@ class DeviceOps:
         self.api.apply_sg_force_slab(dU, U, phi, nx, ny, nz, dx, dy, dz,
                                      None if lo is None else lo.contiguous(),
                                      None if hi is None else hi.contiguous())
+
+    def active_rho_floored(self, U, nx, ny, nz, rho_floor):
+        """The active density as euler3d_rhs! leaves it (floored at rho_floor)."""
+        rho = self.active_rho(U, nx, ny, nz)
+        return rho.clamp_(min=rho_floor)
+
+    def stage(self, Uout, Uin, Un, s, slab, dx, dy, dz, dt, gamma, rho_floor, P_floor, src, precision):
+        """One RK3 stage in one fused launch (bsn_euler3d_stage) with Uin's
+        ghost cells as filled and exchanged."""
+        kw = {}
+        if src is not None:
+            kw = dict(bhs=src.bhs, nsink=src.nsink, f_sink=src.f_sink, torque_free=src.torque_free,
+                      rho_sink_min=src.rho_sink_min, x0=src.x0, y0=src.y0, z0=src.z0, k0=slab.k0, phi=src.phi,
+                      phi_lo=None if src.phi_lo is None else src.phi_lo.contiguous(),
+                      phi_hi=None if src.phi_hi is None else src.phi_hi.contiguous())
+        self.api.euler3d_stage(Uout, Uin, Un, slab.nx, slab.ny, slab.nz, dx, dy, dz, dt, gamma, s,
+                               rho_floor=rho_floor, P_floor=P_floor, precision=precision, **kw)
 
     def bh_gravity(self, dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0, k0):
         self.api.add_bh_gravity_source_slab(dU, U, nx, ny, nz, dx, dy, dz, bhs, x0, y0, z0, k0)

@@ -6,6 +6,7 @@
 
 #include "hydro_f64.cuh"
 #include "poisson.cuh"
+#include "stage_launch.cuh"
 #include "sums.cuh"
 
 namespace bsn {
@@ -509,6 +510,53 @@ extern "C" bsn_status bsn_accrete_from_terms(bsn_bh* bh, const double* terms, lo
     for (long long c = 0; c < n; ++c)
         for (int q = 0; q < 4; ++q) s[q] += terms[4 * c + q];
     accrete_update(bh, s[0], s[1], s[2], s[3]);
+    return BSN_OK;
+}
+
+extern "C" bsn_status bsn_euler3d_stage(bsn_ctx* ctx, double* Uout, double* Uin, const double* Un, int nx, int ny,
+                                        int nz, double dx, double dy, double dz, double dt, double gamma, int stage,
+                                        double rho_floor, double P_floor, int precision,
+                                        const bsn_stage_sources* src) {
+    BSN_TRY(check_dims(ctx, nx, ny, nz));
+    if (!Uout || !Uin || !Un) return set_err(ctx, BSN_ERR_ARG, "null state array");
+    if (Uout == Uin) return set_err(ctx, BSN_ERR_ARG, "Uout must not be the stage input (the stencils read it)");
+    if (stage < 1 || stage > 3) return set_err(ctx, BSN_ERR_ARG, "stage %d outside 1..3", stage);
+    if (precision != PREC_F64 && precision != PREC_F32 && precision != PREC_LEARNED)
+        return set_err(ctx, BSN_ERR_ARG, "unknown precision %d", precision);
+    f64::StageArgs A;
+    stage_args_init(A, nx, ny, nz, dx, dy, dz, gamma, BSN_BC_OUTFLOW, rho_floor, P_floor);
+    A.Uin = Uin;
+    A.Gh = Uin;   // the caller filled (and exchanged) the input's ghost cells
+    A.Un = Un;
+    A.Uout = Uout;
+    A.mode = 0;
+    set_stage(A, stage, dt);
+    A.stiff_guard = ctx->stiff_guard;
+    if (src) {
+        if (src->k0 < 0) return set_err(ctx, BSN_ERR_ARG, "k0 = %d", src->k0);
+        if (src->nsink < 0 || src->nsink > src->nbh) return set_err(ctx, BSN_ERR_ARG, "nsink %d of %d BHs", src->nsink, src->nbh);
+        A.x0 = src->x0; A.y0 = src->y0; A.z0 = src->z0;
+        A.k0 = src->k0;
+        if (src->nbh > 0) {
+            BSN_TRY(fill_bh(ctx, src->bhs, src->nbh, A.bh));
+            A.use_bh = 1;
+        }
+        if (src->nsink > 0) {
+            BSN_TRY(fill_sink(ctx, src->bhs, src->nsink, src->f_sink, src->torque_free, src->rho_sink_min, A.sk));
+            A.use_sink = 1;
+            A.stiff_guard = 1;   // near-vacuum cells beside the sinks (FP32 stencils)
+        }
+        if (src->phi) {
+            A.phi = src->phi;
+            A.use_sg = 1;
+            A.phi_lo = src->phi_lo;
+            A.phi_hi = src->phi_hi;
+        }
+    }
+    BSN_TRY(stage_launch(ctx, precision, A));
+    // the reference combines whole arrays: after stage 3 the ghost cells of U
+    // hold (1/3) U^n's + (2/3) the stage input's (whose right-hand side is zero there)
+    if (stage == 3 && Uout == Un) BSN_TRY(f64_ghost_combine(ctx, Uout, Uin, Uin, nx, ny, nz, BSN_BC_OUTFLOW, dt));
     return BSN_OK;
 }
 

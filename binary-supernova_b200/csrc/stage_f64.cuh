@@ -88,6 +88,13 @@ struct StageArgs {
     // FP32 path: compute faces whose density stencil spans more than three
     // decades in FP64 (the F32Guarded policy)
     int stiff_guard;
+    // the grid as a z-slab of a larger one: global index of its first active
+    // plane (cell centres of the sources), and the planes of Phi just below /
+    // above it (null at the larger grid's boundary) for the self-gravity
+    // gradient at the slab's edge planes
+    int k0;
+    const double* phi_lo;
+    const double* phi_hi;
 };
 
 enum { LED_BND = 0, LED_DRAIN = 1, LED_POST = 2, LED_PRE = 3, LED_TERMS = 4 };

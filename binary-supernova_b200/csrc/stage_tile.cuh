@@ -665,7 +665,7 @@ __device__ __forceinline__ bool stage_block(const f64::StageArgs& A, int a0, int
         double* d = acc[m];
         double xc = A.x0 + ((double)(a + 1) - 0.5) * A.dx;
         double yc = A.y0 + ((double)(b + 1) - 0.5) * A.dy;
-        double zc = A.z0 + ((double)(c + 1) - 0.5) * A.dz;
+        double zc = A.z0 + ((double)(c + 1 + A.k0) - 0.5) * A.dz;
         if (A.use_bh) {   // src/gpu_kernels.jl:199-230
             double vx = u1 / u0, vy = u2 / u0, vz = u3 / u0;
             double ax = 0.0, ay = 0.0, az = 0.0;
@@ -691,7 +691,13 @@ __device__ __forceinline__ bool stage_block(const f64::StageArgs& A, int a0, int
             long long sy = nx, sz = (long long)nx * ny;
             double gx = (Pp[ip + sy * b + sz * c] - Pp[im + sy * b + sz * c]) * fx;
             double gy = (Pp[a + sy * jp + sz * c] - Pp[a + sy * jm + sz * c]) * fy;
-            double gz = (Pp[a + sy * b + sz * kp] - Pp[a + sy * b + sz * km]) * fz;
+            double pzp = Pp[a + sy * b + sz * kp], pzm = Pp[a + sy * b + sz * km];
+            if (A.phi_lo || A.phi_hi) {   // a slab's edge planes: the larger grid's central difference
+                fz = A.inv2dz;
+                if (c == nz - 1 && A.phi_hi) pzp = A.phi_hi[a + sy * b];
+                if (c == 0 && A.phi_lo) pzm = A.phi_lo[a + sy * b];
+            }
+            double gz = (pzp - pzm) * fz;
             double vdotg = (u1 * gx + u2 * gy + u3 * gz) / u0;
             d[1] -= u0 * gx; d[2] -= u0 * gy; d[3] -= u0 * gz; d[4] -= u0 * vdotg;
         }

@@ -280,6 +280,35 @@ bsn_status bsn_gas_force_on_bh_slab_f64(bsn_ctx* ctx, const double* U, int nx, i
                                         double dx, double dy, double dz, const bsn_bh* bh,
                                         double x0, double y0, double z0, int k0, double out[6]);
 bsn_status bsn_merge_force_pairs(const double* pairs, int nparts, double out[3]);
+/* One SSP-RK3 stage of euler3d_step! / coupled_step! (src/euler3d.jl:220-260,
+ * scripts/run_sn50_fiducial.jl:767-790) as one fused launch, with the input's
+ * ghost cells as the caller left them (filled, and on a z-slab exchanged with
+ * the neighbouring slabs): Uout = the stage combination of Un and the floored
+ * Uin with the right-hand side of Uin plus the sources, then floored.  Uout
+ * must differ from Uin; stage 1 takes Un = Uin (the unfloored U^n, as the
+ * reference combines).  Sources (src may be NULL): BH gravity of bhs[0..nbh),
+ * the sinks of bhs[0..nsink) (src/gpu_kernels.jl:199-284), the self-gravity
+ * gradient of phi (nx ny nz, the potential of the stage input's floored
+ * density) with the neighbouring slabs' planes phi_lo / phi_hi (NULL at the
+ * global boundary); cell centres x0 + (i + 0.5) dx ... with the slab's first
+ * global plane k0.  precision: BSN_PREC_*; the FP32 forms compute stiff faces
+ * in FP64 when sinks are on (bsn_ctx_set_stiff_guard otherwise).  The ghost
+ * cells of Uout: after stage 3 with Uout = Un (the state U, whose ghost cells
+ * must then still hold U^n's) the reference's whole-array combination
+ * (1/3) U^n + (2/3) Uin there; otherwise left as they were (the next stage's
+ * fill replaces them).  Stage 1's input must not be U itself when the caller
+ * fills its ghosts (U^n's ghost cells enter that combination).  No single
+ * reference counterpart: the reference's stage is euler3d_rhs! plus the
+ * source calls plus the combination. */
+typedef struct {
+    const bsn_bh* bhs; int nbh; int nsink;
+    double f_sink; int torque_free; double rho_sink_min;
+    double x0, y0, z0; int k0;
+    const double* phi; const double* phi_lo; const double* phi_hi;
+} bsn_stage_sources;
+bsn_status bsn_euler3d_stage(bsn_ctx* ctx, double* Uout, double* Uin, const double* Un, int nx, int ny, int nz,
+                             double dx, double dy, double dz, double dt, double gamma, int stage,
+                             double rho_floor, double P_floor, int precision, const bsn_stage_sources* src);
 /* accrete! (src/sinks.jl:74-109) over slabs, in three parts whose result is
  * the undivided accrete! bit for bit: bsn_sink_box gives the global active
  * box (0-based inclusive {ilo,ihi,jlo,jhi,klo,khi}) that holds the sink

@@ -213,3 +213,52 @@ def test_single_slab_coupled_step_bitwise_to_oracle(orc):
     for i in range(2):
         assert bg[i].mass == bo[i].mass and list(bg[i].vel) == list(bo[i].vel)
         assert bg[i].mass > specs[i]["mass"]
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_fused_stages_equal_the_step(orc, precision):
+    """bsn_euler3d_stage three times (ghosts filled by the caller, inputs and
+    outputs alternating (a copy of U) -> A -> B -> U) is euler3d_step! of the same
+    precision bit for bit; FP64 also equals the oracle."""
+    import bsn
+    n, dx, g = (14, 10, 12), 0.1, 1.4
+    kw = dict(rho_floor=1e-6, P_floor=1e-5)
+    U = random_state(*n, seed=51, vacuum=True)
+    orc.fill_ghost_3d_outflow(U)
+    dt = orc.cfl_dt_3d(U, dx, dx, dx, g, 0.4)
+    Ud, Us = dev(U), dev(U)
+    (bsn.euler3d_step if precision == "f64" else bsn.euler3d_step_f32)(Ud, *n, dx, dx, dx, dt, g, **kw)
+    C, A, B = Us.clone(), torch.zeros_like(Us), torch.zeros_like(Us)
+    for s, (src, dst) in enumerate(((C, A), (A, B), (B, Us))):
+        bsn.fill_ghost_3d_outflow(src, *n)
+        bsn.euler3d_stage(dst, src, Us, *n, dx, dx, dx, dt, g, s + 1, precision=precision, **kw)
+    assert torch.equal(Us, Ud)
+    if precision == "f64":
+        orc.euler3d_step(U, dx, dx, dx, dt, g, **kw)
+        assert_bitwise(host(Us), U, "fused stages")
+
+
+def test_single_slab_fp32_coupled_step_runs_the_fused_stage(orc):
+    """The slab coupled step with FP32 stencils (one fused launch per stage,
+    stiff faces in FP64 beside the sinks) stays within FP32 rounding of the
+    oracle's FP64 coupled_step! over one step."""
+    import bsn
+    from bsn import shard
+    from binary_ic import binary_setup
+    U, dx, x0, specs = binary_setup(orc, n=32)
+    Ud = dev(U)
+    bg = [bsn.BlackHole(s["pos"], s["vel"], s["mass"], s["eps"], s["c_code"], s["r_floor"]) for s in specs]
+    bo = orc.bh_array([orc.make_bh(s["pos"], s["vel"], s["mass"], s["eps"], s["c_code"], s["r_floor"])
+                       for s in specs])
+    dt = orc.cfl_dt_3d(U, dx, dx, dx, 4 / 3, 0.4)
+    shard.coupled_step(Ud, bg, shard.Slab.split(32, 32, 32, 0, 1), dt, 0.0, dx, x0, x0, x0, 4 / 3,
+                       shard.DeviceOps(), rho_floor=1e-8, P_floor=1e-10, rho_sink_min=2e-8, evolve_orbit=False,
+                       precision="f32")
+    orc.coupled_step(U, bo, 2, dt, 0.0, dx, x0, x0, x0, 4 / 3, 1.0, 1e-8, 1e-10, True, False, 0.0, 2e-8,
+                     evolve_orbit=False)
+    G = host(Ud)
+    a = (slice(NG, -NG),) * 3
+    for q in (0, 4):
+        err = np.abs(G[(q,) + a] - U[(q,) + a]).sum() / np.abs(U[(q,) + a]).sum()
+        assert err < 1e-6, (q, err)
+    assert abs(bg[0].mass - bo[0].mass) <= 1e-9 * bo[0].mass

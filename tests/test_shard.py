@@ -48,6 +48,37 @@ class OracleOps:
     def cfl(self, U, nx, ny, nz, dx, dy, dz, gamma, cfl):
         return self.orc.cfl_dt_3d(U, dx, dy, dz, gamma, cfl)
 
+    def active_rho_floored(self, U, nx, ny, nz, rho_floor):
+        import torch
+        r = U[0, NG:NG + nx, NG:NG + ny, NG:NG + nz]
+        return torch.from_numpy(np.asfortranarray(np.where(r < rho_floor, rho_floor, r)))
+
+    def stage(self, Uout, Uin, Un, s, slab, dx, dy, dz, dt, gamma, rho_floor, P_floor, src, precision):
+        """One stage the reference's way: euler3d_rhs! (flooring its input in
+        place), the sources in coupled_step!'s order, the combination, floors."""
+        sys.path.insert(0, os.path.join(ROOT, "binary-supernova_b200"))
+        from bsn import shard
+        nx, ny, nz = slab.nx, slab.ny, slab.nz
+        assert Un is not Uin   # the right-hand side floors its input in place; U^n stays as it was
+        dU = np.zeros_like(Uin, order="F")
+        self.rhs(dU, Uin, nx, ny, nz, dx, dy, dz, gamma, slab.bc, rho_floor, P_floor)
+        if src is not None:
+            if src.bhs:
+                self.bh_gravity(dU, Uin, nx, ny, nz, dx, dy, dz, src.bhs, src.x0, src.y0, src.z0, slab.k0)
+            if src.phi is not None:
+                shard.sg_source(dU, Uin, src.phi, slab, dx, dy, dz, self, src.phi_lo, src.phi_hi)
+            if src.nsink:
+                self.sink_sources(dU, Uin, nx, ny, nz, dx, dy, dz, src.bhs[:src.nsink], src.x0, src.y0, src.z0,
+                                  slab.k0, src.f_sink, src.torque_free, src.rho_sink_min)
+        if s == 1:
+            W = Un + dt * dU
+        elif s == 2:
+            W = 0.75 * Un + 0.25 * Uin + (0.25 * dt) * dU
+        else:
+            W = (1.0 / 3.0) * Un + (2.0 / 3.0) * Uin + ((2.0 / 3.0) * dt) * dU
+        Uout[...] = W
+        self.floors(Uout, nx, ny, nz, rho_floor, P_floor, gamma)
+
     def _obhs(self, bhs):
         return [self.orc.make_bh(tuple(b.pos), tuple(b.vel), b.mass, b.eps, b.c_code, b.r_floor) for b in bhs]
 
