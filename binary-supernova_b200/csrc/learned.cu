@@ -757,7 +757,7 @@ bsn_status launch_learned(bsn_ctx* ctx, const f64::StageArgs& A0) {
     f64::StageArgs A = A0;
     A.split_count = cnt;
     A.split_list = (int*)(cnt + 4);
-    BSN_CUDA(ctx, cudaMemsetAsync(cnt, 0, sizeof(unsigned int), ctx->stream));
+    BSN_CUDA(ctx, cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), ctx->stream));   // list count, queue counter
     // the screening launch stages with the plain loader (its TMA form is not used)
     prof_begin(ctx);
     fs<<<grid, NT, smem_s, ctx->stream>>>(A);

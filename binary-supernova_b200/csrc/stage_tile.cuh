@@ -830,21 +830,29 @@ __global__ void __launch_bounds__(NT, MINB)
 }
 
 // The listed blocks of a split stage (written by its screening launch, which
-// runs first on the same stream), walked by a persistent grid.
+// runs first on the same stream), walked by a persistent grid: each CTA takes
+// its first block by its index, then draws the next from a queue counter
+// (split_count[1], zeroed with the count), so CTAs whose blocks hold more
+// network rows take fewer blocks.
 template <class P, int TX, int TY, int TZ, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel_list(const __grid_constant__ f64::StageArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[NT / 32];
     __shared__ unsigned int nanflag;
+    __shared__ int next;
     if (A.done_dev && *A.done_dev) return;
     const int n = (int)*A.split_count;
     if ((int)blockIdx.x >= n) return;
     P::prologue(policy_smem<P, TX, TY, TZ>(smem_raw), A, NT);   // visible after the first barrier
     const int gx = (A.nx + TX - 1) / TX, gy = (A.ny + TY - 1) / TY;
-    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+    for (int t = blockIdx.x; t < n;) {
         const int b = A.split_list[t];
         stage_block<P, TX, TY, TZ, NT>(A, (b % gx) * TX, ((b / gx) % gy) * TY, (b / (gx * gy)) * TZ, smem_raw, red,
                                        nanflag);
+        // the block's barriers order every thread's reads of `next` before this write
+        if (threadIdx.x == 0) next = (int)gridDim.x + (int)atomicAdd(A.split_count + 1, 1u);
+        __syncthreads();
+        t = next;
     }
 }
 
