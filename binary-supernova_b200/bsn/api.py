@@ -715,6 +715,8 @@ def set_tile(precision="f64", variant=-1):
 
 
 def get_tile(nx, ny, nz, precision="f64"):
+    """(tx, ty, tz, threads, CTAs per SM) of the tile chosen last for this
+    grid; each driver loop keeps its own choice per grid."""
     out = (C.c_int * 5)()
     _call("bsn_ctx_get_tile", context(), PREC[precision], nx, ny, nz, out)
     return tuple(out)

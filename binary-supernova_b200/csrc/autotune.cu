@@ -1,7 +1,8 @@
 // autotune.cu -- picks the tile shape of the fused stage kernel per grid,
 // and whether its block is staged by TMA copies or by the plain loader.
 //
-// On the first stage of a new (precision, nx, ny, nz) the autotuner launches
+// On the first stage of a new (precision, driver class, nx, ny, nz) the
+// autotuner launches
 // every tile variant on stage-1 work (reading the caller's state, writing a
 // scratch array), with each staging the grid allows, times two launches of
 // each with CUDA events after one warm-up, and keeps the fastest for the life
@@ -45,6 +46,18 @@ static bsn_status launch_batch_variant(bsn_ctx* ctx, int prec, int idx, const f6
     return learned_launch_batch_variant(ctx, idx, B);
 }
 static bool prec_ok(int p) { return p == PREC_F64 || p == PREC_F32 || p == PREC_LEARNED; }
+static std::tuple<int, int, int, int, int> tile_key(int prec, const f64::StageArgs& A) {
+    return std::make_tuple(prec, A.tune_class, A.nx, A.ny, A.nz);
+}
+static void record(bsn_ctx* ctx, int prec, const f64::StageArgs& A, int code) {
+    ctx->tile_choice[tile_key(prec, A)] = code;
+    ctx->tile_last[std::make_tuple(prec, A.nx, A.ny, A.nz)] = code;
+}
+
+int tile_code(bsn_ctx* ctx, int prec, const f64::StageArgs& A) {
+    auto it = ctx->tile_choice.find(tile_key(prec, A));
+    return it == ctx->tile_choice.end() ? -1 : it->second;
+}
 
 bsn_status stage_autotune(bsn_ctx* ctx, int prec, const f64::StageArgs& probe, double* scratch) {
     if (prec == PREC_LEARNED) {   // the split learned stage's block list, allocated before any capture
@@ -52,11 +65,13 @@ bsn_status stage_autotune(bsn_ctx* ctx, int prec, const f64::StageArgs& probe, d
         slot(ctx, SLOT_SPLIT, learned_split_bytes(probe.nx, probe.ny, probe.nz), &st);
         BSN_TRY(st);
     }
-    auto key = std::make_tuple(prec, probe.nx, probe.ny, probe.nz);
-    if (ctx->tile_choice.count(key)) return BSN_OK;
+    const auto key = tile_key(prec, probe);
+    if (ctx->tile_choice.count(key) && (probe.tune_class != ctx->retime_class || ctx->retimed.count(key)))
+        return BSN_OK;
+    if (probe.tune_class == ctx->retime_class) ctx->retimed.insert(key);
     int nv = variant_count(prec);
     if (ctx->forced_tile[prec] >= 0) {
-        ctx->tile_choice[key] = forced_code(ctx, prec);
+        record(ctx, prec, probe, forced_code(ctx, prec));
         return BSN_OK;
     }
     f64::StageArgs a = probe;
@@ -104,13 +119,26 @@ bsn_status stage_autotune(bsn_ctx* ctx, int prec, const f64::StageArgs& probe, d
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     BSN_TRY(st);
-    ctx->tile_choice[key] = best;
+    record(ctx, prec, probe, best);
     return BSN_OK;
 }
 
+bool tile_settled(bsn_ctx* ctx, int tune_class, int prec) {
+    return ctx->forced_tile[prec] >= 0 || ctx->settled.count(std::make_pair(tune_class, prec)) > 0;
+}
+
+bsn_status tile_retime(bsn_ctx* ctx, int tune_class, int prec, const std::function<bsn_status()>& tune) {
+    ctx->retime_class = tune_class;
+    ctx->retimed.clear();
+    bsn_status st = tune();
+    ctx->retime_class = -1;
+    ctx->retimed.clear();
+    if (st == BSN_OK) ctx->settled.insert(std::make_pair(tune_class, prec));
+    return st;
+}
+
 bsn_status stage_launch(bsn_ctx* ctx, int prec, const f64::StageArgs& A) {
-    auto key = std::make_tuple(prec, A.nx, A.ny, A.nz);
-    auto it = ctx->tile_choice.find(key);
+    auto it = ctx->tile_choice.find(tile_key(prec, A));
     if (it == ctx->tile_choice.end()) {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         cudaStreamIsCapturing(ctx->stream, &cs);
@@ -121,7 +149,7 @@ bsn_status stage_launch(bsn_ctx* ctx, int prec, const f64::StageArgs& A) {
         double* scratch = (double*)slot(ctx, SLOT_UN, sizeof(double) * (size_t)G.nelem(), &st);
         BSN_TRY(st);
         BSN_TRY(stage_autotune(ctx, prec, A, scratch));
-        it = ctx->tile_choice.find(key);
+        it = ctx->tile_choice.find(tile_key(prec, A));
     }
     return launch_variant(ctx, prec, it->second, A);
 }
@@ -129,8 +157,7 @@ bsn_status stage_launch(bsn_ctx* ctx, int prec, const f64::StageArgs& A) {
 // The variant of a batch is the one chosen for its last level's grid (for
 // two-level FMR the fine level, the larger share of the work per step).
 static bsn_status choose(bsn_ctx* ctx, int prec, const f64::StageArgs& A, int& v) {
-    auto key = std::make_tuple(prec, A.nx, A.ny, A.nz);
-    auto it = ctx->tile_choice.find(key);
+    auto it = ctx->tile_choice.find(tile_key(prec, A));
     if (it != ctx->tile_choice.end()) { v = it->second & (kTmaBit - 1); return BSN_OK; }
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(ctx->stream, &cs);
@@ -143,7 +170,7 @@ static bsn_status choose(bsn_ctx* ctx, int prec, const f64::StageArgs& A, int& v
     double* scratch = (double*)slot(ctx, SLOT_UN, sizeof(double) * (size_t)G.nelem(), &st);
     BSN_TRY(st);
     BSN_TRY(stage_autotune(ctx, prec, A, scratch));
-    v = ctx->tile_choice[key] & (kTmaBit - 1);   // several grids in one launch: the plain loader
+    v = ctx->tile_choice[tile_key(prec, A)] & (kTmaBit - 1);   // several grids in one launch: the plain loader
     return BSN_OK;
 }
 
@@ -165,13 +192,17 @@ extern "C" bsn_status bsn_ctx_set_tile(bsn_ctx* ctx, int precision, int variant)
     ctx->forced_tile[precision] = variant < 0 ? -1 : variant;
     for (auto it = ctx->tile_choice.begin(); it != ctx->tile_choice.end();)
         it = std::get<0>(it->first) == precision ? ctx->tile_choice.erase(it) : std::next(it);
+    for (auto it = ctx->tile_last.begin(); it != ctx->tile_last.end();)
+        it = std::get<0>(it->first) == precision ? ctx->tile_last.erase(it) : std::next(it);
+    for (auto it = ctx->settled.begin(); it != ctx->settled.end();)
+        it = it->second == precision ? ctx->settled.erase(it) : std::next(it);
     return BSN_OK;
 }
 
 extern "C" bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int ny, int nz, int out[5]) {
     if (!ctx || !out) return BSN_ERR_ARG;
-    auto it = ctx->tile_choice.find(std::make_tuple(precision, nx, ny, nz));
-    if (it == ctx->tile_choice.end()) return set_err(ctx, BSN_ERR_ARG, "no tile chosen yet for this grid");
+    auto it = ctx->tile_last.find(std::make_tuple(precision, nx, ny, nz));
+    if (it == ctx->tile_last.end()) return set_err(ctx, BSN_ERR_ARG, "no tile chosen yet for this grid");
     if (!prec_ok(precision)) return set_err(ctx, BSN_ERR_ARG, "bad precision %d", precision);
     TileVariant v = variant(precision, it->second & (kTmaBit - 1));
     out[0] = v.tx; out[1] = v.ty; out[2] = v.tz; out[3] = v.nt; out[4] = v.minb;
@@ -180,8 +211,8 @@ extern "C" bsn_status bsn_ctx_get_tile(bsn_ctx* ctx, int precision, int nx, int 
 
 extern "C" int bsn_ctx_get_tile_tma(bsn_ctx* ctx, int precision, int nx, int ny, int nz) {
     if (!ctx) return -1;
-    auto it = ctx->tile_choice.find(std::make_tuple(precision, nx, ny, nz));
-    if (it == ctx->tile_choice.end()) return -1;
+    auto it = ctx->tile_last.find(std::make_tuple(precision, nx, ny, nz));
+    if (it == ctx->tile_last.end()) return -1;
     return (it->second & kTmaBit) ? 1 : 0;
 }
 

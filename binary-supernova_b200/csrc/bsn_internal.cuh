@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <map>
+#include <set>
 #include <tuple>
 #include <string>
 #include <vector>
@@ -32,8 +33,16 @@ struct bsn_ctx {
     cudaEvent_t pending_start = nullptr;
     struct Rec { std::string name; cudaEvent_t a, b; };
     std::vector<Rec> recs;
-    // stage-kernel tile choice per (precision, nx, ny, nz): autotuned or forced
-    std::map<std::tuple<int, int, int, int>, int> tile_choice;
+    // stage-kernel tile choice per (precision, driver class, nx, ny, nz):
+    // autotuned or forced; tile_last: the latest choice per (precision, nx, ny, nz)
+    std::map<std::tuple<int, int, int, int, int>, int> tile_choice;
+    std::map<std::tuple<int, int, int, int>, int> tile_last;
+    // re-timing pass of a device loop (tile_retime, autotune.cu): the driver
+    // class whose choices are re-timed (-1: none), the grids re-timed so far,
+    // and the (driver class, precision) pairs whose choices are settled
+    int retime_class = -1;
+    std::set<std::tuple<int, int, int, int, int>> retimed;
+    std::set<std::pair<int, int>> settled;
     int forced_tile[3] = {-1, -1, -1};
     void* learned_state = nullptr;   // learned.cu: packed network parameters
     // graph-captured device time loop (run_steps.cu)

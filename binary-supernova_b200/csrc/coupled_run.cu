@@ -332,11 +332,7 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
     base.x0 = x0; base.y0 = y0; base.z0 = z0;
     base.Uin = U; base.Un = U;
     base.stiff_guard = 1;   // near-vacuum cells beside the sinks: stiff FP32 faces in FP64
-    {
-        double* scratch = (double*)slot(ctx, SLOT_UN, bytes, &st); BSN_TRY(st);
-        BSN_TRY(stage_autotune(ctx, precision, base, scratch));
-    }
-    const int variant = ctx->tile_choice[std::make_tuple(precision, nx, ny, nz)];
+    base.tune_class = TUNE_COUPLED;
 
     // BHs to the device (through the context's pinned buffer, sized once for the
     // whole call: BH staging now, the step counters and flags later), initial CFL fold
@@ -349,6 +345,27 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
     BSN_TRY(launch_check(ctx, "coupled_init_kernel"));
     BSN_TRY(f64_cfl_fold(ctx, U, nx, ny, nz, dx, dx, dx, gamma, &r->smax, &r->nanflag));
 
+    // tile choice before any capture, timed on stage-1 work with this loop's
+    // sources (the step graph fills them again; Phi is recomputed every stage)
+    auto tune = [&]() -> bsn_status {
+        f64::StageArgs p = base;
+        if (nbh > 0) {
+            fill_kernel<<<1, 32, 0, ctx->stream>>>(r, f_sink, torque_free, rho_sink_min, t_bh2_sink_on);
+            BSN_TRY(launch_check(ctx, "coupled_fill_kernel"));
+            p.use_bh = 1; p.bh_dev = &r->bsrc; p.use_sink = 1; p.sk_dev = &r->ssrc;
+        }
+        if (self_gravity) {
+            if (precision == PREC_F64) BSN_TRY(poisson_from_state(ctx, U, nx, ny, nz, dx, dx, dx, rho_floor, phi));
+            else BSN_TRY(poisson_from_state_f32(ctx, U, nx, ny, nz, dx, dx, dx, rho_floor, phi));
+            p.phi = phi; p.use_sg = 1;
+        }
+        bsn_status ts;
+        double* scratch = (double*)slot(ctx, SLOT_UN, bytes, &ts); BSN_TRY(ts);
+        return stage_autotune(ctx, precision, p, scratch);
+    };
+    BSN_TRY(tune());
+    int variant = tile_code(ctx, precision, base);
+
     if (!ctx->coupled_run_state) ctx->coupled_run_state = new State();
     State* S = (State*)ctx->coupled_run_state;
     const void* ptrs[7] = {A, B, r, part, phi, diag_out, dpart};
@@ -359,7 +376,7 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
                 S->f_sink == f_sink && S->rho_floor == rho_floor && S->P_floor == P_floor &&
                 S->t_on == t_bh2_sink_on && S->rho_min == rho_sink_min && S->t_end == t_end &&
                 S->diag_cap == diag_cap && memcmp(S->ptrs, ptrs, sizeof(ptrs)) == 0;
-    if (!same) {
+    auto capture = [&]() -> bsn_status {
         S->release();
         if (!S->cap) BSN_CUDA(ctx, cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
         bool prof = ctx->profiling;
@@ -438,9 +455,22 @@ extern "C" bsn_status bsn_coupled_run_steps(bsn_ctx* ctx, double* U, bsn_bh* bhs
         S->t_end = t_end;
         S->diag_cap = diag_cap;
         memcpy(S->ptrs, ptrs, sizeof(ptrs));
-    }
-    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps, t_end > 0.0, &r->done, S->ev,
+        return BSN_OK;
+    };
+    if (!same) BSN_TRY(capture());
+    const bool settle = n_steps >= 2 && !tile_settled(ctx, TUNE_COUPLED, precision);
+    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, settle ? 1 : n_steps, t_end > 0.0, &r->done, S->ev,
                          (volatile int*)((char*)h + sizeof(Dev))));
+    if (settle) {   // the tile re-timed on the state after the first step
+        BSN_TRY(tile_retime(ctx, TUNE_COUPLED, precision, tune));
+        if (tile_code(ctx, precision, base) != variant) {
+            variant = tile_code(ctx, precision, base);
+            BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            BSN_TRY(capture());
+        }
+        BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps - 1, t_end > 0.0, &r->done, S->ev,
+                             (volatile int*)((char*)h + sizeof(Dev))));
+    }
     BSN_CUDA(ctx, cudaMemcpyAsync(h, r, sizeof(Dev), cudaMemcpyDeviceToHost, ctx->stream));
     BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     Dev d;
@@ -529,20 +559,13 @@ extern "C" bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2*
         if (nbh > 0) { a.use_bh = 1; a.bh_dev = &r->bsrc; a.use_sink = 1; a.sk_dev = &r->ssrc; }
         plan.led_raw[l] = &r->led[l][0][0];
         a.stiff_guard = 1;
+        a.tune_class = TUNE_NESTED;
     }
     plan.led_tot = r->led_tot;
     if (self_gravity) {
         const NLevel& v = plan.L[0];
         if (precision == PREC_F64) BSN_TRY(poisson_prepare(ctx, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz));
         else BSN_TRY(poisson_prepare_f32(ctx, v.nx, v.ny, v.nz, v.dx, v.dy, v.dz));
-    }
-    int tiles[NMAXL] = {-1, -1, -1, -1};
-    for (int l = 0; l < nl; ++l) {
-        f64::StageArgs p = plan.base[l];
-        p.Uin = plan.L[l].U; p.dt_dev = nullptr; p.done_dev = nullptr; p.use_reg = 0; p.use_bnd = 0; p.Gh = nullptr;
-        p.use_bh = 0; p.use_sink = 0; p.bh_dev = nullptr; p.sk_dev = nullptr;
-        BSN_TRY(stage_autotune(ctx, precision, p, plan.L[l].A));
-        tiles[l] = ctx->tile_choice[std::make_tuple(precision, plan.L[l].nx, plan.L[l].ny, plan.L[l].nz)];
     }
     // BHs to the device through the pinned buffer, then both records initialised
     double* h = (double*)pinned(ctx, sizeof(Dev) + sizeof(NDev) + 128, &st); BSN_TRY(st);
@@ -554,6 +577,23 @@ extern "C" bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2*
     BSN_TRY(launch_check(ctx, "coupled_init_kernel"));
     n_init_kernel<<<1, 1, 0, ctx->stream>>>(plan.d, *t_inout);
     BSN_TRY(launch_check(ctx, "fmrN_init_kernel"));
+    // tile choices before any capture (the autotuner launches and times), on
+    // stage-1 work with the loop's BH sources (filled again by the step graph)
+    int tiles[NMAXL] = {-1, -1, -1, -1};
+    auto tune = [&]() -> bsn_status {
+        if (nbh > 0) {
+            fill_kernel<<<1, 32, 0, ctx->stream>>>(r, f_sink, torque_free, rho_sink_min, t_bh2_sink_on);
+            BSN_TRY(launch_check(ctx, "coupled_fill_kernel"));
+        }
+        for (int l = 0; l < nl; ++l) {
+            f64::StageArgs p = plan.base[l];
+            p.Uin = plan.L[l].U; p.dt_dev = nullptr; p.done_dev = nullptr; p.use_reg = 0; p.use_bnd = 0; p.Gh = nullptr;
+            BSN_TRY(stage_autotune(ctx, precision, p, plan.L[l].A));
+        }
+        for (int l = 0; l < nl; ++l) tiles[l] = tile_code(ctx, precision, plan.base[l]);
+        return BSN_OK;
+    };
+    BSN_TRY(tune());
 
     const NLevel& fin = plan.L[nl - 1];
     std::vector<double> extra = {(double)nbh, x0, y0, z0, dt_max, f_sink, (double)torque_free, t_bh2_sink_on,
@@ -564,7 +604,7 @@ extern "C" bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2*
                 memcmp(S->key_pairs.data(), pairs, sizeof(bsn_fmr2) * npairs) == 0 && S->prec == precision &&
                 S->sg == self_gravity && S->cfl == cfl && S->t_end == t_end &&
                 memcmp(S->tiles, tiles, sizeof(tiles)) == 0 && S->key_base == S->arena.base && S->key_extra == extra;
-    if (!same) {
+    auto capture = [&]() -> bsn_status {
         S->release();
         if (!S->cap) BSN_CUDA(ctx, cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
         bool prof = ctx->profiling;
@@ -642,9 +682,21 @@ extern "C" bsn_status bsn_coupled_nested_run_steps(bsn_ctx* ctx, const bsn_fmr2*
         memcpy(S->tiles, tiles, sizeof(tiles));
         S->key_base = S->arena.base;
         S->key_extra = extra;
-    }
-    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps, t_end > 0.0, plan.done, S->ev,
+        return BSN_OK;
+    };
+    if (!same) BSN_TRY(capture());
+    const bool settle = n_steps >= 2 && !tile_settled(ctx, TUNE_NESTED, precision);
+    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, settle ? 1 : n_steps, t_end > 0.0, plan.done, S->ev,
                          (volatile int*)((char*)h + sizeof(Dev) + sizeof(NDev))));
+    if (settle) {   // the tiles re-timed on the state after the first step
+        BSN_TRY(tile_retime(ctx, TUNE_NESTED, precision, tune));
+        if (memcmp(S->tiles, tiles, sizeof(tiles)) != 0) {
+            BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            BSN_TRY(capture());
+        }
+        BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps - 1, t_end > 0.0, plan.done, S->ev,
+                             (volatile int*)((char*)h + sizeof(Dev) + sizeof(NDev))));
+    }
     NDev* hn = (NDev*)((char*)h + sizeof(Dev));
     BSN_CUDA(ctx, cudaMemcpyAsync(h, r, sizeof(Dev), cudaMemcpyDeviceToHost, ctx->stream));
     BSN_CUDA(ctx, cudaMemcpyAsync(hn, plan.d, sizeof(NDev), cudaMemcpyDeviceToHost, ctx->stream));

@@ -536,6 +536,7 @@ bsn_status fmr3d_run(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int prec, int 
         cb.reg.t1[d] = G.hi[d] - 1;
     }
     if (self_gravity) { cb.use_sg = 1; cb.phi = phic; }
+    cb.tune_class = TUNE_FMR;
     cb.dt_dev = &rd->dt;
     cb.done_dev = &rd->done;
     stage_args_init(fb, g->nfx, g->nfy, g->nfz, g->dxf, g->dyf, g->dzf, g->gamma, g->bc, g->rho_floor, g->P_floor); fb.stiff_guard = ctx->stiff_guard;
@@ -543,21 +544,24 @@ bsn_status fmr3d_run(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int prec, int 
     fb.use_bnd = 1;
     for (int i = 0; i < 6; ++i) fb.bnd.f[i] = const_cast<double*>(R.f.bnd[i]);
     if (self_gravity) { fb.use_sg = 1; fb.phi = phif; }
+    fb.tune_class = TUNE_FMR;
     fb.dt_dev = &rd->dtf;
     fb.done_dev = &rd->done;
 
     // tile choices before any capture (the autotuner launches and times)
-    {
-        double* scratch = (double*)slot(ctx, SLOT_UN, sizeof(double) * std::max(C.nelem(), F.nelem()), &st);
-        BSN_TRY(st);
+    auto tune = [&]() -> bsn_status {
+        bsn_status ts;
+        double* scratch = (double*)slot(ctx, SLOT_UN, sizeof(double) * std::max(C.nelem(), F.nelem()), &ts);
+        BSN_TRY(ts);
         f64::StageArgs pc = cb, pf = fb;
         pc.Uin = g->Uc; pc.dt_dev = nullptr; pc.done_dev = nullptr; pc.use_reg = 0;
         pf.Uin = g->Uf; pf.dt_dev = nullptr; pf.done_dev = nullptr; pf.use_bnd = 0; pf.Gh = nullptr;
         BSN_TRY(stage_autotune(ctx, prec, pc, scratch));
-        BSN_TRY(stage_autotune(ctx, prec, pf, scratch));
-    }
-    const int vc = ctx->tile_choice[std::make_tuple(prec, g->ncx, g->ncy, g->ncz)];
-    const int vf = ctx->tile_choice[std::make_tuple(prec, g->nfx, g->nfy, g->nfz)];
+        return stage_autotune(ctx, prec, pf, scratch);
+    };
+    BSN_TRY(tune());
+    int vc = tile_code(ctx, prec, cb);
+    int vf = tile_code(ctx, prec, fb);
 
     run_init_kernel<<<1, 1, 0, ctx->stream>>>(rd, *t_inout);
     BSN_TRY(launch_check(ctx, "fmr_run_init_kernel"));
@@ -568,7 +572,7 @@ bsn_status fmr3d_run(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int prec, int 
     bool same = S->exec && memcmp(&S->g, g, sizeof(bsn_fmr2)) == 0 && S->prec == prec && S->sg == self_gravity &&
                 S->G_grav == G_grav && S->cfl == cfl && S->t_end == t_end && S->vc == vc && S->vf == vf &&
                 memcmp(S->ptrs, ptrs, sizeof(ptrs)) == 0;
-    if (!same) {
+    auto capture = [&]() -> bsn_status {
         S->release();
         if (!S->cap) BSN_CUDA(ctx, cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
         bool prof = ctx->profiling;
@@ -674,9 +678,24 @@ bsn_status fmr3d_run(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int prec, int 
         S->g = *g; S->prec = prec; S->sg = self_gravity; S->G_grav = G_grav; S->cfl = cfl; S->t_end = t_end;
         S->vc = vc; S->vf = vf;
         memcpy(S->ptrs, ptrs, sizeof(ptrs));
-    }
+        return BSN_OK;
+    };
+    if (!same) BSN_TRY(capture());
     double* h = (double*)pinned(ctx, 128, &st); BSN_TRY(st);
-    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps, t_end > 0.0, &rd->done, S->ev, (volatile int*)(h + 8)));
+    const bool settle = n_steps >= 2 && !tile_settled(ctx, TUNE_FMR, prec);
+    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, settle ? 1 : n_steps, t_end > 0.0, &rd->done, S->ev,
+                         (volatile int*)(h + 8)));
+    if (settle) {   // the tiles re-timed on the state after the first step
+        BSN_TRY(tile_retime(ctx, TUNE_FMR, prec, tune));
+        if (tile_code(ctx, prec, cb) != vc || tile_code(ctx, prec, fb) != vf) {
+            vc = tile_code(ctx, prec, cb);
+            vf = tile_code(ctx, prec, fb);
+            BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            BSN_TRY(capture());
+        }
+        BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps - 1, t_end > 0.0, &rd->done, S->ev,
+                             (volatile int*)(h + 8)));
+    }
     BSN_CUDA(ctx, cudaMemcpyAsync(h, rd, sizeof(RunDev), cudaMemcpyDeviceToHost, ctx->stream));
     BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     RunDev d;

@@ -363,12 +363,17 @@ bsn_status fmrN_run(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, double cfl,
     }
     // tile choices before any capture (the autotuner launches and times)
     int tiles[NMAXL] = {-1, -1, -1, -1};
-    for (int l = 0; l < plan.nl; ++l) {
-        f64::StageArgs p = plan.base[l];
-        p.Uin = plan.L[l].U; p.dt_dev = nullptr; p.done_dev = nullptr; p.use_reg = 0; p.use_bnd = 0; p.Gh = nullptr;
-        BSN_TRY(stage_autotune(ctx, prec, p, plan.L[l].A));
-        tiles[l] = ctx->tile_choice[std::make_tuple(prec, plan.L[l].nx, plan.L[l].ny, plan.L[l].nz)];
-    }
+    for (int l = 0; l < plan.nl; ++l) plan.base[l].tune_class = TUNE_FMR_N;
+    auto tune = [&]() -> bsn_status {
+        for (int l = 0; l < plan.nl; ++l) {
+            f64::StageArgs p = plan.base[l];
+            p.Uin = plan.L[l].U; p.dt_dev = nullptr; p.done_dev = nullptr; p.use_reg = 0; p.use_bnd = 0; p.Gh = nullptr;
+            BSN_TRY(stage_autotune(ctx, prec, p, plan.L[l].A));
+        }
+        for (int l = 0; l < plan.nl; ++l) tiles[l] = tile_code(ctx, prec, plan.base[l]);
+        return BSN_OK;
+    };
+    BSN_TRY(tune());
     n_init_kernel<<<1, 1, 0, ctx->stream>>>(plan.d, *t_inout);
     BSN_TRY(launch_check(ctx, "fmrN_init_kernel"));
 
@@ -376,7 +381,7 @@ bsn_status fmrN_run(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, double cfl,
                 memcmp(S->key_pairs.data(), pairs, sizeof(bsn_fmr2) * npairs) == 0 && S->prec == prec &&
                 S->sg == sg && S->G_grav == G_grav && S->cfl == cfl && S->t_end == t_end &&
                 memcmp(S->tiles, tiles, sizeof(tiles)) == 0 && S->key_base == S->arena.base;
-    if (!same) {
+    auto capture = [&]() -> bsn_status {
         S->release();
         if (!S->cap) BSN_CUDA(ctx, cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
         bool prof = ctx->profiling;
@@ -413,10 +418,23 @@ bsn_status fmrN_run(bsn_ctx* ctx, const bsn_fmr2* pairs, int npairs, double cfl,
         S->prec = prec; S->sg = sg; S->G_grav = G_grav; S->cfl = cfl; S->t_end = t_end;
         memcpy(S->tiles, tiles, sizeof(tiles));
         S->key_base = S->arena.base;
-    }
+        return BSN_OK;
+    };
+    if (!same) BSN_TRY(capture());
     bsn_status st;
     double* h = (double*)pinned(ctx, 128 + sizeof(NDev), &st); BSN_TRY(st);
-    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps, t_end > 0.0, plan.done, S->ev, (volatile int*)(h + 8)));
+    const bool settle = n_steps >= 2 && !tile_settled(ctx, TUNE_FMR_N, prec);
+    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, settle ? 1 : n_steps, t_end > 0.0, plan.done, S->ev,
+                         (volatile int*)(h + 8)));
+    if (settle) {   // the tiles re-timed on the state after the first step
+        BSN_TRY(tile_retime(ctx, TUNE_FMR_N, prec, tune));
+        if (memcmp(S->tiles, tiles, sizeof(tiles)) != 0) {
+            BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            BSN_TRY(capture());
+        }
+        BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps - 1, t_end > 0.0, plan.done, S->ev,
+                             (volatile int*)(h + 8)));
+    }
     NDev* hd = (NDev*)(h + 16);
     BSN_CUDA(ctx, cudaMemcpyAsync(hd, plan.d, sizeof(NDev), cudaMemcpyDeviceToHost, ctx->stream));
     BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

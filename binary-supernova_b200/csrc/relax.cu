@@ -144,13 +144,14 @@ extern "C" bsn_status bsn_relax_ic(bsn_ctx* ctx, double* U, int nx, int ny, int 
     base.damp_t = t_damp;
     base.damp_inv_td = 1.0 / t_damp;
     base.damp_omega = 0.0;
+    base.tune_class = TUNE_RELAX;
     {
         f64::StageArgs p = base;
         p.Uin = U;
         double* scratch = (double*)slot(ctx, SLOT_UN, bytes, &st); BSN_TRY(st);
         BSN_TRY(stage_autotune(ctx, precision, p, scratch));
     }
-    const int variant = ctx->tile_choice[std::make_tuple(precision, nx, ny, nz)];
+    const int variant = tile_code(ctx, precision, base);
 
     init_kernel<<<1, 1, 0, ctx->stream>>>(r);
     BSN_TRY(launch_check(ctx, "relax_init_kernel"));

@@ -218,12 +218,15 @@ extern "C" bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int
     base.Uin = U; base.Un = U;
     base.learned_split = 1;   // a uniform grid: mostly uniform blocks away from the flow's features
     base.stiff_guard = ctx->stiff_guard;
+    base.tune_class = TUNE_RUN;
     // autotune before any capture (it launches and times kernels)
-    {
-        double* scratch = (double*)slot(ctx, SLOT_UN, bytes, &st); BSN_TRY(st);
-        BSN_TRY(stage_autotune(ctx, precision, base, scratch));
-    }
-    int variant = ctx->tile_choice[std::make_tuple(precision, nx, ny, nz)];
+    auto tune = [&]() -> bsn_status {
+        bsn_status ts;
+        double* scratch = (double*)slot(ctx, SLOT_UN, bytes, &ts); BSN_TRY(ts);
+        return stage_autotune(ctx, precision, base, scratch);
+    };
+    BSN_TRY(tune());
+    int variant = tile_code(ctx, precision, base);
 
     init_kernel<<<1, 1, 0, ctx->stream>>>(r, *t_inout);
     BSN_TRY(launch_check(ctx, "run_init_kernel"));
@@ -233,7 +236,7 @@ extern "C" bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int
                 S->dz == dz && S->gamma == gamma && S->cfl == cfl && S->bc == bc && S->rho_floor == rho_floor &&
                 S->P_floor == P_floor && S->prec == precision && S->t_end == t_end && S->variant == variant &&
                 S->A == A && S->B == B && S->r == r;
-    if (!same) {
+    auto capture = [&]() -> bsn_status {
         release(S);
         if (!S->cap) BSN_CUDA(ctx, cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
         // everything enqueued so far (init, CFL fold) happens before the first replay on ctx->stream
@@ -278,10 +281,24 @@ extern "C" bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int
         S->U = U; S->nx = nx; S->ny = ny; S->nz = nz; S->dx = dx; S->dy = dy; S->dz = dz; S->gamma = gamma;
         S->cfl = cfl; S->bc = bc; S->rho_floor = rho_floor; S->P_floor = P_floor; S->prec = precision;
         S->t_end = t_end; S->variant = variant; S->A = A; S->B = B; S->r = r;
-    }
+        return BSN_OK;
+    };
+    if (!same) BSN_TRY(capture());
     double* h = (double*)pinned(ctx, 128, &st); BSN_TRY(st);
     // replays after t_end are no-ops: with t_end, stop once the device says done
-    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps, t_end > 0.0, &r->done, S->flag_ev, (volatile int*)(h + 8)));
+    const bool settle = n_steps >= 2 && !tile_settled(ctx, TUNE_RUN, precision);
+    BSN_TRY(graph_replay(ctx, S->exec, S->kernels, settle ? 1 : n_steps, t_end > 0.0, &r->done, S->flag_ev,
+                         (volatile int*)(h + 8)));
+    if (settle) {   // the tile re-timed on the state after the first step
+        BSN_TRY(tile_retime(ctx, TUNE_RUN, precision, tune));
+        if (tile_code(ctx, precision, base) != variant) {
+            variant = tile_code(ctx, precision, base);
+            BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            BSN_TRY(capture());
+        }
+        BSN_TRY(graph_replay(ctx, S->exec, S->kernels, n_steps - 1, t_end > 0.0, &r->done, S->flag_ev,
+                             (volatile int*)(h + 8)));
+    }
     BSN_CUDA(ctx, cudaMemcpyAsync(h, r, sizeof(Dev), cudaMemcpyDeviceToHost, ctx->stream));
     BSN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     Dev d;

@@ -95,6 +95,10 @@ struct StageArgs {
     int k0;
     const double* phi_lo;
     const double* phi_hi;
+    // the driver loop this stage belongs to (TUNE_* in stage_launch.cuh): the
+    // autotuner keeps one tile choice per driver and grid, so a driver's
+    // choice is timed on its own stage arguments and grid contents
+    int tune_class;
 };
 
 enum { LED_BND = 0, LED_DRAIN = 1, LED_POST = 2, LED_PRE = 3, LED_TERMS = 4 };

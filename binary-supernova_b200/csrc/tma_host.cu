@@ -106,6 +106,8 @@ extern "C" bsn_status bsn_ctx_set_tma(bsn_ctx* ctx, int on) {
     coupled_nested_state_free(ctx);
     relax_state_free(ctx);
     ctx->tile_choice.clear();
+    ctx->tile_last.clear();
+    ctx->settled.clear();
     return BSN_OK;
 }
 
