@@ -46,6 +46,10 @@ static bsn_status launch_batch_variant(bsn_ctx* ctx, int prec, int idx, const f6
     return learned_launch_batch_variant(ctx, idx, B);
 }
 static bool prec_ok(int p) { return p == PREC_F64 || p == PREC_F32 || p == PREC_LEARNED; }
+// Drivers whose stages run in batched launches over several grids: the batch
+// kernel has no TMA form, so their choices are timed with the plain loader only
+// (a TMA variant timed alone can win and then run plain, and slower, in the batch).
+static bool batched_class(int c) { return c == TUNE_FMR || c == TUNE_FMR_N || c == TUNE_NESTED; }
 static std::tuple<int, int, int, int, int> tile_key(int prec, const f64::StageArgs& A) {
     return std::make_tuple(prec, A.tune_class, A.nx, A.ny, A.nz);
 }
@@ -97,7 +101,7 @@ bsn_status stage_autotune(bsn_ctx* ctx, int prec, const f64::StageArgs& probe, d
     ctx->profiling = false;
     bsn_status st = BSN_OK;
     for (int v = 0; v < nv && st == BSN_OK; ++v) {
-        for (int tma = 0; tma < (ctx->tma_on ? 2 : 1) && st == BSN_OK; ++tma) {
+        for (int tma = 0; tma < (ctx->tma_on && !batched_class(probe.tune_class) ? 2 : 1) && st == BSN_OK; ++tma) {
             const int code = v | (tma ? kTmaBit : 0);
             st = launch_variant(ctx, prec, code, a);   // warm-up (sets smem attributes)
             if (st != BSN_OK) break;
