@@ -351,7 +351,9 @@ extern "C" bsn_status bsn_euler3d_rhs_f64(bsn_ctx* ctx, double* dU, double* Fx, 
     A.dU = dU;
     A.F[0] = Fx; A.F[1] = Fy; A.F[2] = Fz;
     A.mode = 1;
-    return f64_launch_stage(ctx, A);
+    BSN_TRY(f64_launch_stage(ctx, A));
+    // euler3d_rhs! floors U in place; the stage kernel floored its staged copies
+    return f64_floors(ctx, U, nx, ny, nz, rho_floor, P_floor, gamma);
 }
 
 extern "C" bsn_status bsn_euler3d_step_f64(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double dx, double dy,

@@ -176,7 +176,9 @@ extern "C" bsn_status bsn_euler3d_rhs_f32(bsn_ctx* ctx, double* dU, double* Fx, 
     A.F[0] = Fx; A.F[1] = Fy; A.F[2] = Fz;
     A.mode = 1;
     A.stiff_guard = ctx->stiff_guard;
-    return stage_launch(ctx, PREC_F32, A);
+    BSN_TRY(stage_launch(ctx, PREC_F32, A));
+    // euler3d_rhs! floors U in place; the stage kernel floored its staged copies
+    return f64_floors(ctx, U, nx, ny, nz, rho_floor, P_floor, gamma);
 }
 
 extern "C" bsn_status bsn_euler3d_step_f32(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double dx, double dy,

@@ -35,7 +35,7 @@ struct BndFaces {
 };
 
 struct StageArgs {
-    double* Uin;             // stage input (stencil source); written back in RHS mode
+    double* Uin;             // stage input (stencil source); floored after the launch in RHS mode
     const double* Gh;        // ghost source array (same layout); null -> boundary map of Uin
     const double* Un;        // combine base (stage mode)
     double* Uout;            // stage result (stage mode)

@@ -728,9 +728,12 @@ __device__ __forceinline__ bool stage_block(const f64::StageArgs& A, int a0, int
         if (A.use_rot) f64::rot_frame_src(d, u0, u1, u2, xc, yc, A.rot_omega);   // src/relax_ic.jl:150-176
         if (A.use_damp) f64::damp_src(d, u0, u1, u2, u3, xc, yc, A.damp_inv_td, A.damp_t, A.damp_omega);
         if (A.mode == 1) {
+            // Uin is not written here: other blocks are still staging these
+            // cells as halos, and a cell read while its five words were being
+            // replaced by their floored values would mix the two states.  The
+            // RHS entry points floor Uin in a launch of its own afterwards.
 #pragma unroll
             for (int q = 0; q < 5; ++q) A.dU[off + q] = d[q];
-            A.Uin[off + 0] = u0; A.Uin[off + 1] = u1; A.Uin[off + 2] = u2; A.Uin[off + 3] = u3; A.Uin[off + 4] = u4;
             continue;
         }
         double un[5], w[5];

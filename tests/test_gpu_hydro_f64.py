@@ -56,6 +56,39 @@ def test_euler3d_rhs(orc, bsn, n, bc):
     assert_bitwise(host(Fzd), Fz, "Fz")
 
 
+def test_euler3d_rhs_with_many_floored_cells_is_deterministic(orc, bsn):
+    """euler3d_rhs! floors U in place; with thousands of blocks staging one
+    another's cells, U is floored only after the flux launch, so no block
+    stages a half-floored cell: every call equals the oracle (FP64) and the
+    FP32 right-hand side repeats bit for bit."""
+    n = (96, 80, 72)
+    U = random_state(*n, seed=31, vacuum=True)
+    rng = np.random.default_rng(32)
+    a = (slice(NG, -NG),) * 3
+    neg = rng.random(U[0][a].shape) < 0.15
+    U[0][a][neg] *= -1.0   # negative densities: the floors' first branch
+    orc.fill_ghost_3d_outflow(U)
+    d = (0.01, 0.011, 0.012)
+    kw = dict(rho_floor=1e-6, P_floor=1e-4)
+    Fo = orc.flux_arrays(*n)
+    dUo, Uo = np.zeros_like(U, order="F"), U.copy(order="F")
+    orc.euler3d_rhs(dUo, *Fo, Uo, *d, 1.4, fill_ghosts=False, **kw)
+    f32 = []
+    for _ in range(3):
+        Ud, dUd = dev(U), torch.zeros_like(dev(U))
+        Fd = [torch.zeros_like(dev(f)) for f in Fo]
+        bsn.euler3d_rhs(dUd, *Fd, Ud, *n, *d, 1.4, fill_ghosts=False, **kw)
+        assert_bitwise(host(Ud), Uo, "U after rhs")
+        assert_bitwise(host(dUd), dUo, "dU")
+        for f, g in zip(Fd, Fo):
+            assert_bitwise(host(f), g, "F")
+        U32, dU32 = dev(U), torch.zeros_like(dev(U))
+        bsn.euler3d_rhs_f32(dU32, None, None, None, U32, *n, *d, 1.4, fill_ghosts=False, **kw)
+        assert torch.equal(U32, Ud)
+        f32.append(dU32)
+    assert torch.equal(f32[0], f32[1]) and torch.equal(f32[0], f32[2])
+
+
 @pytest.mark.parametrize("n", SIZES)
 @pytest.mark.parametrize("bc", ["outflow", "periodic"])
 def test_euler3d_step_random(orc, bsn, n, bc):
