@@ -271,6 +271,79 @@ def slab_sedov(args, rank, world, log):
     return out
 
 
+def slab_fmr(args, rank, world, log):
+    """The two-level FMR polytrope (the fmr_polytrope workload: 128^3 base,
+    128^3 fine on [-1,1]^3, self-gravity) with the base grid in z-slabs over
+    the ranks and the fine level on rank 0 (bsn.shard_fmr: coarse stages per
+    slab with the register faces, the owner's window of the coarse grid, the
+    fine subcycles, restriction and correction, planes sent back), K FP64
+    steps timed with CUDA events (max over ranks); on a one-rank run the
+    graph-captured device loop (bsn_fmr3d_run_steps) beside it, from the same
+    state with the same dts, and the two results compared bit for bit."""
+    import torch
+    import bsn
+    from bsn import ics, shard, shard_fmr
+    nc, ratio, gam = 128, 2, 2.0
+    dxc = 4.0 / nc
+    lo, hi = 33, 96
+    kw = dict(rho_floor=1e-8, P_floor=1e-10)
+    U0 = bsn.state(nc, nc, nc)
+    ics.polytrope_ic_3d(U0, nc, nc, nc, dxc, dxc, dxc, gam, M_star=1.0, R_star=0.5, x0=-2.0, y0=-2.0, z0=-2.0,
+                        **kw)
+    bsn.fill_ghost_3d_outflow(U0, nc, nc, nc)
+    G = bsn.FMRGrid3D(U0.clone(), nc, nc, nc, dxc, lo, hi, lo, hi, lo, hi, ratio, gam, **kw)
+    slab = shard.Slab.split(nc, nc, nc, rank, world)
+    Us = bsn.state(nc, nc, slab.nz)
+    shard._zmajor(Us)[...] = shard._zmajor(U0)[slab.k0:slab.k0 + slab.nz + 2 * NG]
+    S = shard_fmr.SlabFMR(Us, slab, dxc, lo, hi, lo, hi, lo, hi, ratio, gam, shard.DeviceOps(), owner=0,
+                          Uf=G.Uf.clone(), **kw)
+    nf = (hi - lo + 1) * ratio
+    units = nc ** 3 + ratio * nf ** 3
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    dts = []
+    for _ in range(max(1, args.warmup)):
+        dt = S.cfl_dt(0.4)
+        dts.append(dt)
+        S.step(dt, self_gravity=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        dt = S.cfl_dt(0.4)
+        dts.append(dt)
+        S.step(dt, self_gravity=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    out = {"workload": "polytrope FMR 128^3 + 128^3 (ratio 2), self-gravity, base grid in z-slabs",
+           "ranks": world, "planes_per_rank": slab.nz, "steps": args.steps, "unit": "cell-updates/s",
+           "units_per_step": units, "f64_slab_ms_per_step": ms, "f64_slab_value": units / (ms / 1e3)}
+    log(f"slab FMR polytrope f64, {world} rank(s): {ms:.3f} ms/step")
+    if world == 1:   # the fused device step from the same state with the same dts
+        for dt in dts[:max(1, args.warmup)]:
+            bsn.fmr3d_step(G, dt, self_gravity=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for dt in dts[max(1, args.warmup):]:
+            bsn.fmr3d_step(G, dt, self_gravity=True)
+        e1.record()
+        torch.cuda.synchronize()
+        out["f64_fused_step_ms_per_step"] = e0.elapsed_time(e1) / args.steps
+        a = (slice(None),) + (slice(NG, -NG),) * 3
+        out["bitwise_equal_to_fused_step"] = bool(torch.equal(S.Uc[a], G.Uc[a]) and torch.equal(S.G.Uf[a], G.Uf[a]))
+        log(f"fused fmr3d_step: {out['f64_fused_step_ms_per_step']:.3f} ms/step, "
+            f"bitwise {out['bitwise_equal_to_fused_step']}")
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -892,7 +965,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-fmr", action="store_true",
                     help="skip the two-level FMR polytrope and binary-BH coupled-loop timings")
-    ap.add_argument("--workload", default="sedov", choices=["sedov", "binary_nested", "polytrope_fmr", "poisson", "slab"],
+    ap.add_argument("--workload", default="sedov", choices=["sedov", "binary_nested", "polytrope_fmr", "poisson", "slab",
+                                                     "slab_fmr"],
                     help="binary_nested: time only the binary-BH supernova on three nested FMR levels; "
                          "polytrope_fmr: only the two-level self-gravitating polytrope; "
                          "poisson: only the isolated Poisson solve at 128^3, --steps solves per precision; "
@@ -941,8 +1015,8 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        if args.workload == "slab":
-            out = slab_sedov(args, rank, world, log)
+        if args.workload in ("slab", "slab_fmr"):
+            out = (slab_sedov if args.workload == "slab" else slab_fmr)(args, rank, world, log)
             if rank == 0:
                 print(json.dumps(out), flush=True)
             return

@@ -165,6 +165,7 @@ SIGNATURES = {
     "bsn_cfl_dt_fmr3d_f64": (_I, [_V, _FMR, _D, _dp]),
     "bsn_restrict_density_to_coarse_f64": (_I, [_V, _FMR]),
     "bsn_solve_fmr_poisson_f64": (_I, [_V, _FMR, _P, _P]),
+    "bsn_prolong_scalar_trilinear_f64": (_I, [_V, _FMR, _P, _P]),
     "bsn_solve_poisson_isolated_f32": (_I, [_V, _P, _I, _I, _I, _D, _D, _D, _P]),
     "bsn_fmr3d_run_steps": (_I, [_V, _FMR, _D, _I, _I, _D, _I, _D, _dp, C.POINTER(C.c_int)]),
     "bsn_fmr_nested_step_f64": (_I, [_V, _FMR, _I, _D, _I, _D]),

@@ -550,6 +550,17 @@ class FMRGrid3D:
     def restrict(self):
         _call("bsn_fmr_restrict_f64", context(), _ptr(self.Uc), _ptr(self.Uf), C.byref(self.s))
 
+    def restrict_density_to_coarse(self):
+        _call("bsn_restrict_density_to_coarse_f64", context(), C.byref(self.s))
+
+    def prolong_scalar_trilinear(self, phic):
+        """_prolong_scalar_trilinear! (src/fmr_gravity.jl:70-106): the fine
+        level's potential from the coarse one (column-major active grids)."""
+        _check_grid(phic, *self.coarse_dims, "phic")
+        phif = active_grid(*self.fine_dims, device=phic.device)
+        _call("bsn_prolong_scalar_trilinear_f64", context(), C.byref(self.s), _ptr(phic), _ptr(phif))
+        return phif
+
 
 def fmr3d_step(G: FMRGrid3D, dt_c, *, self_gravity=False, G_grav=1.0):
     _call("bsn_fmr3d_step_f64", context(), C.byref(G.s), float(dt_c), int(bool(self_gravity)), float(G_grav))

@@ -36,6 +36,9 @@ sources per cell with the global plane index, the gas force on the BHs as an
 all-gather of the ranks' compensated partial sums merged in rank order, and
 accrete! as an ordered gather of the sink sphere's cell terms; with the orbit
 frozen it is the undivided step bit for bit.
+
+Two-level FMR over the same slabs (the refined patch on one rank) is in
+`bsn.shard_fmr`.
 """
 from __future__ import annotations
 
@@ -447,6 +450,28 @@ class DeviceOps:
     @staticmethod
     def assign(U, V):
         U.copy_(V)
+
+    def zeros(self, shape):
+        return torch.zeros(shape, dtype=torch.float64, device=self.device)
+
+    def state(self, nx, ny, nz):
+        return self.api.state(nx, ny, nz, device=self.device)
+
+    def active(self, nx, ny, nz):
+        return self.api.active_grid(nx, ny, nz, device=self.device)
+
+    def flux_arrays(self, nx, ny, nz):
+        return self.api.flux_arrays(nx, ny, nz, device=self.device)
+
+    def rhs_fluxes(self, dU, Fx, Fy, Fz, U, nx, ny, nz, dx, dy, dz, gamma, bc, rho_floor, P_floor):
+        """euler3d_rhs! without its ghost fill, keeping the face fluxes."""
+        self.api.euler3d_rhs(dU, Fx, Fy, Fz, U, nx, ny, nz, dx, dy, dz, gamma, bc=bc, rho_floor=rho_floor,
+                             P_floor=P_floor, fill_ghosts=False)
+
+    def fmr_grid(self, Uc, ncx, ncy, ncz, dxc, dyc, dzc, ci_lo, ci_hi, cj_lo, cj_hi, ck_lo, ck_hi, ratio, gamma,
+                 rho_floor, P_floor, init):
+        return self.api.FMRGrid3D(Uc, ncx, ncy, ncz, dxc, ci_lo, ci_hi, cj_lo, cj_hi, ck_lo, ck_hi, ratio, gamma,
+                                  rho_floor=rho_floor, P_floor=P_floor, dyc=dyc, dzc=dzc, init=init)
 
     def fill(self, U, nx, ny, nz, bc):
         (self.api.fill_ghost_3d_outflow if bc == "outflow" else self.api.fill_ghost_3d_periodic)(U, nx, ny, nz)

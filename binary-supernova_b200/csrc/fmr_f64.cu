@@ -787,6 +787,17 @@ extern "C" bsn_status bsn_solve_fmr_poisson_f64(bsn_ctx* ctx, const bsn_fmr2* g,
     return fmr_poisson(ctx, g, G, phi_c, phi_f);
 }
 
+extern "C" bsn_status bsn_prolong_scalar_trilinear_f64(bsn_ctx* ctx, const bsn_fmr2* g, const double* phi_c,
+                                                       double* phi_f) {
+    if (!ctx) return BSN_ERR_ARG;
+    if (!phi_c || !phi_f) return set_err(ctx, BSN_ERR_ARG, "null potential array");
+    Geo G;
+    BSN_TRY(make_geo(ctx, g, G));
+    long long n = (long long)g->nfx * g->nfy * g->nfz;
+    trilinear_kernel<<<grid1d(n, 256), 256, 0, ctx->stream>>>(G, phi_c, phi_f);
+    return launch_check(ctx, "trilinear_kernel");
+}
+
 extern "C" bsn_status bsn_fmr3d_run_steps(bsn_ctx* ctx, const bsn_fmr2* g, double cfl, int precision,
                                           int self_gravity, double G_grav, int n_steps, double t_end,
                                           double* t_inout, int* steps_done) {

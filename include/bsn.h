@@ -480,6 +480,9 @@ bsn_status bsn_cfl_dt_fmr3d_f64(bsn_ctx* ctx, const bsn_fmr2* G, double cfl, dou
 bsn_status bsn_restrict_density_to_coarse_f64(bsn_ctx* ctx, const bsn_fmr2* G);
 /* solve_fmr_poisson (src/fmr_gravity.jl:119-133): phi_c (ncx,ncy,ncz), phi_f (nfx,nfy,nfz) device */
 bsn_status bsn_solve_fmr_poisson_f64(bsn_ctx* ctx, const bsn_fmr2* G, double* phi_c, double* phi_f);
+/* _prolong_scalar_trilinear! (src/fmr_gravity.jl:70-106): phi_f (nfx,nfy,nfz)
+ * from phi_c (ncx,ncy,ncz), both device, column-major active grids */
+bsn_status bsn_prolong_scalar_trilinear_f64(bsn_ctx* ctx, const bsn_fmr2* G, const double* phi_c, double* phi_f);
 /* The FMR driver loop `dt = cfl_dt_fmr3d(G, cfl); dt = min(dt, t_end - t);
  * fmr3d_step!(G, dt; self_gravity, G_grav); t += dt` (src/fmr3d.jl:451-622)
  * run on the device: up to n_steps steps, t_end > 0 stops at t_end exactly

@@ -404,6 +404,12 @@ class FMRGrid:
     def restrict_density_to_coarse(self):
         lib().orc_restrict_density_to_coarse(C.byref(self.s))
 
+    def prolong_scalar_trilinear(self, phic):
+        s = self.s
+        phif = np.zeros((s.nfx, s.nfy, s.nfz), order="F")
+        lib().orc_prolong_scalar_trilinear(_p(phif), _p(np.asfortranarray(phic)), C.byref(s))
+        return phif
+
     def solve_poisson(self):
         s = self.s
         phic = np.zeros((s.ncx, s.ncy, s.ncz), order="F")

@@ -262,3 +262,42 @@ def test_single_slab_fp32_coupled_step_runs_the_fused_stage(orc):
         err = np.abs(G[(q,) + a] - U[(q,) + a]).sum() / np.abs(U[(q,) + a]).sum()
         assert err < 1e-6, (q, err)
     assert abs(bg[0].mass - bo[0].mass) <= 1e-9 * bo[0].mass
+
+
+def _blob(orc, n, nz, gamma):
+    U = orc.state(n, n, nz)
+    x = (np.arange(n) + 0.5) / n - 0.5
+    z = (np.arange(nz) + 0.5) / nz - 0.5
+    X, Y, Z = np.meshgrid(x, x, z, indexing="ij")
+    rho = 1.0 + 4.0 * np.exp(-(X ** 2 + 2 * Y ** 2 + Z ** 2) / 0.02)
+    vx, vy, vz = 0.1 * np.sin(2 * np.pi * Y), 0.1 * np.cos(2 * np.pi * Z), 0.05 * np.sin(2 * np.pi * X)
+    a = (slice(NG, NG + n), slice(NG, NG + n), slice(NG, NG + nz))
+    U[(0,) + a], U[(1,) + a], U[(2,) + a], U[(3,) + a] = rho, rho * vx, rho * vy, rho * vz
+    U[(4,) + a] = 1.0 / (gamma - 1.0) + 0.5 * rho * (vx ** 2 + vy ** 2 + vz ** 2)
+    orc.fill_ghost_3d_outflow(U)
+    return U
+
+
+@pytest.mark.parametrize("self_gravity", [False, True])
+def test_single_slab_fmr_step_bitwise_to_the_device_step(orc, self_gravity):
+    """The slab FMR step (bsn/shard_fmr.py) on one rank through the library's
+    operators -- coarse stages with the register faces, the owner's window,
+    fine subcycles, restriction and Berger-Colella correction -- equals the
+    fused bsn_fmr3d_step_f64 bit for bit (64^3 coarse, 64^3 fine patch)."""
+    import bsn
+    from bsn import shard, shard_fmr
+    n, dxc, g, r = 64, 1.0 / 32.0, 5.0 / 3.0, 2
+    box = (17, 48, 17, 48, 17, 48)
+    kw = dict(rho_floor=1e-6, P_floor=1e-5)
+    U0 = _blob(orc, n, n, g)
+    Gd = bsn.FMRGrid3D(dev(U0), n, n, n, dxc, *box, r, g, **kw)
+    slab = shard.Slab.split(n, n, n, 0, 1)
+    S = shard_fmr.SlabFMR(dev(U0), slab, dxc, *box, r, g, shard.DeviceOps(), Uf=Gd.Uf.clone(), **kw)
+    for _ in range(3):
+        dt = bsn.cfl_dt_fmr3d(Gd, 0.4)
+        assert S.cfl_dt(0.4) == dt
+        S.step(dt, self_gravity=self_gravity, G_grav=0.5)
+        bsn.fmr3d_step(Gd, dt, self_gravity=self_gravity, G_grav=0.5)
+    a = (slice(None),) + (slice(NG, -NG),) * 3
+    assert torch.equal(S.Uc[a], Gd.Uc[a])
+    assert torch.equal(S.G.Uf[a], Gd.Uf[a])

@@ -34,6 +34,29 @@ class OracleOps:
     def assign(U, V):
         U[...] = V
 
+    @staticmethod
+    def zeros(shape):
+        return np.zeros(shape)
+
+    def state(self, nx, ny, nz):
+        return self.orc.state(nx, ny, nz)
+
+    @staticmethod
+    def active(nx, ny, nz):
+        return np.zeros((nx, ny, nz), order="F")
+
+    def flux_arrays(self, nx, ny, nz):
+        return self.orc.flux_arrays(nx, ny, nz)
+
+    def rhs_fluxes(self, dU, Fx, Fy, Fz, U, nx, ny, nz, dx, dy, dz, gamma, bc, rho_floor, P_floor):
+        self.orc.euler3d_rhs(dU, Fx, Fy, Fz, U, dx, dy, dz, gamma, bc=bc, rho_floor=rho_floor, P_floor=P_floor,
+                             fill_ghosts=False)
+
+    def fmr_grid(self, Uc, ncx, ncy, ncz, dxc, dyc, dzc, ci_lo, ci_hi, cj_lo, cj_hi, ck_lo, ck_hi, ratio, gamma,
+                 rho_floor, P_floor, init):
+        return self.orc.FMRGrid(Uc, dxc, ci_lo, ci_hi, cj_lo, cj_hi, ck_lo, ck_hi, ratio, gamma, rho_floor=rho_floor,
+                                P_floor=P_floor, dyc=dyc, dzc=dzc, init=init)
+
     def fill(self, U, nx, ny, nz, bc):
         (self.orc.fill_ghost_3d_outflow if bc == "outflow" else self.orc.fill_ghost_3d_periodic)(U)
 
