@@ -713,7 +713,7 @@ struct F32Screen : F32Physics {
 
 namespace {
 const TileVariant kLearnedVariants[] = {{8, 8, 8, 256, 2}, {16, 8, 4, 256, 2}, {8, 8, 8, 256, 3}, {8, 8, 4, 128, 6},
-                                        {16, 16, 4, 256, 2}, {16, 8, 8, 256, 2}};
+                                        {16, 16, 4, 256, 2}, {16, 8, 8, 256, 2}, {16, 16, 8, 512, 1}};
 
 // One learned stage over every block in one launch (FMR levels and the
 // coupled loops, whose grids are mostly non-uniform).
@@ -734,6 +734,7 @@ bsn_status launch_learned(bsn_ctx* ctx, const f64::StageArgs& A0) {
     auto fl = tile::stage_kernel_list<tile::F32Learned, TX, TY, TZ, NT, MINB>;
     constexpr int smem_s = tile::smem_bytes<tile::F32Screen, TX, TY, TZ>();
     constexpr int smem_l = tile::smem_bytes<tile::F32Learned, TX, TY, TZ>() + tile::F32Learned::kExtraSmem(NT) + 16;
+    static_assert(smem_s <= 232448 && smem_l <= 232448, "tile's shared memory exceeds the per-CTA limit");
     static int occ[64] = {0}, sms[64] = {0};
     int dev = ctx->device & 63;
     if (!occ[dev]) {
@@ -789,6 +790,7 @@ bsn_status learned_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A
         case 3: return launch_learned<8, 8, 4, 128, 6>(ctx, A);
         case 4: return launch_learned<16, 16, 4, 256, 2>(ctx, A);
         case 5: return launch_learned<16, 8, 8, 256, 2>(ctx, A);
+        case 6: return launch_learned<16, 16, 8, 512, 1>(ctx, A);
         default: return set_err(ctx, BSN_ERR_ARG, "no learned tile variant %d", idx);
     }
 }
@@ -808,6 +810,7 @@ bsn_status learned_launch_batch_variant(bsn_ctx* ctx, int idx, const f64::StageB
         case 3: return tile::launch_batch<P, 8, 8, 4, 128, 6>(ctx, B, sm(tile::smem_bytes<P, 8, 8, 4>(), 128), nm);
         case 4: return tile::launch_batch<P, 16, 16, 4, 256, 2>(ctx, B, sm(tile::smem_bytes<P, 16, 16, 4>(), 256), nm);
         case 5: return tile::launch_batch<P, 16, 8, 8, 256, 2>(ctx, B, sm(tile::smem_bytes<P, 16, 8, 8>(), 256), nm);
+        case 6: return tile::launch_batch<P, 16, 16, 8, 512, 1>(ctx, B, sm(tile::smem_bytes<P, 16, 16, 8>(), 512), nm);
         default: return set_err(ctx, BSN_ERR_ARG, "no learned tile variant %d", idx);
     }
 }

@@ -12,10 +12,11 @@ namespace bsn {
 
 namespace {
 const TileVariant kF32Variants[] = {{8, 8, 8, 256, 3}, {16, 8, 4, 256, 3}, {8, 8, 4, 128, 6}, {16, 8, 8, 256, 2},
-                                     {16, 16, 4, 256, 2}};
+                                     {16, 16, 4, 256, 2}, {16, 16, 8, 512, 1}};
 
 template <class P, int TX, int TY, int TZ, int NT, int MINB>
 bsn_status launch_f32_policy(bsn_ctx* ctx, const f64::StageArgs& A) {
+    static_assert(tile::smem_bytes<P, TX, TY, TZ>() <= 200 * 1024, "tile's shared memory exceeds the per-CTA limit");
     bool tma_used = false;
     BSN_TRY((tile::launch_tma<P, TX, TY, TZ, NT, MINB>(ctx, A, "stage_kernel_f32_tma", &tma_used)));
     if (tma_used) return BSN_OK;
@@ -35,6 +36,7 @@ bsn_status launch_f32_batch(bsn_ctx* ctx, int idx, const f64::StageBatch& B) {
         case 2: return tile::launch_batch<P, 8, 8, 4, 128, 6>(ctx, B, tile::smem_bytes<P, 8, 8, 4>(), nm);
         case 3: return tile::launch_batch<P, 16, 8, 8, 256, 2>(ctx, B, tile::smem_bytes<P, 16, 8, 8>(), nm);
         case 4: return tile::launch_batch<P, 16, 16, 4, 256, 2>(ctx, B, tile::smem_bytes<P, 16, 16, 4>(), nm);
+        case 5: return tile::launch_batch<P, 16, 16, 8, 512, 1>(ctx, B, tile::smem_bytes<P, 16, 16, 8>(), nm);
         default: return set_err(ctx, BSN_ERR_ARG, "no FP32 tile variant %d", idx);
     }
 }
@@ -49,6 +51,7 @@ bsn_status f32_launch_variant(bsn_ctx* ctx, int idx, const f64::StageArgs& A) {
         case 2: return launch_f32<8, 8, 4, 128, 6>(ctx, A);
         case 3: return launch_f32<16, 8, 8, 256, 2>(ctx, A);
         case 4: return launch_f32<16, 16, 4, 256, 2>(ctx, A);
+        case 5: return launch_f32<16, 16, 8, 512, 1>(ctx, A);   // one CTA of 512 threads: a smaller halo share
         default: return set_err(ctx, BSN_ERR_ARG, "no FP32 tile variant %d", idx);
     }
 }
