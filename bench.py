@@ -1001,7 +1001,8 @@ def main():
     ap.add_argument("--no-tma", action="store_true",
                     help="stage the stencil tiles with the plain per-thread loader instead of TMA copies")
     ap.add_argument("--tile", type=int, default=-1,
-                    help="force this stage-kernel tile variant for both precisions (default: autotune)")
+                    help="force this stage-kernel tile variant (index into each precision's table, clamped to "
+                         "its last entry) for the Sedov and FMR workloads (default: autotune)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -1018,6 +1019,9 @@ def main():
     if args.workload in ("binary_nested", "polytrope_fmr"):
         import torch
         import bsn
+        if args.tile >= 0:
+            for p_ in ("f32", "f64", "learned"):
+                bsn.set_tile(p_, min(args.tile, bsn.tile_variants(p_) - 1))
         if args.workload == "binary_nested":
             paths = tuple(p_ for p_ in args.paths.split(",") if p_)
             steps, warmup = (1000, 0) if args.full else (args.steps, args.warmup)
