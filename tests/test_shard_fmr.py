@@ -35,22 +35,22 @@ def _smooth(orc):
     return U
 
 
-def _setup(orc, smooth=False):
+def _setup(orc, smooth=False, box=BOX):
     from test_shard import _initial
     U = _smooth(orc) if smooth else _initial(orc, N, NZG, 11, "outflow")
-    G = orc.FMRGrid(U.copy(order="F"), DXC, *BOX, RATIO, GAMMA, **KW)
+    G = orc.FMRGrid(U.copy(order="F"), DXC, *box, RATIO, GAMMA, **KW)
     return U, G
 
 
-def _slab_grid(orc, shard, shard_fmr, U0, Uf0, rank, world, ops, owner):
+def _slab_grid(orc, shard, shard_fmr, U0, Uf0, rank, world, ops, owner, box=BOX):
     slab = shard.Slab.split(N, N, NZG, rank, world)
     Us = orc.state(N, N, slab.nz)
     Us[...] = U0[:, :, :, slab.k0:slab.k0 + slab.nz + 2 * NG]
-    S = shard_fmr.SlabFMR(Us, slab, DXC, *BOX, RATIO, GAMMA, ops, owner=owner, Uf=Uf0, **KW)
+    S = shard_fmr.SlabFMR(Us, slab, DXC, *box, RATIO, GAMMA, ops, owner=owner, Uf=Uf0, **KW)
     return slab, S
 
 
-def _fmr_worker(rank, world, port, q, self_gravity, owner):
+def _fmr_worker(rank, world, port, q, self_gravity, owner, box=BOX):
     try:
         os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
         import torch.distributed as dist
@@ -61,10 +61,10 @@ def _fmr_worker(rank, world, port, q, self_gravity, owner):
         from bsn import shard, shard_fmr
         from test_shard import OracleOps, SGOps
         dist.init_process_group("gloo", rank=rank, world_size=world)
-        U0, G = _setup(orc, smooth=self_gravity)
+        U0, G = _setup(orc, smooth=self_gravity, box=box)
         Uf0 = G.Uf.copy(order="F")
         ops = SGOps(orc) if self_gravity else OracleOps(orc, DXC)
-        slab, S = _slab_grid(orc, shard, shard_fmr, U0, Uf0, rank, world, ops, owner)
+        slab, S = _slab_grid(orc, shard, shard_fmr, U0, Uf0, rank, world, ops, owner, box)
         # the undivided reference: the oracle's step, and (self-gravity) the
         # same slab code on one rank
         W = None
@@ -108,6 +108,15 @@ def _fmr_worker(rank, world, port, q, self_gravity, owner):
 def test_slab_fmr_step_matches_the_undivided_step(world, owner):
     from test_shard import _spawn
     for rank, ok, info in _spawn(_fmr_worker, world, (False, owner)):
+        assert ok, (rank, info)
+
+
+def test_slab_fmr_owner_outside_the_window():
+    """The owner holds none of the window's planes (rank 0 of 4 owns planes
+    1-8; the window of a box on planes 18-23 is 10-31): it still gathers,
+    steps the patch and sends the planes back."""
+    from test_shard import _spawn
+    for rank, ok, info in _spawn(_fmr_worker, 4, (False, 0, (4, 11, 6, 13, 18, 23))):
         assert ok, (rank, info)
 
 
