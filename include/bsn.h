@@ -182,10 +182,13 @@ bsn_status bsn_run_steps(bsn_ctx* ctx, double* U, int nx, int ny, int nz, double
                          double P_floor, int precision, int n_steps, double t_end,
                          double* t_inout, int* steps_done);
 /* Tile shape of the fused stage kernel: the library's autotuner times every
- * variant on the first stage of each grid and keeps the fastest.
+ * variant on the first stage of each grid and keeps the fastest, one choice
+ * per grid and driver loop (single stages, the uniform, coupled, nested,
+ * FMR and relaxation loops); a device loop's first call re-times its tiles
+ * after its first step (results are the same with every tile).
  * bsn_ctx_set_tile forces variant `variant` (-1: autotune again);
- * bsn_ctx_get_tile reports the choice for a grid as {tx, ty, tz, threads,
- * minimum CTAs per SM the kernel's registers are capped for}. */
+ * bsn_ctx_get_tile reports the latest choice for a grid as {tx, ty, tz,
+ * threads, minimum CTAs per SM the kernel's registers are capped for}. */
 /* Staging of the fused stage kernel's block and halos by TMA tensor copies
  * (cp.async.bulk.tensor into shared memory; possible where the tile divides
  * the grid, nx is even and no ghost buffer is involved) beside the plain
